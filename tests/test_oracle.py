@@ -1,0 +1,174 @@
+"""Pin the oracle restatement (oracle/zt_oracle.c) before trusting it.
+
+1. Byte-identical to the reference's own output on the committed golden fixtures (tests/golden, made by running
+   the reference itself).
+2. The known answers of the reference's self-test (tex_bench.c), re-run against the restatement.
+3. Byte-identical to the live reference library on fresh seeded inputs, where that library is built.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib
+from oracle_lib import BC1, BC3, BC4, BC5, BC7, chmask, psnr
+
+
+def _names(golden, prefix):
+    return sorted(k[len(prefix):] for k in golden if k.startswith(prefix))
+
+
+def test_golden_bcn(oracle, golden):
+    for name in _names(golden, "img/"):
+        img = golden["img/" + name]
+        for fmt in range(5):
+            got = oracle.bc_encode(img, fmt)
+            assert np.array_equal(got, golden[f"bc{fmt}/{name}"]), (name, fmt)
+
+
+def test_golden_astc(oracle, golden):
+    for name in _names(golden, "img/"):
+        assert np.array_equal(oracle.astc_encode(golden["img/" + name]), golden["astc/" + name]), name
+
+
+def test_golden_bc6h_and_float_mips(oracle, golden):
+    for name in _names(golden, "himg/"):
+        img = golden["himg/" + name]
+        assert np.array_equal(oracle.bc6h_encode(img), golden["bc6h/" + name]), name
+        assert np.array_equal(oracle.mip_next_f(img).view(np.uint32), golden["mipf/" + name].view(np.uint32)), name
+
+
+def test_golden_mips(oracle, golden):
+    for name in _names(golden, "img/"):
+        img = golden["img/" + name]
+        assert np.array_equal(oracle.mip_next(img, 0), golden["mip0/" + name]), name
+        assert np.array_equal(oracle.mip_next(img, 1), golden["mip1/" + name]), name
+
+
+def test_srgb_tables_match_reference_constants(oracle, golden):
+    lin, thr = oracle.srgb_tables()
+    assert np.array_equal(lin.view(np.uint32), golden["srgb_lin"].view(np.uint32))
+    assert np.array_equal(thr.view(np.uint32), golden["srgb_thr"].view(np.uint32))
+
+
+# ---------------------------------------------------------------- tex_bench.c known answers
+def test_half_float_known_answers(oracle):
+    """tex_bench.c:47-48."""
+    for h in range(0, 0x7BFF + 1, 7):
+        assert oracle.f2h(oracle.h2f(h)) == h
+    assert oracle.f2h(oracle.h2f(0x7BFF)) == 0x7BFF
+    assert oracle.f2h(-1.0) == 0 and oracle.f2h(1e9) == 0x7BFF
+    assert oracle.f2h(1.0) == 0x3C00 and oracle.f2h(1.0 + 1.0 / 4096) == 0x3C00
+
+
+def test_mip_known_answers(oracle):
+    """tex_bench.c:87-100."""
+    assert oracle.mip_levels(1, 1) == 1 and oracle.mip_levels(256, 128) == 9 and oracle.mip_levels(5, 3) == 3
+    bw = np.array([[[0, 0, 0, 255], [255, 255, 255, 255]], [[0, 0, 0, 255], [255, 255, 255, 255]]], np.uint8)
+    m = oracle.mip_next(bw, 0)
+    assert m[0, 0, 0] == 128 and m[0, 0, 3] == 255
+    m = oracle.mip_next(bw, 1)
+    assert m[0, 0, 0] == 188 and m[0, 0, 1] == 188 and m[0, 0, 3] == 255
+    for v in range(256):
+        assert oracle.mip_next(np.full((2, 2, 4), v, np.uint8), 1)[0, 0, 0] == v
+    odd = np.full((3, 5, 4), 77, np.uint8)
+    m2 = oracle.mip_next(odd, 1)
+    assert m2.shape == (1, 2, 4) and m2[0, 0, 0] == 77 and m2[0, 1, 3] == 77
+    fl = np.array([1, 2, 3, 4, 3, 2, 1, 0, 5, 5, 5, 5, 7, 7, 7, 7], np.float32).reshape(2, 2, 4)
+    fo = oracle.mip_next_f(fl)
+    assert fo[0, 0, 0] == 4 and fo[0, 0, 3] == 4
+
+
+def test_astc_ise_roundtrip(oracle):
+    """tex_bench.c:104-117: every range kind, n = 1..16."""
+    import ctypes
+    rng = np.random.default_rng(1)
+    levels = [2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256]
+    for ri, lv in enumerate(levels):
+        for n in range(1, 17):
+            v = rng.integers(0, lv, 16).astype(np.int32)
+            got = np.zeros(16, np.int32)
+            assert oracle._ise_roundtrip(ri, n, v.ctypes.data, got.ctypes.data) >= 0, (ri, n)
+    del ctypes
+
+
+def test_astc_partition_checksum(oracle):
+    """tex_bench.c:118-121: FNV-1a over the 1024 two-partition patterns."""
+    h = 2166136261
+    for sd in range(1024):
+        for i in range(16):
+            h ^= oracle.astc_partition(sd, i & 3, i >> 2, 2)
+            h = (h * 16777619) & 0xFFFFFFFF
+    assert h == 0x5D5FC459
+
+
+def test_astc_void_extent(oracle):
+    """tex_bench.c:123-125."""
+    ve = np.array([0xFC, 0xFD, 0xFF, 0xFF, 0xFF, 0xFF, 0xFF, 0xFF, 0x00, 0x40, 0x00, 0x80, 0x00, 0xC0, 0xFF, 0xFF], np.uint8)
+    vo = oracle.astc_decode(ve, 4, 4)
+    assert tuple(vo[0, 0]) == (0x40, 0x80, 0xC0, 0xFF)
+
+
+def test_selftest_quality_floors(oracle, golden):
+    """tex_bench.c:155-177 at rdo 0: PSNR floors, BC7 beats BC3, BC1 never transparent, 1x1 within 4."""
+    img = golden["img/selftest67x45"]
+    h, w = img.shape[:2]
+    q = {}
+    for fmt in range(5):
+        dec = oracle.bc_decode(oracle.bc_encode(img, fmt), w, h, fmt)
+        q[fmt] = psnr(img, dec, chmask(fmt))
+        assert q[fmt] > 32, (fmt, q[fmt])
+        if fmt == BC1:
+            assert np.all(dec[..., 3] == 255)
+    assert q[BC7] > q[BC3]
+    one = np.array([[[10, 200, 30, 255]]], np.uint8)
+    for fmt in range(5):
+        dec = oracle.bc_decode(oracle.bc_encode(one, fmt), 1, 1, fmt)
+        for c in range(4):
+            if (chmask(fmt) >> c) & 1:
+                assert abs(int(dec[0, 0, c]) - int(one[0, 0, c])) <= 4
+
+
+def test_selftest_bc7_mode5_and_hdr(oracle, golden):
+    """tex_bench.c:51-84: mode 5 chosen on independent alpha; BC6H mean relative error < 0.08."""
+    img = golden["img/mode5_64x64"]
+    bc = oracle.bc_encode(img, BC7)
+    assert np.sum((bc[0::16] & 0x3F) == 0x20) > 0
+    assert psnr(img, oracle.bc_decode(bc, 64, 64, BC7), 15) > 30
+    hdr = golden["himg/hdr37x21"]
+    dec = oracle.bc6h_decode(oracle.bc6h_encode(hdr), 37, 21)
+    df = np.vectorize(oracle.h2f)(dec[..., :3]).astype(np.float64)
+    a = hdr[..., :3].astype(np.float64)
+    assert np.mean(np.abs(a - df) / (a + 0.01)) < 0.08 and dec[0, 0, 3] == 0x3C00
+
+
+def test_selftest_astc_quality(oracle, golden):
+    """tex_bench.c:127-141."""
+    for k, floor in ((0, 41), (1, 26)):
+        img = golden[f"img/astc64x48_k{k}"]
+        assert psnr(img, oracle.astc_decode(oracle.astc_encode(img), 64, 48), 15) > floor
+
+
+# ---------------------------------------------------------------- live reference
+@pytest.mark.parametrize("seed", [11, 12])
+def test_port_matches_reference_live(oracle, reference, seed):
+    rng = np.random.default_rng(seed)
+    for _ in range(4):
+        w, h = int(rng.integers(1, 90)), int(rng.integers(1, 90))
+        img = rng.integers(0, 256, (h, w, 4), dtype=np.uint8)
+        img[: h // 2] = np.sort(img[: h // 2], axis=1)  # smooth half, noisy half
+        if rng.random() < 0.5:
+            img[..., 3] = 255
+        for fmt in (BC1, BC3, BC4, BC5, BC7):
+            assert np.array_equal(oracle.bc_encode(img, fmt), reference.bc_encode(img, fmt)), (fmt, w, h)
+        assert np.array_equal(oracle.astc_encode(img), reference.astc_encode(img)), (w, h)
+        hdr = (2.0 ** rng.uniform(-12, 14, (h, w, 4))).astype(np.float32)
+        assert np.array_equal(oracle.bc6h_encode(hdr), reference.bc6h_encode(hdr)), (w, h)
+
+
+def test_reference_band_parallel_matches_single_call(reference):
+    """The all-cores CPU baseline (8-block-row bands, viewer.cpp:455-471) gives the single-call bytes at rdo 0."""
+    rng = np.random.default_rng(5)
+    img = rng.integers(0, 256, (75, 61, 4), dtype=np.uint8)
+    for fmt in (BC1, BC7):
+        assert np.array_equal(reference.bc_encode(img, fmt, threads=4), reference.bc_encode(img, fmt))
+    assert np.array_equal(reference.astc_encode(img, threads=3), reference.astc_encode(img))
+    assert oracle_lib.bc_size(61, 75, BC7) == reference.bc_encode(img, BC7).size
