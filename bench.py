@@ -1,0 +1,313 @@
+#!/usr/bin/env python
+"""Benchmark: BC7 (and BC1) encode Mpix/s on B200 against the reference CPU encoder.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Headline workload (`value`): BC7 of a 2048x2048 RGBA8 texture (colour gradients + 4-octave value noise + 20 hard
+rectangles, alpha from 2-octave noise thresholded at 30%), seeded synthetic content. A step encodes one texture
+through the device API; steps cycle over a ring of distinct textures whose total size exceeds the 126 MB L2, so no
+step reads a texture still resident in L2. Inputs are in HBM when the timed region starts. With N GPUs (torchrun)
+every rank encodes its own ring (weak scaling, no collective on the data path); value = all ranks' pixels / max time.
+
+`e2e` is the same workload through the synchronous host C ABI (zap_tex_cuda_bc_encode): pinned host texture in,
+host->device copy, encode, device->host copy of the blocks, every step.
+`roofline` is the dominant kernel's algorithmic bytes per launch / its CUDA-event duration, against the measured HBM
+copy bandwidth (the encoders are compute-bound, so `alu` beside it gives the issue-rate view from ncu).
+`cpu_baseline` is the reference's own encoder (oracle/_ref, built from zap_tex.h) on this host's cores, using the
+reference's band-parallel scheme; `--impl reference` times only that, on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "BC1/BC7 encode Mpix/s on 1 B200 at ref PSNR; batched vs plain launch; vs CPU"
+W, H = 2048, 2048
+WORKLOAD = "bc7 2048x2048 rgba8, colour gradients + value noise + rectangles, noise alpha (config 1)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
+    return p.parse_args()
+
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = [r for r in self.rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def reference_cpu(img_np, fmt, reps=3):
+    """Best-of-reps wall time of the reference encoder on all host threads (viewer.cpp band scheme)."""
+    import oracle_lib
+    ref = oracle_lib.reference()
+    if ref is None:
+        return None
+    threads = os.cpu_count() or 1
+    best = float("inf")
+    out = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        out = ref.bc_encode(img_np, fmt, threads=threads)
+        best = min(best, time.perf_counter() - t0)
+    return {"seconds": best, "threads": threads, "out": out}
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the reference's own CPU encoder, all host threads, same workload and metric."""
+    if rank != 0:
+        return
+    import oracle_lib
+    import zap_b200.synth as S
+    ref = oracle_lib.reference()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libzapref.so is not built (reference tree absent)"}))
+        return
+    img = S.colour_texture(W, H, seed=100, alpha="noise").numpy()
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        ref.bc_encode(img, 4, threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ref.bc_encode(img, 4, threads=threads)
+    dt = time.perf_counter() - t0
+    v = args.steps * W * H / 1e6 / dt
+    line = {"metric": METRIC, "value": v, "unit": "Mpix/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "parallelism": f"{threads} host threads, 8-block-row bands"},
+            "cpu_baseline": {"value": v, "unit": "Mpix/s", "cores": threads, "kind": "reference",
+                             "sample": f"full {W}x{H} texture per step, zap_bc_encode on bands (zap_tex.h at -O2)"},
+            "e2e": {"value": v, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def time_device(fn, steps, warmup, world):
+    import torch
+    for k in range(warmup):
+        fn(k)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(steps):
+        fn(k)
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    return e0.elapsed_time(e1)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    import numpy as np
+    import torch
+
+    import zap_b200
+    import zap_b200.synth as S
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ring = 10  # 10 x 16 MB > 126 MB L2
+    texs = [S.colour_texture(W, H, seed=100 + 1000 * rank + k, alpha="noise", device=dev) for k in range(ring)]
+    outs = [torch.empty(zap_b200.bc_size(W, H, zap_b200.BC7), dtype=torch.uint8, device=dev) for _ in range(ring)]
+    torch.cuda.synchronize()
+
+    def step(k):
+        zap_b200.bc_encode_dev(texs[k % ring], zap_b200.BC7, out=outs[k % ring])
+
+    for k in range(max(3, args.warmup)):
+        step(k)
+    torch.cuda.synchronize()
+    zap_b200.trace(True)
+    with ClockSampler(local) as clocks:
+        ms = time_device(step, args.steps, 0, world)
+    rep = zap_b200.trace_report()
+    zap_b200.trace(False)
+    ms = max_over_ranks(ms, world)
+    mpix = W * H / 1e6
+    value = world * args.steps * mpix / (ms / 1e3)
+    launches = sum(v[0] for v in rep.values())
+
+    # dominant kernel roofline: 64 B of texels read + 16 B of block written per 4x4 block processed
+    dom = max(rep.items(), key=lambda kv: kv[1][1])
+    name, (n, tot_ms, units) = dom
+    avg_ms = tot_ms / max(1, n)
+    alg_bytes = units / max(1, n) * 80.0
+    hbm, peak_kind = peaks()
+    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(name)
+    roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": traffic, "peak_source": peak_kind, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
+                "kernels": {k: {"launches": v[0], "ms": v[1], "units": v[2], "share": v[1] / sum(x[1] for x in rep.values())}
+                            for k, v in rep.items()}}
+
+    line = {"metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "l2": f"inputs larger than L2: ring of {ring} distinct {W}x{H} textures",
+                       "parallelism": "independent replicas" if world > 1 else "1 gpu"},
+            "roofline": roofline, "gpu_launches": launches, "clocks": clocks.summary()}
+
+    if rank == 0:
+        # e2e: host C ABI, pinned host memory, copies inside the timed region
+        host_in = torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True)
+        host_in.copy_(texs[0].cpu())
+        host_out = torch.empty(zap_b200.bc_size(W, H, zap_b200.BC7), dtype=torch.uint8, pin_memory=True)
+        hin, hout = host_in.numpy(), host_out.numpy()
+        for _ in range(3):
+            zap_b200.bc_encode(hin, zap_b200.BC7, out=hout)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            zap_b200.bc_encode(hin, zap_b200.BC7, out=hout)
+        e2e_s = time.perf_counter() - t0
+        line["e2e"] = {"value": args.steps * mpix / e2e_s, "unit": "Mpix/s", "h2d_bytes_per_step": W * H * 4,
+                       "d2h_bytes_per_step": int(hout.size), "api": "zap_tex_cuda_bc_encode (host pointers)"}
+        # reference CPU on the same texture; parity of the GPU output against it
+        cpu = reference_cpu(hin, zap_b200.BC7, reps=2) if world == 1 else None
+        if cpu is not None:
+            line["cpu_baseline"] = {"value": mpix / cpu["seconds"], "unit": "Mpix/s", "cores": cpu["threads"], "kind": "reference",
+                                    "sample": f"full {W}x{H} texture, best of 2, 8-block-row bands on all host threads"}
+            same = np.mean(np.all(hout.reshape(-1, 16) == cpu["out"].reshape(-1, 16), axis=1))
+            line["parity"] = {"identical_blocks": float(same)}
+        if not args.no_extra:
+            line["extra"] = extra_workloads(args, dev)
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def extra_workloads(args, dev):
+    """Secondary figures: BC1 (config 0 and 2048^2), BC4 R8 / BC5 RG8 (config 1), BC6H / ASTC (config 3)."""
+    import torch
+
+    import zap_b200
+    import zap_b200.synth as S
+    res = {}
+    steps = max(5, args.steps // 2)
+
+    def bench(name, make, fmt, npix, ring, alg_bytes_per_px, enc=None):
+        texs = [make(k) for k in range(ring)]
+        outs = [None] * ring
+        f = enc or (lambda t, o: zap_b200.bc_encode_dev(t, fmt, out=o))
+
+        def step(k):
+            outs[k % ring] = f(texs[k % ring], outs[k % ring])
+        for k in range(3):
+            step(k)
+        ms = time_device(step, steps, 0, 1)
+        mps = steps * npix / 1e6 / (ms / 1e3)
+        res[name] = {"Mpix_s": mps, "ms_per_encode": ms / steps, "GB_s_algorithmic": mps * 1e6 * alg_bytes_per_px / 1e9}
+
+    bench("bc1_512x512_config0", lambda k: S.colour_texture(512, 512, seed=k, device=dev), zap_b200.BC1, 512 * 512, 64, 4.5)
+    bench("bc1_2048x2048", lambda k: S.colour_texture(2048, 2048, seed=k, device=dev), zap_b200.BC1, 2048 * 2048, 10, 4.5)
+    bench("bc4_2048x2048_r8", lambda k: S.colour_texture(2048, 2048, seed=k, device=dev)[..., :1].contiguous(), zap_b200.BC4,
+          2048 * 2048, 40, 1.5)
+    bench("bc5_2048x2048_rg8", lambda k: S.normal_map(2048, 2048, seed=k, device=dev), zap_b200.BC5, 2048 * 2048, 20, 3.0)
+    bench("astc4x4_2048x2048", lambda k: S.colour_texture(2048, 2048, seed=k, alpha="noise", device=dev), zap_b200.ASTC4X4,
+          2048 * 2048, 10, 5.0)
+    bench("bc6h_2048x2048_rgb16f", lambda k: S.hdr_texture(2048, 2048, seed=k, device=dev), None, 2048 * 2048, 6, 7.0,
+          enc=lambda t, o: zap_b200.bc6h_encode_dev(t, out=o))
+    return res
+
+
+if __name__ == "__main__":
+    main()

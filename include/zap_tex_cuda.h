@@ -1,0 +1,118 @@
+/* zap_tex_cuda.h - B200 (sm_100a) drop-in for the zap_tex.h texture encoders.
+ *
+ * A thin C ABI over hand-written CUDA kernels. Every entry point keeps the argument list and the output bytes
+ * of the zap_tex.h function it replaces (zap 1.3.0; cited as zap_tex.h:line), adds a context as the first
+ * argument, and returns an int status (ZTC_OK = 0) where the reference returns void. Block order and block
+ * layout are the reference's: raster order over the ceil(w/4) x ceil(h/4) block grid, partial edge blocks
+ * replicating the last column / row.
+ *
+ * Host-pointer functions are synchronous, like the reference: they return once `out` holds the blocks.
+ * `_dev` functions take device pointers and enqueue on `stream` (a cudaStream_t passed as void *; NULL = the
+ * legacy default stream); they return after the launch, with launch errors only.
+ *
+ * No CPU fallback exists: without a usable CUDA device every call returns ZTC_ERR_NO_DEVICE.
+ * A context is not thread-safe; use one per host thread (ctx == NULL selects a per-device default context,
+ * guarded by a lock).
+ */
+#ifndef ZAP_TEX_CUDA_H
+#define ZAP_TEX_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZAP_TEX_CUDA_VERSION 10000 /* 1.0.0 */
+
+#if defined(__GNUC__)
+#define ZTC_API __attribute__((visibility("default")))
+#else
+#define ZTC_API
+#endif
+
+typedef enum zap_tex_cuda_status {
+    ZTC_OK = 0,
+    ZTC_ERR_INVALID_ARG = -1, /* null pointer, w or h < 1, stride too small, size beyond the limit */
+    ZTC_ERR_UNSUPPORTED = -2, /* rdo != 0 (rate-distortion mode), or a format the call does not take */
+    ZTC_ERR_CUDA = -3,        /* a CUDA runtime error; zap_tex_cuda_last_error() has the text */
+    ZTC_ERR_NO_MEMORY = -4,   /* device or pinned-host allocation failed */
+    ZTC_ERR_TIMEOUT = -5,     /* a bounded device-side wait gave up (batched queue) */
+    ZTC_ERR_NO_DEVICE = -6    /* no CUDA device, or the device is not sm_100 */
+} zap_tex_cuda_status;
+
+/* Formats: 0..4 are zap_bc_format (zap_tex.h:32); BC6H and ASTC 4x4 have ids for the batched API. */
+enum { ZTC_BC1 = 0, ZTC_BC3 = 1, ZTC_BC4 = 2, ZTC_BC5 = 3, ZTC_BC7 = 4, ZTC_BC6H = 5, ZTC_ASTC4X4 = 6 };
+
+typedef struct zap_tex_cuda_ctx zap_tex_cuda_ctx;
+
+/* ---------------------------------------------------------------- library and context */
+ZTC_API int zap_tex_cuda_version(void);
+ZTC_API const char *zap_tex_cuda_status_string(int status);
+/* the last error message of the calling thread ("" when none) */
+ZTC_API const char *zap_tex_cuda_last_error(void);
+/* creates a context on `device` (its own streams, scratch arena, constant tables); no reference counterpart */
+ZTC_API int zap_tex_cuda_create(int device, zap_tex_cuda_ctx **out);
+ZTC_API int zap_tex_cuda_destroy(zap_tex_cuda_ctx *ctx);
+/* pre-sizes the context's device scratch arena so later _dev calls allocate nothing (e.g. before stream capture) */
+ZTC_API int zap_tex_cuda_reserve(zap_tex_cuda_ctx *ctx, size_t scratch_bytes);
+
+/* Kernel tracing, no reference counterpart (the reference times one call with timespec_get, tex_bench.c:208-210).
+   enable != 0 starts recording CUDA events around every kernel launch (process-wide, off by default);
+   report writes "name launches total_ms" lines into buf, clears the record, and returns the text length. */
+ZTC_API int zap_tex_cuda_trace_enable(int enable);
+ZTC_API int zap_tex_cuda_trace_report(char *buf, size_t cap);
+
+/* ---------------------------------------------------------------- sizes (zap_tex.h:34-37, :1435-1439) */
+ZTC_API size_t zap_tex_cuda_block_bytes(int fmt);          /* replaces zap_bc_block_bytes, zap_tex.h:34 */
+ZTC_API size_t zap_tex_cuda_bc_size(int w, int h, int fmt); /* replaces zap_bc_size, zap_tex.h:35-37 (BC6H/ASTC: 16 B/block) */
+ZTC_API int zap_tex_cuda_mip_levels(int w, int h);          /* replaces zap_mip_levels, zap_tex.h:1435-1439 */
+
+/* ---------------------------------------------------------------- drop-in encoders, host memory */
+/* replaces zap_bc_encode (zap_tex.h:1474); rdo must be 0 (ZTC_ERR_UNSUPPORTED otherwise) */
+ZTC_API int zap_tex_cuda_bc_encode(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo,
+                           void *out);
+/* replaces zap_bc6h_encode (zap_tex.h:946); stride in floats per row */
+ZTC_API int zap_tex_cuda_bc6h_encode(zap_tex_cuda_ctx *ctx, const float *rgba, int w, int h, size_t stride, void *out);
+/* replaces zap_astc_encode (zap_tex.h:1291) */
+ZTC_API int zap_tex_cuda_astc_encode(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, void *out);
+/* replaces zap_mip_next (zap_tex.h:1442) */
+ZTC_API int zap_tex_cuda_mip_next(zap_tex_cuda_ctx *ctx, const uint8_t *src, int w, int h, size_t stride, int srgb, uint8_t *dst,
+                          size_t dst_stride);
+/* replaces zap_mip_next_f (zap_tex.h:1460); strides in floats */
+ZTC_API int zap_tex_cuda_mip_next_f(zap_tex_cuda_ctx *ctx, const float *src, int w, int h, size_t stride, float *dst,
+                            size_t dst_stride);
+
+/* ---------------------------------------------------------------- device memory, asynchronous */
+ZTC_API int zap_tex_cuda_bc_encode_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo,
+                               void *out, void *stream);
+ZTC_API int zap_tex_cuda_bc6h_encode_dev(zap_tex_cuda_ctx *ctx, const float *rgba, int w, int h, size_t stride, void *out,
+                                 void *stream);
+ZTC_API int zap_tex_cuda_astc_encode_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, void *out,
+                                 void *stream);
+ZTC_API int zap_tex_cuda_mip_next_dev(zap_tex_cuda_ctx *ctx, const uint8_t *src, int w, int h, size_t stride, int srgb, uint8_t *dst,
+                              size_t dst_stride, void *stream);
+ZTC_API int zap_tex_cuda_mip_next_f_dev(zap_tex_cuda_ctx *ctx, const float *src, int w, int h, size_t stride, float *dst,
+                                size_t dst_stride, void *stream);
+
+/* Narrow inputs, no reference counterpart: the reference takes RGBA8 (zap_tex.h:1474) and RGBA f32 (:946); these
+   read 1-, 2- or 4-channel uint8 texels (channels absent from the source read as 0, alpha as 255) or RGB(A) half
+   floats, and produce the bytes the reference produces for the same texels widened to its input type.
+   stride: bytes per row for uint8, halfs per row for half. */
+ZTC_API int zap_tex_cuda_bc_encode_u8_dev(zap_tex_cuda_ctx *ctx, const uint8_t *src, int channels, int w, int h, size_t stride,
+                                  int fmt, void *out, void *stream);
+ZTC_API int zap_tex_cuda_bc6h_encode_half_dev(zap_tex_cuda_ctx *ctx, const uint16_t *src, int channels, int w, int h, size_t stride,
+                                      void *out, void *stream);
+
+/* Full mip chain, no single reference counterpart: the caller loop of zap.c:336-342 (zap_mip_next per level).
+   Writes levels 1..levels-1 of `rgba` into `dst` tightly packed (level l at max(1, w>>l) x max(1, h>>l),
+   row pitch 4 * width), largest first. dst must hold zap_tex_cuda_mip_chain_bytes(w, h) bytes. */
+ZTC_API size_t zap_tex_cuda_mip_chain_bytes(int w, int h);
+ZTC_API int zap_tex_cuda_mip_chain_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int srgb,
+                               uint8_t *dst, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZAP_TEX_CUDA_H */

@@ -1,0 +1,196 @@
+"""zap_b200 - B200 (sm_100a) texture block encoders behind zap_tex.h's API (zap 1.3.0).
+
+Host functions mirror zap_tex.h one for one and take / return numpy arrays (HxWx4, row-major):
+    bc_encode(rgba, fmt, rdo=0)   -> zap_bc_encode   (zap_tex.h:1474)
+    bc6h_encode(rgba_f32)         -> zap_bc6h_encode (zap_tex.h:946)
+    astc_encode(rgba)             -> zap_astc_encode (zap_tex.h:1291)
+    mip_next(rgba, srgb)          -> zap_mip_next    (zap_tex.h:1442)
+    mip_next_f(rgba_f32)          -> zap_mip_next_f  (zap_tex.h:1460)
+    bc_size / mip_levels / block_bytes
+`*_dev` variants take torch CUDA tensors and return CUDA tensors (asynchronous on the current torch stream).
+All work runs in the CUDA library (zap_b200/lib/libzap_tex_cuda.so); there is no CPU fallback.
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import ZapTexError, build, check, load
+
+BC1, BC3, BC4, BC5, BC7, BC6H, ASTC4X4 = range(7)
+FORMAT_NAMES = {BC1: "bc1", BC3: "bc3", BC4: "bc4", BC5: "bc5", BC7: "bc7", BC6H: "bc6h", ASTC4X4: "astc4x4"}
+
+__all__ = ["BC1", "BC3", "BC4", "BC5", "BC7", "BC6H", "ASTC4X4", "ZapTexError", "build", "load", "bc_size", "block_bytes",
+           "mip_levels", "bc_encode", "bc6h_encode", "astc_encode", "mip_next", "mip_next_f", "bc_encode_dev",
+           "bc6h_encode_dev", "astc_encode_dev", "mip_next_dev", "mip_next_f_dev", "mip_chain_dev"]
+
+
+def trace(enable=True):
+    """Start (or stop) recording CUDA events around every kernel launch of the library."""
+    check(load().zap_tex_cuda_trace_enable(int(enable)), "trace")
+
+
+def trace_report():
+    """{kernel name: (launches, total ms, units processed)} since trace() was enabled; clears the record.
+    Units are 4x4 blocks for encoders (for the second BC7 / ASTC kernels: the blocks on their work list) and output
+    texels for mips."""
+    buf = C.create_string_buffer(1 << 16)
+    load().zap_tex_cuda_trace_report(buf, len(buf))
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, n, ms, units = line.split()
+        out[name] = (int(n), float(ms), int(units))
+    return out
+
+
+def block_bytes(fmt):
+    return int(load().zap_tex_cuda_block_bytes(fmt))
+
+
+def bc_size(w, h, fmt):
+    return int(load().zap_tex_cuda_bc_size(w, h, fmt))
+
+
+def mip_levels(w, h):
+    return int(load().zap_tex_cuda_mip_levels(w, h))
+
+
+def _img(a, dtype):
+    a = np.asarray(a)
+    if a.dtype != dtype or a.ndim != 3 or a.shape[2] != 4:
+        raise ValueError(f"expected an HxWx4 {np.dtype(dtype).name} image, got {a.shape} {a.dtype}")
+    if not a.flags.c_contiguous and a.strides[1:] != (4 * a.itemsize, a.itemsize):
+        a = np.ascontiguousarray(a)
+    return a, a.shape[1], a.shape[0], a.strides[0]
+
+
+# ---------------------------------------------------------------- host memory (synchronous drop-ins)
+def _out(out, n):
+    if out is None:
+        return np.empty(n, np.uint8)
+    if out.dtype != np.uint8 or out.size < n or not out.flags.c_contiguous:
+        raise ValueError(f"out must be a contiguous uint8 array of at least {n} bytes")
+    return out
+
+
+def bc_encode(rgba, fmt, rdo=0.0, ctx=None, out=None):
+    a, w, h, stride = _img(rgba, np.uint8)
+    out = _out(out, bc_size(w, h, fmt))
+    check(load().zap_tex_cuda_bc_encode(ctx, a.ctypes.data, w, h, stride, fmt, float(rdo), out.ctypes.data), "bc_encode")
+    return out
+
+
+def bc6h_encode(rgba, ctx=None, out=None):
+    a, w, h, stride = _img(rgba, np.float32)
+    out = _out(out, bc_size(w, h, BC6H))
+    check(load().zap_tex_cuda_bc6h_encode(ctx, a.ctypes.data, w, h, stride // 4, out.ctypes.data), "bc6h_encode")
+    return out
+
+
+def astc_encode(rgba, ctx=None, out=None):
+    a, w, h, stride = _img(rgba, np.uint8)
+    out = _out(out, bc_size(w, h, ASTC4X4))
+    check(load().zap_tex_cuda_astc_encode(ctx, a.ctypes.data, w, h, stride, out.ctypes.data), "astc_encode")
+    return out
+
+
+def mip_next(rgba, srgb, ctx=None):
+    a, w, h, stride = _img(rgba, np.uint8)
+    nw, nh = max(1, w // 2), max(1, h // 2)
+    out = np.empty((nh, nw, 4), np.uint8)
+    check(load().zap_tex_cuda_mip_next(ctx, a.ctypes.data, w, h, stride, int(srgb), out.ctypes.data, nw * 4), "mip_next")
+    return out
+
+
+def mip_next_f(rgba, ctx=None):
+    a, w, h, stride = _img(rgba, np.float32)
+    nw, nh = max(1, w // 2), max(1, h // 2)
+    out = np.empty((nh, nw, 4), np.float32)
+    check(load().zap_tex_cuda_mip_next_f(ctx, a.ctypes.data, w, h, stride // 4, out.ctypes.data, nw * 4), "mip_next_f")
+    return out
+
+
+# ---------------------------------------------------------------- device memory (torch CUDA tensors)
+def _stream(stream):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _dev_img(t, channels=(4,)):
+    if not t.is_cuda or t.dim() != 3 or t.shape[2] not in channels or t.stride(2) != 1 or t.stride(1) != t.shape[2]:
+        raise ValueError(f"expected an HxWxC CUDA tensor with C in {channels} and packed rows, got {tuple(t.shape)}")
+    return t.shape[1], t.shape[0], t.stride(0)
+
+
+def bc_encode_dev(t, fmt, out=None, stream=None, ctx=None):
+    """t: HxWxC uint8 CUDA tensor, C in (1, 2, 4); C < 4 reads missing channels as 0 and alpha as 255."""
+    import torch
+    if t.dtype != torch.uint8:
+        raise ValueError("expected uint8")
+    w, h, stride = _dev_img(t, (1, 2, 4))
+    if out is None:
+        out = torch.empty(bc_size(w, h, fmt), dtype=torch.uint8, device=t.device)
+    check(load().zap_tex_cuda_bc_encode_u8_dev(ctx, t.data_ptr(), t.shape[2], w, h, stride, fmt, out.data_ptr(), _stream(stream)),
+          "bc_encode_dev")
+    return out
+
+
+def astc_encode_dev(t, out=None, stream=None, ctx=None):
+    return bc_encode_dev(t, ASTC4X4, out, stream, ctx)
+
+
+def bc6h_encode_dev(t, out=None, stream=None, ctx=None):
+    """t: HxWx4 float32, or HxWx3 / HxWx4 float16 CUDA tensor."""
+    import torch
+    if t.dtype == torch.float32:
+        w, h, stride = _dev_img(t, (4,))
+    elif t.dtype == torch.float16:
+        w, h, stride = _dev_img(t, (3, 4))
+    else:
+        raise ValueError("expected float32 RGBA or float16 RGB(A)")
+    if out is None:
+        out = torch.empty(bc_size(w, h, BC6H), dtype=torch.uint8, device=t.device)
+    lib = load()
+    if t.dtype == torch.float32:
+        st = lib.zap_tex_cuda_bc6h_encode_dev(ctx, t.data_ptr(), w, h, stride, out.data_ptr(), _stream(stream))
+    else:
+        st = lib.zap_tex_cuda_bc6h_encode_half_dev(ctx, t.data_ptr(), t.shape[2], w, h, stride, out.data_ptr(), _stream(stream))
+    check(st, "bc6h_encode_dev")
+    return out
+
+
+def mip_next_dev(t, srgb, out=None, stream=None, ctx=None):
+    import torch
+    w, h, stride = _dev_img(t, (4,))
+    nw, nh = max(1, w // 2), max(1, h // 2)
+    if out is None:
+        out = torch.empty((nh, nw, 4), dtype=torch.uint8, device=t.device)
+    check(load().zap_tex_cuda_mip_next_dev(ctx, t.data_ptr(), w, h, stride, int(srgb), out.data_ptr(), out.stride(0), _stream(stream)),
+          "mip_next_dev")
+    return out
+
+
+def mip_next_f_dev(t, out=None, stream=None, ctx=None):
+    import torch
+    w, h, stride = _dev_img(t, (4,))
+    nw, nh = max(1, w // 2), max(1, h // 2)
+    if out is None:
+        out = torch.empty((nh, nw, 4), dtype=torch.float32, device=t.device)
+    check(load().zap_tex_cuda_mip_next_f_dev(ctx, t.data_ptr(), w, h, stride, out.data_ptr(), out.stride(0), _stream(stream)),
+          "mip_next_f_dev")
+    return out
+
+
+def mip_chain_dev(t, srgb, stream=None, ctx=None):
+    """Levels 1.. of t's mip chain as a list of HxWx4 uint8 CUDA tensors (views of one allocation)."""
+    import torch
+    w, h, stride = _dev_img(t, (4,))
+    lib = load()
+    buf = torch.empty(max(1, int(lib.zap_tex_cuda_mip_chain_bytes(w, h))), dtype=torch.uint8, device=t.device)
+    check(lib.zap_tex_cuda_mip_chain_dev(ctx, t.data_ptr(), w, h, stride, int(srgb), buf.data_ptr(), _stream(stream)), "mip_chain_dev")
+    levels, off = [], 0
+    while w > 1 or h > 1:
+        w, h = max(1, w // 2), max(1, h // 2)
+        levels.append(buf[off:off + w * h * 4].view(h, w, 4))
+        off += w * h * 4
+    return levels

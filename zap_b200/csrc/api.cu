@@ -1,0 +1,515 @@
+// api.cu - the zap_tex_cuda C ABI (include/zap_tex_cuda.h): contexts, argument checks, host staging, dispatch.
+//
+// Host-pointer calls are synchronous like the reference functions they replace. Large images are cut into bands
+// of block rows and pipelined over two streams, so the host->device copy of one band overlaps the kernels and
+// the device->host copy of the previous one. Device-pointer (_dev) calls enqueue on the caller's stream and take
+// their scratch from the stream-ordered allocator, so concurrent calls on different streams do not share it.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "../../include/zap_tex_cuda.h"
+#include "ztc_common.cuh"
+#include "ztc_internal.h"
+
+#include <map>
+#include <string>
+#include <vector>
+
+namespace ztc {
+cudaError_t upload_mip_tables();
+cudaError_t upload_astc_tables();
+
+// ---------------------------------------------------------------- kernel tracing (events around each launch)
+namespace {
+struct TraceRec {
+    const char *name;
+    cudaEvent_t a, b;
+    long units;         // blocks (or texels) the launch processed, when known on the host
+    uint32_t *counter;  // pinned slot receiving a device-side count, or null
+};
+std::mutex g_trace_lock;
+bool g_trace_on = false;
+std::vector<TraceRec> g_trace;
+thread_local std::vector<TraceRec> t_open;
+uint32_t *g_slots = nullptr;  // pinned host slots for device-side unit counts
+int g_slot_next = 0;
+constexpr int kSlots = 1 << 16;
+}  // namespace
+
+void trace_begin(const char *name, cudaStream_t s) {
+    if (!g_trace_on) return;
+    TraceRec r{name, nullptr, nullptr, 0, nullptr};
+    cudaEventCreate(&r.a);
+    cudaEventCreate(&r.b);
+    cudaEventRecord(r.a, s);
+    t_open.push_back(r);
+}
+void trace_units(long n) {
+    if (g_trace_on && !t_open.empty()) t_open.back().units = n;
+}
+void trace_units_dev(const uint32_t *d_count, cudaStream_t s) {
+    if (!g_trace_on || t_open.empty()) return;
+    std::lock_guard<std::mutex> g(g_trace_lock);
+    if (!g_slots && cudaMallocHost((void **)&g_slots, kSlots * sizeof(uint32_t)) != cudaSuccess) { g_slots = nullptr; return; }
+    if (g_slot_next >= kSlots) return;
+    uint32_t *slot = g_slots + g_slot_next++;
+    *slot = 0;
+    if (cudaMemcpyAsync(slot, d_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s) == cudaSuccess) t_open.back().counter = slot;
+}
+void trace_end(cudaStream_t s) {
+    if (!g_trace_on || t_open.empty()) return;
+    TraceRec r = t_open.back();
+    t_open.pop_back();
+    cudaEventRecord(r.b, s);
+    std::lock_guard<std::mutex> g(g_trace_lock);
+    g_trace.push_back(r);
+}
+}  // namespace ztc
+
+struct zap_tex_cuda_ctx {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream[2] = {nullptr, nullptr};
+    // host-call staging, grown on demand
+    uint8_t *d_in = nullptr;
+    size_t d_in_cap = 0;
+    uint8_t *d_out = nullptr;
+    size_t d_out_cap = 0;
+    void *d_scratch[2] = {nullptr, nullptr};
+    size_t d_scratch_cap[2] = {0, 0};
+    bool owned_default = false;
+};
+
+namespace {
+
+thread_local char g_err[512];
+
+int fail(int status, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+    return status;
+}
+int cuda_fail(cudaError_t e, const char *what) {
+    cudaGetLastError();  // clear a sticky launch error so the context stays usable
+    return fail(e == cudaErrorMemoryAllocation ? ZTC_ERR_NO_MEMORY : ZTC_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+#define ZTC_CHECK(expr, what)                          \
+    do {                                               \
+        cudaError_t e_ = (expr);                       \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+std::mutex g_lock;
+constexpr int kMaxDevices = 64;
+bool g_tables_ready[kMaxDevices];
+zap_tex_cuda_ctx *g_default[kMaxDevices];
+
+int device_ok(int device) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) { cudaGetLastError(); return fail(ZTC_ERR_NO_DEVICE, "no CUDA device"); }
+    if (device < 0 || device >= n || device >= kMaxDevices) return fail(ZTC_ERR_INVALID_ARG, "device %d out of range (%d devices)", device, n);
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+    if (major != 10) return fail(ZTC_ERR_NO_DEVICE, "device %d is compute capability %d.x; this build targets sm_100a", device, major);
+    return ZTC_OK;
+}
+
+int ensure_tables(int device) {  // caller holds g_lock, device is current
+    if (g_tables_ready[device]) return ZTC_OK;
+    ZTC_CHECK(ztc::upload_mip_tables(), "upload sRGB tables");
+    ZTC_CHECK(ztc::upload_astc_tables(), "upload ASTC tables");
+    g_tables_ready[device] = true;
+    return ZTC_OK;
+}
+
+int create_ctx(int device, zap_tex_cuda_ctx **out) {
+    int st = device_ok(device);
+    if (st) return st;
+    ZTC_CHECK(cudaSetDevice(device), "cudaSetDevice");
+    {
+        std::lock_guard<std::mutex> g(g_lock);
+        st = ensure_tables(device);
+        if (st) return st;
+    }
+    zap_tex_cuda_ctx *c = new (std::nothrow) zap_tex_cuda_ctx();
+    if (!c) return fail(ZTC_ERR_NO_MEMORY, "context allocation");
+    c->device = device;
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    for (int k = 0; k < 2; k++)
+        if (cudaStreamCreateWithFlags(&c->stream[k], cudaStreamNonBlocking) != cudaSuccess) {
+            zap_tex_cuda_destroy(c);
+            return cuda_fail(cudaErrorUnknown, "stream creation");
+        }
+    *out = c;
+    return ZTC_OK;
+}
+
+// ctx == NULL: the default context of the current device
+int resolve(zap_tex_cuda_ctx *&ctx) {
+    if (ctx) {
+        ZTC_CHECK(cudaSetDevice(ctx->device), "cudaSetDevice");
+        return ZTC_OK;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return fail(ZTC_ERR_NO_DEVICE, "no CUDA device"); }
+    if (dev < 0 || dev >= kMaxDevices) return fail(ZTC_ERR_INVALID_ARG, "device %d", dev);
+    {
+        std::lock_guard<std::mutex> g(g_lock);
+        if (g_default[dev]) { ctx = g_default[dev]; return ZTC_OK; }
+    }
+    zap_tex_cuda_ctx *c = nullptr;
+    int st = create_ctx(dev, &c);
+    if (st) return st;
+    std::lock_guard<std::mutex> g(g_lock);
+    if (g_default[dev]) { zap_tex_cuda_destroy(c); ctx = g_default[dev]; return ZTC_OK; }
+    c->owned_default = true;
+    g_default[dev] = c;
+    ctx = c;
+    return ZTC_OK;
+}
+
+int grow(void **p, size_t *cap, size_t need, const char *what) {
+    if (*cap >= need) return ZTC_OK;
+    if (*p) { cudaFree(*p); *p = nullptr; *cap = 0; }
+    size_t n = need + need / 4 + 4096;
+    ZTC_CHECK(cudaMalloc(p, n), what);
+    *cap = n;
+    return ZTC_OK;
+}
+
+bool valid_fmt_bc(int fmt) { return fmt >= ZTC_BC1 && fmt <= ZTC_BC7; }
+size_t block_bytes(int fmt) { return (fmt == ZTC_BC1 || fmt == ZTC_BC4) ? 8 : 16; }
+size_t round16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+// one encoder launch over block rows [by0, by0 + nby) of a device image
+int launch_encode(int fmt, const ztc::SrcU8 &src, const ztc::SrcHdr *hdr, int by0, int nby, uint8_t *out, void *scratch,
+                  cudaStream_t s) {
+    cudaError_t e;
+    if (fmt == ZTC_BC7) e = ztc_launch_bc7(src, by0, nby, out, scratch, s);
+    else if (fmt == ZTC_BC6H) e = ztc_launch_bc6h(*hdr, by0, nby, out, s);
+    else if (fmt == ZTC_ASTC4X4) e = ztc_launch_astc(src, by0, nby, out, scratch, s);
+    else e = ztc_launch_bcn(fmt, src, by0, nby, out, s);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    return ZTC_OK;
+}
+
+size_t scratch_for(int fmt, size_t nblocks) {
+    if (fmt == ZTC_BC7) return ztc::bc7_scratch_bytes(nblocks);
+    if (fmt == ZTC_ASTC4X4) return ztc::astc_scratch_bytes(nblocks);
+    return 0;
+}
+
+// Host-pointer encode: stage rows to the device band by band, encode, copy blocks back.
+// texel_bytes: 4 (RGBA8) or 16 (RGBA f32); src_stride in bytes.
+int host_encode(zap_tex_cuda_ctx *ctx, int fmt, const void *src, int w, int h, size_t src_stride, size_t texel_bytes, void *out) {
+    const int bw = (w + 3) / 4, bh = (h + 3) / 4;
+    const size_t bs = fmt == ZTC_BC6H || fmt == ZTC_ASTC4X4 ? 16 : block_bytes(fmt);
+    const size_t row_bytes = (size_t)w * texel_bytes, pitch = round16(row_bytes);
+    // band height: about 16 MB of source per band, at least 8 block rows
+    size_t band_rows = (16u << 20) / (pitch * 4) + 1;
+    if (band_rows < 8) band_rows = 8;
+    if (band_rows > (size_t)bh) band_rows = (size_t)bh;
+    const int nbands = (int)((bh + band_rows - 1) / band_rows);
+    int st = grow((void **)&ctx->d_in, &ctx->d_in_cap, pitch * (size_t)h, "cudaMalloc(input)");
+    if (!st) st = grow((void **)&ctx->d_out, &ctx->d_out_cap, (size_t)bw * bh * bs, "cudaMalloc(output)");
+    const size_t scr = scratch_for(fmt, (size_t)band_rows * bw);
+    for (int k = 0; k < 2 && !st && scr; k++) st = grow(&ctx->d_scratch[k], &ctx->d_scratch_cap[k], scr, "cudaMalloc(scratch)");
+    if (st) return st;
+    ztc::SrcU8 s8{ctx->d_in, pitch, w, h, 4, ((uintptr_t)ctx->d_in & 15u) == 0 && (pitch & 15u) == 0};
+    ztc::SrcHdr sh{ctx->d_in, pitch / 4, w, h, 4, 1};
+    for (int b = 0; b < nbands; b++) {
+        cudaStream_t s = ctx->stream[b & 1];
+        const int by0 = b * (int)band_rows, nby = by0 + (int)band_rows <= bh ? (int)band_rows : bh - by0;
+        const int y0 = by0 * 4, y1 = (by0 + nby) * 4 < h ? (by0 + nby) * 4 : h;
+        ZTC_CHECK(cudaMemcpy2DAsync(ctx->d_in + (size_t)y0 * pitch, pitch, (const uint8_t *)src + (size_t)y0 * src_stride, src_stride,
+                                    row_bytes, (size_t)(y1 - y0), cudaMemcpyHostToDevice, s),
+                  "host->device copy");
+        uint8_t *o = ctx->d_out + (size_t)by0 * bw * bs;
+        st = launch_encode(fmt, s8, &sh, by0, nby, o, ctx->d_scratch[b & 1], s);
+        if (st) return st;
+        ZTC_CHECK(cudaMemcpyAsync((uint8_t *)out + (size_t)by0 * bw * bs, o, (size_t)nby * bw * bs, cudaMemcpyDeviceToHost, s),
+                  "device->host copy");
+    }
+    ZTC_CHECK(cudaStreamSynchronize(ctx->stream[0]), "encode");
+    ZTC_CHECK(cudaStreamSynchronize(ctx->stream[1]), "encode");
+    return ZTC_OK;
+}
+
+int dev_encode(zap_tex_cuda_ctx *ctx, int fmt, const ztc::SrcU8 &s8, const ztc::SrcHdr *sh, int w, int h, void *out, cudaStream_t s) {
+    const int bh = (h + 3) / 4, bw = (w + 3) / 4;
+    const size_t scr = scratch_for(fmt, (size_t)bw * bh);
+    void *scratch = nullptr;
+    if (scr) ZTC_CHECK(cudaMallocAsync(&scratch, scr, s), "cudaMallocAsync(scratch)");
+    int st = launch_encode(fmt, s8, sh, 0, bh, (uint8_t *)out, scratch, s);
+    if (scratch) cudaFreeAsync(scratch, s);
+    (void)ctx;
+    return st;
+}
+
+int check_image(const void *p, const void *out, int w, int h, size_t stride, size_t min_stride) {
+    if (!p || !out) return fail(ZTC_ERR_INVALID_ARG, "null pointer");
+    if (w < 1 || h < 1) return fail(ZTC_ERR_INVALID_ARG, "size %dx%d", w, h);
+    if (w > (1 << 24) || h > (1 << 24)) return fail(ZTC_ERR_INVALID_ARG, "size %dx%d beyond 2^24", w, h);
+    if (stride < min_stride) return fail(ZTC_ERR_INVALID_ARG, "stride %zu below %zu", stride, min_stride);
+    return ZTC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zap_tex_cuda_version(void) { return ZAP_TEX_CUDA_VERSION; }
+
+const char *zap_tex_cuda_status_string(int status) {
+    switch (status) {
+    case ZTC_OK: return "ok";
+    case ZTC_ERR_INVALID_ARG: return "invalid argument";
+    case ZTC_ERR_UNSUPPORTED: return "unsupported";
+    case ZTC_ERR_CUDA: return "CUDA error";
+    case ZTC_ERR_NO_MEMORY: return "out of memory";
+    case ZTC_ERR_TIMEOUT: return "device wait timed out";
+    case ZTC_ERR_NO_DEVICE: return "no usable CUDA device";
+    default: return "unknown status";
+    }
+}
+
+const char *zap_tex_cuda_last_error(void) { return g_err; }
+
+int zap_tex_cuda_trace_enable(int enable) {
+    std::lock_guard<std::mutex> g(ztc::g_trace_lock);
+    for (auto &r : ztc::g_trace) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    ztc::g_trace.clear();
+    ztc::g_slot_next = 0;
+    ztc::g_trace_on = enable != 0;
+    return ZTC_OK;
+}
+
+int zap_tex_cuda_trace_report(char *buf, size_t cap) {
+    std::lock_guard<std::mutex> g(ztc::g_trace_lock);
+    struct Agg { long n = 0; double ms = 0; long units = 0; };
+    std::map<std::string, Agg> agg;
+    for (auto &r : ztc::g_trace) {
+        float ms = 0.0f;
+        if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+            auto &e = agg[r.name];
+            e.n += 1;
+            e.ms += ms;
+            e.units += r.counter ? (long)*r.counter : r.units;
+        }
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    cudaGetLastError();
+    ztc::g_trace.clear();
+    ztc::g_slot_next = 0;
+    std::string out;
+    char line[200];
+    for (auto &kv : agg) {
+        std::snprintf(line, sizeof line, "%s %ld %.6f %ld\n", kv.first.c_str(), kv.second.n, kv.second.ms, kv.second.units);
+        out += line;
+    }
+    if (buf && cap) {
+        std::strncpy(buf, out.c_str(), cap - 1);
+        buf[cap - 1] = 0;
+    }
+    return (int)out.size();
+}
+
+int zap_tex_cuda_create(int device, zap_tex_cuda_ctx **out) {
+    if (!out) return fail(ZTC_ERR_INVALID_ARG, "null out");
+    *out = nullptr;
+    return create_ctx(device, out);
+}
+
+int zap_tex_cuda_destroy(zap_tex_cuda_ctx *c) {
+    if (!c) return ZTC_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(c->device);
+    for (int k = 0; k < 2; k++) if (c->stream[k]) { cudaStreamSynchronize(c->stream[k]); cudaStreamDestroy(c->stream[k]); }
+    cudaFree(c->d_in); cudaFree(c->d_out); cudaFree(c->d_scratch[0]); cudaFree(c->d_scratch[1]);
+    if (c->owned_default) {
+        std::lock_guard<std::mutex> g(g_lock);
+        if (g_default[c->device] == c) g_default[c->device] = nullptr;
+    }
+    delete c;
+    cudaSetDevice(prev);
+    return ZTC_OK;
+}
+
+int zap_tex_cuda_reserve(zap_tex_cuda_ctx *ctx, size_t bytes) {
+    int st = resolve(ctx);
+    if (st) return st;
+    // _dev calls draw scratch from the device's default memory pool: keep that much resident across frees
+    cudaMemPool_t pool;
+    ZTC_CHECK(cudaDeviceGetDefaultMemPool(&pool, ctx->device), "cudaDeviceGetDefaultMemPool");
+    uint64_t keep = bytes;
+    ZTC_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+    void *p = nullptr;
+    ZTC_CHECK(cudaMallocAsync(&p, bytes ? bytes : 1, ctx->stream[0]), "cudaMallocAsync(reserve)");
+    ZTC_CHECK(cudaFreeAsync(p, ctx->stream[0]), "cudaFreeAsync(reserve)");
+    ZTC_CHECK(cudaStreamSynchronize(ctx->stream[0]), "reserve");
+    return ZTC_OK;
+}
+
+size_t zap_tex_cuda_block_bytes(int fmt) { return block_bytes(fmt); }
+size_t zap_tex_cuda_bc_size(int w, int h, int fmt) {
+    if (w < 1 || h < 1) return 0;
+    return (size_t)((w + 3) / 4) * (size_t)((h + 3) / 4) * (fmt == ZTC_BC6H || fmt == ZTC_ASTC4X4 ? 16 : block_bytes(fmt));
+}
+int zap_tex_cuda_mip_levels(int w, int h) {
+    int n = 1;
+    while (w > 1 || h > 1) { w = w > 1 ? w / 2 : 1; h = h > 1 ? h / 2 : 1; n++; }
+    return n;
+}
+
+// ------------------------------------------------------------------ host memory
+int zap_tex_cuda_bc_encode(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo, void *out) {
+    int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
+    if (st) return st;
+    if (!valid_fmt_bc(fmt)) return fail(ZTC_ERR_UNSUPPORTED, "format %d", fmt);
+    if (rdo != 0.0f) return fail(ZTC_ERR_UNSUPPORTED, "rdo %g: rate-distortion mode is not implemented on the device", (double)rdo);
+    if ((st = resolve(ctx))) return st;
+    return host_encode(ctx, fmt, rgba, w, h, stride, 4, out);
+}
+
+int zap_tex_cuda_bc6h_encode(zap_tex_cuda_ctx *ctx, const float *rgba, int w, int h, size_t stride, void *out) {
+    int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
+    if (st) return st;
+    if ((st = resolve(ctx))) return st;
+    return host_encode(ctx, ZTC_BC6H, rgba, w, h, stride * 4, 16, out);
+}
+
+int zap_tex_cuda_astc_encode(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, void *out) {
+    int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
+    if (st) return st;
+    if ((st = resolve(ctx))) return st;
+    return host_encode(ctx, ZTC_ASTC4X4, rgba, w, h, stride, 4, out);
+}
+
+static int host_mip(zap_tex_cuda_ctx *ctx, const void *src, int w, int h, size_t stride_b, int srgb, void *dst, size_t dst_stride_b,
+                    size_t texel) {
+    const int nw = w > 1 ? w / 2 : 1, nh = h > 1 ? h / 2 : 1;
+    const size_t pitch = round16((size_t)w * texel), dpitch = round16((size_t)nw * texel);
+    int st = grow((void **)&ctx->d_in, &ctx->d_in_cap, pitch * h, "cudaMalloc(input)");
+    if (!st) st = grow((void **)&ctx->d_out, &ctx->d_out_cap, dpitch * nh, "cudaMalloc(output)");
+    if (st) return st;
+    cudaStream_t s = ctx->stream[0];
+    ZTC_CHECK(cudaMemcpy2DAsync(ctx->d_in, pitch, src, stride_b, (size_t)w * texel, h, cudaMemcpyHostToDevice, s), "host->device copy");
+    cudaError_t e = texel == 4 ? ztc_launch_mip(ctx->d_in, w, h, pitch, srgb, ctx->d_out, dpitch, s)
+                               : ztc_launch_mip_f((const float *)ctx->d_in, w, h, pitch / 4, (float *)ctx->d_out, dpitch / 4, s);
+    if (e != cudaSuccess) return cuda_fail(e, "mip launch");
+    ZTC_CHECK(cudaMemcpy2DAsync(dst, dst_stride_b, ctx->d_out, dpitch, (size_t)nw * texel, nh, cudaMemcpyDeviceToHost, s), "device->host copy");
+    ZTC_CHECK(cudaStreamSynchronize(s), "mip");
+    return ZTC_OK;
+}
+
+int zap_tex_cuda_mip_next(zap_tex_cuda_ctx *ctx, const uint8_t *src, int w, int h, size_t stride, int srgb, uint8_t *dst, size_t dst_stride) {
+    int st = check_image(src, dst, w, h, stride, (size_t)w * 4);
+    if (st) return st;
+    if (dst_stride < (size_t)(w > 1 ? w / 2 : 1) * 4) return fail(ZTC_ERR_INVALID_ARG, "dst_stride %zu too small", dst_stride);
+    if ((st = resolve(ctx))) return st;
+    return host_mip(ctx, src, w, h, stride, srgb, dst, dst_stride, 4);
+}
+
+int zap_tex_cuda_mip_next_f(zap_tex_cuda_ctx *ctx, const float *src, int w, int h, size_t stride, float *dst, size_t dst_stride) {
+    int st = check_image(src, dst, w, h, stride, (size_t)w * 4);
+    if (st) return st;
+    if (dst_stride < (size_t)(w > 1 ? w / 2 : 1) * 4) return fail(ZTC_ERR_INVALID_ARG, "dst_stride %zu too small", dst_stride);
+    if ((st = resolve(ctx))) return st;
+    return host_mip(ctx, src, w, h, stride * 4, 0, dst, dst_stride * 4, 16);
+}
+
+// ------------------------------------------------------------------ device memory
+int zap_tex_cuda_bc_encode_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo, void *out,
+                               void *stream) {
+    if (rdo != 0.0f) return fail(ZTC_ERR_UNSUPPORTED, "rdo %g: rate-distortion mode is not implemented on the device", (double)rdo);
+    if (!valid_fmt_bc(fmt)) return fail(ZTC_ERR_UNSUPPORTED, "format %d", fmt);
+    return zap_tex_cuda_bc_encode_u8_dev(ctx, rgba, 4, w, h, stride, fmt, out, stream);
+}
+
+int zap_tex_cuda_bc_encode_u8_dev(zap_tex_cuda_ctx *ctx, const uint8_t *src, int channels, int w, int h, size_t stride, int fmt, void *out,
+                                  void *stream) {
+    if (channels != 1 && channels != 2 && channels != 4) return fail(ZTC_ERR_INVALID_ARG, "channels %d", channels);
+    int st = check_image(src, out, w, h, stride, (size_t)w * channels);
+    if (st) return st;
+    if (!valid_fmt_bc(fmt) && fmt != ZTC_ASTC4X4) return fail(ZTC_ERR_UNSUPPORTED, "format %d", fmt);
+    if ((st = resolve(ctx))) return st;
+    ztc::SrcU8 s8{src, stride, w, h, channels, channels == 4 && (((uintptr_t)src | stride) & 15u) == 0};
+    return dev_encode(ctx, fmt, s8, nullptr, w, h, out, (cudaStream_t)stream);
+}
+
+int zap_tex_cuda_bc6h_encode_dev(zap_tex_cuda_ctx *ctx, const float *rgba, int w, int h, size_t stride, void *out, void *stream) {
+    int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
+    if (st) return st;
+    if ((st = resolve(ctx))) return st;
+    ztc::SrcU8 none{};
+    ztc::SrcHdr sh{rgba, stride, w, h, 4, 1};
+    return dev_encode(ctx, ZTC_BC6H, none, &sh, w, h, out, (cudaStream_t)stream);
+}
+
+int zap_tex_cuda_bc6h_encode_half_dev(zap_tex_cuda_ctx *ctx, const uint16_t *src, int channels, int w, int h, size_t stride, void *out,
+                                      void *stream) {
+    if (channels != 3 && channels != 4) return fail(ZTC_ERR_INVALID_ARG, "channels %d", channels);
+    int st = check_image(src, out, w, h, stride, (size_t)w * channels);
+    if (st) return st;
+    if ((st = resolve(ctx))) return st;
+    ztc::SrcU8 none{};
+    ztc::SrcHdr sh{src, stride, w, h, channels, 0};
+    return dev_encode(ctx, ZTC_BC6H, none, &sh, w, h, out, (cudaStream_t)stream);
+}
+
+int zap_tex_cuda_astc_encode_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, void *out, void *stream) {
+    return zap_tex_cuda_bc_encode_u8_dev(ctx, rgba, 4, w, h, stride, ZTC_ASTC4X4, out, stream);
+}
+
+int zap_tex_cuda_mip_next_dev(zap_tex_cuda_ctx *ctx, const uint8_t *src, int w, int h, size_t stride, int srgb, uint8_t *dst,
+                              size_t dst_stride, void *stream) {
+    int st = check_image(src, dst, w, h, stride, (size_t)w * 4);
+    if (st) return st;
+    if ((st = resolve(ctx))) return st;
+    cudaError_t e = ztc_launch_mip(src, w, h, stride, srgb, dst, dst_stride, (cudaStream_t)stream);
+    return e == cudaSuccess ? ZTC_OK : cuda_fail(e, "mip launch");
+}
+
+int zap_tex_cuda_mip_next_f_dev(zap_tex_cuda_ctx *ctx, const float *src, int w, int h, size_t stride, float *dst, size_t dst_stride,
+                                void *stream) {
+    int st = check_image(src, dst, w, h, stride, (size_t)w * 4);
+    if (st) return st;
+    if ((st = resolve(ctx))) return st;
+    cudaError_t e = ztc_launch_mip_f(src, w, h, stride, dst, dst_stride, (cudaStream_t)stream);
+    return e == cudaSuccess ? ZTC_OK : cuda_fail(e, "mip launch");
+}
+
+size_t zap_tex_cuda_mip_chain_bytes(int w, int h) {
+    size_t total = 0;
+    while (w > 1 || h > 1) {
+        w = w > 1 ? w / 2 : 1; h = h > 1 ? h / 2 : 1;
+        total += (size_t)w * h * 4;
+    }
+    return total;
+}
+
+int zap_tex_cuda_mip_chain_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int srgb, uint8_t *dst, void *stream) {
+    int st = check_image(rgba, dst, w, h, stride, (size_t)w * 4);
+    if (st) return st;
+    if ((st = resolve(ctx))) return st;
+    const uint8_t *prev = rgba;
+    size_t prev_stride = stride;
+    uint8_t *o = dst;
+    while (w > 1 || h > 1) {
+        int nw = w > 1 ? w / 2 : 1, nh = h > 1 ? h / 2 : 1;
+        cudaError_t e = ztc_launch_mip(prev, w, h, prev_stride, srgb, o, (size_t)nw * 4, (cudaStream_t)stream);
+        if (e != cudaSuccess) return cuda_fail(e, "mip launch");
+        prev = o; prev_stride = (size_t)nw * 4; o += (size_t)nw * nh * 4;
+        w = nw; h = nh;
+    }
+    return ZTC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,535 @@
+// astc.cu - ASTC 4x4 LDR encoder (zap_tex.h:977-1342) for sm_100a, bit-exact with the reference.
+//
+// Kernel A, one thread per block: the three single-partition configurations (CEM 8 for opaque blocks, CEM 12
+// otherwise), each a PCA start, a quantisation, a weight fit and up to three least-squares refits. Opaque blocks
+// still above SSE 192 go to a work list.
+// Kernel B, one 8-lane group per listed block: 2-means split, then the ~1000 usable two-partition patterns are
+// scanned 8-way by Hamming distance and the top 4 by (distance, pattern order) merged across the group (the
+// reference's early stop at four exact matches yields the same four); lane = (candidate, configuration) fits the
+// 8 trials, and the first-best trial below the single-partition SSE is packed by the lane that found it.
+// Tables the reference rebuilds on every call (zap_tex.h:1293-1305) are built once per device.
+#include <cstring>
+
+#include "ztc_common.cuh"
+#include "ztc_internal.h"
+#include "ztc_pca.cuh"
+
+namespace ztc {
+
+// ---------------------------------------------------------------- tables (host-built, ASTC spec rules)
+struct IseRange { int levels, trit, quint, bits; };
+static const IseRange kIse[21] = {  // integer-sequence ranges (ASTC spec)
+    {2, 0, 0, 1}, {3, 1, 0, 0}, {4, 0, 0, 2}, {5, 0, 1, 0}, {6, 1, 0, 1}, {8, 0, 0, 3}, {10, 0, 1, 1},
+    {12, 1, 0, 2}, {16, 0, 0, 4}, {20, 0, 1, 2}, {24, 1, 0, 3}, {32, 0, 0, 5}, {40, 0, 1, 3}, {48, 1, 0, 4},
+    {64, 0, 0, 6}, {80, 0, 1, 4}, {96, 1, 0, 5}, {128, 0, 0, 7}, {160, 0, 1, 5}, {192, 1, 0, 6}, {256, 0, 0, 8}};
+
+struct AstcCfg { int cem, wb, parts, nv, trit, quint, bits; };
+struct AstcTables {
+    AstcCfg cfg[8];
+    uint8_t q[8][256];   // 8-bit target -> nearest colour code (first on ties)
+    uint8_t uq[8][256];  // colour code -> unquantised 0..255
+    uint8_t trit_code[256], quint_code[128];  // value combination -> smallest packed code
+    uint16_t pat_mask[1024], pat_seed[1024];
+    int pat_count;
+};
+__constant__ AstcTables kAstc;
+
+static int ise_bits_h(const IseRange &r, int n) { return n * r.bits + (r.trit ? (8 * n + 4) / 5 : r.quint ? (7 * n + 2) / 3 : 0); }
+static int colour_range_h(int nvals, int avail) {
+    for (int i = 20; i >= 4; i--) if (ise_bits_h(kIse[i], nvals) <= avail) return i;
+    return -1;
+}
+static int replicate_h(int v, int n, int to) {
+    int x = 0;
+    for (int sh = to - n; sh > -n; sh -= n) x |= sh >= 0 ? v << sh : v >> -sh;
+    return x & ((1 << to) - 1);
+}
+static int colour_unquant_h(const IseRange &r, int v) {  // ASTC spec colour unquantisation
+    if (!r.trit && !r.quint) return replicate_h(v, r.bits, 8);
+    int n = r.bits, m = v & ((1 << n) - 1), D = v >> n;
+    int a = m & 1, b = (m >> 1) & 1, c = (m >> 2) & 1, d = (m >> 3) & 1, e = (m >> 4) & 1, f = (m >> 5) & 1;
+    int A = a ? 0x1FF : 0, B = 0, C = 0;
+    switch (r.levels) {
+    case 6: C = 204; break;
+    case 10: C = 113; break;
+    case 12: B = (b << 8) | (b << 4) | (b << 2) | (b << 1); C = 93; break;
+    case 20: B = (b << 8) | (b << 3) | (b << 2); C = 54; break;
+    case 24: B = (c << 8) | (b << 7) | (c << 3) | (b << 2) | (c << 1) | b; C = 44; break;
+    case 40: B = (c << 8) | (b << 7) | (c << 2) | (b << 1) | c; C = 26; break;
+    case 48: B = (d << 8) | (c << 7) | (b << 6) | (d << 2) | (c << 1) | b; C = 22; break;
+    case 80: B = (d << 8) | (c << 7) | (b << 6) | (d << 1) | c; C = 13; break;
+    case 96: B = (e << 8) | (d << 7) | (c << 6) | (b << 5) | (e << 1) | d; C = 11; break;
+    case 160: B = (e << 8) | (d << 7) | (c << 6) | (b << 5) | e; C = 6; break;
+    case 192: B = (f << 8) | (e << 7) | (d << 6) | (c << 5) | (b << 4) | f; C = 5; break;
+    }
+    int T = (D * C + B) ^ A;
+    return (A & 0x80) | (T >> 2);
+}
+static void trits_h(int T, int t[5]) {  // ASTC spec: 8 bits -> 5 trits
+    int C;
+    if (((T >> 2) & 7) == 7) { C = (((T >> 5) & 7) << 2) | (T & 3); t[4] = 2; t[3] = 2; }
+    else {
+        C = T & 31;
+        if (((T >> 5) & 3) == 3) { t[4] = 2; t[3] = (T >> 7) & 1; }
+        else { t[4] = (T >> 7) & 1; t[3] = (T >> 5) & 3; }
+    }
+    if ((C & 3) == 3) { t[2] = 2; t[1] = (C >> 4) & 1; t[0] = (((C >> 3) & 1) << 1) | (((C >> 2) & 1) & ~(C >> 3) & 1); }
+    else if (((C >> 2) & 3) == 3) { t[2] = 2; t[1] = 2; t[0] = C & 3; }
+    else { t[2] = (C >> 4) & 1; t[1] = (C >> 2) & 3; t[0] = (((C >> 1) & 1) << 1) | ((C & 1) & ~(C >> 1) & 1); }
+}
+static void quints_h(int Q, int q[3]) {  // ASTC spec: 7 bits -> 3 quints
+    if (((Q >> 1) & 3) == 3 && ((Q >> 5) & 3) == 0) {
+        q[2] = ((Q & 1) << 2) | ((((Q >> 4) & 1) & ~Q & 1) << 1) | (((Q >> 3) & 1) & ~Q & 1);
+        q[1] = 4; q[0] = 4;
+        return;
+    }
+    int C;
+    if (((Q >> 1) & 3) == 3) { q[2] = 4; C = (((Q >> 3) & 3) << 3) | ((~(Q >> 5) & 3) << 1) | (Q & 1); }
+    else { q[2] = (Q >> 5) & 3; C = Q & 31; }
+    if ((C & 7) == 5) { q[1] = 4; q[0] = (C >> 3) & 3; }
+    else { q[1] = (C >> 3) & 3; q[0] = C & 7; }
+}
+static uint32_t hash52_h(uint32_t p) {  // ASTC spec partition hash
+    p ^= p >> 15; p -= p << 17; p += p << 7; p += p << 4; p ^= p >> 5;
+    p += p << 16; p ^= p >> 7; p ^= p >> 3; p ^= p << 6; p ^= p >> 17;
+    return p;
+}
+static int partition_h(int seed, int x, int y, int count) {  // ASTC spec partition selection, small block
+    x <<= 1; y <<= 1;
+    seed += (count - 1) * 1024;
+    uint32_t h = hash52_h((uint32_t)seed);
+    int s[8];
+    for (int i = 0; i < 8; i++) { s[i] = (int)((h >> (4 * i)) & 15); s[i] *= s[i]; }
+    int sh1, sh2;
+    if (seed & 1) { sh1 = (seed & 2) ? 4 : 5; sh2 = count == 3 ? 6 : 5; }
+    else { sh1 = count == 3 ? 6 : 5; sh2 = (seed & 2) ? 4 : 5; }
+    for (int i = 0; i < 8; i++) s[i] >>= (i & 1) ? sh2 : sh1;
+    int a = (s[0] * x + s[1] * y + (int)(h >> 14)) & 0x3F, b = (s[2] * x + s[3] * y + (int)(h >> 10)) & 0x3F;
+    int c = (s[4] * x + s[5] * y + (int)(h >> 6)) & 0x3F, d = (s[6] * x + s[7] * y + (int)(h >> 2)) & 0x3F;
+    if (count < 4) d = 0;
+    if (count < 3) c = 0;
+    return (a >= b && a >= c && a >= d) ? 0 : (b >= c && b >= d) ? 1 : c >= d ? 2 : 3;
+}
+
+static void build_tables(AstcTables &T) {
+    std::memset(&T, 0, sizeof T);
+    // (CEM, weight bits, partitions) of the eight trial configurations (zap_tex.h:1298-1300)
+    static const int CFG[8][3] = {{8, 4, 1}, {8, 3, 1}, {8, 5, 1}, {12, 4, 1}, {12, 3, 1}, {12, 2, 1}, {8, 3, 2}, {8, 2, 2}};
+    for (int k = 0; k < 8; k++) {
+        AstcCfg &c = T.cfg[k];
+        c.cem = CFG[k][0]; c.wb = CFG[k][1]; c.parts = CFG[k][2]; c.nv = c.cem == 8 ? 6 : 8;
+        int ri = colour_range_h(c.nv * c.parts, 128 - (c.parts == 1 ? 17 : 29) - 16 * c.wb);
+        const IseRange &r = kIse[ri];
+        c.trit = r.trit; c.quint = r.quint; c.bits = r.bits;
+        for (int v = 0; v < 256; v++) T.uq[k][v] = v < r.levels ? (uint8_t)colour_unquant_h(r, v) : 0;
+        for (int x = 0; x < 256; x++) {
+            int best = 0, bd = 1 << 30;
+            for (int v = 0; v < r.levels; v++) {
+                int d = colour_unquant_h(r, v) - x;
+                d = d < 0 ? -d : d;
+                if (d < bd) { bd = d; best = v; }
+            }
+            T.q[k][x] = (uint8_t)best;
+        }
+    }
+    for (int t = 255; t >= 0; t--) { int v[5]; trits_h(t, v); T.trit_code[v[0] + 3 * v[1] + 9 * v[2] + 27 * v[3] + 81 * v[4]] = (uint8_t)t; }
+    for (int q = 127; q >= 0; q--) { int v[3]; quints_h(q, v); T.quint_code[v[0] + 5 * v[1] + 25 * v[2]] = (uint8_t)q; }
+    T.pat_count = 0;
+    for (int sd = 0; sd < 1024; sd++) {
+        unsigned m = 0;
+        for (int i = 0; i < 16; i++) m |= (unsigned)partition_h(sd, i & 3, i >> 2, 2) << i;
+        if (m && m != 0xFFFFu) { T.pat_mask[T.pat_count] = (uint16_t)m; T.pat_seed[T.pat_count++] = (uint16_t)sd; }
+    }
+}
+
+cudaError_t upload_astc_tables() {
+    static AstcTables T;
+    static bool built = false;
+    if (!built) { build_tables(T); built = true; }
+    return cudaMemcpyToSymbol(kAstc, &T, sizeof T);
+}
+
+// ---------------------------------------------------------------- device pieces
+struct AstcSmem {
+    uint8_t q[8][256], uq[8][256];
+    uint8_t trit_code[256], quint_code[128];
+};
+
+ZTC_DEV void load_smem(AstcSmem &S) {
+    const uint32_t *src = (const uint32_t *)&kAstc.q[0][0];
+    uint32_t *dst = (uint32_t *)&S.q[0][0];
+    for (int k = threadIdx.x; k < (int)(sizeof(S.q) + sizeof(S.uq)) / 4; k += blockDim.x) dst[k] = src[k];
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) S.trit_code[k] = kAstc.trit_code[k];
+    for (int k = threadIdx.x; k < 128; k += blockDim.x) S.quint_code[k] = kAstc.quint_code[k];
+}
+
+ZTC_DEV int wunq(int j, int wb) {  // weight n-bit -> 0..64 (power-of-two ranges, zap_tex.h:1030)
+    int x = 0;
+    for (int sh = 6 - wb; sh > -wb; sh -= wb) x |= sh >= 0 ? j << sh : j >> -sh;
+    x &= 63;
+    return x > 32 ? x + 1 : x;
+}
+ZTC_DEV int astc_lerp(int a, int b, int w) { return (((a * 257) * (64 - w) + (b * 257) * w + 32) >> 6) >> 8; }
+ZTC_DEV uint32_t get8(const uint32_t a[4], int i) { return (a[i >> 2] >> (8 * (i & 3))) & 0xFFu; }
+ZTC_DEV void set8(uint32_t a[4], int i, uint32_t v) {
+    #pragma unroll
+    for (int k = 0; k < 4; k++)
+        if (k == (i >> 2)) a[k] = (a[k] & ~(0xFFu << (8 * (i & 3)))) | (v << (8 * (i & 3)));
+}
+
+// CEM 8 / 12 endpoint pair from unquantised values r0 r1 g0 g1 b0 b1 [a0 a1] (zap_tex.h:1125-1129)
+ZTC_DEV void endpoint_pair(int cem, const int v[8], int e0[4], int e1[4]) {
+    int a0 = cem == 12 ? v[6] : 255, a1 = cem == 12 ? v[7] : 255;
+    if (v[1] + v[3] + v[5] >= v[0] + v[2] + v[4]) {
+        e0[0] = v[0]; e0[1] = v[2]; e0[2] = v[4]; e0[3] = a0;
+        e1[0] = v[1]; e1[1] = v[3]; e1[2] = v[5]; e1[3] = a1;
+    } else {  // blue contraction
+        e0[0] = (v[1] + v[5]) >> 1; e0[1] = (v[3] + v[5]) >> 1; e0[2] = v[5]; e0[3] = a1;
+        e1[0] = (v[0] + v[4]) >> 1; e1[1] = (v[2] + v[4]) >> 1; e1[2] = v[4]; e1[3] = a0;
+    }
+}
+
+// float endpoints -> codes + unquantised values of one partition (zap_tex.h:1183-1194)
+ZTC_DEV void astc_quant(const AstcSmem &S, int cfg, int nv, const float lo[4], const float hi[4], int code[8], int uv[8]) {
+    float s0 = lo[0] + lo[1] + lo[2], s1 = hi[0] + hi[1] + hi[2];
+    const bool keep = s1 >= s0;
+    #pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (2 * k >= nv) break;
+        float a = keep ? lo[k] : hi[k], b = keep ? hi[k] : lo[k];
+        int x0 = clampi(f2i_x86(a + 0.5f), 0, 255), x1 = clampi(f2i_x86(b + 0.5f), 0, 255);
+        code[2 * k] = S.q[cfg][x0]; code[2 * k + 1] = S.q[cfg][x1];
+        uv[2 * k] = S.uq[cfg][code[2 * k]]; uv[2 * k + 1] = S.uq[cfg][code[2 * k + 1]];
+    }
+    if (uv[1] + uv[3] + uv[5] < uv[0] + uv[2] + uv[4]) {
+        #pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (2 * k >= nv) break;
+            int s = code[2 * k]; code[2 * k] = code[2 * k + 1]; code[2 * k + 1] = s;
+            s = uv[2 * k]; uv[2 * k] = uv[2 * k + 1]; uv[2 * k + 1] = s;
+        }
+    }
+}
+
+// best weights for fixed endpoints (zap_tex.h:1197-1210); pm: bit i set = texel i in partition 1
+template <int NC, int LMAX, int PARTS>
+ZTC_DEV int astc_fit_weights(const uint32_t t[16], int cem, int wb, uint32_t pm, const int uv[PARTS][8], uint32_t wt[4]) {
+    const int L = 1 << wb;
+    const uint32_t cm = NC == 4 ? 0xFFFFFFFFu : 0x00FFFFFFu;
+    uint32_t pal[PARTS][LMAX];
+    int A[PARTS][LMAX];
+    #pragma unroll
+    for (int k = 0; k < PARTS; k++) {
+        int e0[4], e1[4];
+        endpoint_pair(cem, uv[k], e0, e1);
+        #pragma unroll
+        for (int j = 0; j < LMAX; j++) {
+            if (j >= L) break;
+            int w = wunq(j, wb);
+            uint32_t e = pack_rgba(astc_lerp(e0[0], e1[0], w), astc_lerp(e0[1], e1[1], w), astc_lerp(e0[2], e1[2], w),
+                                   astc_lerp(e0[3], e1[3], w)) & cm;
+            pal[k][j] = e;
+            A[k][j] = (int)dot4(e, e) * LMAX + j;
+        }
+    }
+    int err = 0;
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const int k = PARTS == 2 ? (int)((pm >> i) & 1u) : 0;
+        uint32_t p = t[i] & cm;
+        int m = 0x7FFFFFFF;
+        #pragma unroll
+        for (int j = 0; j < LMAX; j++) {
+            if (j >= L) break;
+            uint32_t pj = PARTS == 2 ? (k ? pal[1][j] : pal[0][j]) : pal[0][j];
+            int aj = PARTS == 2 ? (k ? A[PARTS - 1][j] : A[0][j]) : A[0][j];
+            m = min(m, aj - 2 * LMAX * (int)dot4(p, pj));
+        }
+        // key = (|c|^2 - 2 p.c) * LMAX + j keeps the first best j
+        int q = m >= 0 ? m / LMAX : -((-m + LMAX - 1) / LMAX);
+        err += q + (int)dot4(p, p);
+        set8(wt, i, (uint32_t)(m - q * LMAX));
+    }
+    return err;
+}
+
+// one trial configuration (zap_tex.h:1212-1244); codes: byte per value, partition 0 first
+template <int NC, int LMAX, int PARTS>
+ZTC_DEV int astc_try(const uint32_t t[16], const AstcSmem &S, int cfg, int cem, int wb, uint32_t pm, uint32_t codes[4], uint32_t wt[4]) {
+    constexpr int NV = NC == 4 ? 8 : 6;
+    int code[PARTS][8], uv[PARTS][8];
+    #pragma unroll
+    for (int k = 0; k < PARTS; k++) {
+        #pragma unroll
+        for (int v = 0; v < 8; v++) { code[k][v] = 0; uv[k][v] = 0; }
+        uint32_t m = PARTS == 2 ? (k ? pm : (~pm & 0xFFFFu)) : 0xFFFFu;
+        if (!m) m = 1u;  // empty partition: the reference fits texel 0
+        float lo[4], hi[4];
+        pca_endpoints<NC>(t, m, lo, hi);
+        astc_quant(S, cfg, NV, lo, hi, code[k], uv[k]);
+    }
+    int err = astc_fit_weights<NC, LMAX, PARTS>(t, cem, wb, pm, uv, wt);
+    for (int it = 0; it < 3 && err > 0; it++) {
+        int tc[PARTS][8], tuv[PARTS][8];
+        #pragma unroll
+        for (int k = 0; k < PARTS; k++) {
+            #pragma unroll
+            for (int v = 0; v < 8; v++) { tc[k][v] = code[k][v]; tuv[k][v] = uv[k][v]; }
+            uint32_t m = PARTS == 2 ? (k ? pm : (~pm & 0xFFFFu)) : 0xFFFFu;
+            float aa = 0.0f, ab = 0.0f, bb = 0.0f, sa[NC], sb[NC];
+            #pragma unroll
+            for (int c = 0; c < NC; c++) { sa[c] = 0.0f; sb[c] = 0.0f; }
+            #pragma unroll
+            for (int i = 0; i < 16; i++) {
+                if (!((m >> i) & 1u)) continue;
+                float f = (float)wunq((int)get8(wt, i), wb) / 64.0f, g = 1.0f - f;
+                aa = aa + g * g; ab = ab + g * f; bb = bb + f * f;
+                #pragma unroll
+                for (int c = 0; c < NC; c++) { float x = (float)chan(t[i], c); sa[c] = sa[c] + g * x; sb[c] = sb[c] + f * x; }
+            }
+            float det = aa * bb - ab * ab;
+            if (det < 1e-6f && det > -1e-6f) continue;
+            float nlo[4], nhi[4];
+            #pragma unroll
+            for (int c = 0; c < 4; c++) {
+                if (c < NC) { nlo[c] = (sa[c] * bb - sb[c] * ab) / det; nhi[c] = (sb[c] * aa - sa[c] * ab) / det; }
+                else { nlo[c] = 255.0f; nhi[c] = 255.0f; }
+            }
+            astc_quant(S, cfg, NV, nlo, nhi, tc[k], tuv[k]);
+        }
+        uint32_t tw[4] = {0, 0, 0, 0};
+        int e = astc_fit_weights<NC, LMAX, PARTS>(t, cem, wb, pm, tuv, tw);
+        if (e >= err) break;
+        err = e;
+        #pragma unroll
+        for (int k = 0; k < 4; k++) wt[k] = tw[k];
+        #pragma unroll
+        for (int k = 0; k < PARTS; k++)
+            #pragma unroll
+            for (int v = 0; v < 8; v++) { code[k][v] = tc[k][v]; uv[k][v] = tuv[k][v]; }
+    }
+    #pragma unroll
+    for (int k = 0; k < 4; k++) codes[k] = 0;
+    #pragma unroll
+    for (int k = 0; k < PARTS; k++)
+        #pragma unroll
+        for (int v = 0; v < NV; v++) set8(codes, k * NV + v, (uint32_t)code[k][v]);
+    return err;
+}
+
+// integer-sequence encoding of n codes (zap_tex.h:1080-1095)
+ZTC_DEV void ise_write(Bits128 &o, const AstcSmem &S, const AstcCfg &c, int n, const uint32_t codes[4]) {
+    const int bits = c.bits, mask = (1 << bits) - 1;
+    if (!c.trit && !c.quint) {
+        for (int i = 0; i < n; i++) o.put(get8(codes, i) & (uint32_t)mask, bits);
+        return;
+    }
+    const int gs = c.trit ? 5 : 3, base = c.trit ? 3 : 5;
+    for (int g = 0; g < n; g += gs) {
+        int cnt = min(n - g, gs), key = 0;
+        for (int k = gs - 1; k >= 0; k--) key = key * base + (k < cnt ? (int)(get8(codes, g + k) >> bits) : 0);
+        uint32_t X = c.trit ? S.trit_code[key] : S.quint_code[key];
+        int used = 0;
+        for (int k = 0; k < cnt; k++) {
+            o.put(get8(codes, g + k) & (uint32_t)mask, bits);
+            int xb = c.trit ? (k == 2 || k == 4 ? 1 : 2) : (k == 0 ? 3 : 2);  // packed-code bits after each value
+            o.put((X >> used) & ((1u << xb) - 1u), xb);
+            used += xb;
+        }
+    }
+}
+
+// block layout (zap_tex.h:1246-1260): mode, partitions, seed / CEM, ISE colours, weights reversed from bit 127
+ZTC_DEV uint4 astc_pack(const AstcSmem &S, int cfg, int seed, const uint32_t codes[4], const uint32_t wt[4]) {
+    const AstcCfg c = kAstc.cfg[cfg];
+    const int R = c.wb == 2 ? 4 : c.wb == 3 ? 7 : c.wb == 4 ? 4 : 7, H = c.wb >= 4 ? 1 : 0;
+    uint32_t mode = (uint32_t)(((R >> 1) & 1) | (((R >> 2) & 1) << 1) | ((R & 1) << 4) | (2 << 5) | (H << 9));
+    Bits128 o;
+    o.put(mode, 11);
+    o.put((uint32_t)(c.parts - 1), 2);
+    if (c.parts == 2) { o.put((uint32_t)seed, 10); o.put((uint32_t)c.cem << 2, 6); }
+    else o.put((uint32_t)c.cem, 4);
+    ise_write(o, S, c, c.nv * c.parts, codes);
+    Bits128 ws;
+    for (int i = 0; i < 16; i++) ws.put(get8(wt, i), c.wb);
+    // stream bit i -> block bit 127 - i
+    return make_uint4(o.w[0] | __brev(ws.w[3]), o.w[1] | __brev(ws.w[2]), o.w[2] | __brev(ws.w[1]), o.w[3] | __brev(ws.w[0]));
+}
+
+__global__ void __launch_bounds__(128) astc_single_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out,
+                                                          uint32_t *__restrict__ count, uint2 *__restrict__ items) {
+    __shared__ AstcSmem S;
+    load_smem(S);
+    __syncthreads();
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = b < nblocks, hard = false;
+    int best = 1 << 30;
+    if (valid) {
+        uint32_t t[16];
+        gather_block(src, b % bw, by0 + b / bw, t);
+        bool opaque = true;
+        #pragma unroll
+        for (int i = 0; i < 16; i++) opaque &= (t[i] >> 24) == 255u;
+        int bc = 0;
+        uint32_t bcodes[4] = {0, 0, 0, 0}, bwt[4] = {0, 0, 0, 0};
+        for (int k = 0; k < 3; k++) {
+            const int cfg = opaque ? k : 3 + k;
+            const int wb = kAstc.cfg[cfg].wb;
+            uint32_t codes[4], wt[4] = {0, 0, 0, 0};
+            int e = opaque ? astc_try<3, 32, 1>(t, S, cfg, 8, wb, 0u, codes, wt) : astc_try<4, 32, 1>(t, S, cfg, 12, wb, 0u, codes, wt);
+            if (e < best) {
+                best = e; bc = cfg;
+                #pragma unroll
+                for (int q = 0; q < 4; q++) { bcodes[q] = codes[q]; bwt[q] = wt[q]; }
+            }
+        }
+        store_block16(out + (size_t)b * 16, astc_pack(S, bc, 0, bcodes, bwt));
+        hard = opaque && best > 16 * 3 * 4;  // zap_tex.h:1323
+    }
+    unsigned ballot = __ballot_sync(0xFFFFFFFFu, hard);
+    if (ballot) {
+        int lane = threadIdx.x & 31, leader = __ffs(ballot) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(ballot));
+        base = __shfl_sync(0xFFFFFFFFu, base, leader);
+        if (hard) items[base + __popc(ballot & ((1u << lane) - 1u))] = make_uint2((uint32_t)b, (uint32_t)best);
+    }
+}
+
+// 2-means on RGB (zap_tex.h:1263-1283): bit i set = texel i in cluster 1
+ZTC_DEV uint32_t two_means(const uint32_t t[16]) {
+    int lo = 0, hi = 0, slo = (int)(chan(t[0], 0) + chan(t[0], 1) + chan(t[0], 2)), shi = slo;
+    #pragma unroll
+    for (int i = 1; i < 16; i++) {
+        int s = (int)(chan(t[i], 0) + chan(t[i], 1) + chan(t[i], 2));
+        if (s < slo) { lo = i; slo = s; }
+        if (s > shi) { hi = i; shi = s; }
+    }
+    float c0[3], c1[3];
+    #pragma unroll
+    for (int k = 0; k < 3; k++) {
+        uint32_t tl = t[0], th = t[0];
+        #pragma unroll
+        for (int i = 1; i < 16; i++) { if (i == lo) tl = t[i]; if (i == hi) th = t[i]; }
+        c0[k] = (float)chan(tl, k); c1[k] = (float)chan(th, k);
+    }
+    uint32_t m = 0;
+    for (int it = 0; it < 4; it++) {
+        float s0[3] = {0, 0, 0}, s1[3] = {0, 0, 0};
+        int n0 = 0, n1 = 0;
+        m = 0;
+        #pragma unroll
+        for (int i = 0; i < 16; i++) {
+            float d0 = 0.0f, d1 = 0.0f;
+            #pragma unroll
+            for (int k = 0; k < 3; k++) {
+                float x = (float)chan(t[i], k), a = x - c0[k], b = x - c1[k];
+                d0 = d0 + a * a; d1 = d1 + b * b;
+            }
+            bool s = d1 < d0;
+            m |= (uint32_t)s << i;
+            #pragma unroll
+            for (int k = 0; k < 3; k++) {
+                float x = (float)chan(t[i], k);
+                if (s) s1[k] = s1[k] + x; else s0[k] = s0[k] + x;
+            }
+            n1 += s; n0 += !s;
+        }
+        #pragma unroll
+        for (int k = 0; k < 3; k++) {
+            if (n0) c0[k] = s0[k] / (float)n0;
+            if (n1) c1[k] = s1[k] / (float)n1;
+        }
+    }
+    return m;
+}
+
+constexpr int kGroup = 8;
+
+__global__ void __launch_bounds__(128) astc_two_part_kernel(SrcU8 src, int bw, int by0, uint8_t *__restrict__ out,
+                                                            const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
+    __shared__ AstcSmem S;
+    __shared__ uint16_t pmask[1024], pseed[1024];
+    load_smem(S);
+    const int npat = kAstc.pat_count;
+    for (int k = threadIdx.x; k < npat; k += blockDim.x) { pmask[k] = kAstc.pat_mask[k]; pseed[k] = kAstc.pat_seed[k]; }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, l = lane & (kGroup - 1);
+    const unsigned gmask = 0xFFu << (lane & ~(kGroup - 1));
+    const int ngroups = gridDim.x * (blockDim.x / kGroup);
+    const int n = (int)*(volatile const uint32_t *)count;
+    for (int it = blockIdx.x * (blockDim.x / kGroup) + (threadIdx.x / kGroup); it < n; it += ngroups) {
+        const uint2 item = items[it];
+        const int b = (int)item.x, best = (int)item.y;
+        uint32_t t[16];
+        gather_block(src, b % bw, by0 + b / bw, t);
+        const uint32_t km = two_means(t);
+        // local top 4 by (distance, pattern order) over patterns l, l + 8, ...
+        int cd[4] = {99, 99, 99, 99}, cp[4] = {1 << 20, 1 << 20, 1 << 20, 1 << 20};
+        for (int pi = l; pi < npat; pi += kGroup) {
+            int dd = __popc((uint32_t)pmask[pi] ^ km), dist = min(dd, 16 - dd);
+            if (dist < cd[3]) {
+                int pos = 3;
+                #pragma unroll
+                for (int j = 2; j >= 0; j--) if (dist < cd[j]) pos = j;
+                #pragma unroll
+                for (int j = 3; j > 0; j--) if (j > pos) { cd[j] = cd[j - 1]; cp[j] = cp[j - 1]; }
+                #pragma unroll
+                for (int j = 0; j < 4; j++) if (j == pos) { cd[j] = dist; cp[j] = pi; }
+            }
+        }
+        int cand[4];
+        #pragma unroll
+        for (int j = 0; j < 4; j++) {  // group-wide (distance, pattern) minimum, owner pops
+            uint32_t key = ((uint32_t)cd[0] << 21) | (uint32_t)cp[0];
+            #pragma unroll
+            for (int m = 1; m < kGroup; m <<= 1) key = min(key, __shfl_xor_sync(gmask, key, m, kGroup));
+            int p = (int)(key & 0x1FFFFFu);
+            cand[j] = (key >> 21) < 99 ? p : -1;
+            if (cand[j] >= 0 && (p & (kGroup - 1)) == l) {
+                #pragma unroll
+                for (int s = 0; s < 3; s++) { cd[s] = cd[s + 1]; cp[s] = cp[s + 1]; }
+                cd[3] = 99; cp[3] = 1 << 20;
+            }
+        }
+        // lane = candidate * 2 + configuration (6: 3 weight bits, 7: 2 weight bits)
+        const int j = l >> 1, cfg = 6 + (l & 1), wb = cfg == 6 ? 3 : 2;
+        int pj = -1;
+        #pragma unroll
+        for (int k = 0; k < 4; k++) if (k == j) pj = cand[k];
+        uint32_t codes[4] = {0, 0, 0, 0}, wt[4] = {0, 0, 0, 0};
+        int e = 1 << 30;
+        if (pj >= 0) e = astc_try<3, 8, 2>(t, S, cfg, 8, wb, (uint32_t)pmask[pj], codes, wt);
+        uint32_t key = (pj >= 0 && e < best) ? (((uint32_t)e << 3) | (uint32_t)l) : 0xFFFFFFFFu;
+        #pragma unroll
+        for (int m = 1; m < kGroup; m <<= 1) key = min(key, __shfl_xor_sync(gmask, key, m, kGroup));
+        if (key != 0xFFFFFFFFu && (int)(key & 7u) == l) store_block16(out + (size_t)b * 16, astc_pack(S, cfg, pseed[pj], codes, wt));
+    }
+}
+
+}  // namespace ztc
+
+size_t ztc::astc_scratch_bytes(size_t nblocks) { return 256 + nblocks * sizeof(uint2); }
+
+cudaError_t ztc_launch_astc(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, void *scratch, cudaStream_t stream) {
+    int bw = (src.w + 3) / 4, nblocks = bw * nby;
+    if (nblocks <= 0) return cudaSuccess;
+    uint32_t *count = (uint32_t *)scratch;
+    uint2 *items = (uint2 *)((uint8_t *)scratch + 256);
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    {
+        ztc::TraceScope tr("astc_single", stream);
+        ztc::trace_units(nblocks);
+        ztc::astc_single_kernel<<<(nblocks + 127) / 128, 128, 0, stream>>>(src, bw, by0, nblocks, out, count, items);
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int groups_per_cta = 128 / ztc::kGroup, ctas = (nblocks + groups_per_cta - 1) / groups_per_cta;
+    ctas = ctas < sms * 8 ? ctas : sms * 8;
+    ztc::TraceScope tr("astc_two_part", stream);
+    ztc::trace_units_dev(count, stream);
+    ztc::astc_two_part_kernel<<<ctas, 128, 0, stream>>>(src, bw, by0, out, count, items);
+    return cudaGetLastError();
+}

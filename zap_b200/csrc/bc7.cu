@@ -1,0 +1,548 @@
+// bc7.cu - BC7 encoder for sm_100a (modes 6, 5 and 1, as the reference encoder uses them; zap_tex.h:308-784).
+//
+// Two kernels over a device work list:
+//   A  one thread per block: mode 6 (PCA start, p-bit search, two least-squares refits). Blocks whose SSE is
+//      <= 64 are final (the reference's early exit, zap_tex.h:758); the others are appended to a work list.
+//   B  one 8-lane group per listed block:
+//        mode 5  lane = (rotation, colour|alpha): 8 independent part fits, combined per rotation;
+//        mode 1  the 64 partitions are scored 8 per lane, the top 4 by (score, partition) are merged across the
+//                group, then lane = (candidate, subset) fits the 8 subsets.
+//      Decoded SSE checks of the reference (zap__bc7_err, zap_tex.h:761,780) equal the fit SSE here: the expand and
+//      interpolation are the decoder's, anchor swaps preserve decoded values because every weight table satisfies
+//      w(n-1-j) = 64 - w(j), mode 1 shares its p-bit between a subset's endpoints, and mode 1 decodes alpha 255
+//      on the opaque blocks it is tried on. So kernel B compares fit errors directly.
+// Every float expression keeps the reference's order; integer argmins keep the first candidate on ties.
+#include "ztc_common.cuh"
+#include "ztc_internal.h"
+#include "ztc_pca.cuh"
+
+namespace ztc {
+
+// two-subset partitions (BC7 format spec): bit i set = texel i in subset 1; anchor texel of subset 1
+__constant__ uint16_t kP2[64] = {
+    0xCCCC, 0x8888, 0xEEEE, 0xECC8, 0xC880, 0xFEEC, 0xFEC8, 0xEC80, 0xC800, 0xFFEC, 0xFE80, 0xE800, 0xFFE8, 0xFF00, 0xFFF0, 0xF000,
+    0xF710, 0x008E, 0x7100, 0x08CE, 0x008C, 0x7310, 0x3100, 0x8CCE, 0x088C, 0x3110, 0x6666, 0x366C, 0x17E8, 0x0FF0, 0x718E, 0x399C,
+    0xAAAA, 0xF0F0, 0x5A5A, 0x33CC, 0x3C3C, 0x55AA, 0x9696, 0xA55A, 0x73CE, 0x13C8, 0x324C, 0x3BDC, 0x6996, 0xC33C, 0x9966, 0x0660,
+    0x0272, 0x04E4, 0x4E40, 0x2720, 0xC936, 0x936C, 0x39C6, 0x639C, 0x9336, 0x9CC6, 0x817E, 0xE718, 0xCCF0, 0x0FCC, 0x7744, 0xEE22};
+__constant__ uint8_t kA2[64] = {
+    15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 2, 8, 2, 2, 8, 8, 15, 2, 8, 2, 2, 8, 8, 2, 2,
+    15, 15, 6, 8, 2, 8, 15, 15, 2, 8, 2, 2, 2, 15, 15, 6, 6, 2, 6, 8, 15, 15, 2, 2, 15, 15, 15, 15, 15, 2, 2, 15};
+
+// ---------------------------------------------------------------- shared pieces
+// endpoint quantisation with a fixed p-bit (zap_tex.h:426-438); q: stored values, x8: expanded 8-bit values
+template <int NC>
+ZTC_DEV int quant_pbit(const float v[4], int n, int p, int q[4], int x8[4]) {
+    int err = 0, top = (1 << (n - 1)) - 1;
+    #pragma unroll
+    for (int c = 0; c < NC; c++) {
+        int g = f2i_x86((v[c] / 255.0f * (float)((1 << n) - 1) - (float)p) / 2.0f + 0.5f), bq = 0, be = 1 << 30;
+        #pragma unroll
+        for (int k = 0; k < 3; k++) {
+            int tq = clampi(around(g, k), 0, top);
+            float d = (float)expand_bits((tq << 1) | p, n) - v[c];
+            int e = f2i_x86(d * d);
+            if (e < be) { be = e; bq = tq; }
+        }
+        q[c] = bq; x8[c] = expand_bits((bq << 1) | p, n); err += be;
+    }
+    return err;
+}
+
+// Argmin over a (1 << IB)-entry palette for every selected texel: key = (|c|^2 - 2 p.c) * NP + j is ordered
+// like the reference's first-best scan. idx: nibble i = index of texel i. Returns the SSE.
+template <int NC, int IB>
+ZTC_DEV int palette_fit(const uint32_t t[16], uint32_t mask, const int x0[4], const int x1[4], uint64_t &idx) {
+    constexpr int NP = 1 << IB;
+    const uint32_t cm = NC == 4 ? 0xFFFFFFFFu : 0x00FFFFFFu;
+    uint32_t pal[NP];
+    int A[NP];
+    #pragma unroll
+    for (int j = 0; j < NP; j++) {
+        int wj = wbits(IB, j);
+        uint32_t e = 0;
+        #pragma unroll
+        for (int c = 0; c < NC; c++) e |= (uint32_t)lerp64(x0[c], x1[c], wj) << (8 * c);
+        pal[j] = e;
+        A[j] = (int)dot4(e, e) * NP + j;
+    }
+    int err = 0;
+    uint64_t bits = 0;
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {
+        if (!((mask >> i) & 1u)) continue;
+        uint32_t p = t[i] & cm;
+        int m = A[0] - 2 * NP * (int)dot4(p, pal[0]);
+        #pragma unroll
+        for (int j = 1; j < NP; j++) m = min(m, A[j] - 2 * NP * (int)dot4(p, pal[j]));
+        err += (m >> IB) + (int)dot4(p, p);
+        bits |= (uint64_t)(m & (NP - 1)) << (4 * i);
+    }
+    idx = bits;
+    return err;
+}
+
+// float endpoints -> best p-bits, quantised endpoints, indices (zap_tex.h:466-486)
+template <int NC, int IB>
+ZTC_DEV int subset_fit(const uint32_t t[16], uint32_t mask, int n, bool shared_p, const float lo[4], const float hi[4],
+                       int q[2][4], int pb[2], uint64_t &idx) {
+    int ql[2][4], qh[2][4], xl[2][4], xh[2][4], el[2], eh[2];
+    #pragma unroll
+    for (int p = 0; p < 2; p++) { el[p] = quant_pbit<NC>(lo, n, p, ql[p], xl[p]); eh[p] = quant_pbit<NC>(hi, n, p, qh[p], xh[p]); }
+    int best = 1 << 30, b0 = 0, b1 = 0;
+    #pragma unroll
+    for (int combo = 0; combo < 4; combo++) {
+        int p0 = combo >> 1, p1 = combo & 1;
+        if (shared_p && p0 != p1) continue;
+        int e = el[p0] + eh[p1];
+        if (e < best) { best = e; b0 = p0; b1 = p1; }
+    }
+    int x0[4], x1[4];
+    #pragma unroll
+    for (int c = 0; c < 4; c++) {
+        q[0][c] = b0 ? ql[1][c] : ql[0][c]; q[1][c] = b1 ? qh[1][c] : qh[0][c];
+        x0[c] = b0 ? xl[1][c] : xl[0][c]; x1[c] = b1 ? xh[1][c] : xh[0][c];
+    }
+    pb[0] = b0; pb[1] = b1;
+    return palette_fit<NC, IB>(t, mask, x0, x1, idx);
+}
+
+// PCA start, fit, up to two least-squares refits (zap_tex.h:489-515)
+template <int NC, int IB>
+ZTC_DEV int subset_encode(const uint32_t t[16], uint32_t mask, int n, bool shared_p, int q[2][4], int pb[2], uint64_t &idx) {
+    float lo[4], hi[4];
+    pca_endpoints<NC>(t, mask, lo, hi);
+    int err = subset_fit<NC, IB>(t, mask, n, shared_p, lo, hi, q, pb, idx);
+    for (int it = 0; it < 2 && err > 0; it++) {
+        float aa = 0.0f, ab = 0.0f, bb = 0.0f, sa[NC], sb[NC];
+        #pragma unroll
+        for (int c = 0; c < NC; c++) { sa[c] = 0.0f; sb[c] = 0.0f; }
+        #pragma unroll
+        for (int i = 0; i < 16; i++) {
+            if (!((mask >> i) & 1u)) continue;
+            float w = (float)wbits(IB, (int)((idx >> (4 * i)) & 15u)) / 64.0f, u = 1.0f - w;
+            aa = aa + u * u; ab = ab + u * w; bb = bb + w * w;
+            #pragma unroll
+            for (int c = 0; c < NC; c++) { float x = (float)chan(t[i], c); sa[c] = sa[c] + u * x; sb[c] = sb[c] + w * x; }
+        }
+        float det = aa * bb - ab * ab;
+        if (det < 1e-6f && det > -1e-6f) break;
+        float nlo[4], nhi[4];
+        #pragma unroll
+        for (int c = 0; c < 4; c++) {
+            if (c < NC) { nlo[c] = clamp255((sa[c] * bb - sb[c] * ab) / det); nhi[c] = clamp255((sb[c] * aa - sa[c] * ab) / det); }
+            else { nlo[c] = 255.0f; nhi[c] = 255.0f; }
+        }
+        int nq[2][4], npb[2];
+        uint64_t ni;
+        int ne = subset_fit<NC, IB>(t, mask, n, shared_p, nlo, nhi, nq, npb, ni);
+        if (ne >= err) break;
+        err = ne; idx = ni; pb[0] = npb[0]; pb[1] = npb[1];
+        #pragma unroll
+        for (int c = 0; c < 4; c++) { q[0][c] = nq[0][c]; q[1][c] = nq[1][c]; }
+    }
+    return err;
+}
+
+// ---------------------------------------------------------------- kernel A: mode 6 for every block
+ZTC_DEV int mode6_encode(const uint32_t t[16], uint4 &blk) {  // zap_tex.h:520-527, 582-593
+    int q[2][4], pb[2];
+    uint64_t idx;
+    int err = subset_encode<4, 4>(t, 0xFFFFu, 8, false, q, pb, idx);
+    if (idx & 8u) {  // anchor index MSB must be 0: swap endpoints and p-bits, invert indices (15 - i == i ^ 15)
+        #pragma unroll
+        for (int c = 0; c < 4; c++) { int s = q[0][c]; q[0][c] = q[1][c]; q[1][c] = s; }
+        int s = pb[0]; pb[0] = pb[1]; pb[1] = s;
+        idx ^= 0xFFFFFFFFFFFFFFFFull;
+    }
+    Bits128 o;
+    o.put(1u << 6, 7);
+    #pragma unroll
+    for (int c = 0; c < 4; c++) { o.put((uint32_t)q[0][c], 7); o.put((uint32_t)q[1][c], 7); }
+    o.put((uint32_t)pb[0], 1); o.put((uint32_t)pb[1], 1);
+    o.put((uint32_t)(idx & 7u), 3);
+    #pragma unroll
+    for (int i = 1; i < 16; i++) o.put((uint32_t)((idx >> (4 * i)) & 15u), 4);
+    blk = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
+    return err;
+}
+
+__global__ void __launch_bounds__(128) bc7_mode6_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out,
+                                                        uint32_t *__restrict__ count, uint2 *__restrict__ items) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = b < nblocks;
+    int err = 0;
+    if (valid) {
+        uint32_t t[16];
+        gather_block(src, b % bw, by0 + b / bw, t);
+        uint4 blk;
+        err = mode6_encode(t, blk);
+        store_block16(out + (size_t)b * 16, blk);
+    }
+    bool hard = valid && err > 16 * 4;  // zap_tex.h:758 early exit
+    unsigned ballot = __ballot_sync(0xFFFFFFFFu, hard);
+    if (ballot) {
+        int lane = threadIdx.x & 31, leader = __ffs(ballot) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(ballot));
+        base = __shfl_sync(0xFFFFFFFFu, base, leader);
+        if (hard) items[base + __popc(ballot & ((1u << lane) - 1u))] = make_uint2((uint32_t)b, (uint32_t)err);
+    }
+}
+
+// ---------------------------------------------------------------- kernel B pieces
+// mode 5 part: 2-bit palette on channels [C0, C0 + NC) of the rotated texels (zap_tex.h:597-657)
+template <int NC>
+ZTC_DEV void m5_quant(const float v[4], int n, int q[4], int x8[4]) {
+    int top = (1 << n) - 1;
+    #pragma unroll
+    for (int c = 0; c < NC; c++) {
+        int g = f2i_x86(v[c] * (float)top / 255.0f + 0.5f), bq = 0, bd = 1 << 30;
+        #pragma unroll
+        for (int k = 0; k < 3; k++) {
+            int tq = clampi(around(g, k), 0, top);
+            int d = f2i_x86(fabsf((float)expand_bits(tq, n) - v[c]));
+            if (d < bd) { bd = d; bq = tq; }
+        }
+        q[c] = bq; x8[c] = expand_bits(bq, n);
+    }
+}
+// texels of a part, packed into the low bytes: colour = RGB of the rotated texel, alpha = its A byte
+template <int NC>
+ZTC_DEV uint32_t part_bytes(uint32_t r) { return NC == 3 ? (r & 0x00FFFFFFu) : (r >> 24); }
+
+template <int NC>
+ZTC_DEV int m5_fit(const uint32_t r[16], const int x0[4], const int x1[4], uint32_t &idx) {
+    uint32_t pal[4];
+    int A[4];
+    #pragma unroll
+    for (int j = 0; j < 4; j++) {
+        uint32_t e = 0;
+        #pragma unroll
+        for (int c = 0; c < NC; c++) e |= (uint32_t)lerp64(x0[c], x1[c], w2(j)) << (8 * c);
+        pal[j] = e; A[j] = (int)dot4(e, e) * 4 + j;
+    }
+    int err = 0;
+    uint32_t bits = 0;
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {
+        uint32_t p = part_bytes<NC>(r[i]);
+        int m = min(min(A[0] - 8 * (int)dot4(p, pal[0]), A[1] - 8 * (int)dot4(p, pal[1])),
+                    min(A[2] - 8 * (int)dot4(p, pal[2]), A[3] - 8 * (int)dot4(p, pal[3])));
+        err += (m >> 2) + (int)dot4(p, p);
+        bits |= (uint32_t)(m & 3) << (2 * i);
+    }
+    idx = bits;
+    return err;
+}
+template <int NC>
+ZTC_DEV bool m5_lsq(const uint32_t r[16], uint32_t idx, float lo[4], float hi[4]) {
+    float aa = 0.0f, ab = 0.0f, bb = 0.0f, sa[NC], sb[NC];
+    #pragma unroll
+    for (int c = 0; c < NC; c++) { sa[c] = 0.0f; sb[c] = 0.0f; }
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {
+        float w = (float)w2((int)((idx >> (2 * i)) & 3u)) / 64.0f, u = 1.0f - w;
+        aa = aa + u * u; ab = ab + u * w; bb = bb + w * w;
+        uint32_t p = part_bytes<NC>(r[i]);
+        #pragma unroll
+        for (int c = 0; c < NC; c++) { float x = (float)chan(p, c); sa[c] = sa[c] + u * x; sb[c] = sb[c] + w * x; }
+    }
+    float det = aa * bb - ab * ab;
+    if (det < 1e-6f && det > -1e-6f) return false;
+    #pragma unroll
+    for (int c = 0; c < NC; c++) { lo[c] = clamp255((sa[c] * bb - sb[c] * ab) / det); hi[c] = clamp255((sb[c] * aa - sa[c] * ab) / det); }
+    return true;
+}
+template <int NC>
+ZTC_DEV int m5_part(const uint32_t r[16], int n, const float lo[4], const float hi[4], int q[2][4], uint32_t &idx) {
+    int x0[4], x1[4];
+    m5_quant<NC>(lo, n, q[0], x0); m5_quant<NC>(hi, n, q[1], x1);
+    int err = m5_fit<NC>(r, x0, x1, idx);
+    for (int it = 0; it < 2 && err > 0; it++) {
+        float nlo[4], nhi[4];
+        if (!m5_lsq<NC>(r, idx, nlo, nhi)) break;
+        int tq[2][4];
+        m5_quant<NC>(nlo, n, tq[0], x0); m5_quant<NC>(nhi, n, tq[1], x1);
+        uint32_t ti;
+        int e = m5_fit<NC>(r, x0, x1, ti);
+        if (e >= err) break;
+        err = e; idx = ti;
+        #pragma unroll
+        for (int c = 0; c < NC; c++) { q[0][c] = tq[0][c]; q[1][c] = tq[1][c]; }
+    }
+    return err;
+}
+
+// partition score from per-texel moments (zap_tex.h:722-748); t holds the opaque block's texels
+ZTC_DEV float partition_score(const float mo[16][9], const float tot[9], uint32_t pmask) {
+    float s1[9], s0[9];
+    int n1 = 0;
+    #pragma unroll
+    for (int j = 0; j < 9; j++) s1[j] = 0.0f;
+    #pragma unroll
+    for (int i = 0; i < 16; i++)
+        if ((pmask >> i) & 1u) {
+            n1++;
+            #pragma unroll
+            for (int j = 0; j < 9; j++) s1[j] = s1[j] + mo[i][j];
+        }
+    #pragma unroll
+    for (int j = 0; j < 9; j++) s0[j] = tot[j] - s1[j];
+    float score = 0.0f;
+    #pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const float *m = k ? s1 : s0;
+        float n = (float)(k ? n1 : 16 - n1);
+        if (n < 2) continue;
+        float S00 = m[3] - m[0] * m[0] / n, S01 = m[6] - m[0] * m[1] / n, S02 = m[7] - m[0] * m[2] / n;
+        float S11 = m[4] - m[1] * m[1] / n, S12 = m[8] - m[1] * m[2] / n, S22 = m[5] - m[2] * m[2] / n;
+        float tr = S00 + S11 + S22, a0, a1, a2;
+        if (S00 >= S11 && S00 >= S22) { a0 = S00; a1 = S01; a2 = S02; }
+        else if (S11 >= S22) { a0 = S01; a1 = S11; a2 = S12; }
+        else { a0 = S02; a1 = S12; a2 = S22; }
+        #pragma unroll
+        for (int it = 0; it < 3; it++) {
+            float v0 = S00 * a0 + S01 * a1 + S02 * a2;
+            float v1 = S01 * a0 + S11 * a1 + S12 * a2;
+            float v2 = S02 * a0 + S12 * a1 + S22 * a2;
+            float mx = 1e-12f;
+            mx = v0 > mx ? v0 : -v0 > mx ? -v0 : mx;
+            mx = v1 > mx ? v1 : -v1 > mx ? -v1 : mx;
+            mx = v2 > mx ? v2 : -v2 > mx ? -v2 : mx;
+            a0 = v0 / mx; a1 = v1 / mx; a2 = v2 / mx;
+        }
+        float vv = a0 * a0 + a1 * a1 + a2 * a2, vsv = 0.0f;
+        vsv = vsv + a0 * (S00 * a0 + S01 * a1 + S02 * a2);
+        vsv = vsv + a1 * (S01 * a0 + S11 * a1 + S12 * a2);
+        vsv = vsv + a2 * (S02 * a0 + S12 * a1 + S22 * a2);
+        float lam = vv > 1e-12f ? vsv / vv : 0.0f;
+        score = score + (tr - lam * (48.0f / 49.0f));
+    }
+    return score;
+}
+
+// (score, partition) lexicographic "less", with the reference's float "<" (so -0 == +0)
+ZTC_DEV bool rank_less(float e, int p, float e2, int p2) { return e < e2 || (!(e2 < e) && p < p2); }
+
+constexpr int kGroup = 8;
+constexpr int kMode1Tries = 4;  // partitions fully fitted after ranking (ZAP__BC7_M1K, zap_tex.h:750-752)
+
+__global__ void __launch_bounds__(128) bc7_hard_kernel(SrcU8 src, int bw, int by0, uint8_t *__restrict__ out,
+                                                       const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
+    const int lane = threadIdx.x & 31, l = lane & (kGroup - 1);
+    const unsigned gmask = 0xFFu << (lane & ~(kGroup - 1));
+    const int ngroups = gridDim.x * (blockDim.x / kGroup);
+    const int n = (int)*(volatile const uint32_t *)count;
+    for (int it = blockIdx.x * (blockDim.x / kGroup) + (threadIdx.x / kGroup); it < n; it += ngroups) {
+        const uint2 item = items[it];
+        const int b = (int)item.x;
+        int err = (int)item.y;  // mode-6 SSE
+        uint32_t t[16];
+        gather_block(src, b % bw, by0 + b / bw, t);
+        bool opaque = true;
+        #pragma unroll
+        for (int i = 0; i < 16; i++) opaque &= (t[i] >> 24) == 255u;
+
+        // ---- mode 5: lane = rotation * 2 + part (zap_tex.h:659-684)
+        const int rot = l >> 1;
+        const bool alpha_part = l & 1;
+        uint32_t r[16];
+        #pragma unroll
+        for (int i = 0; i < 16; i++) {
+            uint32_t v = t[i];
+            if (rot) {
+                int sh = 8 * (rot - 1);
+                uint32_t a = v >> 24, c = (v >> sh) & 0xFFu;
+                v = (v & ~((0xFFu << sh) | 0xFF000000u)) | (a << sh) | (c << 24);
+            }
+            r[i] = v;
+        }
+        int q5[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+        uint32_t i5 = 0;
+        int e5;
+        if (!alpha_part) {
+            float lo[4], hi[4];
+            pca_endpoints<3>(r, 0xFFFFu, lo, hi);
+            e5 = m5_part<3>(r, 7, lo, hi, q5, i5);
+        } else {
+            float lo[4] = {255.0f, 0.0f, 0.0f, 0.0f}, hi[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            #pragma unroll
+            for (int i = 0; i < 16; i++) {
+                float a = (float)(r[i] >> 24);
+                if (a < lo[0]) lo[0] = a;
+                if (a > hi[0]) hi[0] = a;
+            }
+            e5 = m5_part<1>(r, 8, lo, hi, q5, i5);
+        }
+        // anchor fix inside the owning lane (zap_tex.h:673-674): 3 - i == i ^ 3 for 2-bit indices
+        if (i5 & 2u) {
+            #pragma unroll
+            for (int c = 0; c < 3; c++) { int s = q5[0][c]; q5[0][c] = q5[1][c]; q5[1][c] = s; }
+            i5 ^= 0xFFFFFFFFu;
+        }
+        int erot = e5 + (int)__shfl_xor_sync(gmask, (uint32_t)e5, 1, kGroup);
+        uint32_t key = ((uint32_t)erot << 2) | (uint32_t)rot;  // (SSE, rotation) lexicographic; SSE < 2^21
+        key = min(key, __shfl_xor_sync(gmask, key, 2, kGroup));
+        key = min(key, __shfl_xor_sync(gmask, key, 4, kGroup));
+        const int brot = (int)(key & 3u), best5 = (int)(key >> 2);
+        uint32_t qw = alpha_part ? (uint32_t)q5[0][0] | ((uint32_t)q5[1][0] << 8)
+                                 : (uint32_t)q5[0][0] | ((uint32_t)q5[0][1] << 7) | ((uint32_t)q5[0][2] << 14) |
+                                       ((uint32_t)q5[1][0] << 21);
+        uint32_t qw2 = (uint32_t)q5[1][1] | ((uint32_t)q5[1][2] << 7);
+        uint32_t cq = __shfl_sync(gmask, qw, 2 * brot, kGroup), cq2 = __shfl_sync(gmask, qw2, 2 * brot, kGroup);
+        uint32_t ci = __shfl_sync(gmask, i5, 2 * brot, kGroup);
+        uint32_t aq = __shfl_sync(gmask, qw, 2 * brot + 1, kGroup), ai = __shfl_sync(gmask, i5, 2 * brot + 1, kGroup);
+        bool take5 = best5 < err;  // decoded SSE == fit SSE (see the file header)
+        uint4 blk = make_uint4(0, 0, 0, 0);
+        if (take5) {
+            err = best5;
+            Bits128 o;
+            o.put(1u << 5, 6);
+            o.put((uint32_t)brot, 2);
+            uint32_t c0[3] = {cq & 127u, (cq >> 7) & 127u, (cq >> 14) & 127u}, c1[3] = {(cq >> 21) & 127u, cq2 & 127u, (cq2 >> 7) & 127u};
+            #pragma unroll
+            for (int c = 0; c < 3; c++) { o.put(c0[c], 7); o.put(c1[c], 7); }
+            o.put(aq & 255u, 8); o.put((aq >> 8) & 255u, 8);
+            o.put(ci & 1u, 1);
+            #pragma unroll
+            for (int i = 1; i < 16; i++) o.put((ci >> (2 * i)) & 3u, 2);
+            o.put(ai & 1u, 1);
+            #pragma unroll
+            for (int i = 1; i < 16; i++) o.put((ai >> (2 * i)) & 3u, 2);
+            blk = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
+        }
+        if (opaque) {  // group-uniform: every lane holds the same texels
+            // ---- mode 1 ranking: lane scores partitions l, l + 8, ..., l + 56 (zap_tex.h:764-775)
+            float mo[16][9], tot[9];
+            #pragma unroll
+            for (int j = 0; j < 9; j++) tot[j] = 0.0f;
+            #pragma unroll
+            for (int i = 0; i < 16; i++) {
+                float rr = (float)chan(t[i], 0), gg = (float)chan(t[i], 1), bb = (float)chan(t[i], 2);
+                mo[i][0] = rr; mo[i][1] = gg; mo[i][2] = bb; mo[i][3] = rr * rr; mo[i][4] = gg * gg; mo[i][5] = bb * bb;
+                mo[i][6] = rr * gg; mo[i][7] = rr * bb; mo[i][8] = gg * bb;
+                #pragma unroll
+                for (int j = 0; j < 9; j++) tot[j] = tot[j] + mo[i][j];
+            }
+            float ce[kMode1Tries];
+            int cp[kMode1Tries];
+            #pragma unroll
+            for (int j = 0; j < kMode1Tries; j++) { ce[j] = 1e30f; cp[j] = 64; }
+            for (int k = 0; k < 64 / kGroup; k++) {
+                int part = l + kGroup * k;
+                float e = partition_score(mo, tot, kP2[part]);
+                // insertion keeps (score, partition) order; NaN and >= 1e30 never enter, as in the reference
+                #pragma unroll
+                for (int j = 0; j < kMode1Tries; j++) {
+                    if (e < ce[j]) {
+                        #pragma unroll
+                        for (int s = kMode1Tries - 1; s > j; s--) { ce[s] = ce[s - 1]; cp[s] = cp[s - 1]; }
+                        ce[j] = e; cp[j] = part;
+                        break;
+                    }
+                }
+            }
+            // merge the eight sorted lists: four rounds of a group-wide (score, partition) minimum
+            int cand[kMode1Tries];
+            #pragma unroll
+            for (int j = 0; j < kMode1Tries; j++) {
+                float he = ce[0];
+                int hp = cp[0];
+                #pragma unroll
+                for (int m = 1; m < kGroup; m <<= 1) {
+                    float oe = __shfl_xor_sync(gmask, he, m, kGroup);
+                    int op = __shfl_xor_sync(gmask, hp, m, kGroup);
+                    if (rank_less(oe, op, he, hp)) { he = oe; hp = op; }
+                }
+                cand[j] = hp < 64 ? hp : -1;
+                if (hp < 64 && (hp & (kGroup - 1)) == l) {  // owner pops its head
+                    #pragma unroll
+                    for (int s = 0; s < kMode1Tries - 1; s++) { ce[s] = ce[s + 1]; cp[s] = cp[s + 1]; }
+                    ce[kMode1Tries - 1] = 1e30f; cp[kMode1Tries - 1] = 64;
+                }
+            }
+            // ---- mode 1 fits: lane = candidate * 2 + subset (zap_tex.h:687-708, 776)
+            const int j = l >> 1, sub = l & 1;
+            int pj = 0;
+            #pragma unroll
+            for (int k = 0; k < kMode1Tries; k++) if (k == j) pj = cand[k];
+            int q1[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}}, pb1[2] = {0, 0}, e1 = 1 << 29;
+            uint64_t i1 = 0;
+            uint32_t pmask = 0;
+            if (pj >= 0) {
+                pmask = sub ? (uint32_t)kP2[pj] : (~(uint32_t)kP2[pj] & 0xFFFFu);
+                e1 = subset_encode<3, 3>(t, pmask, 7, true, q1, pb1, i1);
+                int anchor = sub ? (int)kA2[pj] : 0;
+                if ((i1 >> (4 * anchor)) & 4u) {  // anchor MSB must be 0: swap, 7 - i == i ^ 7 on the subset's texels
+                    #pragma unroll
+                    for (int c = 0; c < 3; c++) { int s = q1[0][c]; q1[0][c] = q1[1][c]; q1[1][c] = s; }
+                    uint64_t sel = 0;
+                    #pragma unroll
+                    for (int i = 0; i < 16; i++) if ((pmask >> i) & 1u) sel |= 7ull << (4 * i);
+                    i1 ^= sel;
+                }
+            }
+            int ecand = e1 + (int)__shfl_xor_sync(gmask, (uint32_t)e1, 1, kGroup);
+            // first candidate (in rank order) with the smallest SSE below the current best
+            uint32_t ckey = (pj >= 0 && ecand < err) ? (((uint32_t)ecand << 2) | (uint32_t)j) : 0xFFFFFFFFu;
+            ckey = min(ckey, __shfl_xor_sync(gmask, ckey, 2, kGroup));
+            ckey = min(ckey, __shfl_xor_sync(gmask, ckey, 4, kGroup));
+            if (ckey != 0xFFFFFFFFu) {
+                const int bj = (int)(ckey & 3u);
+                uint32_t ew0 = (uint32_t)q1[0][0] | ((uint32_t)q1[0][1] << 6) | ((uint32_t)q1[0][2] << 12) | ((uint32_t)pb1[0] << 18);
+                uint32_t ew1 = (uint32_t)q1[1][0] | ((uint32_t)q1[1][1] << 6) | ((uint32_t)q1[1][2] << 12);
+                uint32_t ilo = (uint32_t)i1, ihi = (uint32_t)(i1 >> 32);
+                uint32_t a0 = __shfl_sync(gmask, ew0, 2 * bj, kGroup), a1 = __shfl_sync(gmask, ew1, 2 * bj, kGroup);
+                uint32_t b0w = __shfl_sync(gmask, ew0, 2 * bj + 1, kGroup), b1w = __shfl_sync(gmask, ew1, 2 * bj + 1, kGroup);
+                uint32_t il = __shfl_sync(gmask, ilo, 2 * bj, kGroup) | __shfl_sync(gmask, ilo, 2 * bj + 1, kGroup);
+                uint32_t ih = __shfl_sync(gmask, ihi, 2 * bj, kGroup) | __shfl_sync(gmask, ihi, 2 * bj + 1, kGroup);
+                int part = __shfl_sync(gmask, pj, 2 * bj, kGroup);
+                err = (int)(ckey >> 2);
+                uint64_t full = (uint64_t)il | ((uint64_t)ih << 32);
+                Bits128 o;
+                o.put(2u, 2);
+                o.put((uint32_t)part, 6);
+                #pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    o.put((a0 >> (6 * c)) & 63u, 6); o.put((a1 >> (6 * c)) & 63u, 6);
+                    o.put((b0w >> (6 * c)) & 63u, 6); o.put((b1w >> (6 * c)) & 63u, 6);
+                }
+                o.put((a0 >> 18) & 1u, 1); o.put((b0w >> 18) & 1u, 1);
+                const int anchor = (int)kA2[part];
+                #pragma unroll
+                for (int i = 0; i < 16; i++) o.put((uint32_t)((full >> (4 * i)) & 7u), (i == 0 || i == anchor) ? 2 : 3);
+                blk = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
+                take5 = true;  // a block to write
+            }
+        }
+        if (take5 && l == 0) store_block16(out + (size_t)b * 16, blk);
+    }
+}
+
+}  // namespace ztc
+
+size_t ztc::bc7_scratch_bytes(size_t nblocks) { return 256 + nblocks * sizeof(uint2); }
+
+cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, void *scratch, cudaStream_t stream) {
+    int bw = (src.w + 3) / 4, nblocks = bw * nby;
+    if (nblocks <= 0) return cudaSuccess;
+    uint32_t *count = (uint32_t *)scratch;
+    uint2 *items = (uint2 *)((uint8_t *)scratch + 256);
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    {
+        ztc::TraceScope tr("bc7_mode6", stream);
+        ztc::trace_units(nblocks);
+        ztc::bc7_mode6_kernel<<<(nblocks + 127) / 128, 128, 0, stream>>>(src, bw, by0, nblocks, out, count, items);
+    }
+    int groups_per_cta = 128 / ztc::kGroup;
+    int ctas = (nblocks + groups_per_cta - 1) / groups_per_cta;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    ctas = ctas < sms * 8 ? ctas : sms * 8;
+    ztc::TraceScope tr("bc7_modes51", stream);
+    ztc::trace_units_dev(count, stream);
+    ztc::bc7_hard_kernel<<<ctas, 128, 0, stream>>>(src, bw, by0, out, count, items);
+    return cudaGetLastError();
+}

@@ -1,0 +1,231 @@
+// bcn.cu - BC1 / BC3 / BC4 / BC5 block encoders for sm_100a, one thread per 4x4 block.
+//
+// Bit-exact with the reference encoder (zap_tex.h:39-213 at rdo = 0). The float part (PCA start, least-squares
+// refits) keeps the reference's operation order; the palette searches are exact integer work arranged for the GPU:
+// a texel's squared distance to palette entry k is |p|^2 + |c_k|^2 - 2 p.c_k, with p.c_k from one dp4a, and
+// the key 4 * (|c_k|^2 - 2 p.c_k) + k orders candidates exactly like the reference's first-best scan.
+#include "ztc_common.cuh"
+#include "ztc_internal.h"
+
+namespace ztc {
+
+// ---------------------------------------------------------------- BC1 (zap_tex.h:39-168)
+ZTC_DEV void unpack565(uint32_t c, int &r, int &g, int &b) {
+    int R = (c >> 11) & 31, G = (c >> 5) & 63, B = c & 31;
+    r = (R << 3) | (R >> 2); g = (G << 2) | (G >> 4); b = (B << 3) | (B >> 2);
+}
+ZTC_DEV uint32_t pack565(float r, float g, float b) {  // zap_tex.h:45-49
+    int R = f2i_x86(r * 31.0f / 255.0f + 0.5f), G = f2i_x86(g * 63.0f / 255.0f + 0.5f), B = f2i_x86(b * 31.0f / 255.0f + 0.5f);
+    return ((uint32_t)clampi(R, 0, 31) << 11) | ((uint32_t)clampi(G, 0, 63) << 5) | (uint32_t)clampi(B, 0, 31);
+}
+
+struct Bc1Texels {
+    uint32_t p[16];  // r, g, b bytes; alpha byte cleared
+    int pp;          // sum of |p|^2
+    int sr, sg, sb;  // channel sums
+};
+
+ZTC_DEV void bc1_prepare(const uint32_t t[16], Bc1Texels &T) {
+    T.pp = 0; T.sr = T.sg = T.sb = 0;
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {
+        T.p[i] = t[i] & 0x00FFFFFFu;
+        T.pp += (int)dot4(T.p[i], T.p[i]);
+        T.sr += (int)chan(t[i], 0); T.sg += (int)chan(t[i], 1); T.sb += (int)chan(t[i], 2);
+    }
+}
+
+// best 2-bit indices and SSE for c0 > c1 (4-colour palette, zap_tex.h:52-80 with force4)
+ZTC_DEV int bc1_fit4(const Bc1Texels &T, uint32_t c0, uint32_t c1, uint32_t &idx) {
+    int r0, g0, b0, r1, g1, b1;
+    unpack565(c0, r0, g0, b0); unpack565(c1, r1, g1, b1);
+    uint32_t q0 = pack_rgb(r0, g0, b0), q1 = pack_rgb(r1, g1, b1);
+    uint32_t q2 = pack_rgb((2 * r0 + r1 + 1) / 3, (2 * g0 + g1 + 1) / 3, (2 * b0 + b1 + 1) / 3);
+    uint32_t q3 = pack_rgb((r0 + 2 * r1 + 1) / 3, (g0 + 2 * g1 + 1) / 3, (b0 + 2 * b1 + 1) / 3);
+    int A0 = 4 * (int)dot4(q0, q0), A1 = 4 * (int)dot4(q1, q1) + 1, A2 = 4 * (int)dot4(q2, q2) + 2, A3 = 4 * (int)dot4(q3, q3) + 3;
+    uint32_t bits = 0;
+    int sum = 0;
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {
+        uint32_t p = T.p[i];
+        int k0 = A0 - 8 * (int)dot4(p, q0), k1 = A1 - 8 * (int)dot4(p, q1);
+        int k2 = A2 - 8 * (int)dot4(p, q2), k3 = A3 - 8 * (int)dot4(p, q3);
+        int m = min(min(k0, k1), min(k2, k3));
+        sum += m;
+        bits |= (uint32_t)(m & 3) << (2 * i);
+    }
+    idx = bits;
+    int ksum = __popc(bits & 0x55555555u) + 2 * __popc(bits & 0xAAAAAAAAu);
+    return ((sum - ksum) >> 2) + T.pp;
+}
+
+// canonical order (c0 > c1, or solid c0 == c1 with indices 0) + SSE (zap_tex.h:90-94)
+ZTC_DEV int bc1_try(const Bc1Texels &T, uint32_t &c0, uint32_t &c1, uint32_t &idx) {
+    if (c0 < c1) { uint32_t s = c0; c0 = c1; c1 = s; }
+    if (c0 == c1) {
+        int r, g, b;
+        unpack565(c0, r, g, b);
+        idx = 0;
+        return T.pp + 16 * (r * r + g * g + b * b) - 2 * (T.sr * r + T.sg * g + T.sb * b);
+    }
+    return bc1_fit4(T, c0, c1, idx);
+}
+
+ZTC_DEV float bc1_lsw(uint32_t k) { return k == 0 ? 1.0f : k == 1 ? 0.0f : k == 2 ? 2.0f / 3.0f : 1.0f / 3.0f; }
+
+// quality search (zap_tex.h:97-168)
+ZTC_DEV uint2 bc1_encode(const uint32_t t[16]) {
+    Bc1Texels T;
+    bc1_prepare(t, T);
+    float mu0 = 0.0f, mu1 = 0.0f, mu2 = 0.0f;
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {
+        mu0 = mu0 + (float)chan(t[i], 0) / 16.0f;
+        mu1 = mu1 + (float)chan(t[i], 1) / 16.0f;
+        mu2 = mu2 + (float)chan(t[i], 2) / 16.0f;
+    }
+    float C0 = 0, C1 = 0, C2 = 0, C3 = 0, C4 = 0, C5 = 0;
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {
+        float r = (float)chan(t[i], 0) - mu0, g = (float)chan(t[i], 1) - mu1, b = (float)chan(t[i], 2) - mu2;
+        C0 = C0 + r * r; C1 = C1 + r * g; C2 = C2 + r * b; C3 = C3 + g * g; C4 = C4 + g * b; C5 = C5 + b * b;
+    }
+    float v0 = 1.0f, v1 = 1.0f, v2 = 1.0f;
+    for (int it = 0; it < 6; it++) {
+        float x = C0 * v0 + C1 * v1 + C2 * v2;
+        float y = C1 * v0 + C3 * v1 + C4 * v2;
+        float z = C2 * v0 + C4 * v1 + C5 * v2;
+        float m = fabsf(x);
+        if (fabsf(y) > m) m = fabsf(y);
+        if (fabsf(z) > m) m = fabsf(z);
+        if (m < 1e-6f) break;
+        v0 = x / m; v1 = y / m; v2 = z / m;
+    }
+    float n2 = v0 * v0 + v1 * v1 + v2 * v2, tmin = 1e9f, tmax = -1e9f;
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {
+        float s = ((float)chan(t[i], 0) - mu0) * v0 + ((float)chan(t[i], 1) - mu1) * v1 + ((float)chan(t[i], 2) - mu2) * v2;
+        if (s < tmin) tmin = s;
+        if (s > tmax) tmax = s;
+    }
+    uint32_t b0 = 0, b1 = 0, bidx = 0;
+    int best = 1 << 30;
+    for (int start = 0; start < 2; start++) {
+        float inset = start ? 0.0f : (tmax - tmin) / 16.0f, lo = (tmin + inset) / n2, hi = (tmax - inset) / n2;
+        uint32_t c0 = pack565(mu0 + v0 * hi, mu1 + v1 * hi, mu2 + v2 * hi);
+        uint32_t c1 = pack565(mu0 + v0 * lo, mu1 + v1 * lo, mu2 + v2 * lo);
+        uint32_t idx = 0;
+        int e = bc1_try(T, c0, c1, idx);
+        for (int it = 0; it < 3 && e > 0; it++) {
+            float aa = 0, ab = 0, bb = 0, sa0 = 0, sa1 = 0, sa2 = 0, sb0 = 0, sb1 = 0, sb2 = 0;
+            #pragma unroll
+            for (int i = 0; i < 16; i++) {
+                float wa = bc1_lsw((idx >> (2 * i)) & 3u), wb = 1.0f - wa;
+                aa = aa + wa * wa; ab = ab + wa * wb; bb = bb + wb * wb;
+                float r = (float)chan(t[i], 0), g = (float)chan(t[i], 1), b = (float)chan(t[i], 2);
+                sa0 = sa0 + wa * r; sa1 = sa1 + wa * g; sa2 = sa2 + wa * b;
+                sb0 = sb0 + wb * r; sb1 = sb1 + wb * g; sb2 = sb2 + wb * b;
+            }
+            float det = aa * bb - ab * ab;
+            if (det < 1e-6f && det > -1e-6f) break;
+            uint32_t n0 = pack565((sa0 * bb - sb0 * ab) / det, (sa1 * bb - sb1 * ab) / det, (sa2 * bb - sb2 * ab) / det);
+            uint32_t n1 = pack565((sb0 * aa - sa0 * ab) / det, (sb1 * aa - sa1 * ab) / det, (sb2 * aa - sa2 * ab) / det);
+            uint32_t ni = 0;
+            int ne = bc1_try(T, n0, n1, ni);
+            if (ne >= e) break;
+            e = ne; c0 = n0; c1 = n1; idx = ni;
+        }
+        if (e < best) { best = e; b0 = c0; b1 = c1; bidx = idx; }
+    }
+    // +-1 climb over the six 565 channels of the two endpoints, first improvement taken immediately
+    bool improved = true;
+    for (int pass = 0; improved && pass < 8 && best > 0; pass++) {
+        improved = false;
+        for (int step = 0; step < 12; step++) {
+            int ep = step / 6, ch = (step / 2) % 3, d = (step & 1) ? 1 : -1;
+            int sh = ch == 0 ? 11 : ch == 1 ? 5 : 0, mx = ch == 1 ? 63 : 31;
+            uint32_t c = ep ? b1 : b0;
+            int f = (int)(c >> sh) & mx;
+            if (f + d < 0 || f + d > mx) continue;
+            c = (c & ~((uint32_t)mx << sh)) | ((uint32_t)(f + d) << sh);
+            uint32_t n0 = ep ? b0 : c, n1 = ep ? c : b1, ni = 0;
+            int ne = bc1_try(T, n0, n1, ni);
+            if (ne < best) { best = ne; b0 = n0; b1 = n1; bidx = ni; improved = true; }
+        }
+    }
+    return make_uint2(b0 | (b1 << 16), bidx);
+}
+
+// ---------------------------------------------------------------- BC4 (zap_tex.h:170-213)
+ZTC_DEV uint2 bc4_encode(const uint32_t t[16], int c) {
+    int v[16], lo = 255, hi = 0;
+    #pragma unroll
+    for (int i = 0; i < 16; i++) { v[i] = (int)chan(t[i], c); lo = min(lo, v[i]); hi = max(hi, v[i]); }
+    int best = 1 << 30, ba0 = hi, ba1 = lo;
+    uint64_t bidx = 0;
+    for (int cand = 0; cand < 9; cand++) {
+        int a0 = hi - cand / 3, a1 = lo + cand % 3;
+        if (a0 <= a1) { a0 = hi; a1 = lo; }
+        int err = 0;
+        uint64_t bits = 0;
+        if (a0 == a1) {
+            #pragma unroll
+            for (int i = 0; i < 16; i++) err += (v[i] - a0) * (v[i] - a0);
+        } else {
+            int p[8];
+            p[0] = a0; p[1] = a1;
+            #pragma unroll
+            for (int k = 2; k < 8; k++) p[k] = ((8 - k) * a0 + (k - 1) * a1 + 3) / 7;
+            #pragma unroll
+            for (int i = 0; i < 16; i++) {
+                int m = 1 << 30;
+                #pragma unroll
+                for (int k = 0; k < 8; k++) { int d = v[i] - p[k]; m = min(m, d * d * 8 + k); }
+                err += m >> 3;
+                bits |= (uint64_t)(m & 7) << (3 * i);
+            }
+        }
+        if (err < best) { best = err; ba0 = a0; ba1 = a1; bidx = bits; }
+    }
+    return make_uint2((uint32_t)ba0 | ((uint32_t)ba1 << 8) | ((uint32_t)(bidx & 0xFFFFu) << 16), (uint32_t)(bidx >> 16));
+}
+
+// ---------------------------------------------------------------- kernel: one thread per block
+template <int FMT>
+__global__ void __launch_bounds__(128) bcn_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblocks) return;
+    int bx = b % bw, by = by0 + b / bw;
+    uint32_t t[16];
+    gather_block(src, bx, by, t);
+    if (FMT == ZTC_FMT_BC1) {
+        store_block8(out + (size_t)b * 8, bc1_encode(t));
+    } else if (FMT == ZTC_FMT_BC4) {
+        store_block8(out + (size_t)b * 8, bc4_encode(t, 0));
+    } else if (FMT == ZTC_FMT_BC3) {
+        uint2 a = bc4_encode(t, 3), c = bc1_encode(t);
+        store_block16(out + (size_t)b * 16, make_uint4(a.x, a.y, c.x, c.y));
+    } else {  // BC5
+        uint2 r = bc4_encode(t, 0), g = bc4_encode(t, 1);
+        store_block16(out + (size_t)b * 16, make_uint4(r.x, r.y, g.x, g.y));
+    }
+}
+
+}  // namespace ztc
+
+cudaError_t ztc_launch_bcn(int fmt, const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, cudaStream_t stream) {
+    int bw = (src.w + 3) / 4, nblocks = bw * nby;
+    if (nblocks <= 0) return cudaSuccess;
+    dim3 block(128), grid((nblocks + 127) / 128);
+    static const char *names[4] = {"bc1_encode", "bc3_encode", "bc4_encode", "bc5_encode"};
+    ztc::TraceScope tr(fmt >= 0 && fmt < 4 ? names[fmt] : "bcn_encode", stream);
+    ztc::trace_units(nblocks);
+    switch (fmt) {
+    case ZTC_FMT_BC1: ztc::bcn_kernel<ZTC_FMT_BC1><<<grid, block, 0, stream>>>(src, bw, by0, nblocks, out); break;
+    case ZTC_FMT_BC3: ztc::bcn_kernel<ZTC_FMT_BC3><<<grid, block, 0, stream>>>(src, bw, by0, nblocks, out); break;
+    case ZTC_FMT_BC4: ztc::bcn_kernel<ZTC_FMT_BC4><<<grid, block, 0, stream>>>(src, bw, by0, nblocks, out); break;
+    case ZTC_FMT_BC5: ztc::bcn_kernel<ZTC_FMT_BC5><<<grid, block, 0, stream>>>(src, bw, by0, nblocks, out); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}

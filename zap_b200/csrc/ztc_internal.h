@@ -1,0 +1,48 @@
+// ztc_internal.h - launchers shared between the kernel files and the C-ABI layer (not installed).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+enum { ZTC_FMT_BC1 = 0, ZTC_FMT_BC3 = 1, ZTC_FMT_BC4 = 2, ZTC_FMT_BC5 = 3, ZTC_FMT_BC7 = 4, ZTC_FMT_BC6H = 5, ZTC_FMT_ASTC = 6 };
+
+namespace ztc {
+struct SrcU8;
+
+// Per-device constant tables (sRGB, ASTC). Uploaded once per device by the context.
+
+// Half-float source for BC6H: `channels` halfs per texel (3 or 4), or float RGBA when f32 is set.
+struct SrcHdr {
+    const void *base;
+    size_t stride;  // elements (floats or halfs) per row
+    int w, h, channels, f32;
+};
+
+// Kernel tracing (off by default): CUDA events around each launch, aggregated per kernel name on report.
+void trace_begin(const char *name, cudaStream_t s);
+void trace_end(cudaStream_t s);
+void trace_units(long n);                                     // units the open launch processes (host-known)
+void trace_units_dev(const uint32_t *d_count, cudaStream_t s);  // ... or read from a device counter
+struct TraceScope {
+    cudaStream_t s;
+    TraceScope(const char *name, cudaStream_t st) : s(st) { trace_begin(name, st); }
+    ~TraceScope() { trace_end(s); }
+};
+
+// BC7 work-list scratch: one entry per block that mode 6 alone does not finish
+struct Bc7Scratch {
+    uint32_t *count;  // 1 counter (zeroed by the launcher)
+    uint2 *items;     // (block index, mode-6 SSE), capacity = blocks of the launch
+};
+size_t bc7_scratch_bytes(size_t nblocks);
+// ASTC work list: blocks that go on to the two-partition search
+size_t astc_scratch_bytes(size_t nblocks);
+}  // namespace ztc
+
+cudaError_t ztc_launch_bcn(int fmt, const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, cudaStream_t stream);
+cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, void *scratch, cudaStream_t stream);
+cudaError_t ztc_launch_bc6h(const ztc::SrcHdr &src, int by0, int nby, uint8_t *out, cudaStream_t stream);
+cudaError_t ztc_launch_astc(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, void *scratch, cudaStream_t stream);
+cudaError_t ztc_launch_mip(const uint8_t *src, int w, int h, size_t stride, int srgb, uint8_t *dst, size_t dst_stride,
+                           cudaStream_t stream);
+cudaError_t ztc_launch_mip_f(const float *src, int w, int h, size_t stride, float *dst, size_t dst_stride, cudaStream_t stream);

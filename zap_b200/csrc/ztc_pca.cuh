@@ -1,0 +1,78 @@
+// ztc_pca.cuh - principal-axis endpoint estimate over a texel subset (zap_tex.h:441-462), shared by the BC7 and
+// ASTC kernels. The subset is a 16-bit mask (texel i selected when bit i is set); sums run over the selected
+// texels in increasing texel order, exactly like the reference's sel[] lists.
+#pragma once
+#include "ztc_common.cuh"
+
+namespace ztc {
+
+template <int NC>
+ZTC_DEV void pca_endpoints(const uint32_t t[16], uint32_t mask, float lo[4], float hi[4]) {
+    const float cnt = (float)__popc(mask);
+    float mu[NC];
+    #pragma unroll
+    for (int c = 0; c < NC; c++) mu[c] = 0.0f;
+    #pragma unroll
+    for (int i = 0; i < 16; i++)
+        if ((mask >> i) & 1u) {
+            #pragma unroll
+            for (int c = 0; c < NC; c++) mu[c] = mu[c] + (float)chan(t[i], c) / cnt;
+        }
+    // upper triangle only: cov[a][b] and cov[b][a] add bitwise-identical products in the same order
+    float C[NC][NC];
+    #pragma unroll
+    for (int a = 0; a < NC; a++)
+        #pragma unroll
+        for (int b = 0; b < NC; b++) C[a][b] = 0.0f;
+    #pragma unroll
+    for (int i = 0; i < 16; i++)
+        if ((mask >> i) & 1u) {
+            float d[NC];
+            #pragma unroll
+            for (int c = 0; c < NC; c++) d[c] = (float)chan(t[i], c) - mu[c];
+            #pragma unroll
+            for (int a = 0; a < NC; a++)
+                #pragma unroll
+                for (int b = a; b < NC; b++) C[a][b] = C[a][b] + d[a] * d[b];
+        }
+    #pragma unroll
+    for (int a = 0; a < NC; a++)
+        #pragma unroll
+        for (int b = 0; b < a; b++) C[a][b] = C[b][a];
+    float ax[NC];
+    #pragma unroll
+    for (int c = 0; c < NC; c++) ax[c] = 1.0f;
+    for (int it = 0; it < 6; it++) {
+        float nv[NC], m = 0.0f;
+        #pragma unroll
+        for (int a = 0; a < NC; a++) {
+            float s = 0.0f;
+            #pragma unroll
+            for (int b = 0; b < NC; b++) s = s + C[a][b] * ax[b];
+            nv[a] = s;
+            if (fabsf(s) > m) m = fabsf(s);
+        }
+        if (m < 1e-6f) break;
+        #pragma unroll
+        for (int a = 0; a < NC; a++) ax[a] = nv[a] / m;
+    }
+    float n2 = 0.0f, tl = 1e9f, th = -1e9f;
+    #pragma unroll
+    for (int a = 0; a < NC; a++) n2 = n2 + ax[a] * ax[a];
+    #pragma unroll
+    for (int i = 0; i < 16; i++)
+        if ((mask >> i) & 1u) {
+            float s = 0.0f;
+            #pragma unroll
+            for (int c = 0; c < NC; c++) s = s + ((float)chan(t[i], c) - mu[c]) * ax[c];
+            if (s < tl) tl = s;
+            if (s > th) th = s;
+        }
+    #pragma unroll
+    for (int c = 0; c < 4; c++) {
+        if (c < NC) { lo[c] = mu[c] + ax[c] * tl / n2; hi[c] = mu[c] + ax[c] * th / n2; }
+        else { lo[c] = 255.0f; hi[c] = 255.0f; }
+    }
+}
+
+}  // namespace ztc
