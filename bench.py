@@ -37,11 +37,40 @@ WORKLOAD = "bc7 2048x2048 rgba8, colour gradients + value noise + rectangles, no
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
-    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
+    p.add_argument("--profile", default=None, choices=["bc7", "bc1", "bc4", "bc5", "bc6h", "astc"],
+                   help="profiling case: only that encoder on a ring of 2048x2048 inputs, no e2e / CPU / extras")
     return p.parse_args()
+
+
+def run_profile_case(args):
+    """A small, self-contained case for ncu: W + K encodes of one format over a ring of distinct 2048^2 textures."""
+    import torch
+
+    import zap_b200
+    import zap_b200.synth as S
+    dev = torch.device("cuda", 0)
+    fmt = args.profile
+    ring = 10
+    if fmt == "bc6h":
+        texs = [S.hdr_texture(W, H, seed=k, device=dev) for k in range(ring)]
+        enc = lambda t: zap_b200.bc6h_encode_dev(t)  # noqa: E731
+    else:
+        code = {"bc7": zap_b200.BC7, "bc1": zap_b200.BC1, "bc4": zap_b200.BC4, "bc5": zap_b200.BC5, "astc": zap_b200.ASTC4X4}[fmt]
+        if fmt == "bc5":
+            texs = [S.normal_map(W, H, seed=k, device=dev) for k in range(ring)]
+        else:
+            texs = [S.colour_texture(W, H, seed=100 + k, alpha="opaque" if fmt == "bc1" else "noise", device=dev) for k in range(ring)]
+            if fmt == "bc4":
+                texs = [t[..., :1].contiguous() for t in texs]
+        enc = lambda t: zap_b200.bc_encode_dev(t, code)  # noqa: E731
+    torch.cuda.synchronize()
+    ms = time_device(lambda k: enc(texs[k % ring]), args.steps, args.warmup, 1)
+    print(json.dumps({"profile_case": fmt, "steps": args.steps, "ms_per_step": ms / args.steps,
+                      "Mpix_s": args.steps * W * H / 1e6 / (ms / 1e3)}))
 
 
 def dist_setup(args):
@@ -189,6 +218,9 @@ def time_device(fn, steps, warmup, world):
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.profile:
+        run_profile_case(args)
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
         if world > 1:

@@ -1,0 +1,118 @@
+// emu.cu - TEST INFRASTRUCTURE: the per-block encoder logic of zap_b200/csrc, compiled for the host.
+//
+// The kernels' block functions (ztc::bc1_encode, ztc::mode6_encode, ztc::bc6h_encode_block, ...) are
+// __host__ __device__; this file includes the kernel sources and runs those functions block by block on the CPU,
+// so tests/test_block_logic_on_host.py can diff the device logic against the oracle without a GPU. It is a
+// debugging aid beside the GPU parity tests, not a substitute for them: warp-cooperative kernels (the BC7 mode 5/1
+// and ASTC two-partition work lists) are not emulated, and only blocks those kernels do not revisit are compared.
+#include "../../zap_b200/csrc/astc.cu"
+#include "../../zap_b200/csrc/bc6h.cu"
+#include "../../zap_b200/csrc/bc7.cu"
+#include "../../zap_b200/csrc/bcn.cu"
+#include "../../zap_b200/csrc/mip.cu"
+
+namespace ztc {  // the launchers' tracing hooks live in api.cu, which is not part of this build
+void trace_begin(const char *, cudaStream_t) {}
+void trace_end(cudaStream_t) {}
+void trace_units(long) {}
+void trace_units_dev(const uint32_t *, cudaStream_t) {}
+}  // namespace ztc
+
+using namespace ztc;
+
+extern "C" {
+
+// BC1/BC3/BC4/BC5 exactly; BC7: mode-6 blocks, hard[b] = 1 where kernel B would revisit the block
+__attribute__((visibility("default"))) int emu_bc_encode(const uint8_t *img, int w, int h, size_t stride, int fmt, uint8_t *out,
+                                                         uint8_t *hard) {
+    SrcU8 s{img, stride, w, h, 4, 0};
+    int bw = (w + 3) / 4, bh = (h + 3) / 4;
+    for (int by = 0; by < bh; by++)
+        for (int bx = 0; bx < bw; bx++) {
+            uint32_t t[16];
+            gather_block(s, bx, by, t);
+            size_t b = (size_t)by * bw + bx;
+            if (fmt == ZTC_FMT_BC1) { uint2 v = bc1_encode(t); memcpy(out + b * 8, &v, 8); }
+            else if (fmt == ZTC_FMT_BC4) { uint2 v = bc4_encode(t, 0); memcpy(out + b * 8, &v, 8); }
+            else if (fmt == ZTC_FMT_BC3) { uint2 a = bc4_encode(t, 3), c = bc1_encode(t); memcpy(out + b * 16, &a, 8); memcpy(out + b * 16 + 8, &c, 8); }
+            else if (fmt == ZTC_FMT_BC5) { uint2 r = bc4_encode(t, 0), g = bc4_encode(t, 1); memcpy(out + b * 16, &r, 8); memcpy(out + b * 16 + 8, &g, 8); }
+            else if (fmt == ZTC_FMT_BC7) {
+                uint4 v;
+                int err = mode6_encode(t, v);
+                memcpy(out + b * 16, &v, 16);
+                if (hard) hard[b] = err > 64;
+            } else return -1;
+        }
+    return 0;
+}
+
+__attribute__((visibility("default"))) int emu_bc6h_encode(const float *img, int w, int h, size_t stride, uint8_t *out) {
+    int bw = (w + 3) / 4, bh = (h + 3) / 4;
+    for (int by = 0; by < bh; by++)
+        for (int bx = 0; bx < bw; bx++) {
+            HalfBlock B;
+            for (int i = 0; i < 16; i++) {
+                int x = std::min(bx * 4 + (i & 3), w - 1), y = std::min(by * 4 + (i >> 2), h - 1);
+                for (int c = 0; c < 3; c++) {
+                    uint32_t hb = f2h_unsigned(img[(size_t)y * stride + (size_t)x * 4 + c]);
+                    B.t[i][c] = hb;
+                    B.U[i][c] = (float)hb * 64.0f / 31.0f;
+                }
+            }
+            uint4 v = bc6h_encode_block(B);
+            memcpy(out + ((size_t)by * bw + bx) * 16, &v, 16);
+        }
+    return 0;
+}
+
+// single-partition ASTC blocks; hard[b] = 1 where the two-partition kernel would revisit the block
+__attribute__((visibility("default"))) int emu_astc_encode(const uint8_t *img, int w, int h, size_t stride, uint8_t *out, uint8_t *hard) {
+    static AstcTables T;
+    static AstcSmem S;
+    static bool ready = false;
+    if (!ready) {
+        build_tables(T);
+        memcpy(S.q, T.q, sizeof S.q); memcpy(S.uq, T.uq, sizeof S.uq); memcpy(S.cfg, T.cfg, sizeof S.cfg);
+        memcpy(S.trit_code, T.trit_code, sizeof S.trit_code); memcpy(S.quint_code, T.quint_code, sizeof S.quint_code);
+        ready = true;
+    }
+    SrcU8 s{img, stride, w, h, 4, 0};
+    int bw = (w + 3) / 4, bh = (h + 3) / 4;
+    for (int by = 0; by < bh; by++)
+        for (int bx = 0; bx < bw; bx++) {
+            uint32_t t[16];
+            gather_block(s, bx, by, t);
+            bool opaque = true;
+            for (int i = 0; i < 16; i++) opaque &= (t[i] >> 24) == 255u;
+            int best = 1 << 30, bc = 0;
+            uint32_t bcodes[4] = {0, 0, 0, 0}, bwt[4] = {0, 0, 0, 0};
+            for (int k = 0; k < 3; k++) {
+                int cfg = opaque ? k : 3 + k, wb = S.cfg[cfg].wb;
+                uint32_t codes[4], wt[4] = {0, 0, 0, 0};
+                int e = opaque ? astc_try<3, 32, 1>(t, S, cfg, 8, wb, 0u, codes, wt) : astc_try<4, 32, 1>(t, S, cfg, 12, wb, 0u, codes, wt);
+                if (e < best) { best = e; bc = cfg; memcpy(bcodes, codes, 16); memcpy(bwt, wt, 16); }
+            }
+            uint4 v = astc_pack(S, bc, 0, bcodes, bwt);
+            size_t b = (size_t)by * bw + bx;
+            memcpy(out + b * 16, &v, 16);
+            if (hard) hard[b] = opaque && best > 192;
+        }
+    return 0;
+}
+
+__attribute__((visibility("default"))) int emu_mip_next(const uint8_t *src, int w, int h, size_t stride, int srgb, uint8_t *dst, size_t dst_stride) {
+    float lin[256], thr[256];
+    srgb_tables_host(lin, thr);
+    int nw = w > 1 ? w / 2 : 1, nh = h > 1 ? h / 2 : 1;
+    for (int y = 0; y < nh; y++)
+        for (int x = 0; x < nw; x++) {
+            int x0 = std::min(2 * x, w - 1), x1 = std::min(2 * x + 1, w - 1), y0 = std::min(2 * y, h - 1), y1 = std::min(2 * y + 1, h - 1);
+            uint32_t v = box4(ld_texel(src + (size_t)y0 * stride + (size_t)x0 * 4), ld_texel(src + (size_t)y0 * stride + (size_t)x1 * 4),
+                              ld_texel(src + (size_t)y1 * stride + (size_t)x0 * 4), ld_texel(src + (size_t)y1 * stride + (size_t)x1 * 4),
+                              srgb != 0, lin, thr);
+            memcpy(dst + (size_t)y * dst_stride + (size_t)x * 4, &v, 4);
+        }
+    return 0;
+}
+
+}  // extern "C"

@@ -152,15 +152,17 @@ cudaError_t upload_astc_tables() {
 // ---------------------------------------------------------------- device pieces
 struct AstcSmem {
     uint8_t q[8][256], uq[8][256];
+    AstcCfg cfg[8];
     uint8_t trit_code[256], quint_code[128];
 };
 
-ZTC_DEV void load_smem(AstcSmem &S) {
+__device__ __forceinline__ void load_smem(AstcSmem &S) {
     const uint32_t *src = (const uint32_t *)&kAstc.q[0][0];
     uint32_t *dst = (uint32_t *)&S.q[0][0];
     for (int k = threadIdx.x; k < (int)(sizeof(S.q) + sizeof(S.uq)) / 4; k += blockDim.x) dst[k] = src[k];
     for (int k = threadIdx.x; k < 256; k += blockDim.x) S.trit_code[k] = kAstc.trit_code[k];
     for (int k = threadIdx.x; k < 128; k += blockDim.x) S.quint_code[k] = kAstc.quint_code[k];
+    if (threadIdx.x < 8) S.cfg[threadIdx.x] = kAstc.cfg[threadIdx.x];
 }
 
 ZTC_DEV int wunq(int j, int wb) {  // weight n-bit -> 0..64 (power-of-two ranges, zap_tex.h:1030)
@@ -341,7 +343,7 @@ ZTC_DEV void ise_write(Bits128 &o, const AstcSmem &S, const AstcCfg &c, int n, c
 
 // block layout (zap_tex.h:1246-1260): mode, partitions, seed / CEM, ISE colours, weights reversed from bit 127
 ZTC_DEV uint4 astc_pack(const AstcSmem &S, int cfg, int seed, const uint32_t codes[4], const uint32_t wt[4]) {
-    const AstcCfg c = kAstc.cfg[cfg];
+    const AstcCfg c = S.cfg[cfg];
     const int R = c.wb == 2 ? 4 : c.wb == 3 ? 7 : c.wb == 4 ? 4 : 7, H = c.wb >= 4 ? 1 : 0;
     uint32_t mode = (uint32_t)(((R >> 1) & 1) | (((R >> 2) & 1) << 1) | ((R & 1) << 4) | (2 << 5) | (H << 9));
     Bits128 o;
@@ -353,7 +355,7 @@ ZTC_DEV uint4 astc_pack(const AstcSmem &S, int cfg, int seed, const uint32_t cod
     Bits128 ws;
     for (int i = 0; i < 16; i++) ws.put(get8(wt, i), c.wb);
     // stream bit i -> block bit 127 - i
-    return make_uint4(o.w[0] | __brev(ws.w[3]), o.w[1] | __brev(ws.w[2]), o.w[2] | __brev(ws.w[1]), o.w[3] | __brev(ws.w[0]));
+    return make_uint4(o.w[0] | brev(ws.w[3]), o.w[1] | brev(ws.w[2]), o.w[2] | brev(ws.w[1]), o.w[3] | brev(ws.w[0]));
 }
 
 __global__ void __launch_bounds__(128) astc_single_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out,
@@ -374,7 +376,7 @@ __global__ void __launch_bounds__(128) astc_single_kernel(SrcU8 src, int bw, int
         uint32_t bcodes[4] = {0, 0, 0, 0}, bwt[4] = {0, 0, 0, 0};
         for (int k = 0; k < 3; k++) {
             const int cfg = opaque ? k : 3 + k;
-            const int wb = kAstc.cfg[cfg].wb;
+            const int wb = S.cfg[cfg].wb;
             uint32_t codes[4], wt[4] = {0, 0, 0, 0};
             int e = opaque ? astc_try<3, 32, 1>(t, S, cfg, 8, wb, 0u, codes, wt) : astc_try<4, 32, 1>(t, S, cfg, 12, wb, 0u, codes, wt);
             if (e < best) {
@@ -444,7 +446,7 @@ ZTC_DEV uint32_t two_means(const uint32_t t[16]) {
     return m;
 }
 
-constexpr int kGroup = 8;
+constexpr int kAstcGroup = 8;
 
 __global__ void __launch_bounds__(128) astc_two_part_kernel(SrcU8 src, int bw, int by0, uint8_t *__restrict__ out,
                                                             const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
@@ -454,11 +456,11 @@ __global__ void __launch_bounds__(128) astc_two_part_kernel(SrcU8 src, int bw, i
     const int npat = kAstc.pat_count;
     for (int k = threadIdx.x; k < npat; k += blockDim.x) { pmask[k] = kAstc.pat_mask[k]; pseed[k] = kAstc.pat_seed[k]; }
     __syncthreads();
-    const int lane = threadIdx.x & 31, l = lane & (kGroup - 1);
-    const unsigned gmask = 0xFFu << (lane & ~(kGroup - 1));
-    const int ngroups = gridDim.x * (blockDim.x / kGroup);
+    const int lane = threadIdx.x & 31, l = lane & (kAstcGroup - 1);
+    const unsigned gmask = 0xFFu << (lane & ~(kAstcGroup - 1));
+    const int ngroups = gridDim.x * (blockDim.x / kAstcGroup);
     const int n = (int)*(volatile const uint32_t *)count;
-    for (int it = blockIdx.x * (blockDim.x / kGroup) + (threadIdx.x / kGroup); it < n; it += ngroups) {
+    for (int it = blockIdx.x * (blockDim.x / kAstcGroup) + (threadIdx.x / kAstcGroup); it < n; it += ngroups) {
         const uint2 item = items[it];
         const int b = (int)item.x, best = (int)item.y;
         uint32_t t[16];
@@ -466,7 +468,7 @@ __global__ void __launch_bounds__(128) astc_two_part_kernel(SrcU8 src, int bw, i
         const uint32_t km = two_means(t);
         // local top 4 by (distance, pattern order) over patterns l, l + 8, ...
         int cd[4] = {99, 99, 99, 99}, cp[4] = {1 << 20, 1 << 20, 1 << 20, 1 << 20};
-        for (int pi = l; pi < npat; pi += kGroup) {
+        for (int pi = l; pi < npat; pi += kAstcGroup) {
             int dd = __popc((uint32_t)pmask[pi] ^ km), dist = min(dd, 16 - dd);
             if (dist < cd[3]) {
                 int pos = 3;
@@ -483,10 +485,10 @@ __global__ void __launch_bounds__(128) astc_two_part_kernel(SrcU8 src, int bw, i
         for (int j = 0; j < 4; j++) {  // group-wide (distance, pattern) minimum, owner pops
             uint32_t key = ((uint32_t)cd[0] << 21) | (uint32_t)cp[0];
             #pragma unroll
-            for (int m = 1; m < kGroup; m <<= 1) key = min(key, __shfl_xor_sync(gmask, key, m, kGroup));
+            for (int m = 1; m < kAstcGroup; m <<= 1) key = min(key, __shfl_xor_sync(gmask, key, m, kAstcGroup));
             int p = (int)(key & 0x1FFFFFu);
             cand[j] = (key >> 21) < 99 ? p : -1;
-            if (cand[j] >= 0 && (p & (kGroup - 1)) == l) {
+            if (cand[j] >= 0 && (p & (kAstcGroup - 1)) == l) {
                 #pragma unroll
                 for (int s = 0; s < 3; s++) { cd[s] = cd[s + 1]; cp[s] = cp[s + 1]; }
                 cd[3] = 99; cp[3] = 1 << 20;
@@ -502,7 +504,7 @@ __global__ void __launch_bounds__(128) astc_two_part_kernel(SrcU8 src, int bw, i
         if (pj >= 0) e = astc_try<3, 8, 2>(t, S, cfg, 8, wb, (uint32_t)pmask[pj], codes, wt);
         uint32_t key = (pj >= 0 && e < best) ? (((uint32_t)e << 3) | (uint32_t)l) : 0xFFFFFFFFu;
         #pragma unroll
-        for (int m = 1; m < kGroup; m <<= 1) key = min(key, __shfl_xor_sync(gmask, key, m, kGroup));
+        for (int m = 1; m < kAstcGroup; m <<= 1) key = min(key, __shfl_xor_sync(gmask, key, m, kAstcGroup));
         if (key != 0xFFFFFFFFu && (int)(key & 7u) == l) store_block16(out + (size_t)b * 16, astc_pack(S, cfg, pseed[pj], codes, wt));
     }
 }
@@ -526,7 +528,7 @@ cudaError_t ztc_launch_astc(const ztc::SrcU8 &src, int by0, int nby, uint8_t *ou
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int groups_per_cta = 128 / ztc::kGroup, ctas = (nblocks + groups_per_cta - 1) / groups_per_cta;
+    int groups_per_cta = 128 / ztc::kAstcGroup, ctas = (nblocks + groups_per_cta - 1) / groups_per_cta;
     ctas = ctas < sms * 8 ? ctas : sms * 8;
     ztc::TraceScope tr("astc_two_part", stream);
     ztc::trace_units_dev(count, stream);

@@ -324,16 +324,16 @@ ZTC_DEV float partition_score(const float mo[16][9], const float tot[9], uint32_
 // (score, partition) lexicographic "less", with the reference's float "<" (so -0 == +0)
 ZTC_DEV bool rank_less(float e, int p, float e2, int p2) { return e < e2 || (!(e2 < e) && p < p2); }
 
-constexpr int kGroup = 8;
+constexpr int kBc7Group = 8;
 constexpr int kMode1Tries = 4;  // partitions fully fitted after ranking (ZAP__BC7_M1K, zap_tex.h:750-752)
 
 __global__ void __launch_bounds__(128) bc7_hard_kernel(SrcU8 src, int bw, int by0, uint8_t *__restrict__ out,
                                                        const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
-    const int lane = threadIdx.x & 31, l = lane & (kGroup - 1);
-    const unsigned gmask = 0xFFu << (lane & ~(kGroup - 1));
-    const int ngroups = gridDim.x * (blockDim.x / kGroup);
+    const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
+    const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
+    const int ngroups = gridDim.x * (blockDim.x / kBc7Group);
     const int n = (int)*(volatile const uint32_t *)count;
-    for (int it = blockIdx.x * (blockDim.x / kGroup) + (threadIdx.x / kGroup); it < n; it += ngroups) {
+    for (int it = blockIdx.x * (blockDim.x / kBc7Group) + (threadIdx.x / kBc7Group); it < n; it += ngroups) {
         const uint2 item = items[it];
         const int b = (int)item.x;
         int err = (int)item.y;  // mode-6 SSE
@@ -380,18 +380,18 @@ __global__ void __launch_bounds__(128) bc7_hard_kernel(SrcU8 src, int bw, int by
             for (int c = 0; c < 3; c++) { int s = q5[0][c]; q5[0][c] = q5[1][c]; q5[1][c] = s; }
             i5 ^= 0xFFFFFFFFu;
         }
-        int erot = e5 + (int)__shfl_xor_sync(gmask, (uint32_t)e5, 1, kGroup);
+        int erot = e5 + (int)__shfl_xor_sync(gmask, (uint32_t)e5, 1, kBc7Group);
         uint32_t key = ((uint32_t)erot << 2) | (uint32_t)rot;  // (SSE, rotation) lexicographic; SSE < 2^21
-        key = min(key, __shfl_xor_sync(gmask, key, 2, kGroup));
-        key = min(key, __shfl_xor_sync(gmask, key, 4, kGroup));
+        key = min(key, __shfl_xor_sync(gmask, key, 2, kBc7Group));
+        key = min(key, __shfl_xor_sync(gmask, key, 4, kBc7Group));
         const int brot = (int)(key & 3u), best5 = (int)(key >> 2);
         uint32_t qw = alpha_part ? (uint32_t)q5[0][0] | ((uint32_t)q5[1][0] << 8)
                                  : (uint32_t)q5[0][0] | ((uint32_t)q5[0][1] << 7) | ((uint32_t)q5[0][2] << 14) |
                                        ((uint32_t)q5[1][0] << 21);
         uint32_t qw2 = (uint32_t)q5[1][1] | ((uint32_t)q5[1][2] << 7);
-        uint32_t cq = __shfl_sync(gmask, qw, 2 * brot, kGroup), cq2 = __shfl_sync(gmask, qw2, 2 * brot, kGroup);
-        uint32_t ci = __shfl_sync(gmask, i5, 2 * brot, kGroup);
-        uint32_t aq = __shfl_sync(gmask, qw, 2 * brot + 1, kGroup), ai = __shfl_sync(gmask, i5, 2 * brot + 1, kGroup);
+        uint32_t cq = __shfl_sync(gmask, qw, 2 * brot, kBc7Group), cq2 = __shfl_sync(gmask, qw2, 2 * brot, kBc7Group);
+        uint32_t ci = __shfl_sync(gmask, i5, 2 * brot, kBc7Group);
+        uint32_t aq = __shfl_sync(gmask, qw, 2 * brot + 1, kBc7Group), ai = __shfl_sync(gmask, i5, 2 * brot + 1, kBc7Group);
         bool take5 = best5 < err;  // decoded SSE == fit SSE (see the file header)
         uint4 blk = make_uint4(0, 0, 0, 0);
         if (take5) {
@@ -428,8 +428,8 @@ __global__ void __launch_bounds__(128) bc7_hard_kernel(SrcU8 src, int bw, int by
             int cp[kMode1Tries];
             #pragma unroll
             for (int j = 0; j < kMode1Tries; j++) { ce[j] = 1e30f; cp[j] = 64; }
-            for (int k = 0; k < 64 / kGroup; k++) {
-                int part = l + kGroup * k;
+            for (int k = 0; k < 64 / kBc7Group; k++) {
+                int part = l + kBc7Group * k;
                 float e = partition_score(mo, tot, kP2[part]);
                 // insertion keeps (score, partition) order; NaN and >= 1e30 never enter, as in the reference
                 #pragma unroll
@@ -449,13 +449,13 @@ __global__ void __launch_bounds__(128) bc7_hard_kernel(SrcU8 src, int bw, int by
                 float he = ce[0];
                 int hp = cp[0];
                 #pragma unroll
-                for (int m = 1; m < kGroup; m <<= 1) {
-                    float oe = __shfl_xor_sync(gmask, he, m, kGroup);
-                    int op = __shfl_xor_sync(gmask, hp, m, kGroup);
+                for (int m = 1; m < kBc7Group; m <<= 1) {
+                    float oe = __shfl_xor_sync(gmask, he, m, kBc7Group);
+                    int op = __shfl_xor_sync(gmask, hp, m, kBc7Group);
                     if (rank_less(oe, op, he, hp)) { he = oe; hp = op; }
                 }
                 cand[j] = hp < 64 ? hp : -1;
-                if (hp < 64 && (hp & (kGroup - 1)) == l) {  // owner pops its head
+                if (hp < 64 && (hp & (kBc7Group - 1)) == l) {  // owner pops its head
                     #pragma unroll
                     for (int s = 0; s < kMode1Tries - 1; s++) { ce[s] = ce[s + 1]; cp[s] = cp[s + 1]; }
                     ce[kMode1Tries - 1] = 1e30f; cp[kMode1Tries - 1] = 64;
@@ -482,21 +482,21 @@ __global__ void __launch_bounds__(128) bc7_hard_kernel(SrcU8 src, int bw, int by
                     i1 ^= sel;
                 }
             }
-            int ecand = e1 + (int)__shfl_xor_sync(gmask, (uint32_t)e1, 1, kGroup);
+            int ecand = e1 + (int)__shfl_xor_sync(gmask, (uint32_t)e1, 1, kBc7Group);
             // first candidate (in rank order) with the smallest SSE below the current best
             uint32_t ckey = (pj >= 0 && ecand < err) ? (((uint32_t)ecand << 2) | (uint32_t)j) : 0xFFFFFFFFu;
-            ckey = min(ckey, __shfl_xor_sync(gmask, ckey, 2, kGroup));
-            ckey = min(ckey, __shfl_xor_sync(gmask, ckey, 4, kGroup));
+            ckey = min(ckey, __shfl_xor_sync(gmask, ckey, 2, kBc7Group));
+            ckey = min(ckey, __shfl_xor_sync(gmask, ckey, 4, kBc7Group));
             if (ckey != 0xFFFFFFFFu) {
                 const int bj = (int)(ckey & 3u);
                 uint32_t ew0 = (uint32_t)q1[0][0] | ((uint32_t)q1[0][1] << 6) | ((uint32_t)q1[0][2] << 12) | ((uint32_t)pb1[0] << 18);
                 uint32_t ew1 = (uint32_t)q1[1][0] | ((uint32_t)q1[1][1] << 6) | ((uint32_t)q1[1][2] << 12);
                 uint32_t ilo = (uint32_t)i1, ihi = (uint32_t)(i1 >> 32);
-                uint32_t a0 = __shfl_sync(gmask, ew0, 2 * bj, kGroup), a1 = __shfl_sync(gmask, ew1, 2 * bj, kGroup);
-                uint32_t b0w = __shfl_sync(gmask, ew0, 2 * bj + 1, kGroup), b1w = __shfl_sync(gmask, ew1, 2 * bj + 1, kGroup);
-                uint32_t il = __shfl_sync(gmask, ilo, 2 * bj, kGroup) | __shfl_sync(gmask, ilo, 2 * bj + 1, kGroup);
-                uint32_t ih = __shfl_sync(gmask, ihi, 2 * bj, kGroup) | __shfl_sync(gmask, ihi, 2 * bj + 1, kGroup);
-                int part = __shfl_sync(gmask, pj, 2 * bj, kGroup);
+                uint32_t a0 = __shfl_sync(gmask, ew0, 2 * bj, kBc7Group), a1 = __shfl_sync(gmask, ew1, 2 * bj, kBc7Group);
+                uint32_t b0w = __shfl_sync(gmask, ew0, 2 * bj + 1, kBc7Group), b1w = __shfl_sync(gmask, ew1, 2 * bj + 1, kBc7Group);
+                uint32_t il = __shfl_sync(gmask, ilo, 2 * bj, kBc7Group) | __shfl_sync(gmask, ilo, 2 * bj + 1, kBc7Group);
+                uint32_t ih = __shfl_sync(gmask, ihi, 2 * bj, kBc7Group) | __shfl_sync(gmask, ihi, 2 * bj + 1, kBc7Group);
+                int part = __shfl_sync(gmask, pj, 2 * bj, kBc7Group);
                 err = (int)(ckey >> 2);
                 uint64_t full = (uint64_t)il | ((uint64_t)ih << 32);
                 Bits128 o;
@@ -535,7 +535,7 @@ cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out
         ztc::trace_units(nblocks);
         ztc::bc7_mode6_kernel<<<(nblocks + 127) / 128, 128, 0, stream>>>(src, bw, by0, nblocks, out, count, items);
     }
-    int groups_per_cta = 128 / ztc::kGroup;
+    int groups_per_cta = 128 / ztc::kBc7Group;
     int ctas = (nblocks + groups_per_cta - 1) / groups_per_cta;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);

@@ -55,7 +55,7 @@ ZTC_DEV int bc1_fit4(const Bc1Texels &T, uint32_t c0, uint32_t c1, uint32_t &idx
         bits |= (uint32_t)(m & 3) << (2 * i);
     }
     idx = bits;
-    int ksum = __popc(bits & 0x55555555u) + 2 * __popc(bits & 0xAAAAAAAAu);
+    int ksum = popc(bits & 0x55555555u) + 2 * popc(bits & 0xAAAAAAAAu);
     return ((sum - ksum) >> 2) + T.pp;
 }
 

@@ -47,8 +47,8 @@ ZTC_DEV uint32_t box4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, bool srgb,
 }
 
 ZTC_DEV uint32_t ld_texel(const uint8_t *p) {
-    if ((((uintptr_t)p) & 3u) == 0) return __ldg((const uint32_t *)p);
-    return (uint32_t)__ldg(p) | ((uint32_t)__ldg(p + 1) << 8) | ((uint32_t)__ldg(p + 2) << 16) | ((uint32_t)__ldg(p + 3) << 24);
+    if ((((uintptr_t)p) & 3u) == 0) return ldg((const uint32_t *)p);
+    return (uint32_t)ldg(p) | ((uint32_t)ldg(p + 1) << 8) | ((uint32_t)ldg(p + 2) << 16) | ((uint32_t)ldg(p + 3) << 24);
 }
 ZTC_DEV void st_texel(uint8_t *p, uint32_t v) {
     if ((((uintptr_t)p) & 3u) == 0) { *(uint32_t *)p = v; return; }

@@ -8,17 +8,45 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#define ZTC_DEV __device__ __forceinline__
+#include <cmath>
+#include <cstring>
+
+// Per-block encoder functions are host+device: the device build is the product; the host build lets the CPU test
+// suite run the same block logic against the oracle without a GPU (tests/test_block_logic_on_host.py).
+#define ZTC_DEV __host__ __device__ __forceinline__
 
 namespace ztc {
+
+#ifdef __CUDA_ARCH__
+ZTC_DEV uint32_t dot4(uint32_t a, uint32_t b) { return __dp4a(a, b, 0u); }  // sum of byte products (exact, unsigned)
+ZTC_DEV int popc(uint32_t v) { return __popc(v); }
+ZTC_DEV uint32_t f_as_u(float f) { return __float_as_uint(f); }
+ZTC_DEV uint32_t brev(uint32_t v) { return __brev(v); }
+ZTC_DEV int trunc_i(float f) { return __float2int_rz(f); }
+template <typename T> ZTC_DEV T ldg(const T *p) { return __ldg(p); }
+#else
+inline uint32_t dot4(uint32_t a, uint32_t b) {
+    uint32_t s = 0;
+    for (int k = 0; k < 4; k++) s += ((a >> (8 * k)) & 0xFFu) * ((b >> (8 * k)) & 0xFFu);
+    return s;
+}
+inline int popc(uint32_t v) { return __builtin_popcount(v); }
+inline uint32_t f_as_u(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+inline uint32_t brev(uint32_t v) { uint32_t r = 0; for (int k = 0; k < 32; k++) r |= ((v >> k) & 1u) << (31 - k); return r; }
+inline int trunc_i(float f) { return (int)f; }  // only called on in-range values
+template <typename T> inline T ldg(const T *p) { return *p; }
+#endif
 
 // C's (int)f as the reference is compiled for x86-64 (cvttss2si): truncation toward zero, and INT_MIN for NaN or
 // any value outside [-2^31, 2^31). CUDA's own conversion saturates instead, so out-of-range values (possible in
 // degenerate least-squares solves) would otherwise decode differently.
 ZTC_DEV int f2i_x86(float f) {
-    return (f >= -2147483648.0f && f < 2147483648.0f) ? __float2int_rz(f) : (int)0x80000000;
+    return (f >= -2147483648.0f && f < 2147483648.0f) ? trunc_i(f) : (int)0x80000000;
 }
-ZTC_DEV int clampi(int v, int lo, int hi) { return v < lo ? lo : v > hi ? hi : v; }
+// min/max form on purpose: with nvcc 12.9 for sm_100a, the equivalent ternary chain followed by an equality test on
+// the clamped value (the BC6H endpoint unquantiser) was observed to produce wrong results on the device (a
+// mid-range value took the == 1023 branch); the host build and this form are correct.
+ZTC_DEV int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 ZTC_DEV float clamp255(float v) { return v < 0.0f ? 0.0f : v > 255.0f ? 255.0f : v; }  // NaN passes through
 // candidate k of {g-1, g, g+1}, wrapping like the reference's compiled three-candidate loops
 ZTC_DEV int around(int g, int k) { return (int)((unsigned)g + (unsigned)k - 1u); }
@@ -34,8 +62,6 @@ ZTC_DEV int expand_bits(int v, int n) { v <<= 8 - n; return v | (v >> n); }  // 
 ZTC_DEV uint32_t chan(uint32_t t, int c) { return (t >> (8 * c)) & 0xFFu; }
 ZTC_DEV uint32_t pack_rgb(int r, int g, int b) { return (uint32_t)r | ((uint32_t)g << 8) | ((uint32_t)b << 16); }
 ZTC_DEV uint32_t pack_rgba(int r, int g, int b, int a) { return pack_rgb(r, g, b) | ((uint32_t)a << 24); }
-// sum of byte products of two packed texels (exact, unsigned)
-ZTC_DEV uint32_t dot4(uint32_t a, uint32_t b) { return __dp4a(a, b, 0u); }
 
 // 128-bit little-endian block assembled LSB-first in registers (the reference's bit-writer order)
 struct Bits128 {
@@ -80,11 +106,11 @@ struct SrcU8 {
 ZTC_DEV uint32_t load_texel(const SrcU8 &s, int x, int y) {
     const uint8_t *p = s.base + (size_t)y * s.stride + (size_t)x * (size_t)s.channels;
     if (s.channels == 4) {
-        if ((((uintptr_t)p) & 3u) == 0) return __ldg((const uint32_t *)p);
-        return (uint32_t)__ldg(p) | ((uint32_t)__ldg(p + 1) << 8) | ((uint32_t)__ldg(p + 2) << 16) | ((uint32_t)__ldg(p + 3) << 24);
+        if ((((uintptr_t)p) & 3u) == 0) return ldg((const uint32_t *)p);
+        return (uint32_t)ldg(p) | ((uint32_t)ldg(p + 1) << 8) | ((uint32_t)ldg(p + 2) << 16) | ((uint32_t)ldg(p + 3) << 24);
     }
-    if (s.channels == 2) return (uint32_t)__ldg(p) | ((uint32_t)__ldg(p + 1) << 8) | 0xFF000000u;
-    return (uint32_t)__ldg(p) | 0xFF000000u;
+    if (s.channels == 2) return (uint32_t)ldg(p) | ((uint32_t)ldg(p + 1) << 8) | 0xFF000000u;
+    return (uint32_t)ldg(p) | 0xFF000000u;
 }
 
 // 16 texels of block (bx, by), texel i at (i & 3, i >> 2), clamped to the image like the reference
@@ -93,7 +119,7 @@ ZTC_DEV void gather_block(const SrcU8 &s, int bx, int by, uint32_t t[16]) {
     if (s.vec16 && x0 + 3 < s.w && y0 + 3 < s.h) {
         #pragma unroll
         for (int r = 0; r < 4; r++) {
-            uint4 v = __ldg((const uint4 *)(s.base + (size_t)(y0 + r) * s.stride + (size_t)x0 * 4));
+            uint4 v = ldg((const uint4 *)(s.base + (size_t)(y0 + r) * s.stride + (size_t)x0 * 4));
             t[4 * r + 0] = v.x; t[4 * r + 1] = v.y; t[4 * r + 2] = v.z; t[4 * r + 3] = v.w;
         }
         return;

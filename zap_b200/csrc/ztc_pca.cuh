@@ -8,7 +8,7 @@ namespace ztc {
 
 template <int NC>
 ZTC_DEV void pca_endpoints(const uint32_t t[16], uint32_t mask, float lo[4], float hi[4]) {
-    const float cnt = (float)__popc(mask);
+    const float cnt = (float)popc(mask);
     float mu[NC];
     #pragma unroll
     for (int c = 0; c < NC; c++) mu[c] = 0.0f;

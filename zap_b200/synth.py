@@ -24,6 +24,12 @@ def _gen(seed, device):
     return g
 
 
+def _cells(w, h, finest_period_octaves_scale):
+    """Lattice cells of the base octave so that detail scales with the texture: for the 4-octave colour noise
+    (scale 64) the finest octave has a period of 8 texels, i.e. block-scale detail like a photograph's."""
+    return max(2, min(w, h) // finest_period_octaves_scale)
+
+
 def value_noise(h, w, octaves, base_cells, g, device, channels=1, persistence=0.5):
     """Sum of `octaves` lattice value-noise layers (bicubic-interpolated lattices), normalised to [0, 1]."""
     out = torch.zeros(channels, h, w, device=device)
@@ -56,7 +62,7 @@ def colour_texture(w, h, seed=0, alpha="opaque", device="cpu"):
     """HxWx4 uint8. alpha: "opaque" (255) or "noise" (2-octave noise, thresholded at 30% to 0, else smooth)."""
     g = _gen(seed, device)
     img = _gradients(h, w, 3, g, device)
-    img = img * 0.7 + 0.3 * value_noise(h, w, 4, 4, g, device, channels=3)
+    img = img * 0.7 + 0.3 * value_noise(h, w, 4, _cells(w, h, 64), g, device, channels=3)
     for _ in range(20):
         rw = int(torch.randint(max(1, w // 32), max(2, w // 4), (1,), generator=g, device=device))
         rh = int(torch.randint(max(1, h // 32), max(2, h // 4), (1,), generator=g, device=device))
@@ -68,7 +74,7 @@ def colour_texture(w, h, seed=0, alpha="opaque", device="cpu"):
     if alpha == "opaque":
         rgba[..., 3] = 255
     else:
-        a = value_noise(h, w, 2, 4, g, device)[0]
+        a = value_noise(h, w, 2, _cells(w, h, 32), g, device)[0]
         a = torch.where(a < 0.3, torch.zeros_like(a), (a - 0.3) / 0.7)
         rgba[..., 3] = (a * 255 + 0.5).to(torch.uint8)
     return rgba
@@ -77,7 +83,7 @@ def colour_texture(w, h, seed=0, alpha="opaque", device="cpu"):
 def normal_map(w, h, seed=0, device="cpu"):
     """HxWx2 uint8 tangent-space normal xy (unorm8) from a 5-octave fBm heightfield."""
     g = _gen(seed, device)
-    hf = value_noise(h + 2, w + 2, 5, 8, g, device)[0] * 32.0
+    hf = value_noise(h + 2, w + 2, 5, _cells(w, h, 128), g, device)[0] * 32.0
     p = hf.view(1, 1, h + 2, w + 2)
     kx = torch.tensor([[-1.0, 0, 1], [-2, 0, 2], [-1, 0, 1]], device=device).view(1, 1, 3, 3) / 8
     gx = F.conv2d(p, kx)[0, 0]
@@ -91,7 +97,7 @@ def normal_map(w, h, seed=0, device="cpu"):
 def hdr_texture(w, h, seed=0, device="cpu"):
     """HxWx3 float16 (non-negative, finite)."""
     g = _gen(seed, device)
-    l2 = value_noise(h, w, 3, 4, g, device)[0]
+    l2 = value_noise(h, w, 3, _cells(w, h, 64), g, device)[0]
     l2 = (l2 - l2.min()) / (l2.max() - l2.min() + 1e-9) * 16.0 - 8.0  # log2 luminance spread over [-8, 8]
     hue = _gradients(h, w, 2, g, device) * 0.8 + 0.2
     lum = torch.exp2(l2)
