@@ -108,3 +108,16 @@ def test_mip_block_logic(emu, oracle):
             out = np.zeros((nh, nw, 4), np.uint8)
             emu.emu_mip_next(img.ctypes.data, w, h, w * 4, srgb, out.ctypes.data, nw * 4)
             assert np.array_equal(out, oracle.mip_next(img, srgb))
+
+
+def test_bc6h_block_logic_extreme_values(emu, oracle):
+    """Negative, NaN, +inf, tiny (half-subnormal) and huge (clamped) floats in one image."""
+    rng = np.random.default_rng(4)
+    wild = (2.0 ** rng.uniform(-30, 20, (37, 29, 4))).astype(np.float32)
+    wild[::3, ::2, 1] *= -1
+    wild[5, 5, 0] = np.inf
+    wild[6, 6, 2] = np.nan
+    h, w = wild.shape[:2]
+    out = np.zeros(oracle_lib.bc_size(w, h, BC7), np.uint8)
+    emu.emu_bc6h_encode(wild.ctypes.data, w, h, w * 4, out.ctypes.data)
+    assert np.array_equal(out, oracle.bc6h_encode(wild))

@@ -22,9 +22,8 @@ ZTC_DEV uint32_t half_to_unsigned(uint32_t h) {
     if (((h >> 10) & 31u) == 31u) return (h & 1023u) ? 0u : 0x7BFFu;
     return h;
 }
-// 10-bit endpoint -> 16-bit (zap_tex.h:837): 0 -> 0, 1023 -> 0xFFFF, else ((e << 16) + 0x8000) >> 10. Written
-// branch-free (1023 gives 65536, capped to 0xFFFF): see clampi for the device miscompile the branchy form met.
-ZTC_DEV int bc6_unq(int e) { return e ? min(((e << 16) + 0x8000) >> 10, 0xFFFF) : 0; }
+// 10-bit endpoint -> 16-bit (zap_tex.h:837). Callers clamp e with clampi's min/max form (see ztc_common.cuh).
+ZTC_DEV int bc6_unq(int e) { return e == 0 ? 0 : e == 1023 ? 0xFFFF : ((e << 16) + 0x8000) >> 10; }
 ZTC_DEV int bc6_fin(int u) { return (u * 31) >> 6; }
 ZTC_DEV int bc6_nearest(float u) {  // zap_tex.h:841-851
     int g = f2i_x86((u - 32.0f) / 64.0f + 0.5f), best = 0;
