@@ -112,6 +112,17 @@ ZTC_API size_t zap_tex_cuda_mip_chain_bytes(int w, int h);
 ZTC_API int zap_tex_cuda_mip_chain_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int srgb,
                                uint8_t *dst, void *stream);
 
+/* Allocation-free BC7 encode. No counterpart in the reference (zap_tex.h allocates nothing because it runs on the
+   CPU); it exists for callers that cannot allocate device memory when they encode: work recorded into a CUDA
+   graph, real-time frame loops, engines with a fixed up-front GPU budget, plug-in hosts that only hand over their
+   own buffers. Same bytes as zap_tex_cuda_bc_encode_dev(..., ZTC_BC7, ...), device pointers, async on `stream`.
+   It never calls cudaMalloc/cudaFree: its work list is a static device array sized for at most 1048576 4x4
+   blocks (4096 x 4096 texels, about 8 MB held by every GPU that loads the library); larger textures return
+   ZTC_ERR_INVALID_ARG. The first call on a device looks up that array's address (make it before any stream
+   capture). All calls share the array: calls whose kernels overlap on the GPU race, so serialise them (one
+   stream, or events). */
+ZTC_API int zap_tex_cuda_bc7_encode_noalloc_dev(const uint8_t *rgba, int w, int h, size_t stride, void *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,6 +17,7 @@ void trace_end(cudaStream_t) {}
 void trace_units(long) {}
 void trace_units_dev(const uint32_t *, cudaStream_t) {}
 }  // namespace ztc
+int ztc_set_error(int status, const char *) { return status; }
 
 using namespace ztc;
 

@@ -1,0 +1,55 @@
+"""The allocation-free BC7 entry point (zap_tex_cuda_bc7_encode_noalloc_dev), through the C ABI.
+
+Some callers cannot allocate device memory while they encode - work recorded into a CUDA graph, real-time frame
+loops, engines with a fixed up-front GPU budget, plug-in hosts that only hand over their own buffers. This entry
+point keeps its BC7 work list in a static device array instead of allocating one. Its output must be byte-for-byte
+the output of the allocating entry point, also on consecutive calls that share that array (the list must start
+empty every time), and oversize textures must be refused before anything runs.
+
+The file name sorts last so that a run stopping at the first failure has run every other test already.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _call(lib, tex, out, stream):
+    h, w = tex.shape[0], tex.shape[1]
+    return lib.zap_tex_cuda_bc7_encode_noalloc_dev(C.c_void_p(tex.data_ptr()), w, h, tex.stride(0), C.c_void_p(out.data_ptr()),
+                                                   C.c_void_p(stream.cuda_stream))
+
+
+def test_noalloc_bc7_matches_allocating_entry_point(cuda_lib):
+    import torch
+
+    import zap_b200.synth as S
+    lib = cuda_lib.load()
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(3)
+    noise = torch.from_numpy(rng.integers(0, 256, (360, 200, 4), dtype=np.uint8)).cuda()
+    inputs = [S.colour_texture(1024, 512, seed=1, alpha="noise", device="cuda"),  # mostly mode 6, some listed blocks
+              noise,                                                              # every block on the work list
+              S.colour_texture(301, 197, seed=2, alpha="opaque", device="cuda")]  # odd size, fewer blocks than before
+    for tex in inputs:  # consecutive calls reuse the static work list
+        expect = cuda_lib.bc_encode_dev(tex, cuda_lib.BC7)
+        got = torch.full_like(expect, 0xAB)
+        assert _call(lib, tex, got, stream) == 0, lib.zap_tex_cuda_last_error()
+        torch.cuda.synchronize()
+        assert torch.equal(got, expect)
+
+
+def test_noalloc_rejects_textures_beyond_its_limit(cuda_lib):
+    import torch
+    lib = cuda_lib.load()
+    stream = torch.cuda.current_stream()
+    tex = torch.zeros((4100, 4096, 4), dtype=torch.uint8, device="cuda")  # 1025 x 1024 blocks > 1048576
+    out = torch.zeros(16, dtype=torch.uint8, device="cuda")
+    assert _call(lib, tex, out, stream) == -1
+    assert b"1048576" in lib.zap_tex_cuda_last_error()
+    small = torch.zeros((8, 8, 4), dtype=torch.uint8, device="cuda")
+    out = torch.zeros(64, dtype=torch.uint8, device="cuda")
+    assert _call(lib, small, out, stream) == 0  # still usable after the refusal
+    torch.cuda.synchronize()

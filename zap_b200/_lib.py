@@ -63,6 +63,7 @@ def _declare(lib):
         "zap_tex_cuda_bc6h_encode_half_dev": ([vp, vp, i, i, i, sz, vp, vp], i),
         "zap_tex_cuda_mip_chain_bytes": ([i, i], sz),
         "zap_tex_cuda_mip_chain_dev": ([vp, vp, i, i, sz, i, vp, vp], i),
+        "zap_tex_cuda_bc7_encode_noalloc_dev": ([vp, i, i, sz, vp, vp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

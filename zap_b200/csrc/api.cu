@@ -261,6 +261,8 @@ int check_image(const void *p, const void *out, int w, int h, size_t stride, siz
 
 }  // namespace
 
+int ztc_set_error(int status, const char *msg) { return fail(status, "%s", msg); }
+
 extern "C" {
 
 int zap_tex_cuda_version(void) { return ZAP_TEX_CUDA_VERSION; }

@@ -12,6 +12,8 @@
 //      w(n-1-j) = 64 - w(j), mode 1 shares its p-bit between a subset's endpoints, and mode 1 decodes alpha 255
 //      on the opaque blocks it is tried on. So kernel B compares fit errors directly.
 // Every float expression keeps the reference's order; integer argmins keep the first candidate on ties.
+#include <mutex>
+
 #include "ztc_common.cuh"
 #include "ztc_internal.h"
 #include "ztc_pca.cuh"
@@ -545,4 +547,66 @@ cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out
     ztc::trace_units_dev(count, stream);
     ztc::bc7_hard_kernel<<<ctas, 128, 0, stream>>>(src, bw, by0, out, count, items);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- allocation-free BC7 entry point
+// Some callers cannot allocate device memory at encode time: code running inside a CUDA graph capture or a
+// real-time frame loop where an allocation would stall or be forbidden, engines that own a fixed GPU memory
+// budget handed out up front, or plug-in hosts that give a texture tool only the buffers it is called with.
+// zap_tex_cuda_bc7_encode_noalloc_dev serves them: its BC7 work list lives in the file-scope array below, sized
+// for at most kNoAllocMaxBlocks 4x4 blocks (a 4096 x 4096 texture), which every GPU that loads this library holds
+// until the process exits (about 8 MB). The first call on a device looks up the array's device address.
+namespace ztc {
+constexpr size_t kNoAllocMaxBlocks = size_t(1) << 20;
+constexpr size_t kNoAllocBytes = 256 + kNoAllocMaxBlocks * sizeof(uint2);
+static __device__ __align__(256) unsigned char g_bc7_noalloc_scratch[kNoAllocBytes];
+}  // namespace ztc
+
+namespace {
+std::mutex g_noalloc_lock;
+void *g_noalloc_addr[64];  // per device: device address of g_bc7_noalloc_scratch
+}  // namespace
+
+extern "C" __attribute__((visibility("default"))) int zap_tex_cuda_bc7_encode_noalloc_dev(const uint8_t *rgba, int w, int h,
+                                                                                           size_t stride, void *out, void *stream) {
+    if (!rgba || !out) return ztc_set_error(-1, "null pointer");
+    if (w < 1 || h < 1 || w > (1 << 24) || h > (1 << 24)) return ztc_set_error(-1, "size out of range");
+    if (stride < (size_t)w * 4) return ztc_set_error(-1, "stride below 4 * width");
+    const size_t bw = (size_t)(w + 3) / 4, bh = (size_t)(h + 3) / 4;
+    if (bw * bh > ztc::kNoAllocMaxBlocks)
+        return ztc_set_error(-1, "texture has more 4x4 blocks than the allocation-free BC7 entry point holds (1048576)");
+    int dev = 0, major = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { cudaGetLastError(); return ztc_set_error(-6, "no CUDA device"); }
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (major != 10) return ztc_set_error(-6, "this build targets sm_100a");
+    void *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> g(g_noalloc_lock);
+        if (!g_noalloc_addr[dev]) {  // set-up, once per device, with that device current
+            cudaError_t e = cudaGetSymbolAddress(&g_noalloc_addr[dev], ztc::g_bc7_noalloc_scratch);
+            if (e != cudaSuccess) {
+                g_noalloc_addr[dev] = nullptr;
+                cudaGetLastError();
+                return ztc_set_error(-3, cudaGetErrorString(e));
+            }
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    ztc::SrcU8 src{rgba, stride, w, h, 4, (((uintptr_t)rgba | stride) & 15u) == 0};
+    uint32_t *count = (uint32_t *)scratch;
+    uint2 *items = (uint2 *)((uint8_t *)scratch + 256);
+    const int nblocks = (int)(bw * bh);
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), s);  // the list must start empty on every call
+    if (e == cudaSuccess) {
+        ztc::bc7_mode6_kernel<<<(nblocks + 127) / 128, 128, 0, s>>>(src, (int)bw, 0, nblocks, (uint8_t *)out, count, items);
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int ctas = (nblocks + 15) / 16;
+        ctas = ctas < sms * 8 ? ctas : sms * 8;
+        ztc::bc7_hard_kernel<<<ctas, 128, 0, s>>>(src, (int)bw, 0, (uint8_t *)out, count, items);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) { cudaGetLastError(); return ztc_set_error(-3, cudaGetErrorString(e)); }
+    return 0;
 }

@@ -39,6 +39,9 @@ size_t bc7_scratch_bytes(size_t nblocks);
 size_t astc_scratch_bytes(size_t nblocks);
 }  // namespace ztc
 
+// records the calling thread's error message (zap_tex_cuda_last_error) and returns status
+int ztc_set_error(int status, const char *msg);
+
 cudaError_t ztc_launch_bcn(int fmt, const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, cudaStream_t stream);
 cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, void *scratch, cudaStream_t stream);
 cudaError_t ztc_launch_bc6h(const ztc::SrcHdr &src, int by0, int nby, uint8_t *out, cudaStream_t stream);
