@@ -112,6 +112,35 @@ ZTC_API size_t zap_tex_cuda_mip_chain_bytes(int w, int h);
 ZTC_API int zap_tex_cuda_mip_chain_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int srgb,
                                uint8_t *dst, void *stream);
 
+/* ---------------------------------------------------------------- batched encoding
+   Many textures at once, each with its mip chain, mixed formats. No single reference counterpart: it replaces the
+   caller loop of zap.c:330-342 (zap_bc_encode per level, zap_mip_next between levels) run over many textures.
+   Output per item: its levels' blocks concatenated, largest first (the DDS order of zap.c:332-349); bytes are
+   the reference's for every level. The plan (mip buffer, tile queues, CUDA graph) is built once by
+   zap_tex_cuda_batch_create; zap_tex_cuda_batch_run replays it as one graph launch, reading the items' current
+   source texels. Pointers are device pointers. */
+typedef struct zap_tex_cuda_item {
+    const uint8_t *src; /* level 0, RGBA8 */
+    int w, h;           /* 1 .. 65536 */
+    size_t stride;      /* bytes per row of src */
+    int fmt;            /* ZTC_BC1 .. ZTC_BC7 */
+    int srgb;           /* mip filter in linear light (forced off for BC4/BC5, like zap.c:325) */
+    int levels;         /* 0 = full chain (zap_tex_cuda_mip_levels), else the number of levels to encode */
+    uint8_t *dst;       /* zap_tex_cuda_batch_item_bytes(w, h, fmt, levels) bytes */
+} zap_tex_cuda_item;
+typedef struct zap_tex_cuda_batch zap_tex_cuda_batch;
+#define ZTC_BATCH_AUTOTUNE 1 /* time each format's kernel at 64/128/256 blocks per CTA on the batch, keep the fastest */
+#define ZTC_BATCH_NO_GRAPH 2 /* launch the sequence directly instead of capturing it into a CUDA graph */
+ZTC_API size_t zap_tex_cuda_batch_item_bytes(int w, int h, int fmt, int levels);
+ZTC_API int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *items, int n, int flags,
+                                      zap_tex_cuda_batch **out);
+ZTC_API int zap_tex_cuda_batch_run(zap_tex_cuda_batch *batch, void *stream);
+/* the same work as one plain launch per texture and per level (the per-texture caller loop), for comparison */
+ZTC_API int zap_tex_cuda_batch_run_plain(zap_tex_cuda_batch *batch, void *stream);
+/* text: tile counts, chosen blocks per CTA and autotune timings per format */
+ZTC_API int zap_tex_cuda_batch_info(zap_tex_cuda_batch *batch, char *buf, size_t cap);
+ZTC_API int zap_tex_cuda_batch_destroy(zap_tex_cuda_batch *batch);
+
 /* Allocation-free BC7 encode. No counterpart in the reference (zap_tex.h allocates nothing because it runs on the
    CPU); it exists for callers that cannot allocate device memory when they encode: work recorded into a CUDA
    graph, real-time frame loops, engines with a fixed up-front GPU budget, plug-in hosts that only hand over their

@@ -181,6 +181,81 @@ def mip_next_f_dev(t, out=None, stream=None, ctx=None):
     return out
 
 
+class _Item(C.Structure):
+    """zap_tex_cuda_item (include/zap_tex_cuda.h)."""
+    _fields_ = [("src", C.c_void_p), ("w", C.c_int), ("h", C.c_int), ("stride", C.c_size_t), ("fmt", C.c_int),
+                ("srgb", C.c_int), ("levels", C.c_int), ("dst", C.c_void_p)]
+
+
+class Batch:
+    """Many textures with their mip chains, mixed formats, encoded by one CUDA graph launch.
+
+    textures: HxWx4 uint8 CUDA tensors (level 0); formats / srgb / levels: one per texture (levels 0 = full chain).
+    After run(), outputs[i] holds texture i's levels concatenated, largest first (zap_bc_size bytes per level)."""
+
+    def __init__(self, textures, formats, srgb=None, levels=None, autotune=False, graph=True, ctx=None):
+        import torch
+        n = len(textures)
+        srgb = [1] * n if srgb is None else list(srgb)
+        levels = [0] * n if levels is None else list(levels)
+        lib = load()
+        self.textures = list(textures)
+        self.formats = list(formats)
+        self.outputs = []
+        items = (_Item * n)()
+        for i, t in enumerate(self.textures):
+            w, h, stride = _dev_img(t, (4,))
+            nbytes = int(lib.zap_tex_cuda_batch_item_bytes(w, h, self.formats[i], levels[i]))
+            out = torch.empty(max(1, nbytes), dtype=torch.uint8, device=t.device)
+            self.outputs.append(out[:nbytes])
+            items[i] = _Item(t.data_ptr(), w, h, stride, self.formats[i], int(srgb[i]), int(levels[i]), out.data_ptr())
+        self._items = items
+        flags = (1 if autotune else 0) | (0 if graph else 2)
+        handle = C.c_void_p()
+        check(lib.zap_tex_cuda_batch_create(ctx, items, n, flags, C.byref(handle)), "batch_create")
+        self._h = handle
+        self.levels = [levels[i] or mip_levels(self.textures[i].shape[1], self.textures[i].shape[0]) for i in range(n)]
+        self.pixels = 0
+        for t, L in zip(self.textures, self.levels):
+            w, h = t.shape[1], t.shape[0]
+            for _ in range(L):
+                self.pixels += w * h
+                w, h = max(1, w // 2), max(1, h // 2)
+
+    def run(self, stream=None):
+        check(load().zap_tex_cuda_batch_run(self._h, _stream(stream)), "batch_run")
+
+    def run_plain(self, stream=None):
+        check(load().zap_tex_cuda_batch_run_plain(self._h, _stream(stream)), "batch_run_plain")
+
+    def info(self):
+        buf = C.create_string_buffer(4096)
+        load().zap_tex_cuda_batch_info(self._h, buf, len(buf))
+        return buf.value.decode()
+
+    def level_views(self, i):
+        """Texture i's encoded levels as separate uint8 tensors (views into outputs[i])."""
+        t = self.textures[i]
+        w, h, off, views = t.shape[1], t.shape[0], 0, []
+        for _ in range(self.levels[i]):
+            n = bc_size(w, h, self.formats[i])
+            views.append(self.outputs[i][off:off + n])
+            off += n
+            w, h = max(1, w // 2), max(1, h // 2)
+        return views
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load().zap_tex_cuda_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def mip_chain_dev(t, srgb, stream=None, ctx=None):
     """Levels 1.. of t's mip chain as a list of HxWx4 uint8 CUDA tensors (views of one allocation)."""
     import torch

@@ -64,6 +64,12 @@ def _declare(lib):
         "zap_tex_cuda_mip_chain_bytes": ([i, i], sz),
         "zap_tex_cuda_mip_chain_dev": ([vp, vp, i, i, sz, i, vp, vp], i),
         "zap_tex_cuda_bc7_encode_noalloc_dev": ([vp, i, i, sz, vp, vp], i),
+        "zap_tex_cuda_batch_item_bytes": ([i, i, i, i], sz),
+        "zap_tex_cuda_batch_create": ([vp, vp, i, i, C.POINTER(vp)], i),
+        "zap_tex_cuda_batch_run": ([vp, vp], i),
+        "zap_tex_cuda_batch_run_plain": ([vp, vp], i),
+        "zap_tex_cuda_batch_info": ([vp, C.c_char_p, sz], i),
+        "zap_tex_cuda_batch_destroy": ([vp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -42,6 +42,12 @@ constexpr int kSlots = 1 << 16;
 void trace_begin(const char *name, cudaStream_t s) {
     if (!g_trace_on) return;
     TraceRec r{name, nullptr, nullptr, 0, nullptr};
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {  // nothing to time while capturing
+        cudaGetLastError();
+        t_open.push_back(r);
+        return;
+    }
     cudaEventCreate(&r.a);
     cudaEventCreate(&r.b);
     cudaEventRecord(r.a, s);
@@ -51,7 +57,7 @@ void trace_units(long n) {
     if (g_trace_on && !t_open.empty()) t_open.back().units = n;
 }
 void trace_units_dev(const uint32_t *d_count, cudaStream_t s) {
-    if (!g_trace_on || t_open.empty()) return;
+    if (!g_trace_on || t_open.empty() || !t_open.back().a) return;
     std::lock_guard<std::mutex> g(g_trace_lock);
     if (!g_slots && cudaMallocHost((void **)&g_slots, kSlots * sizeof(uint32_t)) != cudaSuccess) { g_slots = nullptr; return; }
     if (g_slot_next >= kSlots) return;
@@ -63,6 +69,7 @@ void trace_end(cudaStream_t s) {
     if (!g_trace_on || t_open.empty()) return;
     TraceRec r = t_open.back();
     t_open.pop_back();
+    if (!r.a) return;  // began during a capture
     cudaEventRecord(r.b, s);
     std::lock_guard<std::mutex> g(g_trace_lock);
     g_trace.push_back(r);
@@ -262,6 +269,7 @@ int check_image(const void *p, const void *out, int w, int h, size_t stride, siz
 }  // namespace
 
 int ztc_set_error(int status, const char *msg) { return fail(status, "%s", msg); }
+int ztc_ctx_activate(zap_tex_cuda_ctx *ctx) { return resolve(ctx); }
 
 extern "C" {
 

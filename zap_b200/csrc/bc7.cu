@@ -329,18 +329,12 @@ ZTC_DEV bool rank_less(float e, int p, float e2, int p2) { return e < e2 || (!(e
 constexpr int kBc7Group = 8;
 constexpr int kMode1Tries = 4;  // partitions fully fitted after ranking (ZAP__BC7_M1K, zap_tex.h:750-752)
 
-__global__ void __launch_bounds__(128) bc7_hard_kernel(SrcU8 src, int bw, int by0, uint8_t *__restrict__ out,
-                                                       const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
-    const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
-    const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
-    const int ngroups = gridDim.x * (blockDim.x / kBc7Group);
-    const int n = (int)*(volatile const uint32_t *)count;
-    for (int it = blockIdx.x * (blockDim.x / kBc7Group) + (threadIdx.x / kBc7Group); it < n; it += ngroups) {
-        const uint2 item = items[it];
-        const int b = (int)item.x;
-        int err = (int)item.y;  // mode-6 SSE
-        uint32_t t[16];
-        gather_block(src, b % bw, by0 + b / bw, t);
+// One block that mode 6 did not finish, through modes 5 and 1 (zap_tex.h:759-783), by the 8 lanes of a group
+// (lane l, group mask gmask). err is the block's mode-6 SSE; lane 0 writes the block to dst when mode 5 or 1 wins.
+// Every lane holds the block's texels, so all group-level branches below are group-uniform.
+__device__ __forceinline__ void bc7_group_block(const uint32_t t[16], int err, uint8_t *__restrict__ dst, const int l,
+                                                const unsigned gmask) {
+    {
         bool opaque = true;
         #pragma unroll
         for (int i = 0; i < 16; i++) opaque &= (t[i] >> 24) == 255u;
@@ -517,11 +511,87 @@ __global__ void __launch_bounds__(128) bc7_hard_kernel(SrcU8 src, int bw, int by
                 take5 = true;  // a block to write
             }
         }
-        if (take5 && l == 0) store_block16(out + (size_t)b * 16, blk);
+        if (take5 && l == 0) store_block16(dst, blk);
+    }
+}
+
+__global__ void __launch_bounds__(128) bc7_hard_kernel(SrcU8 src, int bw, int by0, uint8_t *__restrict__ out,
+                                                       const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
+    const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
+    const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
+    const int ngroups = gridDim.x * (blockDim.x / kBc7Group);
+    const int n = (int)*(volatile const uint32_t *)count;
+    for (int it = blockIdx.x * (blockDim.x / kBc7Group) + (threadIdx.x / kBc7Group); it < n; it += ngroups) {
+        const uint2 item = items[it];
+        const int b = (int)item.x;
+        uint32_t t[16];
+        gather_block(src, b % bw, by0 + b / bw, t);
+        bc7_group_block(t, (int)item.y, out + (size_t)b * 16, l, gmask);
+    }
+}
+
+// ---------------------------------------------------------------- batched: one persistent launch over a tile queue
+// Each CTA takes tiles of consecutive blocks of one (texture, level) from a device counter. Every thread runs
+// mode 6 on its block; blocks above SSE 64 are compacted in shared memory and finished by the CTA's own 8-lane
+// groups, so modes 6, 5 and 1 run fused in one kernel without a global work list.
+template <int CTA>
+__global__ void __launch_bounds__(CTA) batch_bc7_kernel(const BatchLevel *__restrict__ levels, const BatchTile *__restrict__ tiles,
+                                                        int ntiles, uint32_t *__restrict__ counter) {
+    __shared__ int s_tile, s_count;
+    __shared__ uint2 s_list[CTA];
+    const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
+    const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
+    for (;;) {
+        if (threadIdx.x == 0) { s_tile = (int)atomicAdd(counter, 1u); s_count = 0; }
+        __syncthreads();
+        const int tile = s_tile;
+        if (tile >= ntiles) break;
+        const BatchTile T = tiles[tile];
+        const BatchLevel L = levels[T.level];
+        const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
+        const int b = T.first + (int)threadIdx.x;
+        if ((int)threadIdx.x < T.count) {
+            uint32_t t[16];
+            gather_block(src, b % L.bw, b / L.bw, t);
+            uint4 blk;
+            int err = mode6_encode(t, blk);
+            store_block16(L.dst + (size_t)b * 16, blk);
+            if (err > 16 * 4) s_list[atomicAdd(&s_count, 1)] = make_uint2((uint32_t)b, (uint32_t)err);
+        }
+        __syncthreads();
+        const int n = s_count;
+        for (int k = (int)threadIdx.x / kBc7Group; k < n; k += CTA / kBc7Group) {
+            const uint2 item = s_list[k];
+            const int hb = (int)item.x;
+            uint32_t t[16];
+            gather_block(src, hb % L.bw, hb / L.bw, t);
+            bc7_group_block(t, (int)item.y, L.dst + (size_t)hb * 16, l, gmask);
+        }
+        __syncthreads();
     }
 }
 
 }  // namespace ztc
+
+cudaError_t ztc_launch_batch_bc7(int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
+                                 uint32_t *counter, cudaStream_t stream) {
+    switch (cta) {
+    case 64: ztc::batch_bc7_kernel<64><<<grid, 64, 0, stream>>>(levels, tiles, ntiles, counter); break;
+    case 128: ztc::batch_bc7_kernel<128><<<grid, 128, 0, stream>>>(levels, tiles, ntiles, counter); break;
+    case 256: ztc::batch_bc7_kernel<256><<<grid, 256, 0, stream>>>(levels, tiles, ntiles, counter); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+const void *ztc_batch_bc7_kernel_fn(int cta) {
+    switch (cta) {
+    case 64: return (const void *)ztc::batch_bc7_kernel<64>;
+    case 128: return (const void *)ztc::batch_bc7_kernel<128>;
+    case 256: return (const void *)ztc::batch_bc7_kernel<256>;
+    default: return nullptr;
+    }
+}
 
 size_t ztc::bc7_scratch_bytes(size_t nblocks) { return 256 + nblocks * sizeof(uint2); }
 

@@ -229,3 +229,63 @@ cudaError_t ztc_launch_bcn(int fmt, const ztc::SrcU8 &src, int by0, int nby, uin
     }
     return cudaGetLastError();
 }
+
+// ---------------------------------------------------------------- batched: one persistent launch over a tile queue
+namespace ztc {
+template <int FMT, int CTA>
+__global__ void __launch_bounds__(CTA) batch_bcn_kernel(const BatchLevel *__restrict__ levels, const BatchTile *__restrict__ tiles,
+                                                        int ntiles, uint32_t *__restrict__ counter) {
+    __shared__ int s_tile;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int tile = s_tile;
+        __syncthreads();  // every thread has read s_tile before thread 0 overwrites it
+        if (tile >= ntiles) break;
+        const BatchTile T = tiles[tile];
+        if ((int)threadIdx.x >= T.count) continue;
+        const BatchLevel L = levels[T.level];
+        const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
+        const int b = T.first + (int)threadIdx.x;
+        uint32_t t[16];
+        gather_block(src, b % L.bw, b / L.bw, t);
+        if (FMT == ZTC_FMT_BC1) store_block8(L.dst + (size_t)b * 8, bc1_encode(t));
+        else if (FMT == ZTC_FMT_BC4) store_block8(L.dst + (size_t)b * 8, bc4_encode(t, 0));
+        else if (FMT == ZTC_FMT_BC3) {
+            uint2 a = bc4_encode(t, 3), c = bc1_encode(t);
+            store_block16(L.dst + (size_t)b * 16, make_uint4(a.x, a.y, c.x, c.y));
+        } else {
+            uint2 r = bc4_encode(t, 0), g = bc4_encode(t, 1);
+            store_block16(L.dst + (size_t)b * 16, make_uint4(r.x, r.y, g.x, g.y));
+        }
+    }
+}
+
+template <int FMT>
+static const void *batch_fn(int cta) {
+    switch (cta) {
+    case 64: return (const void *)batch_bcn_kernel<FMT, 64>;
+    case 128: return (const void *)batch_bcn_kernel<FMT, 128>;
+    case 256: return (const void *)batch_bcn_kernel<FMT, 256>;
+    default: return nullptr;
+    }
+}
+}  // namespace ztc
+
+const void *ztc_batch_bcn_kernel_fn(int fmt, int cta) {
+    switch (fmt) {
+    case ZTC_FMT_BC1: return ztc::batch_fn<ZTC_FMT_BC1>(cta);
+    case ZTC_FMT_BC3: return ztc::batch_fn<ZTC_FMT_BC3>(cta);
+    case ZTC_FMT_BC4: return ztc::batch_fn<ZTC_FMT_BC4>(cta);
+    case ZTC_FMT_BC5: return ztc::batch_fn<ZTC_FMT_BC5>(cta);
+    default: return nullptr;
+    }
+}
+
+cudaError_t ztc_launch_batch_bcn(int fmt, int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
+                                 uint32_t *counter, cudaStream_t stream) {
+    const void *fn = ztc_batch_bcn_kernel_fn(fmt, cta);
+    if (!fn) return cudaErrorInvalidValue;
+    void *args[] = {(void *)&levels, (void *)&tiles, (void *)&ntiles, (void *)&counter};
+    return cudaLaunchKernel(fn, dim3(grid), dim3(cta), args, 0, stream);
+}

@@ -155,3 +155,43 @@ cudaError_t ztc_launch_mip_f(const float *src, int w, int h, size_t stride, floa
     ztc::mip_f32_kernel<<<ztc::grid_for(work, 256), 256, 0, stream>>>(src, w, h, stride, dst, dst_stride, nw, nh, vec);
     return cudaGetLastError();
 }
+
+// ---------------------------------------------------------------- batched: one launch per mip depth, all textures
+namespace ztc {
+__global__ void __launch_bounds__(256) batch_mip_kernel(const BatchMip *__restrict__ mips, const BatchMipTile *__restrict__ tiles, int ntiles,
+                                                        const float *__restrict__ tables) {
+    __shared__ float lin[256], thr[256];
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) { lin[k] = tables[k]; thr[k] = tables[256 + k]; }
+    __syncthreads();
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const BatchMipTile T = tiles[tile];
+        if ((int)threadIdx.x >= T.count) continue;
+        const BatchMip M = mips[T.mip];
+        const int pairs = (M.nw + 1) >> 1, id = T.first + (int)threadIdx.x;
+        const int y = id / pairs, x = 2 * (id % pairs);
+        const int y0 = min(2 * y, M.h - 1), y1 = min(2 * y + 1, M.h - 1);
+        const uint8_t *r0 = M.src + (size_t)y0 * M.src_pitch, *r1 = M.src + (size_t)y1 * M.src_pitch;
+        uint8_t *o = M.dst + (size_t)y * M.dst_pitch + (size_t)x * 4;
+        const bool vec = ((((uintptr_t)M.src) | M.src_pitch) & 15u) == 0 && ((((uintptr_t)M.dst) | M.dst_pitch) & 7u) == 0;
+        if (vec && 2 * x + 3 < M.w && x + 1 < M.nw) {
+            uint4 a = ldg((const uint4 *)(r0 + (size_t)x * 8)), b = ldg((const uint4 *)(r1 + (size_t)x * 8));
+            *(uint2 *)o = make_uint2(box4(a.x, a.y, b.x, b.y, M.srgb, lin, thr), box4(a.z, a.w, b.z, b.w, M.srgb, lin, thr));
+        } else {
+            for (int k = 0; k < 2 && x + k < M.nw; k++) {
+                int xx = x + k, x0 = min(2 * xx, M.w - 1), x1 = min(2 * xx + 1, M.w - 1);
+                st_texel(o + (size_t)k * 4, box4(ld_texel(r0 + (size_t)x0 * 4), ld_texel(r0 + (size_t)x1 * 4), ld_texel(r1 + (size_t)x0 * 4),
+                                                 ld_texel(r1 + (size_t)x1 * 4), M.srgb != 0, lin, thr));
+            }
+        }
+    }
+}
+}  // namespace ztc
+
+const void *ztc_batch_mip_kernel_fn() { return (const void *)ztc::batch_mip_kernel; }
+
+cudaError_t ztc_launch_batch_mip(int grid, const ztc::BatchMip *mips, const ztc::BatchMipTile *tiles, int ntiles, const float *srgb_tables,
+                                 cudaStream_t stream) {
+    if (ntiles <= 0) return cudaSuccess;
+    ztc::batch_mip_kernel<<<grid, 256, 0, stream>>>(mips, tiles, ntiles, srgb_tables);
+    return cudaGetLastError();
+}

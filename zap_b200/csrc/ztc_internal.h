@@ -39,8 +39,44 @@ size_t bc7_scratch_bytes(size_t nblocks);
 size_t astc_scratch_bytes(size_t nblocks);
 }  // namespace ztc
 
+// ---------------------------------------------------------------- batched encoder descriptors (device memory)
+namespace ztc {
+struct BatchLevel {     // one (texture, mip level) to encode
+    const uint8_t *src; // RGBA8 texels of the level
+    uint8_t *dst;       // its encoded blocks
+    size_t pitch;       // bytes per texel row
+    int w, h, bw, fmt;
+};
+struct BatchTile {      // consecutive blocks [first, first + count) of one level
+    int level, first, count, pad;
+};
+struct BatchMip {       // one (texture, level d >= 1): built from level d - 1
+    const uint8_t *src;
+    uint8_t *dst;
+    size_t src_pitch, dst_pitch;
+    int w, h, nw, nh, srgb, pad;  // w, h: source level size
+};
+struct BatchMipTile {   // output texel pairs [first, first + count) of one BatchMip, row-major over (nw + 1) / 2 pairs
+    int mip, first, count, pad;
+};
+}  // namespace ztc
+
+cudaError_t ztc_launch_batch_bcn(int fmt, int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
+                                 uint32_t *counter, cudaStream_t stream);
+cudaError_t ztc_launch_batch_bc7(int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
+                                 uint32_t *counter, cudaStream_t stream);
+cudaError_t ztc_launch_batch_mip(int grid, const ztc::BatchMip *mips, const ztc::BatchMipTile *tiles, int ntiles, const float *srgb_tables,
+                                 cudaStream_t stream);
+const void *ztc_batch_bcn_kernel_fn(int fmt, int cta);
+const void *ztc_batch_bc7_kernel_fn(int cta);
+const void *ztc_batch_mip_kernel_fn();
+namespace ztc { void srgb_tables_host(float lin[256], float thr[256]); }
+
 // records the calling thread's error message (zap_tex_cuda_last_error) and returns status
 int ztc_set_error(int status, const char *msg);
+// makes ctx's device current (NULL: the current device's default context) with its tables uploaded
+struct zap_tex_cuda_ctx;
+int ztc_ctx_activate(zap_tex_cuda_ctx *ctx);
 
 cudaError_t ztc_launch_bcn(int fmt, const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, cudaStream_t stream);
 cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, void *scratch, cudaStream_t stream);
