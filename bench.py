@@ -302,6 +302,7 @@ def main():
         if not args.no_extra:
             line["extra"] = extra_workloads(args, dev)
             line["batched"] = batched_workload(args, dev)
+            line["refine"] = refine_workload(args, dev)
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
@@ -343,6 +344,44 @@ def batched_workload(args, dev, n=4096):
            "plan": b.info().strip().splitlines(), "generate_s": gen_s, "plan_s": plan_s}
     b.close()
     del texs, graph_out
+    torch.cuda.empty_cache()
+    return res
+
+
+def refine_workload(args, dev, n=1024, side=256, steps=8, lr=1.0):
+    """Config 4: n textures of side^2 (config 0 content, per-texture seed), BC1 and BC7; the encoder's blocks then
+    `steps` Adam steps of gradient endpoint refinement through the palette-decode adjoint, accepted per block only
+    if the error drops. Textures are stacked into one image: blocks are independent, so this is n encodes at once."""
+    import math
+
+    import torch
+
+    import zap_b200
+    import zap_b200.synth as S
+    tex = torch.cat([S.colour_texture(side, side, seed=20000 + k, device=dev) for k in range(n)], 0).contiguous()
+    npix = tex.shape[0] * tex.shape[1]
+    res = {"textures": n, "side": side, "adam_steps": steps, "lr": lr}
+    for fmt, name, chans in ((zap_b200.BC1, "bc1", 3), (zap_b200.BC7, "bc7", 4)):
+        out = zap_b200.bc_encode_dev(tex, fmt)
+        base = out.clone()
+        ms_enc = time_device(lambda k: zap_b200.bc_encode_dev(tex, fmt, out=out), 5, 2, 1) / 5
+        work = base.clone()
+
+        def refine_step(k):
+            work.copy_(base)
+            zap_b200.refine_dev(tex, fmt, work, steps=steps, lr=lr)
+        ms_ref = time_device(refine_step, 5, 2, 1) / 5
+        work.copy_(base)
+        s0, s1 = zap_b200.refine_dev(tex, fmt, work, steps=steps, lr=lr)
+        torch.cuda.synchronize()
+        e0, e1 = float(s0.double().sum()), float(s1.double().sum())
+        nval = npix * chans
+        psnr = lambda e: 99.0 if e == 0 else 10 * math.log10(255.0 ** 2 * nval / e)  # noqa: E731
+        res[name] = {"encode_ms": ms_enc, "encode_Mpix_s": npix / 1e6 / (ms_enc / 1e3), "refine_ms": ms_ref,
+                     "refine_Mpix_s": npix / 1e6 / (ms_ref / 1e3), "psnr_db": psnr(e0), "psnr_refined_db": psnr(e1),
+                     "psnr_gain_db": psnr(e1) - psnr(e0), "blocks_improved": float((s1 < s0).float().mean()),
+                     "cost_vs_encode": ms_ref / ms_enc}
+    del tex
     torch.cuda.empty_cache()
     return res
 

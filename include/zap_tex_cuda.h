@@ -112,6 +112,33 @@ ZTC_API size_t zap_tex_cuda_mip_chain_bytes(int w, int h);
 ZTC_API int zap_tex_cuda_mip_chain_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int srgb,
                                uint8_t *dst, void *stream);
 
+/* ---------------------------------------------------------------- device decoders
+   replaces zap_bc_decode (zap_tex.h:1526; BC7 all modes) and zap_bc6h_decode (zap_tex.h:963; stride in uint16),
+   device memory, asynchronous; only texels inside the image are written */
+ZTC_API int zap_tex_cuda_bc_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, int fmt, uint8_t *rgba, size_t stride,
+                                       void *stream);
+ZTC_API int zap_tex_cuda_bc6h_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint16_t *rgba, size_t stride,
+                                         void *stream);
+
+/* ---------------------------------------------------------------- differentiable palette decode, refinement
+   No reference counterpart. With indices held fixed, decoding is linear in the endpoints:
+     decoded[b][i][c] = a_i * e0[c] + (1 - a_i) * e1[c]
+   a_i = {1, 0, 2/3, 1/3}[index] for BC1, 1 - w4(index)/64 for BC7 mode 6; endpoints in 8-bit units, float[b][2][4]
+   (BC1 uses RGB); decoded float[b][16][4]. BC7 blocks in other modes are not covered: they decode to 0 and have
+   zero gradient.
+   block_endpoints: the stored endpoints, expanded; palette_adjoint: grad_endpoints = d(sum g . decoded)/d(endpoints).
+   refine: per block, `steps` Adam steps (learning rate lr, 8-bit units) on the block MSE through the adjoint,
+   requantise, re-fit indices, keep the new block only if its squared error is lower; optional per-block squared
+   errors before / after (uint32[nblocks], device). Device pointers, asynchronous. */
+ZTC_API int zap_tex_cuda_block_endpoints_dev(zap_tex_cuda_ctx *ctx, int fmt, const void *blocks, int nblocks, float *endpoints,
+                                             void *stream);
+ZTC_API int zap_tex_cuda_palette_decode_dev(zap_tex_cuda_ctx *ctx, int fmt, const void *blocks, int nblocks, const float *endpoints,
+                                            float *decoded, void *stream);
+ZTC_API int zap_tex_cuda_palette_adjoint_dev(zap_tex_cuda_ctx *ctx, int fmt, const void *blocks, int nblocks, const float *grad_decoded,
+                                             float *grad_endpoints, void *stream);
+ZTC_API int zap_tex_cuda_refine_dev(zap_tex_cuda_ctx *ctx, int fmt, const uint8_t *rgba, int w, int h, size_t stride, void *blocks,
+                                    int steps, float lr, uint32_t *sse_before, uint32_t *sse_after, void *stream);
+
 /* ---------------------------------------------------------------- batched encoding
    Many textures at once, each with its mip chain, mixed formats. No single reference counterpart: it replaces the
    caller loop of zap.c:330-342 (zap_bc_encode per level, zap_mip_next between levels) run over many textures.

@@ -181,6 +181,63 @@ def mip_next_f_dev(t, out=None, stream=None, ctx=None):
     return out
 
 
+def bc_decode_dev(bc, w, h, fmt, stream=None, ctx=None):
+    """Device zap_bc_decode: uint8 CUDA tensor of blocks -> HxWx4 uint8 CUDA tensor."""
+    import torch
+    out = torch.empty((h, w, 4), dtype=torch.uint8, device=bc.device)
+    check(load().zap_tex_cuda_bc_decode_dev(ctx, bc.data_ptr(), w, h, fmt, out.data_ptr(), w * 4, _stream(stream)), "bc_decode_dev")
+    return out
+
+
+def bc6h_decode_dev(bc, w, h, stream=None, ctx=None):
+    """Device zap_bc6h_decode: blocks -> HxWx4 int16 tensor holding half bits (alpha 0x3C00)."""
+    import torch
+    out = torch.empty((h, w, 4), dtype=torch.int16, device=bc.device)
+    check(load().zap_tex_cuda_bc6h_decode_dev(ctx, bc.data_ptr(), w, h, out.data_ptr(), w * 4, _stream(stream)), "bc6h_decode_dev")
+    return out
+
+
+def block_endpoints_dev(blocks, fmt, stream=None, ctx=None):
+    """Stored endpoints of BC1 / BC7-mode-6 blocks, expanded to 8-bit units: float32 [nblocks, 2, 4]."""
+    import torch
+    n = blocks.numel() // block_bytes(fmt)
+    out = torch.empty((n, 2, 4), dtype=torch.float32, device=blocks.device)
+    check(load().zap_tex_cuda_block_endpoints_dev(ctx, fmt, blocks.data_ptr(), n, out.data_ptr(), _stream(stream)), "block_endpoints_dev")
+    return out
+
+
+def palette_decode_dev(blocks, fmt, endpoints, stream=None, ctx=None):
+    """Linear palette decode with the blocks' indices held fixed: endpoints [n, 2, 4] -> texels float32 [n, 16, 4]."""
+    import torch
+    n = endpoints.shape[0]
+    out = torch.empty((n, 16, 4), dtype=torch.float32, device=endpoints.device)
+    check(load().zap_tex_cuda_palette_decode_dev(ctx, fmt, blocks.data_ptr(), n, endpoints.contiguous().data_ptr(), out.data_ptr(),
+                                                 _stream(stream)), "palette_decode_dev")
+    return out
+
+
+def palette_adjoint_dev(blocks, fmt, grad_decoded, stream=None, ctx=None):
+    """Adjoint of palette_decode_dev: gradient on decoded texels [n, 16, 4] -> gradient on endpoints [n, 2, 4]."""
+    import torch
+    n = grad_decoded.shape[0]
+    out = torch.empty((n, 2, 4), dtype=torch.float32, device=grad_decoded.device)
+    check(load().zap_tex_cuda_palette_adjoint_dev(ctx, fmt, blocks.data_ptr(), n, grad_decoded.contiguous().data_ptr(), out.data_ptr(),
+                                                  _stream(stream)), "palette_adjoint_dev")
+    return out
+
+
+def refine_dev(t, fmt, blocks, steps=8, lr=1.0, stream=None, ctx=None):
+    """Gradient endpoint refinement of encoded blocks in place; returns per-block squared errors (before, after)."""
+    import torch
+    w, h, stride = _dev_img(t, (4,))
+    n = ((w + 3) // 4) * ((h + 3) // 4)
+    s0 = torch.empty(n, dtype=torch.int32, device=t.device)
+    s1 = torch.empty(n, dtype=torch.int32, device=t.device)
+    check(load().zap_tex_cuda_refine_dev(ctx, fmt, t.data_ptr(), w, h, stride, blocks.data_ptr(), int(steps), float(lr), s0.data_ptr(),
+                                         s1.data_ptr(), _stream(stream)), "refine_dev")
+    return s0, s1
+
+
 class _Item(C.Structure):
     """zap_tex_cuda_item (include/zap_tex_cuda.h)."""
     _fields_ = [("src", C.c_void_p), ("w", C.c_int), ("h", C.c_int), ("stride", C.c_size_t), ("fmt", C.c_int),

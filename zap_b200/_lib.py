@@ -64,6 +64,12 @@ def _declare(lib):
         "zap_tex_cuda_mip_chain_bytes": ([i, i], sz),
         "zap_tex_cuda_mip_chain_dev": ([vp, vp, i, i, sz, i, vp, vp], i),
         "zap_tex_cuda_bc7_encode_noalloc_dev": ([vp, i, i, sz, vp, vp], i),
+        "zap_tex_cuda_bc_decode_dev": ([vp, vp, i, i, i, vp, sz, vp], i),
+        "zap_tex_cuda_bc6h_decode_dev": ([vp, vp, i, i, vp, sz, vp], i),
+        "zap_tex_cuda_block_endpoints_dev": ([vp, i, vp, i, vp, vp], i),
+        "zap_tex_cuda_palette_decode_dev": ([vp, i, vp, i, vp, vp, vp], i),
+        "zap_tex_cuda_palette_adjoint_dev": ([vp, i, vp, i, vp, vp, vp], i),
+        "zap_tex_cuda_refine_dev": ([vp, i, vp, i, i, sz, vp, i, f, vp, vp, vp], i),
         "zap_tex_cuda_batch_item_bytes": ([i, i, i, i], sz),
         "zap_tex_cuda_batch_create": ([vp, vp, i, i, C.POINTER(vp)], i),
         "zap_tex_cuda_batch_run": ([vp, vp], i),
