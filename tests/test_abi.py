@@ -18,6 +18,18 @@ def declared_functions():
     return sorted(set(names))
 
 
+def test_built_library_is_current():
+    """The in-tree library must be rebuilt after any source change (zap_b200.build())."""
+    import zap_b200
+    lib = zap_b200._lib.LIB_PATH
+    if not os.path.exists(lib):
+        zap_b200.build()
+    csrc = os.path.join(ROOT, "zap_b200", "csrc")
+    sources = [os.path.join(csrc, f) for f in os.listdir(csrc) if f.endswith((".cu", ".cuh", ".h"))] + HEADERS
+    newer = [os.path.basename(s) for s in sources if os.path.getmtime(s) > os.path.getmtime(lib)]
+    assert not newer, f"rebuild zap_b200 (make -C zap_b200/csrc): {newer} changed after the library was built"
+
+
 def test_header_declares_entry_points():
     names = declared_functions()
     assert "zap_tex_cuda_bc_encode" in names and "zap_tex_cuda_bc6h_encode" in names and "zap_tex_cuda_astc_encode" in names
