@@ -358,7 +358,7 @@ ZTC_DEV uint4 astc_pack(const AstcSmem &S, int cfg, int seed, const uint32_t cod
     return make_uint4(o.w[0] | brev(ws.w[3]), o.w[1] | brev(ws.w[2]), o.w[2] | brev(ws.w[1]), o.w[3] | brev(ws.w[0]));
 }
 
-__global__ void __launch_bounds__(128) astc_single_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out,
+__global__ void __launch_bounds__(128, ZTC_MINB_ASTC_SINGLE) astc_single_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out,
                                                           uint32_t *__restrict__ count, uint2 *__restrict__ items) {
     __shared__ AstcSmem S;
     load_smem(S);

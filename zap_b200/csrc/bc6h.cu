@@ -152,7 +152,7 @@ ZTC_DEV uint4 bc6h_encode_block(const HalfBlock &B) {  // zap_tex.h:873-931
     return make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
 }
 
-__global__ void __launch_bounds__(128) bc6h_kernel(SrcHdr src, int bw, int by0, int nblocks, uint8_t *__restrict__ out) {
+__global__ void __launch_bounds__(128, ZTC_MINB_BC6H) bc6h_kernel(SrcHdr src, int bw, int by0, int nblocks, uint8_t *__restrict__ out) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nblocks) return;
     int bx = b % bw, by = by0 + b / bw;

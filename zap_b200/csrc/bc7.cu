@@ -168,7 +168,7 @@ ZTC_DEV int mode6_encode(const uint32_t t[16], uint4 &blk) {  // zap_tex.h:520-5
     return err;
 }
 
-__global__ void __launch_bounds__(128) bc7_mode6_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out,
+__global__ void __launch_bounds__(128, ZTC_MINB_BC7_MODE6) bc7_mode6_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out,
                                                         uint32_t *__restrict__ count, uint2 *__restrict__ items) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = b < nblocks;
@@ -515,7 +515,7 @@ __device__ __forceinline__ void bc7_group_block(const uint32_t t[16], int err, u
     }
 }
 
-__global__ void __launch_bounds__(128) bc7_hard_kernel(SrcU8 src, int bw, int by0, uint8_t *__restrict__ out,
+__global__ void __launch_bounds__(128, ZTC_MINB_BC7_HARD) bc7_hard_kernel(SrcU8 src, int bw, int by0, uint8_t *__restrict__ out,
                                                        const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
     const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
     const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));

@@ -192,7 +192,7 @@ ZTC_DEV uint2 bc4_encode(const uint32_t t[16], int c) {
 
 // ---------------------------------------------------------------- kernel: one thread per block
 template <int FMT>
-__global__ void __launch_bounds__(128) bcn_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out) {
+__global__ void __launch_bounds__(128, ZTC_MINB_BCN) bcn_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nblocks) return;
     int bx = b % bw, by = by0 + b / bw;
