@@ -217,8 +217,8 @@ int host_encode(zap_tex_cuda_ctx *ctx, int fmt, const void *src, int w, int h, s
     const int bw = (w + 3) / 4, bh = (h + 3) / 4;
     const size_t bs = fmt == ZTC_BC6H || fmt == ZTC_ASTC4X4 ? 16 : block_bytes(fmt);
     const size_t row_bytes = (size_t)w * texel_bytes, pitch = round16(row_bytes);
-    // band height: about 16 MB of source per band, at least 8 block rows
-    size_t band_rows = (16u << 20) / (pitch * 4) + 1;
+    // band height: about 2 MB of source per band (a 2048x2048 RGBA8 image gives 8 bands), at least 8 block rows
+    size_t band_rows = (2u << 20) / (pitch * 4) + 1;
     if (band_rows < 8) band_rows = 8;
     if (band_rows > (size_t)bh) band_rows = (size_t)bh;
     const int nbands = (int)((bh + band_rows - 1) / band_rows);
