@@ -75,6 +75,7 @@ __attribute__((visibility("default"))) int emu_astc_encode(const uint8_t *img, i
         build_tables(T);
         memcpy(S.q, T.q, sizeof S.q); memcpy(S.uq, T.uq, sizeof S.uq); memcpy(S.cfg, T.cfg, sizeof S.cfg);
         memcpy(S.trit_code, T.trit_code, sizeof S.trit_code); memcpy(S.quint_code, T.quint_code, sizeof S.quint_code);
+        memcpy(S.wq, T.wq, sizeof S.wq);
         ready = true;
     }
     SrcU8 s{img, stride, w, h, 4, 0};
@@ -85,14 +86,9 @@ __attribute__((visibility("default"))) int emu_astc_encode(const uint8_t *img, i
             gather_block(s, bx, by, t);
             bool opaque = true;
             for (int i = 0; i < 16; i++) opaque &= (t[i] >> 24) == 255u;
-            int best = 1 << 30, bc = 0;
+            int bc = 0;
             uint32_t bcodes[4] = {0, 0, 0, 0}, bwt[4] = {0, 0, 0, 0};
-            for (int k = 0; k < 3; k++) {
-                int cfg = opaque ? k : 3 + k, wb = S.cfg[cfg].wb;
-                uint32_t codes[4], wt[4] = {0, 0, 0, 0};
-                int e = opaque ? astc_try<3, 32, 1>(t, S, cfg, 8, wb, 0u, codes, wt) : astc_try<4, 32, 1>(t, S, cfg, 12, wb, 0u, codes, wt);
-                if (e < best) { best = e; bc = cfg; memcpy(bcodes, codes, 16); memcpy(bwt, wt, 16); }
-            }
+            const int best = astc_single_block(t, TexRef{t, 1}, S, opaque, bc, bcodes, bwt);
             uint4 v = astc_pack(S, bc, 0, bcodes, bwt);
             size_t b = (size_t)by * bw + bx;
             memcpy(out + b * 16, &v, 16);

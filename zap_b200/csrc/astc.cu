@@ -29,6 +29,7 @@ struct AstcTables {
     uint8_t q[8][256];   // 8-bit target -> nearest colour code (first on ties)
     uint8_t uq[8][256];  // colour code -> unquantised 0..255
     uint8_t trit_code[256], quint_code[128];  // value combination -> smallest packed code
+    uint8_t wq[4][32];   // weight code -> 0..64 for 2, 3, 4, 5 weight bits
     uint16_t pat_mask[1024], pat_seed[1024];
     int pat_count;
 };
@@ -111,8 +112,17 @@ static int partition_h(int seed, int x, int y, int count) {  // ASTC spec partit
     return (a >= b && a >= c && a >= d) ? 0 : (b >= c && b >= d) ? 1 : c >= d ? 2 : 3;
 }
 
+ZTC_DEV int wunq(int j, int wb) {  // weight n-bit -> 0..64 (power-of-two ranges, zap_tex.h:1030)
+    int x = 0;
+    for (int sh = 6 - wb; sh > -wb; sh -= wb) x |= sh >= 0 ? j << sh : j >> -sh;
+    x &= 63;
+    return x > 32 ? x + 1 : x;
+}
+
 static void build_tables(AstcTables &T) {
     std::memset(&T, 0, sizeof T);
+    for (int wb = 2; wb <= 5; wb++)
+        for (int j = 0; j < (1 << wb); j++) T.wq[wb - 2][j] = (uint8_t)wunq(j, wb);
     // (CEM, weight bits, partitions) of the eight trial configurations (zap_tex.h:1298-1300)
     static const int CFG[8][3] = {{8, 4, 1}, {8, 3, 1}, {8, 5, 1}, {12, 4, 1}, {12, 3, 1}, {12, 2, 1}, {8, 3, 2}, {8, 2, 2}};
     for (int k = 0; k < 8; k++) {
@@ -154,6 +164,7 @@ struct AstcSmem {
     uint8_t q[8][256], uq[8][256];
     AstcCfg cfg[8];
     uint8_t trit_code[256], quint_code[128];
+    uint8_t wq[4][32];
 };
 
 __device__ __forceinline__ void load_smem(AstcSmem &S) {
@@ -162,15 +173,18 @@ __device__ __forceinline__ void load_smem(AstcSmem &S) {
     for (int k = threadIdx.x; k < (int)(sizeof(S.q) + sizeof(S.uq)) / 4; k += blockDim.x) dst[k] = src[k];
     for (int k = threadIdx.x; k < 256; k += blockDim.x) S.trit_code[k] = kAstc.trit_code[k];
     for (int k = threadIdx.x; k < 128; k += blockDim.x) S.quint_code[k] = kAstc.quint_code[k];
+    for (int k = threadIdx.x; k < 128; k += blockDim.x) (&S.wq[0][0])[k] = (&kAstc.wq[0][0])[k];
     if (threadIdx.x < 8) S.cfg[threadIdx.x] = kAstc.cfg[threadIdx.x];
 }
 
-ZTC_DEV int wunq(int j, int wb) {  // weight n-bit -> 0..64 (power-of-two ranges, zap_tex.h:1030)
-    int x = 0;
-    for (int sh = 6 - wb; sh > -wb; sh -= wb) x |= sh >= 0 ? j << sh : j >> -sh;
-    x &= 63;
-    return x > 32 ? x + 1 : x;
-}
+// The block's texels as the rolled per-texel loops read them: texel i at p[i * stride] (a shared-memory column on
+// the device, so the loops need not be unrolled and the kernels' code stays small enough for the instruction cache)
+struct TexRef {
+    const uint32_t *p;
+    int stride;
+    ZTC_DEV uint32_t operator[](int i) const { return p[i * stride]; }
+};
+
 ZTC_DEV int astc_lerp(int a, int b, int w) { return (((a * 257) * (64 - w) + (b * 257) * w + 32) >> 6) >> 8; }
 ZTC_DEV uint32_t get8(const uint32_t a[4], int i) { return (a[i >> 2] >> (8 * (i & 3))) & 0xFFu; }
 ZTC_DEV void set8(uint32_t a[4], int i, uint32_t v) {
@@ -213,11 +227,12 @@ ZTC_DEV void astc_quant(const AstcSmem &S, int cfg, int nv, const float lo[4], c
     }
 }
 
-// best weights for fixed endpoints (zap_tex.h:1197-1210); pm: bit i set = texel i in partition 1
-template <int NC, int LMAX, int PARTS>
-ZTC_DEV int astc_fit_weights(const uint32_t t[16], int cem, int wb, uint32_t pm, const int uv[PARTS][8], uint32_t wt[4]) {
+// best weights for fixed endpoints (zap_tex.h:1197-1210); pm: bit i set = texel i in partition 1; cm masks the
+// channels the configuration codes (alpha is left out for CEM 8); wq: weight code -> 0..64 for this weight range
+template <int LMAX, int PARTS>
+ZTC_DEV int astc_fit_weights(TexRef ts, uint32_t cm, int cem, int wb, const uint8_t *wq, uint32_t pm, const int uv[PARTS][8],
+                             uint32_t wt[4]) {
     const int L = 1 << wb;
-    const uint32_t cm = NC == 4 ? 0xFFFFFFFFu : 0x00FFFFFFu;
     uint32_t pal[PARTS][LMAX];
     int A[PARTS][LMAX];
     #pragma unroll
@@ -227,7 +242,7 @@ ZTC_DEV int astc_fit_weights(const uint32_t t[16], int cem, int wb, uint32_t pm,
         #pragma unroll
         for (int j = 0; j < LMAX; j++) {
             if (j >= L) break;
-            int w = wunq(j, wb);
+            const int w = wq[j];
             uint32_t e = pack_rgba(astc_lerp(e0[0], e1[0], w), astc_lerp(e0[1], e1[1], w), astc_lerp(e0[2], e1[2], w),
                                    astc_lerp(e0[3], e1[3], w)) & cm;
             pal[k][j] = e;
@@ -235,10 +250,11 @@ ZTC_DEV int astc_fit_weights(const uint32_t t[16], int cem, int wb, uint32_t pm,
         }
     }
     int err = 0;
-    #pragma unroll
+    uint32_t w0 = 0, w1 = 0, w2 = 0, w3 = 0;  // texel i's weight enters at the top byte and is shifted down
+    #pragma unroll 1
     for (int i = 0; i < 16; i++) {
         const int k = PARTS == 2 ? (int)((pm >> i) & 1u) : 0;
-        uint32_t p = t[i] & cm;
+        const uint32_t p = ts[i] & cm;
         int m = 0x7FFFFFFF;
         #pragma unroll
         for (int j = 0; j < LMAX; j++) {
@@ -248,60 +264,75 @@ ZTC_DEV int astc_fit_weights(const uint32_t t[16], int cem, int wb, uint32_t pm,
             m = min(m, aj - 2 * LMAX * (int)dot4(p, pj));
         }
         // key = (|c|^2 - 2 p.c) * LMAX + j keeps the first best j
-        int q = m >= 0 ? m / LMAX : -((-m + LMAX - 1) / LMAX);
+        const int q = m >= 0 ? m / LMAX : -((-m + LMAX - 1) / LMAX);
         err += q + (int)dot4(p, p);
-        set8(wt, i, (uint32_t)(m - q * LMAX));
+        w0 = (w0 >> 8) | (w1 << 24); w1 = (w1 >> 8) | (w2 << 24); w2 = (w2 >> 8) | (w3 << 24);
+        w3 = (w3 >> 8) | ((uint32_t)(m - q * LMAX) << 24);
     }
+    wt[0] = w0; wt[1] = w1; wt[2] = w2; wt[3] = w3;
     return err;
 }
 
-// one trial configuration (zap_tex.h:1212-1244); codes: byte per value, partition 0 first
-template <int NC, int LMAX, int PARTS>
-ZTC_DEV int astc_try(const uint32_t t[16], const AstcSmem &S, int cfg, int cem, int wb, uint32_t pm, uint32_t codes[4], uint32_t wt[4]) {
-    constexpr int NV = NC == 4 ? 8 : 6;
+// one trial configuration (zap_tex.h:1212-1244) from the partitions' principal-axis endpoints lo / hi (which do
+// not depend on the configuration, so callers compute them once per block and partition). nc: 3 (CEM 8) or 4
+// (CEM 12) channels. codes: byte per value, partition 0 first. Returns the SSE; wt: 16 weight bytes.
+template <int LMAX, int PARTS>
+ZTC_DEV int astc_try(TexRef ts, const AstcSmem &S, int cfg, int nc, uint32_t pm, const float lo[PARTS][4], const float hi[PARTS][4],
+                     uint32_t codes[4], uint32_t wt[4]) {
+    const AstcCfg &C = S.cfg[cfg];
+    const int cem = C.cem, wb = C.wb, nv = C.nv;
+    const uint32_t cm = nc == 4 ? 0xFFFFFFFFu : 0x00FFFFFFu;
+    const uint8_t *wq = S.wq[wb - 2];
     int code[PARTS][8], uv[PARTS][8];
     #pragma unroll
     for (int k = 0; k < PARTS; k++) {
         #pragma unroll
         for (int v = 0; v < 8; v++) { code[k][v] = 0; uv[k][v] = 0; }
-        uint32_t m = PARTS == 2 ? (k ? pm : (~pm & 0xFFFFu)) : 0xFFFFu;
-        if (!m) m = 1u;  // empty partition: the reference fits texel 0
-        float lo[4], hi[4];
-        pca_endpoints<NC>(t, m, lo, hi);
-        astc_quant(S, cfg, NV, lo, hi, code[k], uv[k]);
+        astc_quant(S, cfg, nv, lo[k], hi[k], code[k], uv[k]);
     }
-    int err = astc_fit_weights<NC, LMAX, PARTS>(t, cem, wb, pm, uv, wt);
-    for (int it = 0; it < 3 && err > 0; it++) {
+    int err = 0;
+    // pass 0 fits the weights to the PCA endpoints; passes 1..3 are the reference's least-squares refits, which
+    // stop at SSE 0 or at the first one that does not lower the SSE. One fit call site keeps the code small.
+    #pragma unroll 1
+    for (int it = 0; it < 4; it++) {
         int tc[PARTS][8], tuv[PARTS][8];
         #pragma unroll
-        for (int k = 0; k < PARTS; k++) {
+        for (int k = 0; k < PARTS; k++)
             #pragma unroll
             for (int v = 0; v < 8; v++) { tc[k][v] = code[k][v]; tuv[k][v] = uv[k][v]; }
-            uint32_t m = PARTS == 2 ? (k ? pm : (~pm & 0xFFFFu)) : 0xFFFFu;
-            float aa = 0.0f, ab = 0.0f, bb = 0.0f, sa[NC], sb[NC];
+        if (it > 0) {
             #pragma unroll
-            for (int c = 0; c < NC; c++) { sa[c] = 0.0f; sb[c] = 0.0f; }
-            #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                if (!((m >> i) & 1u)) continue;
-                float f = (float)wunq((int)get8(wt, i), wb) / 64.0f, g = 1.0f - f;
-                aa = aa + g * g; ab = ab + g * f; bb = bb + f * f;
+            for (int k = 0; k < PARTS; k++) {
+                const uint32_t m = PARTS == 2 ? (k ? pm : (~pm & 0xFFFFu)) : 0xFFFFu;
+                float aa = 0.0f, ab = 0.0f, bb = 0.0f, sa[4] = {0.0f, 0.0f, 0.0f, 0.0f}, sb[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                uint32_t a0 = wt[0], a1 = wt[1], a2 = wt[2], a3 = wt[3];
+                #pragma unroll 1
+                for (int i = 0; i < 16; i++) {
+                    const uint32_t wi = a0 & 0xFFu;
+                    a0 = (a0 >> 8) | (a1 << 24); a1 = (a1 >> 8) | (a2 << 24); a2 = (a2 >> 8) | (a3 << 24); a3 >>= 8;
+                    if (!((m >> i) & 1u)) continue;
+                    const uint32_t x = ts[i];
+                    float f = (float)wq[wi] / 64.0f, g = 1.0f - f;
+                    aa = aa + g * g; ab = ab + g * f; bb = bb + f * f;
+                    // the alpha sums are computed for CEM 8 too and then not used: each channel's sums are
+                    // independent, so the RGB results are the same as a three-channel loop's
+                    #pragma unroll
+                    for (int c = 0; c < 4; c++) { float xc = (float)chan(x, c); sa[c] = sa[c] + g * xc; sb[c] = sb[c] + f * xc; }
+                }
+                float det = aa * bb - ab * ab;
+                if (det < 1e-6f && det > -1e-6f) continue;
+                float nlo[4], nhi[4];
                 #pragma unroll
-                for (int c = 0; c < NC; c++) { float x = (float)chan(t[i], c); sa[c] = sa[c] + g * x; sb[c] = sb[c] + f * x; }
+                for (int c = 0; c < 4; c++) {
+                    if (c < nc) { nlo[c] = (sa[c] * bb - sb[c] * ab) / det; nhi[c] = (sb[c] * aa - sa[c] * ab) / det; }
+                    else { nlo[c] = 255.0f; nhi[c] = 255.0f; }
+                }
+                astc_quant(S, cfg, nv, nlo, nhi, tc[k], tuv[k]);
             }
-            float det = aa * bb - ab * ab;
-            if (det < 1e-6f && det > -1e-6f) continue;
-            float nlo[4], nhi[4];
-            #pragma unroll
-            for (int c = 0; c < 4; c++) {
-                if (c < NC) { nlo[c] = (sa[c] * bb - sb[c] * ab) / det; nhi[c] = (sb[c] * aa - sa[c] * ab) / det; }
-                else { nlo[c] = 255.0f; nhi[c] = 255.0f; }
-            }
-            astc_quant(S, cfg, NV, nlo, nhi, tc[k], tuv[k]);
         }
-        uint32_t tw[4] = {0, 0, 0, 0};
-        int e = astc_fit_weights<NC, LMAX, PARTS>(t, cem, wb, pm, tuv, tw);
-        if (e >= err) break;
+        uint32_t tw[4];
+        const int e = astc_fit_weights<LMAX, PARTS>(ts, cm, cem, wb, wq, pm, tuv, tw);
+        if (it > 0 && e >= err) break;
         err = e;
         #pragma unroll
         for (int k = 0; k < 4; k++) wt[k] = tw[k];
@@ -309,14 +340,39 @@ ZTC_DEV int astc_try(const uint32_t t[16], const AstcSmem &S, int cfg, int cem, 
         for (int k = 0; k < PARTS; k++)
             #pragma unroll
             for (int v = 0; v < 8; v++) { code[k][v] = tc[k][v]; uv[k][v] = tuv[k][v]; }
+        if (err <= 0) break;
     }
     #pragma unroll
     for (int k = 0; k < 4; k++) codes[k] = 0;
     #pragma unroll
     for (int k = 0; k < PARTS; k++)
         #pragma unroll
-        for (int v = 0; v < NV; v++) set8(codes, k * NV + v, (uint32_t)code[k][v]);
+        for (int v = 0; v < 8; v++)
+            if (v < nv) set8(codes, k * nv + v, (uint32_t)code[k][v]);
     return err;
+}
+
+// the three single-partition trials of one block (zap_tex.h:1306-1318): CEM 8 for opaque blocks, CEM 12 otherwise.
+// t: the texels in registers (for the principal axis), ts: the same texels for the rolled loops.
+ZTC_DEV int astc_single_block(const uint32_t t[16], TexRef ts, const AstcSmem &S, bool opaque, int &bc, uint32_t bcodes[4],
+                              uint32_t bwt[4]) {
+    float lo[1][4], hi[1][4];
+    if (opaque) pca_endpoints<3>(t, 0xFFFFu, lo[0], hi[0]);
+    else pca_endpoints<4>(t, 0xFFFFu, lo[0], hi[0]);
+    int best = 1 << 30;
+    bc = 0;
+    #pragma unroll 1
+    for (int k = 0; k < 3; k++) {
+        const int cfg = opaque ? k : 3 + k;
+        uint32_t codes[4], wt[4];
+        const int e = astc_try<32, 1>(ts, S, cfg, opaque ? 3 : 4, 0u, lo, hi, codes, wt);
+        if (e < best) {
+            best = e; bc = cfg;
+            #pragma unroll
+            for (int q = 0; q < 4; q++) { bcodes[q] = codes[q]; bwt[q] = wt[q]; }
+        }
+    }
+    return best;
 }
 
 // integer-sequence encoding of n codes (zap_tex.h:1080-1095)
@@ -361,6 +417,7 @@ ZTC_DEV uint4 astc_pack(const AstcSmem &S, int cfg, int seed, const uint32_t cod
 __global__ void __launch_bounds__(128, ZTC_MINB_ASTC_SINGLE) astc_single_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out,
                                                           uint32_t *__restrict__ count, uint2 *__restrict__ items) {
     __shared__ AstcSmem S;
+    __shared__ uint32_t s_tex[16][128];  // column threadIdx.x: this thread's block (read only by this thread)
     load_smem(S);
     __syncthreads();
     int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -371,20 +428,10 @@ __global__ void __launch_bounds__(128, ZTC_MINB_ASTC_SINGLE) astc_single_kernel(
         gather_block(src, b % bw, by0 + b / bw, t);
         bool opaque = true;
         #pragma unroll
-        for (int i = 0; i < 16; i++) opaque &= (t[i] >> 24) == 255u;
+        for (int i = 0; i < 16; i++) { opaque &= (t[i] >> 24) == 255u; s_tex[i][threadIdx.x] = t[i]; }
         int bc = 0;
         uint32_t bcodes[4] = {0, 0, 0, 0}, bwt[4] = {0, 0, 0, 0};
-        for (int k = 0; k < 3; k++) {
-            const int cfg = opaque ? k : 3 + k;
-            const int wb = S.cfg[cfg].wb;
-            uint32_t codes[4], wt[4] = {0, 0, 0, 0};
-            int e = opaque ? astc_try<3, 32, 1>(t, S, cfg, 8, wb, 0u, codes, wt) : astc_try<4, 32, 1>(t, S, cfg, 12, wb, 0u, codes, wt);
-            if (e < best) {
-                best = e; bc = cfg;
-                #pragma unroll
-                for (int q = 0; q < 4; q++) { bcodes[q] = codes[q]; bwt[q] = wt[q]; }
-            }
-        }
+        best = astc_single_block(t, TexRef{&s_tex[0][threadIdx.x], 128}, S, opaque, bc, bcodes, bwt);
         store_block16(out + (size_t)b * 16, astc_pack(S, bc, 0, bcodes, bwt));
         hard = opaque && best > 16 * 3 * 4;  // zap_tex.h:1323
     }
@@ -452,6 +499,7 @@ __global__ void __launch_bounds__(128) astc_two_part_kernel(SrcU8 src, int bw, i
                                                             const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
     __shared__ AstcSmem S;
     __shared__ uint16_t pmask[1024], pseed[1024];
+    __shared__ uint32_t s_tex[128 / kAstcGroup][17];  // per group: its block's texels (padded: no bank conflicts)
     load_smem(S);
     const int npat = kAstc.pat_count;
     for (int k = threadIdx.x; k < npat; k += blockDim.x) { pmask[k] = kAstc.pat_mask[k]; pseed[k] = kAstc.pat_seed[k]; }
@@ -460,11 +508,17 @@ __global__ void __launch_bounds__(128) astc_two_part_kernel(SrcU8 src, int bw, i
     const unsigned gmask = 0xFFu << (lane & ~(kAstcGroup - 1));
     const int ngroups = gridDim.x * (blockDim.x / kAstcGroup);
     const int n = (int)*(volatile const uint32_t *)count;
+    uint32_t *gtex = s_tex[threadIdx.x / kAstcGroup];
     for (int it = blockIdx.x * (blockDim.x / kAstcGroup) + (threadIdx.x / kAstcGroup); it < n; it += ngroups) {
         const uint2 item = items[it];
         const int b = (int)item.x, best = (int)item.y;
         uint32_t t[16];
         gather_block(src, b % bw, by0 + b / bw, t);
+        __syncwarp(gmask);  // the group's reads of the previous block are done
+        #pragma unroll
+        for (int i = 0; i < 16; i++)
+            if ((i & (kAstcGroup - 1)) == l) gtex[i] = t[i];
+        __syncwarp(gmask);
         const uint32_t km = two_means(t);
         // local top 4 by (distance, pattern order) over patterns l, l + 8, ...
         int cd[4] = {99, 99, 99, 99}, cp[4] = {1 << 20, 1 << 20, 1 << 20, 1 << 20};
@@ -495,13 +549,23 @@ __global__ void __launch_bounds__(128) astc_two_part_kernel(SrcU8 src, int bw, i
             }
         }
         // lane = candidate * 2 + configuration (6: 3 weight bits, 7: 2 weight bits)
-        const int j = l >> 1, cfg = 6 + (l & 1), wb = cfg == 6 ? 3 : 2;
+        const int j = l >> 1, cfg = 6 + (l & 1);
         int pj = -1;
         #pragma unroll
         for (int k = 0; k < 4; k++) if (k == j) pj = cand[k];
         uint32_t codes[4] = {0, 0, 0, 0}, wt[4] = {0, 0, 0, 0};
         int e = 1 << 30;
-        if (pj >= 0) e = astc_try<3, 8, 2>(t, S, cfg, 8, wb, (uint32_t)pmask[pj], codes, wt);
+        if (pj >= 0) {
+            const uint32_t pm = pmask[pj];
+            float lo[2][4], hi[2][4];
+            #pragma unroll
+            for (int k = 0; k < 2; k++) {
+                uint32_t m = k ? pm : (~pm & 0xFFFFu);
+                if (!m) m = 1u;  // empty partition: the reference fits texel 0
+                pca_endpoints<3>(t, m, lo[k], hi[k]);
+            }
+            e = astc_try<8, 2>(TexRef{gtex, 1}, S, cfg, 3, pm, lo, hi, codes, wt);
+        }
         uint32_t key = (pj >= 0 && e < best) ? (((uint32_t)e << 3) | (uint32_t)l) : 0xFFFFFFFFu;
         #pragma unroll
         for (int m = 1; m < kAstcGroup; m <<= 1) key = min(key, __shfl_xor_sync(gmask, key, m, kAstcGroup));

@@ -18,7 +18,8 @@
 // Minimum resident 128-thread CTAs per SM requested from the register allocator, per kernel (tuned on B200:
 // more resident warps hide the latency of these long dependent integer / float chains; see the ncu summaries).
 // Measured on 2048x2048 encodes: bc7_mode6 0.174 -> 0.145 ms at 4 (128 registers, small spill), BC1 -4.5 % at 6,
-// BC6H -11 % at 3; the BC7 mode 5/1 and ASTC kernels gain nothing from more than 1.
+// BC6H -11 % at 3, ASTC single-partition -6 % at 4 (146 -> 128 registers); the BC7 mode 5/1 kernel gains nothing
+// from more than 1.
 #ifndef ZTC_MINB_BC7_MODE6
 #define ZTC_MINB_BC7_MODE6 4
 #endif
@@ -29,7 +30,7 @@
 #define ZTC_MINB_BCN 6
 #endif
 #ifndef ZTC_MINB_ASTC_SINGLE
-#define ZTC_MINB_ASTC_SINGLE 1
+#define ZTC_MINB_ASTC_SINGLE 4
 #endif
 #ifndef ZTC_MINB_BC6H
 #define ZTC_MINB_BC6H 3
