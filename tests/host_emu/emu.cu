@@ -39,7 +39,7 @@ __attribute__((visibility("default"))) int emu_bc_encode(const uint8_t *img, int
             else if (fmt == ZTC_FMT_BC5) { uint2 r = bc4_encode(t, 0), g = bc4_encode(t, 1); memcpy(out + b * 16, &r, 8); memcpy(out + b * 16 + 8, &g, 8); }
             else if (fmt == ZTC_FMT_BC7) {
                 uint4 v;
-                int err = mode6_encode(t, v);
+                int err = mode6_encode(t, TexRef{t, 1}, v);
                 memcpy(out + b * 16, &v, 16);
                 if (hard) hard[b] = err > 64;
             } else return -1;

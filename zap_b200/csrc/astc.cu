@@ -177,14 +177,6 @@ __device__ __forceinline__ void load_smem(AstcSmem &S) {
     if (threadIdx.x < 8) S.cfg[threadIdx.x] = kAstc.cfg[threadIdx.x];
 }
 
-// The block's texels as the rolled per-texel loops read them: texel i at p[i * stride] (a shared-memory column on
-// the device, so the loops need not be unrolled and the kernels' code stays small enough for the instruction cache)
-struct TexRef {
-    const uint32_t *p;
-    int stride;
-    ZTC_DEV uint32_t operator[](int i) const { return p[i * stride]; }
-};
-
 ZTC_DEV int astc_lerp(int a, int b, int w) { return (((a * 257) * (64 - w) + (b * 257) * w + 32) >> 6) >> 8; }
 ZTC_DEV uint32_t get8(const uint32_t a[4], int i) { return (a[i >> 2] >> (8 * (i & 3))) & 0xFFu; }
 ZTC_DEV void set8(uint32_t a[4], int i, uint32_t v) {

@@ -53,7 +53,7 @@ ZTC_DEV int quant_pbit(const float v[4], int n, int p, int q[4], int x8[4]) {
 // Argmin over a (1 << IB)-entry palette for every selected texel: key = (|c|^2 - 2 p.c) * NP + j is ordered
 // like the reference's first-best scan. idx: nibble i = index of texel i. Returns the SSE.
 template <int NC, int IB>
-ZTC_DEV int palette_fit(const uint32_t t[16], uint32_t mask, const int x0[4], const int x1[4], uint64_t &idx) {
+ZTC_DEV int palette_fit(TexRef ts, uint32_t mask, const int x0[4], const int x1[4], uint64_t &idx) {
     constexpr int NP = 1 << IB;
     const uint32_t cm = NC == 4 ? 0xFFFFFFFFu : 0x00FFFFFFu;
     uint32_t pal[NP];
@@ -69,10 +69,10 @@ ZTC_DEV int palette_fit(const uint32_t t[16], uint32_t mask, const int x0[4], co
     }
     int err = 0;
     uint64_t bits = 0;
-    #pragma unroll
+    #pragma unroll 1
     for (int i = 0; i < 16; i++) {
         if (!((mask >> i) & 1u)) continue;
-        uint32_t p = t[i] & cm;
+        const uint32_t p = ts[i] & cm;
         int m = A[0] - 2 * NP * (int)dot4(p, pal[0]);
         #pragma unroll
         for (int j = 1; j < NP; j++) m = min(m, A[j] - 2 * NP * (int)dot4(p, pal[j]));
@@ -85,7 +85,7 @@ ZTC_DEV int palette_fit(const uint32_t t[16], uint32_t mask, const int x0[4], co
 
 // float endpoints -> best p-bits, quantised endpoints, indices (zap_tex.h:466-486)
 template <int NC, int IB>
-ZTC_DEV int subset_fit(const uint32_t t[16], uint32_t mask, int n, bool shared_p, const float lo[4], const float hi[4],
+ZTC_DEV int subset_fit(TexRef ts, uint32_t mask, int n, bool shared_p, const float lo[4], const float hi[4],
                        int q[2][4], int pb[2], uint64_t &idx) {
     int ql[2][4], qh[2][4], xl[2][4], xh[2][4], el[2], eh[2];
     #pragma unroll
@@ -105,51 +105,59 @@ ZTC_DEV int subset_fit(const uint32_t t[16], uint32_t mask, int n, bool shared_p
         x0[c] = b0 ? xl[1][c] : xl[0][c]; x1[c] = b1 ? xh[1][c] : xh[0][c];
     }
     pb[0] = b0; pb[1] = b1;
-    return palette_fit<NC, IB>(t, mask, x0, x1, idx);
+    return palette_fit<NC, IB>(ts, mask, x0, x1, idx);
 }
 
-// PCA start, fit, up to two least-squares refits (zap_tex.h:489-515)
+// PCA start, fit, up to two least-squares refits (zap_tex.h:489-515). t: the texels in registers (for the
+// principal axis), ts: the same texels for the rolled loops.
 template <int NC, int IB>
-ZTC_DEV int subset_encode(const uint32_t t[16], uint32_t mask, int n, bool shared_p, int q[2][4], int pb[2], uint64_t &idx) {
+ZTC_DEV int subset_encode(const uint32_t t[16], TexRef ts, uint32_t mask, int n, bool shared_p, int q[2][4], int pb[2],
+                          uint64_t &idx) {
     float lo[4], hi[4];
     pca_endpoints<NC>(t, mask, lo, hi);
-    int err = subset_fit<NC, IB>(t, mask, n, shared_p, lo, hi, q, pb, idx);
-    for (int it = 0; it < 2 && err > 0; it++) {
-        float aa = 0.0f, ab = 0.0f, bb = 0.0f, sa[NC], sb[NC];
-        #pragma unroll
-        for (int c = 0; c < NC; c++) { sa[c] = 0.0f; sb[c] = 0.0f; }
-        #pragma unroll
-        for (int i = 0; i < 16; i++) {
-            if (!((mask >> i) & 1u)) continue;
-            float w = (float)wbits(IB, (int)((idx >> (4 * i)) & 15u)) / 64.0f, u = 1.0f - w;
-            aa = aa + u * u; ab = ab + u * w; bb = bb + w * w;
+    int err = 0;
+    // pass 0 fits the PCA endpoints; passes 1 and 2 are the least-squares refits, which stop at SSE 0, at a
+    // singular system or at the first one that does not lower the SSE. One fit call site keeps the code small.
+    #pragma unroll 1
+    for (int it = 0; it < 3; it++) {
+        if (it > 0) {
+            float aa = 0.0f, ab = 0.0f, bb = 0.0f, sa[NC], sb[NC];
             #pragma unroll
-            for (int c = 0; c < NC; c++) { float x = (float)chan(t[i], c); sa[c] = sa[c] + u * x; sb[c] = sb[c] + w * x; }
-        }
-        float det = aa * bb - ab * ab;
-        if (det < 1e-6f && det > -1e-6f) break;
-        float nlo[4], nhi[4];
-        #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            if (c < NC) { nlo[c] = clamp255((sa[c] * bb - sb[c] * ab) / det); nhi[c] = clamp255((sb[c] * aa - sa[c] * ab) / det); }
-            else { nlo[c] = 255.0f; nhi[c] = 255.0f; }
+            for (int c = 0; c < NC; c++) { sa[c] = 0.0f; sb[c] = 0.0f; }
+            #pragma unroll 1
+            for (int i = 0; i < 16; i++) {
+                if (!((mask >> i) & 1u)) continue;
+                float w = (float)wbits(IB, (int)((idx >> (4 * i)) & 15u)) / 64.0f, u = 1.0f - w;
+                aa = aa + u * u; ab = ab + u * w; bb = bb + w * w;
+                const uint32_t x = ts[i];
+                #pragma unroll
+                for (int c = 0; c < NC; c++) { float xc = (float)chan(x, c); sa[c] = sa[c] + u * xc; sb[c] = sb[c] + w * xc; }
+            }
+            float det = aa * bb - ab * ab;
+            if (det < 1e-6f && det > -1e-6f) break;
+            #pragma unroll
+            for (int c = 0; c < 4; c++) {
+                if (c < NC) { lo[c] = clamp255((sa[c] * bb - sb[c] * ab) / det); hi[c] = clamp255((sb[c] * aa - sa[c] * ab) / det); }
+                else { lo[c] = 255.0f; hi[c] = 255.0f; }
+            }
         }
         int nq[2][4], npb[2];
         uint64_t ni;
-        int ne = subset_fit<NC, IB>(t, mask, n, shared_p, nlo, nhi, nq, npb, ni);
-        if (ne >= err) break;
+        const int ne = subset_fit<NC, IB>(ts, mask, n, shared_p, lo, hi, nq, npb, ni);
+        if (it > 0 && ne >= err) break;
         err = ne; idx = ni; pb[0] = npb[0]; pb[1] = npb[1];
         #pragma unroll
         for (int c = 0; c < 4; c++) { q[0][c] = nq[0][c]; q[1][c] = nq[1][c]; }
+        if (err <= 0) break;
     }
     return err;
 }
 
 // ---------------------------------------------------------------- kernel A: mode 6 for every block
-ZTC_DEV int mode6_encode(const uint32_t t[16], uint4 &blk) {  // zap_tex.h:520-527, 582-593
+ZTC_DEV int mode6_encode(const uint32_t t[16], TexRef ts, uint4 &blk) {  // zap_tex.h:520-527, 582-593
     int q[2][4], pb[2];
     uint64_t idx;
-    int err = subset_encode<4, 4>(t, 0xFFFFu, 8, false, q, pb, idx);
+    int err = subset_encode<4, 4>(t, ts, 0xFFFFu, 8, false, q, pb, idx);
     if (idx & 8u) {  // anchor index MSB must be 0: swap endpoints and p-bits, invert indices (15 - i == i ^ 15)
         #pragma unroll
         for (int c = 0; c < 4; c++) { int s = q[0][c]; q[0][c] = q[1][c]; q[1][c] = s; }
@@ -170,14 +178,17 @@ ZTC_DEV int mode6_encode(const uint32_t t[16], uint4 &blk) {  // zap_tex.h:520-5
 
 __global__ void __launch_bounds__(128, ZTC_MINB_BC7_MODE6) bc7_mode6_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out,
                                                         uint32_t *__restrict__ count, uint2 *__restrict__ items) {
+    __shared__ uint32_t s_tex[16][128];  // column threadIdx.x: this thread's block (read only by this thread)
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = b < nblocks;
     int err = 0;
     if (valid) {
         uint32_t t[16];
         gather_block(src, b % bw, by0 + b / bw, t);
+        #pragma unroll
+        for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
         uint4 blk;
-        err = mode6_encode(t, blk);
+        err = mode6_encode(t, TexRef{&s_tex[0][threadIdx.x], 128}, blk);
         store_block16(out + (size_t)b * 16, blk);
     }
     bool hard = valid && err > 16 * 4;  // zap_tex.h:758 early exit
@@ -331,8 +342,9 @@ constexpr int kMode1Tries = 4;  // partitions fully fitted after ranking (ZAP__B
 
 // One block that mode 6 did not finish, through modes 5 and 1 (zap_tex.h:759-783), by the 8 lanes of a group
 // (lane l, group mask gmask). err is the block's mode-6 SSE; lane 0 writes the block to dst when mode 5 or 1 wins.
-// Every lane holds the block's texels, so all group-level branches below are group-uniform.
-__device__ __forceinline__ void bc7_group_block(const uint32_t t[16], int err, uint8_t *__restrict__ dst, const int l,
+// Every lane holds the block's texels, so all group-level branches below are group-uniform; ts: the group's
+// shared-memory copy of them.
+__device__ __forceinline__ void bc7_group_block(const uint32_t t[16], TexRef ts, int err, uint8_t *__restrict__ dst, const int l,
                                                 const unsigned gmask) {
     {
         bool opaque = true;
@@ -467,7 +479,7 @@ __device__ __forceinline__ void bc7_group_block(const uint32_t t[16], int err, u
             uint32_t pmask = 0;
             if (pj >= 0) {
                 pmask = sub ? (uint32_t)kP2[pj] : (~(uint32_t)kP2[pj] & 0xFFFFu);
-                e1 = subset_encode<3, 3>(t, pmask, 7, true, q1, pb1, i1);
+                e1 = subset_encode<3, 3>(t, ts, pmask, 7, true, q1, pb1, i1);
                 int anchor = sub ? (int)kA2[pj] : 0;
                 if ((i1 >> (4 * anchor)) & 4u) {  // anchor MSB must be 0: swap, 7 - i == i ^ 7 on the subset's texels
                     #pragma unroll
@@ -515,18 +527,30 @@ __device__ __forceinline__ void bc7_group_block(const uint32_t t[16], int err, u
     }
 }
 
+// the group's shared-memory copy of its block (lane l writes texels l and l + 8), for the rolled loops
+__device__ __forceinline__ TexRef stage_group_texels(uint32_t *gtex, const uint32_t t[16], int l, unsigned gmask) {
+    __syncwarp(gmask);  // the group's reads of its previous block are done
+    #pragma unroll
+    for (int i = 0; i < 16; i++)
+        if ((i & (kBc7Group - 1)) == l) gtex[i] = t[i];
+    __syncwarp(gmask);
+    return TexRef{gtex, 1};
+}
+
 __global__ void __launch_bounds__(128, ZTC_MINB_BC7_HARD) bc7_hard_kernel(SrcU8 src, int bw, int by0, uint8_t *__restrict__ out,
                                                        const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
+    __shared__ uint32_t s_gtex[128 / kBc7Group][17];  // per group (padded: the four groups of a warp hit distinct banks)
     const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
     const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
     const int ngroups = gridDim.x * (blockDim.x / kBc7Group);
     const int n = (int)*(volatile const uint32_t *)count;
+    uint32_t *gtex = s_gtex[threadIdx.x / kBc7Group];
     for (int it = blockIdx.x * (blockDim.x / kBc7Group) + (threadIdx.x / kBc7Group); it < n; it += ngroups) {
         const uint2 item = items[it];
         const int b = (int)item.x;
         uint32_t t[16];
         gather_block(src, b % bw, by0 + b / bw, t);
-        bc7_group_block(t, (int)item.y, out + (size_t)b * 16, l, gmask);
+        bc7_group_block(t, stage_group_texels(gtex, t, l, gmask), (int)item.y, out + (size_t)b * 16, l, gmask);
     }
 }
 
@@ -539,8 +563,10 @@ __global__ void __launch_bounds__(CTA) batch_bc7_kernel(const BatchLevel *__rest
                                                         int ntiles, uint32_t *__restrict__ counter) {
     __shared__ int s_tile, s_count;
     __shared__ uint2 s_list[CTA];
+    __shared__ uint32_t s_tex[16][CTA], s_gtex[CTA / kBc7Group][17];
     const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
     const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
+    uint32_t *gtex = s_gtex[threadIdx.x / kBc7Group];
     for (;;) {
         if (threadIdx.x == 0) { s_tile = (int)atomicAdd(counter, 1u); s_count = 0; }
         __syncthreads();
@@ -553,8 +579,10 @@ __global__ void __launch_bounds__(CTA) batch_bc7_kernel(const BatchLevel *__rest
         if ((int)threadIdx.x < T.count) {
             uint32_t t[16];
             gather_block(src, b % L.bw, b / L.bw, t);
+            #pragma unroll
+            for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
             uint4 blk;
-            int err = mode6_encode(t, blk);
+            int err = mode6_encode(t, TexRef{&s_tex[0][threadIdx.x], CTA}, blk);
             store_block16(L.dst + (size_t)b * 16, blk);
             if (err > 16 * 4) s_list[atomicAdd(&s_count, 1)] = make_uint2((uint32_t)b, (uint32_t)err);
         }
@@ -565,7 +593,7 @@ __global__ void __launch_bounds__(CTA) batch_bc7_kernel(const BatchLevel *__rest
             const int hb = (int)item.x;
             uint32_t t[16];
             gather_block(src, hb % L.bw, hb / L.bw, t);
-            bc7_group_block(t, (int)item.y, L.dst + (size_t)hb * 16, l, gmask);
+            bc7_group_block(t, stage_group_texels(gtex, t, l, gmask), (int)item.y, L.dst + (size_t)hb * 16, l, gmask);
         }
         __syncthreads();
     }

@@ -152,6 +152,16 @@ ZTC_DEV void gather_block(const SrcU8 &s, int bx, int by, uint32_t t[16]) {
     }
 }
 
+// The block's texels as the rolled per-texel loops read them: texel i at p[i * stride]. On the device this is a
+// shared-memory copy of the block, so those loops need not be unrolled over registers and the kernels' code stays
+// small enough for the instruction cache (fully unrolled 16-texel x 16-entry palette scans, inlined at several
+// call sites, leave the warps waiting on instruction fetch).
+struct TexRef {
+    const uint32_t *p;
+    int stride;
+    ZTC_DEV uint32_t operator[](int i) const { return p[i * stride]; }
+};
+
 ZTC_DEV void store_block8(uint8_t *out, uint2 v) { *(uint2 *)out = v; }
 ZTC_DEV void store_block16(uint8_t *out, uint4 v) { *(uint4 *)out = v; }
 
