@@ -5,7 +5,9 @@
 //   - mip levels 1..L-1 of every texture go to one device buffer; depth d of all textures is built by one
 //     persistent launch over tiles of 256 output texel pairs (level-synchronous, L-1 launches in all);
 //   - every (texture, level) is cut into tiles of consecutive blocks; one persistent launch per format class pulls
-//     tiles from a device counter (largest levels first); BC7 tiles finish their hard blocks inside the same CTA;
+//     tiles from a device counter (largest levels first); for BC7 that launch runs mode 6 and lists the blocks it
+//     does not finish in one batch-wide work list, which a second persistent launch (8-lane groups, modes 5 / 1)
+//     drains;
 //   - an optional autotuner times each format's kernel at 64/128/256 threads (= blocks per tile) on the batch's
 //     own tiles and keeps the fastest;
 //   - the whole sequence (counter resets, mip launches, concurrent encode launches) is captured into one CUDA
@@ -25,6 +27,7 @@
 namespace {
 
 constexpr int kClasses = 5;  // BC1, BC3, BC4, BC5, BC7 (format id == class id)
+constexpr int kHardCounter = 8;  // d_counters slot of the BC7 work-list length
 const int kCtaChoices[3] = {64, 128, 256};
 
 struct HostLevel {
@@ -55,7 +58,11 @@ struct zap_tex_cuda_batch {
     std::vector<ztc::BatchMip *> d_mips;
     std::vector<ztc::BatchMipTile *> d_mip_tiles;
     std::vector<int> n_mip_tiles;
-    uint32_t *d_counters = nullptr;
+    uint32_t *d_counters = nullptr;          // [f]: tile counter of class f; [kHardCounter]: BC7 work-list length
+    uint2 *d_hard_items = nullptr;           // BC7 work list: (batch-wide block id, mode 6 SSE)
+    uint32_t *d_bc7_bases = nullptr;         // first batch-wide id of each BC7 level, ascending
+    int *d_bc7_level_of = nullptr;           // ... and that level's index in d_levels
+    int n_bc7_levels = 0, hard_grid = 1;
     float *d_srgb = nullptr;
     void *plain_scratch = nullptr;
     cudaGraph_t graph = nullptr;
@@ -111,9 +118,23 @@ cudaError_t launch_encode(zap_tex_cuda_batch *b, int f, cudaStream_t s) {
     if (!b->ntiles[f]) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(b->d_counters + f, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
-    ztc::TraceScope tr(f == ZTC_BC7 ? "batch_bc7" : f == ZTC_BC1 ? "batch_bc1" : f == ZTC_BC3 ? "batch_bc3" : f == ZTC_BC4 ? "batch_bc4" : "batch_bc5", s);
+    if (f == ZTC_BC7) {
+        uint32_t *hard_count = b->d_counters + kHardCounter;
+        if ((e = cudaMemsetAsync(hard_count, 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
+        {
+            ztc::TraceScope tr("batch_bc7_mode6", s);
+            ztc::trace_units(b->blocks[f]);
+            e = ztc_launch_batch_bc7_mode6(b->cta[f], b->grid[f], b->d_levels, b->d_tiles[f], b->ntiles[f], b->d_counters + f, hard_count,
+                                           b->d_hard_items, s);
+            if (e != cudaSuccess) return e;
+        }
+        ztc::TraceScope tr("batch_bc7_modes51", s);
+        ztc::trace_units_dev(hard_count, s);
+        return ztc_launch_batch_bc7_hard(b->hard_grid, b->d_levels, b->d_bc7_bases, b->d_bc7_level_of, b->n_bc7_levels, hard_count,
+                                         b->d_hard_items, s);
+    }
+    ztc::TraceScope tr(f == ZTC_BC1 ? "batch_bc1" : f == ZTC_BC3 ? "batch_bc3" : f == ZTC_BC4 ? "batch_bc4" : "batch_bc5", s);
     ztc::trace_units(b->blocks[f]);
-    if (f == ZTC_BC7) return ztc_launch_batch_bc7(b->cta[f], b->grid[f], b->d_levels, b->d_tiles[f], b->ntiles[f], b->d_counters + f, s);
     return ztc_launch_batch_bcn(f, b->cta[f], b->grid[f], b->d_levels, b->d_tiles[f], b->ntiles[f], b->d_counters + f, s);
 }
 
@@ -209,6 +230,7 @@ int zap_tex_cuda_batch_destroy(zap_tex_cuda_batch *b) {
     for (auto p : b->d_mips) cudaFree(p);
     for (auto p : b->d_mip_tiles) cudaFree(p);
     cudaFree(b->mip_buf); cudaFree(b->d_levels); cudaFree(b->d_counters); cudaFree(b->d_srgb); cudaFree(b->plain_scratch);
+    cudaFree(b->d_hard_items); cudaFree(b->d_bc7_bases); cudaFree(b->d_bc7_level_of);
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -301,13 +323,38 @@ int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *it
     }
     // ---- level descriptors, tables, counters
     std::vector<ztc::BatchLevel> dl;
-    size_t max_blocks = 1;
-    for (auto &hl : b->levels) {
-        dl.push_back({hl.src, hl.dst, hl.pitch, hl.w, hl.h, hl.bw, hl.fmt});
-        max_blocks = std::max(max_blocks, (size_t)hl.bw * hl.bh);
+    std::vector<uint32_t> bc7_bases;
+    std::vector<int> bc7_level_of;
+    size_t max_blocks = 1, bc7_blocks = 0;
+    for (size_t k = 0; k < b->levels.size(); k++) {
+        const HostLevel &hl = b->levels[k];
+        const size_t nb = (size_t)hl.bw * hl.bh;
+        uint32_t gbase = 0;
+        if (hl.fmt == ZTC_BC7) {
+            gbase = (uint32_t)bc7_blocks;
+            bc7_bases.push_back(gbase);
+            bc7_level_of.push_back((int)k);
+            bc7_blocks += nb;
+        }
+        dl.push_back({hl.src, hl.dst, hl.pitch, hl.w, hl.h, hl.bw, hl.fmt, gbase, 0});
+        max_blocks = std::max(max_blocks, nb);
     }
+    if (bc7_blocks >= ((size_t)1 << 32))
+        return fail(ztc_set_error(ZTC_ERR_INVALID_ARG, "batch: more than 2^32 - 1 BC7 blocks in one batch; split it"));
     BTRY(cudaMalloc(&b->d_levels, dl.size() * sizeof(ztc::BatchLevel)), "cudaMalloc(levels)");
     BTRY(cudaMemcpy(b->d_levels, dl.data(), dl.size() * sizeof(ztc::BatchLevel), cudaMemcpyHostToDevice), "upload levels");
+    if (bc7_blocks) {  // BC7 work list: room for every BC7 block of the batch
+        b->n_bc7_levels = (int)bc7_bases.size();
+        BTRY(cudaMalloc(&b->d_hard_items, bc7_blocks * sizeof(uint2)), "cudaMalloc(BC7 work list)");
+        BTRY(cudaMalloc(&b->d_bc7_bases, bc7_bases.size() * sizeof(uint32_t)), "cudaMalloc(BC7 level bases)");
+        BTRY(cudaMalloc(&b->d_bc7_level_of, bc7_level_of.size() * sizeof(int)), "cudaMalloc(BC7 level map)");
+        BTRY(cudaMemcpy(b->d_bc7_bases, bc7_bases.data(), bc7_bases.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload BC7 bases");
+        BTRY(cudaMemcpy(b->d_bc7_level_of, bc7_level_of.data(), bc7_level_of.size() * sizeof(int), cudaMemcpyHostToDevice),
+             "upload BC7 level map");
+        int per_sm = 1;
+        BTRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ztc_batch_bc7_hard_kernel_fn(), 128, 0), "occupancy");
+        b->hard_grid = std::max(1, per_sm) * b->sms;
+    }
     float tables[512];
     ztc::srgb_tables_host(tables, tables + 256);
     BTRY(cudaMalloc(&b->d_srgb, sizeof tables), "cudaMalloc(srgb)");

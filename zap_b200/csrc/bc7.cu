@@ -554,72 +554,105 @@ __global__ void __launch_bounds__(128, ZTC_MINB_BC7_HARD) bc7_hard_kernel(SrcU8 
     }
 }
 
-// ---------------------------------------------------------------- batched: one persistent launch over a tile queue
-// Each CTA takes tiles of consecutive blocks of one (texture, level) from a device counter. Every thread runs
-// mode 6 on its block; blocks above SSE 64 are compacted in shared memory and finished by the CTA's own 8-lane
-// groups, so modes 6, 5 and 1 run fused in one kernel without a global work list.
+// ---------------------------------------------------------------- batched: tile queue, then one batch-wide list
+// Mode 6: each CTA takes tiles of consecutive blocks of one (texture, level) from a device counter, one thread per
+// block, at the plain kernel's occupancy. Blocks above SSE 64 go to one work list for the whole batch, keyed by
+// their batch-wide block id (the level's first id + the block index). Modes 5 and 1 then run as one persistent
+// launch of 8-lane groups over that list, so every group has a block to work on until the list is drained.
 template <int CTA>
-__global__ void __launch_bounds__(CTA) batch_bc7_kernel(const BatchLevel *__restrict__ levels, const BatchTile *__restrict__ tiles,
-                                                        int ntiles, uint32_t *__restrict__ counter) {
-    __shared__ int s_tile, s_count;
-    __shared__ uint2 s_list[CTA];
-    __shared__ uint32_t s_tex[16][CTA], s_gtex[CTA / kBc7Group][17];
-    const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
-    const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
-    uint32_t *gtex = s_gtex[threadIdx.x / kBc7Group];
+__global__ void __launch_bounds__(CTA, ZTC_MINB_BC7_MODE6 * 128 / CTA)
+batch_bc7_mode6_kernel(const BatchLevel *__restrict__ levels, const BatchTile *__restrict__ tiles, int ntiles,
+                       uint32_t *__restrict__ counter, uint32_t *__restrict__ hard_count, uint2 *__restrict__ hard_items) {
+    __shared__ int s_tile;
+    __shared__ uint32_t s_tex[16][CTA];  // column threadIdx.x: this thread's block (read only by this thread)
     for (;;) {
-        if (threadIdx.x == 0) { s_tile = (int)atomicAdd(counter, 1u); s_count = 0; }
+        if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
         __syncthreads();
         const int tile = s_tile;
+        __syncthreads();  // every thread has read s_tile before thread 0 overwrites it
         if (tile >= ntiles) break;
         const BatchTile T = tiles[tile];
         const BatchLevel L = levels[T.level];
-        const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
         const int b = T.first + (int)threadIdx.x;
-        if ((int)threadIdx.x < T.count) {
+        const bool valid = (int)threadIdx.x < T.count;
+        int err = 0;
+        if (valid) {
+            const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
             uint32_t t[16];
             gather_block(src, b % L.bw, b / L.bw, t);
             #pragma unroll
             for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
             uint4 blk;
-            int err = mode6_encode(t, TexRef{&s_tex[0][threadIdx.x], CTA}, blk);
+            err = mode6_encode(t, TexRef{&s_tex[0][threadIdx.x], CTA}, blk);
             store_block16(L.dst + (size_t)b * 16, blk);
-            if (err > 16 * 4) s_list[atomicAdd(&s_count, 1)] = make_uint2((uint32_t)b, (uint32_t)err);
         }
-        __syncthreads();
-        const int n = s_count;
-        for (int k = (int)threadIdx.x / kBc7Group; k < n; k += CTA / kBc7Group) {
-            const uint2 item = s_list[k];
-            const int hb = (int)item.x;
-            uint32_t t[16];
-            gather_block(src, hb % L.bw, hb / L.bw, t);
-            bc7_group_block(t, stage_group_texels(gtex, t, l, gmask), (int)item.y, L.dst + (size_t)hb * 16, l, gmask);
+        const bool hard = valid && err > 16 * 4;  // zap_tex.h:758 early exit
+        const unsigned ballot = __ballot_sync(0xFFFFFFFFu, hard);
+        if (ballot) {
+            const int lane = threadIdx.x & 31, leader = __ffs(ballot) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(hard_count, (uint32_t)__popc(ballot));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (hard) hard_items[base + __popc(ballot & ((1u << lane) - 1u))] = make_uint2(L.gbase + (uint32_t)b, (uint32_t)err);
         }
-        __syncthreads();
+    }
+}
+
+// bases[k]: batch-wide id of the first block of BC7 level k (ascending); level_of[k]: its index in `levels`
+__global__ void __launch_bounds__(128, ZTC_MINB_BC7_HARD)
+batch_bc7_hard_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__restrict__ bases, const int *__restrict__ level_of,
+                      int nlevels, const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
+    __shared__ uint32_t s_gtex[128 / kBc7Group][17];
+    const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
+    const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
+    const int ngroups = gridDim.x * (blockDim.x / kBc7Group);
+    const int n = (int)*(volatile const uint32_t *)count;
+    uint32_t *gtex = s_gtex[threadIdx.x / kBc7Group];
+    for (int it = blockIdx.x * (blockDim.x / kBc7Group) + (threadIdx.x / kBc7Group); it < n; it += ngroups) {
+        const uint2 item = items[it];
+        int lo = 0, hi = nlevels - 1;  // last level whose first id is <= the block's id
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(bases + mid) <= item.x) lo = mid; else hi = mid - 1;
+        }
+        const BatchLevel L = levels[__ldg(level_of + lo)];
+        const int b = (int)(item.x - __ldg(bases + lo));
+        const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
+        uint32_t t[16];
+        gather_block(src, b % L.bw, b / L.bw, t);
+        bc7_group_block(t, stage_group_texels(gtex, t, l, gmask), (int)item.y, L.dst + (size_t)b * 16, l, gmask);
     }
 }
 
 }  // namespace ztc
 
-cudaError_t ztc_launch_batch_bc7(int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
-                                 uint32_t *counter, cudaStream_t stream) {
+cudaError_t ztc_launch_batch_bc7_mode6(int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
+                                       uint32_t *counter, uint32_t *hard_count, uint2 *hard_items, cudaStream_t stream) {
     switch (cta) {
-    case 64: ztc::batch_bc7_kernel<64><<<grid, 64, 0, stream>>>(levels, tiles, ntiles, counter); break;
-    case 128: ztc::batch_bc7_kernel<128><<<grid, 128, 0, stream>>>(levels, tiles, ntiles, counter); break;
-    case 256: ztc::batch_bc7_kernel<256><<<grid, 256, 0, stream>>>(levels, tiles, ntiles, counter); break;
+    case 64: ztc::batch_bc7_mode6_kernel<64><<<grid, 64, 0, stream>>>(levels, tiles, ntiles, counter, hard_count, hard_items); break;
+    case 128: ztc::batch_bc7_mode6_kernel<128><<<grid, 128, 0, stream>>>(levels, tiles, ntiles, counter, hard_count, hard_items); break;
+    case 256: ztc::batch_bc7_mode6_kernel<256><<<grid, 256, 0, stream>>>(levels, tiles, ntiles, counter, hard_count, hard_items); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
+cudaError_t ztc_launch_batch_bc7_hard(int grid, const ztc::BatchLevel *levels, const uint32_t *bases, const int *level_of, int nlevels,
+                                      const uint32_t *hard_count, const uint2 *hard_items, cudaStream_t stream) {
+    ztc::batch_bc7_hard_kernel<<<grid, 128, 0, stream>>>(levels, bases, level_of, nlevels, hard_count, hard_items);
+    return cudaGetLastError();
+}
+
 const void *ztc_batch_bc7_kernel_fn(int cta) {
     switch (cta) {
-    case 64: return (const void *)ztc::batch_bc7_kernel<64>;
-    case 128: return (const void *)ztc::batch_bc7_kernel<128>;
-    case 256: return (const void *)ztc::batch_bc7_kernel<256>;
+    case 64: return (const void *)ztc::batch_bc7_mode6_kernel<64>;
+    case 128: return (const void *)ztc::batch_bc7_mode6_kernel<128>;
+    case 256: return (const void *)ztc::batch_bc7_mode6_kernel<256>;
     default: return nullptr;
     }
 }
+
+const void *ztc_batch_bc7_hard_kernel_fn() { return (const void *)ztc::batch_bc7_hard_kernel; }
 
 size_t ztc::bc7_scratch_bytes(size_t nblocks) { return 256 + nblocks * sizeof(uint2); }
 

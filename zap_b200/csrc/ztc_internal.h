@@ -46,6 +46,8 @@ struct BatchLevel {     // one (texture, mip level) to encode
     uint8_t *dst;       // its encoded blocks
     size_t pitch;       // bytes per texel row
     int w, h, bw, fmt;
+    uint32_t gbase;     // BC7 levels: batch-wide id of the level's first block (ids run over the batch's BC7 levels)
+    uint32_t pad;
 };
 struct BatchTile {      // consecutive blocks [first, first + count) of one level
     int level, first, count, pad;
@@ -63,12 +65,18 @@ struct BatchMipTile {   // output texel pairs [first, first + count) of one Batc
 
 cudaError_t ztc_launch_batch_bcn(int fmt, int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
                                  uint32_t *counter, cudaStream_t stream);
-cudaError_t ztc_launch_batch_bc7(int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
-                                 uint32_t *counter, cudaStream_t stream);
+// BC7 in two launches: mode 6 over the tile queue, appending (batch-wide block id, SSE) of the blocks it does not
+// finish to hard_items; then modes 5 / 1 over that list (bases / level_of: the BC7 levels' first ids, ascending,
+// and their indices in `levels`)
+cudaError_t ztc_launch_batch_bc7_mode6(int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
+                                       uint32_t *counter, uint32_t *hard_count, uint2 *hard_items, cudaStream_t stream);
+cudaError_t ztc_launch_batch_bc7_hard(int grid, const ztc::BatchLevel *levels, const uint32_t *bases, const int *level_of, int nlevels,
+                                      const uint32_t *hard_count, const uint2 *hard_items, cudaStream_t stream);
 cudaError_t ztc_launch_batch_mip(int grid, const ztc::BatchMip *mips, const ztc::BatchMipTile *tiles, int ntiles, const float *srgb_tables,
                                  cudaStream_t stream);
 const void *ztc_batch_bcn_kernel_fn(int fmt, int cta);
-const void *ztc_batch_bc7_kernel_fn(int cta);
+const void *ztc_batch_bc7_kernel_fn(int cta);  // the mode 6 tile-queue kernel
+const void *ztc_batch_bc7_hard_kernel_fn();
 const void *ztc_batch_mip_kernel_fn();
 namespace ztc { void srgb_tables_host(float lin[256], float thr[256]); }
 
