@@ -203,12 +203,28 @@ __global__ void __launch_bounds__(128, ZTC_MINB_BC7_MODE6) bc7_mode6_kernel(SrcU
 }
 
 // ---------------------------------------------------------------- kernel B pieces
-// mode 5 part: 2-bit palette on channels [C0, C0 + NC) of the rotated texels (zap_tex.h:597-657)
-template <int NC>
-ZTC_DEV void m5_quant(const float v[4], int n, int q[4], int x8[4]) {
-    int top = (1 << n) - 1;
+// mode 5 part (zap_tex.h:597-657): 2-bit palette on the colour part (RGB of the rotated texels, 7-bit endpoints)
+// or the alpha part (their A byte, 8-bit endpoints). Both kinds run the same code with nc = 3 or 1 channels, so
+// the colour and alpha lanes of a group do not diverge: a part's texel holds its channels in the low bytes and
+// zeros above, and unused palette channels are zero too, so the integer keys and sums are those of an nc-channel
+// computation, and each used channel's float sums run in the reference's order.
+ZTC_DEV uint32_t rotate_texel(uint32_t v, int rot) {  // mode 5 rotation: swap A with R (1), G (2) or B (3)
+    if (rot) {
+        const int sh = 8 * (rot - 1);
+        const uint32_t a = v >> 24, c = (v >> sh) & 0xFFu;
+        v = (v & ~((0xFFu << sh) | 0xFF000000u)) | (a << sh) | (c << 24);
+    }
+    return v;
+}
+ZTC_DEV uint32_t part_texel(uint32_t v, int rot, bool alpha) {
+    const uint32_t r = rotate_texel(v, rot);
+    return alpha ? (r >> 24) : (r & 0x00FFFFFFu);
+}
+ZTC_DEV void m5_quant(const float v[3], int nc, int n, int q[3], int x8[3]) {
+    const int top = (1 << n) - 1;
     #pragma unroll
-    for (int c = 0; c < NC; c++) {
+    for (int c = 0; c < 3; c++) {
+        if (c >= nc) { q[c] = 0; x8[c] = 0; continue; }
         int g = f2i_x86(v[c] * (float)top / 255.0f + 0.5f), bq = 0, bd = 1 << 30;
         #pragma unroll
         for (int k = 0; k < 3; k++) {
@@ -219,26 +235,21 @@ ZTC_DEV void m5_quant(const float v[4], int n, int q[4], int x8[4]) {
         q[c] = bq; x8[c] = expand_bits(bq, n);
     }
 }
-// texels of a part, packed into the low bytes: colour = RGB of the rotated texel, alpha = its A byte
-template <int NC>
-ZTC_DEV uint32_t part_bytes(uint32_t r) { return NC == 3 ? (r & 0x00FFFFFFu) : (r >> 24); }
-
-template <int NC>
-ZTC_DEV int m5_fit(const uint32_t r[16], const int x0[4], const int x1[4], uint32_t &idx) {
+ZTC_DEV int m5_fit(TexRef ts, int rot, bool alpha, const int x0[3], const int x1[3], uint32_t &idx) {
     uint32_t pal[4];
     int A[4];
     #pragma unroll
     for (int j = 0; j < 4; j++) {
         uint32_t e = 0;
         #pragma unroll
-        for (int c = 0; c < NC; c++) e |= (uint32_t)lerp64(x0[c], x1[c], w2(j)) << (8 * c);
+        for (int c = 0; c < 3; c++) e |= (uint32_t)lerp64(x0[c], x1[c], w2(j)) << (8 * c);
         pal[j] = e; A[j] = (int)dot4(e, e) * 4 + j;
     }
     int err = 0;
     uint32_t bits = 0;
-    #pragma unroll
+    #pragma unroll 1
     for (int i = 0; i < 16; i++) {
-        uint32_t p = part_bytes<NC>(r[i]);
+        const uint32_t p = part_texel(ts[i], rot, alpha);
         int m = min(min(A[0] - 8 * (int)dot4(p, pal[0]), A[1] - 8 * (int)dot4(p, pal[1])),
                     min(A[2] - 8 * (int)dot4(p, pal[2]), A[3] - 8 * (int)dot4(p, pal[3])));
         err += (m >> 2) + (int)dot4(p, p);
@@ -247,58 +258,47 @@ ZTC_DEV int m5_fit(const uint32_t r[16], const int x0[4], const int x1[4], uint3
     idx = bits;
     return err;
 }
-template <int NC>
-ZTC_DEV bool m5_lsq(const uint32_t r[16], uint32_t idx, float lo[4], float hi[4]) {
-    float aa = 0.0f, ab = 0.0f, bb = 0.0f, sa[NC], sb[NC];
-    #pragma unroll
-    for (int c = 0; c < NC; c++) { sa[c] = 0.0f; sb[c] = 0.0f; }
-    #pragma unroll
+ZTC_DEV bool m5_lsq(TexRef ts, int rot, bool alpha, int nc, uint32_t idx, float lo[3], float hi[3]) {
+    float aa = 0.0f, ab = 0.0f, bb = 0.0f, sa[3] = {0.0f, 0.0f, 0.0f}, sb[3] = {0.0f, 0.0f, 0.0f};
+    #pragma unroll 1
     for (int i = 0; i < 16; i++) {
         float w = (float)w2((int)((idx >> (2 * i)) & 3u)) / 64.0f, u = 1.0f - w;
         aa = aa + u * u; ab = ab + u * w; bb = bb + w * w;
-        uint32_t p = part_bytes<NC>(r[i]);
+        const uint32_t p = part_texel(ts[i], rot, alpha);
         #pragma unroll
-        for (int c = 0; c < NC; c++) { float x = (float)chan(p, c); sa[c] = sa[c] + u * x; sb[c] = sb[c] + w * x; }
+        for (int c = 0; c < 3; c++) { float x = (float)chan(p, c); sa[c] = sa[c] + u * x; sb[c] = sb[c] + w * x; }
     }
     float det = aa * bb - ab * ab;
     if (det < 1e-6f && det > -1e-6f) return false;
     #pragma unroll
-    for (int c = 0; c < NC; c++) { lo[c] = clamp255((sa[c] * bb - sb[c] * ab) / det); hi[c] = clamp255((sb[c] * aa - sa[c] * ab) / det); }
+    for (int c = 0; c < 3; c++)
+        if (c < nc) { lo[c] = clamp255((sa[c] * bb - sb[c] * ab) / det); hi[c] = clamp255((sb[c] * aa - sa[c] * ab) / det); }
     return true;
 }
-template <int NC>
-ZTC_DEV int m5_part(const uint32_t r[16], int n, const float lo[4], const float hi[4], int q[2][4], uint32_t &idx) {
-    int x0[4], x1[4];
-    m5_quant<NC>(lo, n, q[0], x0); m5_quant<NC>(hi, n, q[1], x1);
-    int err = m5_fit<NC>(r, x0, x1, idx);
-    for (int it = 0; it < 2 && err > 0; it++) {
-        float nlo[4], nhi[4];
-        if (!m5_lsq<NC>(r, idx, nlo, nhi)) break;
-        int tq[2][4];
-        m5_quant<NC>(nlo, n, tq[0], x0); m5_quant<NC>(nhi, n, tq[1], x1);
+// quantise, fit, up to two least-squares refits (zap_tex.h:626-657); lo / hi: the start endpoints
+ZTC_DEV int m5_part(TexRef ts, int rot, bool alpha, float lo[3], float hi[3], int q[2][3], uint32_t &idx) {
+    const int nc = alpha ? 1 : 3, n = alpha ? 8 : 7;
+    int err = 0;
+    #pragma unroll 1
+    for (int it = 0; it < 3; it++) {
+        if (it > 0 && !m5_lsq(ts, rot, alpha, nc, idx, lo, hi)) break;
+        int tq[2][3], x0[3], x1[3];
+        m5_quant(lo, nc, n, tq[0], x0); m5_quant(hi, nc, n, tq[1], x1);
         uint32_t ti;
-        int e = m5_fit<NC>(r, x0, x1, ti);
-        if (e >= err) break;
+        const int e = m5_fit(ts, rot, alpha, x0, x1, ti);
+        if (it > 0 && e >= err) break;
         err = e; idx = ti;
         #pragma unroll
-        for (int c = 0; c < NC; c++) { q[0][c] = tq[0][c]; q[1][c] = tq[1][c]; }
+        for (int c = 0; c < 3; c++) { q[0][c] = tq[0][c]; q[1][c] = tq[1][c]; }
+        if (err <= 0) break;
     }
     return err;
 }
 
-// partition score from per-texel moments (zap_tex.h:722-748); t holds the opaque block's texels
-ZTC_DEV float partition_score(const float mo[16][9], const float tot[9], uint32_t pmask) {
-    float s1[9], s0[9];
-    int n1 = 0;
-    #pragma unroll
-    for (int j = 0; j < 9; j++) s1[j] = 0.0f;
-    #pragma unroll
-    for (int i = 0; i < 16; i++)
-        if ((pmask >> i) & 1u) {
-            n1++;
-            #pragma unroll
-            for (int j = 0; j < 9; j++) s1[j] = s1[j] + mo[i][j];
-        }
+// partition score (zap_tex.h:722-748) from the 9 moment sums of subset 1 (s1, over its n1 texels, added in texel
+// order) and of the whole block (tot); subset 0's sums are tot - s1, as in the reference
+ZTC_DEV float partition_score(const float s1[9], int n1, const float tot[9]) {
+    float s0[9];
     #pragma unroll
     for (int j = 0; j < 9; j++) s0[j] = tot[j] - s1[j];
     float score = 0.0f;
@@ -354,34 +354,26 @@ __device__ __forceinline__ void bc7_group_block(const uint32_t t[16], TexRef ts,
         // ---- mode 5: lane = rotation * 2 + part (zap_tex.h:659-684)
         const int rot = l >> 1;
         const bool alpha_part = l & 1;
-        uint32_t r[16];
-        #pragma unroll
-        for (int i = 0; i < 16; i++) {
-            uint32_t v = t[i];
-            if (rot) {
-                int sh = 8 * (rot - 1);
-                uint32_t a = v >> 24, c = (v >> sh) & 0xFFu;
-                v = (v & ~((0xFFu << sh) | 0xFF000000u)) | (a << sh) | (c << 24);
-            }
-            r[i] = v;
-        }
-        int q5[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+        int q5[2][3] = {{0, 0, 0}, {0, 0, 0}};
         uint32_t i5 = 0;
-        int e5;
-        if (!alpha_part) {
+        float lo5[3] = {255.0f, 0.0f, 0.0f}, hi5[3] = {0.0f, 0.0f, 0.0f};
+        if (!alpha_part) {  // colour part starts from the principal axis of the rotated RGB
+            uint32_t r[16];
+            #pragma unroll
+            for (int i = 0; i < 16; i++) r[i] = rotate_texel(t[i], rot);
             float lo[4], hi[4];
             pca_endpoints<3>(r, 0xFFFFu, lo, hi);
-            e5 = m5_part<3>(r, 7, lo, hi, q5, i5);
-        } else {
-            float lo[4] = {255.0f, 0.0f, 0.0f, 0.0f}, hi[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            #pragma unroll
+            for (int c = 0; c < 3; c++) { lo5[c] = lo[c]; hi5[c] = hi[c]; }
+        } else {  // alpha part starts from the rotated alpha's range
             #pragma unroll
             for (int i = 0; i < 16; i++) {
-                float a = (float)(r[i] >> 24);
-                if (a < lo[0]) lo[0] = a;
-                if (a > hi[0]) hi[0] = a;
+                float a = (float)(rotate_texel(t[i], rot) >> 24);
+                if (a < lo5[0]) lo5[0] = a;
+                if (a > hi5[0]) hi5[0] = a;
             }
-            e5 = m5_part<1>(r, 8, lo, hi, q5, i5);
         }
+        const int e5 = m5_part(ts, rot, alpha_part, lo5, hi5, q5, i5);
         // anchor fix inside the owning lane (zap_tex.h:673-674): 3 - i == i ^ 3 for 2-bit indices
         if (i5 & 2u) {
             #pragma unroll
@@ -420,33 +412,55 @@ __device__ __forceinline__ void bc7_group_block(const uint32_t t[16], TexRef ts,
             blk = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
         }
         if (opaque) {  // group-uniform: every lane holds the same texels
-            // ---- mode 1 ranking: lane scores partitions l, l + 8, ..., l + 56 (zap_tex.h:764-775)
-            float mo[16][9], tot[9];
-            #pragma unroll
-            for (int j = 0; j < 9; j++) tot[j] = 0.0f;
-            #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                float rr = (float)chan(t[i], 0), gg = (float)chan(t[i], 1), bb = (float)chan(t[i], 2);
-                mo[i][0] = rr; mo[i][1] = gg; mo[i][2] = bb; mo[i][3] = rr * rr; mo[i][4] = gg * gg; mo[i][5] = bb * bb;
-                mo[i][6] = rr * gg; mo[i][7] = rr * bb; mo[i][8] = gg * bb;
-                #pragma unroll
-                for (int j = 0; j < 9; j++) tot[j] = tot[j] + mo[i][j];
-            }
+            // ---- mode 1 ranking: lane scores partitions l, l + 8, ..., l + 56 (zap_tex.h:764-775), four per round:
+            // one pass over the texels adds each texel's 9 moments to the block totals and to the sums of the
+            // four partitions' subset 1, every sum in texel order as the reference adds them
             float ce[kMode1Tries];
             int cp[kMode1Tries];
             #pragma unroll
             for (int j = 0; j < kMode1Tries; j++) { ce[j] = 1e30f; cp[j] = 64; }
-            for (int k = 0; k < 64 / kBc7Group; k++) {
-                int part = l + kBc7Group * k;
-                float e = partition_score(mo, tot, kP2[part]);
-                // insertion keeps (score, partition) order; NaN and >= 1e30 never enter, as in the reference
+            #pragma unroll 1
+            for (int round = 0; round < 2; round++) {
+                uint32_t pm[4];
+                int n1[4];
+                float s1[4][9], tot[9];
                 #pragma unroll
-                for (int j = 0; j < kMode1Tries; j++) {
-                    if (e < ce[j]) {
-                        #pragma unroll
-                        for (int s = kMode1Tries - 1; s > j; s--) { ce[s] = ce[s - 1]; cp[s] = cp[s - 1]; }
-                        ce[j] = e; cp[j] = part;
-                        break;
+                for (int k = 0; k < 4; k++) {
+                    pm[k] = kP2[l + kBc7Group * (4 * round + k)];
+                    n1[k] = 0;
+                    #pragma unroll
+                    for (int j = 0; j < 9; j++) s1[k][j] = 0.0f;
+                }
+                #pragma unroll
+                for (int j = 0; j < 9; j++) tot[j] = 0.0f;
+                #pragma unroll 1
+                for (int i = 0; i < 16; i++) {
+                    const uint32_t x = ts[i];
+                    const float rr = (float)chan(x, 0), gg = (float)chan(x, 1), bb = (float)chan(x, 2);
+                    const float mo[9] = {rr, gg, bb, rr * rr, gg * gg, bb * bb, rr * gg, rr * bb, gg * bb};
+                    #pragma unroll
+                    for (int j = 0; j < 9; j++) tot[j] = tot[j] + mo[j];
+                    #pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        if ((pm[k] >> i) & 1u) {
+                            n1[k]++;
+                            #pragma unroll
+                            for (int j = 0; j < 9; j++) s1[k][j] = s1[k][j] + mo[j];
+                        }
+                }
+                #pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int part = l + kBc7Group * (4 * round + k);
+                    const float e = partition_score(s1[k], n1[k], tot);
+                    // insertion keeps (score, partition) order; NaN and >= 1e30 never enter, as in the reference
+                    #pragma unroll
+                    for (int j = 0; j < kMode1Tries; j++) {
+                        if (e < ce[j]) {
+                            #pragma unroll
+                            for (int s = kMode1Tries - 1; s > j; s--) { ce[s] = ce[s - 1]; cp[s] = cp[s - 1]; }
+                            ce[j] = e; cp[j] = part;
+                            break;
+                        }
                     }
                 }
             }
