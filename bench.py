@@ -12,7 +12,9 @@ every rank encodes its own ring (weak scaling, no collective on the data path); 
 `e2e` is the same workload through the synchronous host C ABI (zap_tex_cuda_bc_encode): pinned host texture in,
 host->device copy, encode, device->host copy of the blocks, every step.
 `roofline` is the dominant kernel's algorithmic bytes per launch / its CUDA-event duration, against the measured HBM
-copy bandwidth (the encoders are compute-bound, so `alu` beside it gives the issue-rate view from ncu).
+copy bandwidth. The encoders are compute-bound, so `roofline.alu` adds the bound that binds: the reference
+algorithm's counted operations per launch (profiles/alu_ops.json, from oracle/count_ops.py on these textures) over
+the same duration, against 128 lanes x SMs x the SM clock sampled during the timed region.
 `cpu_baseline` is the reference's own encoder (oracle/_ref, built from zap_tex.h) on this host's cores, using the
 reference's band-parallel scheme; `--impl reference` times only that, on the same workload.
 """
@@ -166,6 +168,39 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def alu_roofline(kernel, ops_per_launch_ms, sm_mhz, sms):
+    """ALU roofline of one kernel: the reference algorithm's counted operations per launch (profiles/alu_ops.json,
+    written by oracle/count_ops.py on this workload's textures) over the kernel's average launch time, against a
+    derived issue peak of 128 32-bit lanes per SM x SMs x the median SM clock of the timed region. The kernels do a
+    texel-to-entry distance (13 counted ops for RGBA) in one dp4a + one multiply-add + one min, so a fraction above
+    1 is possible; the fraction is a throughput figure against scalar issue, not a utilisation."""
+    ops, ms = ops_per_launch_ms
+    table = alu_ops()
+    if ops is None or not ms or not sm_mhz:
+        return None
+    peak = sms * 128 * sm_mhz * 1e6 / 1e9
+    achieved = ops / (ms / 1e3) / 1e9
+    return {"bound": "alu", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "Gop/s", "frac": achieved / peak,
+            "ops_per_launch": ops, "peak_source": f"derived: {sms} SMs x 128 lanes x {sm_mhz:.0f} MHz (median SM clock, timed region)",
+            "ops_definition": table.get("definition") if table else None}
+
+
+def alu_ops():
+    try:
+        with open(os.path.join(ROOT, "profiles", "alu_ops.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def ops_per_texture(kernel):
+    table = alu_ops() or {}
+    for entry in table.values():
+        if isinstance(entry, dict) and kernel in entry.get("ops_per_texture", {}):
+            return entry["ops_per_texture"][kernel]
+    return None
+
+
 def reference_cpu(img_np, fmt, reps=3):
     """Best-of-reps wall time of the reference encoder on all host threads (viewer.cpp band scheme)."""
     import oracle_lib
@@ -286,6 +321,12 @@ def main():
                 "traffic": traffic, "peak_source": peak_kind, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
                 "kernels": {k: {"launches": v[0], "ms": v[1], "units": v[2], "share": v[1] / sum(x[1] for x in rep.values())}
                             for k, v in rep.items()}}
+    # the bound that binds: counted algorithmic ops against the SMs' issue rate (one launch = one 2048^2 texture)
+    csum = clocks.summary()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = csum.get("sm_mhz") or csum.get("sm_max_mhz")
+    roofline["alu"] = alu_roofline(name, (ops_per_texture(name), avg_ms), mhz, sms)
+    roofline["alu_kernels"] = {k: alu_roofline(k, (ops_per_texture(k), v[1] / max(1, v[0])), mhz, sms) for k, v in rep.items()}
 
     line = {"metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
@@ -316,7 +357,7 @@ def main():
             same = np.mean(np.all(hout.reshape(-1, 16) == cpu["out"].reshape(-1, 16), axis=1))
             line["parity"] = {"identical_blocks": float(same)}
         if not args.no_extra:
-            line["extra"] = extra_workloads(args, dev)
+            line["extra"] = extra_workloads(args, dev, mhz, sms)
             line["batched"] = batched_workload(args, dev)
             line["refine"] = refine_workload(args, dev)
         print(json.dumps(line))
@@ -402,7 +443,7 @@ def refine_workload(args, dev, n=1024, side=256, steps=8, lr=1.0):
     return res
 
 
-def extra_workloads(args, dev):
+def extra_workloads(args, dev, sm_mhz=None, sms=148):
     """Secondary figures: BC1 (config 0 and 2048^2), BC4 R8 / BC5 RG8 (config 1), BC6H / ASTC (config 3)."""
     import torch
 
@@ -423,6 +464,8 @@ def extra_workloads(args, dev):
         ms = time_device(step, steps, 0, 1)
         mps = steps * npix / 1e6 / (ms / 1e3)
         res[name] = {"Mpix_s": mps, "ms_per_encode": ms / steps, "GB_s_algorithmic": mps * 1e6 * alg_bytes_per_px / 1e9}
+        if name == "bc1_2048x2048":  # whole encode (one kernel) against the ALU roofline
+            res[name]["alu"] = alu_roofline("bc1_encode", (ops_per_texture("bc1_encode"), ms / steps), sm_mhz, sms)
 
     bench("bc1_512x512_config0", lambda k: S.colour_texture(512, 512, seed=k, device=dev), zap_b200.BC1, 512 * 512, 64, 4.5)
     bench("bc1_2048x2048", lambda k: S.colour_texture(2048, 2048, seed=k, device=dev), zap_b200.BC1, 2048 * 2048, 10, 4.5)

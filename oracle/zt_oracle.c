@@ -20,6 +20,18 @@
 
 typedef uint8_t tx4[4]; /* one RGBA8 texel */
 
+/* Algorithmic op counts, compiled only into oracle/liboracle_ops.so (-DZO_COUNT_OPS; oracle/count_ops.py). One
+ * texel-to-palette-entry distance over C channels counts 3C + 1 ops (C differences, C squares, C accumulations,
+ * one comparison); the BC7 mode 1 ranking counts 9 additions per texel summed into a subset's moments. Counters
+ * are plain globals: count with one thread. Slot 0: everything; slot 1: BC7 mode 6 only. */
+#ifdef ZO_COUNT_OPS
+static uint64_t g_ops[2];
+#define ZO_OPS(n) (g_ops[0] += (uint64_t)(n))
+void zo_ops_take(uint64_t out[2]) { out[0] = g_ops[0]; out[1] = g_ops[1]; g_ops[0] = g_ops[1] = 0; }
+#else
+#define ZO_OPS(n) ((void)0)
+#endif
+
 static int imin(int a, int b) { return a < b ? a : b; }
 static int iclamp(int v, int lo, int hi) { return v < lo ? lo : v > hi ? hi : v; }
 static float fclamp255(float v) { return v < 0 ? 0 : v > 255 ? 255 : v; } /* NaN passes through, as in the reference */
@@ -76,9 +88,11 @@ static int bc1_eval_pair(const tx4 t[16], uint16_t *c0, uint16_t *c1, uint32_t *
     bc1_pal4(*c0, *c1, pal);
     if (*c0 == *c1) {
         *idx = 0;
+        ZO_OPS(16 * 10);
         for (int i = 0; i < 16; i++) err += d3(t[i], pal[0]);
         return err;
     }
+    ZO_OPS(16 * 4 * 10);
     uint32_t bits = 0;
     for (int i = 0; i < 16; i++) {
         int bk = 0, be = d3(t[i], pal[0]);
@@ -185,6 +199,7 @@ static int bc4_block(const uint8_t v[16], uint8_t *oa0, uint8_t *oa1, uint64_t *
             int pal[8], err = 0;
             uint64_t bits = 0;
             bc4_pal(a0, a1, pal);
+            ZO_OPS(a0 == a1 ? 16 * 4 : 16 * 8 * 4);
             for (int i = 0; i < 16; i++) {
                 if (a0 == a1) { err += (v[i] - pal[0]) * (v[i] - pal[0]); continue; }
                 int bk = 0, be = (v[i] - pal[0]) * (v[i] - pal[0]);
@@ -362,6 +377,7 @@ static int bc7_subset_fit(const tx4 t[16], const int *sel, int cnt, int nc, int 
     for (int k = 0; k < 2; k++) for (int c = 0; c < nc; c++) x8[k][c] = bc7_expand((q[k][c] << 1) | pb[k], n);
     int pal[16][4], np = 1 << ib, err = 0;
     for (int j = 0; j < np; j++) for (int c = 0; c < nc; c++) pal[j][c] = lerp64(x8[0][c], x8[1][c], bc7_weight(ib, j));
+    ZO_OPS(cnt * np * (3 * nc + 1));
     for (int k = 0; k < cnt; k++) {
         int bj = 0, be = 1 << 30;
         for (int j = 0; j < np; j++) {
@@ -426,6 +442,7 @@ static int bc7_mode6(const tx4 t[16], uint8_t out[16]) {
 static int m5_fit(const tx4 r[16], int c0, int nc, const int *e0, const int *e1, int idx[16]) {
     int pal[4][4], err = 0;
     for (int j = 0; j < 4; j++) for (int c = 0; c < nc; c++) pal[j][c] = lerp64(e0[c], e1[c], BC7_W2[j]);
+    ZO_OPS(16 * 4 * (3 * nc + 1));
     for (int i = 0; i < 16; i++) {
         int bj = 0, be = 1 << 30;
         for (int j = 0; j < 4; j++) {
@@ -541,6 +558,7 @@ static float bc7_partition_score(const float mo[16][9], const float tot[9], int 
     for (int j = 0; j < 9; j++) s[1][j] = 0;
     for (int i = 0; i < 16; i++)
         if ((BC7_P2[part] >> i) & 1) { n1++; for (int j = 0; j < 9; j++) s[1][j] += mo[i][j]; }
+    ZO_OPS(9 * n1);
     for (int j = 0; j < 9; j++) s[0][j] = tot[j] - s[1][j];
     float score = 0;
     for (int k = 0; k < 2; k++) {
@@ -573,7 +591,13 @@ static float bc7_partition_score(const float mo[16][9], const float tot[9], int 
 
 /* mode 6, early exit at SSE <= 64, then mode 5, then (opaque) mode 1 over the best-scored partitions (:755-784) */
 static void bc7_block(const tx4 t[16], uint8_t out[16]) {
+#ifdef ZO_COUNT_OPS
+    const uint64_t ops0 = g_ops[0];
+#endif
     int err = bc7_mode6(t, out), opaque = 1;
+#ifdef ZO_COUNT_OPS
+    g_ops[1] += g_ops[0] - ops0;
+#endif
     for (int i = 0; i < 16; i++) opaque &= t[i][3] == 255;
     if (err <= 16 * 4) return;
     uint8_t m5[16];
@@ -734,6 +758,7 @@ static int64_t bc6_fit(const uint16_t t[16][3], const int e[2][3], int idx[16]) 
     int64_t err = 0;
     for (int j = 0; j < 16; j++)
         for (int c = 0; c < 3; c++) pal[j][c] = bc6_finish(lerp64(bc6_unquant(e[0][c]), bc6_unquant(e[1][c]), BC7_W4[j]));
+    ZO_OPS(16 * 16 * 10);
     for (int i = 0; i < 16; i++) {
         int64_t be = INT64_MAX;
         int bi = 0;
@@ -1085,6 +1110,7 @@ static int astc_fit_weights(const tx4 px[16], const astc_cfg *c, const int *uv, 
             for (int ch = 0; ch < 4; ch++) pal[k][j][ch] = astc_lerp(e0[ch], e1[ch], wt);
         }
     }
+    ZO_OPS(16 * L * (3 * nc + 1));
     for (int i = 0; i < 16; i++) {
         int bj = 0, be = 1 << 30, k = part[i];
         for (int j = 0; j < L; j++) {
