@@ -120,6 +120,22 @@ ZTC_API int zap_tex_cuda_bc_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, in
 ZTC_API int zap_tex_cuda_bc6h_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint16_t *rgba, size_t stride,
                                          void *stream);
 
+/* ---------------------------------------------------------------- split / merge (zap_tex.h:1549-1571)
+   Plane k of the split form holds field k of every block, the planes one after another: BC1 {4, 4}, BC3
+   {2, 6, 4, 4}, BC4 {2, 6}, BC5 {2, 6, 2, 6}, BC7 {8, 1, 7} bytes; bytes after the last whole block are copied
+   unchanged. n bytes in, n bytes out; in and out must not overlap (ZTC_ERR_INVALID_ARG). */
+/* replace zap_bc_split / zap_bc_merge (zap_tex.h:1567-1568), host memory, synchronous */
+ZTC_API int zap_tex_cuda_bc_split(zap_tex_cuda_ctx *ctx, const void *bc, size_t n, int fmt, void *out);
+ZTC_API int zap_tex_cuda_bc_merge(zap_tex_cuda_ctx *ctx, const void *planes, size_t n, int fmt, void *out);
+/* the same, device memory, asynchronous on stream */
+ZTC_API int zap_tex_cuda_bc_split_dev(zap_tex_cuda_ctx *ctx, const void *bc, size_t n, int fmt, void *out, void *stream);
+ZTC_API int zap_tex_cuda_bc_merge_dev(zap_tex_cuda_ctx *ctx, const void *planes, size_t n, int fmt, void *out, void *stream);
+/* Encode straight into the split form, no reference counterpart: the bytes of zap_bc_encode (rdo 0) followed by
+   zap_bc_split (the caller sequence of tex_bench.c:209-212), with the encoders storing each
+   field into its plane, so no second pass over the blocks. out holds zap_tex_cuda_bc_size(w, h, fmt) bytes. */
+ZTC_API int zap_tex_cuda_bc_encode_split_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt,
+                                             void *out, void *stream);
+
 /* ---------------------------------------------------------------- differentiable palette decode, refinement
    No reference counterpart. With indices held fixed, decoding is linear in the endpoints:
      decoded[b][i][c] = a_i * e0[c] + (1 - a_i) * e1[c]

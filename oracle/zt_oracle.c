@@ -713,6 +713,30 @@ void zo_bc_decode(const void *bc_, int w, int h, int fmt, uint8_t *rgba, size_t 
         }
 }
 
+/* split / merge (:1549-1571): plane k holds field k of every block, fields in block order; the planes follow one
+ * another, and bytes after the last whole block are copied unchanged */
+static int bc_fields(int fmt, int sz[4]) {
+    static const int F[5][5] = { { 2, 4, 4 }, { 4, 2, 6, 4, 4 }, { 2, 2, 6 }, { 4, 2, 6, 2, 6 }, { 3, 8, 1, 7 } };
+    for (int k = 0; k < F[fmt][0]; k++) sz[k] = F[fmt][k + 1];
+    return F[fmt][0];
+}
+static void bc_regroup(const uint8_t *in, uint8_t *out, size_t n, int fmt, int to_planes) {
+    int sz[4], nf = bc_fields(fmt, sz);
+    size_t bs = (fmt == ZO_BC1 || fmt == ZO_BC4) ? 8 : 16, nb = n / bs, plane = 0, off = 0;
+    for (int k = 0; k < nf; k++) {
+        for (size_t b = 0; b < nb; b++) {
+            size_t blk = b * bs + off, pl = plane + b * (size_t)sz[k];
+            if (to_planes) memcpy(out + pl, in + blk, (size_t)sz[k]);
+            else memcpy(out + blk, in + pl, (size_t)sz[k]);
+        }
+        plane += nb * (size_t)sz[k];
+        off += (size_t)sz[k];
+    }
+    memcpy(out + nb * bs, in + nb * bs, n - nb * bs);
+}
+void zo_bc_split(const void *bc, size_t n, int fmt, void *out) { bc_regroup((const uint8_t *)bc, (uint8_t *)out, n, fmt, 1); }
+void zo_bc_merge(const void *planes, size_t n, int fmt, void *out) { bc_regroup((const uint8_t *)planes, (uint8_t *)out, n, fmt, 0); }
+
 void zo_bc7_mode_hist(const void *bc, size_t nblocks, int hist[9]) {
     const uint8_t *b = (const uint8_t *)bc;
     for (int m = 0; m < 9; m++) hist[m] = 0;

@@ -27,6 +27,8 @@ void zo_astc_decode(const void *bc, int w, int h, uint8_t *rgba, size_t stride);
 int zo_mip_levels(int w, int h);                                                                  /* :1435 */
 void zo_mip_next(const uint8_t *src, int w, int h, size_t stride, int srgb, uint8_t *dst, size_t dst_stride); /* :1442 */
 void zo_mip_next_f(const float *src, int w, int h, size_t stride, float *dst, size_t dst_stride);              /* :1460 */
+void zo_bc_split(const void *bc, size_t n, int fmt, void *out);                                   /* :1567 */
+void zo_bc_merge(const void *planes, size_t n, int fmt, void *out);                               /* :1568 */
 
 /* internals pinned by the reference's self-test (tex_bench.c:47-48, :104-125) */
 uint16_t zo_f2h(float f);

@@ -55,6 +55,8 @@ class Oracle:
         self._fn("mip_next_f", [vp, i, i, sz, vp, sz], None)
         self._fn("f2h", [C.c_float], C.c_uint16)
         self._fn("h2f", [C.c_uint16], C.c_float)
+        self._fn("bc_split", [vp, sz, i, vp], None)
+        self._fn("bc_merge", [vp, sz, i, vp], None)
         if kind == "port":
             self._fn("astc_partition", [i, i, i, i], C.c_int)
             self._fn("ise_roundtrip", [i, i, vp, vp], C.c_int)
@@ -105,6 +107,18 @@ class Oracle:
         return out
 
     # ---- decoders
+    def bc_split(self, bc, fmt):
+        bc = np.ascontiguousarray(bc, dtype=np.uint8)
+        out = np.zeros_like(bc)
+        self._bc_split(bc.ctypes.data, bc.size, fmt, out.ctypes.data)
+        return out
+
+    def bc_merge(self, planes, fmt):
+        planes = np.ascontiguousarray(planes, dtype=np.uint8)
+        out = np.zeros_like(planes)
+        self._bc_merge(planes.ctypes.data, planes.size, fmt, out.ctypes.data)
+        return out
+
     def bc_decode(self, bc, w, h, fmt):
         out = np.zeros((h, w, 4), np.uint8)
         bc = np.ascontiguousarray(bc)

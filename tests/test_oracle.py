@@ -172,3 +172,27 @@ def test_reference_band_parallel_matches_single_call(reference):
         assert np.array_equal(reference.bc_encode(img, fmt, threads=4), reference.bc_encode(img, fmt))
     assert np.array_equal(reference.astc_encode(img, threads=3), reference.astc_encode(img))
     assert oracle_lib.bc_size(61, 75, BC7) == reference.bc_encode(img, BC7).size
+
+
+# ---------------------------------------------------------------- split / merge (zap_tex.h:1549-1571)
+def test_split_merge_identity(oracle):
+    """tex_bench.c:166-168: merge(split(x)) == x, for every format, whole blocks and stray tail bytes."""
+    rng = np.random.default_rng(8)
+    for fmt in (BC1, BC3, BC4, BC5, BC7):
+        for n in (0, 5, 8, 16, 17, 8 * 37 + 3, 16 * 41, 16 * 41 + 9):
+            x = rng.integers(0, 256, n, dtype=np.uint8)
+            s = oracle.bc_split(x, fmt)
+            assert np.array_equal(oracle.bc_merge(s, fmt), x), (fmt, n)
+            bs = oracle_lib.block_bytes(fmt)
+            if n >= 2 * bs:  # plane 0 starts with field 0 of blocks 0, 1, ...
+                f0 = {BC1: 4, BC3: 2, BC4: 2, BC5: 2, BC7: 8}[fmt]
+                assert np.array_equal(s[:f0], x[:f0]) and np.array_equal(s[f0:2 * f0], x[bs:bs + f0]), (fmt, n)
+
+
+def test_split_merge_match_reference_live(oracle, reference):
+    rng = np.random.default_rng(9)
+    for fmt in (BC1, BC3, BC4, BC5, BC7):
+        for n in (3, 16 * 53, 16 * 53 + 11):
+            x = rng.integers(0, 256, n, dtype=np.uint8)
+            assert np.array_equal(oracle.bc_split(x, fmt), reference.bc_split(x, fmt)), (fmt, n)
+            assert np.array_equal(oracle.bc_merge(x, fmt), reference.bc_merge(x, fmt)), (fmt, n)

@@ -189,6 +189,49 @@ def bc_decode_dev(bc, w, h, fmt, stream=None, ctx=None):
     return out
 
 
+def bc_split(bc, fmt, ctx=None):
+    """zap_bc_split (zap_tex.h:1567) on the device: numpy uint8 blocks -> field planes (same size)."""
+    bc = np.ascontiguousarray(bc, dtype=np.uint8)
+    out = np.empty_like(bc)
+    check(load().zap_tex_cuda_bc_split(ctx, bc.ctypes.data, bc.size, fmt, out.ctypes.data), "bc_split")
+    return out
+
+
+def bc_merge(planes, fmt, ctx=None):
+    """zap_bc_merge (zap_tex.h:1568) on the device: numpy uint8 field planes -> blocks."""
+    planes = np.ascontiguousarray(planes, dtype=np.uint8)
+    out = np.empty_like(planes)
+    check(load().zap_tex_cuda_bc_merge(ctx, planes.ctypes.data, planes.size, fmt, out.ctypes.data), "bc_merge")
+    return out
+
+
+def bc_split_dev(bc, fmt, out=None, stream=None, ctx=None):
+    """Device split: uint8 CUDA tensor of blocks -> field planes (a new tensor unless out is given)."""
+    import torch
+    out = torch.empty_like(bc) if out is None else out
+    check(load().zap_tex_cuda_bc_split_dev(ctx, bc.data_ptr(), bc.numel(), fmt, out.data_ptr(), _stream(stream)), "bc_split_dev")
+    return out
+
+
+def bc_merge_dev(planes, fmt, out=None, stream=None, ctx=None):
+    """Device merge: uint8 CUDA tensor of field planes -> blocks."""
+    import torch
+    out = torch.empty_like(planes) if out is None else out
+    check(load().zap_tex_cuda_bc_merge_dev(ctx, planes.data_ptr(), planes.numel(), fmt, out.data_ptr(), _stream(stream)), "bc_merge_dev")
+    return out
+
+
+def bc_encode_split_dev(t, fmt, out=None, stream=None, ctx=None):
+    """Encode an HxWx4 uint8 CUDA tensor straight into the split form (the bytes of bc_split(bc_encode(t)))."""
+    import torch
+    w, h, stride = _dev_img(t, (4,))
+    if out is None:
+        out = torch.empty(bc_size(w, h, fmt), dtype=torch.uint8, device=t.device)
+    check(load().zap_tex_cuda_bc_encode_split_dev(ctx, t.data_ptr(), w, h, stride, fmt, out.data_ptr(), _stream(stream)),
+          "bc_encode_split_dev")
+    return out
+
+
 def bc6h_decode_dev(bc, w, h, stream=None, ctx=None):
     """Device zap_bc6h_decode: blocks -> HxWx4 int16 tensor holding half bits (alpha 0x3C00)."""
     import torch

@@ -66,6 +66,11 @@ def _declare(lib):
         "zap_tex_cuda_bc7_encode_noalloc_dev": ([vp, i, i, sz, vp, vp], i),
         "zap_tex_cuda_bc_decode_dev": ([vp, vp, i, i, i, vp, sz, vp], i),
         "zap_tex_cuda_bc6h_decode_dev": ([vp, vp, i, i, vp, sz, vp], i),
+        "zap_tex_cuda_bc_split": ([vp, vp, sz, i, vp], i),
+        "zap_tex_cuda_bc_merge": ([vp, vp, sz, i, vp], i),
+        "zap_tex_cuda_bc_split_dev": ([vp, vp, sz, i, vp, vp], i),
+        "zap_tex_cuda_bc_merge_dev": ([vp, vp, sz, i, vp, vp], i),
+        "zap_tex_cuda_bc_encode_split_dev": ([vp, vp, i, i, sz, i, vp, vp], i),
         "zap_tex_cuda_block_endpoints_dev": ([vp, i, vp, i, vp, vp], i),
         "zap_tex_cuda_palette_decode_dev": ([vp, i, vp, i, vp, vp, vp], i),
         "zap_tex_cuda_palette_adjoint_dev": ([vp, i, vp, i, vp, vp, vp], i),

@@ -454,6 +454,70 @@ int zap_tex_cuda_bc_encode_u8_dev(zap_tex_cuda_ctx *ctx, const uint8_t *src, int
     return dev_encode(ctx, fmt, s8, nullptr, w, h, out, (cudaStream_t)stream);
 }
 
+// ---------------------------------------------------------------- split / merge (zap_tex.h:1549-1571)
+static int regroup_args(const void *in, size_t n, int fmt, const void *out) {
+    if (!valid_fmt_bc(fmt)) return fail(ZTC_ERR_UNSUPPORTED, "format %d (split / merge take BC1..BC7)", fmt);
+    if (n && (!in || !out)) return fail(ZTC_ERR_INVALID_ARG, "null pointer");
+    const uint8_t *a = (const uint8_t *)in, *b = (const uint8_t *)out;
+    if (n && a < b + n && b < a + n) return fail(ZTC_ERR_INVALID_ARG, "input and output overlap");
+    return ZTC_OK;
+}
+
+static int host_regroup(zap_tex_cuda_ctx *ctx, const void *in, size_t n, int fmt, void *out, int to_planes) {
+    int st = regroup_args(in, n, fmt, out);
+    if (st || !n) return st;
+    if ((st = resolve(ctx))) return st;
+    if ((st = grow((void **)&ctx->d_in, &ctx->d_in_cap, n, "cudaMalloc(input)"))) return st;
+    if ((st = grow((void **)&ctx->d_out, &ctx->d_out_cap, n, "cudaMalloc(output)"))) return st;
+    cudaStream_t s = ctx->stream[0];
+    ZTC_CHECK(cudaMemcpyAsync(ctx->d_in, in, n, cudaMemcpyHostToDevice, s), "host->device copy");
+    ZTC_CHECK(ztc_launch_bc_regroup(ctx->d_in, ctx->d_out, n, fmt, to_planes, s), "split / merge launch");
+    ZTC_CHECK(cudaMemcpyAsync(out, ctx->d_out, n, cudaMemcpyDeviceToHost, s), "device->host copy");
+    ZTC_CHECK(cudaStreamSynchronize(s), "split / merge");
+    return ZTC_OK;
+}
+
+static int dev_regroup(zap_tex_cuda_ctx *ctx, const void *in, size_t n, int fmt, void *out, int to_planes, void *stream) {
+    int st = regroup_args(in, n, fmt, out);
+    if (st || !n) return st;
+    if ((st = resolve(ctx))) return st;
+    ZTC_CHECK(ztc_launch_bc_regroup((const uint8_t *)in, (uint8_t *)out, n, fmt, to_planes, (cudaStream_t)stream), "split / merge launch");
+    return ZTC_OK;
+}
+
+int zap_tex_cuda_bc_split(zap_tex_cuda_ctx *ctx, const void *bc, size_t n, int fmt, void *out) { return host_regroup(ctx, bc, n, fmt, out, 1); }
+int zap_tex_cuda_bc_merge(zap_tex_cuda_ctx *ctx, const void *planes, size_t n, int fmt, void *out) {
+    return host_regroup(ctx, planes, n, fmt, out, 0);
+}
+int zap_tex_cuda_bc_split_dev(zap_tex_cuda_ctx *ctx, const void *bc, size_t n, int fmt, void *out, void *stream) {
+    return dev_regroup(ctx, bc, n, fmt, out, 1, stream);
+}
+int zap_tex_cuda_bc_merge_dev(zap_tex_cuda_ctx *ctx, const void *planes, size_t n, int fmt, void *out, void *stream) {
+    return dev_regroup(ctx, planes, n, fmt, out, 0, stream);
+}
+
+int zap_tex_cuda_bc_encode_split_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, void *out,
+                                     void *stream) {
+    int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
+    if (st) return st;
+    if (!valid_fmt_bc(fmt)) return fail(ZTC_ERR_UNSUPPORTED, "format %d (the split form exists for BC1..BC7)", fmt);
+    if ((st = resolve(ctx))) return st;
+    const ztc::SrcU8 s8{rgba, stride, w, h, 4, (((uintptr_t)rgba | stride) & 15u) == 0};
+    const int bw = (w + 3) / 4, bh = (h + 3) / 4;
+    const ztc::BlockOut planes{(uint8_t *)out, (size_t)bw * (size_t)bh, fmt, 1};
+    cudaStream_t s = (cudaStream_t)stream;
+    if (fmt != ZTC_BC7) {
+        ZTC_CHECK(ztc_launch_bcn_to(fmt, s8, 0, bh, planes, 0, s), "kernel launch");
+        return ZTC_OK;
+    }
+    void *scratch = nullptr;
+    ZTC_CHECK(cudaMallocAsync(&scratch, ztc::bc7_scratch_bytes((size_t)bw * bh), s), "cudaMallocAsync(scratch)");
+    cudaError_t e = ztc_launch_bc7_to(s8, 0, bh, planes, 0, scratch, s);
+    cudaFreeAsync(scratch, s);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    return ZTC_OK;
+}
+
 int zap_tex_cuda_bc6h_encode_dev(zap_tex_cuda_ctx *ctx, const float *rgba, int w, int h, size_t stride, void *out, void *stream) {
     int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
     if (st) return st;

@@ -176,7 +176,7 @@ ZTC_DEV int mode6_encode(const uint32_t t[16], TexRef ts, uint4 &blk) {  // zap_
     return err;
 }
 
-__global__ void __launch_bounds__(128, ZTC_MINB_BC7_MODE6) bc7_mode6_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out,
+__global__ void __launch_bounds__(128, ZTC_MINB_BC7_MODE6) bc7_mode6_kernel(SrcU8 src, int bw, int by0, int nblocks, BlockOut out, size_t b0,
                                                         uint32_t *__restrict__ count, uint2 *__restrict__ items) {
     __shared__ uint32_t s_tex[16][128];  // column threadIdx.x: this thread's block (read only by this thread)
     int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(128, ZTC_MINB_BC7_MODE6) bc7_mode6_kernel(SrcU
         for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
         uint4 blk;
         err = mode6_encode(t, TexRef{&s_tex[0][threadIdx.x], 128}, blk);
-        store_block16(out + (size_t)b * 16, blk);
+        put_block16(out, b0 + (size_t)b, blk);
     }
     bool hard = valid && err > 16 * 4;  // zap_tex.h:758 early exit
     unsigned ballot = __ballot_sync(0xFFFFFFFFu, hard);
@@ -344,7 +344,7 @@ constexpr int kMode1Tries = 4;  // partitions fully fitted after ranking (ZAP__B
 // (lane l, group mask gmask). err is the block's mode-6 SSE; lane 0 writes the block to dst when mode 5 or 1 wins.
 // Every lane holds the block's texels, so all group-level branches below are group-uniform; ts: the group's
 // shared-memory copy of them.
-__device__ __forceinline__ void bc7_group_block(const uint32_t t[16], TexRef ts, int err, uint8_t *__restrict__ dst, const int l,
+__device__ __forceinline__ void bc7_group_block(const uint32_t t[16], TexRef ts, int err, const BlockOut &out, size_t ob, const int l,
                                                 const unsigned gmask) {
     {
         bool opaque = true;
@@ -537,7 +537,7 @@ __device__ __forceinline__ void bc7_group_block(const uint32_t t[16], TexRef ts,
                 take5 = true;  // a block to write
             }
         }
-        if (take5 && l == 0) store_block16(dst, blk);
+        if (take5 && l == 0) put_block16(out, ob, blk);
     }
 }
 
@@ -551,7 +551,7 @@ __device__ __forceinline__ TexRef stage_group_texels(uint32_t *gtex, const uint3
     return TexRef{gtex, 1};
 }
 
-__global__ void __launch_bounds__(128, ZTC_MINB_BC7_HARD) bc7_hard_kernel(SrcU8 src, int bw, int by0, uint8_t *__restrict__ out,
+__global__ void __launch_bounds__(128, ZTC_MINB_BC7_HARD) bc7_hard_kernel(SrcU8 src, int bw, int by0, BlockOut out, size_t b0,
                                                        const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
     __shared__ uint32_t s_gtex[128 / kBc7Group][17];  // per group (padded: the four groups of a warp hit distinct banks)
     const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
@@ -564,7 +564,7 @@ __global__ void __launch_bounds__(128, ZTC_MINB_BC7_HARD) bc7_hard_kernel(SrcU8 
         const int b = (int)item.x;
         uint32_t t[16];
         gather_block(src, b % bw, by0 + b / bw, t);
-        bc7_group_block(t, stage_group_texels(gtex, t, l, gmask), (int)item.y, out + (size_t)b * 16, l, gmask);
+        bc7_group_block(t, stage_group_texels(gtex, t, l, gmask), (int)item.y, out, b0 + (size_t)b, l, gmask);
     }
 }
 
@@ -634,7 +634,7 @@ batch_bc7_hard_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__r
         const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
         uint32_t t[16];
         gather_block(src, b % L.bw, b / L.bw, t);
-        bc7_group_block(t, stage_group_texels(gtex, t, l, gmask), (int)item.y, L.dst + (size_t)b * 16, l, gmask);
+        bc7_group_block(t, stage_group_texels(gtex, t, l, gmask), (int)item.y, BlockOut{L.dst, 0, 4, 0}, (size_t)b, l, gmask);
     }
 }
 
@@ -670,7 +670,8 @@ const void *ztc_batch_bc7_hard_kernel_fn() { return (const void *)ztc::batch_bc7
 
 size_t ztc::bc7_scratch_bytes(size_t nblocks) { return 256 + nblocks * sizeof(uint2); }
 
-cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, void *scratch, cudaStream_t stream) {
+cudaError_t ztc_launch_bc7_to(const ztc::SrcU8 &src, int by0, int nby, const ztc::BlockOut &out, size_t b0, void *scratch,
+                              cudaStream_t stream) {
     int bw = (src.w + 3) / 4, nblocks = bw * nby;
     if (nblocks <= 0) return cudaSuccess;
     uint32_t *count = (uint32_t *)scratch;
@@ -680,7 +681,7 @@ cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out
     {
         ztc::TraceScope tr("bc7_mode6", stream);
         ztc::trace_units(nblocks);
-        ztc::bc7_mode6_kernel<<<(nblocks + 127) / 128, 128, 0, stream>>>(src, bw, by0, nblocks, out, count, items);
+        ztc::bc7_mode6_kernel<<<(nblocks + 127) / 128, 128, 0, stream>>>(src, bw, by0, nblocks, out, b0, count, items);
     }
     int groups_per_cta = 128 / ztc::kBc7Group;
     int ctas = (nblocks + groups_per_cta - 1) / groups_per_cta;
@@ -690,8 +691,12 @@ cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out
     ctas = ctas < sms * 8 ? ctas : sms * 8;
     ztc::TraceScope tr("bc7_modes51", stream);
     ztc::trace_units_dev(count, stream);
-    ztc::bc7_hard_kernel<<<ctas, 128, 0, stream>>>(src, bw, by0, out, count, items);
+    ztc::bc7_hard_kernel<<<ctas, 128, 0, stream>>>(src, bw, by0, out, b0, count, items);
     return cudaGetLastError();
+}
+
+cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, void *scratch, cudaStream_t stream) {
+    return ztc_launch_bc7_to(src, by0, nby, ztc::BlockOut{out, 0, ZTC_FMT_BC7, 0}, 0, scratch, stream);
 }
 
 // ---------------------------------------------------------------- allocation-free BC7 entry point
@@ -742,14 +747,15 @@ extern "C" __attribute__((visibility("default"))) int zap_tex_cuda_bc7_encode_no
     uint32_t *count = (uint32_t *)scratch;
     uint2 *items = (uint2 *)((uint8_t *)scratch + 256);
     const int nblocks = (int)(bw * bh);
+    const ztc::BlockOut blocks{(uint8_t *)out, 0, ZTC_FMT_BC7, 0};
     cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), s);  // the list must start empty on every call
     if (e == cudaSuccess) {
-        ztc::bc7_mode6_kernel<<<(nblocks + 127) / 128, 128, 0, s>>>(src, (int)bw, 0, nblocks, (uint8_t *)out, count, items);
+        ztc::bc7_mode6_kernel<<<(nblocks + 127) / 128, 128, 0, s>>>(src, (int)bw, 0, nblocks, blocks, 0, count, items);
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         int ctas = (nblocks + 15) / 16;
         ctas = ctas < sms * 8 ? ctas : sms * 8;
-        ztc::bc7_hard_kernel<<<ctas, 128, 0, s>>>(src, (int)bw, 0, (uint8_t *)out, count, items);
+        ztc::bc7_hard_kernel<<<ctas, 128, 0, s>>>(src, (int)bw, 0, blocks, 0, count, items);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) { cudaGetLastError(); return ztc_set_error(-3, cudaGetErrorString(e)); }

@@ -192,28 +192,29 @@ ZTC_DEV uint2 bc4_encode(const uint32_t t[16], int c) {
 
 // ---------------------------------------------------------------- kernel: one thread per block
 template <int FMT>
-__global__ void __launch_bounds__(128, ZTC_MINB_BCN) bcn_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out) {
+__global__ void __launch_bounds__(128, ZTC_MINB_BCN) bcn_kernel(SrcU8 src, int bw, int by0, int nblocks, BlockOut out, size_t b0) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nblocks) return;
     int bx = b % bw, by = by0 + b / bw;
     uint32_t t[16];
     gather_block(src, bx, by, t);
+    const size_t ob = b0 + (size_t)b;  // the block's index in the output
     if (FMT == ZTC_FMT_BC1) {
-        store_block8(out + (size_t)b * 8, bc1_encode(t));
+        put_block8(out, ob, bc1_encode(t));
     } else if (FMT == ZTC_FMT_BC4) {
-        store_block8(out + (size_t)b * 8, bc4_encode(t, 0));
+        put_block8(out, ob, bc4_encode(t, 0));
     } else if (FMT == ZTC_FMT_BC3) {
         uint2 a = bc4_encode(t, 3), c = bc1_encode(t);
-        store_block16(out + (size_t)b * 16, make_uint4(a.x, a.y, c.x, c.y));
+        put_block16(out, ob, make_uint4(a.x, a.y, c.x, c.y));
     } else {  // BC5
         uint2 r = bc4_encode(t, 0), g = bc4_encode(t, 1);
-        store_block16(out + (size_t)b * 16, make_uint4(r.x, r.y, g.x, g.y));
+        put_block16(out, ob, make_uint4(r.x, r.y, g.x, g.y));
     }
 }
 
 }  // namespace ztc
 
-cudaError_t ztc_launch_bcn(int fmt, const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, cudaStream_t stream) {
+cudaError_t ztc_launch_bcn_to(int fmt, const ztc::SrcU8 &src, int by0, int nby, const ztc::BlockOut &out, size_t b0, cudaStream_t stream) {
     int bw = (src.w + 3) / 4, nblocks = bw * nby;
     if (nblocks <= 0) return cudaSuccess;
     dim3 block(128), grid((nblocks + 127) / 128);
@@ -221,13 +222,17 @@ cudaError_t ztc_launch_bcn(int fmt, const ztc::SrcU8 &src, int by0, int nby, uin
     ztc::TraceScope tr(fmt >= 0 && fmt < 4 ? names[fmt] : "bcn_encode", stream);
     ztc::trace_units(nblocks);
     switch (fmt) {
-    case ZTC_FMT_BC1: ztc::bcn_kernel<ZTC_FMT_BC1><<<grid, block, 0, stream>>>(src, bw, by0, nblocks, out); break;
-    case ZTC_FMT_BC3: ztc::bcn_kernel<ZTC_FMT_BC3><<<grid, block, 0, stream>>>(src, bw, by0, nblocks, out); break;
-    case ZTC_FMT_BC4: ztc::bcn_kernel<ZTC_FMT_BC4><<<grid, block, 0, stream>>>(src, bw, by0, nblocks, out); break;
-    case ZTC_FMT_BC5: ztc::bcn_kernel<ZTC_FMT_BC5><<<grid, block, 0, stream>>>(src, bw, by0, nblocks, out); break;
+    case ZTC_FMT_BC1: ztc::bcn_kernel<ZTC_FMT_BC1><<<grid, block, 0, stream>>>(src, bw, by0, nblocks, out, b0); break;
+    case ZTC_FMT_BC3: ztc::bcn_kernel<ZTC_FMT_BC3><<<grid, block, 0, stream>>>(src, bw, by0, nblocks, out, b0); break;
+    case ZTC_FMT_BC4: ztc::bcn_kernel<ZTC_FMT_BC4><<<grid, block, 0, stream>>>(src, bw, by0, nblocks, out, b0); break;
+    case ZTC_FMT_BC5: ztc::bcn_kernel<ZTC_FMT_BC5><<<grid, block, 0, stream>>>(src, bw, by0, nblocks, out, b0); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+cudaError_t ztc_launch_bcn(int fmt, const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, cudaStream_t stream) {
+    return ztc_launch_bcn_to(fmt, src, by0, nby, ztc::BlockOut{out, 0, fmt, 0}, 0, stream);
 }
 
 // ---------------------------------------------------------------- batched: one persistent launch over a tile queue

@@ -165,4 +165,52 @@ struct TexRef {
 ZTC_DEV void store_block8(uint8_t *out, uint2 v) { *(uint2 *)out = v; }
 ZTC_DEV void store_block16(uint8_t *out, uint4 v) { *(uint4 *)out = v; }
 
+// ---------------------------------------------------------------- block fields (zap_tex.h:1549-1571)
+// The split form of an encoded image: plane k holds field k of every block, the planes one after another.
+// Fields, in block order: BC1 {4, 4} (endpoints, indices), BC3 {2, 6, 4, 4}, BC4 {2, 6}, BC5 {2, 6, 2, 6},
+// BC7 {8, 1, 7}.
+ZTC_DEV int bc_fields(int fmt, int sz[4]) {
+    sz[0] = sz[1] = sz[2] = sz[3] = 0;
+    switch (fmt) {
+    case 0: sz[0] = 4; sz[1] = 4; return 2;
+    case 1: sz[0] = 2; sz[1] = 6; sz[2] = 4; sz[3] = 4; return 4;
+    case 2: sz[0] = 2; sz[1] = 6; return 2;
+    case 3: sz[0] = 2; sz[1] = 6; sz[2] = 2; sz[3] = 6; return 4;
+    case 4: sz[0] = 8; sz[1] = 1; sz[2] = 7; return 3;
+    default: return 0;
+    }
+}
+
+// Where an encoder puts block b: raster block order (base + b * block bytes), or, with split set, the field planes
+// of an image of nblocks blocks (field k of block b at base + nblocks * (offset of field k) + b * (size of field k)),
+// so a caller who stores or compresses the split form gets it without a second pass over the blocks.
+struct BlockOut {
+    uint8_t *base;
+    size_t nblocks;
+    int fmt, split;
+};
+ZTC_DEV void put_block(const BlockOut &o, size_t b, const uint32_t w[4], int bytes) {
+    if (!o.split) {
+        if (bytes == 8) store_block8(o.base + b * 8, make_uint2(w[0], w[1]));
+        else store_block16(o.base + b * 16, make_uint4(w[0], w[1], w[2], w[3]));
+        return;
+    }
+    int sz[4];
+    const int nf = bc_fields(o.fmt, sz);
+    int off = 0;
+    #pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (k >= nf) break;
+        uint8_t *dst = o.base + o.nblocks * (size_t)off + b * (size_t)sz[k];
+        for (int j = 0; j < sz[k]; j++) {
+            const int i = off + j;  // byte i of the block (selects, not an indexed load: w stays in registers)
+            const uint32_t x = i < 4 ? w[0] : i < 8 ? w[1] : i < 12 ? w[2] : w[3];
+            dst[j] = (uint8_t)(x >> (8 * (i & 3)));
+        }
+        off += sz[k];
+    }
+}
+ZTC_DEV void put_block8(const BlockOut &o, size_t b, uint2 v) { const uint32_t w[4] = {v.x, v.y, 0u, 0u}; put_block(o, b, w, 8); }
+ZTC_DEV void put_block16(const BlockOut &o, size_t b, uint4 v) { const uint32_t w[4] = {v.x, v.y, v.z, v.w}; put_block(o, b, w, 16); }
+
 }  // namespace ztc

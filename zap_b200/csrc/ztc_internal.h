@@ -88,6 +88,13 @@ int ztc_ctx_activate(zap_tex_cuda_ctx *ctx);
 
 cudaError_t ztc_launch_bcn(int fmt, const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, cudaStream_t stream);
 cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, void *scratch, cudaStream_t stream);
+// the same encoders into a BlockOut (raster blocks or split field planes); b0: output index of the first block
+namespace ztc { struct BlockOut; }
+cudaError_t ztc_launch_bcn_to(int fmt, const ztc::SrcU8 &src, int by0, int nby, const ztc::BlockOut &out, size_t b0, cudaStream_t stream);
+cudaError_t ztc_launch_bc7_to(const ztc::SrcU8 &src, int by0, int nby, const ztc::BlockOut &out, size_t b0, void *scratch,
+                              cudaStream_t stream);
+// split (to_planes = 1) or merge n bytes of BC1..BC7 data, device to device (zap_tex.h:1549-1571)
+cudaError_t ztc_launch_bc_regroup(const uint8_t *in, uint8_t *out, size_t n, int fmt, int to_planes, cudaStream_t stream);
 cudaError_t ztc_launch_bc6h(const ztc::SrcHdr &src, int by0, int nby, uint8_t *out, cudaStream_t stream);
 cudaError_t ztc_launch_astc(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, void *scratch, cudaStream_t stream);
 cudaError_t ztc_launch_mip(const uint8_t *src, int w, int h, size_t stride, int srgb, uint8_t *dst, size_t dst_stride,
