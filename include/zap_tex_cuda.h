@@ -119,6 +119,15 @@ ZTC_API int zap_tex_cuda_bc_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, in
                                        void *stream);
 ZTC_API int zap_tex_cuda_bc6h_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint16_t *rgba, size_t stride,
                                          void *stream);
+/* replaces zap_astc_decode (zap_tex.h:1344-1356): void-extent blocks and the block modes the reference decodes
+   (4x4 weight grid, power-of-two weight range, 1-2 partitions of CEM 8 / 12); any other block decodes to magenta */
+ZTC_API int zap_tex_cuda_astc_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint8_t *rgba, size_t stride,
+                                         void *stream);
+/* the same three decoders with host memory, synchronous (zap_tex.h:1526, :963, :1344); block pointers of the _dev
+   variants must be aligned to the block size (8 bytes for BC1 / BC4, else 16), ZTC_ERR_INVALID_ARG otherwise */
+ZTC_API int zap_tex_cuda_bc_decode(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, int fmt, uint8_t *rgba, size_t stride);
+ZTC_API int zap_tex_cuda_bc6h_decode(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint16_t *rgba, size_t stride);
+ZTC_API int zap_tex_cuda_astc_decode(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint8_t *rgba, size_t stride);
 
 /* ---------------------------------------------------------------- split / merge (zap_tex.h:1549-1571)
    Plane k of the split form holds field k of every block, the planes one after another: BC1 {4, 4}, BC3

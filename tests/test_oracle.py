@@ -196,3 +196,23 @@ def test_split_merge_match_reference_live(oracle, reference):
             x = rng.integers(0, 256, n, dtype=np.uint8)
             assert np.array_equal(oracle.bc_split(x, fmt), reference.bc_split(x, fmt)), (fmt, n)
             assert np.array_equal(oracle.bc_merge(x, fmt), reference.bc_merge(x, fmt)), (fmt, n)
+
+
+def _astc_block_mix(rng, n):
+    """Random 16-byte ASTC blocks with void-extent blocks and the reference encoder's own mode words mixed in."""
+    blocks = rng.integers(0, 256, (n, 16), dtype=np.uint8)
+    blocks[::7, 0] = 0xFC  # void extent: low 9 mode bits 0x1FC
+    blocks[::7, 1] = (blocks[::7, 1] & 0xFE) | 0x01
+    modes = [0x242, 0x443, 0x642, 0x253, 0x653, 0x243]  # 4x4 grids of several weight ranges, as the encoder writes them
+    for k, m in enumerate(modes):
+        rows = blocks[3 + k::11]
+        rows[:, 0] = m & 0xFF
+        rows[:, 1] = (rows[:, 1] & 0xF8) | (m >> 8)
+    return blocks
+
+
+def test_astc_decode_matches_reference_live(oracle, reference):
+    """The port's decoder on arbitrary blocks (void extent, supported modes, everything it must reject)."""
+    rng = np.random.default_rng(14)
+    bc = _astc_block_mix(rng, 24 * 20).reshape(-1)
+    assert np.array_equal(oracle.astc_decode(bc, 95, 77), reference.astc_decode(bc, 95, 77))

@@ -240,6 +240,38 @@ def bc6h_decode_dev(bc, w, h, stream=None, ctx=None):
     return out
 
 
+def astc_decode_dev(bc, w, h, stream=None, ctx=None):
+    """Device zap_astc_decode: uint8 CUDA tensor of ASTC 4x4 blocks -> HxWx4 uint8 CUDA tensor."""
+    import torch
+    out = torch.empty((h, w, 4), dtype=torch.uint8, device=bc.device)
+    check(load().zap_tex_cuda_astc_decode_dev(ctx, bc.data_ptr(), w, h, out.data_ptr(), w * 4, _stream(stream)), "astc_decode_dev")
+    return out
+
+
+def bc_decode(bc, w, h, fmt, ctx=None):
+    """zap_bc_decode (zap_tex.h:1526) through the device: numpy blocks -> HxWx4 uint8 numpy array."""
+    bc = np.ascontiguousarray(bc, dtype=np.uint8)
+    out = np.empty((h, w, 4), np.uint8)
+    check(load().zap_tex_cuda_bc_decode(ctx, bc.ctypes.data, w, h, fmt, out.ctypes.data, w * 4), "bc_decode")
+    return out
+
+
+def bc6h_decode(bc, w, h, ctx=None):
+    """zap_bc6h_decode (zap_tex.h:963) through the device: numpy blocks -> HxWx4 uint16 half bits (alpha 0x3C00)."""
+    bc = np.ascontiguousarray(bc, dtype=np.uint8)
+    out = np.empty((h, w, 4), np.uint16)
+    check(load().zap_tex_cuda_bc6h_decode(ctx, bc.ctypes.data, w, h, out.ctypes.data, w * 4), "bc6h_decode")
+    return out
+
+
+def astc_decode(bc, w, h, ctx=None):
+    """zap_astc_decode (zap_tex.h:1344) through the device: numpy blocks -> HxWx4 uint8 numpy array."""
+    bc = np.ascontiguousarray(bc, dtype=np.uint8)
+    out = np.empty((h, w, 4), np.uint8)
+    check(load().zap_tex_cuda_astc_decode(ctx, bc.ctypes.data, w, h, out.ctypes.data, w * 4), "astc_decode")
+    return out
+
+
 def block_endpoints_dev(blocks, fmt, stream=None, ctx=None):
     """Stored endpoints of BC1 / BC7-mode-6 blocks, expanded to 8-bit units: float32 [nblocks, 2, 4]."""
     import torch

@@ -66,6 +66,10 @@ def _declare(lib):
         "zap_tex_cuda_bc7_encode_noalloc_dev": ([vp, i, i, sz, vp, vp], i),
         "zap_tex_cuda_bc_decode_dev": ([vp, vp, i, i, i, vp, sz, vp], i),
         "zap_tex_cuda_bc6h_decode_dev": ([vp, vp, i, i, vp, sz, vp], i),
+        "zap_tex_cuda_astc_decode_dev": ([vp, vp, i, i, vp, sz, vp], i),
+        "zap_tex_cuda_bc_decode": ([vp, vp, i, i, i, vp, sz], i),
+        "zap_tex_cuda_bc6h_decode": ([vp, vp, i, i, vp, sz], i),
+        "zap_tex_cuda_astc_decode": ([vp, vp, i, i, vp, sz], i),
         "zap_tex_cuda_bc_split": ([vp, vp, sz, i, vp], i),
         "zap_tex_cuda_bc_merge": ([vp, vp, sz, i, vp], i),
         "zap_tex_cuda_bc_split_dev": ([vp, vp, sz, i, vp, vp], i),

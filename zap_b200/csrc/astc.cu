@@ -16,12 +16,18 @@
 
 namespace ztc {
 
-// ---------------------------------------------------------------- tables (host-built, ASTC spec rules)
+// ---------------------------------------------------------------- ASTC spec rules (host and device)
 struct IseRange { int levels, trit, quint, bits; };
-static const IseRange kIse[21] = {  // integer-sequence ranges (ASTC spec)
-    {2, 0, 0, 1}, {3, 1, 0, 0}, {4, 0, 0, 2}, {5, 0, 1, 0}, {6, 1, 0, 1}, {8, 0, 0, 3}, {10, 0, 1, 1},
-    {12, 1, 0, 2}, {16, 0, 0, 4}, {20, 0, 1, 2}, {24, 1, 0, 3}, {32, 0, 0, 5}, {40, 0, 1, 3}, {48, 1, 0, 4},
-    {64, 0, 0, 6}, {80, 0, 1, 4}, {96, 1, 0, 5}, {128, 0, 0, 7}, {160, 0, 1, 5}, {192, 1, 0, 6}, {256, 0, 0, 8}};
+// integer-sequence range i of the ASTC spec's 21 (2, 3, 4, 5, 6, 8, 10, 12, 16, 20, ..., 192, 256 levels): after
+// the first two the ranges repeat (2^(k+2) values, 5 * 2^k with a quint, 3 * 2^(k+1) with a trit), k = 0, 1, ...
+ZTC_DEV IseRange ise_range(int i) {
+    if (i == 0) return {2, 0, 0, 1};
+    if (i == 1) return {3, 1, 0, 0};
+    const int m = (i - 2) % 3, k = (i - 2) / 3;
+    if (m == 0) return {1 << (k + 2), 0, 0, k + 2};
+    if (m == 1) return {5 << k, 0, 1, k};
+    return {3 << (k + 1), 1, 0, k + 1};
+}
 
 struct AstcCfg { int cem, wb, parts, nv, trit, quint, bits; };
 struct AstcTables {
@@ -35,18 +41,19 @@ struct AstcTables {
 };
 __constant__ AstcTables kAstc;
 
-static int ise_bits_h(const IseRange &r, int n) { return n * r.bits + (r.trit ? (8 * n + 4) / 5 : r.quint ? (7 * n + 2) / 3 : 0); }
-static int colour_range_h(int nvals, int avail) {
-    for (int i = 20; i >= 4; i--) if (ise_bits_h(kIse[i], nvals) <= avail) return i;
+ZTC_DEV int ise_bits(const IseRange &r, int n) { return n * r.bits + (r.trit ? (8 * n + 4) / 5 : r.quint ? (7 * n + 2) / 3 : 0); }
+// the largest range with at least 6 levels whose nvals values fit in avail bits (zap_tex.h:996-999)
+ZTC_DEV int colour_range(int nvals, int avail) {
+    for (int i = 20; i >= 4; i--) if (ise_bits(ise_range(i), nvals) <= avail) return i;
     return -1;
 }
-static int replicate_h(int v, int n, int to) {
+ZTC_DEV int replicate(int v, int n, int to) {
     int x = 0;
     for (int sh = to - n; sh > -n; sh -= n) x |= sh >= 0 ? v << sh : v >> -sh;
     return x & ((1 << to) - 1);
 }
-static int colour_unquant_h(const IseRange &r, int v) {  // ASTC spec colour unquantisation
-    if (!r.trit && !r.quint) return replicate_h(v, r.bits, 8);
+ZTC_DEV int colour_unquant(const IseRange &r, int v) {  // ASTC spec colour unquantisation
+    if (!r.trit && !r.quint) return replicate(v, r.bits, 8);
     int n = r.bits, m = v & ((1 << n) - 1), D = v >> n;
     int a = m & 1, b = (m >> 1) & 1, c = (m >> 2) & 1, d = (m >> 3) & 1, e = (m >> 4) & 1, f = (m >> 5) & 1;
     int A = a ? 0x1FF : 0, B = 0, C = 0;
@@ -66,7 +73,7 @@ static int colour_unquant_h(const IseRange &r, int v) {  // ASTC spec colour unq
     int T = (D * C + B) ^ A;
     return (A & 0x80) | (T >> 2);
 }
-static void trits_h(int T, int t[5]) {  // ASTC spec: 8 bits -> 5 trits
+ZTC_DEV void trit_unpack(int T, int t[5]) {  // ASTC spec: 8 bits -> 5 trits
     int C;
     if (((T >> 2) & 7) == 7) { C = (((T >> 5) & 7) << 2) | (T & 3); t[4] = 2; t[3] = 2; }
     else {
@@ -78,7 +85,7 @@ static void trits_h(int T, int t[5]) {  // ASTC spec: 8 bits -> 5 trits
     else if (((C >> 2) & 3) == 3) { t[2] = 2; t[1] = 2; t[0] = C & 3; }
     else { t[2] = (C >> 4) & 1; t[1] = (C >> 2) & 3; t[0] = (((C >> 1) & 1) << 1) | ((C & 1) & ~(C >> 1) & 1); }
 }
-static void quints_h(int Q, int q[3]) {  // ASTC spec: 7 bits -> 3 quints
+ZTC_DEV void quint_unpack(int Q, int q[3]) {  // ASTC spec: 7 bits -> 3 quints
     if (((Q >> 1) & 3) == 3 && ((Q >> 5) & 3) == 0) {
         q[2] = ((Q & 1) << 2) | ((((Q >> 4) & 1) & ~Q & 1) << 1) | (((Q >> 3) & 1) & ~Q & 1);
         q[1] = 4; q[0] = 4;
@@ -90,15 +97,15 @@ static void quints_h(int Q, int q[3]) {  // ASTC spec: 7 bits -> 3 quints
     if ((C & 7) == 5) { q[1] = 4; q[0] = (C >> 3) & 3; }
     else { q[1] = (C >> 3) & 3; q[0] = C & 7; }
 }
-static uint32_t hash52_h(uint32_t p) {  // ASTC spec partition hash
+ZTC_DEV uint32_t hash52(uint32_t p) {  // ASTC spec partition hash
     p ^= p >> 15; p -= p << 17; p += p << 7; p += p << 4; p ^= p >> 5;
     p += p << 16; p ^= p >> 7; p ^= p >> 3; p ^= p << 6; p ^= p >> 17;
     return p;
 }
-static int partition_h(int seed, int x, int y, int count) {  // ASTC spec partition selection, small block
+ZTC_DEV int astc_partition(int seed, int x, int y, int count) {  // ASTC spec partition selection, small block
     x <<= 1; y <<= 1;
     seed += (count - 1) * 1024;
-    uint32_t h = hash52_h((uint32_t)seed);
+    uint32_t h = hash52((uint32_t)seed);
     int s[8];
     for (int i = 0; i < 8; i++) { s[i] = (int)((h >> (4 * i)) & 15); s[i] *= s[i]; }
     int sh1, sh2;
@@ -128,26 +135,26 @@ static void build_tables(AstcTables &T) {
     for (int k = 0; k < 8; k++) {
         AstcCfg &c = T.cfg[k];
         c.cem = CFG[k][0]; c.wb = CFG[k][1]; c.parts = CFG[k][2]; c.nv = c.cem == 8 ? 6 : 8;
-        int ri = colour_range_h(c.nv * c.parts, 128 - (c.parts == 1 ? 17 : 29) - 16 * c.wb);
-        const IseRange &r = kIse[ri];
+        int ri = colour_range(c.nv * c.parts, 128 - (c.parts == 1 ? 17 : 29) - 16 * c.wb);
+        const IseRange r = ise_range(ri);
         c.trit = r.trit; c.quint = r.quint; c.bits = r.bits;
-        for (int v = 0; v < 256; v++) T.uq[k][v] = v < r.levels ? (uint8_t)colour_unquant_h(r, v) : 0;
+        for (int v = 0; v < 256; v++) T.uq[k][v] = v < r.levels ? (uint8_t)colour_unquant(r, v) : 0;
         for (int x = 0; x < 256; x++) {
             int best = 0, bd = 1 << 30;
             for (int v = 0; v < r.levels; v++) {
-                int d = colour_unquant_h(r, v) - x;
+                int d = colour_unquant(r, v) - x;
                 d = d < 0 ? -d : d;
                 if (d < bd) { bd = d; best = v; }
             }
             T.q[k][x] = (uint8_t)best;
         }
     }
-    for (int t = 255; t >= 0; t--) { int v[5]; trits_h(t, v); T.trit_code[v[0] + 3 * v[1] + 9 * v[2] + 27 * v[3] + 81 * v[4]] = (uint8_t)t; }
-    for (int q = 127; q >= 0; q--) { int v[3]; quints_h(q, v); T.quint_code[v[0] + 5 * v[1] + 25 * v[2]] = (uint8_t)q; }
+    for (int t = 255; t >= 0; t--) { int v[5]; trit_unpack(t, v); T.trit_code[v[0] + 3 * v[1] + 9 * v[2] + 27 * v[3] + 81 * v[4]] = (uint8_t)t; }
+    for (int q = 127; q >= 0; q--) { int v[3]; quint_unpack(q, v); T.quint_code[v[0] + 5 * v[1] + 25 * v[2]] = (uint8_t)q; }
     T.pat_count = 0;
     for (int sd = 0; sd < 1024; sd++) {
         unsigned m = 0;
-        for (int i = 0; i < 16; i++) m |= (unsigned)partition_h(sd, i & 3, i >> 2, 2) << i;
+        for (int i = 0; i < 16; i++) m |= (unsigned)astc_partition(sd, i & 3, i >> 2, 2) << i;
         if (m && m != 0xFFFFu) { T.pat_mask[T.pat_count] = (uint16_t)m; T.pat_seed[T.pat_count++] = (uint16_t)sd; }
     }
 }
@@ -565,7 +572,112 @@ __global__ void __launch_bounds__(128) astc_two_part_kernel(SrcU8 src, int bw, i
     }
 }
 
+// ---------------------------------------------------------------- decoder (zap_tex.h:1135-1168, :1344-1356)
+// The blocks the reference decodes: void-extent blocks, and 4x4 weight grids with a power-of-two weight range and
+// one or two partitions sharing CEM 8 or 12. Any other block decodes to magenta (255, 0, 255, 255), as there.
+ZTC_DEV uint32_t take_bits(const uint32_t w[4], int &pos, int n) {  // LSB-first, n <= 16 (zap__bits)
+    const uint32_t v = n ? get_bits128(w, pos, n) : 0u;
+    pos += n;
+    return v;
+}
+ZTC_DEV uint32_t bit_at(const uint32_t w[4], int p) {
+    const uint32_t x = p < 32 ? w[0] : p < 64 ? w[1] : p < 96 ? w[2] : w[3];
+    return (x >> (p & 31)) & 1u;
+}
+ZTC_DEV void astc_decode_block(const uint32_t w[4], uint32_t px[16]) {
+    #pragma unroll
+    for (int i = 0; i < 16; i++) px[i] = 0xFFFF00FFu;  // magenta
+    int pos = 0;
+    const int mode = (int)take_bits(w, pos, 11);
+    if ((mode & 0x1FF) == 0x1FC) {  // void extent: one colour, 16-bit UNORM RGBA at bits 64..127
+        uint32_t c = 0;
+        #pragma unroll
+        for (int k = 0; k < 4; k++) c |= (get_bits128(w, 64 + 16 * k, 16) >> 8) << (8 * k);
+        #pragma unroll
+        for (int i = 0; i < 16; i++) px[i] = c;
+        return;
+    }
+    const int R = ((mode & 1) << 1) | (((mode >> 1) & 1) << 2) | ((mode >> 4) & 1), H = (mode >> 9) & 1;
+    if (!(mode & 3) || ((mode >> 2) & 3) || ((mode >> 5) & 3) != 2 || ((mode >> 7) & 3) || ((mode >> 10) & 1)) return;
+    // weight levels (R, H): {-, -, 2, 3, 4, 5, 6, 8} and {-, -, 10, 12, 16, 20, 24, 32}; only powers of two decode
+    const int wb = !H ? (R == 2 ? 1 : R == 4 ? 2 : R == 7 ? 3 : 0) : (R == 4 ? 4 : R == 7 ? 5 : 0);
+    const int parts = (int)take_bits(w, pos, 2) + 1;
+    if (!wb || parts > 2) return;
+    int seed = 0, cem;
+    if (parts == 2) {
+        seed = (int)take_bits(w, pos, 10);
+        const int cf = (int)take_bits(w, pos, 6);
+        if (cf & 3) return;  // both partitions must use the same endpoint mode
+        cem = cf >> 2;
+    } else {
+        cem = (int)take_bits(w, pos, 4);
+    }
+    const int nv = cem == 8 ? 6 : cem == 12 ? 8 : 0, n = nv * parts;
+    if (!nv) return;
+    const int ri = colour_range(n, 128 - pos - 16 * wb);
+    if (ri < 0) return;
+    const IseRange r = ise_range(ri);
+    int v[16];
+    const int gs = r.trit ? 5 : r.quint ? 3 : 1;
+    for (int g = 0; g < n; g += gs) {  // integer-sequence decode (zap__ise_get, zap_tex.h:1065-1078)
+        const int cnt = min(n - g, gs);
+        int m[5] = {0, 0, 0, 0, 0}, t[5] = {0, 0, 0, 0, 0}, X = 0, xp = 0;
+        for (int k = 0; k < cnt; k++) {
+            m[k] = (int)take_bits(w, pos, r.bits);
+            if (gs > 1) {
+                const int xb = r.trit ? ((k == 2 || k == 4) ? 1 : 2) : (k == 0 ? 3 : 2);  // packed-code bits after value k
+                X |= (int)take_bits(w, pos, xb) << xp;
+                xp += xb;
+            }
+        }
+        if (r.trit) trit_unpack(X, t);
+        else if (r.quint) quint_unpack(X, t);
+        for (int k = 0; k < cnt; k++) v[g + k] = colour_unquant(r, gs > 1 ? (t[k] << r.bits) | m[k] : m[k]);
+    }
+    int e0[2][4], e1[2][4];
+    for (int k = 0; k < parts; k++) endpoint_pair(cem, v + k * nv, e0[k], e1[k]);
+    #pragma unroll 1
+    for (int i = 0; i < 16; i++) {
+        const int k = parts == 2 ? astc_partition(seed, i & 3, i >> 2, 2) : 0;
+        int wt = 0;
+        for (int j = 0; j < wb; j++) wt |= (int)bit_at(w, 127 - (i * wb + j)) << j;  // weights run down from bit 127
+        wt = wunq(wt, wb);
+        const int *a = k ? e0[1] : e0[0], *b = k ? e1[1] : e1[0];
+        px[i] = pack_rgba(astc_lerp(a[0], b[0], wt), astc_lerp(a[1], b[1], wt), astc_lerp(a[2], b[2], wt), astc_lerp(a[3], b[3], wt));
+    }
+}
+
+__global__ void __launch_bounds__(128) astc_decode_kernel(const uint8_t *__restrict__ bc, int w, int h, uint8_t *__restrict__ out,
+                                                          size_t stride) {
+    const int bw = (w + 3) / 4;
+    const long nblocks = (long)bw * ((h + 3) / 4), b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblocks) return;
+    const uint4 q = __ldg((const uint4 *)(bc + (size_t)b * 16));
+    const uint32_t wd[4] = {q.x, q.y, q.z, q.w};
+    uint32_t px[16];
+    astc_decode_block(wd, px);
+    const int bx = (int)(b % bw), by = (int)(b / bw);
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const int x = bx * 4 + (i & 3), y = by * 4 + (i >> 2);
+        if (x < w && y < h) {
+            uint8_t *p = out + (size_t)y * stride + (size_t)x * 4;
+            p[0] = (uint8_t)px[i]; p[1] = (uint8_t)(px[i] >> 8); p[2] = (uint8_t)(px[i] >> 16); p[3] = (uint8_t)(px[i] >> 24);
+        }
+    }
+}
+
 }  // namespace ztc
+
+// zap_astc_decode (zap_tex.h:1344-1356) into device memory; bc must be 16-byte aligned
+cudaError_t ztc_launch_astc_decode(const uint8_t *bc, int w, int h, uint8_t *out, size_t stride, cudaStream_t stream) {
+    const long nblocks = (long)((w + 3) / 4) * ((h + 3) / 4);
+    if (nblocks <= 0) return cudaSuccess;
+    ztc::TraceScope tr("astc_decode", stream);
+    ztc::trace_units(nblocks);
+    ztc::astc_decode_kernel<<<(unsigned)((nblocks + 127) / 128), 128, 0, stream>>>(bc, w, h, out, stride);
+    return cudaGetLastError();
+}
 
 size_t ztc::astc_scratch_bytes(size_t nblocks) { return 256 + nblocks * sizeof(uint2); }
 

@@ -1,5 +1,6 @@
-// decode.cu - device block decoders: zap_bc_decode (zap_tex.h:1526-1547, BC7 all modes) and zap_bc6h_decode
-// (zap_tex.h:963-975). One thread per block; only texels inside the image are written (partial edge blocks).
+// decode.cu - device block decoders: zap_bc_decode (zap_tex.h:1526-1547, BC7 all modes), zap_bc6h_decode
+// (zap_tex.h:963-975) and zap_astc_decode (zap_tex.h:1344-1356, kernel in astc.cu), device and host memory. One
+// thread per block; only texels inside the image are written (partial edge blocks).
 // They give on-device quality checks for encoded batches without a host round trip.
 #include <string>
 
@@ -44,27 +45,92 @@ __global__ void __launch_bounds__(128) bc6h_decode_kernel(const uint8_t *__restr
 
 }  // namespace ztc
 
+namespace {
+
+enum Kind { kBcn, kBc6h, kAstc };
+
+// block bytes of the format, and the alignment the decoder's block loads need
+size_t block_bytes_of(Kind k, int fmt) { return k == kBcn && (fmt == ZTC_BC1 || fmt == ZTC_BC4) ? 8 : 16; }
+
+int check_decode(Kind k, const void *bc, int w, int h, int fmt, const void *rgba, size_t stride, size_t texel_units) {
+    if (!bc || !rgba || w < 1 || h < 1 || stride < (size_t)w * texel_units) return ztc_set_error(ZTC_ERR_INVALID_ARG, "bad decode arguments");
+    if ((long)((w + 3) / 4) * ((h + 3) / 4) >= (1L << 31)) return ztc_set_error(ZTC_ERR_INVALID_ARG, "more than 2^31 - 1 blocks");
+    if (k == kBcn && (fmt < ZTC_BC1 || fmt > ZTC_BC7)) return ztc_set_error(ZTC_ERR_UNSUPPORTED, "decode format must be BC1..BC7");
+    if ((uintptr_t)bc % block_bytes_of(k, fmt)) return ztc_set_error(ZTC_ERR_INVALID_ARG, "blocks must be aligned to the block size");
+    return ZTC_OK;
+}
+
+cudaError_t launch_decode(Kind k, const void *bc, int w, int h, int fmt, void *rgba, size_t stride, cudaStream_t s) {
+    const long nblocks = (long)((w + 3) / 4) * ((h + 3) / 4);
+    const unsigned grid = (unsigned)((nblocks + 127) / 128);
+    if (k == kAstc) return ztc_launch_astc_decode((const uint8_t *)bc, w, h, (uint8_t *)rgba, stride, s);
+    if (k == kBc6h) ztc::bc6h_decode_kernel<<<grid, 128, 0, s>>>((const uint8_t *)bc, w, h, (uint16_t *)rgba, stride);
+    else ztc::bcn_decode_kernel<<<grid, 128, 0, s>>>(fmt, (const uint8_t *)bc, w, h, (uint8_t *)rgba, stride);
+    return cudaGetLastError();
+}
+
+int dev_decode(Kind k, zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, int fmt, void *rgba, size_t stride, void *stream) {
+    int st = check_decode(k, bc, w, h, fmt, rgba, stride, 4);
+    if (st) return st;
+    if ((st = ztc_ctx_activate(ctx))) return st;
+    cudaError_t e = launch_decode(k, bc, w, h, fmt, rgba, stride, (cudaStream_t)stream);
+    if (e != cudaSuccess) { cudaGetLastError(); return ztc_set_error(ZTC_ERR_CUDA, cudaGetErrorString(e)); }
+    return ZTC_OK;
+}
+
+// host memory in and out, synchronous: blocks to a device buffer, decode, texel rows back with the caller's stride
+int host_decode(Kind k, zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, int fmt, void *rgba, size_t stride, size_t texel_bytes) {
+    // host blocks need no alignment (they are copied): the check sees a stand-in aligned address
+    int st = check_decode(k, (const void *)16, w, h, fmt, rgba, stride * (k == kBc6h ? 2 : 1), texel_bytes);
+    if (!st && !bc) st = ztc_set_error(ZTC_ERR_INVALID_ARG, "bad decode arguments");
+    if (st) return st;
+    if ((st = ztc_ctx_activate(ctx))) return st;
+    const size_t nb = (size_t)((w + 3) / 4) * ((h + 3) / 4) * block_bytes_of(k, fmt), row = (size_t)w * texel_bytes;
+    const size_t host_stride = k == kBc6h ? stride * 2 : stride;  // BC6H strides count uint16 elements
+    cudaStream_t s = cudaStreamPerThread;
+    uint8_t *d_bc = nullptr, *d_px = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&d_bc, nb, s);
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)&d_px, row * (size_t)h, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_bc, bc, nb, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = launch_decode(k, d_bc, w, h, fmt, d_px, k == kBc6h ? (size_t)w * 4 : row, s);
+    if (e == cudaSuccess) e = cudaMemcpy2DAsync(rgba, host_stride, d_px, row, row, (size_t)h, cudaMemcpyDeviceToHost, s);
+    if (d_px) cudaFreeAsync(d_px, s);
+    if (d_bc) cudaFreeAsync(d_bc, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return ztc_set_error(e == cudaErrorMemoryAllocation ? ZTC_ERR_NO_MEMORY : ZTC_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return ZTC_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int zap_tex_cuda_bc_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, int fmt, uint8_t *rgba, size_t stride, void *stream) {
-    if (!bc || !rgba || w < 1 || h < 1 || stride < (size_t)w * 4) return ztc_set_error(ZTC_ERR_INVALID_ARG, "bad decode arguments");
-    if (fmt < ZTC_BC1 || fmt > ZTC_BC7) return ztc_set_error(ZTC_ERR_UNSUPPORTED, "decode format must be BC1..BC7");
-    int st = ztc_ctx_activate(ctx);
-    if (st) return st;
-    const long nblocks = (long)((w + 3) / 4) * ((h + 3) / 4);
-    ztc::bcn_decode_kernel<<<(unsigned)((nblocks + 127) / 128), 128, 0, (cudaStream_t)stream>>>(fmt, (const uint8_t *)bc, w, h, rgba, stride);
-    cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? ZTC_OK : ztc_set_error(ZTC_ERR_CUDA, cudaGetErrorString(e));
+    return dev_decode(kBcn, ctx, bc, w, h, fmt, rgba, stride, stream);
 }
 
 int zap_tex_cuda_bc6h_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint16_t *rgba, size_t stride, void *stream) {
-    if (!bc || !rgba || w < 1 || h < 1 || stride < (size_t)w * 4) return ztc_set_error(ZTC_ERR_INVALID_ARG, "bad decode arguments");
-    int st = ztc_ctx_activate(ctx);
-    if (st) return st;
-    const long nblocks = (long)((w + 3) / 4) * ((h + 3) / 4);
-    ztc::bc6h_decode_kernel<<<(unsigned)((nblocks + 127) / 128), 128, 0, (cudaStream_t)stream>>>((const uint8_t *)bc, w, h, rgba, stride);
-    cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? ZTC_OK : ztc_set_error(ZTC_ERR_CUDA, cudaGetErrorString(e));
+    return dev_decode(kBc6h, ctx, bc, w, h, ZTC_BC6H, rgba, stride, stream);
+}
+
+int zap_tex_cuda_astc_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint8_t *rgba, size_t stride, void *stream) {
+    return dev_decode(kAstc, ctx, bc, w, h, ZTC_ASTC4X4, rgba, stride, stream);
+}
+
+int zap_tex_cuda_bc_decode(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, int fmt, uint8_t *rgba, size_t stride) {
+    return host_decode(kBcn, ctx, bc, w, h, fmt, rgba, stride, 4);
+}
+
+int zap_tex_cuda_bc6h_decode(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint16_t *rgba, size_t stride) {
+    return host_decode(kBc6h, ctx, bc, w, h, ZTC_BC6H, rgba, stride, 8);
+}
+
+int zap_tex_cuda_astc_decode(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint8_t *rgba, size_t stride) {
+    return host_decode(kAstc, ctx, bc, w, h, ZTC_ASTC4X4, rgba, stride, 4);
 }
 
 }  // extern "C"

@@ -97,6 +97,8 @@ cudaError_t ztc_launch_bc7_to(const ztc::SrcU8 &src, int by0, int nby, const ztc
 cudaError_t ztc_launch_bc_regroup(const uint8_t *in, uint8_t *out, size_t n, int fmt, int to_planes, cudaStream_t stream);
 cudaError_t ztc_launch_bc6h(const ztc::SrcHdr &src, int by0, int nby, uint8_t *out, cudaStream_t stream);
 cudaError_t ztc_launch_astc(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, void *scratch, cudaStream_t stream);
+// zap_astc_decode (zap_tex.h:1344-1356), device to device; bc 16-byte aligned
+cudaError_t ztc_launch_astc_decode(const uint8_t *bc, int w, int h, uint8_t *out, size_t stride, cudaStream_t stream);
 cudaError_t ztc_launch_mip(const uint8_t *src, int w, int h, size_t stride, int srgb, uint8_t *dst, size_t dst_stride,
                            cudaStream_t stream);
 cudaError_t ztc_launch_mip_f(const float *src, int w, int h, size_t stride, float *dst, size_t dst_stride, cudaStream_t stream);
