@@ -279,8 +279,10 @@ __global__ void __launch_bounds__(128) refine_kernel(int fmt, SrcU8 src, int bw,
 static int adj_check(int fmt, const void *p, int n) {
     if (fmt != ZTC_BC1 && fmt != ZTC_BC7) return ztc_set_error(ZTC_ERR_UNSUPPORTED, "differentiable decode covers BC1 and BC7 mode 6");
     if (!p || n < 0) return ztc_set_error(ZTC_ERR_INVALID_ARG, "null pointer or negative block count");
+    if ((uintptr_t)p % (fmt == ZTC_BC1 ? 8u : 16u)) return ztc_set_error(ZTC_ERR_INVALID_ARG, "blocks must be aligned to the block size");
     return ZTC_OK;
 }
+static bool floats_misaligned(const void *a, const void *b = nullptr) { return ((uintptr_t)a | (uintptr_t)b) & 3u; }
 static int launch_status(const char *what) {
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? ZTC_OK : ztc_set_error(ZTC_ERR_CUDA, (std::string(what) + ": " + cudaGetErrorString(e)).c_str());
@@ -291,7 +293,7 @@ extern "C" {
 int zap_tex_cuda_block_endpoints_dev(zap_tex_cuda_ctx *ctx, int fmt, const void *blocks, int nblocks, float *endpoints, void *stream) {
     int st = adj_check(fmt, blocks, nblocks);
     if (st || (st = ztc_ctx_activate(ctx))) return st;
-    if (!endpoints) return ztc_set_error(ZTC_ERR_INVALID_ARG, "null endpoints");
+    if (!endpoints || floats_misaligned(endpoints)) return ztc_set_error(ZTC_ERR_INVALID_ARG, "null or misaligned endpoints");
     if (nblocks) ztc::endpoints_kernel<<<(nblocks + 127) / 128, 128, 0, (cudaStream_t)stream>>>(fmt, (const uint8_t *)blocks, nblocks, endpoints);
     return launch_status("endpoints launch");
 }
@@ -300,7 +302,8 @@ int zap_tex_cuda_palette_decode_dev(zap_tex_cuda_ctx *ctx, int fmt, const void *
                                     void *stream) {
     int st = adj_check(fmt, blocks, nblocks);
     if (st || (st = ztc_ctx_activate(ctx))) return st;
-    if (!endpoints || !decoded) return ztc_set_error(ZTC_ERR_INVALID_ARG, "null endpoints / decoded");
+    if (!endpoints || !decoded || floats_misaligned(endpoints, decoded))
+        return ztc_set_error(ZTC_ERR_INVALID_ARG, "null or misaligned endpoints / decoded");
     if (nblocks) ztc::decode_kernel<<<(nblocks + 127) / 128, 128, 0, (cudaStream_t)stream>>>(fmt, (const uint8_t *)blocks, nblocks, endpoints, decoded);
     return launch_status("decode launch");
 }
@@ -309,7 +312,8 @@ int zap_tex_cuda_palette_adjoint_dev(zap_tex_cuda_ctx *ctx, int fmt, const void 
                                      float *grad_endpoints, void *stream) {
     int st = adj_check(fmt, blocks, nblocks);
     if (st || (st = ztc_ctx_activate(ctx))) return st;
-    if (!grad_decoded || !grad_endpoints) return ztc_set_error(ZTC_ERR_INVALID_ARG, "null gradient pointer");
+    if (!grad_decoded || !grad_endpoints || floats_misaligned(grad_decoded, grad_endpoints))
+        return ztc_set_error(ZTC_ERR_INVALID_ARG, "null or misaligned gradient pointer");
     if (nblocks)
         ztc::adjoint_kernel<<<(nblocks + 127) / 128, 128, 0, (cudaStream_t)stream>>>(fmt, (const uint8_t *)blocks, nblocks, grad_decoded,
                                                                                    grad_endpoints);
@@ -322,6 +326,7 @@ int zap_tex_cuda_refine_dev(zap_tex_cuda_ctx *ctx, int fmt, const uint8_t *rgba,
     if (st || (st = ztc_ctx_activate(ctx))) return st;
     if (!rgba || w < 1 || h < 1 || stride < (size_t)w * 4 || steps < 0 || steps > 1000 || !(lr >= 0.0f))
         return ztc_set_error(ZTC_ERR_INVALID_ARG, "bad image, steps or learning rate");
+    if (floats_misaligned(sse_before, sse_after)) return ztc_set_error(ZTC_ERR_INVALID_ARG, "misaligned SSE outputs");
     const int bw = (w + 3) / 4, nblocks = bw * ((h + 3) / 4);
     ztc::SrcU8 src{rgba, stride, w, h, 4, (((uintptr_t)rgba | stride) & 15u) == 0};
     ztc::TraceScope tr(fmt == ZTC_BC1 ? "refine_bc1" : "refine_bc7", (cudaStream_t)stream);

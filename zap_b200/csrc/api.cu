@@ -190,6 +190,9 @@ int grow(void **p, size_t *cap, size_t need, const char *what) {
 }
 
 bool valid_fmt_bc(int fmt) { return fmt >= ZTC_BC1 && fmt <= ZTC_BC7; }
+// device pointers the kernels access with vector or word loads / stores must be aligned: blocks to their size,
+// floats to 4 bytes, halfs to 2 (a misaligned vector access would be a device fault, so it is an argument error)
+bool misaligned(const void *p, size_t a) { return ((uintptr_t)p) % a != 0; }
 size_t block_bytes(int fmt) { return (fmt == ZTC_BC1 || fmt == ZTC_BC4) ? 8 : 16; }
 size_t round16(size_t v) { return (v + 15) & ~(size_t)15; }
 
@@ -449,6 +452,7 @@ int zap_tex_cuda_bc_encode_u8_dev(zap_tex_cuda_ctx *ctx, const uint8_t *src, int
     int st = check_image(src, out, w, h, stride, (size_t)w * channels);
     if (st) return st;
     if (!valid_fmt_bc(fmt) && fmt != ZTC_ASTC4X4) return fail(ZTC_ERR_UNSUPPORTED, "format %d", fmt);
+    if (misaligned(out, block_bytes(fmt == ZTC_ASTC4X4 ? ZTC_BC7 : fmt))) return fail(ZTC_ERR_INVALID_ARG, "out must be aligned to the block size");
     if ((st = resolve(ctx))) return st;
     ztc::SrcU8 s8{src, stride, w, h, channels, channels == 4 && (((uintptr_t)src | stride) & 15u) == 0};
     return dev_encode(ctx, fmt, s8, nullptr, w, h, out, (cudaStream_t)stream);
@@ -521,6 +525,7 @@ int zap_tex_cuda_bc_encode_split_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba,
 int zap_tex_cuda_bc6h_encode_dev(zap_tex_cuda_ctx *ctx, const float *rgba, int w, int h, size_t stride, void *out, void *stream) {
     int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
     if (st) return st;
+    if (misaligned(rgba, 4) || misaligned(out, 16)) return fail(ZTC_ERR_INVALID_ARG, "misaligned texels (4 B) or blocks (16 B)");
     if ((st = resolve(ctx))) return st;
     ztc::SrcU8 none{};
     ztc::SrcHdr sh{rgba, stride, w, h, 4, 1};
@@ -532,6 +537,7 @@ int zap_tex_cuda_bc6h_encode_half_dev(zap_tex_cuda_ctx *ctx, const uint16_t *src
     if (channels != 3 && channels != 4) return fail(ZTC_ERR_INVALID_ARG, "channels %d", channels);
     int st = check_image(src, out, w, h, stride, (size_t)w * channels);
     if (st) return st;
+    if (misaligned(src, 2) || misaligned(out, 16)) return fail(ZTC_ERR_INVALID_ARG, "misaligned texels (2 B) or blocks (16 B)");
     if ((st = resolve(ctx))) return st;
     ztc::SrcU8 none{};
     ztc::SrcHdr sh{src, stride, w, h, channels, 0};
@@ -555,6 +561,7 @@ int zap_tex_cuda_mip_next_f_dev(zap_tex_cuda_ctx *ctx, const float *src, int w, 
                                 void *stream) {
     int st = check_image(src, dst, w, h, stride, (size_t)w * 4);
     if (st) return st;
+    if (misaligned(src, 4) || misaligned(dst, 4)) return fail(ZTC_ERR_INVALID_ARG, "float texels must be 4-byte aligned");
     if ((st = resolve(ctx))) return st;
     cudaError_t e = ztc_launch_mip_f(src, w, h, stride, dst, dst_stride, (cudaStream_t)stream);
     return e == cudaSuccess ? ZTC_OK : cuda_fail(e, "mip launch");

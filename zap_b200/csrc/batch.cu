@@ -247,6 +247,8 @@ int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *it
             return ztc_set_error(ZTC_ERR_INVALID_ARG, ("batch item " + std::to_string(i) + ": bad pointer, size or stride").c_str());
         if (it.fmt < ZTC_BC1 || it.fmt > ZTC_BC7)
             return ztc_set_error(ZTC_ERR_UNSUPPORTED, ("batch item " + std::to_string(i) + ": format must be BC1..BC7").c_str());
+        if ((uintptr_t)it.dst % block_bytes(it.fmt))  // blocks are stored 8 or 16 bytes at a time
+            return ztc_set_error(ZTC_ERR_INVALID_ARG, ("batch item " + std::to_string(i) + ": dst not aligned to the block size").c_str());
     }
     int st0 = ztc_ctx_activate(ctx);  // makes the context's device current (NULL: the current device's default context)
     if (st0) return st0;

@@ -722,6 +722,7 @@ extern "C" __attribute__((visibility("default"))) int zap_tex_cuda_bc7_encode_no
     if (!rgba || !out) return ztc_set_error(-1, "null pointer");
     if (w < 1 || h < 1 || w > (1 << 24) || h > (1 << 24)) return ztc_set_error(-1, "size out of range");
     if (stride < (size_t)w * 4) return ztc_set_error(-1, "stride below 4 * width");
+    if ((uintptr_t)out % 16u) return ztc_set_error(-1, "out must be 16-byte aligned (BC7 blocks are stored 16 bytes at a time)");
     const size_t bw = (size_t)(w + 3) / 4, bh = (size_t)(h + 3) / 4;
     if (bw * bh > ztc::kNoAllocMaxBlocks)
         return ztc_set_error(-1, "texture has more 4x4 blocks than the allocation-free BC7 entry point holds (1048576)");
