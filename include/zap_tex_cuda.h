@@ -70,7 +70,8 @@ ZTC_API size_t zap_tex_cuda_bc_size(int w, int h, int fmt); /* replaces zap_bc_s
 ZTC_API int zap_tex_cuda_mip_levels(int w, int h);          /* replaces zap_mip_levels, zap_tex.h:1435-1439 */
 
 /* ---------------------------------------------------------------- drop-in encoders, host memory */
-/* replaces zap_bc_encode (zap_tex.h:1474); rdo must be 0 (ZTC_ERR_UNSUPPORTED otherwise) */
+/* replaces zap_bc_encode (zap_tex.h:1474). rdo <= 0: the plain encode; rdo > 0: rate-distortion mode
+   (zap_tex.h:223-306, :786-815), the reference's bytes for one call over the whole image; rdo must be finite */
 ZTC_API int zap_tex_cuda_bc_encode(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo,
                            void *out);
 /* replaces zap_bc6h_encode (zap_tex.h:946); stride in floats per row */
@@ -87,6 +88,12 @@ ZTC_API int zap_tex_cuda_mip_next_f(zap_tex_cuda_ctx *ctx, const float *src, int
 /* ---------------------------------------------------------------- device memory, asynchronous */
 ZTC_API int zap_tex_cuda_bc_encode_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo,
                                void *out, void *stream);
+/* Rate-distortion mode in bands, no single reference counterpart: the bytes of one zap_bc_encode call per band of
+   band_rows block rows (4 * band_rows texel rows; 0 = one band), as callers that encode a texture in bands get them
+   (samples/dx11/viewer.cpp:455-471 uses 8-block-row bands). Each band's choices form one serial chain on the
+   device (one warp), so more bands run in parallel. rdo finite; rdo <= 0 is the plain encode. */
+ZTC_API int zap_tex_cuda_bc_encode_rdo_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo,
+                                           int band_rows, void *out, void *stream);
 ZTC_API int zap_tex_cuda_bc6h_encode_dev(zap_tex_cuda_ctx *ctx, const float *rgba, int w, int h, size_t stride, void *out,
                                  void *stream);
 ZTC_API int zap_tex_cuda_astc_encode_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, void *out,

@@ -590,7 +590,7 @@ static float bc7_partition_score(const float mo[16][9], const float tot[9], int 
 #define BC7_MODE1_TRIES 4 /* ZAP__BC7_M1K default (zap_tex.h:750-752) */
 
 /* mode 6, early exit at SSE <= 64, then mode 5, then (opaque) mode 1 over the best-scored partitions (:755-784) */
-static void bc7_block(const tx4 t[16], uint8_t out[16]) {
+static int bc7_block(const tx4 t[16], uint8_t out[16]) { /* returns the SSE of the block it wrote, as :755-784 */
 #ifdef ZO_COUNT_OPS
     const uint64_t ops0 = g_ops[0];
 #endif
@@ -599,12 +599,12 @@ static void bc7_block(const tx4 t[16], uint8_t out[16]) {
     g_ops[1] += g_ops[0] - ops0;
 #endif
     for (int i = 0; i < 16; i++) opaque &= t[i][3] == 255;
-    if (err <= 16 * 4) return;
+    if (err <= 16 * 4) return err;
     uint8_t m5[16];
     bc7_mode5(t, m5);
     int e5 = bc7_decoded_sse(t, m5);
     if (e5 < err) { memcpy(out, m5, 16); err = e5; }
-    if (!opaque) return;
+    if (!opaque) return err;
     float mo[16][9], tot[9] = { 0 }, ce[BC7_MODE1_TRIES];
     int cand[BC7_MODE1_TRIES], bp = -1, be = err;
     for (int i = 0; i < 16; i++) {
@@ -631,18 +631,265 @@ static void bc7_block(const tx4 t[16], uint8_t out[16]) {
         uint8_t m1[16];
         bc7_mode1(t, bp, m1);
         int e1 = bc7_decoded_sse(t, m1);
-        if (e1 < err) memcpy(out, m1, 16);
+        if (e1 < err) { memcpy(out, m1, 16); err = e1; }
     }
+    return err;
+}
+
+/* ================================================================== RDO (zap_tex.h:223-306, :786-815)
+ * With lambda > 0 each sub-block is picked among its own encoding and candidates rebuilt from the 16 blocks before
+ * it in the call's raster order (the bytes already chosen for them), minimising SSE + lambda * rate. A field's rate
+ * models zap's LZ on the split planes: 0 if it repeats the field at the current match distance, min(size, 3) if it
+ * repeats one elsewhere in the window (a new match), else its size in literals. The choice is a sequential scan
+ * with strict "<", so the first candidate of the lowest cost wins. */
+#define RDO_WINDOW 16
+typedef struct { int dist[2]; } rdo_state; /* current match distance of each field, per sub-block kind */
+
+static float rdo_rate(const uint8_t *f, int n, const uint8_t *base, size_t cur, size_t stride, size_t off, int dist, int *nd) {
+    *nd = dist;
+    if (dist > 0 && (size_t)dist <= cur && memcmp(f, base + (cur - (size_t)dist) * stride + off, (size_t)n) == 0) return 0.0f;
+    for (size_t j = 1; j <= RDO_WINDOW && j <= cur; j++)
+        if (memcmp(f, base + (cur - j) * stride + off, (size_t)n) == 0) { *nd = (int)j; return n < 3 ? (float)n : 3.0f; }
+    return (float)n;
+}
+
+/* BC1 palette for any endpoint order (:52-62): 3 colours + transparent black when c0 <= c1 and not force4 */
+static int bc1_palette(uint16_t c0, uint16_t c1, int force4, int pal[4][3]) {
+    int a[3], b[3], four = force4 || c0 > c1;
+    unpack565(c0, a); unpack565(c1, b);
+    for (int k = 0; k < 3; k++) {
+        pal[0][k] = a[k]; pal[1][k] = b[k];
+        pal[2][k] = four ? (2 * a[k] + b[k] + 1) / 3 : (a[k] + b[k] + 1) / 2;
+        pal[3][k] = four ? (a[k] + 2 * b[k] + 1) / 3 : 0;
+    }
+    return four ? 4 : 3;
+}
+static int bc1_fit_any(const tx4 t[16], uint16_t c0, uint16_t c1, int force4, uint32_t *idx) { /* :66-77 */
+    int pal[4][3], n = bc1_palette(c0, c1, force4, pal), err = 0;
+    uint32_t bits = 0;
+    for (int i = 0; i < 16; i++) {
+        int bk = 0, be = d3(t[i], pal[0]);
+        for (int k = 1; k < n; k++) { int e = d3(t[i], pal[k]); if (e < be) { be = e; bk = k; } }
+        bits |= (uint32_t)bk << (2 * i);
+        err += be;
+    }
+    *idx = bits;
+    return err;
+}
+static int bc1_eval_idx(const tx4 t[16], uint16_t c0, uint16_t c1, int force4, uint32_t idx) { /* :79-84 */
+    int pal[4][3], err = 0;
+    bc1_palette(c0, c1, force4, pal);
+    for (int i = 0; i < 16; i++) err += d3(t[i], pal[(idx >> (2 * i)) & 3]);
+    return err;
+}
+
+static void bc1_rdo(const tx4 t[16], int force4, float lambda, uint8_t *base, size_t cur, size_t stride, size_t off, rdo_state *rs) {
+    uint16_t c0, c1;
+    uint32_t idx;
+    const int e0 = bc1_block(t, &c0, &c1, &idx);
+    uint8_t best[8], cand[8];
+    bc1_store(best, c0, c1, idx);
+    if (lambda > 0) {
+        int bd0 = 0, bd1 = 0, d0, d1;
+        float bj = (float)e0 + lambda * (rdo_rate(best, 4, base, cur, stride, off, rs->dist[0], &bd0) +
+                                         rdo_rate(best + 4, 4, base, cur, stride, off + 4, rs->dist[1], &bd1));
+        for (size_t j = 1; j <= RDO_WINDOW && j <= cur; j++) {
+            const uint8_t *prev = base + (cur - j) * stride + off;
+            const uint16_t p0 = (uint16_t)load_le(prev, 2), p1 = (uint16_t)load_le(prev + 2, 2);
+            const uint32_t pi = (uint32_t)load_le(prev + 4, 4);
+            for (int kind = 0; kind < 3; kind++) {
+                int e;
+                uint32_t fi;
+                if (kind == 0) { e = bc1_fit_any(t, p0, p1, force4, &fi); bc1_store(cand, p0, p1, fi); } /* its endpoints */
+                else if (kind == 1) { e = bc1_eval_idx(t, c0, c1, force4, pi); bc1_store(cand, c0, c1, pi); } /* its indices */
+                else { e = bc1_eval_idx(t, p0, p1, force4, pi); memcpy(cand, prev, 8); } /* the whole block */
+                if (!force4 && load_le(cand, 2) <= load_le(cand + 2, 2)) { /* 3-colour block: index 3 would be transparent */
+                    const uint32_t ci = (uint32_t)load_le(cand + 4, 4);
+                    int transparent = 0;
+                    for (int i = 0; i < 16; i++) transparent |= ((ci >> (2 * i)) & 3) == 3;
+                    if (transparent) continue;
+                }
+                float jj = (float)e;
+                if (jj >= bj) continue;
+                jj += lambda * (rdo_rate(cand, 4, base, cur, stride, off, rs->dist[0], &d0) +
+                                rdo_rate(cand + 4, 4, base, cur, stride, off + 4, rs->dist[1], &d1));
+                if (jj < bj) { bj = jj; memcpy(best, cand, 8); bd0 = d0; bd1 = d1; }
+            }
+        }
+        rs->dist[0] = bd0; rs->dist[1] = bd1;
+    }
+    memcpy(base + cur * stride + off, best, 8);
+}
+
+static int bc4_fit_any(const uint8_t v[16], int a0, int a1, uint64_t *idx) { /* :178-189 */
+    int pal[8], err = 0;
+    uint64_t bits = 0;
+    bc4_pal(a0, a1, pal);
+    for (int i = 0; i < 16; i++) {
+        int bk = 0, be = (v[i] - pal[0]) * (v[i] - pal[0]);
+        for (int k = 1; k < 8; k++) { int e = (v[i] - pal[k]) * (v[i] - pal[k]); if (e < be) { be = e; bk = k; } }
+        bits |= (uint64_t)bk << (3 * i);
+        err += be;
+    }
+    *idx = bits;
+    return err;
+}
+static int bc4_eval_idx(const uint8_t v[16], int a0, int a1, uint64_t idx) { /* :191-196 */
+    int pal[8], err = 0;
+    bc4_pal(a0, a1, pal);
+    for (int i = 0; i < 16; i++) { int d = v[i] - pal[(idx >> (3 * i)) & 7]; err += d * d; }
+    return err;
+}
+static void bc4_put(uint8_t *o, int a0, int a1, uint64_t idx) { o[0] = (uint8_t)a0; o[1] = (uint8_t)a1; store_le(o + 2, idx, 6); }
+
+static void bc4_rdo(const uint8_t v[16], float lambda, uint8_t *base, size_t cur, size_t stride, size_t off, rdo_state *rs) {
+    uint8_t a0, a1, best[8], cand[8];
+    uint64_t idx;
+    const int e0 = bc4_block(v, &a0, &a1, &idx);
+    bc4_put(best, a0, a1, idx);
+    if (lambda > 0) {
+        int bd0 = 0, bd1 = 0, d0, d1;
+        float bj = (float)e0 + lambda * (rdo_rate(best, 2, base, cur, stride, off, rs->dist[0], &bd0) +
+                                         rdo_rate(best + 2, 6, base, cur, stride, off + 2, rs->dist[1], &bd1));
+        for (size_t j = 1; j <= RDO_WINDOW && j <= cur; j++) {
+            const uint8_t *prev = base + (cur - j) * stride + off;
+            const uint64_t pi = load_le(prev + 2, 6);
+            for (int kind = 0; kind < 3; kind++) {
+                int e;
+                uint64_t fi;
+                if (kind == 0) { e = bc4_fit_any(v, prev[0], prev[1], &fi); bc4_put(cand, prev[0], prev[1], fi); }
+                else if (kind == 1) { e = bc4_eval_idx(v, a0, a1, pi); bc4_put(cand, a0, a1, pi); }
+                else { e = bc4_eval_idx(v, prev[0], prev[1], pi); memcpy(cand, prev, 8); }
+                float jj = (float)e;
+                if (jj >= bj) continue;
+                jj += lambda * (rdo_rate(cand, 2, base, cur, stride, off, rs->dist[0], &d0) +
+                                rdo_rate(cand + 2, 6, base, cur, stride, off + 2, rs->dist[1], &d1));
+                if (jj < bj) { bj = jj; memcpy(best, cand, 8); bd0 = d0; bd1 = d1; }
+            }
+        }
+        rs->dist[0] = bd0; rs->dist[1] = bd1;
+    }
+    memcpy(base + cur * stride + off, best, 8);
+}
+
+/* BC7 mode 6 pieces for RDO (:529-580): bytes 0-7 hold mode + endpoints, byte 8 straddles, bytes 9-15 indices */
+static int bc7_is_mode6(const uint8_t *b) { return (b[0] & 0x7F) == 0x40; }
+static void bc7_unpack_mode6(const uint8_t *b, int q[2][4], int pb[2], int idx[16]) {
+    bitr r = { b, 7 };
+    for (int c = 0; c < 4; c++) for (int e = 0; e < 2; e++) q[e][c] = (int)get_bits(&r, 7);
+    pb[0] = (int)get_bits(&r, 1); pb[1] = (int)get_bits(&r, 1);
+    for (int i = 0; i < 16; i++) idx[i] = (int)get_bits(&r, i ? 4 : 3);
+}
+static void bc7_pack_mode6(int q[2][4], const int pb[2], const int idx[16], uint8_t out[16]) {
+    memset(out, 0, 16);
+    bitw w = { out, 0 };
+    put_bits(&w, 1u << 6, 7);
+    for (int c = 0; c < 4; c++) for (int e = 0; e < 2; e++) put_bits(&w, (unsigned)q[e][c], 7);
+    put_bits(&w, (unsigned)pb[0], 1); put_bits(&w, (unsigned)pb[1], 1);
+    for (int i = 0; i < 16; i++) put_bits(&w, (unsigned)idx[i], i ? 4 : 3);
+}
+static void bc7_palette6(int q[2][4], const int pb[2], int pal[16][4]) {
+    int x[2][4];
+    for (int k = 0; k < 2; k++) for (int c = 0; c < 4; c++) x[k][c] = bc7_expand((q[k][c] << 1) | pb[k], 8);
+    for (int j = 0; j < 16; j++) for (int c = 0; c < 4; c++) pal[j][c] = lerp64(x[0][c], x[1][c], BC7_W4[j]);
+}
+static int d4(const uint8_t *p, const int *q) { int s = 0; for (int c = 0; c < 4; c++) { int x = p[c] - q[c]; s += x * x; } return s; }
+/* indices for given endpoints; texel 0 keeps to 0..7 so the block needs no anchor swap (:544-555) */
+static int bc7_mode6_fit_indices(const tx4 t[16], int q[2][4], const int pb[2], int idx[16]) {
+    int pal[16][4], err = 0;
+    bc7_palette6(q, pb, pal);
+    for (int i = 0; i < 16; i++) {
+        int bj = 0, be = 1 << 30;
+        for (int j = 0; j < (i ? 16 : 8); j++) { int d = d4(t[i], pal[j]); if (d < be) { be = d; bj = j; } }
+        idx[i] = bj; err += be;
+    }
+    return err;
+}
+/* endpoints for given indices: least squares, then each endpoint's own best p-bit (:557-580) */
+static int bc7_mode6_fit_endpoints(const tx4 t[16], const int idx[16], int q[2][4], int pb[2]) {
+    float aa = 0, ab = 0, bb = 0, sa[4] = { 0, 0, 0, 0 }, sb[4] = { 0, 0, 0, 0 }, lo[4], hi[4];
+    for (int i = 0; i < 16; i++) {
+        float w = BC7_W4[idx[i]] / 64.0f, u = 1 - w;
+        aa += u * u; ab += u * w; bb += w * w;
+        for (int c = 0; c < 4; c++) { sa[c] += u * t[i][c]; sb[c] += w * t[i][c]; }
+    }
+    float det = aa * bb - ab * ab;
+    for (int c = 0; c < 4; c++) {
+        if (det < 1e-6f && det > -1e-6f) lo[c] = hi[c] = (sa[c] + sb[c]) / 16.0f; /* one index everywhere */
+        else { lo[c] = (sa[c] * bb - sb[c] * ab) / det; hi[c] = (sb[c] * aa - sa[c] * ab) / det; }
+        lo[c] = fclamp255(lo[c]); hi[c] = fclamp255(hi[c]);
+    }
+    int x0[4], x1[4], t0[4], t1[4], b0 = 1 << 30, b1 = 1 << 30;
+    for (int p = 0; p < 2; p++) {
+        int e0 = bc7_quant_pbit(lo, 4, 8, p, t0, x0), e1 = bc7_quant_pbit(hi, 4, 8, p, t1, x1);
+        if (e0 < b0) { b0 = e0; memcpy(q[0], t0, sizeof t0); pb[0] = p; }
+        if (e1 < b1) { b1 = e1; memcpy(q[1], t1, sizeof t1); pb[1] = p; }
+    }
+    int pal[16][4], err = 0;
+    bc7_palette6(q, pb, pal);
+    for (int i = 0; i < 16; i++) err += d4(t[i], pal[idx[i]]);
+    return err;
+}
+static float bc7_rdo_rate(const uint8_t *c, const uint8_t *base, size_t cur, const rdo_state *rs, int d[2]) { /* :788-790 */
+    return rdo_rate(c, 8, base, cur, 16, 0, rs->dist[0], &d[0]) + rdo_rate(c + 9, 7, base, cur, 16, 9, rs->dist[1], &d[1]) + 1;
+}
+static void bc7_rdo(const tx4 t[16], float lambda, uint8_t *base, size_t cur, rdo_state *rs) {
+    uint8_t best[16], cand[16];
+    const int e0 = bc7_block(t, best);
+    if (lambda > 0) {
+        int bd[2] = { 0, 0 }, d[2];
+        float bj = (float)e0 + lambda * bc7_rdo_rate(best, base, cur, rs, bd);
+        for (size_t j = 1; j <= RDO_WINDOW && j <= cur; j++) {
+            const uint8_t *prev = base + (cur - j) * 16;
+            int pq[2][4], ppb[2], pidx[16], nq[2][4], npb[2], nidx[16];
+            const int six = bc7_is_mode6(prev);
+            if (six) bc7_unpack_mode6(prev, pq, ppb, pidx);
+            for (int kind = 0; kind < (six ? 3 : 1); kind++) {
+                int e;
+                if (kind == 0) { e = bc7_decoded_sse(t, prev); memcpy(cand, prev, 16); }
+                else if (kind == 1) { e = bc7_mode6_fit_indices(t, pq, ppb, nidx); bc7_pack_mode6(pq, ppb, nidx, cand); }
+                else { e = bc7_mode6_fit_endpoints(t, pidx, nq, npb); bc7_pack_mode6(nq, npb, pidx, cand); }
+                if ((float)e >= bj) continue;
+                float jj = (float)e + lambda * bc7_rdo_rate(cand, base, cur, rs, d);
+                if (jj < bj) { bj = jj; memcpy(best, cand, 16); bd[0] = d[0]; bd[1] = d[1]; }
+            }
+        }
+        rs->dist[0] = bd[0]; rs->dist[1] = bd[1];
+    }
+    memcpy(base + cur * 16, best, 16);
 }
 
 /* ================================================================== public BC entry (zap_tex.h:1474-1506) */
 size_t zo_bc_size(int w, int h, int fmt) { return (size_t)((w + 3) / 4) * (size_t)((h + 3) / 4) * (fmt == ZO_BC1 || fmt == ZO_BC4 ? 8u : 16u); }
 
 int zo_bc_encode(const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo, void *out_) {
-    if (rdo != 0 || fmt < 0 || fmt > 4) return -1; /* rate-distortion mode is not part of the restatement */
+    if (fmt < 0 || fmt > 4) return -1;
     uint8_t *out = (uint8_t *)out_;
     int bw = (w + 3) / 4, bh = (h + 3) / 4;
     size_t bs = (fmt == ZO_BC1 || fmt == ZO_BC4) ? 8 : 16;
+    if (rdo > 0) { /* one chain over the call's blocks in raster order; a match state per sub-block kind */
+        rdo_state rs[2] = { { { 1, 1 } }, { { 1, 1 } } };
+        for (int by = 0; by < bh; by++)
+            for (int bx = 0; bx < bw; bx++) {
+                tx4 t[16];
+                uint8_t ch[2][16];
+                const size_t cur = (size_t)by * (size_t)bw + (size_t)bx;
+                gather8(rgba, w, h, stride, bx, by, t);
+                if (fmt == ZO_BC1) bc1_rdo((const tx4 *)t, 0, rdo, out, cur, bs, 0, &rs[0]);
+                else if (fmt == ZO_BC3) {
+                    for (int i = 0; i < 16; i++) ch[0][i] = t[i][3];
+                    bc4_rdo(ch[0], rdo, out, cur, bs, 0, &rs[0]);
+                    bc1_rdo((const tx4 *)t, 1, rdo, out, cur, bs, 8, &rs[1]);
+                } else if (fmt == ZO_BC4 || fmt == ZO_BC5) {
+                    for (int i = 0; i < 16; i++) { ch[0][i] = t[i][0]; ch[1][i] = t[i][1]; }
+                    bc4_rdo(ch[0], rdo, out, cur, bs, 0, &rs[0]);
+                    if (fmt == ZO_BC5) bc4_rdo(ch[1], rdo, out, cur, bs, 8, &rs[1]);
+                } else {
+                    bc7_rdo((const tx4 *)t, rdo, out, cur, &rs[0]);
+                }
+            }
+        return 0;
+    }
     for (int by = 0; by < bh; by++)
         for (int bx = 0; bx < bw; bx++) {
             tx4 t[16];

@@ -76,14 +76,14 @@ class Oracle:
         setattr(self, "_" + name, fn)
 
     # ---- encoders (img: HxWx4 uint8 or float32, C-contiguous rows; stride = row pitch)
-    def bc_encode(self, img, fmt, threads=1):
+    def bc_encode(self, img, fmt, threads=1, rdo=0.0):
         img = np.ascontiguousarray(img)
         h, w = img.shape[:2]
         out = np.zeros(bc_size(w, h, fmt), np.uint8)
-        if threads > 1 and self.kind == "reference":
+        if threads > 1 and self.kind == "reference" and rdo <= 0:
             self._bc_encode_mt(img.ctypes.data, w, h, w * 4, fmt, out.ctypes.data, threads)
         else:
-            self._bc_encode(img.ctypes.data, w, h, w * 4, fmt, 0.0, out.ctypes.data)
+            self._bc_encode(img.ctypes.data, w, h, w * 4, fmt, float(rdo), out.ctypes.data)
         return out
 
     def bc6h_encode(self, img, threads=1):

@@ -83,7 +83,8 @@ def test_host_api_rejects_bad_arguments_without_device():
     out = np.zeros(64, np.uint8)
     assert lib.zap_tex_cuda_bc_encode(None, img.ctypes.data, 0, 8, 32, 0, 0.0, out.ctypes.data) == -1
     assert lib.zap_tex_cuda_bc_encode(None, None, 8, 8, 32, 0, 0.0, out.ctypes.data) == -1
-    assert lib.zap_tex_cuda_bc_encode(None, img.ctypes.data, 8, 8, 32, 0, 5.0, out.ctypes.data) == -2
+    assert lib.zap_tex_cuda_bc_encode(None, img.ctypes.data, 8, 8, 32, 7, 0.0, out.ctypes.data) == -2  # no such format
+    assert lib.zap_tex_cuda_bc_encode(None, img.ctypes.data, 8, 8, 32, 0, float("nan"), out.ctypes.data) == -1
     assert zap_b200.bc_size(0, 4, 0) == 0 and zap_b200.mip_levels(5, 3) == 3 and zap_b200.block_bytes(4) == 16
 
 

@@ -216,3 +216,21 @@ def test_astc_decode_matches_reference_live(oracle, reference):
     rng = np.random.default_rng(14)
     bc = _astc_block_mix(rng, 24 * 20).reshape(-1)
     assert np.array_equal(oracle.astc_decode(bc, 95, 77), reference.astc_decode(bc, 95, 77))
+
+
+# ---------------------------------------------------------------- rate-distortion mode (zap_tex.h:223-306, :786-815)
+@pytest.mark.parametrize("rdo", [10.0, 30.0, 300.0])
+def test_rdo_port_matches_reference_live(oracle, reference, rdo):
+    import zap_b200.synth as S
+    rng = np.random.default_rng(int(rdo))
+    imgs = [S.colour_texture(64, 48, seed=3, alpha="noise").numpy(), S.colour_texture(37, 29, seed=4).numpy(),
+            rng.integers(0, 256, (21, 27, 4), dtype=np.uint8)]
+    for img in imgs:
+        for fmt in (BC1, BC3, BC4, BC5, BC7):
+            assert np.array_equal(oracle.bc_encode(img, fmt, rdo=rdo), reference.bc_encode(img, fmt, rdo=rdo)), (fmt, rdo, img.shape)
+
+
+def test_rdo_nonpositive_lambda_is_the_plain_encode(oracle):
+    img = np.random.default_rng(2).integers(0, 256, (20, 24, 4), dtype=np.uint8)
+    for fmt in (BC1, BC7):
+        assert np.array_equal(oracle.bc_encode(img, fmt, rdo=-5.0), oracle.bc_encode(img, fmt))

@@ -135,6 +135,18 @@ def bc_encode_dev(t, fmt, out=None, stream=None, ctx=None):
     return out
 
 
+def bc_encode_rdo_dev(t, fmt, rdo, band_rows=0, out=None, stream=None, ctx=None):
+    """Rate-distortion encode (zap_bc_encode with rdo > 0) of an HxWx4 uint8 CUDA tensor: one reference call over
+    the whole image (band_rows 0), or one per band of band_rows block rows."""
+    import torch
+    w, h, stride = _dev_img(t, (4,))
+    if out is None:
+        out = torch.empty(bc_size(w, h, fmt), dtype=torch.uint8, device=t.device)
+    check(load().zap_tex_cuda_bc_encode_rdo_dev(ctx, t.data_ptr(), w, h, stride, fmt, float(rdo), int(band_rows), out.data_ptr(),
+                                                _stream(stream)), "bc_encode_rdo_dev")
+    return out
+
+
 def astc_encode_dev(t, out=None, stream=None, ctx=None):
     return bc_encode_dev(t, ASTC4X4, out, stream, ctx)
 

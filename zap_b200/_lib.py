@@ -55,6 +55,7 @@ def _declare(lib):
         "zap_tex_cuda_mip_next": ([vp, vp, i, i, sz, i, vp, sz], i),
         "zap_tex_cuda_mip_next_f": ([vp, vp, i, i, sz, vp, sz], i),
         "zap_tex_cuda_bc_encode_dev": ([vp, vp, i, i, sz, i, f, vp, vp], i),
+        "zap_tex_cuda_bc_encode_rdo_dev": ([vp, vp, i, i, sz, i, f, i, vp, vp], i),
         "zap_tex_cuda_bc6h_encode_dev": ([vp, vp, i, i, sz, vp, vp], i),
         "zap_tex_cuda_astc_encode_dev": ([vp, vp, i, i, sz, vp, vp], i),
         "zap_tex_cuda_mip_next_dev": ([vp, vp, i, i, sz, i, vp, sz, vp], i),

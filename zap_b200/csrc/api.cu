@@ -261,6 +261,22 @@ int dev_encode(zap_tex_cuda_ctx *ctx, int fmt, const ztc::SrcU8 &s8, const ztc::
     return st;
 }
 
+// rate-distortion mode (zap_tex.h:223-306, :786-815): the base encodings of every block, then the RDO chain(s)
+// over them in place; band_rows block rows per chain (0: one chain, as one reference call)
+int rdo_encode(zap_tex_cuda_ctx *ctx, int fmt, const ztc::SrcU8 &s8, int w, int h, float lambda, int band_rows, void *out, cudaStream_t s) {
+    int st = dev_encode(ctx, fmt, s8, nullptr, w, h, out, s);
+    if (st) return st;
+    ZTC_CHECK(ztc_launch_rdo(fmt, s8, (uint8_t *)out, lambda, band_rows, s), "rdo launch");
+    return ZTC_OK;
+}
+
+// lambda as the reference reads it: <= 0 is the plain encode; a finite positive value selects RDO; NaN and
+// infinities are rejected (the chain's choice rule relies on finite, non-negative costs)
+int check_lambda(float rdo) {
+    if (!(rdo == rdo) || rdo > 3.0e38f || rdo < -3.0e38f) return fail(ZTC_ERR_INVALID_ARG, "rdo must be a finite number");
+    return ZTC_OK;
+}
+
 int check_image(const void *p, const void *out, int w, int h, size_t stride, size_t min_stride) {
     if (!p || !out) return fail(ZTC_ERR_INVALID_ARG, "null pointer");
     if (w < 1 || h < 1) return fail(ZTC_ERR_INVALID_ARG, "size %dx%d", w, h);
@@ -386,9 +402,20 @@ int zap_tex_cuda_bc_encode(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, in
     int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
     if (st) return st;
     if (!valid_fmt_bc(fmt)) return fail(ZTC_ERR_UNSUPPORTED, "format %d", fmt);
-    if (rdo != 0.0f) return fail(ZTC_ERR_UNSUPPORTED, "rdo %g: rate-distortion mode is not implemented on the device", (double)rdo);
+    if ((st = check_lambda(rdo))) return st;
     if ((st = resolve(ctx))) return st;
-    return host_encode(ctx, fmt, rgba, w, h, stride, 4, out);
+    if (rdo <= 0.0f) return host_encode(ctx, fmt, rgba, w, h, stride, 4, out);
+    // RDO: one chain over the whole image, so the image is staged whole (no bands)
+    const size_t row = (size_t)w * 4, pitch = round16(row), bytes = (size_t)((w + 3) / 4) * ((h + 3) / 4) * block_bytes(fmt);
+    if ((st = grow((void **)&ctx->d_in, &ctx->d_in_cap, pitch * (size_t)h, "cudaMalloc(input)"))) return st;
+    if ((st = grow((void **)&ctx->d_out, &ctx->d_out_cap, bytes, "cudaMalloc(output)"))) return st;
+    cudaStream_t s = ctx->stream[0];
+    ZTC_CHECK(cudaMemcpy2DAsync(ctx->d_in, pitch, rgba, stride, row, (size_t)h, cudaMemcpyHostToDevice, s), "host->device copy");
+    const ztc::SrcU8 s8{ctx->d_in, pitch, w, h, 4, ((uintptr_t)ctx->d_in & 15u) == 0};
+    if ((st = rdo_encode(ctx, fmt, s8, w, h, rdo, 0, ctx->d_out, s))) return st;
+    ZTC_CHECK(cudaMemcpyAsync(out, ctx->d_out, bytes, cudaMemcpyDeviceToHost, s), "device->host copy");
+    ZTC_CHECK(cudaStreamSynchronize(s), "encode");
+    return ZTC_OK;
 }
 
 int zap_tex_cuda_bc6h_encode(zap_tex_cuda_ctx *ctx, const float *rgba, int w, int h, size_t stride, void *out) {
@@ -441,9 +468,25 @@ int zap_tex_cuda_mip_next_f(zap_tex_cuda_ctx *ctx, const float *src, int w, int 
 // ------------------------------------------------------------------ device memory
 int zap_tex_cuda_bc_encode_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo, void *out,
                                void *stream) {
-    if (rdo != 0.0f) return fail(ZTC_ERR_UNSUPPORTED, "rdo %g: rate-distortion mode is not implemented on the device", (double)rdo);
     if (!valid_fmt_bc(fmt)) return fail(ZTC_ERR_UNSUPPORTED, "format %d", fmt);
+    int st = check_lambda(rdo);
+    if (st) return st;
+    if (rdo > 0.0f) return zap_tex_cuda_bc_encode_rdo_dev(ctx, rgba, w, h, stride, fmt, rdo, 0, out, stream);
     return zap_tex_cuda_bc_encode_u8_dev(ctx, rgba, 4, w, h, stride, fmt, out, stream);
+}
+
+int zap_tex_cuda_bc_encode_rdo_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo, int band_rows,
+                                   void *out, void *stream) {
+    int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
+    if (st) return st;
+    if (!valid_fmt_bc(fmt)) return fail(ZTC_ERR_UNSUPPORTED, "format %d", fmt);
+    if ((st = check_lambda(rdo))) return st;
+    if (band_rows < 0) return fail(ZTC_ERR_INVALID_ARG, "band_rows %d", band_rows);
+    if (misaligned(out, block_bytes(fmt))) return fail(ZTC_ERR_INVALID_ARG, "out must be aligned to the block size");
+    if ((st = resolve(ctx))) return st;
+    const ztc::SrcU8 s8{rgba, stride, w, h, 4, (((uintptr_t)rgba | stride) & 15u) == 0};
+    if (rdo <= 0.0f) return dev_encode(ctx, fmt, s8, nullptr, w, h, out, (cudaStream_t)stream);
+    return rdo_encode(ctx, fmt, s8, w, h, rdo, band_rows, out, (cudaStream_t)stream);
 }
 
 int zap_tex_cuda_bc_encode_u8_dev(zap_tex_cuda_ctx *ctx, const uint8_t *src, int channels, int w, int h, size_t stride, int fmt, void *out,

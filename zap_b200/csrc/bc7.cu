@@ -30,26 +30,7 @@ __constant__ uint8_t kA2[64] = {
     15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 2, 8, 2, 2, 8, 8, 15, 2, 8, 2, 2, 8, 8, 2, 2,
     15, 15, 6, 8, 2, 8, 15, 15, 2, 8, 2, 2, 2, 15, 15, 6, 6, 2, 6, 8, 15, 15, 2, 2, 15, 15, 15, 15, 15, 2, 2, 15};
 
-// ---------------------------------------------------------------- shared pieces
-// endpoint quantisation with a fixed p-bit (zap_tex.h:426-438); q: stored values, x8: expanded 8-bit values
-template <int NC>
-ZTC_DEV int quant_pbit(const float v[4], int n, int p, int q[4], int x8[4]) {
-    int err = 0, top = (1 << (n - 1)) - 1;
-    #pragma unroll
-    for (int c = 0; c < NC; c++) {
-        int g = f2i_x86((v[c] / 255.0f * (float)((1 << n) - 1) - (float)p) / 2.0f + 0.5f), bq = 0, be = 1 << 30;
-        #pragma unroll
-        for (int k = 0; k < 3; k++) {
-            int tq = clampi(around(g, k), 0, top);
-            float d = (float)expand_bits((tq << 1) | p, n) - v[c];
-            int e = f2i_x86(d * d);
-            if (e < be) { be = e; bq = tq; }
-        }
-        q[c] = bq; x8[c] = expand_bits((bq << 1) | p, n); err += be;
-    }
-    return err;
-}
-
+// ---------------------------------------------------------------- shared pieces (quant_pbit: ztc_common.cuh)
 // Argmin over a (1 << IB)-entry palette for every selected texel: key = (|c|^2 - 2 p.c) * NP + j is ordered
 // like the reference's first-best scan. idx: nibble i = index of texel i. Returns the SSE.
 template <int NC, int IB>

@@ -10,10 +10,6 @@
 namespace ztc {
 
 // ---------------------------------------------------------------- BC1 (zap_tex.h:39-168)
-ZTC_DEV void unpack565(uint32_t c, int &r, int &g, int &b) {
-    int R = (c >> 11) & 31, G = (c >> 5) & 63, B = c & 31;
-    r = (R << 3) | (R >> 2); g = (G << 2) | (G >> 4); b = (B << 3) | (B >> 2);
-}
 ZTC_DEV uint32_t pack565(float r, float g, float b) {  // zap_tex.h:45-49
     int R = f2i_x86(r * 31.0f / 255.0f + 0.5f), G = f2i_x86(g * 63.0f / 255.0f + 0.5f), B = f2i_x86(b * 31.0f / 255.0f + 0.5f);
     return ((uint32_t)clampi(R, 0, 31) << 11) | ((uint32_t)clampi(G, 0, 63) << 5) | (uint32_t)clampi(B, 0, 31);

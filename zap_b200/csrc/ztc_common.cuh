@@ -80,6 +80,31 @@ ZTC_DEV int wbits(int bits, int j) { return bits == 2 ? w2(j) : bits == 3 ? w3(j
 ZTC_DEV int lerp64(int a, int b, int w) { return ((64 - w) * a + w * b + 32) >> 6; }
 ZTC_DEV int expand_bits(int v, int n) { v <<= 8 - n; return v | (v >> n); }  // n-bit -> 8-bit replication
 
+// endpoint quantisation with a fixed p-bit (zap_tex.h:426-438); q: stored values, x8: expanded 8-bit values
+template <int NC>
+ZTC_DEV int quant_pbit(const float v[4], int n, int p, int q[4], int x8[4]) {
+    int err = 0, top = (1 << (n - 1)) - 1;
+    #pragma unroll
+    for (int c = 0; c < NC; c++) {
+        int g = f2i_x86((v[c] / 255.0f * (float)((1 << n) - 1) - (float)p) / 2.0f + 0.5f), bq = 0, be = 1 << 30;
+        #pragma unroll
+        for (int k = 0; k < 3; k++) {
+            int tq = clampi(around(g, k), 0, top);
+            float d = (float)expand_bits((tq << 1) | p, n) - v[c];
+            int e = f2i_x86(d * d);
+            if (e < be) { be = e; bq = tq; }
+        }
+        q[c] = bq; x8[c] = expand_bits((bq << 1) | p, n); err += be;
+    }
+    return err;
+}
+
+// 565 endpoint -> 8-bit RGB by bit replication (zap_tex.h:41-44)
+ZTC_DEV void unpack565(uint32_t c, int &r, int &g, int &b) {
+    int R = (c >> 11) & 31, G = (c >> 5) & 63, B = c & 31;
+    r = (R << 3) | (R >> 2); g = (G << 2) | (G >> 4); b = (B << 3) | (B >> 2);
+}
+
 ZTC_DEV uint32_t chan(uint32_t t, int c) { return (t >> (8 * c)) & 0xFFu; }
 ZTC_DEV uint32_t pack_rgb(int r, int g, int b) { return (uint32_t)r | ((uint32_t)g << 8) | ((uint32_t)b << 16); }
 ZTC_DEV uint32_t pack_rgba(int r, int g, int b, int a) { return pack_rgb(r, g, b) | ((uint32_t)a << 24); }
