@@ -360,6 +360,7 @@ def main():
             line["extra"] = extra_workloads(args, dev, mhz, sms)
             line["batched"] = batched_workload(args, dev)
             line["refine"] = refine_workload(args, dev)
+            line["rdo"] = rdo_workload(dev)
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
@@ -402,6 +403,39 @@ def batched_workload(args, dev, n=4096):
     b.close()
     del texs, graph_out
     torch.cuda.empty_cache()
+    return res
+
+
+def rdo_workload(dev, lam=30.0):
+    """Rate-distortion mode (rdo > 0): the reference's choice of each block depends on the 16 blocks chosen before
+    it, so one call is one serial chain (one CTA on the device); callers that encode in 8-block-row bands get one
+    chain per band. GPU: device API, CUDA events, inputs resident; the reference on one host core for the same call
+    (its own code, oracle/_ref), and whether the bytes are identical."""
+    import numpy as np
+    import torch
+
+    import zap_b200
+    import zap_b200.synth as S
+    import oracle_lib
+    ref = oracle_lib.reference()
+    res = {"lambda": lam}
+    for name, side, fmt, band in (("bc1_512_one_call", 512, zap_b200.BC1, 0), ("bc7_512_one_call", 512, zap_b200.BC7, 0),
+                                  ("bc1_2048_bands8", 2048, zap_b200.BC1, 8), ("bc7_2048_bands8", 2048, zap_b200.BC7, 8)):
+        img = S.colour_texture(side, side, seed=300, alpha="noise").numpy()
+        t = torch.from_numpy(img).to(dev)
+        out = zap_b200.bc_encode_rdo_dev(t, fmt, lam, band_rows=band)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = zap_b200.bc_encode_rdo_dev(t, fmt, lam, band_rows=band, out=out)
+        e1.record()
+        torch.cuda.synchronize()
+        r = {"gpu_ms": e0.elapsed_time(e1), "chains": 1 if not band else (side // 4 + band - 1) // band}
+        if ref is not None and side <= 512:
+            t0 = time.perf_counter()
+            want = ref.bc_encode(img, fmt, rdo=lam)
+            r["reference_1core_ms"] = (time.perf_counter() - t0) * 1e3
+            r["identical"] = bool(np.array_equal(out.cpu().numpy(), want))
+        res[name] = r
     return res
 
 
