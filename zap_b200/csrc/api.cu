@@ -214,14 +214,20 @@ size_t scratch_for(int fmt, size_t nblocks) {
     return 0;
 }
 
+// Source bytes per band of the host-pointer pipeline: larger bands copy closer to the link's peak, smaller ones
+// overlap more of the encode and the copy back with the copy in.
+#ifndef ZTC_HOST_BAND_BYTES
+#define ZTC_HOST_BAND_BYTES (2u << 20)
+#endif
+
 // Host-pointer encode: stage rows to the device band by band, encode, copy blocks back.
 // texel_bytes: 4 (RGBA8) or 16 (RGBA f32); src_stride in bytes.
 int host_encode(zap_tex_cuda_ctx *ctx, int fmt, const void *src, int w, int h, size_t src_stride, size_t texel_bytes, void *out) {
     const int bw = (w + 3) / 4, bh = (h + 3) / 4;
     const size_t bs = fmt == ZTC_BC6H || fmt == ZTC_ASTC4X4 ? 16 : block_bytes(fmt);
     const size_t row_bytes = (size_t)w * texel_bytes, pitch = round16(row_bytes);
-    // band height: about 2 MB of source per band (a 2048x2048 RGBA8 image gives 8 bands), at least 8 block rows
-    size_t band_rows = (2u << 20) / (pitch * 4) + 1;
+    // band height: about ZTC_HOST_BAND_BYTES of source per band, at least 8 block rows
+    size_t band_rows = (size_t)ZTC_HOST_BAND_BYTES / (pitch * 4) + 1;
     if (band_rows < 8) band_rows = 8;
     if (band_rows > (size_t)bh) band_rows = (size_t)bh;
     const int nbands = (int)((bh + band_rows - 1) / band_rows);
