@@ -27,8 +27,9 @@ namespace {
 struct TraceRec {
     const char *name;
     cudaEvent_t a, b;
-    long units;         // blocks (or texels) the launch processed, when known on the host
-    uint32_t *counter;  // pinned slot receiving a device-side count, or null
+    long units;                // blocks (or texels) the launch processed, when known on the host
+    uint32_t *counter;         // pinned slot receiving a device-side count, or null
+    const uint32_t *d_count;   // that count on the device, copied after the end event (outside the interval)
 };
 std::mutex g_trace_lock;
 bool g_trace_on = false;
@@ -41,7 +42,7 @@ constexpr int kSlots = 1 << 16;
 
 void trace_begin(const char *name, cudaStream_t s) {
     if (!g_trace_on) return;
-    TraceRec r{name, nullptr, nullptr, 0, nullptr};
+    TraceRec r{name, nullptr, nullptr, 0, nullptr, nullptr};
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {  // nothing to time while capturing
         cudaGetLastError();
@@ -56,14 +57,9 @@ void trace_begin(const char *name, cudaStream_t s) {
 void trace_units(long n) {
     if (g_trace_on && !t_open.empty()) t_open.back().units = n;
 }
-void trace_units_dev(const uint32_t *d_count, cudaStream_t s) {
-    if (!g_trace_on || t_open.empty() || !t_open.back().a) return;
-    std::lock_guard<std::mutex> g(g_trace_lock);
-    if (!g_slots && cudaMallocHost((void **)&g_slots, kSlots * sizeof(uint32_t)) != cudaSuccess) { g_slots = nullptr; return; }
-    if (g_slot_next >= kSlots) return;
-    uint32_t *slot = g_slots + g_slot_next++;
-    *slot = 0;
-    if (cudaMemcpyAsync(slot, d_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s) == cudaSuccess) t_open.back().counter = slot;
+void trace_units_dev(const uint32_t *d_count, cudaStream_t s) {  // the launch does not change the count it reads
+    (void)s;
+    if (g_trace_on && !t_open.empty() && t_open.back().a) t_open.back().d_count = d_count;
 }
 void trace_end(cudaStream_t s) {
     if (!g_trace_on || t_open.empty()) return;
@@ -72,6 +68,14 @@ void trace_end(cudaStream_t s) {
     if (!r.a) return;  // began during a capture
     cudaEventRecord(r.b, s);
     std::lock_guard<std::mutex> g(g_trace_lock);
+    if (r.d_count) {
+        if (!g_slots && cudaMallocHost((void **)&g_slots, kSlots * sizeof(uint32_t)) != cudaSuccess) g_slots = nullptr;
+        if (g_slots && g_slot_next < kSlots) {
+            uint32_t *slot = g_slots + g_slot_next++;
+            *slot = 0;
+            if (cudaMemcpyAsync(slot, r.d_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s) == cudaSuccess) r.counter = slot;
+        }
+    }
     g_trace.push_back(r);
 }
 }  // namespace ztc
