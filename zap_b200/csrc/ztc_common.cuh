@@ -17,20 +17,20 @@
 
 // Minimum resident 128-thread CTAs per SM requested from the register allocator, per kernel (tuned on B200:
 // more resident warps hide the latency of these long dependent integer / float chains; see the ncu summaries).
-// Measured on 2048x2048 encodes: bc7_mode6 0.174 -> 0.145 ms at 4 (128 registers, small spill), BC1 -4.5 % at 6,
-// BC6H -11 % at 3, ASTC single-partition -6 % at 4 (146 -> 128 registers); the BC7 mode 5/1 kernel gains nothing
-// from more than 1.
+// Measured on 2048x2048 encodes (re-swept after the loops were rolled): bc7_mode6 0.120 -> 0.113 ms at 6 (85
+// registers; the small spill stays in L1), BC1 -1.2 % at 8, ASTC single-partition -4 % at 5, BC6H -11 % at 3; the
+// BC7 mode 5/1 kernel (124 registers already allow 4 CTAs) gains nothing from more.
 #ifndef ZTC_MINB_BC7_MODE6
-#define ZTC_MINB_BC7_MODE6 4
+#define ZTC_MINB_BC7_MODE6 6
 #endif
 #ifndef ZTC_MINB_BC7_HARD
 #define ZTC_MINB_BC7_HARD 1
 #endif
 #ifndef ZTC_MINB_BCN
-#define ZTC_MINB_BCN 6
+#define ZTC_MINB_BCN 8
 #endif
 #ifndef ZTC_MINB_ASTC_SINGLE
-#define ZTC_MINB_ASTC_SINGLE 4
+#define ZTC_MINB_ASTC_SINGLE 5
 #endif
 #ifndef ZTC_MINB_BC6H
 #define ZTC_MINB_BC6H 3
