@@ -234,7 +234,7 @@ cudaError_t ztc_launch_bcn(int fmt, const ztc::SrcU8 &src, int by0, int nby, uin
 // ---------------------------------------------------------------- batched: one persistent launch over a tile queue
 namespace ztc {
 template <int FMT, int CTA>
-__global__ void __launch_bounds__(CTA, ZTC_MINB_BCN * 128 / CTA) batch_bcn_kernel(const BatchLevel *__restrict__ levels, const BatchTile *__restrict__ tiles,
+__global__ void __launch_bounds__(CTA, ZTC_MINB_BCN_BATCH * 128 / CTA) batch_bcn_kernel(const BatchLevel *__restrict__ levels, const BatchTile *__restrict__ tiles,
                                                         int ntiles, uint32_t *__restrict__ counter) {
     __shared__ int s_tile;
     for (;;) {

@@ -29,6 +29,9 @@
 #ifndef ZTC_MINB_BCN
 #define ZTC_MINB_BCN 8
 #endif
+#ifndef ZTC_MINB_BCN_BATCH
+#define ZTC_MINB_BCN_BATCH ZTC_MINB_BCN
+#endif
 #ifndef ZTC_MINB_ASTC_SINGLE
 #define ZTC_MINB_ASTC_SINGLE 5
 #endif
