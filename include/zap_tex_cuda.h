@@ -200,6 +200,24 @@ ZTC_API int zap_tex_cuda_batch_run_plain(zap_tex_cuda_batch *batch, void *stream
 ZTC_API int zap_tex_cuda_batch_info(zap_tex_cuda_batch *batch, char *buf, size_t cap);
 ZTC_API int zap_tex_cuda_batch_destroy(zap_tex_cuda_batch *batch);
 
+/* ---------------------------------------------------------------- texture containers (the CLI's tex, zap.c:309-355)
+   zap_tex_cuda_dds_header: the header zap.c:344-349 writes before the levels: "DDS " and 124 bytes, plus the 20-byte
+   DX10 extension for BC7 or sRGB (148 bytes in all). fmt ZTC_BC1..ZTC_BC7; mips != 0 declares the full chain; srgb
+   picks the _SRGB DXGI code and is ignored for BC4/BC5 (zap.c:325). hdr holds 148 bytes; *hdr_bytes (optional)
+   receives 128 or 148. Host only: no device work.
+   zap_tex_cuda_astc_header: the 16-byte .astc header of zap.c:312-321 (4x4x1 blocks, 24-bit sizes, depth 1).
+   With zap_tex_cuda_batch_item_bytes, a batch caller writes each item's header and then its dst.
+   zap_tex_cuda_tex_file: the whole file `zap tex [-f fmt] [-r rdo] [-m] [-S] w h in out` writes, computed on the
+   device: the header, then every level's blocks, largest first (level l + 1 is zap_mip_next of level l, in linear
+   light with srgb; each level is one zap_bc_encode call, so rdo > 0 runs one chain per level). fmt ZTC_ASTC4X4
+   gives the .astc file (one level; mips, srgb and rdo are ignored, as by the CLI). rgba and out are host memory;
+   out holds zap_tex_cuda_tex_file_bytes(w, h, fmt, mips, srgb) bytes (out_cap is checked); synchronous. */
+ZTC_API int zap_tex_cuda_dds_header(int w, int h, int fmt, int mips, int srgb, void *hdr, size_t *hdr_bytes);
+ZTC_API int zap_tex_cuda_astc_header(int w, int h, void *hdr);
+ZTC_API size_t zap_tex_cuda_tex_file_bytes(int w, int h, int fmt, int mips, int srgb);
+ZTC_API int zap_tex_cuda_tex_file(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo,
+                                  int mips, int srgb, void *out, size_t out_cap);
+
 /* Allocation-free BC7 encode. No counterpart in the reference (zap_tex.h allocates nothing because it runs on the
    CPU); it exists for callers that cannot allocate device memory when they encode: work recorded into a CUDA
    graph, real-time frame loops, engines with a fixed up-front GPU budget, plug-in hosts that only hand over their

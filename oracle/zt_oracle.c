@@ -1579,3 +1579,71 @@ void zo_mip_next_f(const float *src, int w, int h, size_t stride, float *dst, si
                              src[(size_t)y1 * stride + (size_t)x0 * 4 + c] + src[(size_t)y1 * stride + (size_t)x1 * 4 + c]);
         }
 }
+
+/* ================================================================== texture containers (zap.c:309-355, the CLI's tex)
+ * .astc: 16-byte header (magic 5CA1AB13 little-endian, block 4x4x1, 24-bit sizes, depth 1) then one level of ASTC blocks
+ * (zap.c:312-321). DDS: "DDS " + 124-byte header; the 20-byte DX10 extension follows for BC7 and for sRGB (zap.c:344-349);
+ * then every level's blocks, largest first. BC4/BC5 are never sRGB (zap.c:325). */
+static void put32(uint8_t *p, uint32_t v) { for (int k = 0; k < 4; k++) p[k] = (uint8_t)(v >> (8 * k)); }
+
+size_t zo_dds_header(int w, int h, int fmt, int mips, int srgb, uint8_t hdr[148]) {
+    static const char *fourcc[5] = { "DXT1", "DXT5", "BC4U", "BC5U", "DX10" };
+    static const uint32_t dxgi_unorm[5] = { 71, 77, 80, 83, 98 };
+    if (fmt == ZO_BC4 || fmt == ZO_BC5) srgb = 0;
+    int dx10 = fmt == ZO_BC7 || srgb != 0, levels = mips ? zo_mip_levels(w, h) : 1;
+    memset(hdr, 0, 148);
+    memcpy(hdr, "DDS ", 4);
+    put32(hdr + 4, 124);
+    put32(hdr + 8, 0x1u | 0x2u | 0x4u | 0x1000u | 0x80000u | (mips ? 0x20000u : 0u)); /* CAPS HEIGHT WIDTH PIXELFORMAT LINEARSIZE (MIPMAPCOUNT) */
+    put32(hdr + 12, (uint32_t)h);
+    put32(hdr + 16, (uint32_t)w);
+    put32(hdr + 20, (uint32_t)zo_bc_size(w, h, fmt));
+    put32(hdr + 28, (uint32_t)levels);
+    put32(hdr + 76, 32);   /* pixel format size */
+    put32(hdr + 80, 0x4);  /* FOURCC */
+    memcpy(hdr + 84, dx10 ? "DX10" : fourcc[fmt], 4);
+    put32(hdr + 108, 0x1000u | (mips ? 0x400008u : 0u));
+    if (!dx10) return 128;
+    put32(hdr + 128, dxgi_unorm[fmt] + (srgb ? 1u : 0u)); /* the _SRGB code follows each UNORM one */
+    put32(hdr + 132, 3);   /* TEXTURE2D */
+    put32(hdr + 140, 1);   /* array size */
+    return 148;
+}
+
+void zo_astc_header(int w, int h, uint8_t hdr[16]) {
+    static const uint8_t head[7] = { 0x13, 0xAB, 0xA1, 0x5C, 4, 4, 1 };
+    memset(hdr, 0, 16);
+    memcpy(hdr, head, 7);
+    for (int k = 0; k < 3; k++) { hdr[7 + k] = (uint8_t)(w >> (8 * k)); hdr[10 + k] = (uint8_t)(h >> (8 * k)); }
+    hdr[13] = 1;
+}
+
+/* the whole file `zap tex` writes; fmt 6 = .astc; out == NULL returns the size only */
+size_t zo_tex_file(const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo, int mips, int srgb, uint8_t *out) {
+    if (fmt == 6) {
+        size_t bn = zo_bc_size(w, h, ZO_BC7);
+        if (out) { zo_astc_header(w, h, out); zo_astc_encode(rgba, w, h, stride, out + 16); }
+        return 16 + bn;
+    }
+    if (fmt == ZO_BC4 || fmt == ZO_BC5) srgb = 0;
+    uint8_t hdr[148];
+    size_t hn = zo_dds_header(w, h, fmt, mips, srgb, hdr), total = 0;
+    int levels = mips ? zo_mip_levels(w, h) : 1;
+    for (int l = 0, lw = w, lh = h; l < levels; l++, lw = lw > 1 ? lw / 2 : 1, lh = lh > 1 ? lh / 2 : 1) total += zo_bc_size(lw, lh, fmt);
+    if (!out) return hn + total;
+    memcpy(out, hdr, hn);
+    uint8_t *p = out + hn, *img = (uint8_t *)malloc((size_t)w * h * 4), *next = (uint8_t *)malloc((size_t)w * h * 4 + 4);
+    for (int y = 0; y < h; y++) memcpy(img + (size_t)y * w * 4, rgba + (size_t)y * stride, (size_t)w * 4);
+    for (int l = 0, lw = w, lh = h; l < levels; l++) {
+        zo_bc_encode(img, lw, lh, (size_t)lw * 4, fmt, rdo, p);
+        p += zo_bc_size(lw, lh, fmt);
+        if (l + 1 < levels) {
+            int nw = lw > 1 ? lw / 2 : 1, nh = lh > 1 ? lh / 2 : 1;
+            zo_mip_next(img, lw, lh, (size_t)lw * 4, srgb, next, (size_t)nw * 4);
+            lw = nw; lh = nh;
+            memcpy(img, next, (size_t)lw * lh * 4);
+        }
+    }
+    free(img); free(next);
+    return hn + total;
+}

@@ -30,6 +30,12 @@ void zo_mip_next_f(const float *src, int w, int h, size_t stride, float *dst, si
 void zo_bc_split(const void *bc, size_t n, int fmt, void *out);                                   /* :1567 */
 void zo_bc_merge(const void *planes, size_t n, int fmt, void *out);                               /* :1568 */
 
+/* the CLI's texture containers (zap.c:309-355): DDS header (returns 128 or 148 bytes), .astc header, and the whole
+   file `zap tex [-f fmt] [-r rdo] [-m] [-S] w h in out` writes (fmt 6 = .astc; out NULL returns the size only) */
+size_t zo_dds_header(int w, int h, int fmt, int mips, int srgb, uint8_t hdr[148]);
+void zo_astc_header(int w, int h, uint8_t hdr[16]);
+size_t zo_tex_file(const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo, int mips, int srgb, uint8_t *out);
+
 /* internals pinned by the reference's self-test (tex_bench.c:47-48, :104-125) */
 uint16_t zo_f2h(float f);
 float zo_h2f(uint16_t h);

@@ -43,6 +43,16 @@ def golden():
 
 
 @pytest.fixture(scope="session")
+def golden_containers():
+    """Files the reference CLI's `zap tex` wrote (tests/golden/make_containers.py): key -> (image, args, bytes)."""
+    import numpy as np
+    path = os.path.join(TESTS, "golden", "golden_containers.npz")
+    with np.load(path) as z:
+        return {k[5:]: (z["img/" + str(z["image/" + k[5:]])], tuple(z["args/" + k[5:]]), z[k])
+                for k in z.files if k.startswith("file/")}
+
+
+@pytest.fixture(scope="session")
 def cuda_lib():
     """The product library on a real device; GPU tests only."""
     import torch

@@ -61,6 +61,9 @@ class Oracle:
             self._fn("astc_partition", [i, i, i, i], C.c_int)
             self._fn("ise_roundtrip", [i, i, vp, vp], C.c_int)
             self._fn("srgb_tables", [vp, vp], None)
+            self._fn("dds_header", [i, i, i, i, i, vp], sz)
+            self._fn("astc_header", [i, i, vp], None)
+            self._fn("tex_file", [vp, i, i, sz, i, f, i, i, vp], sz)
         else:
             self._fn("astc_part", [i, i, i, i], C.c_int)
             self._fn("srgb_lin", [], C.POINTER(C.c_float))
@@ -104,6 +107,25 @@ class Oracle:
             self._astc_encode_mt(img.ctypes.data, w, h, w * 4, out.ctypes.data, threads)
         else:
             self._astc_encode(img.ctypes.data, w, h, w * 4, out.ctypes.data)
+        return out
+
+    # ---- the CLI's containers (zap.c:309-355; restatement only)
+    def dds_header(self, w, h, fmt, mips, srgb):
+        hdr = np.zeros(148, np.uint8)
+        n = self._dds_header(w, h, fmt, int(mips), int(srgb), hdr.ctypes.data)
+        return hdr[:n]
+
+    def astc_header(self, w, h):
+        hdr = np.zeros(16, np.uint8)
+        self._astc_header(w, h, hdr.ctypes.data)
+        return hdr
+
+    def tex_file(self, img, fmt, rdo=0.0, mips=0, srgb=0):
+        img = np.ascontiguousarray(img)
+        h, w = img.shape[:2]
+        n = self._tex_file(img.ctypes.data, w, h, w * 4, fmt, float(rdo), int(mips), int(srgb), None)
+        out = np.zeros(n, np.uint8)
+        self._tex_file(img.ctypes.data, w, h, w * 4, fmt, float(rdo), int(mips), int(srgb), out.ctypes.data)
         return out
 
     # ---- decoders

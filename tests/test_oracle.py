@@ -234,3 +234,36 @@ def test_rdo_nonpositive_lambda_is_the_plain_encode(oracle):
     img = np.random.default_rng(2).integers(0, 256, (20, 24, 4), dtype=np.uint8)
     for fmt in (BC1, BC7):
         assert np.array_equal(oracle.bc_encode(img, fmt, rdo=-5.0), oracle.bc_encode(img, fmt))
+
+
+def test_container_files_match_reference_cli(oracle, golden_containers):
+    """The restated `zap tex` (zap.c:309-355) against the files the reference CLI wrote: DDS with and without the DX10
+    extension, sRGB codes, BC4/BC5 never sRGB, full mip chains down to 1x1, rdo per level, the one-level .astc file."""
+    assert len(golden_containers) == 17
+    for key, (img, (fmt, rdo, mips, srgb), want) in golden_containers.items():
+        got = oracle.tex_file(img, int(fmt), rdo, int(mips), int(srgb))
+        assert np.array_equal(got, want), key
+        h, w = img.shape[:2]
+        if int(fmt) == 6:
+            assert np.array_equal(oracle.astc_header(w, h), want[:16]), key
+        else:
+            hdr = oracle.dds_header(w, h, int(fmt), int(mips), int(srgb))
+            assert hdr.size in (128, 148) and np.array_equal(hdr, want[:hdr.size]), key
+
+
+def test_dds_header_fields(oracle):
+    """Field values of zap.c:344-349 for one case per branch, read back as little-endian words."""
+    def words(hdr):
+        return np.frombuffer(hdr.tobytes(), "<u4")
+    h = oracle.dds_header(4096, 2048, 4, 1, 1)
+    wd = words(h)
+    assert h.size == 148 and bytes(h[:4]) == b"DDS " and wd[1] == 124
+    assert wd[3] == 2048 and wd[4] == 4096 and wd[5] == 4096 * 2048 and wd[7] == 13
+    assert wd[2] == 0x1 | 0x2 | 0x4 | 0x1000 | 0x80000 | 0x20000 and wd[27] == 0x401008
+    assert bytes(h[84:88]) == b"DX10" and wd[32] == 99 and wd[33] == 3 and wd[35] == 1
+    h = oracle.dds_header(5, 3, 2, 0, 1)  # BC4: sRGB ignored, no DX10 extension
+    wd = words(h)
+    assert h.size == 128 and bytes(h[84:88]) == b"BC4U" and wd[7] == 1 and wd[2] == 0x81007 and wd[27] == 0x1000
+    assert oracle.dds_header(8, 8, 0, 0, 1).size == 148 and words(oracle.dds_header(8, 8, 0, 0, 1))[32] == 72
+    a = oracle.astc_header(0x123456, 0x10203)
+    assert list(a) == [0x13, 0xAB, 0xA1, 0x5C, 4, 4, 1, 0x56, 0x34, 0x12, 0x03, 0x02, 0x01, 1, 0, 0]

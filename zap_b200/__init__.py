@@ -21,7 +21,8 @@ FORMAT_NAMES = {BC1: "bc1", BC3: "bc3", BC4: "bc4", BC5: "bc5", BC7: "bc7", BC6H
 
 __all__ = ["BC1", "BC3", "BC4", "BC5", "BC7", "BC6H", "ASTC4X4", "ZapTexError", "build", "load", "bc_size", "block_bytes",
            "mip_levels", "bc_encode", "bc6h_encode", "astc_encode", "mip_next", "mip_next_f", "bc_encode_dev",
-           "bc6h_encode_dev", "astc_encode_dev", "mip_next_dev", "mip_next_f_dev", "mip_chain_dev"]
+           "bc6h_encode_dev", "astc_encode_dev", "mip_next_dev", "mip_next_f_dev", "mip_chain_dev", "dds_header",
+           "astc_header", "tex_file"]
 
 
 def trace(enable=True):
@@ -258,6 +259,35 @@ def astc_decode_dev(bc, w, h, stream=None, ctx=None):
     out = torch.empty((h, w, 4), dtype=torch.uint8, device=bc.device)
     check(load().zap_tex_cuda_astc_decode_dev(ctx, bc.data_ptr(), w, h, out.data_ptr(), w * 4, _stream(stream)), "astc_decode_dev")
     return out
+
+
+def dds_header(w, h, fmt, mips=False, srgb=False):
+    """The DDS header the CLI's tex command writes (zap.c:344-349): 128 or 148 bytes (DX10 extension) as numpy uint8."""
+    hdr = np.zeros(148, np.uint8)
+    n = C.c_size_t(0)
+    check(load().zap_tex_cuda_dds_header(w, h, fmt, int(mips), int(srgb), hdr.ctypes.data, C.byref(n)), "dds_header")
+    return hdr[:n.value]
+
+
+def astc_header(w, h):
+    """The 16-byte .astc header of zap.c:312-321."""
+    hdr = np.zeros(16, np.uint8)
+    check(load().zap_tex_cuda_astc_header(w, h, hdr.ctypes.data), "astc_header")
+    return hdr
+
+
+def tex_file(img, fmt, rdo=0.0, mips=False, srgb=False, ctx=None):
+    """The whole file `zap tex` writes (zap.c:309-355), mip chain and blocks computed on the device: HxWx4 uint8 numpy
+    image (rows may be padded) -> numpy uint8 file bytes (DDS for BC1..BC7, .astc for ASTC4X4)."""
+    img = np.asarray(img, dtype=np.uint8)
+    if img.strides[1:] != (4, 1):
+        img = np.ascontiguousarray(img)
+    h, w = img.shape[:2]
+    n = load().zap_tex_cuda_tex_file_bytes(w, h, fmt, int(mips), int(srgb))
+    out = np.empty(max(n, 1), np.uint8)
+    check(load().zap_tex_cuda_tex_file(ctx, img.ctypes.data, w, h, img.strides[0], fmt, float(rdo), int(mips), int(srgb),
+                                        out.ctypes.data, n), "tex_file")
+    return out[:n]
 
 
 def bc_decode(bc, w, h, fmt, ctx=None):

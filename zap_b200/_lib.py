@@ -86,6 +86,10 @@ def _declare(lib):
         "zap_tex_cuda_batch_run_plain": ([vp, vp], i),
         "zap_tex_cuda_batch_info": ([vp, C.c_char_p, sz], i),
         "zap_tex_cuda_batch_destroy": ([vp], i),
+        "zap_tex_cuda_dds_header": ([i, i, i, i, i, vp, C.POINTER(sz)], i),
+        "zap_tex_cuda_astc_header": ([i, i, vp], i),
+        "zap_tex_cuda_tex_file_bytes": ([i, i, i, i, i], sz),
+        "zap_tex_cuda_tex_file": ([vp, vp, i, i, sz, i, f, i, i, vp, sz], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
