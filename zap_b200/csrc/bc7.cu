@@ -89,19 +89,19 @@ ZTC_DEV int subset_fit(TexRef ts, uint32_t mask, int n, bool shared_p, const flo
     return palette_fit<NC, IB>(ts, mask, x0, x1, idx);
 }
 
-// PCA start, fit, up to two least-squares refits (zap_tex.h:489-515). t: the texels in registers (for the
-// principal axis), ts: the same texels for the rolled loops.
+// Passes [first, last) of a subset's fit sequence (zap_tex.h:489-515): pass 0 fits the endpoints (lo, hi); pass
+// k > 0 is the k-th least-squares refit on the indices `idx` holds, which does not run at SSE 0, stops at a
+// singular system, and is dropped (ending the sequence) when it does not lower the SSE. err: the SSE before
+// `first`; q, pb, idx take each accepted pass. Returns the SSE; more: all the passes ran and the SSE is still
+// above 0, so pass `last` would run. One fit call site keeps the code small.
 template <int NC, int IB>
-ZTC_DEV int subset_encode(const uint32_t t[16], TexRef ts, uint32_t mask, int n, bool shared_p, int q[2][4], int pb[2],
-                          uint64_t &idx) {
-    float lo[4], hi[4];
-    pca_endpoints<NC>(t, mask, lo, hi);
-    int err = 0;
-    // pass 0 fits the PCA endpoints; passes 1 and 2 are the least-squares refits, which stop at SSE 0, at a
-    // singular system or at the first one that does not lower the SSE. One fit call site keeps the code small.
+ZTC_DEV int subset_passes(TexRef ts, uint32_t mask, int n, bool shared_p, float lo[4], float hi[4], int first, int last, int err,
+                          int q[2][4], int pb[2], uint64_t &idx, bool &more) {
+    more = false;
     #pragma unroll 1
-    for (int it = 0; it < 3; it++) {
+    for (int it = first; it < last; it++) {
         if (it > 0) {
+            if (err <= 0) return err;
             float aa = 0.0f, ab = 0.0f, bb = 0.0f, sa[NC], sb[NC];
             #pragma unroll
             for (int c = 0; c < NC; c++) { sa[c] = 0.0f; sb[c] = 0.0f; }
@@ -115,7 +115,7 @@ ZTC_DEV int subset_encode(const uint32_t t[16], TexRef ts, uint32_t mask, int n,
                 for (int c = 0; c < NC; c++) { float xc = (float)chan(x, c); sa[c] = sa[c] + u * xc; sb[c] = sb[c] + w * xc; }
             }
             float det = aa * bb - ab * ab;
-            if (det < 1e-6f && det > -1e-6f) break;
+            if (det < 1e-6f && det > -1e-6f) return err;
             #pragma unroll
             for (int c = 0; c < 4; c++) {
                 if (c < NC) { lo[c] = clamp255((sa[c] * bb - sb[c] * ab) / det); hi[c] = clamp255((sb[c] * aa - sa[c] * ab) / det); }
@@ -125,21 +125,31 @@ ZTC_DEV int subset_encode(const uint32_t t[16], TexRef ts, uint32_t mask, int n,
         int nq[2][4], npb[2];
         uint64_t ni;
         const int ne = subset_fit<NC, IB>(ts, mask, n, shared_p, lo, hi, nq, npb, ni);
-        if (it > 0 && ne >= err) break;
+        if (it > 0 && ne >= err) return err;
         err = ne; idx = ni; pb[0] = npb[0]; pb[1] = npb[1];
         #pragma unroll
         for (int c = 0; c < 4; c++) { q[0][c] = nq[0][c]; q[1][c] = nq[1][c]; }
-        if (err <= 0) break;
     }
+    more = err > 0;
     return err;
 }
 
+// PCA start, fit, up to two least-squares refits (zap_tex.h:489-515). t: the texels in registers (for the
+// principal axis), ts: the same texels for the rolled loops.
+template <int NC, int IB>
+ZTC_DEV int subset_encode(const uint32_t t[16], TexRef ts, uint32_t mask, int n, bool shared_p, int q[2][4], int pb[2],
+                          uint64_t &idx) {
+    float lo[4], hi[4];
+    pca_endpoints<NC>(t, mask, lo, hi);
+    bool more;
+    return subset_passes<NC, IB>(ts, mask, n, shared_p, lo, hi, 0, 3, 0, q, pb, idx, more);
+}
+
 // ---------------------------------------------------------------- kernel A: mode 6 for every block
-ZTC_DEV int mode6_encode(const uint32_t t[16], TexRef ts, uint4 &blk) {  // zap_tex.h:520-527, 582-593
-    int q[2][4], pb[2];
-    uint64_t idx;
-    int err = subset_encode<4, 4>(t, ts, 0xFFFFu, 8, false, q, pb, idx);
-    if (idx & 8u) {  // anchor index MSB must be 0: swap endpoints and p-bits, invert indices (15 - i == i ^ 15)
+// mode-6 block from its fields (zap_tex.h:520-527): the anchor index's MSB must be 0, else the endpoints and
+// p-bits swap and the indices invert (15 - i == i ^ 15)
+ZTC_DEV uint4 pack_mode6_block(int q[2][4], int pb[2], uint64_t idx) {
+    if (idx & 8u) {
         #pragma unroll
         for (int c = 0; c < 4; c++) { int s = q[0][c]; q[0][c] = q[1][c]; q[1][c] = s; }
         int s = pb[0]; pb[0] = pb[1]; pb[1] = s;
@@ -153,25 +163,91 @@ ZTC_DEV int mode6_encode(const uint32_t t[16], TexRef ts, uint4 &blk) {  // zap_
     o.put((uint32_t)(idx & 7u), 3);
     #pragma unroll
     for (int i = 1; i < 16; i++) o.put((uint32_t)((idx >> (4 * i)) & 15u), 4);
-    blk = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
+    return make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
+}
+
+ZTC_DEV int mode6_encode(const uint32_t t[16], TexRef ts, uint4 &blk) {  // zap_tex.h:582-593
+    int q[2][4], pb[2];
+    uint64_t idx;
+    int err = subset_encode<4, 4>(t, ts, 0xFFFFu, 8, false, q, pb, idx);
+    blk = pack_mode6_block(q, pb, idx);
     return err;
+}
+
+// endpoints (7 bits each, endpoint-major) and p-bits of a mode-6 fit in one word
+ZTC_DEV uint64_t pack_qp(const int q[2][4], const int pb[2]) {
+    uint64_t v = (uint64_t)pb[0] << 56 | (uint64_t)pb[1] << 57;
+    #pragma unroll
+    for (int k = 0; k < 8; k++) v |= (uint64_t)q[k >> 2][k & 3] << (7 * k);
+    return v;
+}
+ZTC_DEV void unpack_qp(uint64_t v, int q[2][4], int pb[2]) {
+    #pragma unroll
+    for (int k = 0; k < 8; k++) q[k >> 2][k & 3] = (int)((v >> (7 * k)) & 0x7Fu);
+    pb[0] = (int)((v >> 56) & 1u); pb[1] = (int)((v >> 57) & 1u);
+}
+
+// Mode 6 for the CTA's blocks, one per thread, with the second least-squares refit compacted. Every thread runs
+// the PCA, the first fit and the first refit of its block; the blocks whose second refit would run (about a fifth
+// of them on photographic content, yet nearly every warp holds one) are listed in shared memory, and the first
+// threads of the CTA run those refits on the owners' texels, so they cost about a fifth of the warps instead of
+// nearly all. Same bytes and SSE as mode6_encode. Every thread of the CTA calls it (it synchronises); a `valid`
+// thread's block is in t and in column threadIdx.x of s_tex.
+template <int CTA>
+__device__ __forceinline__ int mode6_encode_cta(bool valid, const uint32_t t[16], uint32_t (*s_tex)[CTA], uint4 &blk) {
+    static_assert(CTA % 32 == 0 && CTA <= 256, "whole warps, owners fit a byte");
+    __shared__ uint64_t s_idx[CTA], s_qp[CTA];
+    __shared__ int s_err[CTA], s_wcnt[CTA / 32];
+    __shared__ uint8_t s_list[CTA];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float lo[4], hi[4];
+    if (valid) pca_endpoints<4>(t, 0xFFFFu, lo, hi);
+    bool active = valid;
+    int owner = tid, first = 0, err = 0;
+    uint64_t idx = 0;
+    #pragma unroll 1
+    for (int round = 0; round < 2; round++) {
+        int q[2][4], pb[2];
+        bool more = false;
+        const int e_in = err;
+        if (active)
+            err = subset_passes<4, 4>(TexRef{&s_tex[0][owner], CTA}, 0xFFFFu, 8, false, lo, hi, first, round ? 3 : 2, err, q, pb, idx, more);
+        if (active && (round == 0 || err < e_in)) { s_err[owner] = err; s_idx[owner] = idx; s_qp[owner] = pack_qp(q, pb); }
+        if (round == 1) break;
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, more);
+        if (lane == 0) s_wcnt[warp] = __popc(bal);
+        __syncthreads();
+        int base = 0, total = 0;
+        #pragma unroll
+        for (int w = 0; w < CTA / 32; w++) { const int c = s_wcnt[w]; base += w < warp ? c : 0; total += c; }
+        if (more) s_list[base + __popc(bal & ((1u << lane) - 1u))] = (uint8_t)tid;
+        __syncthreads();
+        active = tid < total;
+        if (active) { owner = s_list[tid]; err = s_err[owner]; idx = s_idx[owner]; }
+        first = 2;
+    }
+    __syncthreads();
+    if (!valid) return 0;
+    int q[2][4], pb[2];
+    unpack_qp(s_qp[tid], q, pb);
+    blk = pack_mode6_block(q, pb, s_idx[tid]);
+    return s_err[tid];
 }
 
 __global__ void __launch_bounds__(128, ZTC_MINB_BC7_MODE6) bc7_mode6_kernel(SrcU8 src, int bw, int by0, int nblocks, BlockOut out, size_t b0,
                                                         uint32_t *__restrict__ count, uint2 *__restrict__ items) {
-    __shared__ uint32_t s_tex[16][128];  // column threadIdx.x: this thread's block (read only by this thread)
+    __shared__ uint32_t s_tex[16][128];  // column threadIdx.x: this thread's block
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = b < nblocks;
-    int err = 0;
+    uint32_t t[16];
     if (valid) {
-        uint32_t t[16];
         gather_block(src, b % bw, by0 + b / bw, t);
         #pragma unroll
         for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
-        uint4 blk;
-        err = mode6_encode(t, TexRef{&s_tex[0][threadIdx.x], 128}, blk);
-        put_block16(out, b0 + (size_t)b, blk);
     }
+    uint4 blk;
+    const int err = mode6_encode_cta<128>(valid, t, s_tex, blk);
+    if (valid) put_block16(out, b0 + (size_t)b, blk);
     bool hard = valid && err > 16 * 4;  // zap_tex.h:758 early exit
     unsigned ballot = __ballot_sync(0xFFFFFFFFu, hard);
     if (ballot) {
@@ -559,7 +635,7 @@ __global__ void __launch_bounds__(CTA, ZTC_MINB_BC7_MODE6 * 128 / CTA)
 batch_bc7_mode6_kernel(const BatchLevel *__restrict__ levels, const BatchTile *__restrict__ tiles, int ntiles,
                        uint32_t *__restrict__ counter, uint32_t *__restrict__ hard_count, uint2 *__restrict__ hard_items) {
     __shared__ int s_tile;
-    __shared__ uint32_t s_tex[16][CTA];  // column threadIdx.x: this thread's block (read only by this thread)
+    __shared__ uint32_t s_tex[16][CTA];  // column threadIdx.x: this thread's block
     for (;;) {
         if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
         __syncthreads();
@@ -570,17 +646,16 @@ batch_bc7_mode6_kernel(const BatchLevel *__restrict__ levels, const BatchTile *_
         const BatchLevel L = levels[T.level];
         const int b = T.first + (int)threadIdx.x;
         const bool valid = (int)threadIdx.x < T.count;
-        int err = 0;
+        uint32_t t[16];
         if (valid) {
             const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
-            uint32_t t[16];
             gather_block(src, b % L.bw, b / L.bw, t);
             #pragma unroll
             for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
-            uint4 blk;
-            err = mode6_encode(t, TexRef{&s_tex[0][threadIdx.x], CTA}, blk);
-            store_block16(L.dst + (size_t)b * 16, blk);
         }
+        uint4 blk;
+        const int err = mode6_encode_cta<CTA>(valid, t, s_tex, blk);
+        if (valid) store_block16(L.dst + (size_t)b * 16, blk);
         const bool hard = valid && err > 16 * 4;  // zap_tex.h:758 early exit
         const unsigned ballot = __ballot_sync(0xFFFFFFFFu, hard);
         if (ballot) {
