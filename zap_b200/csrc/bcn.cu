@@ -69,21 +69,42 @@ ZTC_DEV int bc1_try(const Bc1Texels &T, uint32_t &c0, uint32_t &c1, uint32_t &id
 
 ZTC_DEV float bc1_lsw(uint32_t k) { return k == 0 ? 1.0f : k == 1 ? 0.0f : k == 2 ? 2.0f / 3.0f : 1.0f / 3.0f; }
 
-// quality search (zap_tex.h:97-168)
-ZTC_DEV uint2 bc1_encode(const uint32_t t[16]) {
-    Bc1Texels T;
-    bc1_prepare(t, T);
+// +-1 climb passes [first, last) over the six 565 channels of the two endpoints, first improvement taken
+// immediately (zap_tex.h:146-165); the climb stops early at SSE 0 or after a pass without improvement. Returns
+// whether the last pass that ran improved.
+ZTC_DEV bool bc1_climb(const Bc1Texels &T, uint32_t &b0, uint32_t &b1, uint32_t &bidx, int &best, int first, int last) {
+    bool improved = true;
+    for (int pass = first; improved && pass < last && best > 0; pass++) {
+        improved = false;
+        for (int step = 0; step < 12; step++) {
+            int ep = step / 6, ch = (step / 2) % 3, d = (step & 1) ? 1 : -1;
+            int sh = ch == 0 ? 11 : ch == 1 ? 5 : 0, mx = ch == 1 ? 63 : 31;
+            uint32_t c = ep ? b1 : b0;
+            int f = (int)(c >> sh) & mx;
+            if (f + d < 0 || f + d > mx) continue;
+            c = (c & ~((uint32_t)mx << sh)) | ((uint32_t)(f + d) << sh);
+            uint32_t n0 = ep ? b0 : c, n1 = ep ? c : b1, ni = 0;
+            int ne = bc1_try(T, n0, n1, ni);
+            if (ne < best) { best = ne; b0 = n0; b1 = n1; bidx = ni; improved = true; }
+        }
+    }
+    return improved;
+}
+
+// quality search up to the climb (zap_tex.h:97-145): PCA axis, two starts with least-squares refits (the colour
+// channels of T.p are the texels' r, g, b)
+ZTC_DEV void bc1_start(const Bc1Texels &T, uint32_t &b0, uint32_t &b1, uint32_t &bidx, int &best) {
     float mu0 = 0.0f, mu1 = 0.0f, mu2 = 0.0f;
     #pragma unroll
     for (int i = 0; i < 16; i++) {
-        mu0 = mu0 + (float)chan(t[i], 0) / 16.0f;
-        mu1 = mu1 + (float)chan(t[i], 1) / 16.0f;
-        mu2 = mu2 + (float)chan(t[i], 2) / 16.0f;
+        mu0 = mu0 + (float)chan(T.p[i], 0) / 16.0f;
+        mu1 = mu1 + (float)chan(T.p[i], 1) / 16.0f;
+        mu2 = mu2 + (float)chan(T.p[i], 2) / 16.0f;
     }
     float C0 = 0, C1 = 0, C2 = 0, C3 = 0, C4 = 0, C5 = 0;
     #pragma unroll
     for (int i = 0; i < 16; i++) {
-        float r = (float)chan(t[i], 0) - mu0, g = (float)chan(t[i], 1) - mu1, b = (float)chan(t[i], 2) - mu2;
+        float r = (float)chan(T.p[i], 0) - mu0, g = (float)chan(T.p[i], 1) - mu1, b = (float)chan(T.p[i], 2) - mu2;
         C0 = C0 + r * r; C1 = C1 + r * g; C2 = C2 + r * b; C3 = C3 + g * g; C4 = C4 + g * b; C5 = C5 + b * b;
     }
     float v0 = 1.0f, v1 = 1.0f, v2 = 1.0f;
@@ -100,12 +121,12 @@ ZTC_DEV uint2 bc1_encode(const uint32_t t[16]) {
     float n2 = v0 * v0 + v1 * v1 + v2 * v2, tmin = 1e9f, tmax = -1e9f;
     #pragma unroll
     for (int i = 0; i < 16; i++) {
-        float s = ((float)chan(t[i], 0) - mu0) * v0 + ((float)chan(t[i], 1) - mu1) * v1 + ((float)chan(t[i], 2) - mu2) * v2;
+        float s = ((float)chan(T.p[i], 0) - mu0) * v0 + ((float)chan(T.p[i], 1) - mu1) * v1 + ((float)chan(T.p[i], 2) - mu2) * v2;
         if (s < tmin) tmin = s;
         if (s > tmax) tmax = s;
     }
-    uint32_t b0 = 0, b1 = 0, bidx = 0;
-    int best = 1 << 30;
+    b0 = 0; b1 = 0; bidx = 0;
+    best = 1 << 30;
     for (int start = 0; start < 2; start++) {
         float inset = start ? 0.0f : (tmax - tmin) / 16.0f, lo = (tmin + inset) / n2, hi = (tmax - inset) / n2;
         uint32_t c0 = pack565(mu0 + v0 * hi, mu1 + v1 * hi, mu2 + v2 * hi);
@@ -118,7 +139,7 @@ ZTC_DEV uint2 bc1_encode(const uint32_t t[16]) {
             for (int i = 0; i < 16; i++) {
                 float wa = bc1_lsw((idx >> (2 * i)) & 3u), wb = 1.0f - wa;
                 aa = aa + wa * wa; ab = ab + wa * wb; bb = bb + wb * wb;
-                float r = (float)chan(t[i], 0), g = (float)chan(t[i], 1), b = (float)chan(t[i], 2);
+                float r = (float)chan(T.p[i], 0), g = (float)chan(T.p[i], 1), b = (float)chan(T.p[i], 2);
                 sa0 = sa0 + wa * r; sa1 = sa1 + wa * g; sa2 = sa2 + wa * b;
                 sb0 = sb0 + wb * r; sb1 = sb1 + wb * g; sb2 = sb2 + wb * b;
             }
@@ -133,23 +154,67 @@ ZTC_DEV uint2 bc1_encode(const uint32_t t[16]) {
         }
         if (e < best) { best = e; b0 = c0; b1 = c1; bidx = idx; }
     }
-    // +-1 climb over the six 565 channels of the two endpoints, first improvement taken immediately
-    bool improved = true;
-    for (int pass = 0; improved && pass < 8 && best > 0; pass++) {
-        improved = false;
-        for (int step = 0; step < 12; step++) {
-            int ep = step / 6, ch = (step / 2) % 3, d = (step & 1) ? 1 : -1;
-            int sh = ch == 0 ? 11 : ch == 1 ? 5 : 0, mx = ch == 1 ? 63 : 31;
-            uint32_t c = ep ? b1 : b0;
-            int f = (int)(c >> sh) & mx;
-            if (f + d < 0 || f + d > mx) continue;
-            c = (c & ~((uint32_t)mx << sh)) | ((uint32_t)(f + d) << sh);
-            uint32_t n0 = ep ? b0 : c, n1 = ep ? c : b1, ni = 0;
-            int ne = bc1_try(T, n0, n1, ni);
-            if (ne < best) { best = ne; b0 = n0; b1 = n1; bidx = ni; improved = true; }
+}
+
+// quality search (zap_tex.h:97-168), one thread
+ZTC_DEV uint2 bc1_encode(const uint32_t t[16]) {
+    Bc1Texels T;
+    bc1_prepare(t, T);
+    uint32_t b0, b1, bidx;
+    int best;
+    bc1_start(T, b0, b1, bidx, best);
+    bc1_climb(T, b0, b1, bidx, best, 0, 8);
+    return make_uint2(b0 | (b1 << 16), bidx);
+}
+
+// The quality search for the CTA's blocks, one per thread, with the climb past its second pass compacted. Every
+// thread runs the starts and the first two climb passes of its block; the blocks whose climb goes on (about a
+// tenth on photographic content, yet nearly every warp holds one) are listed in shared memory, and the first
+// threads of the CTA climb them on to the end from the owners' texels, so the long tail of the climb costs about
+// a tenth of the warps. Same bytes as bc1_encode. Every thread of the CTA calls it (it synchronises); a `valid`
+// thread's block is in t and in column threadIdx.x of s_tex.
+template <int CTA>
+__device__ __forceinline__ uint2 bc1_encode_cta(bool valid, const uint32_t t[16], uint32_t (*s_tex)[CTA]) {
+    static_assert(CTA % 32 == 0 && CTA <= 256, "whole warps, owners fit a byte");
+    __shared__ uint32_t s_ends[CTA], s_idx[CTA];
+    __shared__ int s_best[CTA], s_wcnt[CTA / 32];
+    __shared__ uint8_t s_list[CTA];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    Bc1Texels T;
+    uint32_t b0 = 0, b1 = 0, bidx = 0;
+    int best = 0;
+    if (valid) {
+        bc1_prepare(t, T);
+        bc1_start(T, b0, b1, bidx, best);
+    }
+    bool active = valid;
+    int owner = tid;
+    #pragma unroll 1
+    for (int round = 0; round < 2; round++) {
+        bool more = false;
+        if (active) more = bc1_climb(T, b0, b1, bidx, best, round ? 2 : 0, round ? 8 : 2) && best > 0;
+        if (active) { s_ends[owner] = b0 | (b1 << 16); s_idx[owner] = bidx; s_best[owner] = best; }
+        if (round == 1) break;
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, more);
+        if (lane == 0) s_wcnt[warp] = __popc(bal);
+        __syncthreads();
+        int base = 0, total = 0;
+        #pragma unroll
+        for (int w = 0; w < CTA / 32; w++) { const int c = s_wcnt[w]; base += w < warp ? c : 0; total += c; }
+        if (more) s_list[base + __popc(bal & ((1u << lane) - 1u))] = (uint8_t)tid;
+        __syncthreads();
+        active = tid < total;
+        if (active) {
+            owner = s_list[tid];
+            uint32_t u[16];
+            #pragma unroll
+            for (int i = 0; i < 16; i++) u[i] = s_tex[i][owner];
+            bc1_prepare(u, T);
+            b0 = s_ends[owner] & 0xFFFFu; b1 = s_ends[owner] >> 16; bidx = s_idx[owner]; best = s_best[owner];
         }
     }
-    return make_uint2(b0 | (b1 << 16), bidx);
+    __syncthreads();
+    return make_uint2(s_ends[tid], s_idx[tid]);
 }
 
 // ---------------------------------------------------------------- BC4 (zap_tex.h:170-213)
@@ -189,19 +254,29 @@ ZTC_DEV uint2 bc4_encode(const uint32_t t[16], int c) {
 // ---------------------------------------------------------------- kernel: one thread per block
 template <int FMT>
 __global__ void __launch_bounds__(128, ZTC_MINB_BCN) bcn_kernel(SrcU8 src, int bw, int by0, int nblocks, BlockOut out, size_t b0) {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nblocks) return;
-    int bx = b % bw, by = by0 + b / bw;
+    constexpr bool kColour = FMT == ZTC_FMT_BC1 || FMT == ZTC_FMT_BC3;
+    __shared__ uint32_t s_tex[16][kColour ? 128 : 1];  // column threadIdx.x: this thread's block (BC1 / BC3)
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = b < nblocks;
+    if (!kColour && !valid) return;  // BC4 / BC5 never synchronise
     uint32_t t[16];
-    gather_block(src, bx, by, t);
+    if (valid) {
+        gather_block(src, b % bw, by0 + b / bw, t);
+        if (kColour) {
+            #pragma unroll
+            for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
+        }
+    }
     const size_t ob = b0 + (size_t)b;  // the block's index in the output
     if (FMT == ZTC_FMT_BC1) {
-        put_block8(out, ob, bc1_encode(t));
+        const uint2 c = bc1_encode_cta<128>(valid, t, (uint32_t(*)[128])s_tex);
+        if (valid) put_block8(out, ob, c);
     } else if (FMT == ZTC_FMT_BC4) {
         put_block8(out, ob, bc4_encode(t, 0));
     } else if (FMT == ZTC_FMT_BC3) {
-        uint2 a = bc4_encode(t, 3), c = bc1_encode(t);
-        put_block16(out, ob, make_uint4(a.x, a.y, c.x, c.y));
+        uint2 a = valid ? bc4_encode(t, 3) : make_uint2(0u, 0u);
+        const uint2 c = bc1_encode_cta<128>(valid, t, (uint32_t(*)[128])s_tex);
+        if (valid) put_block16(out, ob, make_uint4(a.x, a.y, c.x, c.y));
     } else {  // BC5
         uint2 r = bc4_encode(t, 0), g = bc4_encode(t, 1);
         put_block16(out, ob, make_uint4(r.x, r.y, g.x, g.y));
@@ -236,7 +311,9 @@ namespace ztc {
 template <int FMT, int CTA>
 __global__ void __launch_bounds__(CTA, ZTC_MINB_BCN_BATCH * 128 / CTA) batch_bcn_kernel(const BatchLevel *__restrict__ levels, const BatchTile *__restrict__ tiles,
                                                         int ntiles, uint32_t *__restrict__ counter) {
+    constexpr bool kColour = FMT == ZTC_FMT_BC1 || FMT == ZTC_FMT_BC3;
     __shared__ int s_tile;
+    __shared__ uint32_t s_tex[16][kColour ? CTA : 1];  // column threadIdx.x: this thread's block (BC1 / BC3)
     for (;;) {
         if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
         __syncthreads();
@@ -244,17 +321,27 @@ __global__ void __launch_bounds__(CTA, ZTC_MINB_BCN_BATCH * 128 / CTA) batch_bcn
         __syncthreads();  // every thread has read s_tile before thread 0 overwrites it
         if (tile >= ntiles) break;
         const BatchTile T = tiles[tile];
-        if ((int)threadIdx.x >= T.count) continue;
+        const bool valid = (int)threadIdx.x < T.count;
+        if (!kColour && !valid) continue;  // BC4 / BC5 never synchronise inside a tile
         const BatchLevel L = levels[T.level];
         const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
         const int b = T.first + (int)threadIdx.x;
         uint32_t t[16];
-        gather_block(src, b % L.bw, b / L.bw, t);
-        if (FMT == ZTC_FMT_BC1) store_block8(L.dst + (size_t)b * 8, bc1_encode(t));
-        else if (FMT == ZTC_FMT_BC4) store_block8(L.dst + (size_t)b * 8, bc4_encode(t, 0));
+        if (valid) {
+            gather_block(src, b % L.bw, b / L.bw, t);
+            if (kColour) {
+                #pragma unroll
+                for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
+            }
+        }
+        if (FMT == ZTC_FMT_BC1) {
+            const uint2 c = bc1_encode_cta<CTA>(valid, t, (uint32_t(*)[CTA])s_tex);
+            if (valid) store_block8(L.dst + (size_t)b * 8, c);
+        } else if (FMT == ZTC_FMT_BC4) store_block8(L.dst + (size_t)b * 8, bc4_encode(t, 0));
         else if (FMT == ZTC_FMT_BC3) {
-            uint2 a = bc4_encode(t, 3), c = bc1_encode(t);
-            store_block16(L.dst + (size_t)b * 16, make_uint4(a.x, a.y, c.x, c.y));
+            const uint2 a = valid ? bc4_encode(t, 3) : make_uint2(0u, 0u);
+            const uint2 c = bc1_encode_cta<CTA>(valid, t, (uint32_t(*)[CTA])s_tex);
+            if (valid) store_block16(L.dst + (size_t)b * 16, make_uint4(a.x, a.y, c.x, c.y));
         } else {
             uint2 r = bc4_encode(t, 0), g = bc4_encode(t, 1);
             store_block16(L.dst + (size_t)b * 16, make_uint4(r.x, r.y, g.x, g.y));
