@@ -433,6 +433,214 @@ __global__ void __launch_bounds__(kChainThreads) rdo_chain_kernel(SrcU8 src, int
     }
 }
 
+// ---------------------------------------------------------------- BC7: one lane per texel
+// A BC7 candidate costs a whole palette search or least-squares solve, so this chain spreads each candidate over a
+// 16-lane group: lane i takes texel i (and window slot i when the rate is counted). 25 warps = 50 groups:
+// groups 0-15 kind 1 (neighbour j = group + 1: its endpoints, refit indices), 16-31 kind 2 (its indices, refit
+// endpoints), 32-47 kind 0 (the whole neighbour), 48 the base, 49 loads the next block. Every chosen block enters
+// the window with its decoded texels and, for mode 6, its palette and indices, so no candidate decodes a block:
+// kind 0 compares the texels with the stored decode, kind 1 searches the stored palette. The base encodings are
+// decoded for every block by a parallel pass before the chains. Kind 2's least-squares sums are exact in the
+// reference's float accumulation (weights k/64, texels integers: every partial sum is a multiple of 1/4096 below
+// 2^17 of them), so they are reduced as integers and scaled, which gives the same floats in any order.
+constexpr int kB7Warps = 25, kB7Threads = kB7Warps * 32;
+
+__device__ __forceinline__ int grp_sum(int v, unsigned gm) {
+    #pragma unroll
+    for (int m = 8; m >= 1; m >>= 1) v += __shfl_xor_sync(gm, v, m, 16);
+    return v;
+}
+__device__ __forceinline__ uint64_t grp_or64(uint64_t v, unsigned gm) {
+    #pragma unroll
+    for (int m = 8; m >= 1; m >>= 1) {
+        const uint32_t lo = __shfl_xor_sync(gm, (uint32_t)v, m, 16), hi = __shfl_xor_sync(gm, (uint32_t)(v >> 32), m, 16);
+        v |= ((uint64_t)hi << 32) | lo;
+    }
+    return v;
+}
+ZTC_DEV int sq4px(uint32_t a, uint32_t b) {  // squared RGBA difference (zap__sq4 over 4 channels)
+    int s = 0;
+    #pragma unroll
+    for (int c = 0; c < 4; c++) { const int d = (int)chan(a, c) - (int)chan(b, c); s += d * d; }
+    return s;
+}
+ZTC_DEV uint32_t lerp_px(const int x0[4], const int x1[4], int w) {
+    return pack_rgba(lerp64(x0[0], x1[0], w), lerp64(x0[1], x1[1], w), lerp64(x0[2], x1[2], w), lerp64(x0[3], x1[3], w));
+}
+// mode 6 bit layout: mode bits 0-6, R0 R1 G0 G1 B0 B1 A0 A1 (7 bits each) from bit 7, P0 bit 63, P1 bit 64, then
+// the indices (texel 0: 3 bits, the others 4) from bit 65
+ZTC_DEV void mode6_ends_of(uint64_t lo, uint64_t hi, int x0[4], int x1[4]) {  // expanded endpoints
+    const int p0 = (int)(lo >> 63), p1 = (int)(hi & 1u);
+    #pragma unroll
+    for (int c = 0; c < 4; c++) {
+        x0[c] = (int)(((lo >> (7 + 14 * c)) & 0x7Fu) << 1) | p0;
+        x1[c] = (int)(((lo >> (14 + 14 * c)) & 0x7Fu) << 1) | p1;
+    }
+}
+ZTC_DEV uint64_t mode6_idx_of(uint64_t hi) { return ((hi >> 1) & 7u) | (hi & ~0xFull); }  // 4 bits per texel
+ZTC_DEV uint64_t mode6_hi(int p1, uint64_t idx) { return (uint64_t)p1 | ((idx & 7u) << 1) | (idx & ~0xFull); }
+
+// the base encodings of blocks [0, nblocks), decoded: 16 texels per block
+__global__ void __launch_bounds__(128) bc7_decode_bases_kernel(const uint8_t *__restrict__ blocks, int nblocks, uint4 *__restrict__ dec) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblocks) return;
+    const uint4 v = *(const uint4 *)(blocks + (size_t)b * 16);
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+    uint32_t px[16];
+    dec::bc7_block(w, px);
+    #pragma unroll
+    for (int k = 0; k < 4; k++) dec[(size_t)b * 4 + k] = make_uint4(px[4 * k], px[4 * k + 1], px[4 * k + 2], px[4 * k + 3]);
+}
+
+__global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src, int bw, int nby, int chain_rows, uint8_t *__restrict__ out,
+                                                                      const uint32_t *__restrict__ dec_base, float lambda) {
+    __shared__ uint64_t ring[kWindow][2];       // the last 16 chosen blocks, slot = block & 15
+    __shared__ uint32_t ring_dec[kWindow][16];  // their decoded texels
+    __shared__ uint32_t ring_pal[kWindow][16];  // mode 6: their palettes
+    __shared__ uint64_t ring_idx[kWindow];      // mode 6: their indices, 4 bits per texel
+    __shared__ uint32_t s_tex[2][16], s_dbase[2][16];
+    __shared__ uint64_t s_base[2][2];
+    __shared__ uint64_t s_key[kB7Warps];
+    __shared__ int s_dist[2];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, i = lane & 15, grp = tid >> 4;
+    const int kind = grp < 16 ? 1 : grp < 32 ? 2 : grp < 48 ? 0 : grp == 48 ? -1 : -2, j = (grp & 15) + 1;
+    // warps 0-23 run one kind in both halves; warp 24 splits into the base and the loader
+    const unsigned gm = warp == kB7Warps - 1 ? 0xFFFFu << (lane & 16) : 0xFFFFFFFFu;
+    const int row0 = blockIdx.x * chain_rows, rows = min(chain_rows, nby - row0);
+    if (rows <= 0) return;
+    const int first = row0 * bw, count = rows * bw;
+    if (kind == -2) {
+        s_tex[0][i] = load_texel(src, min((first % bw) * 4 + (i & 3), src.w - 1), min((first / bw) * 4 + (i >> 2), src.h - 1));
+        s_dbase[0][i] = dec_base[(size_t)first * 16 + i];
+        if (i < 2) s_base[0][i] = *(const uint64_t *)(out + (size_t)first * 16 + 8 * i);
+    }
+    if (tid == 0) { s_dist[0] = 1; s_dist[1] = 1; }
+    __syncthreads();
+    for (int cur = 0; cur < count; cur++) {
+        const int g = first + cur, slot = cur & 1, d0 = s_dist[0], d1 = s_dist[1];
+        uint64_t key = ~0ull, clo = 0, chi = 0, cidx = 0;
+        uint32_t dec = 0, pal = 0;
+        int nd0 = 0, nd1 = 0;
+        if (kind >= -1) {
+            const uint32_t t = s_tex[slot][i];
+            const int r = (cur - j) & (kWindow - 1);
+            bool ok;
+            int e;
+            if (kind == -1) {  // the base (its SSE: the one the reference's encoder returns)
+                clo = s_base[slot][0]; chi = s_base[slot][1];
+                dec = s_dbase[slot][i];
+                e = grp_sum(sq4px(t, dec), gm);
+                int x0[4], x1[4];
+                mode6_ends_of(clo, chi, x0, x1);
+                pal = lerp_px(x0, x1, w4(i));
+                cidx = mode6_idx_of(chi);
+                ok = true;
+            } else if (kind == 0) {  // the whole neighbour (zap__bc7_err)
+                clo = ring[r][0]; chi = ring[r][1];
+                dec = ring_dec[r][i]; pal = ring_pal[r][i]; cidx = ring_idx[r];
+                e = grp_sum(sq4px(t, dec), gm);
+                ok = j <= cur;
+            } else if (kind == 1) {  // its endpoints, best indices; texel 0 keeps to 0..7 (zap__bc7_fit6_idx)
+                const uint64_t nlo = ring[r][0], nhi = ring[r][1];
+                ok = j <= cur && is_mode6(nlo);
+                pal = ring_pal[r][i];
+                int m = 0x7FFFFFFF;
+                #pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    const uint32_t pk = ring_pal[r][k];
+                    const int kk = 16 * ((int)dot4(pk, pk) - 2 * (int)dot4(t, pk)) + k;
+                    if ((i || k < 8) && kk < m) { m = kk; dec = pk; }
+                }
+                e = grp_sum((m >> 4) + (int)dot4(t, t), gm);
+                cidx = grp_or64((uint64_t)(m & 15) << (4 * i), gm);
+                clo = nlo; chi = mode6_hi((int)(nhi & 1u), cidx);
+            } else {  // its indices, least-squares endpoints, each endpoint's own p-bit (zap__bc7_fit6_ep)
+                const uint64_t nlo = ring[r][0], nhi = ring[r][1];
+                ok = j <= cur && is_mode6(nlo);
+                cidx = ring_idx[r];
+                const int w = w4((int)((cidx >> (4 * i)) & 15u)), u = 64 - w;
+                const int AA = grp_sum(u * u, gm), AB = grp_sum(u * w, gm), BB = grp_sum(w * w, gm);
+                const int ch = i & 3, ep = (i >> 2) & 1, p = i >> 3;
+                // this lane's channel sums: the four channels' sums reduced side by side, then picked
+                int SA = 0, SB = 0;
+                #pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const int sa = grp_sum(u * (int)chan(t, c), gm), sb = grp_sum(w * (int)chan(t, c), gm);
+                    if (c == ch) { SA = sa; SB = sb; }
+                }
+                const float aa = (float)AA / 4096.0f, ab = (float)AB / 4096.0f, bb = (float)BB / 4096.0f;
+                const float ax = (float)SA / 64.0f, bx = (float)SB / 64.0f, det = aa * bb - ab * ab;
+                float v;
+                if (det < 1e-6f && det > -1e-6f) v = (ax + bx) / 16.0f;  // one index everywhere: flat
+                else v = ep ? (bx * aa - ax * ab) / det : (ax * bb - bx * ab) / det;
+                v = clamp255(v);
+                // lane (channel, endpoint, p-bit): zap__bc7q for one channel, 7 bits + p
+                const int gq = f2i_x86((v / 255.0f * 255.0f - (float)p) / 2.0f + 0.5f);
+                int bq = 0, be = 1 << 30;
+                #pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const int tq = clampi(around(gq, k), 0, 127);
+                    const float d = (float)((tq << 1) | p) - v;
+                    const int ek = f2i_x86(d * d);
+                    if (ek < be) { be = ek; bq = tq; }
+                }
+                int s4 = be + __shfl_xor_sync(gm, be, 1, 16);
+                s4 += __shfl_xor_sync(gm, s4, 2, 16);
+                const int e00 = __shfl_sync(gm, s4, 0, 16), e01 = __shfl_sync(gm, s4, 8, 16);
+                const int e10 = __shfl_sync(gm, s4, 4, 16), e11 = __shfl_sync(gm, s4, 12, 16);
+                const int pb0 = e01 < e00 ? 1 : 0, pb1 = e11 < e10 ? 1 : 0;
+                int x0[4], x1[4];
+                uint64_t lo = 0x40u | ((uint64_t)pb0 << 63);
+                #pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const int q0 = __shfl_sync(gm, bq, pb0 * 8 + c, 16), q1 = __shfl_sync(gm, bq, pb1 * 8 + 4 + c, 16);
+                    x0[c] = (q0 << 1) | pb0; x1[c] = (q1 << 1) | pb1;
+                    lo |= ((uint64_t)q0 << (7 + 14 * c)) | ((uint64_t)q1 << (14 + 14 * c));
+                }
+                dec = lerp_px(x0, x1, w);
+                e = grp_sum(sq4px(t, dec), gm);
+                pal = lerp_px(x0, x1, w4(i));
+                clo = lo; chi = (nhi & ~1ull) | (uint64_t)pb1;
+            }
+            // rate (zap__bc7_rate): lane i compares the candidate's fields with window slot j' = i + 1
+            const int rw = (cur - i - 1) & (kWindow - 1);
+            const bool vw = i + 1 <= cur;
+            const uint64_t wlo = ring[rw][0], whi = ring[rw][1];
+            const unsigned sh = lane & 16;
+            const unsigned mA = (__ballot_sync(gm, vw && wlo == clo) >> sh) & 0xFFFFu;
+            const unsigned mB = (__ballot_sync(gm, vw && (whi >> 8) == (chi >> 8)) >> sh) & 0xFFFFu;
+            float fa = 8.0f, fb = 7.0f;
+            nd0 = d0; nd1 = d1;
+            if (d0 > 0 && d0 <= cur && ((mA >> (d0 - 1)) & 1u)) fa = 0.0f;
+            else if (mA) { nd0 = __ffs((int)mA); fa = 3.0f; }
+            if (d1 > 0 && d1 <= cur && ((mB >> (d1 - 1)) & 1u)) fb = 0.0f;
+            else if (mB) { nd1 = __ffs((int)mB); fb = 3.0f; }
+            if (ok) key = key_of((float)e + lambda * (fa + fb + 1.0f), kind < 0 ? 0 : (j - 1) * 3 + kind + 1);
+        } else if (cur + 1 < count) {  // the loader: the next block's texels, decoded base and base
+            const int gn = g + 1, ns = slot ^ 1;
+            s_tex[ns][i] = load_texel(src, min((gn % bw) * 4 + (i & 3), src.w - 1), min((gn / bw) * 4 + (i >> 2), src.h - 1));
+            s_dbase[ns][i] = dec_base[(size_t)gn * 16 + i];
+            if (i < 2) s_base[ns][i] = *(const uint64_t *)(out + (size_t)gn * 16 + 8 * i);
+        }
+        const uint64_t wk = warp_min(key);
+        if (lane == 0) s_key[warp] = wk;
+        __syncthreads();
+        const int order = (int)(uint32_t)warp_min(lane < kB7Warps ? s_key[lane] : ~0ull);
+        const int oc = order - 1, wkind = oc % 3, wgrp = order == 0 ? 48 : wkind == 1 ? oc / 3 : wkind == 2 ? 16 + oc / 3 : 32 + oc / 3;
+        if (grp == wgrp) {  // the winner enters the window
+            const int ws = cur & (kWindow - 1);
+            ring_dec[ws][i] = dec;
+            ring_pal[ws][i] = pal;
+            if (i == 0) {
+                ring[ws][0] = clo; ring[ws][1] = chi; ring_idx[ws] = cidx;
+                s_dist[0] = nd0; s_dist[1] = nd1;
+                if (order != 0) { *(uint64_t *)(out + (size_t)g * 16) = clo; *(uint64_t *)(out + (size_t)g * 16 + 8) = chi; }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 }  // namespace ztc
 
@@ -444,6 +652,17 @@ cudaError_t ztc_launch_rdo(int fmt, const ztc::SrcU8 &src, uint8_t *out, float l
     const int chains = (nby + band_rows - 1) / band_rows;
     ztc::TraceScope tr("rdo_chain", stream);
     ztc::trace_units((long)bw * nby);
+    if (fmt == ZTC_FMT_BC7) {
+        const int nblocks = bw * nby;
+        uint32_t *dec = nullptr;
+        cudaError_t e = cudaMallocAsync((void **)&dec, (size_t)nblocks * 64, stream);
+        if (e != cudaSuccess) return e;
+        ztc::bc7_decode_bases_kernel<<<(nblocks + 127) / 128, 128, 0, stream>>>(out, nblocks, (uint4 *)dec);
+        ztc::rdo_bc7_chain_kernel<<<chains, ztc::kB7Threads, 0, stream>>>(src, bw, nby, band_rows, out, dec, lambda);
+        e = cudaGetLastError();
+        cudaFreeAsync(dec, stream);
+        return e;
+    }
     switch (fmt) {
     case ZTC_FMT_BC1: ztc::rdo_chain_kernel<ZTC_FMT_BC1><<<chains, ztc::kChainThreads, 0, stream>>>(src, bw, nby, band_rows, out, lambda); break;
     case ZTC_FMT_BC3: ztc::rdo_chain_kernel<ZTC_FMT_BC3><<<chains, ztc::kChainThreads, 0, stream>>>(src, bw, nby, band_rows, out, lambda); break;
