@@ -43,9 +43,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
-    p.add_argument("--profile", default=None, choices=["bc7", "bc1", "bc4", "bc5", "bc6h", "astc", "batch", "rdo"],
+    p.add_argument("--profile", default=None, choices=["bc7", "bc1", "bc4", "bc5", "bc6h", "astc", "batch", "rdo", "rdo7"],
                    help="profiling case: only that encoder on a ring of 2048x2048 inputs, no e2e / CPU / extras "
-                        "(rdo: BC1 at lambda 30, one chain over a 256x256 texture per step)")
+                        "(rdo / rdo7: BC1 / BC7 at lambda 30, one chain over a 256x256 texture per step)")
     return p.parse_args()
 
 
@@ -68,10 +68,11 @@ def run_profile_case(args):
                           "Mpix_s": args.steps * b.pixels / 1e6 / (ms / 1e3)}))
         b.close()
         return
-    if fmt == "rdo":  # one serial chain per step: zap_bc_encode(BC1, rdo 30) of a 256x256 texture
+    if fmt in ("rdo", "rdo7"):  # one serial chain per step: zap_bc_encode(BC1 or BC7, rdo 30) of a 256x256 texture
         tex = S.colour_texture(256, 256, seed=7, alpha="noise", device=dev)
-        out = zap_b200.bc_encode_rdo_dev(tex, zap_b200.BC1, 30.0)
-        ms = time_device(lambda k: zap_b200.bc_encode_rdo_dev(tex, zap_b200.BC1, 30.0, out=out), args.steps, args.warmup, 1)
+        code = zap_b200.BC1 if fmt == "rdo" else zap_b200.BC7
+        out = zap_b200.bc_encode_rdo_dev(tex, code, 30.0)
+        ms = time_device(lambda k: zap_b200.bc_encode_rdo_dev(tex, code, 30.0, out=out), args.steps, args.warmup, 1)
         print(json.dumps({"profile_case": fmt, "steps": args.steps, "ms_per_step": ms / args.steps,
                           "Mpix_s": args.steps * 256 * 256 / 1e6 / (ms / 1e3)}))
         return

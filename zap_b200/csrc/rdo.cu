@@ -445,18 +445,45 @@ __global__ void __launch_bounds__(kChainThreads) rdo_chain_kernel(SrcU8 src, int
 // 2^17 of them), so they are reduced as integers and scaled, which gives the same floats in any order.
 constexpr int kB7Warps = 25, kB7Threads = kB7Warps * 32;
 
+// Group collectives over a 16-lane group: gm names the caller's half-warp (each half of a warp passes its own
+// mask, as 16-thread tiles do). ZTC_RDO_REDUX selects redux.sync (1) or xor-shuffle trees (0) for the sums and ORs;
+// ZTC_RDO_MIN_REDUX the same for the warp-wide key minimum.
+#ifndef ZTC_RDO_REDUX
+#define ZTC_RDO_REDUX 0
+#endif
+#ifndef ZTC_RDO_MIN_REDUX
+#define ZTC_RDO_MIN_REDUX 1
+#endif
 __device__ __forceinline__ int grp_sum(int v, unsigned gm) {
+#if ZTC_RDO_REDUX
+    return __reduce_add_sync(gm, v);
+#else
     #pragma unroll
     for (int m = 8; m >= 1; m >>= 1) v += __shfl_xor_sync(gm, v, m, 16);
     return v;
+#endif
 }
 __device__ __forceinline__ uint64_t grp_or64(uint64_t v, unsigned gm) {
+#if ZTC_RDO_REDUX
+    return ((uint64_t)__reduce_or_sync(gm, (uint32_t)(v >> 32)) << 32) | __reduce_or_sync(gm, (uint32_t)v);
+#else
     #pragma unroll
     for (int m = 8; m >= 1; m >>= 1) {
         const uint32_t lo = __shfl_xor_sync(gm, (uint32_t)v, m, 16), hi = __shfl_xor_sync(gm, (uint32_t)(v >> 32), m, 16);
         v |= ((uint64_t)hi << 32) | lo;
     }
     return v;
+#endif
+}
+// warp-wide minimum of 64-bit keys
+__device__ __forceinline__ uint64_t warp_min_redux(uint64_t k) {
+#if ZTC_RDO_MIN_REDUX  // the high words' minimum, then the low words' among the lanes holding it
+    const uint32_t hi = __reduce_min_sync(0xFFFFFFFFu, (uint32_t)(k >> 32));
+    const uint32_t lo = __reduce_min_sync(0xFFFFFFFFu, (uint32_t)(k >> 32) == hi ? (uint32_t)k : 0xFFFFFFFFu);
+    return ((uint64_t)hi << 32) | lo;
+#else
+    return warp_min(k);
+#endif
 }
 ZTC_DEV int sq4px(uint32_t a, uint32_t b) {  // squared RGBA difference (zap__sq4 over 4 channels)
     int s = 0;
@@ -492,32 +519,44 @@ __global__ void __launch_bounds__(128) bc7_decode_bases_kernel(const uint8_t *__
     for (int k = 0; k < 4; k++) dec[(size_t)b * 4 + k] = make_uint4(px[4 * k], px[4 * k + 1], px[4 * k + 2], px[4 * k + 3]);
 }
 
+// the loader group's work for block gk: its texels, decoded base, base and channel sums into slot ns
+__device__ __forceinline__ void load_bc7_block(const SrcU8 &src, int bw, const uint8_t *out, const uint32_t *dec_base, int gk, int ns, int i,
+                                               unsigned gm, uint32_t (*s_tex)[16], uint32_t (*s_dbase)[16], uint64_t (*s_base)[2],
+                                               int (*s_sumx)[4]) {
+    const uint32_t t = load_texel(src, min((gk % bw) * 4 + (i & 3), src.w - 1), min((gk / bw) * 4 + (i >> 2), src.h - 1));
+    s_tex[ns][i] = t;
+    s_dbase[ns][i] = dec_base[(size_t)gk * 16 + i];
+    if (i < 2) s_base[ns][i] = *(const uint64_t *)(out + (size_t)gk * 16 + 8 * i);
+    #pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int sx = grp_sum((int)chan(t, c), gm);
+        if (i == c) s_sumx[ns][c] = sx;
+    }
+}
+
 __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src, int bw, int nby, int chain_rows, uint8_t *__restrict__ out,
                                                                       const uint32_t *__restrict__ dec_base, float lambda) {
     __shared__ uint64_t ring[kWindow][2];       // the last 16 chosen blocks, slot = block & 15
     __shared__ uint32_t ring_dec[kWindow][16];  // their decoded texels
     __shared__ uint32_t ring_pal[kWindow][16];  // mode 6: their palettes
     __shared__ uint64_t ring_idx[kWindow];      // mode 6: their indices, 4 bits per texel
-    __shared__ uint32_t s_tex[2][16], s_dbase[2][16];
-    __shared__ uint64_t s_base[2][2];
+    __shared__ uint32_t s_tex[3][16], s_dbase[3][16];  // block cur in slot cur % 3, loaded two blocks ahead
+    __shared__ uint64_t s_base[3][2];
+    __shared__ int s_sumx[3][4];                       // the block's channel sums
     __shared__ uint64_t s_key[kB7Warps];
     __shared__ int s_dist[2];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, i = lane & 15, grp = tid >> 4;
     const int kind = grp < 16 ? 1 : grp < 32 ? 2 : grp < 48 ? 0 : grp == 48 ? -1 : -2, j = (grp & 15) + 1;
-    // warps 0-23 run one kind in both halves; warp 24 splits into the base and the loader
-    const unsigned gm = warp == kB7Warps - 1 ? 0xFFFFu << (lane & 16) : 0xFFFFFFFFu;
+    const unsigned gm = 0xFFFFu << (lane & 16);  // this lane's group
     const int row0 = blockIdx.x * chain_rows, rows = min(chain_rows, nby - row0);
     if (rows <= 0) return;
     const int first = row0 * bw, count = rows * bw;
-    if (kind == -2) {
-        s_tex[0][i] = load_texel(src, min((first % bw) * 4 + (i & 3), src.w - 1), min((first / bw) * 4 + (i >> 2), src.h - 1));
-        s_dbase[0][i] = dec_base[(size_t)first * 16 + i];
-        if (i < 2) s_base[0][i] = *(const uint64_t *)(out + (size_t)first * 16 + 8 * i);
-    }
+    if (kind == -2)
+        for (int k = 0; k < 2 && k < count; k++) load_bc7_block(src, bw, out, dec_base, first + k, k, i, gm, s_tex, s_dbase, s_base, s_sumx);
     if (tid == 0) { s_dist[0] = 1; s_dist[1] = 1; }
     __syncthreads();
     for (int cur = 0; cur < count; cur++) {
-        const int g = first + cur, slot = cur & 1, d0 = s_dist[0], d1 = s_dist[1];
+        const int g = first + cur, slot = cur % 3, d0 = s_dist[0], d1 = s_dist[1];
         uint64_t key = ~0ull, clo = 0, chi = 0, cidx = 0;
         uint32_t dec = 0, pal = 0;
         int nd0 = 0, nd1 = 0;
@@ -558,16 +597,18 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src,
                 const uint64_t nlo = ring[r][0], nhi = ring[r][1];
                 ok = j <= cur && is_mode6(nlo);
                 cidx = ring_idx[r];
-                const int w = w4((int)((cidx >> (4 * i)) & 15u)), u = 64 - w;
-                const int AA = grp_sum(u * u, gm), AB = grp_sum(u * w, gm), BB = grp_sum(w * w, gm);
+                const int w = w4((int)((cidx >> (4 * i)) & 15u));
                 const int ch = i & 3, ep = (i >> 2) & 1, p = i >> 3;
-                // this lane's channel sums: the four channels' sums reduced side by side, then picked
-                int SA = 0, SB = 0;
+                // with u = 64 - w: sum u^2 = 16 * 4096 - 128 sum w + sum w^2, sum u w = 64 sum w - sum w^2,
+                // sum u x = 64 sum x - sum w x; sum w (<= 1024) and sum w^2 (<= 65536) share one word
+                const int W12 = grp_sum((w * w) << 11 | w, gm), W1 = W12 & 0x7FF, W2 = W12 >> 11;
+                int SB = 0;
                 #pragma unroll
                 for (int c = 0; c < 4; c++) {
-                    const int sa = grp_sum(u * (int)chan(t, c), gm), sb = grp_sum(w * (int)chan(t, c), gm);
-                    if (c == ch) { SA = sa; SB = sb; }
+                    const int sb = grp_sum(w * (int)chan(t, c), gm);
+                    if (c == ch) SB = sb;
                 }
+                const int AA = 16 * 4096 - 128 * W1 + W2, AB = 64 * W1 - W2, BB = W2, SA = 64 * s_sumx[slot][ch] - SB;
                 const float aa = (float)AA / 4096.0f, ab = (float)AB / 4096.0f, bb = (float)BB / 4096.0f;
                 const float ax = (float)SA / 64.0f, bx = (float)SB / 64.0f, det = aa * bb - ab * ab;
                 float v;
@@ -616,16 +657,13 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src,
             if (d1 > 0 && d1 <= cur && ((mB >> (d1 - 1)) & 1u)) fb = 0.0f;
             else if (mB) { nd1 = __ffs((int)mB); fb = 3.0f; }
             if (ok) key = key_of((float)e + lambda * (fa + fb + 1.0f), kind < 0 ? 0 : (j - 1) * 3 + kind + 1);
-        } else if (cur + 1 < count) {  // the loader: the next block's texels, decoded base and base
-            const int gn = g + 1, ns = slot ^ 1;
-            s_tex[ns][i] = load_texel(src, min((gn % bw) * 4 + (i & 3), src.w - 1), min((gn / bw) * 4 + (i >> 2), src.h - 1));
-            s_dbase[ns][i] = dec_base[(size_t)gn * 16 + i];
-            if (i < 2) s_base[ns][i] = *(const uint64_t *)(out + (size_t)gn * 16 + 8 * i);
+        } else if (cur + 2 < count) {  // the loader: the block after next
+            load_bc7_block(src, bw, out, dec_base, g + 2, (cur + 2) % 3, i, gm, s_tex, s_dbase, s_base, s_sumx);
         }
-        const uint64_t wk = warp_min(key);
+        const uint64_t wk = warp_min_redux(key);
         if (lane == 0) s_key[warp] = wk;
         __syncthreads();
-        const int order = (int)(uint32_t)warp_min(lane < kB7Warps ? s_key[lane] : ~0ull);
+        const int order = (int)(uint32_t)warp_min_redux(lane < kB7Warps ? s_key[lane] : ~0ull);
         const int oc = order - 1, wkind = oc % 3, wgrp = order == 0 ? 48 : wkind == 1 ? oc / 3 : wkind == 2 ? 16 + oc / 3 : 32 + oc / 3;
         if (grp == wgrp) {  // the winner enters the window
             const int ws = cur & (kWindow - 1);
@@ -636,6 +674,142 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src,
                 s_dist[0] = nd0; s_dist[1] = nd1;
                 if (order != 0) { *(uint64_t *)(out + (size_t)g * 16) = clo; *(uint64_t *)(out + (size_t)g * 16 + 8) = chi; }
             }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- BC1 / BC4 sub-blocks: one lane per texel
+// The BC7 chain's layout for one sub-block of a BC1-BC5 block: groups 0-15 kind 0 (neighbour j = group + 1: its
+// endpoints, fitted indices), 16-31 kind 1 (these endpoints, its indices), 32-47 kind 2 (the whole neighbour),
+// 48 the base, 49 loads the next block. The two sub-blocks of a BC3 or BC5 block are independent chains (each
+// looks only at its own fields of earlier blocks, with its own match distances, zap_tex.h:1494-1501), so each
+// runs in its own CTA (blockIdx.y) and writes its own 8 bytes of the blocks.
+ZTC_DEV void bc1_palette(uint32_t c0, uint32_t c1, int force4, uint32_t pal[4]) {  // entries as RGB texels
+    #pragma unroll
+    for (int k = 0; k < 4; k++) {
+        int r, g, b;
+        bc1_entry(c0, c1, force4, k, r, g, b);
+        pal[k] = pack_rgb(r, g, b);
+    }
+}
+ZTC_DEV int sq3px(uint32_t t, uint32_t p) {
+    int s = 0;
+    #pragma unroll
+    for (int c = 0; c < 3; c++) { const int d = (int)chan(t, c) - (int)chan(p, c); s += d * d; }
+    return s;
+}
+
+__global__ void __launch_bounds__(kB7Threads, 1) rdo_sub_chain_kernel(SrcU8 src, int bw, int nby, int chain_rows, uint8_t *__restrict__ out,
+                                                                      int bs, Sub S0, Sub S1, float lambda) {
+    __shared__ uint64_t ring[kWindow];  // the sub-block of the last 16 chosen blocks, slot = block & 15
+    __shared__ uint32_t s_tex[3][16];  // block cur in slot cur % 3, loaded two blocks ahead
+    __shared__ uint64_t s_base[3];
+    __shared__ uint64_t s_key[kB7Warps];
+    __shared__ int s_dist[2];
+    const Sub S = blockIdx.y ? S1 : S0;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, i = lane & 15, grp = tid >> 4;
+    const int kind = grp < 16 ? 0 : grp < 32 ? 1 : grp < 48 ? 2 : grp == 48 ? -1 : -2, j = (grp & 15) + 1;
+    const unsigned gm = 0xFFFFu << (lane & 16);  // this lane's group
+    const int row0 = blockIdx.x * chain_rows, rows = min(chain_rows, nby - row0);
+    if (rows <= 0) return;
+    const int first = row0 * bw, count = rows * bw;
+    if (kind == -2)
+        for (int k = 0; k < 2 && k < count; k++) {
+            const int gk = first + k;
+            s_tex[k][i] = load_texel(src, min((gk % bw) * 4 + (i & 3), src.w - 1), min((gk / bw) * 4 + (i >> 2), src.h - 1));
+            if (i == 0) s_base[k] = *(const uint64_t *)(out + (size_t)gk * bs + S.off);
+        }
+    if (tid == 0) { s_dist[0] = 1; s_dist[1] = 1; }
+    __syncthreads();
+    // fields: BC1 {c0 c1, indices} = {4, 4} bytes, BC4 {a0 a1, indices} = {2, 6}
+    const bool bc1 = S.type == kBc1;
+    const int nA = bc1 ? 4 : 2, nB = bc1 ? 4 : 6;
+    const uint64_t maskA = (1ull << (8 * nA)) - 1ull;
+    const float newA = bc1 ? 3.0f : 2.0f, newB = 3.0f;  // min(size, 3)
+    for (int cur = 0; cur < count; cur++) {
+        const int g = first + cur, slot = cur % 3, d0 = s_dist[0], d1 = s_dist[1];
+        uint64_t key = ~0ull, cand = 0;
+        int nd0 = 0, nd1 = 0;
+        if (kind >= -1) {
+            const uint32_t t = s_tex[slot][i];
+            const uint64_t base = s_base[slot], nb = ring[(cur - j) & (kWindow - 1)];
+            bool ok = kind == -1 || j <= cur;
+            int e;
+            if (bc1) {  // the CTA's sub-block type: uniform
+                const uint32_t p0 = (uint32_t)(nb & 0xFFFFu), p1 = (uint32_t)((nb >> 16) & 0xFFFFu);
+                // kind 1 and the base: these endpoints; kinds 0 and 2: the neighbour's
+                const uint32_t a = kind == 1 || kind == -1 ? (uint32_t)(base & 0xFFFFu) : p0;
+                const uint32_t b = kind == 1 || kind == -1 ? (uint32_t)((base >> 16) & 0xFFFFu) : p1;
+                uint32_t pal[4];
+                bc1_palette(a, b, S.force4, pal);
+                uint32_t idx;
+                if (kind == 0) {  // zap__bc1_fit: best of the 4 (3 in 3-colour order) entries, first on ties
+                    const int n = (S.force4 || a > b) ? 4 : 3;
+                    int bk = 0, be = sq3px(t, pal[0]);
+                    #pragma unroll
+                    for (int k = 1; k < 4; k++) {
+                        const int ek = sq3px(t, pal[k]);
+                        if (k < n && ek < be) { be = ek; bk = k; }
+                    }
+                    e = grp_sum(be, gm);
+                    idx = (uint32_t)grp_or64((uint64_t)bk << (2 * i), gm);
+                } else {  // zap__bc1_eval with the base's or the neighbour's indices
+                    idx = (uint32_t)((kind == -1 ? base : nb) >> 32);
+                    const int k = (int)((idx >> (2 * i)) & 3u);
+                    e = grp_sum(sq3px(t, k == 0 ? pal[0] : k == 1 ? pal[1] : k == 2 ? pal[2] : pal[3]), gm);
+                }
+                cand = (uint64_t)a | ((uint64_t)b << 16) | ((uint64_t)idx << 32);
+                // a 3-colour block may not use index 3 (transparent); the base is never checked
+                if (kind >= 0 && !S.force4 && a <= b && (idx & (idx >> 1) & 0x55555555u)) ok = false;
+            } else {
+                const int pa0 = (int)(nb & 0xFFu), pa1 = (int)((nb >> 8) & 0xFFu);
+                const int a = kind == 1 || kind == -1 ? (int)(base & 0xFFu) : pa0, b = kind == 1 || kind == -1 ? (int)((base >> 8) & 0xFFu) : pa1;
+                const int v = (int)chan(t, S.chan);
+                uint64_t idx;
+                if (kind == 0) {  // zap__bc4_fit
+                    int bk = 0, be = (v - bc4_entry(a, b, 0)) * (v - bc4_entry(a, b, 0));
+                    #pragma unroll
+                    for (int k = 1; k < 8; k++) {
+                        const int d = v - bc4_entry(a, b, k);
+                        if (d * d < be) { be = d * d; bk = k; }
+                    }
+                    e = grp_sum(be, gm);
+                    idx = grp_or64((uint64_t)bk << (3 * i), gm);
+                } else {  // zap__bc4_eval
+                    idx = (kind == -1 ? base : nb) >> 16;
+                    const int d = v - bc4_entry(a, b, (int)((idx >> (3 * i)) & 7u));
+                    e = grp_sum(d * d, gm);
+                }
+                cand = (uint64_t)a | ((uint64_t)b << 8) | (idx << 16);
+            }
+            // rate (zap__field_rate per field): lane i compares with window slot j' = i + 1
+            const uint64_t w = ring[(cur - i - 1) & (kWindow - 1)];
+            const bool vw = i + 1 <= cur;
+            const unsigned sh = lane & 16;
+            const unsigned mA = (__ballot_sync(gm, vw && (w & maskA) == (cand & maskA)) >> sh) & 0xFFFFu;
+            const unsigned mB = (__ballot_sync(gm, vw && (w >> (8 * nA)) == (cand >> (8 * nA))) >> sh) & 0xFFFFu;
+            float fa = (float)nA, fb = (float)nB;
+            nd0 = d0; nd1 = d1;
+            if (d0 > 0 && d0 <= cur && ((mA >> (d0 - 1)) & 1u)) fa = 0.0f;
+            else if (mA) { nd0 = __ffs((int)mA); fa = newA; }
+            if (d1 > 0 && d1 <= cur && ((mB >> (d1 - 1)) & 1u)) fb = 0.0f;
+            else if (mB) { nd1 = __ffs((int)mB); fb = newB; }
+            if (ok) key = key_of((float)e + lambda * (fa + fb), kind < 0 ? 0 : (j - 1) * 3 + kind + 1);
+        } else if (cur + 2 < count) {  // the loader: texels and base sub-block of the block after next
+            const int gn = g + 2, ns = (cur + 2) % 3;
+            s_tex[ns][i] = load_texel(src, min((gn % bw) * 4 + (i & 3), src.w - 1), min((gn / bw) * 4 + (i >> 2), src.h - 1));
+            if (i == 0) s_base[ns] = *(const uint64_t *)(out + (size_t)gn * bs + S.off);
+        }
+        const uint64_t wk = warp_min_redux(key);
+        if (lane == 0) s_key[warp] = wk;
+        __syncthreads();
+        const int order = (int)(uint32_t)warp_min_redux(lane < kB7Warps ? s_key[lane] : ~0ull);
+        const int oc = order - 1, wkind = oc % 3, wgrp = order == 0 ? 48 : wkind * 16 + oc / 3;
+        if (grp == wgrp && i == 0) {  // the winner enters the window
+            ring[cur & (kWindow - 1)] = cand;
+            s_dist[0] = nd0; s_dist[1] = nd1;
+            if (order != 0) *(uint64_t *)(out + (size_t)g * bs + S.off) = cand;
         }
         __syncthreads();
     }
@@ -662,6 +836,14 @@ cudaError_t ztc_launch_rdo(int fmt, const ztc::SrcU8 &src, uint8_t *out, float l
         e = cudaGetLastError();
         cudaFreeAsync(dec, stream);
         return e;
+    }
+    {
+        const ztc::Sub S0 = ztc::sub_of(fmt, 0), S1 = ztc::sub_of(fmt, 1);
+        const int ns = ztc::sub_count(fmt), bs = fmt == ZTC_FMT_BC1 || fmt == ZTC_FMT_BC4 ? 8 : 16;
+        const dim3 grid(chains, ns);
+        if (fmt < ZTC_FMT_BC1 || fmt > ZTC_FMT_BC5) return cudaErrorInvalidValue;
+        ztc::rdo_sub_chain_kernel<<<grid, ztc::kB7Threads, 0, stream>>>(src, bw, nby, band_rows, out, bs, S0, S1, lambda);
+        return cudaGetLastError();
     }
     switch (fmt) {
     case ZTC_FMT_BC1: ztc::rdo_chain_kernel<ZTC_FMT_BC1><<<chains, ztc::kChainThreads, 0, stream>>>(src, bw, nby, band_rows, out, lambda); break;
