@@ -475,6 +475,16 @@ __device__ __forceinline__ uint64_t grp_or64(uint64_t v, unsigned gm) {
     return v;
 #endif
 }
+// The mask a lane passes to its group's collectives: its half-warp, or (ZTC_RDO_FULL_MASK) the whole warp in
+// warps 0-23, whose two groups run the same kind of candidate and meet every collective together; warp 24
+// splits into the base and the loader, which run different code. Whole-warp masks measured faster on B200
+// (512x512 one chain: BC7 30.6 -> 28.3 ms, BC1 25.8 -> 25.5 ms).
+#ifndef ZTC_RDO_FULL_MASK
+#define ZTC_RDO_FULL_MASK 1
+#endif
+__device__ __forceinline__ unsigned group_mask(int warp, int lane) {
+    return ZTC_RDO_FULL_MASK && warp < 24 ? 0xFFFFFFFFu : 0xFFFFu << (lane & 16);
+}
 // warp-wide minimum of 64-bit keys
 __device__ __forceinline__ uint64_t warp_min_redux(uint64_t k) {
 #if ZTC_RDO_MIN_REDUX  // the high words' minimum, then the low words' among the lanes holding it
@@ -547,7 +557,7 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src,
     __shared__ int s_dist[2];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, i = lane & 15, grp = tid >> 4;
     const int kind = grp < 16 ? 1 : grp < 32 ? 2 : grp < 48 ? 0 : grp == 48 ? -1 : -2, j = (grp & 15) + 1;
-    const unsigned gm = 0xFFFFu << (lane & 16);  // this lane's group
+    const unsigned gm = group_mask(warp, lane);
     const int row0 = blockIdx.x * chain_rows, rows = min(chain_rows, nby - row0);
     if (rows <= 0) return;
     const int first = row0 * bw, count = rows * bw;
@@ -710,7 +720,7 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_sub_chain_kernel(SrcU8 src,
     const Sub S = blockIdx.y ? S1 : S0;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, i = lane & 15, grp = tid >> 4;
     const int kind = grp < 16 ? 0 : grp < 32 ? 1 : grp < 48 ? 2 : grp == 48 ? -1 : -2, j = (grp & 15) + 1;
-    const unsigned gm = 0xFFFFu << (lane & 16);  // this lane's group
+    const unsigned gm = group_mask(warp, lane);
     const int row0 = blockIdx.x * chain_rows, rows = min(chain_rows, nby - row0);
     if (rows <= 0) return;
     const int first = row0 * bw, count = rows * bw;
