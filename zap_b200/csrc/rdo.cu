@@ -8,9 +8,10 @@
 // min(size, 3) for a new match in the window, its size in literals otherwise.
 //
 // Only that window makes the work serial. The base encodings do not depend on it, so the ordinary encoder kernels
-// write them for every block first, in parallel. The chain then runs as one warp per call (or per band of block
-// rows: each band is its own call in the reference's banded callers): per block the lanes evaluate the candidates
-// side by side and one warp-wide minimum of (cost, candidate order) picks the winner. That minimum is the
+// write them for every block first, in parallel. The chain then runs as one CTA per call (or per band of block
+// rows: each band is its own call in the reference's banded callers; and per sub-block kind, whose chains are
+// independent): per block, 16-lane groups evaluate the candidates side by side, one lane per texel, and a
+// CTA-wide minimum of (cost, candidate order) picks the winner. That minimum is the
 // reference's choice: its scan takes a candidate only if its cost is below the best so far (strict "<"), so it ends
 // on the first candidate of the lowest cost, and its early "skip if SSE >= best" never changes that, because
 // SSE + lambda * rate >= SSE in float arithmetic when lambda * rate >= 0 (finite lambda > 0: the entry points reject
@@ -39,37 +40,6 @@ __host__ __device__ constexpr Sub sub_of(int fmt, int s) {
                                 : Sub{kBc7, 0, 0, 0};
 }
 
-// bytes [off, off + n) of a 16-byte sub-block held as two little-endian words, n <= 8
-ZTC_DEV uint64_t field_of(uint64_t lo, uint64_t hi, int off, int n) {
-    const uint64_t v = off >= 8 ? hi >> (8 * (off - 8)) : off ? (lo >> (8 * off)) | (hi << (64 - 8 * off)) : lo;
-    return n >= 8 ? v : v & ((1ull << (8 * n)) - 1ull);
-}
-
-// rate of one field (zap__field_rate, zap_tex.h:234-241); ring: the last 16 chosen sub-blocks, slot = block & 15.
-// The 16 window comparisons are independent (a match mask, then its lowest bit), not a loop that stops early:
-// the same result, without a chain of dependent shared-memory loads.
-__device__ __forceinline__ float field_rate(uint64_t f, int off, int n, const uint64_t (*ring)[2], int cur, int dist, int &nd) {
-    uint32_t m = 0;
-    #pragma unroll
-    for (int j = 1; j <= kWindow; j++) {
-        const uint64_t *p = ring[(cur - j) & (kWindow - 1)];
-        m |= (uint32_t)(j <= cur && field_of(p[0], p[1], off, n) == f) << (j - 1);
-    }
-    nd = dist;
-    if (dist > 0 && dist <= cur && ((m >> (dist - 1)) & 1u)) return 0.0f;  // the current match continues
-    if (m) { nd = __ffs((int)m); return n < 3 ? (float)n : 3.0f; }          // a new match: the nearest one
-    return (float)n;
-}
-
-// a sub-block's rate: its two fields (BC1 {4, 4}, BC4 {2, 6}); BC7 {bytes 0-7, bytes 9-15} plus the straddling
-// byte 8, always paid (zap__bc7_rate, zap_tex.h:788-790)
-__device__ __forceinline__ float sub_rate(int type, uint64_t lo, uint64_t hi, const uint64_t (*ring)[2], int cur, const int dist[2], int nd[2]) {
-    if (type == kBc7)
-        return field_rate(field_of(lo, hi, 0, 8), 0, 8, ring, cur, dist[0], nd[0]) + field_rate(field_of(lo, hi, 9, 7), 9, 7, ring, cur, dist[1], nd[1]) + 1;
-    const int n0 = type == kBc1 ? 4 : 2, n1 = type == kBc1 ? 4 : 6;
-    return field_rate(field_of(lo, hi, 0, n0), 0, n0, ring, cur, dist[0], nd[0]) + field_rate(field_of(lo, hi, n0, n1), n0, n1, ring, cur, dist[1], nd[1]);
-}
-
 // ---- BC1 sub-block (zap_tex.h:52-94): u16 c0, u16 c1, 2-bit indices; 3 colours + transparent when c0 <= c1
 ZTC_DEV void bc1_entry(uint32_t c0, uint32_t c1, int force4, int k, int &r, int &g, int &b) {
     int r0, g0, b0, r1, g1, b1;
@@ -85,48 +55,6 @@ ZTC_DEV void bc1_entry(uint32_t c0, uint32_t c1, int force4, int k, int &r, int 
         else { r = g = b = 0; }
     }
 }
-ZTC_DEV int sq3(uint32_t t, int r, int g, int b) {
-    const int dr = (int)chan(t, 0) - r, dg = (int)chan(t, 1) - g, db = (int)chan(t, 2) - b;
-    return dr * dr + dg * dg + db * db;
-}
-ZTC_DEV int bc1_fit_any(const uint32_t t[16], uint32_t c0, uint32_t c1, int force4, uint32_t &idx) {  // zap__bc1_fit
-    int pr[4], pg[4], pb[4];
-    #pragma unroll
-    for (int k = 0; k < 4; k++) bc1_entry(c0, c1, force4, k, pr[k], pg[k], pb[k]);
-    const int n = (force4 || c0 > c1) ? 4 : 3;
-    int err = 0;
-    uint32_t bits = 0;
-    #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        int best = 0, be = sq3(t[i], pr[0], pg[0], pb[0]);
-        #pragma unroll
-        for (int k = 1; k < 4; k++) {
-            if (k >= n) break;
-            const int e = sq3(t[i], pr[k], pg[k], pb[k]);
-            if (e < be) { be = e; best = k; }
-        }
-        bits |= (uint32_t)best << (2 * i);
-        err += be;
-    }
-    idx = bits;
-    return err;
-}
-ZTC_DEV int bc1_eval(const uint32_t t[16], uint32_t c0, uint32_t c1, int force4, uint32_t idx) {  // zap__bc1_eval
-    int pr[4], pg[4], pb[4];
-    #pragma unroll
-    for (int k = 0; k < 4; k++) bc1_entry(c0, c1, force4, k, pr[k], pg[k], pb[k]);
-    int err = 0;
-    #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        const int k = (int)((idx >> (2 * i)) & 3u);
-        const int r = k == 0 ? pr[0] : k == 1 ? pr[1] : k == 2 ? pr[2] : pr[3];
-        const int g = k == 0 ? pg[0] : k == 1 ? pg[1] : k == 2 ? pg[2] : pg[3];
-        const int b = k == 0 ? pb[0] : k == 1 ? pb[1] : k == 2 ? pb[2] : pb[3];
-        err += sq3(t[i], r, g, b);
-    }
-    return err;
-}
-
 // ---- BC4 sub-block (zap_tex.h:172-196): u8 a0, u8 a1, 3-bit indices; 6 values + 0 and 255 when a0 <= a1
 ZTC_DEV int bc4_entry(int a0, int a1, int k) {
     if (k == 0) return a0;
@@ -134,304 +62,10 @@ ZTC_DEV int bc4_entry(int a0, int a1, int k) {
     if (a0 > a1) return ((8 - k) * a0 + (k - 1) * a1 + 3) / 7;
     return k < 6 ? ((6 - k) * a0 + (k - 1) * a1 + 2) / 5 : k == 6 ? 0 : 255;
 }
-ZTC_DEV int bc4_fit_any(const uint32_t t[16], int ch, int a0, int a1, uint64_t &idx) {  // zap__bc4_fit
-    int pal[8];
-    #pragma unroll
-    for (int k = 0; k < 8; k++) pal[k] = bc4_entry(a0, a1, k);
-    int err = 0;
-    uint64_t bits = 0;
-    #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        const int v = (int)chan(t[i], ch);
-        int best = 0, be = (v - pal[0]) * (v - pal[0]);
-        #pragma unroll
-        for (int k = 1; k < 8; k++) { const int e = (v - pal[k]) * (v - pal[k]); if (e < be) { be = e; best = k; } }
-        bits |= (uint64_t)best << (3 * i);
-        err += be;
-    }
-    idx = bits;
-    return err;
-}
-ZTC_DEV int bc4_eval(const uint32_t t[16], int ch, int a0, int a1, uint64_t idx) {  // zap__bc4_eval
-    int err = 0;
-    #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        const int d = (int)chan(t[i], ch) - bc4_entry(a0, a1, (int)((idx >> (3 * i)) & 7u));
-        err += d * d;
-    }
-    return err;
-}
-
-// ---- BC7 (zap_tex.h:529-580, :710-716)
-ZTC_DEV void words_of(uint64_t lo, uint64_t hi, uint32_t w[4]) { w[0] = (uint32_t)lo; w[1] = (uint32_t)(lo >> 32); w[2] = (uint32_t)hi; w[3] = (uint32_t)(hi >> 32); }
-ZTC_DEV int decoded_sse(const uint32_t t[16], uint64_t lo, uint64_t hi) {
-    uint32_t w[4], px[16];
-    words_of(lo, hi, w);
-    dec::bc7_block(w, px);
-    int err = 0;
-    #pragma unroll
-    for (int i = 0; i < 16; i++)
-        #pragma unroll
-        for (int c = 0; c < 4; c++) { const int x = (int)chan(t[i], c) - (int)chan(px[i], c); err += x * x; }
-    return err;
-}
+// ---- BC7 mode-6 blocks (zap_tex.h:529)
 ZTC_DEV bool is_mode6(uint64_t lo) { return (lo & 0x7Fu) == 0x40u; }
 // mode-6 fields: q[e][c] 7 bits each (c-major), p-bits, 4-bit indices (texel 0: 3 bits) packed into idx, 4 bits each
-ZTC_DEV void unpack_mode6(uint64_t lo, uint64_t hi, int q[2][4], int pb[2], uint64_t &idx) {
-    uint32_t w[4];
-    words_of(lo, hi, w);
-    int pos = 7;
-    #pragma unroll
-    for (int c = 0; c < 4; c++)
-        #pragma unroll
-        for (int e = 0; e < 2; e++) { q[e][c] = (int)get_bits128(w, pos, 7); pos += 7; }
-    pb[0] = (int)get_bits128(w, pos, 1); pb[1] = (int)get_bits128(w, pos + 1, 1);
-    pos += 2;
-    idx = 0;
-    #pragma unroll
-    for (int i = 0; i < 16; i++) { idx |= (uint64_t)get_bits128(w, pos, i ? 4 : 3) << (4 * i); pos += i ? 4 : 3; }
-}
-ZTC_DEV void pack_mode6(const int q[2][4], const int pb[2], uint64_t idx, uint64_t &lo, uint64_t &hi) {
-    Bits128 o;
-    o.put(1u << 6, 7);
-    #pragma unroll
-    for (int c = 0; c < 4; c++)
-        #pragma unroll
-        for (int e = 0; e < 2; e++) o.put((uint32_t)q[e][c], 7);
-    o.put((uint32_t)pb[0], 1); o.put((uint32_t)pb[1], 1);
-    #pragma unroll
-    for (int i = 0; i < 16; i++) o.put((uint32_t)((idx >> (4 * i)) & 15u), i ? 4 : 3);
-    lo = (uint64_t)o.w[0] | ((uint64_t)o.w[1] << 32);
-    hi = (uint64_t)o.w[2] | ((uint64_t)o.w[3] << 32);
-}
-ZTC_DEV void mode6_ends(const int q[2][4], const int pb[2], int x0[4], int x1[4]) {
-    #pragma unroll
-    for (int c = 0; c < 4; c++) { x0[c] = expand_bits((q[0][c] << 1) | pb[0], 8); x1[c] = expand_bits((q[1][c] << 1) | pb[1], 8); }
-}
-ZTC_DEV int sq4(uint32_t t, const int x0[4], const int x1[4], int w) {
-    int s = 0;
-    #pragma unroll
-    for (int c = 0; c < 4; c++) { const int d = (int)chan(t, c) - lerp64(x0[c], x1[c], w); s += d * d; }
-    return s;
-}
-// indices for a neighbour's endpoints; texel 0 keeps to 0..7 so no anchor swap is needed (zap__bc7_fit6_idx)
-ZTC_DEV int mode6_fit_indices(const uint32_t t[16], const int q[2][4], const int pb[2], uint64_t &idx) {
-    int x0[4], x1[4];
-    mode6_ends(q, pb, x0, x1);
-    uint32_t pal[16];
-    #pragma unroll
-    for (int j = 0; j < 16; j++)
-        pal[j] = pack_rgba(lerp64(x0[0], x1[0], w4(j)), lerp64(x0[1], x1[1], w4(j)), lerp64(x0[2], x1[2], w4(j)), lerp64(x0[3], x1[3], w4(j)));
-    int err = 0;
-    uint64_t bits = 0;
-    #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        int bj = 0, be = 1 << 30;
-        #pragma unroll
-        for (int j = 0; j < 16; j++) {
-            if (i == 0 && j >= 8) break;
-            int d = 0;
-            #pragma unroll
-            for (int c = 0; c < 4; c++) { const int x = (int)chan(t[i], c) - (int)chan(pal[j], c); d += x * x; }
-            if (d < be) { be = d; bj = j; }
-        }
-        bits |= (uint64_t)bj << (4 * i);
-        err += be;
-    }
-    idx = bits;
-    return err;
-}
-// endpoints for a neighbour's indices: least squares, then each endpoint's own p-bit (zap__bc7_fit6_ep)
-ZTC_DEV int mode6_fit_endpoints(const uint32_t t[16], uint64_t idx, int q[2][4], int pb[2]) {
-    float aa = 0.0f, ab = 0.0f, bb = 0.0f, sa[4] = {0.0f, 0.0f, 0.0f, 0.0f}, sb[4] = {0.0f, 0.0f, 0.0f, 0.0f}, lo[4], hi[4];
-    #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        const float w = (float)w4((int)((idx >> (4 * i)) & 15u)) / 64.0f, u = 1.0f - w;
-        aa = aa + u * u; ab = ab + u * w; bb = bb + w * w;
-        #pragma unroll
-        for (int c = 0; c < 4; c++) { const float x = (float)chan(t[i], c); sa[c] = sa[c] + u * x; sb[c] = sb[c] + w * x; }
-    }
-    const float det = aa * bb - ab * ab;
-    #pragma unroll
-    for (int c = 0; c < 4; c++) {
-        if (det < 1e-6f && det > -1e-6f) { lo[c] = (sa[c] + sb[c]) / 16.0f; hi[c] = lo[c]; }  // one index everywhere
-        else { lo[c] = (sa[c] * bb - sb[c] * ab) / det; hi[c] = (sb[c] * aa - sa[c] * ab) / det; }
-        lo[c] = clamp255(lo[c]); hi[c] = clamp255(hi[c]);
-    }
-    int b0 = 1 << 30, b1 = 1 << 30;
-    #pragma unroll
-    for (int p = 0; p < 2; p++) {
-        int t0[4], t1[4], e0[4], e1[4];
-        const int x = quant_pbit<4>(lo, 8, p, t0, e0), y = quant_pbit<4>(hi, 8, p, t1, e1);
-        if (x < b0) { b0 = x; pb[0] = p; for (int c = 0; c < 4; c++) q[0][c] = t0[c]; }
-        if (y < b1) { b1 = y; pb[1] = p; for (int c = 0; c < 4; c++) q[1][c] = t1[c]; }
-    }
-    int x0[4], x1[4];
-    mode6_ends(q, pb, x0, x1);
-    int err = 0;
-    #pragma unroll
-    for (int i = 0; i < 16; i++) err += sq4(t[i], x0, x1, w4((int)((idx >> (4 * i)) & 15u)));
-    return err;
-}
-
-// SSE of the base encoding (the value the reference's encoder returns: the chosen block's decoded SSE)
-ZTC_DEV int base_sse(const Sub &S, const uint32_t t[16], uint64_t lo, uint64_t hi) {
-    if (S.type == kBc1) return bc1_eval(t, (uint32_t)(lo & 0xFFFFu), (uint32_t)((lo >> 16) & 0xFFFFu), S.force4, (uint32_t)(lo >> 32));
-    if (S.type == kBc4) return bc4_eval(t, S.chan, (int)(lo & 0xFFu), (int)((lo >> 8) & 0xFFu), lo >> 16);
-    return decoded_sse(t, lo, hi);
-}
-
-// candidate `kind` built from neighbour (plo, phi) and the base (blo); false if it does not exist or is not allowed
-ZTC_DEV bool candidate(const Sub &S, int kind, const uint32_t t[16], uint64_t plo, uint64_t phi, uint64_t blo, int &e, uint64_t &clo,
-                       uint64_t &chi) {
-    chi = 0;
-    if (S.type == kBc1) {
-        const uint32_t p0 = (uint32_t)(plo & 0xFFFFu), p1 = (uint32_t)((plo >> 16) & 0xFFFFu), pi = (uint32_t)(plo >> 32);
-        const uint32_t c0 = (uint32_t)(blo & 0xFFFFu), c1 = (uint32_t)((blo >> 16) & 0xFFFFu);
-        if (kind == 0) { uint32_t fi; e = bc1_fit_any(t, p0, p1, S.force4, fi); clo = p0 | (p1 << 16) | ((uint64_t)fi << 32); }
-        else {  // kind 1: these endpoints, kind 2: the neighbour's; both with its indices (one call site: no divergence)
-            const uint32_t a = kind == 1 ? c0 : p0, b = kind == 1 ? c1 : p1;
-            e = bc1_eval(t, a, b, S.force4, pi);
-            clo = a | (b << 16) | ((uint64_t)pi << 32);
-        }
-        if (!S.force4 && (clo & 0xFFFFu) <= ((clo >> 16) & 0xFFFFu)) {  // 3-colour block: index 3 would be transparent
-            const uint32_t ci = (uint32_t)(clo >> 32);
-            if (ci & (ci >> 1) & 0x55555555u) return false;
-        }
-        return true;
-    }
-    if (S.type == kBc4) {
-        const int pa0 = (int)(plo & 0xFFu), pa1 = (int)((plo >> 8) & 0xFFu);
-        const uint64_t pi = plo >> 16;
-        if (kind == 0) { uint64_t fi; e = bc4_fit_any(t, S.chan, pa0, pa1, fi); clo = (uint64_t)pa0 | ((uint64_t)pa1 << 8) | (fi << 16); }
-        else {
-            const int a = kind == 1 ? (int)(blo & 0xFFu) : pa0, b = kind == 1 ? (int)((blo >> 8) & 0xFFu) : pa1;
-            e = bc4_eval(t, S.chan, a, b, pi);
-            clo = (uint64_t)a | ((uint64_t)b << 8) | (pi << 16);
-        }
-        return true;
-    }
-    if (kind == 0) { e = decoded_sse(t, plo, phi); clo = plo; chi = phi; return true; }
-    if (!is_mode6(plo)) return false;  // the endpoint / index reuse kinds exist for mode-6 neighbours only
-    int q[2][4], pb[2];
-    uint64_t pidx;
-    unpack_mode6(plo, phi, q, pb, pidx);
-    if (kind == 1) {
-        uint64_t nidx;
-        e = mode6_fit_indices(t, q, pb, nidx);
-        pack_mode6(q, pb, nidx, clo, chi);
-    } else {
-        int nq[2][4], npb[2];
-        e = mode6_fit_endpoints(t, pidx, nq, npb);
-        pack_mode6(nq, npb, pidx, clo, chi);
-    }
-    return true;
-}
-
 __device__ __forceinline__ uint64_t key_of(float cost, int order) { return ((uint64_t)__float_as_uint(cost) << 32) | (uint32_t)order; }
-__device__ __forceinline__ uint64_t warp_min(uint64_t k) {
-    #pragma unroll
-    for (int m = 16; m >= 1; m >>= 1) {
-        const uint32_t lo = __shfl_xor_sync(0xFFFFFFFFu, (uint32_t)k, m), hi = __shfl_xor_sync(0xFFFFFFFFu, (uint32_t)(k >> 32), m);
-        const uint64_t o = ((uint64_t)hi << 32) | lo;
-        k = o < k ? o : k;
-    }
-    return k;
-}
-
-// One chain per CTA: block rows [c * chain_rows, min((c + 1) * chain_rows, nby)) of the image, whose base
-// encodings `out` already holds; each sub-block is replaced by the reference's RDO choice, in raster order.
-// Three warps; lanes of one warp run the same code path (the candidate order, (j - 1) * 3 + kind + 1, is kept in
-// the key): BC1-BC5 warp 0 = kinds 1 and 2 (both evaluations), warp 1 = kind 0 (fits), warp 2 lane 0 = the base;
-// BC7 warp 0 = kind 1, warp 1 = kind 2, warp 2 = kind 0 and the base (both decode). A CTA-wide minimum of
-// (cost, order) picks the winner, whose thread stores it. Texels and base of the next block are loaded one step
-// ahead.
-constexpr int kChainThreads = 96;
-// (window distance j, kind) of a thread, kind -1 for the base, -2 for none
-__device__ __forceinline__ void chain_role(bool bc7, int tid, int &j, int &kind) {
-    const int warp = tid >> 5, lane = tid & 31;
-    j = (lane & 15) + 1;
-    if (!bc7) kind = warp == 0 ? (lane < 16 ? 1 : 2) : warp == 1 ? (lane < 16 ? 0 : -2) : (lane == 0 ? -1 : -2);
-    else kind = lane < 16 ? (warp == 0 ? 1 : warp == 1 ? 2 : 0) : (warp == 2 && lane == 16 ? -1 : -2);
-}
-__device__ __forceinline__ int chain_owner(bool bc7, int order) {
-    if (order == 0) return bc7 ? 80 : 64;
-    const int c = order - 1, j = c / 3 + 1, kind = c % 3;
-    if (!bc7) return kind == 0 ? 32 + j - 1 : kind == 1 ? j - 1 : 16 + j - 1;
-    return kind == 1 ? j - 1 : kind == 2 ? 32 + j - 1 : 64 + j - 1;
-}
-template <int FMT>
-__global__ void __launch_bounds__(kChainThreads) rdo_chain_kernel(SrcU8 src, int bw, int nby, int chain_rows, uint8_t *__restrict__ out,
-                                                                 float lambda) {
-    constexpr int NS = sub_count(FMT), BS = (FMT == ZTC_FMT_BC1 || FMT == ZTC_FMT_BC4) ? 8 : 16;
-    __shared__ uint64_t ring[NS][kWindow][2];
-    __shared__ uint32_t s_tex[2][16];
-    __shared__ uint64_t s_base[2][2];  // the block's base encoding (16 bytes), loaded one step ahead like its texels
-    __shared__ uint64_t s_key[kChainThreads / 32];
-    __shared__ int s_dist[2];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int row0 = blockIdx.x * chain_rows, rows = min(chain_rows, nby - row0);
-    if (rows <= 0) return;
-    const int first = row0 * bw, count = rows * bw;
-    int dist[NS][2];
-    #pragma unroll
-    for (int s = 0; s < NS; s++) { dist[s][0] = 1; dist[s][1] = 1; }
-    if (tid < 16) s_tex[0][tid] = load_texel(src, min((first % bw) * 4 + (tid & 3), src.w - 1), min((first / bw) * 4 + (tid >> 2), src.h - 1));
-    if (tid >= 16 && tid < 16 + BS / 8) s_base[0][tid - 16] = *(const uint64_t *)(out + (size_t)first * BS + 8 * (tid - 16));
-    __syncthreads();
-    for (int cur = 0; cur < count; cur++) {
-        const int g = first + cur;
-        uint32_t t[16];
-        #pragma unroll
-        for (int i = 0; i < 16; i++) t[i] = s_tex[cur & 1][i];
-        const uint64_t base_lo = s_base[cur & 1][0], base_hi = BS == 16 ? s_base[cur & 1][1] : 0ull;
-        if (cur + 1 < count && tid < 16) {  // the next block's texels and base, consumed after the next barrier
-            const int gn = g + 1;
-            s_tex[(cur + 1) & 1][tid] = load_texel(src, min((gn % bw) * 4 + (tid & 3), src.w - 1), min((gn / bw) * 4 + (tid >> 2), src.h - 1));
-        } else if (cur + 1 < count && tid < 16 + BS / 8) {
-            s_base[(cur + 1) & 1][tid - 16] = *(const uint64_t *)(out + (size_t)(g + 1) * BS + 8 * (tid - 16));
-        }
-        uint8_t *blk = out + (size_t)g * BS;
-        #pragma unroll
-        for (int s = 0; s < NS; s++) {
-            const Sub S = sub_of(FMT, s);
-            const uint64_t blo = S.off ? base_hi : base_lo, bhi = S.type == kBc7 ? base_hi : 0ull;
-            uint64_t key = ~0ull, clo = 0, chi = 0;
-            int nd[2] = {0, 0}, j, kind;
-            chain_role(FMT == ZTC_FMT_BC7, tid, j, kind);
-            if (kind == -1) {  // the base: order 0
-                const int e0 = base_sse(S, t, blo, bhi);
-                key = key_of((float)e0 + lambda * sub_rate(S.type, blo, bhi, ring[s], cur, dist[s], nd), 0);
-                clo = blo; chi = bhi;
-            } else if (kind >= 0 && j <= cur) {
-                const uint64_t *prev = ring[s][(cur - j) & (kWindow - 1)];
-                int e;
-                if (candidate(S, kind, t, prev[0], prev[1], blo, e, clo, chi))
-                    key = key_of((float)e + lambda * sub_rate(S.type, clo, chi, ring[s], cur, dist[s], nd), (j - 1) * 3 + kind + 1);
-            }
-            const uint64_t wk = warp_min(key);
-            if (lane == 0) s_key[warp] = wk;
-            __syncthreads();
-            uint64_t win = s_key[0];
-            #pragma unroll
-            for (int w = 1; w < kChainThreads / 32; w++) win = s_key[w] < win ? s_key[w] : win;
-            const int order = (int)(uint32_t)win;
-            if (tid == chain_owner(FMT == ZTC_FMT_BC7, order)) {  // the winner's thread stores it
-                ring[s][cur & (kWindow - 1)][0] = clo;
-                ring[s][cur & (kWindow - 1)][1] = chi;
-                if (order != 0) {
-                    *(uint64_t *)(blk + S.off) = clo;
-                    if (S.type == kBc7) *(uint64_t *)(blk + 8) = chi;
-                }
-                s_dist[0] = nd[0];
-                s_dist[1] = nd[1];
-            }
-            __syncthreads();
-            dist[s][0] = s_dist[0];
-            dist[s][1] = s_dist[1];
-        }
-    }
-}
 
 // ---------------------------------------------------------------- BC7: one lane per texel
 // A BC7 candidate costs a whole palette search or least-squares solve, so this chain spreads each candidate over a
@@ -491,8 +125,14 @@ __device__ __forceinline__ uint64_t warp_min_redux(uint64_t k) {
     const uint32_t hi = __reduce_min_sync(0xFFFFFFFFu, (uint32_t)(k >> 32));
     const uint32_t lo = __reduce_min_sync(0xFFFFFFFFu, (uint32_t)(k >> 32) == hi ? (uint32_t)k : 0xFFFFFFFFu);
     return ((uint64_t)hi << 32) | lo;
-#else
-    return warp_min(k);
+#else  // xor-shuffle tree
+    #pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) {
+        const uint32_t lo = __shfl_xor_sync(0xFFFFFFFFu, (uint32_t)k, m), hi = __shfl_xor_sync(0xFFFFFFFFu, (uint32_t)(k >> 32), m);
+        const uint64_t o = ((uint64_t)hi << 32) | lo;
+        k = o < k ? o : k;
+    }
+    return k;
 #endif
 }
 ZTC_DEV int sq4px(uint32_t a, uint32_t b) {  // squared RGBA difference (zap__sq4 over 4 channels)
@@ -855,13 +495,4 @@ cudaError_t ztc_launch_rdo(int fmt, const ztc::SrcU8 &src, uint8_t *out, float l
         ztc::rdo_sub_chain_kernel<<<grid, ztc::kB7Threads, 0, stream>>>(src, bw, nby, band_rows, out, bs, S0, S1, lambda);
         return cudaGetLastError();
     }
-    switch (fmt) {
-    case ZTC_FMT_BC1: ztc::rdo_chain_kernel<ZTC_FMT_BC1><<<chains, ztc::kChainThreads, 0, stream>>>(src, bw, nby, band_rows, out, lambda); break;
-    case ZTC_FMT_BC3: ztc::rdo_chain_kernel<ZTC_FMT_BC3><<<chains, ztc::kChainThreads, 0, stream>>>(src, bw, nby, band_rows, out, lambda); break;
-    case ZTC_FMT_BC4: ztc::rdo_chain_kernel<ZTC_FMT_BC4><<<chains, ztc::kChainThreads, 0, stream>>>(src, bw, nby, band_rows, out, lambda); break;
-    case ZTC_FMT_BC5: ztc::rdo_chain_kernel<ZTC_FMT_BC5><<<chains, ztc::kChainThreads, 0, stream>>>(src, bw, nby, band_rows, out, lambda); break;
-    case ZTC_FMT_BC7: ztc::rdo_chain_kernel<ZTC_FMT_BC7><<<chains, ztc::kChainThreads, 0, stream>>>(src, bw, nby, band_rows, out, lambda); break;
-    default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
 }
