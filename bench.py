@@ -226,6 +226,20 @@ def reference_cpu(img_np, fmt, reps=3):
     return {"seconds": best, "threads": threads, "out": out}
 
 
+def reference_cpu_1core(img_np, fmt, reps=3):
+    """Best-of-reps wall time of one reference zap_bc_encode call on one thread (tex_bench.c:208-210)."""
+    import oracle_lib
+    ref = oracle_lib.reference()
+    if ref is None:
+        return None
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        ref.bc_encode(img_np, fmt)
+        best = min(best, time.perf_counter() - t0)
+    return best
+
+
 def run_reference(args, world, rank):
     """--impl reference: the reference's own CPU encoder, all host threads, same workload and metric."""
     if rank != 0:
@@ -390,6 +404,10 @@ def main():
         if cpu is not None:
             line["cpu_baseline"] = {"value": mpix / cpu["seconds"], "unit": "Mpix/s", "cores": cpu["threads"], "kind": "reference",
                                     "sample": f"full {W}x{H} texture, best of 2, 8-block-row bands on all host threads"}
+            one = reference_cpu_1core(hin, zap_b200.BC7)
+            if one is not None:  # the reference self-test's own method (tex_bench.c:208-210): one call, best of 3
+                line["cpu_baseline"]["one_core"] = {"value": mpix / one, "unit": "Mpix/s", "cores": 1,
+                                                    "sample": f"full {W}x{H} texture, one zap_bc_encode call, best of 3"}
             same = np.mean(np.all(hout.reshape(-1, 16) == cpu["out"].reshape(-1, 16), axis=1))
             line["parity"] = {"identical_blocks": float(same)}
         if not args.no_extra:
