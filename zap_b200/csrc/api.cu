@@ -14,6 +14,7 @@
 #include "ztc_common.cuh"
 #include "ztc_internal.h"
 
+#include <atomic>
 #include <map>
 #include <string>
 #include <vector>
@@ -328,6 +329,17 @@ int check_image(const void *p, const void *out, int w, int h, size_t stride, siz
 }  // namespace
 
 int ztc_set_error(int status, const char *msg) { return fail(status, "%s", msg); }
+int ztc_sm_count() {  // SMs of the current device, cached per device (148 on B200; a tuning input only)
+    static std::atomic<int> cache[kMaxDevices];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) { cudaGetLastError(); return 148; }
+    int n = cache[dev].load(std::memory_order_relaxed);
+    if (n <= 0) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) { cudaGetLastError(); n = 148; }
+        cache[dev].store(n, std::memory_order_relaxed);
+    }
+    return n;
+}
 int ztc_ctx_activate(zap_tex_cuda_ctx *ctx) { return resolve(ctx); }
 
 extern "C" {

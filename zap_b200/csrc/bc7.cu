@@ -234,15 +234,14 @@ __device__ __forceinline__ int mode6_encode_cta(bool valid, const uint32_t t[16]
     return s_err[tid];
 }
 
-// threads per CTA of the mode-6 kernel (a tunable: the CTA shares one list of compacted refits). Measured on
-// 2048x2048: 64 0.119 ms, 128 0.105 ms, 256 0.099 ms, 384 0.100 ms, 512 0.103 ms.
-#ifndef ZTC_BC7_MODE6_CTA
-#define ZTC_BC7_MODE6_CTA 256
-#endif
-constexpr int kMode6Cta = ZTC_BC7_MODE6_CTA;
-__global__ void __launch_bounds__(kMode6Cta, ZTC_MINB_BC7_MODE6 * 128 / kMode6Cta) bc7_mode6_kernel(SrcU8 src, int bw, int by0, int nblocks,
+// CTA sizes of the mode-6 kernel. A larger CTA shares one compacted-refit list among more blocks (2048x2048:
+// 64 threads 0.119 ms, 128 0.105, 256 0.099, 384 0.100, 512 0.103); a launch smaller than one full wave of large
+// CTAs takes the small size instead, which keeps more SMs busy (512x512 in 256-thread CTAs: 64 CTAs for 148 SMs).
+constexpr int kMode6Small = 128, kMode6Large = 256;
+template <int CTA>
+__global__ void __launch_bounds__(CTA, ZTC_MINB_BC7_MODE6 * 128 / CTA) bc7_mode6_kernel(SrcU8 src, int bw, int by0, int nblocks,
                                                         BlockOut out, size_t b0, uint32_t *__restrict__ count, uint2 *__restrict__ items) {
-    __shared__ uint32_t s_tex[16][kMode6Cta];  // column threadIdx.x: this thread's block
+    __shared__ uint32_t s_tex[16][CTA];  // column threadIdx.x: this thread's block
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = b < nblocks;
     uint32_t t[16];
@@ -252,7 +251,7 @@ __global__ void __launch_bounds__(kMode6Cta, ZTC_MINB_BC7_MODE6 * 128 / kMode6Ct
         for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
     }
     uint4 blk;
-    const int err = mode6_encode_cta<kMode6Cta>(valid, t, s_tex, blk);
+    const int err = mode6_encode_cta<CTA>(valid, t, s_tex, blk);
     if (valid) put_block16(out, b0 + (size_t)b, blk);
     bool hard = valid && err > 16 * 4;  // zap_tex.h:758 early exit
     unsigned ballot = __ballot_sync(0xFFFFFFFFu, hard);
@@ -263,6 +262,16 @@ __global__ void __launch_bounds__(kMode6Cta, ZTC_MINB_BC7_MODE6 * 128 / kMode6Ct
         base = __shfl_sync(0xFFFFFFFFu, base, leader);
         if (hard) items[base + __popc(ballot & ((1u << lane) - 1u))] = make_uint2((uint32_t)b, (uint32_t)err);
     }
+}
+
+// the mode-6 launch, at the CTA size that suits its block count
+cudaError_t launch_mode6(const SrcU8 &src, int bw, int by0, int nblocks, const BlockOut &out, size_t b0, uint32_t *count, uint2 *items,
+                         cudaStream_t s) {
+    if (nblocks >= ztc_sm_count() * (ZTC_MINB_BC7_MODE6 * 128 / kMode6Large) * kMode6Large)
+        bc7_mode6_kernel<kMode6Large><<<(nblocks + kMode6Large - 1) / kMode6Large, kMode6Large, 0, s>>>(src, bw, by0, nblocks, out, b0, count, items);
+    else
+        bc7_mode6_kernel<kMode6Small><<<(nblocks + kMode6Small - 1) / kMode6Small, kMode6Small, 0, s>>>(src, bw, by0, nblocks, out, b0, count, items);
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- kernel B pieces
@@ -743,7 +752,7 @@ cudaError_t ztc_launch_bc7_to(const ztc::SrcU8 &src, int by0, int nby, const ztc
     {
         ztc::TraceScope tr("bc7_mode6", stream);
         ztc::trace_units(nblocks);
-        ztc::bc7_mode6_kernel<<<(nblocks + ztc::kMode6Cta - 1) / ztc::kMode6Cta, ztc::kMode6Cta, 0, stream>>>(src, bw, by0, nblocks, out, b0, count, items);
+        ztc::launch_mode6(src, bw, by0, nblocks, out, b0, count, items, stream);
     }
     int groups_per_cta = 128 / ztc::kBc7Group;
     int ctas = (nblocks + groups_per_cta - 1) / groups_per_cta;
@@ -813,7 +822,7 @@ extern "C" __attribute__((visibility("default"))) int zap_tex_cuda_bc7_encode_no
     const ztc::BlockOut blocks{(uint8_t *)out, 0, ZTC_FMT_BC7, 0};
     cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), s);  // the list must start empty on every call
     if (e == cudaSuccess) {
-        ztc::bc7_mode6_kernel<<<(nblocks + ztc::kMode6Cta - 1) / ztc::kMode6Cta, ztc::kMode6Cta, 0, s>>>(src, (int)bw, 0, nblocks, blocks, 0, count, items);
+        ztc::launch_mode6(src, (int)bw, 0, nblocks, blocks, 0, count, items, s);
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         int ctas = (nblocks + 15) / 16;

@@ -94,6 +94,8 @@ cudaError_t ztc_launch_bcn_to(int fmt, const ztc::SrcU8 &src, int by0, int nby, 
 cudaError_t ztc_launch_bc7_to(const ztc::SrcU8 &src, int by0, int nby, const ztc::BlockOut &out, size_t b0, void *scratch,
                               cudaStream_t stream);
 // RDO (lambda > 0) over base encodings already in `out`, in place: one chain per band_rows block rows (0: one)
+// SMs of the current device (cached per device)
+int ztc_sm_count();
 cudaError_t ztc_launch_rdo(int fmt, const ztc::SrcU8 &src, uint8_t *out, float lambda, int band_rows, cudaStream_t stream);
 // split (to_planes = 1) or merge n bytes of BC1..BC7 data, device to device (zap_tex.h:1549-1571)
 cudaError_t ztc_launch_bc_regroup(const uint8_t *in, uint8_t *out, size_t n, int fmt, int to_planes, cudaStream_t stream);
