@@ -226,6 +226,31 @@ def reference_cpu(img_np, fmt, reps=3):
     return {"seconds": best, "threads": threads, "out": out}
 
 
+def bind_to_gpu_local_cpus(dev):
+    """Restrict this process to the CPUs NVML reports as local to the device (read-only queries); returns the
+    previous CPU set to restore, or None when NVML or the affinity call is unavailable."""
+    try:
+        import pynvml
+        import torch
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        pynvml.nvmlInit()
+        try:
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            n = os.cpu_count() or 1
+            words = pynvml.nvmlDeviceGetCpuAffinity(h, (n + 63) // 64)
+        finally:
+            pynvml.nvmlShutdown()
+        cpus = {64 * k + b for k, wd in enumerate(words) for b in range(64) if (int(wd) >> b) & 1}
+        saved = os.sched_getaffinity(0)
+        cpus &= saved
+        if not cpus:
+            return None
+        os.sched_setaffinity(0, cpus)
+        return saved
+    except Exception:
+        return None
+
+
 def reference_cpu_1core(img_np, fmt, reps=3):
     """Best-of-reps wall time of one reference zap_bc_encode call on one thread (tex_bench.c:208-210)."""
     import oracle_lib
@@ -379,7 +404,10 @@ def main():
             "roofline": roofline, "gpu_launches": launches, "clocks": clocks.summary()}
 
     if rank == 0:
-        # e2e: host C ABI, pinned host memory, copies inside the timed region
+        # e2e: host C ABI, pinned host memory, copies inside the timed region. The buffers are allocated and the
+        # calls timed on the CPUs local to the GPU (its NUMA node), as a host pipeline would be deployed; pinned
+        # pages on the far socket would send every copy across the inter-socket link.
+        saved_cpus = bind_to_gpu_local_cpus(dev)
         host_in = torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True)
         host_in.copy_(texs[0].cpu())
         host_out = torch.empty(zap_b200.bc_size(W, H, zap_b200.BC7), dtype=torch.uint8, pin_memory=True)
@@ -398,7 +426,10 @@ def main():
         e2e_s = statistics.median(runs)
         line["e2e"] = {"value": mpix / e2e_s, "unit": "Mpix/s", "h2d_bytes_per_step": W * H * 4,
                        "d2h_bytes_per_step": int(hout.size), "api": "zap_tex_cuda_bc_encode (host pointers)",
-                       "ms_per_call_segments": [r * 1e3 for r in runs], "timing": "median of 5 segments of wall-clock calls"}
+                       "ms_per_call_segments": [r * 1e3 for r in runs], "timing": "median of 5 segments of wall-clock calls",
+                       "host_cpus": "GPU-local (NVML CPU affinity)" if saved_cpus is not None else "unbound"}
+        if saved_cpus is not None:
+            os.sched_setaffinity(0, saved_cpus)  # the CPU baseline below uses every host thread
         # reference CPU on the same texture; parity of the GPU output against it
         cpu = reference_cpu(hin, zap_b200.BC7, reps=2) if world == 1 else None
         if cpu is not None:
