@@ -583,8 +583,10 @@ def extra_workloads(args, dev, sm_mhz=None, sms=148):
         ms = time_device(step, steps, 0, 1)
         mps = steps * npix / 1e6 / (ms / 1e3)
         res[name] = {"Mpix_s": mps, "ms_per_encode": ms / steps, "GB_s_algorithmic": mps * 1e6 * alg_bytes_per_px / 1e9}
-        if name == "bc1_2048x2048":  # whole encode (one kernel) against the ALU roofline
-            res[name]["alu"] = alu_roofline("bc1_encode", (ops_per_texture("bc1_encode"), ms / steps), sm_mhz, sms)
+        counted = {"bc1_2048x2048": "bc1_encode", "bc4_2048x2048_r8": "bc4_encode", "bc5_2048x2048_rg8": "bc5_encode",
+                   "astc4x4_2048x2048": "astc_encode", "bc6h_2048x2048_rgb16f": "bc6h_encode"}.get(name)
+        if counted:  # the whole encode (all its kernels) against the ALU roofline
+            res[name]["alu"] = alu_roofline(counted, (ops_per_texture(counted), ms / steps), sm_mhz, sms)
 
     bench("bc1_512x512_config0", lambda k: S.colour_texture(512, 512, seed=k, device=dev), zap_b200.BC1, 512 * 512, 64, 4.5)
     bench("bc1_2048x2048", lambda k: S.colour_texture(2048, 2048, seed=k, device=dev), zap_b200.BC1, 2048 * 2048, 10, 4.5)
