@@ -52,16 +52,17 @@ __attribute__((visibility("default"))) int emu_bc6h_encode(const float *img, int
     int bw = (w + 3) / 4, bh = (h + 3) / 4;
     for (int by = 0; by < bh; by++)
         for (int bx = 0; bx < bw; bx++) {
-            HalfBlock B;
+            uint16_t t[48];
+            float U[48];
             for (int i = 0; i < 16; i++) {
                 int x = std::min(bx * 4 + (i & 3), w - 1), y = std::min(by * 4 + (i >> 2), h - 1);
                 for (int c = 0; c < 3; c++) {
                     uint32_t hb = f2h_unsigned(img[(size_t)y * stride + (size_t)x * 4 + c]);
-                    B.t[i][c] = hb;
-                    B.U[i][c] = (float)hb * 64.0f / 31.0f;
+                    t[3 * i + c] = (uint16_t)hb;
+                    U[3 * i + c] = (float)hb * 64.0f / 31.0f;
                 }
             }
-            uint4 v = bc6h_encode_block(B);
+            uint4 v = bc6h_encode_block(HalfRef{t, U, 1});
             memcpy(out + ((size_t)by * bw + bx) * 16, &v, 16);
         }
     return 0;

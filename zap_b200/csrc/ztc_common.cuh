@@ -18,7 +18,8 @@
 // Minimum resident 128-thread CTAs per SM requested from the register allocator, per kernel (tuned on B200:
 // more resident warps hide the latency of these long dependent integer / float chains; see the ncu summaries).
 // Measured on 2048x2048 encodes (re-swept after the loops were rolled): bc7_mode6 0.120 -> 0.113 ms at 6 (85
-// registers; the small spill stays in L1), BC1 -1.2 % at 8, ASTC single-partition -4 % at 5, BC6H -11 % at 3; the
+// registers; the small spill stays in L1), BC1 -1.2 % at 8, ASTC single-partition -4 % at 5, BC6H (texels staged in
+// shared memory) 0.383 -> 0.351 ms at 5 against 3; the
 // BC7 mode 5/1 kernel (124 registers already allow 4 CTAs) gains nothing from more.
 #ifndef ZTC_MINB_BC7_MODE6
 #define ZTC_MINB_BC7_MODE6 6
@@ -36,7 +37,7 @@
 #define ZTC_MINB_ASTC_SINGLE 5
 #endif
 #ifndef ZTC_MINB_BC6H
-#define ZTC_MINB_BC6H 3
+#define ZTC_MINB_BC6H 5
 #endif
 
 namespace ztc {
