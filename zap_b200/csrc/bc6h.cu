@@ -73,10 +73,46 @@ ZTC_DEV uint64_t bc6_fit(const HalfRef &B, const int e0[3], const int e1[3], uin
     return err;
 }
 
-// the search (zap_tex.h:873-931): PCA and bounding-box starts, each fitted and refitted by least squares up to
-// three times (stopping at SSE 0, a singular system or the first refit that does not lower the SSE); the texel
-// loops are rolled and the fit has one call site, which keeps the code small
-ZTC_DEV uint4 bc6h_encode_block(const HalfRef &B) {
+// Passes [first, last) of one start of the search (zap_tex.h:900-925): pass 0 fits the start's endpoints (lo, hi);
+// pass k > 0 is the k-th least-squares refit on the indices idx holds, which does not run at SSE 0, stops at a
+// singular system, and is dropped (ending the start) when it does not lower the SSE. e0, e1, idx, err take each
+// accepted pass. Returns true when every pass ran and the SSE is still above 0, so pass `last` would run. The
+// texel loops are rolled and the fit has one call site, which keeps the code small.
+ZTC_DEV bool bc6_passes(const HalfRef &B, const float lo[3], const float hi[3], int first, int last, int e0[3], int e1[3],
+                        uint64_t &idx, uint64_t &err) {
+    #pragma unroll 1
+    for (int pass = first; pass < last; pass++) {
+        int n0[3], n1[3];
+        if (pass == 0) {
+            #pragma unroll
+            for (int c = 0; c < 3; c++) { n0[c] = bc6_nearest(lo[c]); n1[c] = bc6_nearest(hi[c]); }
+        } else {
+            if (err == 0) return false;
+            float aa = 0, ab = 0, bb = 0, sa[3] = {0, 0, 0}, sb[3] = {0, 0, 0};
+            #pragma unroll 1
+            for (int i = 0; i < 16; i++) {
+                float w = (float)w4((int)((idx >> (4 * i)) & 15u)) / 64.0f, u = 1.0f - w;
+                aa = aa + u * u; ab = ab + u * w; bb = bb + w * w;
+                #pragma unroll
+                for (int c = 0; c < 3; c++) { const float uc = B.u(i, c); sa[c] = sa[c] + u * uc; sb[c] = sb[c] + w * uc; }
+            }
+            float det = aa * bb - ab * ab;
+            if (det < 1e-6f && det > -1e-6f) return false;
+            #pragma unroll
+            for (int c = 0; c < 3; c++) { n0[c] = bc6_nearest((sa[c] * bb - sb[c] * ab) / det); n1[c] = bc6_nearest((sb[c] * aa - sa[c] * ab) / det); }
+        }
+        uint64_t ni;
+        const uint64_t e2 = bc6_fit(B, n0, n1, ni);
+        if (pass > 0 && e2 >= err) return false;
+        err = e2; idx = ni;
+        #pragma unroll
+        for (int c = 0; c < 3; c++) { e0[c] = n0[c]; e1[c] = n1[c]; }
+    }
+    return err > 0;
+}
+
+// the two starts' endpoints (zap_tex.h:873-899): slo/shi[0] from the principal axis, [1] the bounding box
+ZTC_DEV void bc6_starts(const HalfRef &B, float slo[2][3], float shi[2][3]) {
     float mu0 = 0.0f, mu1 = 0.0f, mu2 = 0.0f;
     #pragma unroll 1
     for (int i = 0; i < 16; i++) { mu0 = mu0 + B.u(i, 0) / 16.0f; mu1 = mu1 + B.u(i, 1) / 16.0f; mu2 = mu2 + B.u(i, 2) / 16.0f; }
@@ -106,57 +142,16 @@ ZTC_DEV uint4 bc6h_encode_block(const HalfRef &B) {
         for (int c = 0; c < 3; c++) { const float uc = B.u(i, c); if (uc < bl[c]) bl[c] = uc; if (uc > bh[c]) bh[c] = uc; }
     }
     const float mu[3] = {mu0, mu1, mu2}, ax[3] = {v0, v1, v2};
-    uint64_t best = ~0ull, bidx = 0, idx = 0, err = 0;
-    int be0[3] = {0, 0, 0}, be1[3] = {0, 0, 0}, e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0};
-    int start = 0, pass = 0;  // pass 0: the start's first fit; 1..3: least-squares refits
-    #pragma unroll 1
-    for (;;) {
-        int n0[3], n1[3];
-        bool fit = true;
-        if (pass == 0) {
-            #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                float lo = start ? bl[c] : mu[c] + ax[c] * tl / n2, hi = start ? bh[c] : mu[c] + ax[c] * th / n2;
-                n0[c] = bc6_nearest(lo); n1[c] = bc6_nearest(hi);
-            }
-        } else {
-            float aa = 0, ab = 0, bb = 0, sa[3] = {0, 0, 0}, sb[3] = {0, 0, 0};
-            #pragma unroll 1
-            for (int i = 0; i < 16; i++) {
-                float w = (float)w4((int)((idx >> (4 * i)) & 15u)) / 64.0f, u = 1.0f - w;
-                aa = aa + u * u; ab = ab + u * w; bb = bb + w * w;
-                #pragma unroll
-                for (int c = 0; c < 3; c++) { const float uc = B.u(i, c); sa[c] = sa[c] + u * uc; sb[c] = sb[c] + w * uc; }
-            }
-            float det = aa * bb - ab * ab;
-            if (det < 1e-6f && det > -1e-6f) fit = false;
-            #pragma unroll
-            for (int c = 0; c < 3; c++) { n0[c] = bc6_nearest((sa[c] * bb - sb[c] * ab) / det); n1[c] = bc6_nearest((sb[c] * aa - sa[c] * ab) / det); }
-        }
-        bool done = !fit;
-        if (fit) {
-            uint64_t ni;
-            const uint64_t e2 = bc6_fit(B, n0, n1, ni);
-            if (pass == 0 || e2 < err) {
-                err = e2; idx = ni;
-                #pragma unroll
-                for (int c = 0; c < 3; c++) { e0[c] = n0[c]; e1[c] = n1[c]; }
-                done = ++pass == 4 || err == 0;
-            } else {
-                done = true;
-            }
-        }
-        if (done) {  // the start is finished: keep it if it is the best so far
-            if (err < best) {
-                best = err; bidx = idx;
-                #pragma unroll
-                for (int c = 0; c < 3; c++) { be0[c] = e0[c]; be1[c] = e1[c]; }
-            }
-            if (++start == 2) break;
-            pass = 0;
-        }
+    #pragma unroll
+    for (int c = 0; c < 3; c++) {
+        slo[0][c] = mu[c] + ax[c] * tl / n2; shi[0][c] = mu[c] + ax[c] * th / n2;
+        slo[1][c] = bl[c]; shi[1][c] = bh[c];
     }
-    if (bidx & 8u) {  // anchor MSB must be 0
+}
+
+// mode 11 block (zap_tex.h:926-931): anchor index MSB 0 (else swap the endpoints and invert the indices)
+ZTC_DEV uint4 bc6_pack(int be0[3], int be1[3], uint64_t bidx) {
+    if (bidx & 8u) {
         #pragma unroll
         for (int c = 0; c < 3; c++) { int s = be0[c]; be0[c] = be1[c]; be1[c] = s; }
         bidx ^= ~0ull;
@@ -173,27 +168,120 @@ ZTC_DEV uint4 bc6h_encode_block(const HalfRef &B) {
     return make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
 }
 
-constexpr int kBc6hCta = 128;
-__global__ void __launch_bounds__(kBc6hCta, ZTC_MINB_BC6H) bc6h_kernel(SrcHdr src, int bw, int by0, int nblocks, uint8_t *__restrict__ out) {
-    // column threadIdx.x: this thread's block (read only by this thread)
-    __shared__ uint16_t s_t[48][kBc6hCta];
-    __shared__ float s_U[48][kBc6hCta];
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nblocks) return;
-    int bx = b % bw, by = by0 + b / bw;
-    #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        int x = min(bx * 4 + (i & 3), src.w - 1), y = min(by * 4 + (i >> 2), src.h - 1);
-        size_t off = (size_t)y * src.stride + (size_t)x * (size_t)src.channels;
-        #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            uint32_t h = src.f32 ? f2h_unsigned(__ldg((const float *)src.base + off + c))
-                                 : half_to_unsigned(__ldg((const unsigned short *)src.base + off + c));
-            s_t[3 * i + c][threadIdx.x] = (uint16_t)h;
-            s_U[3 * i + c][threadIdx.x] = (float)h * 64.0f / 31.0f;
+// the search (zap_tex.h:873-931), one thread: both starts, all passes, the first start of least SSE
+ZTC_DEV uint4 bc6h_encode_block(const HalfRef &B) {
+    float slo[2][3], shi[2][3];
+    bc6_starts(B, slo, shi);
+    uint64_t best = ~0ull, bidx = 0;
+    int be0[3] = {0, 0, 0}, be1[3] = {0, 0, 0};
+    #pragma unroll 1
+    for (int start = 0; start < 2; start++) {
+        int e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0};
+        uint64_t idx = 0, err = 0;
+        bc6_passes(B, slo[start], shi[start], 0, 4, e0, e1, idx, err);
+        if (err < best) {
+            best = err; bidx = idx;
+            #pragma unroll
+            for (int c = 0; c < 3; c++) { be0[c] = e0[c]; be1[c] = e1[c]; }
         }
     }
-    store_block16(out + (size_t)b * 16, bc6h_encode_block(HalfRef{&s_t[0][threadIdx.x], &s_U[0][threadIdx.x], kBc6hCta}));
+    return bc6_pack(be0, be1, bidx);
+}
+
+ZTC_DEV uint64_t pack_ends10(const int e0[3], const int e1[3]) {
+    uint64_t v = 0;
+    #pragma unroll
+    for (int c = 0; c < 3; c++) v |= ((uint64_t)e0[c] << (10 * c)) | ((uint64_t)e1[c] << (30 + 10 * c));
+    return v;
+}
+ZTC_DEV void unpack_ends10(uint64_t v, int e0[3], int e1[3]) {
+    #pragma unroll
+    for (int c = 0; c < 3; c++) { e0[c] = (int)((v >> (10 * c)) & 1023u); e1[c] = (int)((v >> (30 + 10 * c)) & 1023u); }
+}
+
+// The search for the CTA's blocks, one per thread, with each start's last least-squares refit compacted: every
+// thread runs its block's two starts up to the third pass; the (block, start) pairs whose fourth pass would run
+// (a tenth of them on the HDR test content, yet nearly every warp holds one) are listed in shared memory, and the
+// first threads of the CTA run those passes on the owners' texels. Same bytes as bc6h_encode_block. Every thread
+// of the CTA calls it (it synchronises); a `valid` thread's block is in column threadIdx.x of s_t / s_U.
+template <int CTA>
+__device__ __forceinline__ uint4 bc6h_encode_cta(bool valid, uint16_t (*s_t)[CTA], float (*s_U)[CTA]) {
+    __shared__ uint64_t s_ends[2][CTA], s_idx[2][CTA], s_err[2][CTA];
+    __shared__ int s_wcnt[2][CTA / 32];
+    __shared__ uint16_t s_list[2 * CTA];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float slo[2][3], shi[2][3];
+    if (valid) bc6_starts(HalfRef{&s_t[0][tid], &s_U[0][tid], CTA}, slo, shi);
+    bool more0 = false, more1 = false;
+    int total = 0;
+    #pragma unroll 1
+    for (int job = 0; job < 4; job++) {
+        if (job == 2) {  // list the (block, start) pairs whose fourth pass would run, in thread order
+            const unsigned b0 = __ballot_sync(0xFFFFFFFFu, more0), b1 = __ballot_sync(0xFFFFFFFFu, more1);
+            if (lane == 0) { s_wcnt[0][warp] = __popc(b0); s_wcnt[1][warp] = __popc(b1); }
+            __syncthreads();
+            int base0 = 0, base1 = 0, t0 = 0, t1 = 0;
+            #pragma unroll
+            for (int w = 0; w < CTA / 32; w++) {
+                const int c0 = s_wcnt[0][w], c1 = s_wcnt[1][w];
+                base0 += w < warp ? c0 : 0; base1 += w < warp ? c1 : 0; t0 += c0; t1 += c1;
+            }
+            const unsigned below = (1u << lane) - 1u;
+            if (more0) s_list[base0 + __popc(b0 & below)] = (uint16_t)(tid << 1);
+            if (more1) s_list[t0 + base1 + __popc(b1 & below)] = (uint16_t)((tid << 1) | 1);
+            total = t0 + t1;
+            __syncthreads();
+        }
+        int owner = tid, st = job, first = 0, last = 3;
+        bool active = valid;
+        if (job >= 2) {
+            const int k = tid + (job - 2) * CTA;
+            active = k < total;
+            if (active) { owner = s_list[k] >> 1; st = s_list[k] & 1; }
+            first = 3; last = 4;
+        }
+        if (active) {
+            int e0[3] = {0, 0, 0}, e1[3] = {0, 0, 0};
+            uint64_t idx = 0, err = 0;
+            if (job >= 2) { unpack_ends10(s_ends[st][owner], e0, e1); idx = s_idx[st][owner]; err = s_err[st][owner]; }
+            const uint64_t e_in = err;
+            const bool more = bc6_passes(HalfRef{&s_t[0][owner], &s_U[0][owner], CTA}, slo[st], shi[st], first, last, e0, e1, idx, err);
+            if (job < 2 || err < e_in) { s_ends[st][owner] = pack_ends10(e0, e1); s_idx[st][owner] = idx; s_err[st][owner] = err; }
+            if (job == 0) more0 = more;
+            if (job == 1) more1 = more;
+        }
+    }
+    __syncthreads();
+    if (!valid) return make_uint4(0, 0, 0, 0);
+    const int st = s_err[1][tid] < s_err[0][tid] ? 1 : 0;  // the first start of least SSE
+    int be0[3], be1[3];
+    unpack_ends10(s_ends[st][tid], be0, be1);
+    return bc6_pack(be0, be1, s_idx[st][tid]);
+}
+
+constexpr int kBc6hCta = 128;
+__global__ void __launch_bounds__(kBc6hCta, ZTC_MINB_BC6H) bc6h_kernel(SrcHdr src, int bw, int by0, int nblocks, uint8_t *__restrict__ out) {
+    __shared__ uint16_t s_t[48][kBc6hCta];  // column threadIdx.x: this thread's block
+    __shared__ float s_U[48][kBc6hCta];
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = b < nblocks;
+    if (valid) {
+        const int bx = b % bw, by = by0 + b / bw;
+        #pragma unroll
+        for (int i = 0; i < 16; i++) {
+            int x = min(bx * 4 + (i & 3), src.w - 1), y = min(by * 4 + (i >> 2), src.h - 1);
+            size_t off = (size_t)y * src.stride + (size_t)x * (size_t)src.channels;
+            #pragma unroll
+            for (int c = 0; c < 3; c++) {
+                uint32_t h = src.f32 ? f2h_unsigned(__ldg((const float *)src.base + off + c))
+                                     : half_to_unsigned(__ldg((const unsigned short *)src.base + off + c));
+                s_t[3 * i + c][threadIdx.x] = (uint16_t)h;
+                s_U[3 * i + c][threadIdx.x] = (float)h * 64.0f / 31.0f;
+            }
+        }
+    }
+    const uint4 blk = bc6h_encode_cta<kBc6hCta>(valid, s_t, s_U);
+    if (valid) store_block16(out + (size_t)b * 16, blk);
 }
 
 }  // namespace ztc
