@@ -272,28 +272,20 @@ ZTC_DEV int astc_fit_weights(TexRef ts, uint32_t cm, int cem, int wb, const uint
     return err;
 }
 
-// one trial configuration (zap_tex.h:1212-1244) from the partitions' principal-axis endpoints lo / hi (which do
-// not depend on the configuration, so callers compute them once per block and partition). nc: 3 (CEM 8) or 4
-// (CEM 12) channels. codes: byte per value, partition 0 first. Returns the SSE; wt: 16 weight bytes.
+// Passes [first, last) of one trial configuration (zap_tex.h:1212-1244): pass 0 fits the weights to the endpoint
+// codes code / uv; pass k > 0 is the k-th least-squares refit on the weights wt holds, which stops at SSE 0 or at
+// the first refit that does not lower the SSE (a partition whose system is singular keeps its codes). code, uv, wt
+// and err take each accepted pass. Returns true when every pass ran and the SSE is still above 0, so pass `last`
+// would run. One fit call site keeps the code small.
 template <int LMAX, int PARTS>
-ZTC_DEV int astc_try(TexRef ts, const AstcSmem &S, int cfg, int nc, uint32_t pm, const float lo[PARTS][4], const float hi[PARTS][4],
-                     uint32_t codes[4], uint32_t wt[4]) {
+ZTC_DEV bool astc_passes(TexRef ts, const AstcSmem &S, int cfg, int nc, uint32_t pm, int first, int last, int code[PARTS][8],
+                         int uv[PARTS][8], uint32_t wt[4], int &err) {
     const AstcCfg &C = S.cfg[cfg];
     const int cem = C.cem, wb = C.wb, nv = C.nv;
     const uint32_t cm = nc == 4 ? 0xFFFFFFFFu : 0x00FFFFFFu;
     const uint8_t *wq = S.wq[wb - 2];
-    int code[PARTS][8], uv[PARTS][8];
-    #pragma unroll
-    for (int k = 0; k < PARTS; k++) {
-        #pragma unroll
-        for (int v = 0; v < 8; v++) { code[k][v] = 0; uv[k][v] = 0; }
-        astc_quant(S, cfg, nv, lo[k], hi[k], code[k], uv[k]);
-    }
-    int err = 0;
-    // pass 0 fits the weights to the PCA endpoints; passes 1..3 are the reference's least-squares refits, which
-    // stop at SSE 0 or at the first one that does not lower the SSE. One fit call site keeps the code small.
     #pragma unroll 1
-    for (int it = 0; it < 4; it++) {
+    for (int it = first; it < last; it++) {
         int tc[PARTS][8], tuv[PARTS][8];
         #pragma unroll
         for (int k = 0; k < PARTS; k++)
@@ -331,7 +323,7 @@ ZTC_DEV int astc_try(TexRef ts, const AstcSmem &S, int cfg, int nc, uint32_t pm,
         }
         uint32_t tw[4];
         const int e = astc_fit_weights<LMAX, PARTS>(ts, cm, cem, wb, wq, pm, tuv, tw);
-        if (it > 0 && e >= err) break;
+        if (it > 0 && e >= err) return false;
         err = e;
         #pragma unroll
         for (int k = 0; k < 4; k++) wt[k] = tw[k];
@@ -339,8 +331,27 @@ ZTC_DEV int astc_try(TexRef ts, const AstcSmem &S, int cfg, int nc, uint32_t pm,
         for (int k = 0; k < PARTS; k++)
             #pragma unroll
             for (int v = 0; v < 8; v++) { code[k][v] = tc[k][v]; uv[k][v] = tuv[k][v]; }
-        if (err <= 0) break;
+        if (err <= 0) return false;
     }
+    return true;
+}
+
+// a trial's starting endpoint codes (code) and unquantised values (uv) from the partitions' endpoints lo / hi
+template <int LMAX, int PARTS>
+ZTC_DEV void astc_trial_codes(const AstcSmem &S, int cfg, const float lo[PARTS][4], const float hi[PARTS][4], int code[PARTS][8],
+                              int uv[PARTS][8]) {
+    const int nv = S.cfg[cfg].nv;
+    #pragma unroll
+    for (int k = 0; k < PARTS; k++) {
+        #pragma unroll
+        for (int v = 0; v < 8; v++) { code[k][v] = 0; uv[k][v] = 0; }
+        astc_quant(S, cfg, nv, lo[k], hi[k], code[k], uv[k]);
+    }
+}
+// the codes as the block stores them: a byte per value, partition 0 first
+template <int PARTS>
+ZTC_DEV void astc_codes_bytes(const AstcSmem &S, int cfg, const int code[PARTS][8], uint32_t codes[4]) {
+    const int nv = S.cfg[cfg].nv;
     #pragma unroll
     for (int k = 0; k < 4; k++) codes[k] = 0;
     #pragma unroll
@@ -348,6 +359,17 @@ ZTC_DEV int astc_try(TexRef ts, const AstcSmem &S, int cfg, int nc, uint32_t pm,
         #pragma unroll
         for (int v = 0; v < 8; v++)
             if (v < nv) set8(codes, k * nv + v, (uint32_t)code[k][v]);
+}
+// one trial configuration (zap_tex.h:1212-1244) from the partitions' principal-axis endpoints lo / hi (which do
+// not depend on the configuration, so callers compute them once per block and partition). nc: 3 (CEM 8) or 4
+// (CEM 12) channels. codes: byte per value, partition 0 first. Returns the SSE; wt: 16 weight bytes.
+template <int LMAX, int PARTS>
+ZTC_DEV int astc_try(TexRef ts, const AstcSmem &S, int cfg, int nc, uint32_t pm, const float lo[PARTS][4], const float hi[PARTS][4],
+                     uint32_t codes[4], uint32_t wt[4]) {
+    int code[PARTS][8], uv[PARTS][8], err = 0;
+    astc_trial_codes<LMAX, PARTS>(S, cfg, lo, hi, code, uv);
+    astc_passes<LMAX, PARTS>(ts, S, cfg, nc, pm, 0, 4, code, uv, wt, err);
+    astc_codes_bytes<PARTS>(S, cfg, code, codes);
     return err;
 }
 
@@ -369,6 +391,110 @@ ZTC_DEV int astc_single_block(const uint32_t t[16], TexRef ts, const AstcSmem &S
             best = e; bc = cfg;
             #pragma unroll
             for (int q = 0; q < 4; q++) { bcodes[q] = codes[q]; bwt[q] = wt[q]; }
+        }
+    }
+    return best;
+}
+
+ZTC_DEV uint64_t bytes8(const int v[8]) {
+    uint64_t r = 0;
+    #pragma unroll
+    for (int k = 0; k < 8; k++) r |= (uint64_t)(v[k] & 0xFF) << (8 * k);
+    return r;
+}
+ZTC_DEV void unbytes8(uint64_t r, int v[8]) {
+    #pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = (int)((r >> (8 * k)) & 0xFFu);
+}
+
+// The three single-partition trials for the CTA's blocks, one per thread, with each trial's third and fourth fits
+// compacted: every thread runs its block's trials up to the second fit; the (block, trial) pairs whose third fit
+// would run (a third of them on the test content, yet nearly every warp holds one) are listed in shared memory and
+// the first threads of the CTA finish them on the owners' texels. Same result as astc_single_block. Every thread of
+// the CTA calls it (it synchronises); a `valid` thread's block is in t and in column threadIdx.x of s_tex.
+template <int CTA>
+__device__ __forceinline__ int astc_single_cta(bool valid, const uint32_t t[16], uint32_t (*s_tex)[CTA], const AstcSmem &S, bool opaque,
+                                               int &bc, uint32_t bcodes[4], uint32_t bwt[4]) {
+    __shared__ uint64_t s_code[3][CTA], s_uv[3][CTA];
+    __shared__ uint4 s_wt[3][CTA];
+    __shared__ int s_err[3][CTA], s_wcnt[3][CTA / 32];
+    __shared__ uint16_t s_list[3 * CTA];
+    __shared__ uint8_t s_opq[CTA];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float lo[1][4], hi[1][4];
+    if (valid) {
+        if (opaque) pca_endpoints<3>(t, 0xFFFFu, lo[0], hi[0]);
+        else pca_endpoints<4>(t, 0xFFFFu, lo[0], hi[0]);
+        s_opq[tid] = opaque;
+    }
+    unsigned mores = 0;  // bit k: trial k's third fit would run
+    int total = 0;
+    #pragma unroll 1
+    for (int job = 0; job < 6; job++) {
+        if (job == 3) {  // list the (block, trial) pairs whose third fit would run, trial by trial in thread order
+            unsigned bal[3];
+            #pragma unroll
+            for (int k = 0; k < 3; k++) {
+                bal[k] = __ballot_sync(0xFFFFFFFFu, (mores >> k) & 1u);
+                if (lane == 0) s_wcnt[k][warp] = __popc(bal[k]);
+            }
+            __syncthreads();
+            int off = 0;
+            #pragma unroll
+            for (int k = 0; k < 3; k++) {
+                int base = 0, tk = 0;
+                #pragma unroll
+                for (int w = 0; w < CTA / 32; w++) { const int c = s_wcnt[k][w]; base += w < warp ? c : 0; tk += c; }
+                if ((mores >> k) & 1u) s_list[off + base + __popc(bal[k] & ((1u << lane) - 1u))] = (uint16_t)((tid << 2) | k);
+                off += tk;
+            }
+            total = off;
+            __syncthreads();
+        }
+        int owner = tid, k = job, first = 0, last = 2;
+        bool active = valid;
+        if (job >= 3) {
+            const int q = tid + (job - 3) * CTA;
+            active = q < total;
+            if (active) { owner = s_list[q] >> 2; k = s_list[q] & 3; }
+            first = 2; last = 4;
+        }
+        if (active) {
+            const bool opq = job < 3 ? opaque : s_opq[owner] != 0;
+            const int cfg = opq ? k : 3 + k;
+            int code[1][8], uv[1][8], err = 0;
+            uint32_t wt[4] = {0, 0, 0, 0};
+            if (job < 3) {
+                astc_trial_codes<32, 1>(S, cfg, lo, hi, code, uv);
+            } else {
+                unbytes8(s_code[k][owner], code[0]); unbytes8(s_uv[k][owner], uv[0]);
+                const uint4 w = s_wt[k][owner];
+                wt[0] = w.x; wt[1] = w.y; wt[2] = w.z; wt[3] = w.w;
+                err = s_err[k][owner];
+            }
+            const int e_in = err;
+            const bool more = astc_passes<32, 1>(TexRef{&s_tex[0][owner], CTA}, S, cfg, opq ? 3 : 4, 0u, first, last, code, uv, wt, err);
+            if (job < 3 || err < e_in) {
+                s_code[k][owner] = bytes8(code[0]); s_uv[k][owner] = bytes8(uv[0]);
+                s_wt[k][owner] = make_uint4(wt[0], wt[1], wt[2], wt[3]); s_err[k][owner] = err;
+            }
+            if (job < 3 && more) mores |= 1u << k;
+        }
+    }
+    __syncthreads();
+    int best = 1 << 30;
+    bc = 0;
+    if (!valid) return best;
+    #pragma unroll 1
+    for (int k = 0; k < 3; k++) {  // the first trial of least SSE (zap_tex.h:1306-1318)
+        const int e = s_err[k][tid];
+        if (e < best) {
+            best = e; bc = opaque ? k : 3 + k;
+            int code[1][8];
+            unbytes8(s_code[k][tid], code[0]);
+            astc_codes_bytes<1>(S, bc, code, bcodes);
+            const uint4 w = s_wt[k][tid];
+            bwt[0] = w.x; bwt[1] = w.y; bwt[2] = w.z; bwt[3] = w.w;
         }
     }
     return best;
@@ -416,21 +542,21 @@ ZTC_DEV uint4 astc_pack(const AstcSmem &S, int cfg, int seed, const uint32_t cod
 __global__ void __launch_bounds__(128, ZTC_MINB_ASTC_SINGLE) astc_single_kernel(SrcU8 src, int bw, int by0, int nblocks, uint8_t *__restrict__ out,
                                                           uint32_t *__restrict__ count, uint2 *__restrict__ items) {
     __shared__ AstcSmem S;
-    __shared__ uint32_t s_tex[16][128];  // column threadIdx.x: this thread's block (read only by this thread)
+    __shared__ uint32_t s_tex[16][128];  // column threadIdx.x: this thread's block
     load_smem(S);
     __syncthreads();
     int b = blockIdx.x * blockDim.x + threadIdx.x;
-    bool valid = b < nblocks, hard = false;
-    int best = 1 << 30;
+    bool valid = b < nblocks, hard = false, opaque = true;
+    uint32_t t[16];
     if (valid) {
-        uint32_t t[16];
         gather_block(src, b % bw, by0 + b / bw, t);
-        bool opaque = true;
         #pragma unroll
         for (int i = 0; i < 16; i++) { opaque &= (t[i] >> 24) == 255u; s_tex[i][threadIdx.x] = t[i]; }
-        int bc = 0;
-        uint32_t bcodes[4] = {0, 0, 0, 0}, bwt[4] = {0, 0, 0, 0};
-        best = astc_single_block(t, TexRef{&s_tex[0][threadIdx.x], 128}, S, opaque, bc, bcodes, bwt);
+    }
+    int bc = 0;
+    uint32_t bcodes[4] = {0, 0, 0, 0}, bwt[4] = {0, 0, 0, 0};
+    const int best = astc_single_cta<128>(valid, t, s_tex, S, opaque, bc, bcodes, bwt);
+    if (valid) {
         store_block16(out + (size_t)b * 16, astc_pack(S, bc, 0, bcodes, bwt));
         hard = opaque && best > 16 * 3 * 4;  // zap_tex.h:1323
     }
