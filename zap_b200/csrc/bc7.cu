@@ -234,6 +234,11 @@ __device__ __forceinline__ int mode6_encode_cta(bool valid, const uint32_t t[16]
     return s_err[tid];
 }
 
+// batched modes 5/1: rounds of one block per group with a CTA barrier per round (1), or each group through its blocks
+// on its own (0). Measured on 256 textures: 0.578 ms (0) -> 0.537 ms (1), "no_instruction" stalls falling.
+#ifndef ZTC_BATCH_HARD_SYNC
+#define ZTC_BATCH_HARD_SYNC 1
+#endif
 // CTA sizes of the mode-6 kernel. A larger CTA shares one compacted-refit list among more blocks (2048x2048:
 // 64 threads 0.119 ms, 128 0.105, 256 0.099, 384 0.100, 512 0.103); a launch smaller than one full wave of large
 // CTAs takes the small size instead, which keeps more SMs busy (512x512 in 256-thread CTAs: 64 CTAs for 148 SMs).
@@ -693,7 +698,18 @@ batch_bc7_hard_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__r
     const int ngroups = gridDim.x * (blockDim.x / kBc7Group);
     const int n = (int)*(volatile const uint32_t *)count;
     uint32_t *gtex = s_gtex[threadIdx.x / kBc7Group];
-    for (int it = blockIdx.x * (blockDim.x / kBc7Group) + (threadIdx.x / kBc7Group); it < n; it += ngroups) {
+    const int gid = blockIdx.x * (blockDim.x / kBc7Group) + (threadIdx.x / kBc7Group);
+#if ZTC_BATCH_HARD_SYNC
+    // rounds of one block per group, the CTA's groups starting each round together: their warps then run the same
+    // phase of the search at the same time, which keeps the code the SM fetches small
+    const int rounds = (n + ngroups - 1) / ngroups;
+    for (int r = 0; r < rounds; r++) {
+        __syncthreads();
+        const int it = r * ngroups + gid;
+        if (it >= n) continue;
+#else
+    for (int it = gid; it < n; it += ngroups) {
+#endif
         const uint2 item = items[it];
         int lo = 0, hi = nlevels - 1;  // last level whose first id is <= the block's id
         while (lo < hi) {
