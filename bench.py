@@ -99,6 +99,8 @@ def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":  # CPU only: rank 0 runs the reference, the other ranks exit; no process group
+        return world, rank, local
     if world > 1:
         import datetime
         import torch.distributed as dist
@@ -322,9 +324,6 @@ def main():
         return
     if args.impl == "reference":
         run_reference(args, world, rank)
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
         return
     import numpy as np
     import torch

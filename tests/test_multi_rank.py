@@ -58,3 +58,20 @@ def test_two_gloo_ranks_take_the_slowest_time():
         assert value == pytest.approx(2 * 4 * 4.194304 / 0.015)
         if rank == 1:
             assert printed == ""  # the reference arm prints on rank 0 only
+
+
+def test_reference_arm_under_torchrun_prints_once(tmp_path):
+    """`bench.py --impl reference` launched by torchrun with two ranks: rank 0 alone times the reference and prints
+    one JSON line, the other rank exits 0 without work, and no process group is needed (no GPU here)."""
+    import json
+    import subprocess
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libzapref.so")):
+        pytest.skip("the reference library is not built here")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
+           "--master-port", str(_free_port()), os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+           "--steps", "1", "--warmup", "0"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1 and lines[0]["impl"] == "reference" and lines[0]["value"] > 0
+    assert lines[0]["e2e"]["h2d_bytes_per_step"] == 0 and lines[0]["cpu_baseline"]["kind"] == "reference"
