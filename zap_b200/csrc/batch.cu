@@ -27,7 +27,7 @@
 namespace {
 
 constexpr int kClasses = 5;  // BC1, BC3, BC4, BC5, BC7 (format id == class id)
-constexpr int kHardCounter = 8;  // d_counters slot of the BC7 work-list length
+constexpr int kHardCounter = 8;  // d_counters slots of the BC7 work-list lengths: after mode 6 (8), after mode 5 (9)
 const int kCtaChoices[3] = {64, 128, 256};
 
 struct HostLevel {
@@ -59,7 +59,7 @@ struct zap_tex_cuda_batch {
     std::vector<ztc::BatchMipTile *> d_mip_tiles;
     std::vector<int> n_mip_tiles;
     uint32_t *d_counters = nullptr;          // [f]: tile counter of class f; [kHardCounter]: BC7 work-list length
-    uint2 *d_hard_items = nullptr;           // BC7 work list: (batch-wide block id, mode 6 SSE)
+    uint2 *d_hard_items = nullptr;           // BC7 work lists: (batch-wide block id, SSE) after mode 6, then after mode 5
     uint32_t *d_bc7_bases = nullptr;         // first batch-wide id of each BC7 level, ascending
     int *d_bc7_level_of = nullptr;           // ... and that level's index in d_levels
     int n_bc7_levels = 0, hard_grid = 1;
@@ -120,7 +120,7 @@ cudaError_t launch_encode(zap_tex_cuda_batch *b, int f, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     if (f == ZTC_BC7) {
         uint32_t *hard_count = b->d_counters + kHardCounter;
-        if ((e = cudaMemsetAsync(hard_count, 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(hard_count, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
         {
             ztc::TraceScope tr("batch_bc7_mode6", s);
             ztc::trace_units(b->blocks[f]);
@@ -131,7 +131,7 @@ cudaError_t launch_encode(zap_tex_cuda_batch *b, int f, cudaStream_t s) {
         ztc::TraceScope tr("batch_bc7_modes51", s);
         ztc::trace_units_dev(hard_count, s);
         return ztc_launch_batch_bc7_hard(b->hard_grid, b->d_levels, b->d_bc7_bases, b->d_bc7_level_of, b->n_bc7_levels, hard_count,
-                                         b->d_hard_items, s);
+                                         b->d_hard_items, hard_count + 1, b->d_hard_items + b->blocks[f], s);
     }
     ztc::TraceScope tr(f == ZTC_BC1 ? "batch_bc1" : f == ZTC_BC3 ? "batch_bc3" : f == ZTC_BC4 ? "batch_bc4" : "batch_bc5", s);
     ztc::trace_units(b->blocks[f]);
@@ -347,7 +347,7 @@ int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *it
     BTRY(cudaMemcpy(b->d_levels, dl.data(), dl.size() * sizeof(ztc::BatchLevel), cudaMemcpyHostToDevice), "upload levels");
     if (bc7_blocks) {  // BC7 work list: room for every BC7 block of the batch
         b->n_bc7_levels = (int)bc7_bases.size();
-        BTRY(cudaMalloc(&b->d_hard_items, bc7_blocks * sizeof(uint2)), "cudaMalloc(BC7 work list)");
+        BTRY(cudaMalloc(&b->d_hard_items, 2 * bc7_blocks * sizeof(uint2)), "cudaMalloc(BC7 work lists)");
         BTRY(cudaMalloc(&b->d_bc7_bases, bc7_bases.size() * sizeof(uint32_t)), "cudaMalloc(BC7 level bases)");
         BTRY(cudaMalloc(&b->d_bc7_level_of, bc7_level_of.size() * sizeof(int)), "cudaMalloc(BC7 level map)");
         BTRY(cudaMemcpy(b->d_bc7_bases, bc7_bases.data(), bc7_bases.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload BC7 bases");

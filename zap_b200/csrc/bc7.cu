@@ -234,11 +234,6 @@ __device__ __forceinline__ int mode6_encode_cta(bool valid, const uint32_t t[16]
     return s_err[tid];
 }
 
-// batched modes 5/1: rounds of one block per group with a CTA barrier per round (1), or each group through its blocks
-// on its own (0). Measured on 256 textures: 0.578 ms (0) -> 0.537 ms (1), "no_instruction" stalls falling.
-#ifndef ZTC_BATCH_HARD_SYNC
-#define ZTC_BATCH_HARD_SYNC 1
-#endif
 // CTA sizes of the mode-6 kernel. A larger CTA shares one compacted-refit list among more blocks (2048x2048:
 // 64 threads 0.119 ms, 128 0.105, 256 0.099, 384 0.100, 512 0.103); a launch smaller than one full wave of large
 // CTAs takes the small size instead, which keeps more SMs busy (512x512 in 256-thread CTAs: 64 CTAs for 148 SMs).
@@ -375,13 +370,12 @@ ZTC_DEV int m5_part(TexRef ts, int rot, bool alpha, float lo[3], float hi[3], in
 // partition score (zap_tex.h:722-748) from the 9 moment sums of subset 1 (s1, over its n1 texels, added in texel
 // order) and of the whole block (tot); subset 0's sums are tot - s1, as in the reference
 ZTC_DEV float partition_score(const float s1[9], int n1, const float tot[9]) {
-    float s0[9];
-    #pragma unroll
-    for (int j = 0; j < 9; j++) s0[j] = tot[j] - s1[j];
     float score = 0.0f;
-    #pragma unroll
-    for (int k = 0; k < 2; k++) {
-        const float *m = k ? s1 : s0;
+    #pragma unroll 1
+    for (int k = 0; k < 2; k++) {  // rolled (with the power iteration): one copy of the divisions
+        float m[9];
+        #pragma unroll
+        for (int j = 0; j < 9; j++) m[j] = k ? s1[j] : tot[j] - s1[j];
         float n = (float)(k ? n1 : 16 - n1);
         if (n < 2) continue;
         float S00 = m[3] - m[0] * m[0] / n, S01 = m[6] - m[0] * m[1] / n, S02 = m[7] - m[0] * m[2] / n;
@@ -390,7 +384,7 @@ ZTC_DEV float partition_score(const float s1[9], int n1, const float tot[9]) {
         if (S00 >= S11 && S00 >= S22) { a0 = S00; a1 = S01; a2 = S02; }
         else if (S11 >= S22) { a0 = S01; a1 = S11; a2 = S12; }
         else { a0 = S02; a1 = S12; a2 = S22; }
-        #pragma unroll
+        #pragma unroll 1
         for (int it = 0; it < 3; it++) {
             float v0 = S00 * a0 + S01 * a1 + S02 * a2;
             float v1 = S01 * a0 + S11 * a1 + S12 * a2;
@@ -417,205 +411,230 @@ ZTC_DEV bool rank_less(float e, int p, float e2, int p2) { return e < e2 || (!(e
 constexpr int kBc7Group = 8;
 constexpr int kMode1Tries = 4;  // partitions fully fitted after ranking (ZAP__BC7_M1K, zap_tex.h:750-752)
 
+// Mode 5 of one block (zap_tex.h:659-684) by the 8 lanes of a group (lane l, group mask gmask): when the best
+// rotation's SSE is below err, err becomes that SSE, blk the mode-5 block, and the call returns true. Every lane
+// holds the block's texels t, so all group-level branches are group-uniform; ts: the group's shared-memory copy.
+__device__ __forceinline__ bool bc7_group_mode5(const uint32_t t[16], TexRef ts, int &err, uint4 &blk, const int l,
+                                                const unsigned gmask) {
+    // ---- mode 5: lane = rotation * 2 + part (zap_tex.h:659-684)
+    const int rot = l >> 1;
+    const bool alpha_part = l & 1;
+    int q5[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    uint32_t i5 = 0;
+    float lo5[3] = {255.0f, 0.0f, 0.0f}, hi5[3] = {0.0f, 0.0f, 0.0f};
+    if (!alpha_part) {  // colour part starts from the principal axis of the rotated RGB
+        uint32_t r[16];
+        #pragma unroll
+        for (int i = 0; i < 16; i++) r[i] = rotate_texel(t[i], rot);
+        float lo[4], hi[4];
+        pca_endpoints<3>(r, 0xFFFFu, lo, hi);
+        #pragma unroll
+        for (int c = 0; c < 3; c++) { lo5[c] = lo[c]; hi5[c] = hi[c]; }
+    } else {  // alpha part starts from the rotated alpha's range
+        #pragma unroll
+        for (int i = 0; i < 16; i++) {
+            float a = (float)(rotate_texel(t[i], rot) >> 24);
+            if (a < lo5[0]) lo5[0] = a;
+            if (a > hi5[0]) hi5[0] = a;
+        }
+    }
+    const int e5 = m5_part(ts, rot, alpha_part, lo5, hi5, q5, i5);
+    // anchor fix inside the owning lane (zap_tex.h:673-674): 3 - i == i ^ 3 for 2-bit indices
+    if (i5 & 2u) {
+        #pragma unroll
+        for (int c = 0; c < 3; c++) { int s = q5[0][c]; q5[0][c] = q5[1][c]; q5[1][c] = s; }
+        i5 ^= 0xFFFFFFFFu;
+    }
+    int erot = e5 + (int)__shfl_xor_sync(gmask, (uint32_t)e5, 1, kBc7Group);
+    uint32_t key = ((uint32_t)erot << 2) | (uint32_t)rot;  // (SSE, rotation) lexicographic; SSE < 2^21
+    key = min(key, __shfl_xor_sync(gmask, key, 2, kBc7Group));
+    key = min(key, __shfl_xor_sync(gmask, key, 4, kBc7Group));
+    const int brot = (int)(key & 3u), best5 = (int)(key >> 2);
+    uint32_t qw = alpha_part ? (uint32_t)q5[0][0] | ((uint32_t)q5[1][0] << 8)
+                             : (uint32_t)q5[0][0] | ((uint32_t)q5[0][1] << 7) | ((uint32_t)q5[0][2] << 14) |
+                                   ((uint32_t)q5[1][0] << 21);
+    uint32_t qw2 = (uint32_t)q5[1][1] | ((uint32_t)q5[1][2] << 7);
+    uint32_t cq = __shfl_sync(gmask, qw, 2 * brot, kBc7Group), cq2 = __shfl_sync(gmask, qw2, 2 * brot, kBc7Group);
+    uint32_t ci = __shfl_sync(gmask, i5, 2 * brot, kBc7Group);
+    uint32_t aq = __shfl_sync(gmask, qw, 2 * brot + 1, kBc7Group), ai = __shfl_sync(gmask, i5, 2 * brot + 1, kBc7Group);
+    bool take5 = best5 < err;  // decoded SSE == fit SSE (see the file header)
+    if (take5) {
+        err = best5;
+        Bits128 o;
+        o.put(1u << 5, 6);
+        o.put((uint32_t)brot, 2);
+        uint32_t c0[3] = {cq & 127u, (cq >> 7) & 127u, (cq >> 14) & 127u}, c1[3] = {(cq >> 21) & 127u, cq2 & 127u, (cq2 >> 7) & 127u};
+        #pragma unroll
+        for (int c = 0; c < 3; c++) { o.put(c0[c], 7); o.put(c1[c], 7); }
+        o.put(aq & 255u, 8); o.put((aq >> 8) & 255u, 8);
+        o.put(ci & 1u, 1);
+        #pragma unroll
+        for (int i = 1; i < 16; i++) o.put((ci >> (2 * i)) & 3u, 2);
+        o.put(ai & 1u, 1);
+        #pragma unroll
+        for (int i = 1; i < 16; i++) o.put((ai >> (2 * i)) & 3u, 2);
+        blk = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
+    }
+    return take5;
+}
+
+// Mode 1 of one opaque block (zap_tex.h:764-783), same lanes and contract as bc7_group_mode5: true, with err and
+// blk updated, when the best of the ranked partitions has an SSE below err.
+__device__ __forceinline__ bool bc7_group_mode1(const uint32_t t[16], TexRef ts, int &err, uint4 &blk, const int l,
+                                                const unsigned gmask) {
+    // ---- mode 1 ranking: lane scores partitions l, l + 8, ..., l + 56 (zap_tex.h:764-775), four per round:
+    // one pass over the texels adds each texel's 9 moments to the block totals and to the sums of the
+    // four partitions' subset 1, every sum in texel order as the reference adds them
+    float ce[kMode1Tries];
+    int cp[kMode1Tries];
+    #pragma unroll
+    for (int j = 0; j < kMode1Tries; j++) { ce[j] = 1e30f; cp[j] = 64; }
+    #pragma unroll 1
+    for (int round = 0; round < 2; round++) {
+        uint32_t pm[4];
+        int n1[4];
+        float s1[4][9], tot[9];
+        #pragma unroll
+        for (int k = 0; k < 4; k++) {
+            pm[k] = kP2[l + kBc7Group * (4 * round + k)];
+            n1[k] = 0;
+            #pragma unroll
+            for (int j = 0; j < 9; j++) s1[k][j] = 0.0f;
+        }
+        #pragma unroll
+        for (int j = 0; j < 9; j++) tot[j] = 0.0f;
+        #pragma unroll 1
+        for (int i = 0; i < 16; i++) {
+            const uint32_t x = ts[i];
+            const float rr = (float)chan(x, 0), gg = (float)chan(x, 1), bb = (float)chan(x, 2);
+            const float mo[9] = {rr, gg, bb, rr * rr, gg * gg, bb * bb, rr * gg, rr * bb, gg * bb};
+            #pragma unroll
+            for (int j = 0; j < 9; j++) tot[j] = tot[j] + mo[j];
+            #pragma unroll
+            for (int k = 0; k < 4; k++)
+                if ((pm[k] >> i) & 1u) {
+                    n1[k]++;
+                    #pragma unroll
+                    for (int j = 0; j < 9; j++) s1[k][j] = s1[k][j] + mo[j];
+                }
+        }
+        #pragma unroll 1
+        for (int k = 0; k < 4; k++) {  // rolled: partition k's sums are at [0], the later ones shift down after it
+            const int part = l + kBc7Group * (4 * round + k);
+            const float e = partition_score(s1[0], n1[0], tot);
+            #pragma unroll
+            for (int r = 0; r < 3; r++) {
+                n1[r] = n1[r + 1];
+                #pragma unroll
+                for (int j = 0; j < 9; j++) s1[r][j] = s1[r + 1][j];
+            }
+            // insertion keeps (score, partition) order; NaN and >= 1e30 never enter, as in the reference
+            #pragma unroll
+            for (int j = 0; j < kMode1Tries; j++) {
+                if (e < ce[j]) {
+                    #pragma unroll
+                    for (int s = kMode1Tries - 1; s > j; s--) { ce[s] = ce[s - 1]; cp[s] = cp[s - 1]; }
+                    ce[j] = e; cp[j] = part;
+                    break;
+                }
+            }
+        }
+    }
+    // merge the eight sorted lists: four rounds of a group-wide (score, partition) minimum
+    int cand[kMode1Tries];
+    #pragma unroll
+    for (int j = 0; j < kMode1Tries; j++) {
+        float he = ce[0];
+        int hp = cp[0];
+        #pragma unroll
+        for (int m = 1; m < kBc7Group; m <<= 1) {
+            float oe = __shfl_xor_sync(gmask, he, m, kBc7Group);
+            int op = __shfl_xor_sync(gmask, hp, m, kBc7Group);
+            if (rank_less(oe, op, he, hp)) { he = oe; hp = op; }
+        }
+        cand[j] = hp < 64 ? hp : -1;
+        if (hp < 64 && (hp & (kBc7Group - 1)) == l) {  // owner pops its head
+            #pragma unroll
+            for (int s = 0; s < kMode1Tries - 1; s++) { ce[s] = ce[s + 1]; cp[s] = cp[s + 1]; }
+            ce[kMode1Tries - 1] = 1e30f; cp[kMode1Tries - 1] = 64;
+        }
+    }
+    // ---- mode 1 fits: lane = candidate * 2 + subset (zap_tex.h:687-708, 776)
+    const int j = l >> 1, sub = l & 1;
+    int pj = 0;
+    #pragma unroll
+    for (int k = 0; k < kMode1Tries; k++) if (k == j) pj = cand[k];
+    int q1[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}}, pb1[2] = {0, 0}, e1 = 1 << 29;
+    uint64_t i1 = 0;
+    uint32_t pmask = 0;
+    if (pj >= 0) {
+        pmask = sub ? (uint32_t)kP2[pj] : (~(uint32_t)kP2[pj] & 0xFFFFu);
+        float lo[4], hi[4];  // subset_encode with the principal axis taken in rolled loops over ts
+        pca_endpoints<3, 1>(ts, pmask, lo, hi);
+        bool more;
+        e1 = subset_passes<3, 3>(ts, pmask, 7, true, lo, hi, 0, 3, 0, q1, pb1, i1, more);
+        int anchor = sub ? (int)kA2[pj] : 0;
+        if ((i1 >> (4 * anchor)) & 4u) {  // anchor MSB must be 0: swap, 7 - i == i ^ 7 on the subset's texels
+            #pragma unroll
+            for (int c = 0; c < 3; c++) { int s = q1[0][c]; q1[0][c] = q1[1][c]; q1[1][c] = s; }
+            uint64_t sel = 0;
+            #pragma unroll
+            for (int i = 0; i < 16; i++) if ((pmask >> i) & 1u) sel |= 7ull << (4 * i);
+            i1 ^= sel;
+        }
+    }
+    int ecand = e1 + (int)__shfl_xor_sync(gmask, (uint32_t)e1, 1, kBc7Group);
+    // first candidate (in rank order) with the smallest SSE below the current best
+    uint32_t ckey = (pj >= 0 && ecand < err) ? (((uint32_t)ecand << 2) | (uint32_t)j) : 0xFFFFFFFFu;
+    ckey = min(ckey, __shfl_xor_sync(gmask, ckey, 2, kBc7Group));
+    ckey = min(ckey, __shfl_xor_sync(gmask, ckey, 4, kBc7Group));
+    if (ckey != 0xFFFFFFFFu) {
+        const int bj = (int)(ckey & 3u);
+        uint32_t ew0 = (uint32_t)q1[0][0] | ((uint32_t)q1[0][1] << 6) | ((uint32_t)q1[0][2] << 12) | ((uint32_t)pb1[0] << 18);
+        uint32_t ew1 = (uint32_t)q1[1][0] | ((uint32_t)q1[1][1] << 6) | ((uint32_t)q1[1][2] << 12);
+        uint32_t ilo = (uint32_t)i1, ihi = (uint32_t)(i1 >> 32);
+        uint32_t a0 = __shfl_sync(gmask, ew0, 2 * bj, kBc7Group), a1 = __shfl_sync(gmask, ew1, 2 * bj, kBc7Group);
+        uint32_t b0w = __shfl_sync(gmask, ew0, 2 * bj + 1, kBc7Group), b1w = __shfl_sync(gmask, ew1, 2 * bj + 1, kBc7Group);
+        uint32_t il = __shfl_sync(gmask, ilo, 2 * bj, kBc7Group) | __shfl_sync(gmask, ilo, 2 * bj + 1, kBc7Group);
+        uint32_t ih = __shfl_sync(gmask, ihi, 2 * bj, kBc7Group) | __shfl_sync(gmask, ihi, 2 * bj + 1, kBc7Group);
+        int part = __shfl_sync(gmask, pj, 2 * bj, kBc7Group);
+        err = (int)(ckey >> 2);
+        uint64_t full = (uint64_t)il | ((uint64_t)ih << 32);
+        Bits128 o;
+        o.put(2u, 2);
+        o.put((uint32_t)part, 6);
+        #pragma unroll
+        for (int c = 0; c < 3; c++) {
+            o.put((a0 >> (6 * c)) & 63u, 6); o.put((a1 >> (6 * c)) & 63u, 6);
+            o.put((b0w >> (6 * c)) & 63u, 6); o.put((b1w >> (6 * c)) & 63u, 6);
+        }
+        o.put((a0 >> 18) & 1u, 1); o.put((b0w >> 18) & 1u, 1);
+        const int anchor = (int)kA2[part];
+        #pragma unroll
+        for (int i = 0; i < 16; i++) o.put((uint32_t)((full >> (4 * i)) & 7u), (i == 0 || i == anchor) ? 2 : 3);
+        blk = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
+        return true;
+    }
+    return false;
+}
+
+ZTC_DEV bool block_opaque(const uint32_t t[16]) {
+    bool opaque = true;
+    #pragma unroll
+    for (int i = 0; i < 16; i++) opaque &= (t[i] >> 24) == 255u;
+    return opaque;
+}
+
 // One block that mode 6 did not finish, through modes 5 and 1 (zap_tex.h:759-783), by the 8 lanes of a group
 // (lane l, group mask gmask). err is the block's mode-6 SSE; lane 0 writes the block to dst when mode 5 or 1 wins.
 // Every lane holds the block's texels, so all group-level branches below are group-uniform; ts: the group's
 // shared-memory copy of them.
 __device__ __forceinline__ void bc7_group_block(const uint32_t t[16], TexRef ts, int err, const BlockOut &out, size_t ob, const int l,
                                                 const unsigned gmask) {
-    {
-        bool opaque = true;
-        #pragma unroll
-        for (int i = 0; i < 16; i++) opaque &= (t[i] >> 24) == 255u;
-
-        // ---- mode 5: lane = rotation * 2 + part (zap_tex.h:659-684)
-        const int rot = l >> 1;
-        const bool alpha_part = l & 1;
-        int q5[2][3] = {{0, 0, 0}, {0, 0, 0}};
-        uint32_t i5 = 0;
-        float lo5[3] = {255.0f, 0.0f, 0.0f}, hi5[3] = {0.0f, 0.0f, 0.0f};
-        if (!alpha_part) {  // colour part starts from the principal axis of the rotated RGB
-            uint32_t r[16];
-            #pragma unroll
-            for (int i = 0; i < 16; i++) r[i] = rotate_texel(t[i], rot);
-            float lo[4], hi[4];
-            pca_endpoints<3>(r, 0xFFFFu, lo, hi);
-            #pragma unroll
-            for (int c = 0; c < 3; c++) { lo5[c] = lo[c]; hi5[c] = hi[c]; }
-        } else {  // alpha part starts from the rotated alpha's range
-            #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                float a = (float)(rotate_texel(t[i], rot) >> 24);
-                if (a < lo5[0]) lo5[0] = a;
-                if (a > hi5[0]) hi5[0] = a;
-            }
-        }
-        const int e5 = m5_part(ts, rot, alpha_part, lo5, hi5, q5, i5);
-        // anchor fix inside the owning lane (zap_tex.h:673-674): 3 - i == i ^ 3 for 2-bit indices
-        if (i5 & 2u) {
-            #pragma unroll
-            for (int c = 0; c < 3; c++) { int s = q5[0][c]; q5[0][c] = q5[1][c]; q5[1][c] = s; }
-            i5 ^= 0xFFFFFFFFu;
-        }
-        int erot = e5 + (int)__shfl_xor_sync(gmask, (uint32_t)e5, 1, kBc7Group);
-        uint32_t key = ((uint32_t)erot << 2) | (uint32_t)rot;  // (SSE, rotation) lexicographic; SSE < 2^21
-        key = min(key, __shfl_xor_sync(gmask, key, 2, kBc7Group));
-        key = min(key, __shfl_xor_sync(gmask, key, 4, kBc7Group));
-        const int brot = (int)(key & 3u), best5 = (int)(key >> 2);
-        uint32_t qw = alpha_part ? (uint32_t)q5[0][0] | ((uint32_t)q5[1][0] << 8)
-                                 : (uint32_t)q5[0][0] | ((uint32_t)q5[0][1] << 7) | ((uint32_t)q5[0][2] << 14) |
-                                       ((uint32_t)q5[1][0] << 21);
-        uint32_t qw2 = (uint32_t)q5[1][1] | ((uint32_t)q5[1][2] << 7);
-        uint32_t cq = __shfl_sync(gmask, qw, 2 * brot, kBc7Group), cq2 = __shfl_sync(gmask, qw2, 2 * brot, kBc7Group);
-        uint32_t ci = __shfl_sync(gmask, i5, 2 * brot, kBc7Group);
-        uint32_t aq = __shfl_sync(gmask, qw, 2 * brot + 1, kBc7Group), ai = __shfl_sync(gmask, i5, 2 * brot + 1, kBc7Group);
-        bool take5 = best5 < err;  // decoded SSE == fit SSE (see the file header)
-        uint4 blk = make_uint4(0, 0, 0, 0);
-        if (take5) {
-            err = best5;
-            Bits128 o;
-            o.put(1u << 5, 6);
-            o.put((uint32_t)brot, 2);
-            uint32_t c0[3] = {cq & 127u, (cq >> 7) & 127u, (cq >> 14) & 127u}, c1[3] = {(cq >> 21) & 127u, cq2 & 127u, (cq2 >> 7) & 127u};
-            #pragma unroll
-            for (int c = 0; c < 3; c++) { o.put(c0[c], 7); o.put(c1[c], 7); }
-            o.put(aq & 255u, 8); o.put((aq >> 8) & 255u, 8);
-            o.put(ci & 1u, 1);
-            #pragma unroll
-            for (int i = 1; i < 16; i++) o.put((ci >> (2 * i)) & 3u, 2);
-            o.put(ai & 1u, 1);
-            #pragma unroll
-            for (int i = 1; i < 16; i++) o.put((ai >> (2 * i)) & 3u, 2);
-            blk = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
-        }
-        if (opaque) {  // group-uniform: every lane holds the same texels
-            // ---- mode 1 ranking: lane scores partitions l, l + 8, ..., l + 56 (zap_tex.h:764-775), four per round:
-            // one pass over the texels adds each texel's 9 moments to the block totals and to the sums of the
-            // four partitions' subset 1, every sum in texel order as the reference adds them
-            float ce[kMode1Tries];
-            int cp[kMode1Tries];
-            #pragma unroll
-            for (int j = 0; j < kMode1Tries; j++) { ce[j] = 1e30f; cp[j] = 64; }
-            #pragma unroll 1
-            for (int round = 0; round < 2; round++) {
-                uint32_t pm[4];
-                int n1[4];
-                float s1[4][9], tot[9];
-                #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    pm[k] = kP2[l + kBc7Group * (4 * round + k)];
-                    n1[k] = 0;
-                    #pragma unroll
-                    for (int j = 0; j < 9; j++) s1[k][j] = 0.0f;
-                }
-                #pragma unroll
-                for (int j = 0; j < 9; j++) tot[j] = 0.0f;
-                #pragma unroll 1
-                for (int i = 0; i < 16; i++) {
-                    const uint32_t x = ts[i];
-                    const float rr = (float)chan(x, 0), gg = (float)chan(x, 1), bb = (float)chan(x, 2);
-                    const float mo[9] = {rr, gg, bb, rr * rr, gg * gg, bb * bb, rr * gg, rr * bb, gg * bb};
-                    #pragma unroll
-                    for (int j = 0; j < 9; j++) tot[j] = tot[j] + mo[j];
-                    #pragma unroll
-                    for (int k = 0; k < 4; k++)
-                        if ((pm[k] >> i) & 1u) {
-                            n1[k]++;
-                            #pragma unroll
-                            for (int j = 0; j < 9; j++) s1[k][j] = s1[k][j] + mo[j];
-                        }
-                }
-                #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const int part = l + kBc7Group * (4 * round + k);
-                    const float e = partition_score(s1[k], n1[k], tot);
-                    // insertion keeps (score, partition) order; NaN and >= 1e30 never enter, as in the reference
-                    #pragma unroll
-                    for (int j = 0; j < kMode1Tries; j++) {
-                        if (e < ce[j]) {
-                            #pragma unroll
-                            for (int s = kMode1Tries - 1; s > j; s--) { ce[s] = ce[s - 1]; cp[s] = cp[s - 1]; }
-                            ce[j] = e; cp[j] = part;
-                            break;
-                        }
-                    }
-                }
-            }
-            // merge the eight sorted lists: four rounds of a group-wide (score, partition) minimum
-            int cand[kMode1Tries];
-            #pragma unroll
-            for (int j = 0; j < kMode1Tries; j++) {
-                float he = ce[0];
-                int hp = cp[0];
-                #pragma unroll
-                for (int m = 1; m < kBc7Group; m <<= 1) {
-                    float oe = __shfl_xor_sync(gmask, he, m, kBc7Group);
-                    int op = __shfl_xor_sync(gmask, hp, m, kBc7Group);
-                    if (rank_less(oe, op, he, hp)) { he = oe; hp = op; }
-                }
-                cand[j] = hp < 64 ? hp : -1;
-                if (hp < 64 && (hp & (kBc7Group - 1)) == l) {  // owner pops its head
-                    #pragma unroll
-                    for (int s = 0; s < kMode1Tries - 1; s++) { ce[s] = ce[s + 1]; cp[s] = cp[s + 1]; }
-                    ce[kMode1Tries - 1] = 1e30f; cp[kMode1Tries - 1] = 64;
-                }
-            }
-            // ---- mode 1 fits: lane = candidate * 2 + subset (zap_tex.h:687-708, 776)
-            const int j = l >> 1, sub = l & 1;
-            int pj = 0;
-            #pragma unroll
-            for (int k = 0; k < kMode1Tries; k++) if (k == j) pj = cand[k];
-            int q1[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}}, pb1[2] = {0, 0}, e1 = 1 << 29;
-            uint64_t i1 = 0;
-            uint32_t pmask = 0;
-            if (pj >= 0) {
-                pmask = sub ? (uint32_t)kP2[pj] : (~(uint32_t)kP2[pj] & 0xFFFFu);
-                e1 = subset_encode<3, 3>(t, ts, pmask, 7, true, q1, pb1, i1);
-                int anchor = sub ? (int)kA2[pj] : 0;
-                if ((i1 >> (4 * anchor)) & 4u) {  // anchor MSB must be 0: swap, 7 - i == i ^ 7 on the subset's texels
-                    #pragma unroll
-                    for (int c = 0; c < 3; c++) { int s = q1[0][c]; q1[0][c] = q1[1][c]; q1[1][c] = s; }
-                    uint64_t sel = 0;
-                    #pragma unroll
-                    for (int i = 0; i < 16; i++) if ((pmask >> i) & 1u) sel |= 7ull << (4 * i);
-                    i1 ^= sel;
-                }
-            }
-            int ecand = e1 + (int)__shfl_xor_sync(gmask, (uint32_t)e1, 1, kBc7Group);
-            // first candidate (in rank order) with the smallest SSE below the current best
-            uint32_t ckey = (pj >= 0 && ecand < err) ? (((uint32_t)ecand << 2) | (uint32_t)j) : 0xFFFFFFFFu;
-            ckey = min(ckey, __shfl_xor_sync(gmask, ckey, 2, kBc7Group));
-            ckey = min(ckey, __shfl_xor_sync(gmask, ckey, 4, kBc7Group));
-            if (ckey != 0xFFFFFFFFu) {
-                const int bj = (int)(ckey & 3u);
-                uint32_t ew0 = (uint32_t)q1[0][0] | ((uint32_t)q1[0][1] << 6) | ((uint32_t)q1[0][2] << 12) | ((uint32_t)pb1[0] << 18);
-                uint32_t ew1 = (uint32_t)q1[1][0] | ((uint32_t)q1[1][1] << 6) | ((uint32_t)q1[1][2] << 12);
-                uint32_t ilo = (uint32_t)i1, ihi = (uint32_t)(i1 >> 32);
-                uint32_t a0 = __shfl_sync(gmask, ew0, 2 * bj, kBc7Group), a1 = __shfl_sync(gmask, ew1, 2 * bj, kBc7Group);
-                uint32_t b0w = __shfl_sync(gmask, ew0, 2 * bj + 1, kBc7Group), b1w = __shfl_sync(gmask, ew1, 2 * bj + 1, kBc7Group);
-                uint32_t il = __shfl_sync(gmask, ilo, 2 * bj, kBc7Group) | __shfl_sync(gmask, ilo, 2 * bj + 1, kBc7Group);
-                uint32_t ih = __shfl_sync(gmask, ihi, 2 * bj, kBc7Group) | __shfl_sync(gmask, ihi, 2 * bj + 1, kBc7Group);
-                int part = __shfl_sync(gmask, pj, 2 * bj, kBc7Group);
-                err = (int)(ckey >> 2);
-                uint64_t full = (uint64_t)il | ((uint64_t)ih << 32);
-                Bits128 o;
-                o.put(2u, 2);
-                o.put((uint32_t)part, 6);
-                #pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    o.put((a0 >> (6 * c)) & 63u, 6); o.put((a1 >> (6 * c)) & 63u, 6);
-                    o.put((b0w >> (6 * c)) & 63u, 6); o.put((b1w >> (6 * c)) & 63u, 6);
-                }
-                o.put((a0 >> 18) & 1u, 1); o.put((b0w >> 18) & 1u, 1);
-                const int anchor = (int)kA2[part];
-                #pragma unroll
-                for (int i = 0; i < 16; i++) o.put((uint32_t)((full >> (4 * i)) & 7u), (i == 0 || i == anchor) ? 2 : 3);
-                blk = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
-                take5 = true;  // a block to write
-            }
-        }
-        if (take5 && l == 0) put_block16(out, ob, blk);
-    }
+    uint4 blk = make_uint4(0, 0, 0, 0);
+    bool take = bc7_group_mode5(t, ts, err, blk, l, gmask);
+    if (block_opaque(t) && bc7_group_mode1(t, ts, err, blk, l, gmask)) take = true;  // group-uniform
+    if (take && l == 0) put_block16(out, ob, blk);
 }
 
 // the group's shared-memory copy of its block (lane l writes texels l and l + 8), for the rolled loops
@@ -688,10 +707,17 @@ batch_bc7_mode6_kernel(const BatchLevel *__restrict__ levels, const BatchTile *_
     }
 }
 
-// bases[k]: batch-wide id of the first block of BC7 level k (ascending); level_of[k]: its index in `levels`
+// Batched modes 5 and 1 as two launches of one kernel over work lists (bases[k]: batch-wide id of the first block
+// of BC7 level k, ascending; level_of[k]: its index in `levels`). PHASE 5 runs mode 5 on every block of the mode-6
+// list (count, items) and appends each opaque block, with its SSE after mode 5, to (next_count, next_items); PHASE 1
+// runs mode 1 on that list. Groups take one block each per round with a CTA barrier between rounds, so the warps of
+// a CTA run the same part of the search together; each launch holds half the code of one mode-5-then-1 pass, which
+// keeps the code the SM fetches small.
+template <int PHASE>
 __global__ void __launch_bounds__(128, ZTC_MINB_BC7_HARD)
-batch_bc7_hard_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__restrict__ bases, const int *__restrict__ level_of,
-                      int nlevels, const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
+batch_bc7_phase_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__restrict__ bases, const int *__restrict__ level_of,
+                       int nlevels, const uint32_t *__restrict__ count, const uint2 *__restrict__ items, uint32_t *__restrict__ next_count,
+                       uint2 *__restrict__ next_items) {
     __shared__ uint32_t s_gtex[128 / kBc7Group][17];
     const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
     const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
@@ -699,29 +725,44 @@ batch_bc7_hard_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__r
     const int n = (int)*(volatile const uint32_t *)count;
     uint32_t *gtex = s_gtex[threadIdx.x / kBc7Group];
     const int gid = blockIdx.x * (blockDim.x / kBc7Group) + (threadIdx.x / kBc7Group);
-#if ZTC_BATCH_HARD_SYNC
-    // rounds of one block per group, the CTA's groups starting each round together: their warps then run the same
-    // phase of the search at the same time, which keeps the code the SM fetches small
-    const int rounds = (n + ngroups - 1) / ngroups;
+    const int rounds = (n + ngroups - 1) / ngroups;  // the same for every warp: the ballot below sees all 32 lanes
     for (int r = 0; r < rounds; r++) {
         __syncthreads();
         const int it = r * ngroups + gid;
-        if (it >= n) continue;
-#else
-    for (int it = gid; it < n; it += ngroups) {
-#endif
-        const uint2 item = items[it];
-        int lo = 0, hi = nlevels - 1;  // last level whose first id is <= the block's id
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(bases + mid) <= item.x) lo = mid; else hi = mid - 1;
+        uint2 item = make_uint2(0, 0);
+        bool push = false;
+        if (it < n) {
+            item = items[it];
+            int lo = 0, hi = nlevels - 1;  // last level whose first id is <= the block's id
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(bases + mid) <= item.x) lo = mid; else hi = mid - 1;
+            }
+            const BatchLevel L = levels[__ldg(level_of + lo)];
+            const int b = (int)(item.x - __ldg(bases + lo));
+            const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
+            uint32_t t[16];
+            gather_block(src, b % L.bw, b / L.bw, t);
+            const TexRef ts = stage_group_texels(gtex, t, l, gmask);
+            int err = (int)item.y;
+            uint4 blk = make_uint4(0, 0, 0, 0);
+            const bool take = PHASE == 5 ? bc7_group_mode5(t, ts, err, blk, l, gmask) : bc7_group_mode1(t, ts, err, blk, l, gmask);
+            if (take && l == 0) put_block16(BlockOut{L.dst, 0, 4, 0}, (size_t)b, blk);
+            if (PHASE == 5) {
+                push = l == 0 && block_opaque(t);
+                item.y = (uint32_t)err;
+            }
         }
-        const BatchLevel L = levels[__ldg(level_of + lo)];
-        const int b = (int)(item.x - __ldg(bases + lo));
-        const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
-        uint32_t t[16];
-        gather_block(src, b % L.bw, b / L.bw, t);
-        bc7_group_block(t, stage_group_texels(gtex, t, l, gmask), (int)item.y, BlockOut{L.dst, 0, 4, 0}, (size_t)b, l, gmask);
+        if (PHASE == 5) {  // one atomic per warp for its groups' opaque blocks
+            const unsigned ballot = __ballot_sync(0xFFFFFFFFu, push);
+            if (ballot) {
+                const int leader = __ffs(ballot) - 1;
+                uint32_t base = 0;
+                if (lane == leader) base = atomicAdd(next_count, (uint32_t)__popc(ballot));
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                if (push) next_items[base + __popc(ballot & ((1u << lane) - 1u))] = item;
+            }
+        }
     }
 }
 
@@ -739,8 +780,14 @@ cudaError_t ztc_launch_batch_bc7_mode6(int cta, int grid, const ztc::BatchLevel 
 }
 
 cudaError_t ztc_launch_batch_bc7_hard(int grid, const ztc::BatchLevel *levels, const uint32_t *bases, const int *level_of, int nlevels,
-                                      const uint32_t *hard_count, const uint2 *hard_items, cudaStream_t stream) {
-    ztc::batch_bc7_hard_kernel<<<grid, 128, 0, stream>>>(levels, bases, level_of, nlevels, hard_count, hard_items);
+                                      const uint32_t *hard_count, const uint2 *hard_items, uint32_t *opaque_count, uint2 *opaque_items,
+                                      cudaStream_t stream) {
+    ztc::batch_bc7_phase_kernel<5><<<grid, 128, 0, stream>>>(levels, bases, level_of, nlevels, hard_count, hard_items, opaque_count,
+                                                              opaque_items);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    ztc::batch_bc7_phase_kernel<1><<<grid, 128, 0, stream>>>(levels, bases, level_of, nlevels, opaque_count, opaque_items, nullptr,
+                                                              nullptr);
     return cudaGetLastError();
 }
 
@@ -753,7 +800,7 @@ const void *ztc_batch_bc7_kernel_fn(int cta) {
     }
 }
 
-const void *ztc_batch_bc7_hard_kernel_fn() { return (const void *)ztc::batch_bc7_hard_kernel; }
+const void *ztc_batch_bc7_hard_kernel_fn() { return (const void *)ztc::batch_bc7_phase_kernel<5>; }  // both phases: same bounds
 
 size_t ztc::bc7_scratch_bytes(size_t nblocks) { return 256 + nblocks * sizeof(uint2); }
 

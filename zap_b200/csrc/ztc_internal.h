@@ -66,12 +66,14 @@ struct BatchMipTile {   // output texel pairs [first, first + count) of one Batc
 cudaError_t ztc_launch_batch_bcn(int fmt, int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
                                  uint32_t *counter, cudaStream_t stream);
 // BC7 in two launches: mode 6 over the tile queue, appending (batch-wide block id, SSE) of the blocks it does not
-// finish to hard_items; then modes 5 / 1 over that list (bases / level_of: the BC7 levels' first ids, ascending,
-// and their indices in `levels`)
+// finish to hard_items; then mode 5 over that list, appending its opaque blocks to opaque_items (opaque_count zeroed
+// by the caller), and mode 1 over those (bases / level_of: the BC7 levels' first ids, ascending, and their indices in
+// `levels`)
 cudaError_t ztc_launch_batch_bc7_mode6(int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
                                        uint32_t *counter, uint32_t *hard_count, uint2 *hard_items, cudaStream_t stream);
 cudaError_t ztc_launch_batch_bc7_hard(int grid, const ztc::BatchLevel *levels, const uint32_t *bases, const int *level_of, int nlevels,
-                                      const uint32_t *hard_count, const uint2 *hard_items, cudaStream_t stream);
+                                      const uint32_t *hard_count, const uint2 *hard_items, uint32_t *opaque_count, uint2 *opaque_items,
+                                      cudaStream_t stream);
 cudaError_t ztc_launch_batch_mip(int grid, const ztc::BatchMip *mips, const ztc::BatchMipTile *tiles, int ntiles, const float *srgb_tables,
                                  cudaStream_t stream);
 const void *ztc_batch_bcn_kernel_fn(int fmt, int cta);

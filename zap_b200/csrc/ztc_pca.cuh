@@ -6,13 +6,34 @@
 
 namespace ztc {
 
+// one power-iteration step on the axis ax; false (ax unchanged) when C ax vanishes
 template <int NC>
-ZTC_DEV void pca_endpoints(const uint32_t t[16], uint32_t mask, float lo[4], float hi[4]) {
+ZTC_DEV bool pca_power_step(const float C[NC][NC], float ax[NC]) {
+    float nv[NC], m = 0.0f;
+    #pragma unroll
+    for (int a = 0; a < NC; a++) {
+        float s = 0.0f;
+        #pragma unroll
+        for (int b = 0; b < NC; b++) s = s + C[a][b] * ax[b];
+        nv[a] = s;
+        if (fabsf(s) > m) m = fabsf(s);
+    }
+    if (m < 1e-6f) return false;
+    #pragma unroll
+    for (int a = 0; a < NC; a++) ax[a] = nv[a] / m;
+    return true;
+}
+
+// t: the texels in registers (uint32_t[16]) or a TexRef; UNROLL 1 rolls the texel loops and the power iteration
+// (the same operations in the same order, in less code)
+template <int NC, int UNROLL = 16, typename Tex>
+ZTC_DEV void pca_endpoints(const Tex &t, uint32_t mask, float lo[4], float hi[4]) {
+    constexpr int kTexUnroll = UNROLL;
     const float cnt = (float)popc(mask);
     float mu[NC];
     #pragma unroll
     for (int c = 0; c < NC; c++) mu[c] = 0.0f;
-    #pragma unroll
+    #pragma unroll (kTexUnroll)
     for (int i = 0; i < 16; i++)
         if ((mask >> i) & 1u) {
             #pragma unroll
@@ -24,7 +45,7 @@ ZTC_DEV void pca_endpoints(const uint32_t t[16], uint32_t mask, float lo[4], flo
     for (int a = 0; a < NC; a++)
         #pragma unroll
         for (int b = 0; b < NC; b++) C[a][b] = 0.0f;
-    #pragma unroll
+    #pragma unroll (kTexUnroll)
     for (int i = 0; i < 16; i++)
         if ((mask >> i) & 1u) {
             float d[NC];
@@ -42,24 +63,18 @@ ZTC_DEV void pca_endpoints(const uint32_t t[16], uint32_t mask, float lo[4], flo
     float ax[NC];
     #pragma unroll
     for (int c = 0; c < NC; c++) ax[c] = 1.0f;
-    for (int it = 0; it < 6; it++) {
-        float nv[NC], m = 0.0f;
-        #pragma unroll
-        for (int a = 0; a < NC; a++) {
-            float s = 0.0f;
-            #pragma unroll
-            for (int b = 0; b < NC; b++) s = s + C[a][b] * ax[b];
-            nv[a] = s;
-            if (fabsf(s) > m) m = fabsf(s);
-        }
-        if (m < 1e-6f) break;
-        #pragma unroll
-        for (int a = 0; a < NC; a++) ax[a] = nv[a] / m;
+    if (UNROLL == 1) {
+        #pragma unroll 1
+        for (int it = 0; it < 6; it++)
+            if (!pca_power_step<NC>(C, ax)) break;
+    } else {
+        for (int it = 0; it < 6; it++)
+            if (!pca_power_step<NC>(C, ax)) break;
     }
     float n2 = 0.0f, tl = 1e9f, th = -1e9f;
     #pragma unroll
     for (int a = 0; a < NC; a++) n2 = n2 + ax[a] * ax[a];
-    #pragma unroll
+    #pragma unroll (kTexUnroll)
     for (int i = 0; i < 16; i++)
         if ((mask >> i) & 1u) {
             float s = 0.0f;
