@@ -422,9 +422,10 @@ __device__ __forceinline__ int astc_single_cta(bool valid, const uint32_t t[16],
     __shared__ uint8_t s_opq[CTA];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     float lo[1][4], hi[1][4];
-    if (valid) {
-        if (opaque) pca_endpoints<3>(t, 0xFFFFu, lo[0], hi[0]);
-        else pca_endpoints<4>(t, 0xFFFFu, lo[0], hi[0]);
+    if (valid) {  // principal axis in rolled loops over the block's column of s_tex
+        const TexRef own{&s_tex[0][tid], CTA};
+        if (opaque) pca_endpoints<3, 1>(own, 0xFFFFu, lo[0], hi[0]);
+        else pca_endpoints<4, 1>(own, 0xFFFFu, lo[0], hi[0]);
         s_opq[tid] = opaque;
     }
     unsigned mores = 0;  // bit k: trial k's third fit would run

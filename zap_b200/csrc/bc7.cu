@@ -201,7 +201,7 @@ __device__ __forceinline__ int mode6_encode_cta(bool valid, const uint32_t t[16]
     __shared__ uint16_t s_list[CTA];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     float lo[4], hi[4];
-    if (valid) pca_endpoints<4>(t, 0xFFFFu, lo, hi);
+    if (valid) pca_endpoints<4, 1>(TexRef{&s_tex[0][tid], CTA}, 0xFFFFu, lo, hi);  // rolled: less code, no spills
     bool active = valid;
     int owner = tid, first = 0, err = 0;
     uint64_t idx = 0;
