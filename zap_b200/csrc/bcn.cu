@@ -93,18 +93,21 @@ ZTC_DEV bool bc1_climb(const Bc1Texels &T, uint32_t &b0, uint32_t &b1, uint32_t 
 
 // quality search up to the climb (zap_tex.h:97-145): PCA axis, two starts with least-squares refits (the colour
 // channels of T.p are the texels' r, g, b)
-ZTC_DEV void bc1_start(const Bc1Texels &T, uint32_t &b0, uint32_t &b1, uint32_t &bidx, int &best) {
+// tx: the texels for the principal axis and least-squares sums (T.p, or a TexRef with UNROLL 1 for rolled loops)
+template <int UNROLL = 16, typename Tex>
+ZTC_DEV void bc1_start(const Bc1Texels &T, const Tex &tx, uint32_t &b0, uint32_t &b1, uint32_t &bidx, int &best) {
+    constexpr int kTex = UNROLL, kLoop = UNROLL == 1 ? 1 : 2;
     float mu0 = 0.0f, mu1 = 0.0f, mu2 = 0.0f;
-    #pragma unroll
+    #pragma unroll (kTex)
     for (int i = 0; i < 16; i++) {
-        mu0 = mu0 + (float)chan(T.p[i], 0) / 16.0f;
-        mu1 = mu1 + (float)chan(T.p[i], 1) / 16.0f;
-        mu2 = mu2 + (float)chan(T.p[i], 2) / 16.0f;
+        mu0 = mu0 + (float)chan(tx[i], 0) / 16.0f;
+        mu1 = mu1 + (float)chan(tx[i], 1) / 16.0f;
+        mu2 = mu2 + (float)chan(tx[i], 2) / 16.0f;
     }
     float C0 = 0, C1 = 0, C2 = 0, C3 = 0, C4 = 0, C5 = 0;
-    #pragma unroll
+    #pragma unroll (kTex)
     for (int i = 0; i < 16; i++) {
-        float r = (float)chan(T.p[i], 0) - mu0, g = (float)chan(T.p[i], 1) - mu1, b = (float)chan(T.p[i], 2) - mu2;
+        float r = (float)chan(tx[i], 0) - mu0, g = (float)chan(tx[i], 1) - mu1, b = (float)chan(tx[i], 2) - mu2;
         C0 = C0 + r * r; C1 = C1 + r * g; C2 = C2 + r * b; C3 = C3 + g * g; C4 = C4 + g * b; C5 = C5 + b * b;
     }
     float v0 = 1.0f, v1 = 1.0f, v2 = 1.0f;
@@ -119,14 +122,15 @@ ZTC_DEV void bc1_start(const Bc1Texels &T, uint32_t &b0, uint32_t &b1, uint32_t 
         v0 = x / m; v1 = y / m; v2 = z / m;
     }
     float n2 = v0 * v0 + v1 * v1 + v2 * v2, tmin = 1e9f, tmax = -1e9f;
-    #pragma unroll
+    #pragma unroll (kTex)
     for (int i = 0; i < 16; i++) {
-        float s = ((float)chan(T.p[i], 0) - mu0) * v0 + ((float)chan(T.p[i], 1) - mu1) * v1 + ((float)chan(T.p[i], 2) - mu2) * v2;
+        float s = ((float)chan(tx[i], 0) - mu0) * v0 + ((float)chan(tx[i], 1) - mu1) * v1 + ((float)chan(tx[i], 2) - mu2) * v2;
         if (s < tmin) tmin = s;
         if (s > tmax) tmax = s;
     }
     b0 = 0; b1 = 0; bidx = 0;
     best = 1 << 30;
+    #pragma unroll (kLoop)
     for (int start = 0; start < 2; start++) {
         float inset = start ? 0.0f : (tmax - tmin) / 16.0f, lo = (tmin + inset) / n2, hi = (tmax - inset) / n2;
         uint32_t c0 = pack565(mu0 + v0 * hi, mu1 + v1 * hi, mu2 + v2 * hi);
@@ -135,11 +139,11 @@ ZTC_DEV void bc1_start(const Bc1Texels &T, uint32_t &b0, uint32_t &b1, uint32_t 
         int e = bc1_try(T, c0, c1, idx);
         for (int it = 0; it < 3 && e > 0; it++) {
             float aa = 0, ab = 0, bb = 0, sa0 = 0, sa1 = 0, sa2 = 0, sb0 = 0, sb1 = 0, sb2 = 0;
-            #pragma unroll
+            #pragma unroll (kTex)
             for (int i = 0; i < 16; i++) {
                 float wa = bc1_lsw((idx >> (2 * i)) & 3u), wb = 1.0f - wa;
                 aa = aa + wa * wa; ab = ab + wa * wb; bb = bb + wb * wb;
-                float r = (float)chan(T.p[i], 0), g = (float)chan(T.p[i], 1), b = (float)chan(T.p[i], 2);
+                float r = (float)chan(tx[i], 0), g = (float)chan(tx[i], 1), b = (float)chan(tx[i], 2);
                 sa0 = sa0 + wa * r; sa1 = sa1 + wa * g; sa2 = sa2 + wa * b;
                 sb0 = sb0 + wb * r; sb1 = sb1 + wb * g; sb2 = sb2 + wb * b;
             }
@@ -162,7 +166,7 @@ ZTC_DEV uint2 bc1_encode(const uint32_t t[16]) {
     bc1_prepare(t, T);
     uint32_t b0, b1, bidx;
     int best;
-    bc1_start(T, b0, b1, bidx, best);
+    bc1_start(T, T.p, b0, b1, bidx, best);
     bc1_climb(T, b0, b1, bidx, best, 0, 8);
     return make_uint2(b0 | (b1 << 16), bidx);
 }
@@ -185,7 +189,7 @@ __device__ __forceinline__ uint2 bc1_encode_cta(bool valid, const uint32_t t[16]
     int best = 0;
     if (valid) {
         bc1_prepare(t, T);
-        bc1_start(T, b0, b1, bidx, best);
+        bc1_start<1>(T, TexRef{&s_tex[0][tid], CTA}, b0, b1, bidx, best);
     }
     bool active = valid;
     int owner = tid;
