@@ -193,7 +193,8 @@ ZTC_DEV void unpack_qp(uint64_t v, int q[2][4], int pb[2]) {
 // threads of the CTA run those refits on the owners' texels, so they cost about a fifth of the warps instead of
 // nearly all. Same bytes and SSE as mode6_encode. Every thread of the CTA calls it (it synchronises); a `valid`
 // thread's block is in t and in column threadIdx.x of s_tex.
-template <int CTA>
+// ROLLED: the principal axis in rolled loops over s_tex, for launches of several waves (see bc1_encode_cta)
+template <int CTA, bool ROLLED>
 __device__ __forceinline__ int mode6_encode_cta(bool valid, const uint32_t t[16], uint32_t (*s_tex)[CTA], uint4 &blk) {
     static_assert(CTA % 32 == 0 && CTA <= 1024, "whole warps");
     __shared__ uint64_t s_idx[CTA], s_qp[CTA];
@@ -201,7 +202,10 @@ __device__ __forceinline__ int mode6_encode_cta(bool valid, const uint32_t t[16]
     __shared__ uint16_t s_list[CTA];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     float lo[4], hi[4];
-    if (valid) pca_endpoints<4, 1>(TexRef{&s_tex[0][tid], CTA}, 0xFFFFu, lo, hi);  // rolled: less code, no spills
+    if (valid) {
+        if (ROLLED) pca_endpoints<4, 1>(TexRef{&s_tex[0][tid], CTA}, 0xFFFFu, lo, hi);  // less code, no spills
+        else pca_endpoints<4>(t, 0xFFFFu, lo, hi);
+    }
     bool active = valid;
     int owner = tid, first = 0, err = 0;
     uint64_t idx = 0;
@@ -237,9 +241,13 @@ __device__ __forceinline__ int mode6_encode_cta(bool valid, const uint32_t t[16]
 // CTA sizes of the mode-6 kernel. A larger CTA shares one compacted-refit list among more blocks (2048x2048:
 // 64 threads 0.119 ms, 128 0.105, 256 0.099, 384 0.100, 512 0.103); a launch smaller than one full wave of large
 // CTAs takes the small size instead, which keeps more SMs busy (512x512 in 256-thread CTAs: 64 CTAs for 148 SMs).
-constexpr int kMode6Small = 128, kMode6Large = 256;
+// The large size is 224 threads at 4 CTAs per SM (72 registers): 896 threads per SM instead of 768 at 256 x 3,
+// so 2048x2048 fills 1.98 waves instead of 2.31 (0.0980 -> 0.0966 ms).
+constexpr int kMode6Small = 128, kMode6Large = 224;
 template <int CTA>
-__global__ void __launch_bounds__(CTA, ZTC_MINB_BC7_MODE6 * 128 / CTA) bc7_mode6_kernel(SrcU8 src, int bw, int by0, int nblocks,
+constexpr int mode6_min_ctas() { return CTA == kMode6Large ? 4 : ZTC_MINB_BC7_MODE6 * 128 / CTA; }
+template <int CTA>
+__global__ void __launch_bounds__(CTA, mode6_min_ctas<CTA>()) bc7_mode6_kernel(SrcU8 src, int bw, int by0, int nblocks,
                                                         BlockOut out, size_t b0, uint32_t *__restrict__ count, uint2 *__restrict__ items) {
     __shared__ uint32_t s_tex[16][CTA];  // column threadIdx.x: this thread's block
     int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -251,7 +259,7 @@ __global__ void __launch_bounds__(CTA, ZTC_MINB_BC7_MODE6 * 128 / CTA) bc7_mode6
         for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
     }
     uint4 blk;
-    const int err = mode6_encode_cta<CTA>(valid, t, s_tex, blk);
+    const int err = mode6_encode_cta<CTA, CTA != kMode6Small>(valid, t, s_tex, blk);
     if (valid) put_block16(out, b0 + (size_t)b, blk);
     bool hard = valid && err > 16 * 4;  // zap_tex.h:758 early exit
     unsigned ballot = __ballot_sync(0xFFFFFFFFu, hard);
@@ -267,7 +275,7 @@ __global__ void __launch_bounds__(CTA, ZTC_MINB_BC7_MODE6 * 128 / CTA) bc7_mode6
 // the mode-6 launch, at the CTA size that suits its block count
 cudaError_t launch_mode6(const SrcU8 &src, int bw, int by0, int nblocks, const BlockOut &out, size_t b0, uint32_t *count, uint2 *items,
                          cudaStream_t s) {
-    if (nblocks >= ztc_sm_count() * (ZTC_MINB_BC7_MODE6 * 128 / kMode6Large) * kMode6Large)
+    if (nblocks >= ztc_sm_count() * mode6_min_ctas<kMode6Large>() * kMode6Large)
         bc7_mode6_kernel<kMode6Large><<<(nblocks + kMode6Large - 1) / kMode6Large, kMode6Large, 0, s>>>(src, bw, by0, nblocks, out, b0, count, items);
     else
         bc7_mode6_kernel<kMode6Small><<<(nblocks + kMode6Small - 1) / kMode6Small, kMode6Small, 0, s>>>(src, bw, by0, nblocks, out, b0, count, items);
@@ -693,7 +701,7 @@ batch_bc7_mode6_kernel(const BatchLevel *__restrict__ levels, const BatchTile *_
             for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
         }
         uint4 blk;
-        const int err = mode6_encode_cta<CTA>(valid, t, s_tex, blk);
+        const int err = mode6_encode_cta<CTA, true>(valid, t, s_tex, blk);
         if (valid) store_block16(L.dst + (size_t)b * 16, blk);
         const bool hard = valid && err > 16 * 4;  // zap_tex.h:758 early exit
         const unsigned ballot = __ballot_sync(0xFFFFFFFFu, hard);

@@ -91,25 +91,59 @@ ZTC_DEV bool bc1_climb(const Bc1Texels &T, uint32_t &b0, uint32_t &b1, uint32_t 
     return improved;
 }
 
+template <int UNROLL>
+ZTC_DEV uint32_t bc1_texel(const Bc1Texels &T, TexRef tx, int i) { return UNROLL == 1 ? tx[i] : T.p[i]; }
+
+// one start of the quality search (zap_tex.h:118-143): endpoints from the axis, then up to three least-squares refits
+template <int UNROLL>
+ZTC_DEV void bc1_one_start(const Bc1Texels &T, TexRef tx, int start, float mu0, float mu1, float mu2, float v0, float v1,
+                           float v2, float n2, float tmin, float tmax, uint32_t &b0, uint32_t &b1, uint32_t &bidx, int &best) {
+    float inset = start ? 0.0f : (tmax - tmin) / 16.0f, lo = (tmin + inset) / n2, hi = (tmax - inset) / n2;
+    uint32_t c0 = pack565(mu0 + v0 * hi, mu1 + v1 * hi, mu2 + v2 * hi);
+    uint32_t c1 = pack565(mu0 + v0 * lo, mu1 + v1 * lo, mu2 + v2 * lo);
+    uint32_t idx = 0;
+    int e = bc1_try(T, c0, c1, idx);
+    for (int it = 0; it < 3 && e > 0; it++) {
+        float aa = 0, ab = 0, bb = 0, sa0 = 0, sa1 = 0, sa2 = 0, sb0 = 0, sb1 = 0, sb2 = 0;
+        for_texels<UNROLL>([&](int i) {
+            float wa = bc1_lsw((idx >> (2 * i)) & 3u), wb = 1.0f - wa;
+            aa = aa + wa * wa; ab = ab + wa * wb; bb = bb + wb * wb;
+            const uint32_t x = bc1_texel<UNROLL>(T, tx, i);
+            float r = (float)chan(x, 0), g = (float)chan(x, 1), b = (float)chan(x, 2);
+            sa0 = sa0 + wa * r; sa1 = sa1 + wa * g; sa2 = sa2 + wa * b;
+            sb0 = sb0 + wb * r; sb1 = sb1 + wb * g; sb2 = sb2 + wb * b;
+        });
+        float det = aa * bb - ab * ab;
+        if (det < 1e-6f && det > -1e-6f) break;
+        uint32_t n0 = pack565((sa0 * bb - sb0 * ab) / det, (sa1 * bb - sb1 * ab) / det, (sa2 * bb - sb2 * ab) / det);
+        uint32_t n1 = pack565((sb0 * aa - sa0 * ab) / det, (sb1 * aa - sa1 * ab) / det, (sb2 * aa - sa2 * ab) / det);
+        uint32_t ni = 0;
+        int ne = bc1_try(T, n0, n1, ni);
+        if (ne >= e) break;
+        e = ne; c0 = n0; c1 = n1; idx = ni;
+    }
+    if (e < best) { best = e; b0 = c0; b1 = c1; bidx = idx; }
+}
+
 // quality search up to the climb (zap_tex.h:97-145): PCA axis, two starts with least-squares refits (the colour
 // channels of T.p are the texels' r, g, b)
-// tx: the texels for the principal axis and least-squares sums (T.p, or a TexRef with UNROLL 1 for rolled loops)
-template <int UNROLL = 16, typename Tex>
-ZTC_DEV void bc1_start(const Bc1Texels &T, const Tex &tx, uint32_t &b0, uint32_t &b1, uint32_t &bidx, int &best) {
-    constexpr int kTex = UNROLL, kLoop = UNROLL == 1 ? 1 : 2;
+// UNROLL 16: the texel loops unrolled over T.p (tx unused); UNROLL 1: rolled loops over tx, the block's texels in
+// shared memory
+template <int UNROLL = 16>
+ZTC_DEV void bc1_start(const Bc1Texels &T, TexRef tx, uint32_t &b0, uint32_t &b1, uint32_t &bidx, int &best) {
     float mu0 = 0.0f, mu1 = 0.0f, mu2 = 0.0f;
-    #pragma unroll (kTex)
-    for (int i = 0; i < 16; i++) {
-        mu0 = mu0 + (float)chan(tx[i], 0) / 16.0f;
-        mu1 = mu1 + (float)chan(tx[i], 1) / 16.0f;
-        mu2 = mu2 + (float)chan(tx[i], 2) / 16.0f;
-    }
+    for_texels<UNROLL>([&](int i) {
+        const uint32_t x = bc1_texel<UNROLL>(T, tx, i);
+        mu0 = mu0 + (float)chan(x, 0) / 16.0f;
+        mu1 = mu1 + (float)chan(x, 1) / 16.0f;
+        mu2 = mu2 + (float)chan(x, 2) / 16.0f;
+    });
     float C0 = 0, C1 = 0, C2 = 0, C3 = 0, C4 = 0, C5 = 0;
-    #pragma unroll (kTex)
-    for (int i = 0; i < 16; i++) {
-        float r = (float)chan(tx[i], 0) - mu0, g = (float)chan(tx[i], 1) - mu1, b = (float)chan(tx[i], 2) - mu2;
+    for_texels<UNROLL>([&](int i) {
+        const uint32_t x = bc1_texel<UNROLL>(T, tx, i);
+        float r = (float)chan(x, 0) - mu0, g = (float)chan(x, 1) - mu1, b = (float)chan(x, 2) - mu2;
         C0 = C0 + r * r; C1 = C1 + r * g; C2 = C2 + r * b; C3 = C3 + g * g; C4 = C4 + g * b; C5 = C5 + b * b;
-    }
+    });
     float v0 = 1.0f, v1 = 1.0f, v2 = 1.0f;
     for (int it = 0; it < 6; it++) {
         float x = C0 * v0 + C1 * v1 + C2 * v2;
@@ -122,42 +156,17 @@ ZTC_DEV void bc1_start(const Bc1Texels &T, const Tex &tx, uint32_t &b0, uint32_t
         v0 = x / m; v1 = y / m; v2 = z / m;
     }
     float n2 = v0 * v0 + v1 * v1 + v2 * v2, tmin = 1e9f, tmax = -1e9f;
-    #pragma unroll (kTex)
-    for (int i = 0; i < 16; i++) {
-        float s = ((float)chan(tx[i], 0) - mu0) * v0 + ((float)chan(tx[i], 1) - mu1) * v1 + ((float)chan(tx[i], 2) - mu2) * v2;
+    for_texels<UNROLL>([&](int i) {
+        const uint32_t x = bc1_texel<UNROLL>(T, tx, i);
+        float s = ((float)chan(x, 0) - mu0) * v0 + ((float)chan(x, 1) - mu1) * v1 + ((float)chan(x, 2) - mu2) * v2;
         if (s < tmin) tmin = s;
         if (s > tmax) tmax = s;
-    }
+    });
     b0 = 0; b1 = 0; bidx = 0;
     best = 1 << 30;
-    #pragma unroll (kLoop)
-    for (int start = 0; start < 2; start++) {
-        float inset = start ? 0.0f : (tmax - tmin) / 16.0f, lo = (tmin + inset) / n2, hi = (tmax - inset) / n2;
-        uint32_t c0 = pack565(mu0 + v0 * hi, mu1 + v1 * hi, mu2 + v2 * hi);
-        uint32_t c1 = pack565(mu0 + v0 * lo, mu1 + v1 * lo, mu2 + v2 * lo);
-        uint32_t idx = 0;
-        int e = bc1_try(T, c0, c1, idx);
-        for (int it = 0; it < 3 && e > 0; it++) {
-            float aa = 0, ab = 0, bb = 0, sa0 = 0, sa1 = 0, sa2 = 0, sb0 = 0, sb1 = 0, sb2 = 0;
-            #pragma unroll (kTex)
-            for (int i = 0; i < 16; i++) {
-                float wa = bc1_lsw((idx >> (2 * i)) & 3u), wb = 1.0f - wa;
-                aa = aa + wa * wa; ab = ab + wa * wb; bb = bb + wb * wb;
-                float r = (float)chan(tx[i], 0), g = (float)chan(tx[i], 1), b = (float)chan(tx[i], 2);
-                sa0 = sa0 + wa * r; sa1 = sa1 + wa * g; sa2 = sa2 + wa * b;
-                sb0 = sb0 + wb * r; sb1 = sb1 + wb * g; sb2 = sb2 + wb * b;
-            }
-            float det = aa * bb - ab * ab;
-            if (det < 1e-6f && det > -1e-6f) break;
-            uint32_t n0 = pack565((sa0 * bb - sb0 * ab) / det, (sa1 * bb - sb1 * ab) / det, (sa2 * bb - sb2 * ab) / det);
-            uint32_t n1 = pack565((sb0 * aa - sa0 * ab) / det, (sb1 * aa - sa1 * ab) / det, (sb2 * aa - sa2 * ab) / det);
-            uint32_t ni = 0;
-            int ne = bc1_try(T, n0, n1, ni);
-            if (ne >= e) break;
-            e = ne; c0 = n0; c1 = n1; idx = ni;
-        }
-        if (e < best) { best = e; b0 = c0; b1 = c1; bidx = idx; }
-    }
+    #pragma unroll 1
+    for (int start = 0; start < 2; start++)
+        bc1_one_start<UNROLL>(T, tx, start, mu0, mu1, mu2, v0, v1, v2, n2, tmin, tmax, b0, b1, bidx, best);
 }
 
 // quality search (zap_tex.h:97-168), one thread
@@ -166,7 +175,7 @@ ZTC_DEV uint2 bc1_encode(const uint32_t t[16]) {
     bc1_prepare(t, T);
     uint32_t b0, b1, bidx;
     int best;
-    bc1_start(T, T.p, b0, b1, bidx, best);
+    bc1_start(T, TexRef{nullptr, 0}, b0, b1, bidx, best);
     bc1_climb(T, b0, b1, bidx, best, 0, 8);
     return make_uint2(b0 | (b1 << 16), bidx);
 }
@@ -177,7 +186,10 @@ ZTC_DEV uint2 bc1_encode(const uint32_t t[16]) {
 // threads of the CTA climb them on to the end from the owners' texels, so the long tail of the climb costs about
 // a tenth of the warps. Same bytes as bc1_encode. Every thread of the CTA calls it (it synchronises); a `valid`
 // thread's block is in t and in column threadIdx.x of s_tex.
-template <int CTA>
+// ROLLED: the starts' principal axis and least-squares sums run in rolled loops over s_tex (less code, more
+// instructions): faster in launches of several waves, slower in a launch of less than one wave, where each
+// thread's own chain of dependent instructions sets the time (512x512 BC1: 0.0415 -> 0.0441 ms).
+template <int CTA, bool ROLLED>
 __device__ __forceinline__ uint2 bc1_encode_cta(bool valid, const uint32_t t[16], uint32_t (*s_tex)[CTA]) {
     static_assert(CTA % 32 == 0 && CTA <= 256, "whole warps, owners fit a byte");
     __shared__ uint32_t s_ends[CTA], s_idx[CTA];
@@ -189,7 +201,8 @@ __device__ __forceinline__ uint2 bc1_encode_cta(bool valid, const uint32_t t[16]
     int best = 0;
     if (valid) {
         bc1_prepare(t, T);
-        bc1_start<1>(T, TexRef{&s_tex[0][tid], CTA}, b0, b1, bidx, best);
+        if (ROLLED) bc1_start<1>(T, TexRef{&s_tex[0][tid], CTA}, b0, b1, bidx, best);
+        else bc1_start(T, TexRef{nullptr, 0}, b0, b1, bidx, best);
     }
     bool active = valid;
     int owner = tid;
@@ -258,8 +271,12 @@ ZTC_DEV uint2 bc4_encode(const uint32_t t[16], int c) {
 // ---------------------------------------------------------------- kernel: one thread per block
 // CTA sizes of the BC1-BC5 kernel. For BC1 / BC3 a larger CTA shares one list of compacted climbs among more
 // blocks (2048x2048 BC1: 64 threads 0.217 ms, 128 0.189, 256 0.185; BC4 the same at all three); a launch smaller
-// than one full wave of large CTAs takes the small size, which keeps more SMs busy.
-constexpr int kBcnSmall = 128, kBcnLarge = 256;
+// than one full wave of large CTAs takes the small size, which keeps more SMs busy. BC1 / BC3 take 224 threads at
+// 4 CTAs per SM (72 registers; 2048x2048 BC1 fills 1.98 waves instead of 1.73: 0.172 -> 0.168 ms); BC4 / BC5 keep
+// 256 (224 measured 0.0558 -> 0.0567 ms on BC4).
+constexpr int kBcnSmall = 128;
+template <int FMT>
+constexpr int bcn_large() { return FMT == ZTC_FMT_BC1 || FMT == ZTC_FMT_BC3 ? 224 : 256; }
 template <int FMT, int CTA>
 __global__ void __launch_bounds__(CTA, ZTC_MINB_BCN * 128 / CTA) bcn_kernel(SrcU8 src, int bw, int by0, int nblocks, BlockOut out, size_t b0) {
     constexpr bool kColour = FMT == ZTC_FMT_BC1 || FMT == ZTC_FMT_BC3;
@@ -277,13 +294,13 @@ __global__ void __launch_bounds__(CTA, ZTC_MINB_BCN * 128 / CTA) bcn_kernel(SrcU
     }
     const size_t ob = b0 + (size_t)b;  // the block's index in the output
     if (FMT == ZTC_FMT_BC1) {
-        const uint2 c = bc1_encode_cta<CTA>(valid, t, (uint32_t(*)[CTA])s_tex);
+        const uint2 c = bc1_encode_cta<CTA, CTA != kBcnSmall>(valid, t, (uint32_t(*)[CTA])s_tex);
         if (valid) put_block8(out, ob, c);
     } else if (FMT == ZTC_FMT_BC4) {
         put_block8(out, ob, bc4_encode(t, 0));
     } else if (FMT == ZTC_FMT_BC3) {
         uint2 a = valid ? bc4_encode(t, 3) : make_uint2(0u, 0u);
-        const uint2 c = bc1_encode_cta<CTA>(valid, t, (uint32_t(*)[CTA])s_tex);
+        const uint2 c = bc1_encode_cta<CTA, CTA != kBcnSmall>(valid, t, (uint32_t(*)[CTA])s_tex);
         if (valid) put_block16(out, ob, make_uint4(a.x, a.y, c.x, c.y));
     } else {  // BC5
         uint2 r = bc4_encode(t, 0), g = bc4_encode(t, 1);
@@ -299,11 +316,14 @@ cudaError_t ztc_launch_bcn_to(int fmt, const ztc::SrcU8 &src, int by0, int nby, 
     static const char *names[4] = {"bc1_encode", "bc3_encode", "bc4_encode", "bc5_encode"};
     ztc::TraceScope tr(fmt >= 0 && fmt < 4 ? names[fmt] : "bcn_encode", stream);
     ztc::trace_units(nblocks);
-    const bool large = nblocks >= ztc_sm_count() * (ZTC_MINB_BCN * 128 / ztc::kBcnLarge) * ztc::kBcnLarge;
-    const int cta = large ? ztc::kBcnLarge : ztc::kBcnSmall, grid = (nblocks + cta - 1) / cta;
 #define ZTC_BCN_LAUNCH(F)                                                                                              \
-    (large ? ztc::bcn_kernel<F, ztc::kBcnLarge><<<grid, cta, 0, stream>>>(src, bw, by0, nblocks, out, b0)           \
-           : ztc::bcn_kernel<F, ztc::kBcnSmall><<<grid, cta, 0, stream>>>(src, bw, by0, nblocks, out, b0))
+    do {                                                                                                               \
+        constexpr int kLarge = ztc::bcn_large<F>();                                                                    \
+        const bool large = nblocks >= ztc_sm_count() * (ZTC_MINB_BCN * 128 / kLarge) * kLarge;                        \
+        const int cta = large ? kLarge : ztc::kBcnSmall, grid = (nblocks + cta - 1) / cta;                            \
+        if (large) ztc::bcn_kernel<F, kLarge><<<grid, cta, 0, stream>>>(src, bw, by0, nblocks, out, b0);               \
+        else ztc::bcn_kernel<F, ztc::kBcnSmall><<<grid, cta, 0, stream>>>(src, bw, by0, nblocks, out, b0);            \
+    } while (0)
     switch (fmt) {
     case ZTC_FMT_BC1: ZTC_BCN_LAUNCH(ZTC_FMT_BC1); break;
     case ZTC_FMT_BC3: ZTC_BCN_LAUNCH(ZTC_FMT_BC3); break;
@@ -348,12 +368,12 @@ __global__ void __launch_bounds__(CTA, ZTC_MINB_BCN_BATCH * 128 / CTA) batch_bcn
             }
         }
         if (FMT == ZTC_FMT_BC1) {
-            const uint2 c = bc1_encode_cta<CTA>(valid, t, (uint32_t(*)[CTA])s_tex);
+            const uint2 c = bc1_encode_cta<CTA, true>(valid, t, (uint32_t(*)[CTA])s_tex);
             if (valid) store_block8(L.dst + (size_t)b * 8, c);
         } else if (FMT == ZTC_FMT_BC4) store_block8(L.dst + (size_t)b * 8, bc4_encode(t, 0));
         else if (FMT == ZTC_FMT_BC3) {
             const uint2 a = valid ? bc4_encode(t, 3) : make_uint2(0u, 0u);
-            const uint2 c = bc1_encode_cta<CTA>(valid, t, (uint32_t(*)[CTA])s_tex);
+            const uint2 c = bc1_encode_cta<CTA, true>(valid, t, (uint32_t(*)[CTA])s_tex);
             if (valid) store_block16(L.dst + (size_t)b * 16, make_uint4(a.x, a.y, c.x, c.y));
         } else {
             uint2 r = bc4_encode(t, 0), g = bc4_encode(t, 1);

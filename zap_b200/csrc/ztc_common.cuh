@@ -185,6 +185,19 @@ ZTC_DEV void gather_block(const SrcU8 &s, int bx, int by, uint32_t t[16]) {
 // shared-memory copy of the block, so those loops need not be unrolled over registers and the kernels' code stays
 // small enough for the instruction cache (fully unrolled 16-texel x 16-entry palette scans, inlined at several
 // call sites, leave the warps waiting on instruction fetch).
+// f(0) .. f(15) in texel order: fully unrolled (UNROLL 16), or rolled (UNROLL 1) for loops over a TexRef
+template <int UNROLL, typename F>
+ZTC_DEV void for_texels(F &&f) {
+    static_assert(UNROLL == 1 || UNROLL == 16, "rolled or fully unrolled");
+    if (UNROLL == 1) {
+        #pragma unroll 1
+        for (int i = 0; i < 16; i++) f(i);
+    } else {
+        #pragma unroll
+        for (int i = 0; i < 16; i++) f(i);
+    }
+}
+
 struct TexRef {
     const uint32_t *p;
     int stride;

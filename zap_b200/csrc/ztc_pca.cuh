@@ -25,28 +25,26 @@ ZTC_DEV bool pca_power_step(const float C[NC][NC], float ax[NC]) {
 }
 
 // t: the texels in registers (uint32_t[16]) or a TexRef; UNROLL 1 rolls the texel loops and the power iteration
-// (the same operations in the same order, in less code)
+// (the same operations in the same order, in less code), UNROLL 16 unrolls them
 template <int NC, int UNROLL = 16, typename Tex>
 ZTC_DEV void pca_endpoints(const Tex &t, uint32_t mask, float lo[4], float hi[4]) {
-    constexpr int kTexUnroll = UNROLL;
     const float cnt = (float)popc(mask);
     float mu[NC];
     #pragma unroll
     for (int c = 0; c < NC; c++) mu[c] = 0.0f;
-    #pragma unroll (kTexUnroll)
-    for (int i = 0; i < 16; i++)
+    for_texels<UNROLL>([&](int i) {
         if ((mask >> i) & 1u) {
             #pragma unroll
             for (int c = 0; c < NC; c++) mu[c] = mu[c] + (float)chan(t[i], c) / cnt;
         }
+    });
     // upper triangle only: cov[a][b] and cov[b][a] add bitwise-identical products in the same order
     float C[NC][NC];
     #pragma unroll
     for (int a = 0; a < NC; a++)
         #pragma unroll
         for (int b = 0; b < NC; b++) C[a][b] = 0.0f;
-    #pragma unroll (kTexUnroll)
-    for (int i = 0; i < 16; i++)
+    for_texels<UNROLL>([&](int i) {
         if ((mask >> i) & 1u) {
             float d[NC];
             #pragma unroll
@@ -56,6 +54,7 @@ ZTC_DEV void pca_endpoints(const Tex &t, uint32_t mask, float lo[4], float hi[4]
                 #pragma unroll
                 for (int b = a; b < NC; b++) C[a][b] = C[a][b] + d[a] * d[b];
         }
+    });
     #pragma unroll
     for (int a = 0; a < NC; a++)
         #pragma unroll
@@ -74,8 +73,7 @@ ZTC_DEV void pca_endpoints(const Tex &t, uint32_t mask, float lo[4], float hi[4]
     float n2 = 0.0f, tl = 1e9f, th = -1e9f;
     #pragma unroll
     for (int a = 0; a < NC; a++) n2 = n2 + ax[a] * ax[a];
-    #pragma unroll (kTexUnroll)
-    for (int i = 0; i < 16; i++)
+    for_texels<UNROLL>([&](int i) {
         if ((mask >> i) & 1u) {
             float s = 0.0f;
             #pragma unroll
@@ -83,6 +81,7 @@ ZTC_DEV void pca_endpoints(const Tex &t, uint32_t mask, float lo[4], float hi[4]
             if (s < tl) tl = s;
             if (s > th) th = s;
         }
+    });
     #pragma unroll
     for (int c = 0; c < 4; c++) {
         if (c < NC) { lo[c] = mu[c] + ax[c] * tl / n2; hi[c] = mu[c] + ax[c] * th / n2; }
