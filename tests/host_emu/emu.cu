@@ -114,4 +114,20 @@ __attribute__((visibility("default"))) int emu_mip_next(const uint8_t *src, int 
     return 0;
 }
 
+// finite floats x with bit patterns in [lo, hi) for which ztc::div255(x) differs bitwise from the division x / 255.0f
+// (-0, whose documented quotient is +0, excepted)
+__attribute__((visibility("default"))) uint64_t emu_div255_mismatches(uint64_t lo, uint64_t hi) {
+    volatile float d = 255.0f;  // a runtime divisor: the host compiler emits a true division
+    uint64_t bad = 0;
+    for (uint64_t u = lo; u < hi; u++) {
+        float x;
+        const uint32_t b = (uint32_t)u;
+        std::memcpy(&x, &b, 4);
+        if (!std::isfinite(x) || b == 0x80000000u) continue;
+        const float a = x / d, m = div255(x);
+        if (std::memcmp(&a, &m, 4) != 0) bad++;
+    }
+    return bad;
+}
+
 }  // extern "C"

@@ -36,6 +36,8 @@ def emu():
     lib.emu_bc6h_encode.argtypes = [vp, i, i, sz, vp]
     lib.emu_astc_encode.argtypes = [vp, i, i, sz, vp, vp]
     lib.emu_mip_next.argtypes = [vp, i, i, sz, i, vp, sz]
+    lib.emu_div255_mismatches.argtypes = [C.c_uint64, C.c_uint64]
+    lib.emu_div255_mismatches.restype = C.c_uint64
     return lib
 
 
@@ -121,3 +123,14 @@ def test_bc6h_block_logic_extreme_values(emu, oracle):
     out = np.zeros(oracle_lib.bc_size(w, h, BC7), np.uint8)
     emu.emu_bc6h_encode(wild.ctypes.data, w, h, w * 4, out.ctypes.data)
     assert np.array_equal(out, oracle.bc6h_encode(wild))
+
+
+def test_div255_equals_division_for_every_float(emu):
+    """The quantisers divide by 255 with Markstein's FMA correction instead of a division; that must give the
+    correctly rounded quotient, bit for bit, for all 2^32 bit patterns (non-finite ones and -0 skipped)."""
+    from concurrent.futures import ThreadPoolExecutor
+    chunks = 64
+    step = (1 << 32) // chunks
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        bad = sum(ex.map(lambda k: emu.emu_div255_mismatches(k * step, (k + 1) * step), range(chunks)))
+    assert bad == 0

@@ -305,7 +305,7 @@ ZTC_DEV void m5_quant(const float v[3], int nc, int n, int q[3], int x8[3]) {
     #pragma unroll
     for (int c = 0; c < 3; c++) {
         if (c >= nc) { q[c] = 0; x8[c] = 0; continue; }
-        int g = f2i_x86(v[c] * (float)top / 255.0f + 0.5f), bq = 0, bd = 1 << 30;
+        int g = f2i_x86(div255(v[c] * (float)top) + 0.5f), bq = 0, bd = 1 << 30;
         #pragma unroll
         for (int k = 0; k < 3; k++) {
             int tq = clampi(around(g, k), 0, top);

@@ -11,7 +11,7 @@ namespace ztc {
 
 // ---------------------------------------------------------------- BC1 (zap_tex.h:39-168)
 ZTC_DEV uint32_t pack565(float r, float g, float b) {  // zap_tex.h:45-49
-    int R = f2i_x86(r * 31.0f / 255.0f + 0.5f), G = f2i_x86(g * 63.0f / 255.0f + 0.5f), B = f2i_x86(b * 31.0f / 255.0f + 0.5f);
+    int R = f2i_x86(div255(r * 31.0f) + 0.5f), G = f2i_x86(div255(g * 63.0f) + 0.5f), B = f2i_x86(div255(b * 31.0f) + 0.5f);
     return ((uint32_t)clampi(R, 0, 31) << 11) | ((uint32_t)clampi(G, 0, 63) << 5) | (uint32_t)clampi(B, 0, 31);
 }
 

@@ -48,6 +48,7 @@ ZTC_DEV int popc(uint32_t v) { return __popc(v); }
 ZTC_DEV uint32_t f_as_u(float f) { return __float_as_uint(f); }
 ZTC_DEV uint32_t brev(uint32_t v) { return __brev(v); }
 ZTC_DEV int trunc_i(float f) { return __float2int_rz(f); }
+ZTC_DEV float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 template <typename T> ZTC_DEV T ldg(const T *p) { return __ldg(p); }
 #else
 inline uint32_t dot4(uint32_t a, uint32_t b) {
@@ -59,6 +60,7 @@ inline int popc(uint32_t v) { return __builtin_popcount(v); }
 inline uint32_t f_as_u(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
 inline uint32_t brev(uint32_t v) { uint32_t r = 0; for (int k = 0; k < 32; k++) r |= ((v >> k) & 1u) << (31 - k); return r; }
 inline int trunc_i(float f) { return (int)f; }  // only called on in-range values
+inline float fma_rn(float a, float b, float c) { return std::fmaf(a, b, c); }
 template <typename T> inline T ldg(const T *p) { return *p; }
 #endif
 
@@ -73,6 +75,17 @@ ZTC_DEV int f2i_x86(float f) {
 // mid-range value took the == 1023 branch); the host build and this form are correct.
 ZTC_DEV int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 ZTC_DEV float clamp255(float v) { return v < 0.0f ? 0.0f : v > 255.0f ? 255.0f : v; }  // NaN passes through
+// x / 255 correctly rounded, without a division instruction sequence: Markstein's method (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990):
+// q = RN(x * RN(1/255)) is within an ulp of x / 255, the remainder x - 255 q is exact in one FMA, and
+// RN(q + remainder * RN(1/255)) is the correctly rounded quotient. Equal to IEEE x / 255.0f for every finite float x
+// (the host test checks all of them) except -0, which gives +0 (every caller adds to the quotient before it rounds
+// to an integer, which erases the sign of a zero); NaN gives NaN.
+ZTC_DEV float div255(float x) {
+    constexpr float kInv = 0x1.010102p-8f;  // RN(1 / 255)
+    const float q = x * kInv;
+    return fma_rn(fma_rn(-255.0f, q, x), kInv, q);
+}
 // candidate k of {g-1, g, g+1}, wrapping like the reference's compiled three-candidate loops
 ZTC_DEV int around(int g, int k) { return (int)((unsigned)g + (unsigned)k - 1u); }
 
@@ -90,7 +103,7 @@ ZTC_DEV int quant_pbit(const float v[4], int n, int p, int q[4], int x8[4]) {
     int err = 0, top = (1 << (n - 1)) - 1;
     #pragma unroll
     for (int c = 0; c < NC; c++) {
-        int g = f2i_x86((v[c] / 255.0f * (float)((1 << n) - 1) - (float)p) / 2.0f + 0.5f), bq = 0, be = 1 << 30;
+        int g = f2i_x86((div255(v[c]) * (float)((1 << n) - 1) - (float)p) / 2.0f + 0.5f), bq = 0, be = 1 << 30;
         #pragma unroll
         for (int k = 0; k < 3; k++) {
             int tq = clampi(around(g, k), 0, top);
