@@ -130,4 +130,17 @@ __attribute__((visibility("default"))) uint64_t emu_div255_mismatches(uint64_t l
     return bad;
 }
 
+// (x, n) pairs, x an integer in [0, 2^24) and n in [1, 16], for which ztc::div_small(x, n, 1 / n) differs bitwise from
+// the division x / n
+__attribute__((visibility("default"))) uint64_t emu_div_small_mismatches(int n) {
+    volatile float dv = (float)n;  // a runtime divisor: the host compiler emits true divisions
+    const float ni = 1.0f / dv;
+    uint64_t bad = 0;
+    for (uint32_t v = 0; v < (1u << 24); v++) {
+        const float x = (float)v, a = x / dv, m = div_small(x, dv, ni);
+        if (std::memcmp(&a, &m, 4) != 0) bad++;
+    }
+    return bad;
+}
+
 }  // extern "C"

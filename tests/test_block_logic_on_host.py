@@ -38,6 +38,8 @@ def emu():
     lib.emu_mip_next.argtypes = [vp, i, i, sz, i, vp, sz]
     lib.emu_div255_mismatches.argtypes = [C.c_uint64, C.c_uint64]
     lib.emu_div255_mismatches.restype = C.c_uint64
+    lib.emu_div_small_mismatches.argtypes = [i]
+    lib.emu_div_small_mismatches.restype = C.c_uint64
     return lib
 
 
@@ -133,4 +135,13 @@ def test_div255_equals_division_for_every_float(emu):
     step = (1 << 32) // chunks
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
         bad = sum(ex.map(lambda k: emu.emu_div255_mismatches(k * step, (k + 1) * step), range(chunks)))
+    assert bad == 0
+
+
+def test_small_divisor_division_equals_ieee_on_its_domain(emu):
+    """The partition scores and subset means divide integer-valued floats below 2^24 by counts 1..16 with the same
+    FMA correction; every such pair must give the IEEE quotient bit for bit."""
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        bad = sum(ex.map(emu.emu_div_small_mismatches, range(1, 17)))
     assert bad == 0

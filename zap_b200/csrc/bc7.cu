@@ -386,8 +386,10 @@ ZTC_DEV float partition_score(const float s1[9], int n1, const float tot[9]) {
         for (int j = 0; j < 9; j++) m[j] = k ? s1[j] : tot[j] - s1[j];
         float n = (float)(k ? n1 : 16 - n1);
         if (n < 2) continue;
-        float S00 = m[3] - m[0] * m[0] / n, S01 = m[6] - m[0] * m[1] / n, S02 = m[7] - m[0] * m[2] / n;
-        float S11 = m[4] - m[1] * m[1] / n, S12 = m[8] - m[1] * m[2] / n, S22 = m[5] - m[2] * m[2] / n;
+        const float ni = 1.0f / n;  // the six quotients below: integer-valued numerators below 2^24 (div_small)
+        float S00 = m[3] - div_small(m[0] * m[0], n, ni), S01 = m[6] - div_small(m[0] * m[1], n, ni);
+        float S02 = m[7] - div_small(m[0] * m[2], n, ni), S11 = m[4] - div_small(m[1] * m[1], n, ni);
+        float S12 = m[8] - div_small(m[1] * m[2], n, ni), S22 = m[5] - div_small(m[2] * m[2], n, ni);
         float tr = S00 + S11 + S22, a0, a1, a2;
         if (S00 >= S11 && S00 >= S22) { a0 = S00; a1 = S01; a2 = S02; }
         else if (S11 >= S22) { a0 = S01; a1 = S11; a2 = S12; }

@@ -86,6 +86,13 @@ ZTC_DEV float div255(float x) {
     const float q = x * kInv;
     return fma_rn(fma_rn(-255.0f, q, x), kInv, q);
 }
+// x / n for an integer-valued x in [0, 2^24) and an integer n in [1, 16], from ni = RN(1/n): the same correction as
+// div255, exact on that whole domain (the host test enumerates it). The callers' operands are texel channel values
+// or products of two sums of at most 16 of them (at most 4080^2 < 2^24), all exact integers in float.
+ZTC_DEV float div_small(float x, float n, float ni) {
+    const float q = x * ni;
+    return fma_rn(fma_rn(-n, q, x), ni, q);
+}
 // candidate k of {g-1, g, g+1}, wrapping like the reference's compiled three-candidate loops
 ZTC_DEV int around(int g, int k) { return (int)((unsigned)g + (unsigned)k - 1u); }
 

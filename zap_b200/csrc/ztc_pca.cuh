@@ -28,14 +28,18 @@ ZTC_DEV bool pca_power_step(const float C[NC][NC], float ax[NC]) {
 // (the same operations in the same order, in less code), UNROLL 16 unrolls them
 template <int NC, int UNROLL = 16, typename Tex>
 ZTC_DEV void pca_endpoints(const Tex &t, uint32_t mask, float lo[4], float hi[4]) {
-    const float cnt = (float)popc(mask);
+    const float cnt = (float)popc(mask), cnti = 1.0f / cnt;
+    const bool whole = mask == 0xFFFFu;  // a compile-time constant for whole-block calls: x / 16 is a multiply there
     float mu[NC];
     #pragma unroll
     for (int c = 0; c < NC; c++) mu[c] = 0.0f;
     for_texels<UNROLL>([&](int i) {
         if ((mask >> i) & 1u) {
             #pragma unroll
-            for (int c = 0; c < NC; c++) mu[c] = mu[c] + (float)chan(t[i], c) / cnt;
+            for (int c = 0; c < NC; c++) {
+                const float x = (float)chan(t[i], c);
+                mu[c] = mu[c] + (whole ? x / 16.0f : div_small(x, cnt, cnti));
+            }
         }
     });
     // upper triangle only: cov[a][b] and cov[b][a] add bitwise-identical products in the same order
