@@ -583,9 +583,14 @@ def extra_workloads(args, dev, sm_mhz=None, sms=148):
             outs[k % ring] = f(texs[k % ring], outs[k % ring])
         for k in range(ring):  # allocates every output before the timed region
             step(k)
-        ms = time_device(step, steps, 0, 1)
+        # the median of five timed segments: one host-side stall (tens of ms) inside a single short window would
+        # otherwise dominate these few-millisecond figures
+        seg = max(4, steps // 5)
+        per = sorted(time_device(step, seg, 0, 1) / seg for _ in range(5))
+        ms = per[2] * steps
         mps = steps * npix / 1e6 / (ms / 1e3)
-        res[name] = {"Mpix_s": mps, "ms_per_encode": ms / steps, "GB_s_algorithmic": mps * 1e6 * alg_bytes_per_px / 1e9}
+        res[name] = {"Mpix_s": mps, "ms_per_encode": ms / steps, "GB_s_algorithmic": mps * 1e6 * alg_bytes_per_px / 1e9,
+                     "timing": "median of 5 segments of %d encodes (CUDA events)" % seg}
         counted = {"bc1_2048x2048": "bc1_encode", "bc4_2048x2048_r8": "bc4_encode", "bc5_2048x2048_rg8": "bc5_encode",
                    "astc4x4_2048x2048": "astc_encode", "bc6h_2048x2048_rgb16f": "bc6h_encode"}.get(name)
         if counted:  # the whole encode (all its kernels) against the ALU roofline
