@@ -1,6 +1,6 @@
 """Full-size and very large inputs on the device, byte for byte.
 
-- The BASELINE configurations at their full sizes (2048x2048): BC7 RGBA8, BC4 from R8, BC5 from RG8, BC6H from
+- The benchmark configurations at their full sizes (2048x2048): BC7 RGBA8, BC4 from R8, BC5 from RG8, BC6H from
   RGB16F, ASTC 4x4, BC1, against the reference encoder (all host threads when the reference library is built).
 - A 32768x16400 RGBA8 image (2.1 GB, past 32-bit byte offsets; odd last block row) encoded to BC1 and BC7 through
   the device API. At rdo 0 each block depends only on its own 16 texels (edge texels replicated), so the texels of
