@@ -179,21 +179,89 @@ def peaks():
         return 6650.0, "fallback"
 
 
+# the measured scalar issue rate (instructions per clock per SM), set by measure_alu_peak() before any roofline
+ALU_PEAK = {}
+
+
+def measure_alu_peak(dev, sms, local, seconds=1.0):
+    """Measures the SMs' instruction rate for the kinds the encoders are built from (zap_tex_cuda_alu_probe_dev:
+    8 CTAs of 256 threads per SM, 8 independent chains per thread of mad.lo.u32, fma.rn.f32, dp4a, or mad/fma
+    alternating), each kind one launch of about `seconds`, timed with CUDA events while the SM clock is sampled.
+    Rates are in instructions per clock per SM (time x median sampled SM MHz), so a roofline can be scaled to the
+    clock of the region it is compared with."""
+    import ctypes as C
+
+    import torch
+
+    import zap_b200
+    lib = zap_b200.load()
+    sink = torch.zeros(4, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    ins = C.c_double()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(kind, iters):
+        e0.record()
+        zap_b200.check(lib.zap_tex_cuda_alu_probe_dev(kind, iters, sink.data_ptr(), C.c_void_p(stream.cuda_stream), C.byref(ins)),
+                       "alu_probe")
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    kinds = {}
+    for kind, name in ((0, "imad"), (1, "ffma"), (2, "dp4a"), (3, "imad+ffma")):
+        timed(kind, 64)
+        ms = timed(kind, 256)
+        iters = max(256, min(2_000_000, int(256 * seconds * 1e3 / max(ms, 1e-3))))
+        with ClockSampler(local) as clk:
+            ms = timed(kind, iters)
+        mhz = clk.summary()["sm_mhz"] or clk.summary()["sm_max_mhz"]
+        if not mhz:
+            continue
+        kinds[name] = {"ms": ms, "instructions": ins.value, "sm_mhz": mhz, "G_per_s": ins.value / (ms / 1e3) / 1e9,
+                       "per_clk_per_sm": ins.value / (ms / 1e3) / (mhz * 1e6) / sms}
+    if kinds:
+        best = max((k for k in kinds if k != "dp4a"), key=lambda k: kinds[k]["per_clk_per_sm"])
+        ALU_PEAK.update({"per_clk_per_sm": kinds[best]["per_clk_per_sm"], "kind": best, "kinds": kinds})
+    return ALU_PEAK
+
+
 def alu_roofline(kernel, ops_per_launch_ms, sm_mhz, sms):
     """ALU roofline of one kernel: the reference algorithm's counted operations per launch (profiles/alu_ops.json,
-    written by oracle/count_ops.py on this workload's textures) over the kernel's average launch time, against a
-    derived issue peak of 128 32-bit lanes per SM x SMs x the median SM clock of the timed region. The kernels do a
-    texel-to-entry distance (13 counted ops for RGBA) in one dp4a + one multiply-add + one min, so a fraction above
-    1 is possible; the fraction is a throughput figure against scalar issue, not a utilisation."""
+    written by oracle/count_ops.py on this workload's textures) over the kernel's average launch time, against the
+    measured scalar issue rate (the fastest of mad.lo.u32, fma.rn.f32 and their mix, instructions per clock per SM
+    from measure_alu_peak) x SMs x the median SM clock of the timed region; without a measurement, the derived 128
+    lanes per SM. The kernels do a texel-to-entry distance (13 counted ops for RGBA) in one dp4a + one multiply-add +
+    one min, so a fraction above 1 is possible: it is a throughput figure against scalar issue; the ncu issue-slot
+    use of each kernel (profiles/issue_active.json) is the utilisation."""
     ops, ms = ops_per_launch_ms
     table = alu_ops()
     if ops is None or not ms or not sm_mhz:
         return None
-    peak = sms * 128 * sm_mhz * 1e6 / 1e9
+    if ALU_PEAK:
+        per_clk = ALU_PEAK["per_clk_per_sm"]
+        source = (f"measured: {per_clk:.1f} {ALU_PEAK['kind']} instructions per clock per SM (alu probe) x {sms} SMs x "
+                  f"{sm_mhz:.0f} MHz (median SM clock, timed region)")
+    else:
+        per_clk = 128.0
+        source = f"derived: {sms} SMs x 128 lanes x {sm_mhz:.0f} MHz (median SM clock, timed region)"
+    peak = sms * per_clk * sm_mhz * 1e6 / 1e9
     achieved = ops / (ms / 1e3) / 1e9
-    return {"bound": "alu", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "Gop/s", "frac": achieved / peak,
-            "ops_per_launch": ops, "peak_source": f"derived: {sms} SMs x 128 lanes x {sm_mhz:.0f} MHz (median SM clock, timed region)",
-            "ops_definition": table.get("definition") if table else None}
+    out = {"bound": "alu", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "Gop/s", "frac": achieved / peak,
+           "ops_per_launch": ops, "peak_source": source, "ops_definition": table.get("definition") if table else None}
+    issue = issue_active().get(kernel)
+    if issue is not None:
+        out["ncu_issue_active"] = issue
+    return out
+
+
+def issue_active():
+    """smsp__issue_active (% of issue slots) per kernel or encode, from the committed ncu captures."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "issue_active.json")) as f:
+            return json.load(f).get("kernels", {})
+    except (OSError, ValueError):
+        return {}
 
 
 def alu_ops():
@@ -387,9 +455,11 @@ def main():
                 "traffic": traffic, "peak_source": peak_kind, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
                 "kernels": {k: {"launches": v[0], "ms": v[1], "units": v[2], "share": v[1] / sum(x[1] for x in rep.values())}
                             for k, v in rep.items()}}
-    # the bound that binds: counted algorithmic ops against the SMs' issue rate (one launch = one 2048^2 texture)
+    # the bound that binds: counted algorithmic ops against the SMs' measured issue rate (one launch = one 2048^2
+    # texture); the probe runs after the timed region
     csum = clocks.summary()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    measure_alu_peak(dev, sms, local)
     mhz = csum.get("sm_mhz") or csum.get("sm_max_mhz")
     roofline["alu"] = alu_roofline(name, (ops_per_texture(name), avg_ms), mhz, sms)
     roofline["alu_kernels"] = {k: alu_roofline(k, (ops_per_texture(k), v[1] / max(1, v[0])), mhz, sms) for k, v in rep.items()}
@@ -400,7 +470,7 @@ def main():
             "config": {"workload": WORKLOAD, "l2": f"inputs larger than L2: ring of {ring} distinct {W}x{H} textures",
                        "parallelism": "independent replicas" if world > 1 else "1 gpu",
                        "step": "replay of a CUDA graph of one zap_tex_cuda_bc_encode_dev call per ring slot"},
-            "roofline": roofline, "gpu_launches": launches, "clocks": clocks.summary()}
+            "roofline": roofline, "gpu_launches": launches, "clocks": clocks.summary(), "alu_peak": ALU_PEAK}
 
     if rank == 0:
         # e2e: host C ABI, pinned host memory, copies inside the timed region. The buffers are allocated and the
@@ -565,16 +635,96 @@ def refine_workload(args, dev, n=1024, side=256, steps=8, lr=1.0):
     return res
 
 
-def extra_workloads(args, dev, sm_mhz=None, sms=148):
-    """Secondary figures: BC1 (config 0 and 2048^2), BC4 R8 / BC5 RG8 (config 1), BC6H / ASTC (config 3)."""
+def atlas_texture(side, tile, seed, device, order_seed):
+    """A side x side texture atlas of tile x tile textures of the batch's recipe (colour_texture, one seed per tile),
+    placed in an order drawn from order_seed: small textures carry more detail per 4x4 block, so more BC7 blocks
+    leave mode 6 than in one large texture of the same recipe."""
     import torch
 
+    import zap_b200.synth as S
+    n = side // tile
+    tiles = [S.colour_texture(tile, tile, seed=seed + k, device=device) for k in range(n * n)]
+    perm = torch.randperm(n * n, generator=torch.Generator().manual_seed(order_seed)).tolist()
+    rows = [torch.cat([tiles[perm[r * n + c]] for c in range(n)], 1) for r in range(n)]
+    return torch.cat(rows, 0).contiguous()
+
+
+def log2_psnr(src, dec):
+    """BC6H quality in log space: L(v) = log2(max(v, 2^-14)) per RGB channel, 10 log10(30^2 / mean squared
+    difference); 99 when identical (the reference defines no HDR PSNR)."""
+    import numpy as np
+    a = np.log2(np.maximum(src[..., :3].astype(np.float64), 2.0 ** -14))
+    b = np.log2(np.maximum(dec[..., :3].astype(np.float64), 2.0 ** -14))
+    mse = float(np.mean((a - b) ** 2))
+    return 99.0 if mse == 0 else 10 * np.log10(30.0 ** 2 / mse)
+
+
+def extra_workloads(args, dev, sm_mhz=None, sms=148):
+    """Secondary figures, one entry per format and input: BC1 (config 0 512^2, and 2048^2), BC4 R8 / BC5 RG8
+    (config 1), BC6H / ASTC (config 3), and BC7 on content where many blocks go past mode 6 (opaque 2048^2, and an
+    atlas of 64^2 textures). Each entry has, beside its device figure (CUDA events, inputs resident): the fraction of
+    blocks identical to the reference encoder on the first ring texture, the PSNR of both outputs (as the reference's
+    tex_bench.c:200-214 table prints it), and the reference's CPU figure on that texture, on all host threads
+    (8-block-row bands) and on one core (one call, wall clock, tex_bench.c:205-208)."""
+    import numpy as np
+    import torch
+
+    import oracle_lib
     import zap_b200
     import zap_b200.synth as S
+    ref = oracle_lib.reference()
+    threads = os.cpu_count() or 1
     res = {}
     steps = max(5, args.steps // 2)
 
-    def bench(name, make, fmt, npix, ring, alg_bytes_per_px, enc=None):
+    def widen(t, chans):  # narrow input -> the RGBA8 texels the reference reads (missing channels 0, alpha 255)
+        host = t.cpu().numpy()
+        if chans == 4:
+            return host
+        wide = np.zeros(host.shape[:2] + (4,), np.uint8)
+        wide[..., :chans] = host
+        wide[..., 3] = 255
+        return wide
+
+    def parity(t, got, fmt, chans):
+        """identical blocks, PSNR of ours and of the reference, and the reference's CPU time on texture t"""
+        if ref is None:
+            return {"unavailable": "oracle/_ref/libzapref.so is not built"}
+        h, w = t.shape[0], t.shape[1]
+        if fmt == "bc6h":
+            src = np.ones((h, w, 4), np.float32)
+            src[..., :3] = t.cpu().numpy().astype(np.float32)
+            run = lambda k: ref.bc6h_encode(src, threads=k)  # noqa: E731
+            dec = lambda bc: ref.bc6h_decode(bc, w, h).view(np.float16).astype(np.float32)  # noqa: E731
+            quality = lambda bc: log2_psnr(src, dec(bc))  # noqa: E731
+        elif fmt == "astc":
+            src = widen(t, chans)
+            run = lambda k: ref.astc_encode(src, threads=k)  # noqa: E731
+            quality = lambda bc: oracle_lib.psnr(src, ref.astc_decode(bc, w, h), 15)  # noqa: E731
+        else:
+            src = widen(t, chans)
+            run = lambda k: ref.bc_encode(src, fmt, threads=k)  # noqa: E731
+            quality = lambda bc: oracle_lib.psnr(src, ref.bc_decode(bc, w, h, fmt), oracle_lib.chmask(fmt))  # noqa: E731
+        t0 = time.perf_counter()
+        want = run(1)
+        one = time.perf_counter() - t0
+        best = float("inf")
+        for _ in range(2):
+            t0 = time.perf_counter()
+            run(threads)
+            best = min(best, time.perf_counter() - t0)
+        mine = got.cpu().numpy()
+        bs = 8 if fmt in (oracle_lib.BC1, oracle_lib.BC4) else 16
+        same = float(np.mean(np.all(mine.reshape(-1, bs) == want.reshape(-1, bs), axis=1)))
+        mpix = w * h / 1e6
+        return {"identical_blocks": same, "psnr_db": quality(mine), "psnr_reference_db": quality(want),
+                "psnr_kind": "log2 RGB, 30 dB span" if fmt == "bc6h" else "tex_bench.c:17-22",
+                "cpu_baseline": {"value": mpix / best, "unit": "Mpix/s", "cores": threads, "kind": "reference",
+                                 "sample": f"first ring texture ({w}x{h}), best of 2, 8-block-row bands on all host threads",
+                                 "one_core": {"value": mpix / one, "unit": "Mpix/s", "cores": 1,
+                                              "sample": "same texture, one call, wall clock (tex_bench.c:205-208)"}}}
+
+    def bench(name, make, fmt, npix, ring, alg_bytes_per_px, chans=4, enc=None, counted=None):
         texs = [make(k) for k in range(ring)]
         outs = [None] * ring
         f = enc or (lambda t, o: zap_b200.bc_encode_dev(t, fmt, out=o))
@@ -591,20 +741,31 @@ def extra_workloads(args, dev, sm_mhz=None, sms=148):
         mps = steps * npix / 1e6 / (ms / 1e3)
         res[name] = {"Mpix_s": mps, "ms_per_encode": ms / steps, "GB_s_algorithmic": mps * 1e6 * alg_bytes_per_px / 1e9,
                      "timing": "median of 5 segments of %d encodes (CUDA events)" % seg}
-        counted = {"bc1_2048x2048": "bc1_encode", "bc4_2048x2048_r8": "bc4_encode", "bc5_2048x2048_rg8": "bc5_encode",
-                   "astc4x4_2048x2048": "astc_encode", "bc6h_2048x2048_rgb16f": "bc6h_encode"}.get(name)
         if counted:  # the whole encode (all its kernels) against the ALU roofline
             res[name]["alu"] = alu_roofline(counted, (ops_per_texture(counted), ms / steps), sm_mhz, sms)
+        torch.cuda.synchronize()
+        res[name].update(parity(texs[0], outs[0], fmt, chans))
+        cpu = res[name].get("cpu_baseline")
+        if cpu:
+            res[name]["speedup_vs_cpu_all_threads"] = mps / cpu["value"]
+        del texs, outs
 
     bench("bc1_512x512_config0", lambda k: S.colour_texture(512, 512, seed=k, device=dev), zap_b200.BC1, 512 * 512, 64, 4.5)
-    bench("bc1_2048x2048", lambda k: S.colour_texture(2048, 2048, seed=k, device=dev), zap_b200.BC1, 2048 * 2048, 10, 4.5)
+    bench("bc1_2048x2048", lambda k: S.colour_texture(2048, 2048, seed=k, device=dev), zap_b200.BC1, 2048 * 2048, 10, 4.5,
+          counted="bc1_encode")
     bench("bc4_2048x2048_r8", lambda k: S.colour_texture(2048, 2048, seed=k, device=dev)[..., :1].contiguous(), zap_b200.BC4,
-          2048 * 2048, 40, 1.5)
-    bench("bc5_2048x2048_rg8", lambda k: S.normal_map(2048, 2048, seed=k, device=dev), zap_b200.BC5, 2048 * 2048, 20, 3.0)
-    bench("astc4x4_2048x2048", lambda k: S.colour_texture(2048, 2048, seed=k, alpha="noise", device=dev), zap_b200.ASTC4X4,
+          2048 * 2048, 40, 1.5, chans=1, counted="bc4_encode")
+    bench("bc5_2048x2048_rg8", lambda k: S.normal_map(2048, 2048, seed=k, device=dev), zap_b200.BC5, 2048 * 2048, 20, 3.0,
+          chans=2, counted="bc5_encode")
+    bench("astc4x4_2048x2048", lambda k: S.colour_texture(2048, 2048, seed=k, alpha="noise", device=dev), "astc",
+          2048 * 2048, 10, 5.0, enc=lambda t, o: zap_b200.astc_encode_dev(t, out=o), counted="astc_encode")
+    bench("bc6h_2048x2048_rgb16f", lambda k: S.hdr_texture(2048, 2048, seed=k, device=dev), "bc6h", 2048 * 2048, 6, 7.0,
+          chans=3, enc=lambda t, o: zap_b200.bc6h_encode_dev(t, out=o), counted="bc6h_encode")
+    bench("bc7_2048x2048_opaque", lambda k: S.colour_texture(2048, 2048, seed=k, device=dev), zap_b200.BC7, 2048 * 2048, 10, 5.0)
+    atlas = atlas_texture(2048, 64, 40000, dev, 0)
+    bench("bc7_2048x2048_atlas_of_64x64", lambda k: atlas if k == 0 else atlas_texture(2048, 64, 40000, dev, k), zap_b200.BC7,
           2048 * 2048, 10, 5.0)
-    bench("bc6h_2048x2048_rgb16f", lambda k: S.hdr_texture(2048, 2048, seed=k, device=dev), None, 2048 * 2048, 6, 7.0,
-          enc=lambda t, o: zap_b200.bc6h_encode_dev(t, out=o))
+    torch.cuda.empty_cache()
     return res
 
 

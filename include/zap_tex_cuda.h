@@ -218,6 +218,14 @@ ZTC_API size_t zap_tex_cuda_tex_file_bytes(int w, int h, int fmt, int mips, int 
 ZTC_API int zap_tex_cuda_tex_file(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo,
                                   int mips, int srgb, void *out, size_t out_cap);
 
+/* ---------------------------------------------------------------- diagnostics (no reference counterpart) */
+/* Issue-rate probe for the encoders' ALU roofline: enqueues on `stream` one launch of 8 CTAs of 256 threads per
+   SM, every thread running 8 independent chains of one instruction kind for iters x 256 instructions (kind 0
+   mad.lo.u32, 1 fma.rn.f32, 2 dp4a, 3 mad.lo.u32 and fma.rn.f32 alternating). *instructions receives the number of
+   probe instructions the launch executes; the caller times it (CUDA events) and divides. sink: 4 bytes of device
+   memory the kernel may write. */
+ZTC_API int zap_tex_cuda_alu_probe_dev(int kind, int iters, void *sink, void *stream, double *instructions);
+
 /* Allocation-free BC7 encode. No counterpart in the reference (zap_tex.h allocates nothing because it runs on the
    CPU); it exists for callers that cannot allocate device memory when they encode: work recorded into a CUDA
    graph, real-time frame loops, engines with a fixed up-front GPU budget, plug-in hosts that only hand over their
@@ -225,8 +233,9 @@ ZTC_API int zap_tex_cuda_tex_file(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, in
    It never calls cudaMalloc/cudaFree: its work list is a static device array sized for at most 1048576 4x4
    blocks (4096 x 4096 texels, about 8 MB held by every GPU that loads the library); larger textures return
    ZTC_ERR_INVALID_ARG. The first call on a device looks up that array's address (make it before any stream
-   capture). All calls share the array: calls whose kernels overlap on the GPU race, so serialise them (one
-   stream, or events). */
+   capture) and keeps it for the life of the process: a cudaDeviceReset unloads the library's device code and
+   leaves that address stale, so do not call this entry point again after resetting a device it has run on. All
+   calls share the array: calls whose kernels overlap on the GPU race, so serialise them (one stream, or events). */
 ZTC_API int zap_tex_cuda_bc7_encode_noalloc_dev(const uint8_t *rgba, int w, int h, size_t stride, void *out, void *stream);
 
 #ifdef __cplusplus

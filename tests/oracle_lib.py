@@ -17,7 +17,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 PORT_SO = os.path.join(ORACLE_DIR, "liboracle.so")
 REF_SO = os.path.join(ORACLE_DIR, "_ref", "libzapref.so")
-REF_TREE = "/root/reference"
+REF_TREE = os.environ.get("ZAP_REF_DIR", "/root/reference")  # the reference source tree, where one exists
 
 BC1, BC3, BC4, BC5, BC7 = 0, 1, 2, 3, 4
 _lock = threading.Lock()

@@ -2,6 +2,9 @@
 
 - The benchmark configurations at their full sizes (2048x2048): BC7 RGBA8, BC4 from R8, BC5 from RG8, BC6H from
   RGB16F, ASTC 4x4, BC1, against the reference encoder (all host threads when the reference library is built).
+- The exact textures the benchmark times, generated the way it generates them: BC1 of the 512x512 seed-0 texture
+  (the reference's plain BC1 case, which must be byte-identical), the headline BC7 texture, and the first texture
+  of every secondary figure's ring.
 - A 32768x16400 RGBA8 image (2.1 GB, past 32-bit byte offsets; odd last block row) encoded to BC1 and BC7 through
   the device API. At rdo 0 each block depends only on its own 16 texels (edge texels replicated), so the texels of
   any block, cut out as a 4x4 image (smaller at the right and bottom edges), encode to that block's bytes: sampled
@@ -45,6 +48,29 @@ def test_full_size_configs_match_reference(cuda_lib):
     f32 = np.ones((2048, 2048, 4), np.float32)
     f32[..., :3] = half.cpu().numpy().astype(np.float32)
     assert np.array_equal(cuda_lib.bc6h_encode_dev(half).cpu().numpy(), ref.bc6h_encode(f32, threads=THREADS))
+
+
+def test_benchmark_textures_match_reference(cuda_lib):
+    import torch
+
+    import zap_b200.synth as S
+    ref = oracle_lib.best()
+    dev = torch.device("cuda", 0)
+    # plain BC1 (default quality, rdo 0) of one 512x512 RGBA8 texture from seed 0, alpha 255: byte-identical
+    c0 = S.colour_texture(512, 512, seed=0, device=dev)
+    assert bool((c0[..., 3] == 255).all())
+    got = cuda_lib.bc_encode_dev(c0, BC1).cpu().numpy()
+    assert np.array_equal(got, ref.bc_encode(c0.cpu().numpy(), BC1))
+    # the headline texture (BC7, noise alpha, seed 100) and each secondary figure's first ring texture (seed 0)
+    c1 = S.colour_texture(2048, 2048, seed=100, alpha="noise", device=dev)
+    assert np.array_equal(cuda_lib.bc_encode_dev(c1, BC7).cpu().numpy(), ref.bc_encode(c1.cpu().numpy(), BC7, threads=THREADS))
+    opaque = S.colour_texture(2048, 2048, seed=0, device=dev)
+    host = opaque.cpu().numpy()
+    assert np.array_equal(cuda_lib.bc_encode_dev(opaque, BC1).cpu().numpy(), ref.bc_encode(host, BC1, threads=THREADS))
+    wide = np.zeros_like(host)
+    wide[..., 0], wide[..., 3] = host[..., 0], 255
+    assert np.array_equal(cuda_lib.bc_encode_dev(opaque[..., :1].contiguous(), BC4).cpu().numpy(),
+                          ref.bc_encode(wide, BC4, threads=THREADS))
 
 
 def _huge_image(w, h, device):

@@ -4,14 +4,19 @@ Some callers cannot allocate device memory while they encode - work recorded int
 loops, engines with a fixed up-front GPU budget, plug-in hosts that only hand over their own buffers. This entry
 point keeps its BC7 work list in a static device array instead of allocating one. Its output must be byte-for-byte
 the output of the allocating entry point, also on consecutive calls that share that array (the list must start
-empty every time), and oversize textures must be refused before anything runs.
+empty every time), and oversize textures must be refused before anything runs. At exactly its limit (4096 x 4096
+texels, 1048576 blocks) of uniform noise, where every block goes on the list, its bytes must be the reference
+encoder's.
 
 The file name sorts last so that a run stopping at the first failure has run every other test already.
 """
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
+
+import oracle_lib
 
 pytestmark = pytest.mark.gpu
 
@@ -39,6 +44,30 @@ def test_noalloc_bc7_matches_allocating_entry_point(cuda_lib):
         assert _call(lib, tex, got, stream) == 0, lib.zap_tex_cuda_last_error()
         torch.cuda.synchronize()
         assert torch.equal(got, expect)
+
+
+def test_noalloc_bc7_at_its_block_limit(cuda_lib):
+    import torch
+
+    import zap_b200.synth as S
+    lib = cuda_lib.load()
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(11)
+    host = rng.integers(0, 256, (4096, 4096, 4), dtype=np.uint8)  # 1048576 blocks, every one past mode 6
+    host[:2048, :, 3] = 255                                         # opaque top half: mode 1 runs there too
+    noise = torch.from_numpy(host).cuda()
+    got = torch.full((4096 * 4096,), 0xAB, dtype=torch.uint8, device="cuda")
+    assert _call(lib, noise, got, stream) == 0, lib.zap_tex_cuda_last_error()
+    torch.cuda.synchronize()
+    want = oracle_lib.best().bc_encode(host, oracle_lib.BC7, threads=os.cpu_count() or 1)
+    assert np.array_equal(got.cpu().numpy(), want)
+    # the next call after a full list: smooth content at the same size, few listed blocks, same bytes as the
+    # allocating entry point
+    smooth = S.colour_texture(4096, 4096, seed=5, alpha="noise", device="cuda")
+    got.fill_(0xAB)
+    assert _call(lib, smooth, got, stream) == 0, lib.zap_tex_cuda_last_error()
+    torch.cuda.synchronize()
+    assert torch.equal(got, cuda_lib.bc_encode_dev(smooth, cuda_lib.BC7))
 
 
 def test_noalloc_rejects_textures_beyond_its_limit(cuda_lib):

@@ -90,6 +90,7 @@ def _declare(lib):
         "zap_tex_cuda_astc_header": ([i, i, vp], i),
         "zap_tex_cuda_tex_file_bytes": ([i, i, i, i, i], sz),
         "zap_tex_cuda_tex_file": ([vp, vp, i, i, sz, i, f, i, i, vp, sz], i),
+        "zap_tex_cuda_alu_probe_dev": ([i, i, vp, vp, C.POINTER(C.c_double)], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -14,6 +14,7 @@
 // Every float expression keeps the reference's order; integer argmins keep the first candidate on ties.
 #include <mutex>
 
+#include "../../include/zap_tex_cuda.h"
 #include "ztc_common.cuh"
 #include "ztc_internal.h"
 #include "ztc_pca.cuh"
@@ -825,7 +826,8 @@ cudaError_t ztc_launch_bc7_to(const ztc::SrcU8 &src, int by0, int nby, const ztc
     {
         ztc::TraceScope tr("bc7_mode6", stream);
         ztc::trace_units(nblocks);
-        ztc::launch_mode6(src, bw, by0, nblocks, out, b0, count, items, stream);
+        e = ztc::launch_mode6(src, bw, by0, nblocks, out, b0, count, items, stream);
+        if (e != cudaSuccess) return e;  // launch_mode6 read (and cleared) the launch error; the list is not valid
     }
     int groups_per_cta = 128 / ztc::kBc7Group;
     int ctas = (nblocks + groups_per_cta - 1) / groups_per_cta;
@@ -863,17 +865,22 @@ void *g_noalloc_addr[64];  // per device: device address of g_bc7_noalloc_scratc
 
 extern "C" __attribute__((visibility("default"))) int zap_tex_cuda_bc7_encode_noalloc_dev(const uint8_t *rgba, int w, int h,
                                                                                            size_t stride, void *out, void *stream) {
-    if (!rgba || !out) return ztc_set_error(-1, "null pointer");
-    if (w < 1 || h < 1 || w > (1 << 24) || h > (1 << 24)) return ztc_set_error(-1, "size out of range");
-    if (stride < (size_t)w * 4) return ztc_set_error(-1, "stride below 4 * width");
-    if ((uintptr_t)out % 16u) return ztc_set_error(-1, "out must be 16-byte aligned (BC7 blocks are stored 16 bytes at a time)");
+    if (!rgba || !out) return ztc_set_error(ZTC_ERR_INVALID_ARG, "null pointer");
+    if (w < 1 || h < 1 || w > (1 << 24) || h > (1 << 24)) return ztc_set_error(ZTC_ERR_INVALID_ARG, "size out of range");
+    if (stride < (size_t)w * 4) return ztc_set_error(ZTC_ERR_INVALID_ARG, "stride below 4 * width");
+    if ((uintptr_t)out % 16u)
+        return ztc_set_error(ZTC_ERR_INVALID_ARG, "out must be 16-byte aligned (BC7 blocks are stored 16 bytes at a time)");
     const size_t bw = (size_t)(w + 3) / 4, bh = (size_t)(h + 3) / 4;
     if (bw * bh > ztc::kNoAllocMaxBlocks)
-        return ztc_set_error(-1, "texture has more 4x4 blocks than the allocation-free BC7 entry point holds (1048576)");
+        return ztc_set_error(ZTC_ERR_INVALID_ARG,
+                             "texture has more 4x4 blocks than the allocation-free BC7 entry point holds (1048576)");
     int dev = 0, major = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { cudaGetLastError(); return ztc_set_error(-6, "no CUDA device"); }
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return ztc_set_error(ZTC_ERR_NO_DEVICE, "no CUDA device");
+    }
     cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
-    if (major != 10) return ztc_set_error(-6, "this build targets sm_100a");
+    if (major != 10) return ztc_set_error(ZTC_ERR_NO_DEVICE, "this build targets sm_100a");
     void *scratch = nullptr;
     {
         std::lock_guard<std::mutex> g(g_noalloc_lock);
@@ -882,7 +889,7 @@ extern "C" __attribute__((visibility("default"))) int zap_tex_cuda_bc7_encode_no
             if (e != cudaSuccess) {
                 g_noalloc_addr[dev] = nullptr;
                 cudaGetLastError();
-                return ztc_set_error(-3, cudaGetErrorString(e));
+                return ztc_set_error(ZTC_ERR_CUDA, cudaGetErrorString(e));
             }
         }
         scratch = g_noalloc_addr[dev];
@@ -894,8 +901,8 @@ extern "C" __attribute__((visibility("default"))) int zap_tex_cuda_bc7_encode_no
     const int nblocks = (int)(bw * bh);
     const ztc::BlockOut blocks{(uint8_t *)out, 0, ZTC_FMT_BC7, 0};
     cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), s);  // the list must start empty on every call
-    if (e == cudaSuccess) {
-        ztc::launch_mode6(src, (int)bw, 0, nblocks, blocks, 0, count, items, s);
+    if (e == cudaSuccess) e = ztc::launch_mode6(src, (int)bw, 0, nblocks, blocks, 0, count, items, s);
+    if (e == cudaSuccess) {  // modes 5/1 run only over a list that mode 6 has filled
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         int ctas = (nblocks + 15) / 16;
@@ -903,6 +910,6 @@ extern "C" __attribute__((visibility("default"))) int zap_tex_cuda_bc7_encode_no
         ztc::bc7_hard_kernel<<<ctas, 128, 0, s>>>(src, (int)bw, 0, blocks, 0, count, items);
         e = cudaGetLastError();
     }
-    if (e != cudaSuccess) { cudaGetLastError(); return ztc_set_error(-3, cudaGetErrorString(e)); }
-    return 0;
+    if (e != cudaSuccess) { cudaGetLastError(); return ztc_set_error(ZTC_ERR_CUDA, cudaGetErrorString(e)); }
+    return ZTC_OK;
 }
