@@ -597,10 +597,22 @@ def rdo_workload(dev, lam=30.0):
     return res
 
 
+def bc7_modes(blocks):
+    """Mode of every BC7 block (the lowest set bit of its first byte; 8 = reserved), as an int64 tensor."""
+    import torch
+    b0 = blocks.view(-1, 16)[:, 0].long()
+    mode = torch.full_like(b0, 8)
+    for m in range(7, -1, -1):
+        mode = torch.where(((b0 >> m) & 1) == 1, torch.full_like(b0, m), mode)
+    return mode
+
+
 def refine_workload(args, dev, n=1024, side=256, steps=8, lr=1.0):
     """Config 4: n textures of side^2 (config 0 content, per-texture seed), BC1 and BC7; the encoder's blocks then
     `steps` Adam steps of gradient endpoint refinement through the palette-decode adjoint, accepted per block only
-    if the error drops. Textures are stacked into one image: blocks are independent, so this is n encodes at once."""
+    if the error drops. Textures are stacked into one image: blocks are independent, so this is n encodes at once.
+    BC7's gain is split by the blocks' mode (6, 5, 1); its cost is also timed on an atlas of 64x64 textures, where
+    modes 5 and 1 are a third of the blocks instead of a few per cent."""
     import math
 
     import torch
@@ -608,29 +620,48 @@ def refine_workload(args, dev, n=1024, side=256, steps=8, lr=1.0):
     import zap_b200
     import zap_b200.synth as S
     tex = torch.cat([S.colour_texture(side, side, seed=20000 + k, device=dev) for k in range(n)], 0).contiguous()
-    npix = tex.shape[0] * tex.shape[1]
+    atlas = atlas_texture(2048, 64, 50000, dev, 0)
     res = {"textures": n, "side": side, "adam_steps": steps, "lr": lr}
-    for fmt, name, chans in ((zap_b200.BC1, "bc1", 3), (zap_b200.BC7, "bc7", 4)):
-        out = zap_b200.bc_encode_dev(tex, fmt)
+    psnr = lambda e, nval: 99.0 if e == 0 else 10 * math.log10(255.0 ** 2 * nval / e)  # noqa: E731
+    for fmt, name, chans, img in ((zap_b200.BC1, "bc1", 3, tex), (zap_b200.BC7, "bc7", 4, tex),
+                                  (zap_b200.BC7, "bc7_atlas_of_64x64", 4, atlas)):
+        npix = img.shape[0] * img.shape[1]
+        out = zap_b200.bc_encode_dev(img, fmt)
         base = out.clone()
-        ms_enc = time_device(lambda k: zap_b200.bc_encode_dev(tex, fmt, out=out), 5, 2, 1) / 5
+        ms_enc = time_device(lambda k: zap_b200.bc_encode_dev(img, fmt, out=out), 5, 2, 1) / 5
         work = base.clone()
 
         def refine_step(k):
             work.copy_(base)
-            zap_b200.refine_dev(tex, fmt, work, steps=steps, lr=lr)
+            zap_b200.refine_dev(img, fmt, work, steps=steps, lr=lr)
         ms_ref = time_device(refine_step, 5, 2, 1) / 5
         work.copy_(base)
-        s0, s1 = zap_b200.refine_dev(tex, fmt, work, steps=steps, lr=lr)
+        s0, s1 = zap_b200.refine_dev(img, fmt, work, steps=steps, lr=lr)
         torch.cuda.synchronize()
         e0, e1 = float(s0.double().sum()), float(s1.double().sum())
         nval = npix * chans
-        psnr = lambda e: 99.0 if e == 0 else 10 * math.log10(255.0 ** 2 * nval / e)  # noqa: E731
-        res[name] = {"encode_ms": ms_enc, "encode_Mpix_s": npix / 1e6 / (ms_enc / 1e3), "refine_ms": ms_ref,
-                     "refine_Mpix_s": npix / 1e6 / (ms_ref / 1e3), "psnr_db": psnr(e0), "psnr_refined_db": psnr(e1),
-                     "psnr_gain_db": psnr(e1) - psnr(e0), "blocks_improved": float((s1 < s0).float().mean()),
-                     "cost_vs_encode": ms_ref / ms_enc}
-    del tex
+        r = {"pixels": npix, "encode_ms": ms_enc, "encode_Mpix_s": npix / 1e6 / (ms_enc / 1e3), "refine_ms": ms_ref,
+             "refine_Mpix_s": npix / 1e6 / (ms_ref / 1e3), "psnr_db": psnr(e0, nval), "psnr_refined_db": psnr(e1, nval),
+             "psnr_gain_db": psnr(e1, nval) - psnr(e0, nval), "blocks_improved": float((s1 < s0).float().mean()),
+             "cost_vs_encode": ms_ref / ms_enc}
+        if fmt == zap_b200.BC7:
+            modes = bc7_modes(base)
+            same_mode = bool(torch.equal(modes, bc7_modes(work)))
+            by = {}
+            for m in (6, 5, 1):
+                sel = modes == m
+                cnt = int(sel.sum())
+                if not cnt:
+                    continue
+                a0, a1 = float(s0[sel].double().sum()), float(s1[sel].double().sum())
+                by[f"mode{m}"] = {"blocks": cnt, "share": cnt / modes.numel(), "sse_before": a0, "sse_after": a1,
+                                  "sse_reduction": (a0 - a1) / a0 if a0 else 0.0,
+                                  "blocks_improved": float((s1[sel] < s0[sel]).float().mean()),
+                                  "psnr_gain_db_over_these_blocks": psnr(a1, cnt * 16 * chans) - psnr(a0, cnt * 16 * chans)}
+            r["by_mode"] = by
+            r["modes_kept"] = same_mode
+        res[name] = r
+    del tex, atlas
     torch.cuda.empty_cache()
     return res
 

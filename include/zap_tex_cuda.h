@@ -153,15 +153,21 @@ ZTC_API int zap_tex_cuda_bc_encode_split_dev(zap_tex_cuda_ctx *ctx, const uint8_
                                              void *out, void *stream);
 
 /* ---------------------------------------------------------------- differentiable palette decode, refinement
-   No reference counterpart. With indices held fixed, decoding is linear in the endpoints:
-     decoded[b][i][c] = a_i * e0[c] + (1 - a_i) * e1[c]
-   a_i = {1, 0, 2/3, 1/3}[index] for BC1, 1 - w4(index)/64 for BC7 mode 6; endpoints in 8-bit units, float[b][2][4]
-   (BC1 uses RGB); decoded float[b][16][4]. BC7 blocks in other modes are not covered: they decode to 0 and have
-   zero gradient.
+   No reference counterpart. With indices held fixed, decoding is linear in the endpoints: texel i of subset s,
+   stored channel c, decodes to
+     a_i * E[2s][c] + (1 - a_i) * E[2s+1][c]
+   a_i = {1, 0, 2/3, 1/3}[index] for BC1 (the 4-colour order; zap_tex.h:52-62) and 1 - w(index)/64 for BC7 with the
+   mode's 2-, 3- or 4-bit weights (zap_tex.h:367-417). BC7 covers all eight modes: up to three subsets, separate
+   colour / alpha index sets (modes 4, 5: alpha takes the second set's weight), the rotation (alpha swapped with
+   channel rot - 1 after the interpolation; endpoints are in stored order, texels in decoded order), and modes
+   without alpha bits (alpha decodes to 255, zero gradient); the reserved mode decodes to 0 with zero gradient.
+   Endpoints in 8-bit units: float[b][2][4] for BC1 (RGB used; alpha decodes to 0), float[b][6][4] for BC7
+   (endpoint 2s + k of subset s; unused rows 0); decoded float[b][16][4].
    block_endpoints: the stored endpoints, expanded; palette_adjoint: grad_endpoints = d(sum g . decoded)/d(endpoints).
    refine: per block, `steps` Adam steps (learning rate lr, 8-bit units) on the block MSE through the adjoint,
-   requantise, re-fit indices, keep the new block only if its squared error is lower; optional per-block squared
-   errors before / after (uint32[nblocks], device). Device pointers, asynchronous. */
+   requantise in the block's own mode (BC1 565; BC7 modes 6, 5 and 1, the modes the encoder writes, rotation and
+   partition kept), re-fit the indices, keep the new block only if its squared error is lower; optional per-block
+   squared errors before / after (uint32[nblocks], device). Device pointers, asynchronous. */
 ZTC_API int zap_tex_cuda_block_endpoints_dev(zap_tex_cuda_ctx *ctx, int fmt, const void *blocks, int nblocks, float *endpoints,
                                              void *stream);
 ZTC_API int zap_tex_cuda_palette_decode_dev(zap_tex_cuda_ctx *ctx, int fmt, const void *blocks, int nblocks, const float *endpoints,
@@ -188,8 +194,20 @@ typedef struct zap_tex_cuda_item {
     uint8_t *dst;       /* zap_tex_cuda_batch_item_bytes(w, h, fmt, levels) bytes */
 } zap_tex_cuda_item;
 typedef struct zap_tex_cuda_batch zap_tex_cuda_batch;
-#define ZTC_BATCH_AUTOTUNE 1 /* time each format's kernel at 64/128/256 blocks per CTA on the batch, keep the fastest */
+/* AUTOTUNE: per format class, time on the batch's own levels, one knob at a time, and keep the fastest: CTA size
+   (64/128/256), register cap (tight: the single-image kernels' resident CTAs; loose: fewer CTAs, fewer spills),
+   blocks per tile (1/2/4 CTAs' worth), tile shape (row strip / 2-D tile), and for BC7 the modes-5/1 grid (1 or 2
+   CTAs per SM, or all that fit). zap_tex_cuda_batch_info reports the choices and the timings.
+   Without AUTOTUNE the plan is 128 threads, tight registers, 1 CTA's worth of blocks per tile, row strips, unless
+   the TILES_2D / REGS_LOOSE / TILE_X2 / TILE_X4 / CTA_64 / CTA_256 flags set a knob for every class. */
+#define ZTC_BATCH_AUTOTUNE 1
 #define ZTC_BATCH_NO_GRAPH 2 /* launch the sequence directly instead of capturing it into a CUDA graph */
+#define ZTC_BATCH_TILES_2D 4
+#define ZTC_BATCH_REGS_LOOSE 8
+#define ZTC_BATCH_TILE_X2 16
+#define ZTC_BATCH_TILE_X4 32
+#define ZTC_BATCH_CTA_64 64
+#define ZTC_BATCH_CTA_256 128
 ZTC_API size_t zap_tex_cuda_batch_item_bytes(int w, int h, int fmt, int levels);
 ZTC_API int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *items, int n, int flags,
                                       zap_tex_cuda_batch **out);

@@ -269,32 +269,36 @@ static int bc7_anchor_of(int ns, int part, int s) { return s == 0 ? 0 : ns == 2 
 static int bc7_expand(int v, int n) { v <<= 8 - n; return v | (v >> n); } /* n-bit value -> 8 bits (:375) */
 static int lerp64(int a, int b, int w) { return ((64 - w) * a + w * b + 32) >> 6; }
 
-/* full decoder, all 8 modes; reserved mode decodes to transparent black (:378-417) */
-static void bc7_decode_block(const uint8_t *blk, tx4 out[16]) {
+/* a block's fields (:378-412): mode (8 = reserved), subsets, partition, rotation, whether alpha has its own bits,
+   the expanded 8-bit endpoints, and each texel's subset and colour / alpha interpolation weight (0..64) */
+typedef struct { int mode, ns, part, rot, ab, ep[6][4], subset[16], cw[16], aw[16]; } bc7_fields;
+static int bc7_parse(const uint8_t *blk, bc7_fields *F) {
     int mode = 0;
     while (mode < 8 && !((blk[0] >> mode) & 1)) mode++;
-    if (mode == 8) { memset(out, 0, 64); return; }
+    memset(F, 0, sizeof *F);
+    F->mode = mode;
+    if (mode == 8) return 0;
     const bc7_mode *M = &BC7_MODES[mode];
     bitr r = { blk, mode + 1 };
     int part = (int)get_bits(&r, M->pb), rot = (int)get_bits(&r, M->rb), isb = (int)get_bits(&r, M->isb);
-    int ne = 2 * M->ns, ep[6][4], cb = M->cb, ab = M->ab;
-    for (int c = 0; c < 3; c++) for (int e = 0; e < ne; e++) ep[e][c] = (int)get_bits(&r, cb);
-    for (int e = 0; e < ne; e++) ep[e][3] = ab ? (int)get_bits(&r, ab) : 255;
+    int ne = 2 * M->ns, cb = M->cb, ab = M->ab;
+    for (int c = 0; c < 3; c++) for (int e = 0; e < ne; e++) F->ep[e][c] = (int)get_bits(&r, cb);
+    for (int e = 0; e < ne; e++) F->ep[e][3] = ab ? (int)get_bits(&r, ab) : 255;
     if (M->epb || M->spb) {
         for (int e = 0; e < ne; e++) {
             if (!M->epb && (e & 1)) continue; /* shared p-bit: read once per subset */
             int p = (int)get_bits(&r, 1), last = M->epb ? e : e + 1;
             for (int k = e; k <= last; k++) {
-                for (int c = 0; c < 3; c++) ep[k][c] = (ep[k][c] << 1) | p;
-                if (ab) ep[k][3] = (ep[k][3] << 1) | p;
+                for (int c = 0; c < 3; c++) F->ep[k][c] = (F->ep[k][c] << 1) | p;
+                if (ab) F->ep[k][3] = (F->ep[k][3] << 1) | p;
             }
         }
         cb++;
         if (ab) ab++;
     }
     for (int e = 0; e < ne; e++) {
-        for (int c = 0; c < 3; c++) ep[e][c] = bc7_expand(ep[e][c], cb);
-        if (ab) ep[e][3] = bc7_expand(ep[e][3], ab);
+        for (int c = 0; c < 3; c++) F->ep[e][c] = bc7_expand(F->ep[e][c], cb);
+        if (ab) F->ep[e][3] = bc7_expand(F->ep[e][3], ab);
     }
     int i1[16], i2[16] = { 0 };
     for (int i = 0; i < 16; i++) {
@@ -303,12 +307,23 @@ static void bc7_decode_block(const uint8_t *blk, tx4 out[16]) {
     }
     if (M->ib2) for (int i = 0; i < 16; i++) i2[i] = (int)get_bits(&r, M->ib2 - (i == 0));
     for (int i = 0; i < 16; i++) {
-        int s = bc7_subset_of(M->ns, part, i);
-        int cw = (M->ib2 && isb) ? bc7_weight(M->ib2, i2[i]) : bc7_weight(M->ib, i1[i]);
-        int aw = !M->ib2 ? cw : isb ? bc7_weight(M->ib, i1[i]) : bc7_weight(M->ib2, i2[i]);
-        for (int c = 0; c < 3; c++) out[i][c] = (uint8_t)lerp64(ep[2 * s][c], ep[2 * s + 1][c], cw);
-        out[i][3] = (uint8_t)lerp64(ep[2 * s][3], ep[2 * s + 1][3], aw);
-        if (rot) { uint8_t s2 = out[i][3]; out[i][3] = out[i][rot - 1]; out[i][rot - 1] = s2; }
+        F->subset[i] = bc7_subset_of(M->ns, part, i);
+        F->cw[i] = (M->ib2 && isb) ? bc7_weight(M->ib2, i2[i]) : bc7_weight(M->ib, i1[i]);
+        F->aw[i] = !M->ib2 ? F->cw[i] : isb ? bc7_weight(M->ib, i1[i]) : bc7_weight(M->ib2, i2[i]);
+    }
+    F->ns = M->ns; F->part = part; F->rot = rot; F->ab = M->ab > 0;
+    return 1;
+}
+
+/* full decoder, all 8 modes; reserved mode decodes to transparent black (:378-417) */
+static void bc7_decode_block(const uint8_t *blk, tx4 out[16]) {
+    bc7_fields F;
+    if (!bc7_parse(blk, &F)) { memset(out, 0, 64); return; }
+    for (int i = 0; i < 16; i++) {
+        int s = F.subset[i];
+        for (int c = 0; c < 3; c++) out[i][c] = (uint8_t)lerp64(F.ep[2 * s][c], F.ep[2 * s + 1][c], F.cw[i]);
+        out[i][3] = (uint8_t)lerp64(F.ep[2 * s][3], F.ep[2 * s + 1][3], F.aw[i]);
+        if (F.rot) { uint8_t s2 = out[i][3]; out[i][3] = out[i][F.rot - 1]; out[i][F.rot - 1] = s2; }
     }
 }
 static int bc7_decoded_sse(const tx4 t[16], const uint8_t *blk) { /* :710-716 */
@@ -983,6 +998,17 @@ static void bc_regroup(const uint8_t *in, uint8_t *out, size_t n, int fmt, int t
 }
 void zo_bc_split(const void *bc, size_t n, int fmt, void *out) { bc_regroup((const uint8_t *)bc, (uint8_t *)out, n, fmt, 1); }
 void zo_bc_merge(const void *planes, size_t n, int fmt, void *out) { bc_regroup((const uint8_t *)planes, (uint8_t *)out, n, fmt, 0); }
+
+int zo_bc7_fields(const void *blk, int info[5], int ep[6][4], int subset[16], int cw[16], int aw[16]) {
+    bc7_fields F;
+    int ok = bc7_parse((const uint8_t *)blk, &F);
+    info[0] = F.mode; info[1] = F.ns; info[2] = F.part; info[3] = F.rot; info[4] = F.ab;
+    memcpy(ep, F.ep, sizeof F.ep);
+    memcpy(subset, F.subset, sizeof F.subset);
+    memcpy(cw, F.cw, sizeof F.cw);
+    memcpy(aw, F.aw, sizeof F.aw);
+    return ok;
+}
 
 void zo_bc7_mode_hist(const void *bc, size_t nblocks, int hist[9]) {
     const uint8_t *b = (const uint8_t *)bc;

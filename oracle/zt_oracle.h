@@ -44,6 +44,12 @@ void zo_srgb_tables(float lin[256], float thr[255]);
 /* ISE put then get of n values in range `range` (0..20); returns bits written, or -1 if the read-back differs */
 int zo_ise_roundtrip(int range, int n, const int *v, int *got);
 
+/* the fields of one BC7 block, all modes (zap_tex.h:378-412): info = {mode (8 = reserved), subsets, partition,
+   rotation, alpha has own bits}, expanded 8-bit endpoints (endpoint 2s + k of subset s), each texel's subset and its
+   colour / alpha interpolation weight (0..64); returns 0 for the reserved mode. The decode is
+   lerp64(ep[2s][c], ep[2s+1][c], w), then alpha swapped with channel rot - 1 when rot > 0. */
+int zo_bc7_fields(const void *blk, int info[5], int ep[6][4], int subset[16], int cw[16], int aw[16]);
+
 /* per-block BC7 mode histogram of an encoded BC7 image (modes 0..7, 8 = reserved) */
 void zo_bc7_mode_hist(const void *bc, size_t nblocks, int hist[9]);
 

@@ -64,6 +64,7 @@ class Oracle:
             self._fn("dds_header", [i, i, i, i, i, vp], sz)
             self._fn("astc_header", [i, i, vp], None)
             self._fn("tex_file", [vp, i, i, sz, i, f, i, i, vp], sz)
+            self._fn("bc7_fields", [vp, vp, vp, vp, vp, vp], C.c_int)
         else:
             self._fn("astc_part", [i, i, i, i], C.c_int)
             self._fn("srgb_lin", [], C.POINTER(C.c_float))
@@ -108,6 +109,17 @@ class Oracle:
         else:
             self._astc_encode(img.ctypes.data, w, h, w * 4, out.ctypes.data)
         return out
+
+    def bc7_fields(self, blk):
+        """One BC7 block's fields (restatement only): mode, subsets, partition, rotation, alpha bits, expanded
+        endpoints [6][4] (endpoint 2s + k of subset s), per-texel subset and colour / alpha weights (0..64)."""
+        blk = np.ascontiguousarray(blk, dtype=np.uint8)
+        info = np.zeros(5, np.int32)
+        ep = np.zeros((6, 4), np.int32)
+        sub, cw, aw = np.zeros(16, np.int32), np.zeros(16, np.int32), np.zeros(16, np.int32)
+        self._bc7_fields(blk.ctypes.data, info.ctypes.data, ep.ctypes.data, sub.ctypes.data, cw.ctypes.data, aw.ctypes.data)
+        return {"mode": int(info[0]), "ns": int(info[1]), "part": int(info[2]), "rot": int(info[3]), "ab": int(info[4]),
+                "ep": ep.tolist(), "subset": sub.tolist(), "cw": cw.tolist(), "aw": aw.tolist()}
 
     # ---- the CLI's containers (zap.c:309-355; restatement only)
     def dds_header(self, w, h, fmt, mips, srgb):

@@ -29,8 +29,13 @@ def _check_item(batch, i, ref, srgb):
         assert np.array_equal(got, exp), (i, fmt, tex.shape, lv, int(np.sum(got != exp)))
 
 
-@pytest.mark.parametrize("autotune,graph", [(False, True), (True, True), (False, False)])
-def test_batch_matches_oracle(cuda_lib, autotune, graph):
+@pytest.mark.parametrize("autotune,graph,plan", [(False, True, ()), (True, True, ()), (False, False, ()),
+                                                 (False, True, ("tiles_2d", "regs_loose", "tile_x4", "cta_64")),
+                                                 (False, True, ("tiles_2d", "tile_x2", "cta_256")),
+                                                 (False, True, ("regs_loose", "tile_x2"))])
+def test_batch_matches_oracle(cuda_lib, autotune, graph, plan):
+    """Every launch plan the autotuner can pick (CTA size, register cap, blocks per tile, strip or 2-D tiles) gives the
+    reference's bytes."""
     import torch
     ref = oracle_lib.best()
     sizes = [(1, 1), (3, 2), (5, 3), (17, 9), (64, 64), (128, 32), (96, 200), (256, 256), (300, 131), (33, 257), (512, 128), (7, 70)]
@@ -39,13 +44,19 @@ def test_batch_matches_oracle(cuda_lib, autotune, graph):
     srgb = [k % 3 != 0 for k in range(len(sizes))]
     levels = [0] * len(sizes)
     levels[4] = 2  # a partial chain
-    b = cuda_lib.Batch(texs, fmts, srgb=srgb, levels=levels, autotune=autotune, graph=graph)
+    b = cuda_lib.Batch(texs, fmts, srgb=srgb, levels=levels, autotune=autotune, graph=graph, plan=plan)
     b.run()
     torch.cuda.synchronize()
     for i in range(len(texs)):
         _check_item(b, i, ref, srgb[i])
+    info = b.info()
     if autotune:
-        assert "cta" in b.info()
+        for knob in ("cta", "regs", "blocks_per_tile", "shape", "hard_grid", "tuned_ms"):
+            assert knob in info, (knob, info)
+    if "tiles_2d" in plan:
+        assert "shape 2d_" in info
+    if "regs_loose" in plan:
+        assert "regs loose" in info
     b.close()
 
 

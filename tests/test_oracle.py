@@ -218,6 +218,38 @@ def test_astc_decode_matches_reference_live(oracle, reference):
     assert np.array_equal(oracle.astc_decode(bc, 95, 77), reference.astc_decode(bc, 95, 77))
 
 
+def test_bc7_decode_all_modes_matches_reference_live(oracle, reference):
+    """The port's BC7 decoder on arbitrary blocks: every mode (each block's lowest set bit of byte 0 picks it), every
+    partition, rotation and index selector, and the reserved mode."""
+    rng = np.random.default_rng(15)
+    bc = rng.integers(0, 256, (9 * 512, 16), dtype=np.uint8)
+    for m in range(9):  # mode m: bits below m clear, bit m set (m = 8: byte 0 zero, the reserved mode)
+        rows = bc[m::9]
+        rows[:, 0] = 0 if m == 8 else ((rows[:, 0] >> (m + 1)) << (m + 1)) | (1 << m)
+    w, h = 4 * 64, 4 * (9 * 512 // 64)
+    assert np.array_equal(oracle.bc_decode(bc.reshape(-1), w, h, BC7), reference.bc_decode(bc.reshape(-1), w, h, BC7))
+
+
+def test_bc7_fields_rebuild_the_decoder_output(oracle):
+    """zo_bc7_fields (the linear form the adjoint tests use) gives back the decoder's texels on every mode."""
+    rng = np.random.default_rng(16)
+    bc = rng.integers(0, 256, (8 * 64, 16), dtype=np.uint8)
+    for m in range(8):
+        rows = bc[m::8]
+        rows[:, 0] = ((rows[:, 0] >> (m + 1)) << (m + 1)) | (1 << m)
+    dec = oracle.bc_decode(bc.reshape(-1), 4 * 8, 4 * 64, BC7).reshape(64, 4, 8, 4, 4).transpose(0, 2, 1, 3, 4).reshape(-1, 16, 4)
+    for k in range(bc.shape[0]):
+        f = oracle.bc7_fields(bc[k])
+        assert f["mode"] == k % 8
+        ep, s = f["ep"], f["subset"]
+        for i in range(16):
+            px = [((64 - f["cw"][i]) * ep[2 * s[i]][c] + f["cw"][i] * ep[2 * s[i] + 1][c] + 32) >> 6 for c in range(3)]
+            px.append(((64 - f["aw"][i]) * ep[2 * s[i]][3] + f["aw"][i] * ep[2 * s[i] + 1][3] + 32) >> 6)
+            if f["rot"]:
+                px[3], px[f["rot"] - 1] = px[f["rot"] - 1], px[3]
+            assert px == list(dec[k, i]), (k, i)
+
+
 # ---------------------------------------------------------------- rate-distortion mode (zap_tex.h:223-306, :786-815)
 @pytest.mark.parametrize("rdo", [10.0, 30.0, 300.0])
 def test_rdo_port_matches_reference_live(oracle, reference, rdo):

@@ -314,17 +314,22 @@ def astc_decode(bc, w, h, ctx=None):
     return out
 
 
+def endpoint_rows(fmt):
+    """Endpoints per block in the differentiable decode: BC1 2 (RGB used), BC7 6 (endpoint 2s + k of subset s)."""
+    return 2 if fmt == BC1 else 6
+
+
 def block_endpoints_dev(blocks, fmt, stream=None, ctx=None):
-    """Stored endpoints of BC1 / BC7-mode-6 blocks, expanded to 8-bit units: float32 [nblocks, 2, 4]."""
+    """Stored endpoints of BC1 / BC7 blocks, expanded to 8-bit units: float32 [nblocks, endpoint_rows(fmt), 4]."""
     import torch
     n = blocks.numel() // block_bytes(fmt)
-    out = torch.empty((n, 2, 4), dtype=torch.float32, device=blocks.device)
+    out = torch.empty((n, endpoint_rows(fmt), 4), dtype=torch.float32, device=blocks.device)
     check(load().zap_tex_cuda_block_endpoints_dev(ctx, fmt, blocks.data_ptr(), n, out.data_ptr(), _stream(stream)), "block_endpoints_dev")
     return out
 
 
 def palette_decode_dev(blocks, fmt, endpoints, stream=None, ctx=None):
-    """Linear palette decode with the blocks' indices held fixed: endpoints [n, 2, 4] -> texels float32 [n, 16, 4]."""
+    """Linear palette decode with the blocks' indices held fixed: endpoints [n, rows, 4] -> texels float32 [n, 16, 4]."""
     import torch
     n = endpoints.shape[0]
     out = torch.empty((n, 16, 4), dtype=torch.float32, device=endpoints.device)
@@ -334,10 +339,10 @@ def palette_decode_dev(blocks, fmt, endpoints, stream=None, ctx=None):
 
 
 def palette_adjoint_dev(blocks, fmt, grad_decoded, stream=None, ctx=None):
-    """Adjoint of palette_decode_dev: gradient on decoded texels [n, 16, 4] -> gradient on endpoints [n, 2, 4]."""
+    """Adjoint of palette_decode_dev: gradient on decoded texels [n, 16, 4] -> gradient on endpoints [n, rows, 4]."""
     import torch
     n = grad_decoded.shape[0]
-    out = torch.empty((n, 2, 4), dtype=torch.float32, device=grad_decoded.device)
+    out = torch.empty((n, endpoint_rows(fmt), 4), dtype=torch.float32, device=grad_decoded.device)
     check(load().zap_tex_cuda_palette_adjoint_dev(ctx, fmt, blocks.data_ptr(), n, grad_decoded.contiguous().data_ptr(), out.data_ptr(),
                                                   _stream(stream)), "palette_adjoint_dev")
     return out
@@ -367,7 +372,10 @@ class Batch:
     textures: HxWx4 uint8 CUDA tensors (level 0); formats / srgb / levels: one per texture (levels 0 = full chain).
     After run(), outputs[i] holds texture i's levels concatenated, largest first (zap_bc_size bytes per level)."""
 
-    def __init__(self, textures, formats, srgb=None, levels=None, autotune=False, graph=True, ctx=None):
+    PLAN_FLAGS = {"tiles_2d": 4, "regs_loose": 8, "tile_x2": 16, "tile_x4": 32, "cta_64": 64, "cta_256": 128}
+
+    def __init__(self, textures, formats, srgb=None, levels=None, autotune=False, graph=True, ctx=None, plan=()):
+        """plan: names from PLAN_FLAGS that fix a launch knob for every format class (without autotune)."""
         import torch
         n = len(textures)
         srgb = [1] * n if srgb is None else list(srgb)
@@ -385,6 +393,8 @@ class Batch:
             items[i] = _Item(t.data_ptr(), w, h, stride, self.formats[i], int(srgb[i]), int(levels[i]), out.data_ptr())
         self._items = items
         flags = (1 if autotune else 0) | (0 if graph else 2)
+        for name in plan:
+            flags |= self.PLAN_FLAGS[name]
         handle = C.c_void_p()
         check(lib.zap_tex_cuda_batch_create(ctx, items, n, flags, C.byref(handle)), "batch_create")
         self._h = handle

@@ -1,15 +1,23 @@
 // adjoint.cu - differentiable palette decode and gradient endpoint refinement (no reference counterpart).
 //
-// With a block's indices held fixed, the BCn palette decode is linear in the endpoints:
-//   decoded_i = a_i * e0 + (1 - a_i) * e1
-// with a_i = {1, 0, 2/3, 1/3}[idx_i] for BC1 (4-colour order) and a_i = 1 - w4(idx_i) / 64 for BC7 mode 6
-// (the continuous form of the integer palettes of zap_tex.h:52-62 and :538-542; endpoints in 8-bit units).
-// Its adjoint maps an upstream gradient on the decoded texels to the endpoints:
-//   dL/de0 = sum_i a_i g_i,   dL/de1 = sum_i (1 - a_i) g_i.
-// zap_tex_cuda_refine_dev runs, per block, 8 Adam steps on the block's MSE through that adjoint, requantises the
-// endpoints (565 for BC1; 7 bits + best p-bit per endpoint for BC7 mode 6), re-fits the indices, and keeps the new
-// block only if its true squared error is lower than the encoder's. BC7 blocks in modes other than 6 are left as
-// they are (their adjoint is reported as zero).
+// With a block's indices held fixed, the BCn palette decode is linear in the endpoints. Texel i of subset s,
+// stored channel c, decodes to
+//   a_i * E[2s][c] + (1 - a_i) * E[2s+1][c]
+// the continuous form of the integer palettes (zap_tex.h:52-62 for BC1, a_i = {1, 0, 2/3, 1/3}[idx] in 4-colour
+// order; :367-417 for BC7, a_i = 1 - w(idx) / 64 with the mode's 2-, 3- or 4-bit weights). BC7 covers every mode:
+// up to three subsets (endpoint 2s + k of subset s), mode 4/5's separate colour and alpha index sets (the alpha
+// weight is the second set's), the rotation that swaps alpha with one colour channel after the interpolation, and
+// the modes without alpha bits, whose alpha decodes to 255 whatever the endpoints are (zero gradient).
+// Endpoints are in 8-bit units: float[b][2][4] for BC1 (RGB used), float[b][6][4] for BC7, in stored channel order
+// (before the rotation), texels in decoded order. Its adjoint maps an upstream gradient on the decoded texels to
+// the endpoints: dL/dE[2s][c] = sum_i a_i g_i,  dL/dE[2s+1][c] = sum_i (1 - a_i) g_i over the texels of subset s.
+//
+// zap_tex_cuda_refine_dev runs, per block, Adam steps on the block's MSE through that adjoint, requantises the
+// endpoints in the block's own mode (BC1 565; BC7 mode 6: 7 bits + a p-bit per endpoint; mode 5: 7-bit colour and
+// 8-bit alpha; mode 1: 6 bits + a p-bit shared per subset), re-fits the indices (anchor indices made valid by
+// swapping a subset's endpoints, which leaves every decoded value unchanged because w(n-1-j) = 64 - w(j)), and keeps
+// the new block only if its true squared error is lower than the encoder's. The encoder writes BC7 modes 6, 5 and 1
+// only (zap_tex.h:755-784); blocks of other modes are left as they are.
 #include <string>
 
 #include "../../include/zap_tex_cuda.h"
@@ -19,98 +27,124 @@
 
 namespace ztc {
 
-// per-texel weight of endpoint 0 and channel count; returns false for blocks the adjoint does not cover
-ZTC_DEV bool block_weights(int fmt, const uint8_t *blk, float a[16], int &nc) {
+ZTC_DEV int endpoint_floats(int fmt) { return fmt == ZTC_FMT_BC1 ? 8 : 24; }
+
+// A block's linear form: per texel the weight of the subset's first endpoint for the colour channels (a) and for
+// alpha (aa), the subset (bit i of `s1`: subset 1; `s2`: subset 2), the rotation, and which channels the endpoints
+// decide (nc: BC1 3, BC7 4; alpha_fixed: BC7 alpha without bits, 255).
+struct LinBlock {
+    float a[16], aa[16];
+    uint32_t s1, s2;
+    int rot, nc, mode;
+    bool covered, alpha_fixed;
+};
+
+ZTC_DEV void linear_form(int fmt, const uint8_t *blk, LinBlock &L, float e[6][4]) {
+    L.s1 = L.s2 = 0u;
+    L.rot = 0;
+    L.alpha_fixed = false;
     if (fmt == ZTC_FMT_BC1) {
         uint2 v = *(const uint2 *)blk;
         uint32_t c0 = v.x & 0xFFFFu, c1 = v.x >> 16;
-        nc = 3;
+        L.nc = 3; L.mode = 0; L.covered = true;
         #pragma unroll
         for (int i = 0; i < 16; i++) {
             uint32_t k = (v.y >> (2 * i)) & 3u;
             if (c0 <= c1) k = k == 1 ? 1u : 0u;  // solid / 3-colour blocks: our encoder only emits index 0 there
-            a[i] = k == 0 ? 1.0f : k == 1 ? 0.0f : k == 2 ? 2.0f / 3.0f : 1.0f / 3.0f;
+            L.a[i] = L.aa[i] = k == 0 ? 1.0f : k == 1 ? 0.0f : k == 2 ? 2.0f / 3.0f : 1.0f / 3.0f;
         }
-        return true;
-    }
-    uint4 v = *(const uint4 *)blk;
-    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-    nc = 4;
-    if ((w[0] & 0x7Fu) != 0x40u) {  // not mode 6
-        #pragma unroll
-        for (int i = 0; i < 16; i++) a[i] = 0.0f;
-        return false;
-    }
-    #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        int idx = i == 0 ? (int)get_bits128(w, 65, 3) : (int)get_bits128(w, 68 + 4 * (i - 1), 4);
-        a[i] = 1.0f - (float)w4(idx) / 64.0f;
-    }
-    return true;
-}
-
-// expanded 8-bit endpoints of a block as floats [2][4]
-ZTC_DEV void block_endpoints(int fmt, const uint8_t *blk, float e[2][4]) {
-    if (fmt == ZTC_FMT_BC1) {
-        uint2 v = *(const uint2 *)blk;
         for (int k = 0; k < 2; k++) {
-            uint32_t c = k ? (v.x >> 16) : (v.x & 0xFFFFu);
+            uint32_t c = k ? c1 : c0;
             int R = (c >> 11) & 31, G = (c >> 5) & 63, B = c & 31;
             e[k][0] = (float)((R << 3) | (R >> 2)); e[k][1] = (float)((G << 2) | (G >> 4)); e[k][2] = (float)((B << 3) | (B >> 2));
             e[k][3] = 255.0f;
         }
+        for (int k = 2; k < 6; k++) for (int c = 0; c < 4; c++) e[k][c] = 0.0f;
         return;
     }
     uint4 v = *(const uint4 *)blk;
     const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-    if ((w[0] & 0x7Fu) != 0x40u) {
-        for (int k = 0; k < 2; k++) for (int c = 0; c < 4; c++) e[k][c] = 0.0f;
+    dec::Bc7Fields F;
+    L.nc = 4;
+    L.covered = dec::bc7_parse(w, F);
+    L.mode = F.mode;
+    if (!L.covered) {  // reserved mode: decodes to 0, zero gradient
+        for (int i = 0; i < 16; i++) L.a[i] = L.aa[i] = 0.0f;
+        for (int k = 0; k < 6; k++) for (int c = 0; c < 4; c++) e[k][c] = 0.0f;
         return;
     }
-    for (int c = 0; c < 4; c++)
-        for (int k = 0; k < 2; k++) {
-            int q = (int)get_bits128(w, 7 + 14 * c + 7 * k, 7), p = (int)get_bits128(w, 63 + k, 1);
-            e[k][c] = (float)((q << 1) | p);
-        }
+    L.rot = F.rot;
+    L.alpha_fixed = !F.ab;
+    for (int i = 0; i < 16; i++) {
+        L.a[i] = 1.0f - (float)F.cw[i] / 64.0f;
+        L.aa[i] = 1.0f - (float)F.aw[i] / 64.0f;
+        L.s1 |= (uint32_t)(F.subset[i] == 1) << i;
+        L.s2 |= (uint32_t)(F.subset[i] == 2) << i;
+    }
+    for (int k = 0; k < 6; k++) for (int c = 0; c < 4; c++) e[k][c] = (float)F.ep[k][c];
 }
+
+// stored channel of decoded channel c (the rotation swaps alpha with channel rot - 1 after the interpolation)
+ZTC_DEV int stored_channel(int rot, int c) { return rot == 0 ? c : c == 3 ? rot - 1 : c == rot - 1 ? 3 : c; }
+ZTC_DEV int subset_of_texel(const LinBlock &L, int i) { return ((L.s1 >> i) & 1u) ? 1 : ((L.s2 >> i) & 1u) ? 2 : 0; }
 
 __global__ void endpoints_kernel(int fmt, const uint8_t *__restrict__ blocks, int n, float *__restrict__ ep) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= n) return;
-    float e[2][4];
-    block_endpoints(fmt, blocks + (size_t)b * (fmt == ZTC_FMT_BC1 ? 8 : 16), e);
-    for (int k = 0; k < 2; k++) for (int c = 0; c < 4; c++) ep[(size_t)b * 8 + 4 * k + c] = e[k][c];
+    LinBlock L;
+    float e[6][4];
+    linear_form(fmt, blocks + (size_t)b * (fmt == ZTC_FMT_BC1 ? 8 : 16), L, e);
+    const int nf = endpoint_floats(fmt);
+    for (int k = 0; k < nf / 4; k++) for (int c = 0; c < 4; c++) ep[(size_t)b * nf + 4 * k + c] = e[k][c];
 }
 
 __global__ void decode_kernel(int fmt, const uint8_t *__restrict__ blocks, int n, const float *__restrict__ ep, float *__restrict__ out) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= n) return;
-    float a[16];
-    int nc;
-    const bool covered = block_weights(fmt, blocks + (size_t)b * (fmt == ZTC_FMT_BC1 ? 8 : 16), a, nc);
-    const float *e = ep + (size_t)b * 8;
-    for (int i = 0; i < 16; i++)
-        for (int c = 0; c < 4; c++)
-            out[((size_t)b * 16 + i) * 4 + c] = (covered && c < nc) ? a[i] * e[c] + (1.0f - a[i]) * e[4 + c] : 0.0f;
+    LinBlock L;
+    float e[6][4];
+    linear_form(fmt, blocks + (size_t)b * (fmt == ZTC_FMT_BC1 ? 8 : 16), L, e);
+    const int nf = endpoint_floats(fmt);
+    const float *E = ep + (size_t)b * nf;
+    for (int i = 0; i < 16; i++) {
+        const int s = subset_of_texel(L, i);
+        for (int c = 0; c < 4; c++) {
+            const int sc = stored_channel(L.rot, c);
+            float d = 0.0f;
+            if (L.covered && c < L.nc) {
+                if (sc == 3 && L.alpha_fixed) d = 255.0f;
+                else {
+                    const float a = sc == 3 ? L.aa[i] : L.a[i];
+                    d = a * E[4 * (2 * s) + sc] + (1.0f - a) * E[4 * (2 * s + 1) + sc];
+                }
+            }
+            out[((size_t)b * 16 + i) * 4 + c] = d;
+        }
+    }
 }
 
 __global__ void adjoint_kernel(int fmt, const uint8_t *__restrict__ blocks, int n, const float *__restrict__ g, float *__restrict__ ge) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= n) return;
-    float a[16];
-    int nc;
-    const bool covered = block_weights(fmt, blocks + (size_t)b * (fmt == ZTC_FMT_BC1 ? 8 : 16), a, nc);
-    float g0[4] = {0, 0, 0, 0}, g1[4] = {0, 0, 0, 0};
-    for (int i = 0; i < 16; i++)
+    LinBlock L;
+    float e[6][4], G[6][4];
+    linear_form(fmt, blocks + (size_t)b * (fmt == ZTC_FMT_BC1 ? 8 : 16), L, e);
+    for (int k = 0; k < 6; k++) for (int c = 0; c < 4; c++) G[k][c] = 0.0f;
+    for (int i = 0; i < 16; i++) {
+        const int s = subset_of_texel(L, i);
         for (int c = 0; c < 4; c++) {
-            float gi = (covered && c < nc) ? g[((size_t)b * 16 + i) * 4 + c] : 0.0f;
-            g0[c] += a[i] * gi;
-            g1[c] += (1.0f - a[i]) * gi;
+            const int sc = stored_channel(L.rot, c);
+            if (!L.covered || c >= L.nc || (sc == 3 && L.alpha_fixed)) continue;
+            const float gi = g[((size_t)b * 16 + i) * 4 + c], a = sc == 3 ? L.aa[i] : L.a[i];
+            G[2 * s][sc] += a * gi;
+            G[2 * s + 1][sc] += (1.0f - a) * gi;
         }
-    for (int c = 0; c < 4; c++) { ge[(size_t)b * 8 + c] = g0[c]; ge[(size_t)b * 8 + 4 + c] = g1[c]; }
+    }
+    const int nf = endpoint_floats(fmt);
+    for (int k = 0; k < nf / 4; k++) for (int c = 0; c < 4; c++) ge[(size_t)b * nf + 4 * k + c] = G[k][c];
 }
 
-// ---------------------------------------------------------------- refinement
+// ---------------------------------------------------------------- refinement: requantise and re-fit per mode
 ZTC_DEV uint32_t q565(float r, float g, float b) {  // zap_tex.h:45-49
     int R = f2i_x86(r * 31.0f / 255.0f + 0.5f), G = f2i_x86(g * 63.0f / 255.0f + 0.5f), B = f2i_x86(b * 31.0f / 255.0f + 0.5f);
     return ((uint32_t)clampi(R, 0, 31) << 11) | ((uint32_t)clampi(G, 0, 63) << 5) | (uint32_t)clampi(B, 0, 31);
@@ -145,75 +179,187 @@ ZTC_DEV int bc1_block_sse(const uint32_t t[16], uint32_t c0, uint32_t c1, uint2 
     blk = make_uint2(c0 | (c1 << 16), bits);
     return err;
 }
-// BC7 mode-6 block for expanded endpoints (7 bits + p-bit chosen per endpoint), indices re-fitted with texel 0
-// limited to 0..7 so no swap is needed, and its SSE
-ZTC_DEV int mode6_block_sse(const uint32_t t[16], const float e[2][4], uint4 &out) {
+
+// nearest n-bit code (no p-bit) whose expansion is closest to v: the rounded guess and its neighbours
+ZTC_DEV int quant_plain(float v, int n) {
+    const int top = (1 << n) - 1;
+    const int g = f2i_x86(v * (float)top / 255.0f + 0.5f);
+    int bq = 0;
+    float bd = 3.0e38f;
+    for (int k = 0; k < 3; k++) {
+        const int q = clampi(around(g, k), 0, top);
+        const float d = fabsf((float)expand_bits(q, n) - v);
+        if (d < bd) { bd = d; bq = q; }
+    }
+    return bq;
+}
+// nearest (n-1)-bit code q with a fixed p-bit p, whose n-bit value (q << 1) | p expands closest to v; its distance
+ZTC_DEV int quant_pbit(float v, int n, int p, float &dist) {
+    const int top = (1 << (n - 1)) - 1;
+    const int g = f2i_x86(((v * (float)((1 << n) - 1) / 255.0f) - (float)p) / 2.0f + 0.5f);
+    int bq = 0;
+    float bd = 3.0e38f;
+    for (int k = 0; k < 3; k++) {
+        const int q = clampi(around(g, k), 0, top);
+        const float d = fabsf((float)expand_bits((q << 1) | p, n) - v);
+        if (d < bd) { bd = d; bq = q; }
+    }
+    dist = bd;
+    return bq;
+}
+
+// BC7 mode 6 (zap_tex.h:520-527 layout): 7 bits + a p-bit per endpoint, 4-bit indices, anchor texel 0
+ZTC_DEV int mode6_block_sse(const uint32_t t[16], const float e[6][4], uint4 &out) {
     int q[2][4], pb[2], x[2][4];
     for (int k = 0; k < 2; k++) {
-        int best = 1 << 30;
+        float best = 3.0e38f;
         for (int p = 0; p < 2; p++) {
-            int qq[4], xx[4], err = 0;
-            for (int c = 0; c < 4; c++) {
-                int g = clampi(f2i_x86((e[k][c] - (float)p) / 2.0f + 0.5f), 0, 127);
-                qq[c] = g; xx[c] = (g << 1) | p;
-                int d = xx[c] - f2i_x86(e[k][c] + 0.5f);
-                err += d * d;
-            }
-            if (err < best) { best = err; pb[k] = p; for (int c = 0; c < 4; c++) { q[k][c] = qq[c]; x[k][c] = xx[c]; } }
+            int qq[4];
+            float err = 0.0f, d;
+            for (int c = 0; c < 4; c++) { qq[c] = quant_pbit(e[k][c], 8, p, d); err += d * d; }
+            if (err < best) { best = err; pb[k] = p; for (int c = 0; c < 4; c++) q[k][c] = qq[c]; }
         }
+        for (int c = 0; c < 4; c++) x[k][c] = expand_bits((q[k][c] << 1) | pb[k], 8);
     }
-    uint32_t pal[16];
-    for (int j = 0; j < 16; j++) {
-        uint32_t v = 0;
-        for (int c = 0; c < 4; c++) v |= (uint32_t)lerp64(x[0][c], x[1][c], w4(j)) << (8 * c);
-        pal[j] = v;
-    }
-    int err = 0;
-    uint64_t idx = 0;
+    int idx[16], err = 0;
     for (int i = 0; i < 16; i++) {
         int bj = 0, be = 1 << 30;
-        for (int j = 0; j < (i ? 16 : 8); j++) {
+        for (int j = 0; j < 16; j++) {
             int d = 0;
-            for (int c = 0; c < 4; c++) { int y = (int)chan(t[i], c) - (int)chan(pal[j], c); d += y * y; }
+            for (int c = 0; c < 4; c++) { int y = (int)chan(t[i], c) - lerp64(x[0][c], x[1][c], w4(j)); d += y * y; }
             if (d < be) { be = d; bj = j; }
         }
-        idx |= (uint64_t)bj << (4 * i);
+        idx[i] = bj;
         err += be;
+    }
+    if (idx[0] >= 8) {  // anchor: swap the endpoints, mirror the indices (decoded values unchanged)
+        for (int c = 0; c < 4; c++) { int s = q[0][c]; q[0][c] = q[1][c]; q[1][c] = s; }
+        int s = pb[0]; pb[0] = pb[1]; pb[1] = s;
+        for (int i = 0; i < 16; i++) idx[i] = 15 - idx[i];
     }
     Bits128 o;
     o.put(1u << 6, 7);
     for (int c = 0; c < 4; c++) { o.put((uint32_t)q[0][c], 7); o.put((uint32_t)q[1][c], 7); }
     o.put((uint32_t)pb[0], 1); o.put((uint32_t)pb[1], 1);
-    o.put((uint32_t)(idx & 7u), 3);
-    for (int i = 1; i < 16; i++) o.put((uint32_t)((idx >> (4 * i)) & 15u), 4);
+    o.put((uint32_t)idx[0], 3);
+    for (int i = 1; i < 16; i++) o.put((uint32_t)idx[i], 4);
     out = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
     return err;
 }
-// squared error of the block as stored (the decoder's integer palette)
-ZTC_DEV int stored_sse(int fmt, const uint32_t t[16], const uint8_t *blk) {
-    if (fmt == ZTC_FMT_BC1) {
-        uint2 v = *(const uint2 *)blk;
-        uint32_t c0 = v.x & 0xFFFFu, c1 = v.x >> 16;
-        int pal[4][3];
-        bc1_palette(c0, c1, pal);
-        if (c0 <= c1) for (int c = 0; c < 3; c++) { pal[2][c] = (pal[0][c] + pal[1][c] + 1) / 2; pal[3][c] = 0; }
-        int err = 0;
-        for (int i = 0; i < 16; i++) {
-            int k = (v.y >> (2 * i)) & 3;
-            for (int c = 0; c < 3; c++) { int d = (int)chan(t[i], c) - pal[k][c]; err += d * d; }
-        }
-        return err;
+
+// BC7 mode 5 (zap_tex.h:597-684): rotation kept, 7-bit colour and 8-bit alpha endpoints (stored order), 2-bit
+// colour and alpha indices, each set with its anchor at texel 0; ts: the texels in stored channel order
+ZTC_DEV int mode5_block_sse(const uint32_t ts[16], const float e[6][4], int rot, uint4 &out) {
+    int q[2][4], x[2][4];
+    for (int k = 0; k < 2; k++) {
+        for (int c = 0; c < 3; c++) { q[k][c] = quant_plain(e[k][c], 7); x[k][c] = expand_bits(q[k][c], 7); }
+        q[k][3] = x[k][3] = clampi(f2i_x86(e[k][3] + 0.5f), 0, 255);
     }
-    uint4 v = *(const uint4 *)blk;
-    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-    float e[2][4];
-    block_endpoints(fmt, blk, e);
-    int err = 0;
+    int ci[16], ai[16], err = 0;
     for (int i = 0; i < 16; i++) {
-        int idx = i == 0 ? (int)get_bits128(w, 65, 3) : (int)get_bits128(w, 68 + 4 * (i - 1), 4);
-        for (int c = 0; c < 4; c++) { int d = (int)chan(t[i], c) - lerp64((int)e[0][c], (int)e[1][c], w4(idx)); err += d * d; }
+        int bj = 0, be = 1 << 30, bk = 0, bae = 1 << 30;
+        for (int j = 0; j < 4; j++) {
+            int d = 0;
+            for (int c = 0; c < 3; c++) { int y = (int)chan(ts[i], c) - lerp64(x[0][c], x[1][c], w2(j)); d += y * y; }
+            if (d < be) { be = d; bj = j; }
+            int y = (int)chan(ts[i], 3) - lerp64(x[0][3], x[1][3], w2(j));
+            if (y * y < bae) { bae = y * y; bk = j; }
+        }
+        ci[i] = bj; ai[i] = bk;
+        err += be + bae;
     }
+    if (ci[0] >= 2) {
+        for (int c = 0; c < 3; c++) { int s = q[0][c]; q[0][c] = q[1][c]; q[1][c] = s; }
+        for (int i = 0; i < 16; i++) ci[i] = 3 - ci[i];
+    }
+    if (ai[0] >= 2) {
+        int s = q[0][3]; q[0][3] = q[1][3]; q[1][3] = s;
+        for (int i = 0; i < 16; i++) ai[i] = 3 - ai[i];
+    }
+    Bits128 o;
+    o.put(1u << 5, 6);
+    o.put((uint32_t)rot, 2);
+    for (int c = 0; c < 3; c++) { o.put((uint32_t)q[0][c], 7); o.put((uint32_t)q[1][c], 7); }
+    o.put((uint32_t)q[0][3], 8); o.put((uint32_t)q[1][3], 8);
+    o.put((uint32_t)ci[0], 1);
+    for (int i = 1; i < 16; i++) o.put((uint32_t)ci[i], 2);
+    o.put((uint32_t)ai[0], 1);
+    for (int i = 1; i < 16; i++) o.put((uint32_t)ai[i], 2);
+    out = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
     return err;
+}
+
+// BC7 mode 1 (zap_tex.h:687-708): partition kept, two subsets of 6-bit RGB endpoints with one p-bit per subset,
+// 3-bit indices, anchors at texel 0 and at the partition's second-subset anchor; alpha decodes to 255
+ZTC_DEV int mode1_block_sse(const uint32_t t[16], const float e[6][4], int part, uint4 &out) {
+#ifdef __CUDA_ARCH__
+    const uint32_t mask = dec::kP2d[part];
+    const int anchor1 = dec::kA2d[part];
+#else
+    const uint32_t mask = 0u;
+    const int anchor1 = 15;
+#endif
+    int q[4][3], pb[2], x[4][3];
+    for (int s = 0; s < 2; s++) {
+        float best = 3.0e38f;
+        for (int p = 0; p < 2; p++) {
+            int qq[2][3];
+            float err = 0.0f, d;
+            for (int k = 0; k < 2; k++)
+                for (int c = 0; c < 3; c++) { qq[k][c] = quant_pbit(e[2 * s + k][c], 7, p, d); err += d * d; }
+            if (err < best) {
+                best = err; pb[s] = p;
+                for (int k = 0; k < 2; k++) for (int c = 0; c < 3; c++) q[2 * s + k][c] = qq[k][c];
+            }
+        }
+        for (int k = 0; k < 2; k++) for (int c = 0; c < 3; c++) x[2 * s + k][c] = expand_bits((q[2 * s + k][c] << 1) | pb[s], 7);
+    }
+    int idx[16], err = 0;
+    for (int i = 0; i < 16; i++) {
+        const int s = (mask >> i) & 1u;
+        int bj = 0, be = 1 << 30;
+        for (int j = 0; j < 8; j++) {
+            int d = 0;
+            for (int c = 0; c < 3; c++) { int y = (int)chan(t[i], c) - lerp64(x[2 * s][c], x[2 * s + 1][c], w3(j)); d += y * y; }
+            if (d < be) { be = d; bj = j; }
+        }
+        const int ya = (int)chan(t[i], 3) - 255;
+        idx[i] = bj;
+        err += be + ya * ya;
+    }
+    for (int s = 0; s < 2; s++) {
+        const int anchor = s ? anchor1 : 0;
+        if (idx[anchor] < 4) continue;
+        for (int c = 0; c < 3; c++) { int v = q[2 * s][c]; q[2 * s][c] = q[2 * s + 1][c]; q[2 * s + 1][c] = v; }
+        for (int i = 0; i < 16; i++) if ((int)((mask >> i) & 1u) == s) idx[i] = 7 - idx[i];
+    }
+    Bits128 o;
+    o.put(1u << 1, 2);
+    o.put((uint32_t)part, 6);
+    for (int c = 0; c < 3; c++) for (int k = 0; k < 4; k++) o.put((uint32_t)q[k][c], 6);
+    o.put((uint32_t)pb[0], 1); o.put((uint32_t)pb[1], 1);
+    for (int i = 0; i < 16; i++) o.put((uint32_t)idx[i], (i == 0 || i == anchor1) ? 2 : 3);
+    out = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
+    return err;
+}
+
+// squared error of a block as stored (the decoder's integer palette)
+ZTC_DEV int stored_sse(int fmt, const uint32_t t[16], const uint8_t *blk) {
+    uint32_t d[16];
+    dec::bcn_block(fmt, blk, d);
+    const int nc = fmt == ZTC_FMT_BC1 ? 3 : 4;
+    int err = 0;
+    for (int i = 0; i < 16; i++)
+        for (int c = 0; c < nc; c++) { int x = (int)chan(t[i], c) - (int)chan(d[i], c); err += x * x; }
+    return err;
+}
+
+// mode 5's rotation on a texel (swap A with R, G or B): decoded order <-> stored order
+ZTC_DEV uint32_t swap_alpha(uint32_t v, int rot) {
+    if (!rot) return v;
+    const int sh = 8 * (rot - 1);
+    const uint32_t a = v >> 24, c = (v >> sh) & 0xFFu;
+    return (v & ~((0xFFu << sh) | 0xFF000000u)) | (a << sh) | (c << 24);
 }
 
 __global__ void __launch_bounds__(128) refine_kernel(int fmt, SrcU8 src, int bw, int nblocks, uint8_t *__restrict__ blocks, int steps,
@@ -224,50 +370,58 @@ __global__ void __launch_bounds__(128) refine_kernel(int fmt, SrcU8 src, int bw,
     uint8_t *blk = blocks + (size_t)b * bs;
     uint32_t t[16];
     gather_block(src, b % bw, b / bw, t);
-    float a[16], e[2][4];
-    int nc;
-    const bool covered = !(fmt == ZTC_FMT_BC7 && (blk[0] & 0x7F) != 0x40);
-    int before;
-    if (covered) before = stored_sse(fmt, t, blk);
-    else {  // modes 5 / 1: not refined; their error still counts in the statistics
-        uint32_t d[16];
-        dec::bcn_block(ZTC_FMT_BC7, blk, d);
-        before = 0;
-        for (int i = 0; i < 16; i++)
-            for (int c = 0; c < 4; c++) { int x = (int)chan(t[i], c) - (int)chan(d[i], c); before += x * x; }
-    }
+    const int before = stored_sse(fmt, t, blk);
     int after = before;
-    if (covered && before > 0 && block_weights(fmt, blk, a, nc)) {
-        block_endpoints(fmt, blk, e);
-        float m[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}}, v[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-        const float b1 = 0.9f, b2 = 0.999f, inv_n = 2.0f / (16.0f * (float)nc);
+    LinBlock L;
+    float e[6][4];
+    linear_form(fmt, blk, L, e);
+    const bool refinable = fmt == ZTC_FMT_BC1 || L.mode == 6 || L.mode == 5 || L.mode == 1;
+    if (refinable && before > 0) {
+        // Adam in stored channel order (the rotation only permutes channels, so the squared error is the same);
+        // mode 1's alpha is fixed at 255 and not a parameter; a texel of subset 1 moves endpoints 2 and 3
+        uint32_t ts[16];
+        for (int i = 0; i < 16; i++) ts[i] = swap_alpha(t[i], L.rot);
+        const int npar = L.alpha_fixed ? 3 : L.nc;
+        float m[4][4], v[4][4];
+        for (int k = 0; k < 4; k++) for (int c = 0; c < 4; c++) m[k][c] = v[k][c] = 0.0f;
+        const float b1 = 0.9f, b2 = 0.999f, inv_n = 2.0f / (16.0f * (float)L.nc);
         float p1 = 1.0f, p2 = 1.0f;
         for (int s = 0; s < steps; s++) {
-            float g[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-            for (int i = 0; i < 16; i++)
-                for (int c = 0; c < nc; c++) {  // forward decode, residual, adjoint
-                    float r = (a[i] * e[0][c] + (1.0f - a[i]) * e[1][c] - (float)chan(t[i], c)) * inv_n;
-                    g[0][c] += a[i] * r;
-                    g[1][c] += (1.0f - a[i]) * r;
+            float g[4][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+            for (int i = 0; i < 16; i++) {
+                const bool in1 = (L.s1 >> i) & 1u;
+                for (int c = 0; c < npar; c++) {  // forward decode, residual, adjoint
+                    const float a = c == 3 ? L.aa[i] : L.a[i];
+                    const float e0 = in1 ? e[2][c] : e[0][c], e1 = in1 ? e[3][c] : e[1][c];
+                    const float r = (a * e0 + (1.0f - a) * e1 - (float)chan(ts[i], c)) * inv_n;
+                    const float g0 = a * r, g1 = (1.0f - a) * r;
+                    if (in1) { g[2][c] += g0; g[3][c] += g1; }
+                    else { g[0][c] += g0; g[1][c] += g1; }
                 }
+            }
             p1 *= b1; p2 *= b2;
-            for (int k = 0; k < 2; k++)
-                for (int c = 0; c < nc; c++) {
+            const int nk = L.s1 ? 4 : 2;
+            for (int k = 0; k < nk; k++)
+                for (int c = 0; c < npar; c++) {
                     m[k][c] = b1 * m[k][c] + (1.0f - b1) * g[k][c];
                     v[k][c] = b2 * v[k][c] + (1.0f - b2) * g[k][c] * g[k][c];
                     float mh = m[k][c] / (1.0f - p1), vh = v[k][c] / (1.0f - p2);
                     e[k][c] = fminf(255.0f, fmaxf(0.0f, e[k][c] - lr * mh / (sqrtf(vh) + 1e-8f)));
                 }
         }
+        int ne = 1 << 30;
         if (fmt == ZTC_FMT_BC1) {
             uint2 nb;
-            int ne = bc1_block_sse(t, q565(e[0][0], e[0][1], e[0][2]), q565(e[1][0], e[1][1], e[1][2]), nb);
-            if (ne < before) { *(uint2 *)blk = nb; after = ne; }
+            ne = bc1_block_sse(t, q565(e[0][0], e[0][1], e[0][2]), q565(e[1][0], e[1][1], e[1][2]), nb);
+            if (ne < before) *(uint2 *)blk = nb;
         } else {
             uint4 nb;
-            int ne = mode6_block_sse(t, e, nb);
-            if (ne < before) { *(uint4 *)blk = nb; after = ne; }
+            if (L.mode == 6) ne = mode6_block_sse(t, e, nb);
+            else if (L.mode == 5) ne = mode5_block_sse(ts, e, L.rot, nb);
+            else ne = mode1_block_sse(t, e, (int)get_bits128((const uint32_t *)blk, 2, 6), nb);
+            if (ne < before) *(uint4 *)blk = nb;
         }
+        if (ne < before) after = ne;
     }
     if (sse0) sse0[b] = (uint32_t)before;
     if (sse1) sse1[b] = (uint32_t)after;
@@ -277,7 +431,7 @@ __global__ void __launch_bounds__(128) refine_kernel(int fmt, SrcU8 src, int bw,
 
 // ---------------------------------------------------------------- C ABI
 static int adj_check(int fmt, const void *p, int n) {
-    if (fmt != ZTC_BC1 && fmt != ZTC_BC7) return ztc_set_error(ZTC_ERR_UNSUPPORTED, "differentiable decode covers BC1 and BC7 mode 6");
+    if (fmt != ZTC_BC1 && fmt != ZTC_BC7) return ztc_set_error(ZTC_ERR_UNSUPPORTED, "differentiable decode covers BC1 and BC7");
     if (!p || n < 0) return ztc_set_error(ZTC_ERR_INVALID_ARG, "null pointer or negative block count");
     if ((uintptr_t)p % (fmt == ZTC_BC1 ? 8u : 16u)) return ztc_set_error(ZTC_ERR_INVALID_ARG, "blocks must be aligned to the block size");
     return ZTC_OK;

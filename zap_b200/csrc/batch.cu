@@ -8,8 +8,11 @@
 //     tiles from a device counter (largest levels first); for BC7 that launch runs mode 6 and lists the blocks it
 //     does not finish in one batch-wide work list, which a second persistent launch (8-lane groups, modes 5 / 1)
 //     drains;
-//   - an optional autotuner times each format's kernel at 64/128/256 threads (= blocks per tile) on the batch's
-//     own tiles and keeps the fastest;
+//   - an optional autotuner times, per format class, on the batch's own levels: the CTA size (64/128/256 threads),
+//     the register cap (the single-image kernels' minimum resident CTAs, or a looser one), the blocks per tile
+//     (1, 2 or 4 CTAs' worth, a CTA running its tile in chunks), the tile shape (a row strip of consecutive blocks
+//     or a 2-D tile of block rows), and for BC7 the grid of the modes-5/1 launches (1 or 2 CTAs per SM, or as many
+//     as fit); one knob at a time, in that order, each keeping the fastest setting;
 //   - the whole sequence (counter resets, mip launches, concurrent encode launches) is captured into one CUDA
 //     graph; zap_tex_cuda_batch_run is one graph launch.
 // zap_tex_cuda_batch_run_plain issues the same work as one plain launch per texture and per level (the
@@ -29,6 +32,13 @@ namespace {
 constexpr int kClasses = 5;  // BC1, BC3, BC4, BC5, BC7 (format id == class id)
 constexpr int kHardCounter = 8;  // d_counters slots of the BC7 work-list lengths: after mode 6 (8), after mode 5 (9)
 const int kCtaChoices[3] = {64, 128, 256};
+const int kTileMult[3] = {1, 2, 4};  // blocks per tile = CTA size x this
+
+// one format class's launch configuration (the autotuner's knobs)
+struct ClassPlan {
+    int cta = 128, regs = 0, mult = 1, shape = 0;  // shape 0: row strip, 1: 2-D tile
+    int tile_w = 0, tile_h = 0;                     // the 2-D tile in blocks
+};
 
 struct HostLevel {
     int item, level, w, h, fmt, srgb;
@@ -54,7 +64,8 @@ struct zap_tex_cuda_batch {
     size_t mip_bytes = 0;
     ztc::BatchLevel *d_levels = nullptr;
     ztc::BatchTile *d_tiles[kClasses] = {};
-    int ntiles[kClasses] = {}, cta[kClasses] = {128, 128, 128, 128, 128}, grid[kClasses] = {};
+    int ntiles[kClasses] = {}, grid[kClasses] = {};
+    ClassPlan plan[kClasses];
     std::vector<ztc::BatchMip *> d_mips;
     std::vector<ztc::BatchMipTile *> d_mip_tiles;
     std::vector<int> n_mip_tiles;
@@ -62,12 +73,12 @@ struct zap_tex_cuda_batch {
     uint2 *d_hard_items = nullptr;           // BC7 work lists: (batch-wide block id, SSE) after mode 6, then after mode 5
     uint32_t *d_bc7_bases = nullptr;         // first batch-wide id of each BC7 level, ascending
     int *d_bc7_level_of = nullptr;           // ... and that level's index in d_levels
-    int n_bc7_levels = 0, hard_grid = 1;
+    int n_bc7_levels = 0, hard_grid = 1, hard_per_sm = 1;
     float *d_srgb = nullptr;
     void *plain_scratch = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    double tune_ms[kClasses][3] = {};
+    std::string tune_log[kClasses];  // the autotuner's timings, per knob
     long pixels = 0, blocks[kClasses] = {};
 };
 
@@ -84,32 +95,46 @@ int cuda_err(cudaError_t e, const char *what) {
         if (e_ != cudaSuccess) return cuda_err(e_, what);  \
     } while (0)
 
-// tiles of `cta` consecutive blocks for every level of class f, largest levels first
-std::vector<ztc::BatchTile> make_tiles(const zap_tex_cuda_batch *b, int f, int cta) {
+// the tiles of class f under plan p, largest levels first: row strips of cta x mult consecutive blocks, or 2-D
+// tiles of that many blocks (tile_w x tile_h, clipped at the level's edges)
+std::vector<ztc::BatchTile> make_tiles(const zap_tex_cuda_batch *b, int f, const ClassPlan &p) {
     std::vector<int> order;
     for (int i = 0; i < (int)b->levels.size(); i++) if (b->levels[i].fmt == f) order.push_back(i);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
         return (long)b->levels[x].bw * b->levels[x].bh > (long)b->levels[y].bw * b->levels[y].bh;
     });
+    const int per_tile = p.cta * p.mult;
     std::vector<ztc::BatchTile> t;
     for (int i : order) {
-        int n = b->levels[i].bw * b->levels[i].bh;
-        for (int first = 0; first < n; first += cta) t.push_back({i, first, std::min(cta, n - first), 0});
+        const int bw = b->levels[i].bw, bh = b->levels[i].bh, n = bw * bh;
+        if (p.shape == 0 || bw <= p.tile_w) {  // strips (a level no wider than a tile: its strips are its rows)
+            for (int first = 0; first < n; first += per_tile) t.push_back({i, first, std::min(per_tile, n - first), 0});
+            continue;
+        }
+        for (int by = 0; by < bh; by += p.tile_h)
+            for (int bx = 0; bx < bw; bx += p.tile_w) {
+                const int tw = std::min(p.tile_w, bw - bx), th = std::min(p.tile_h, bh - by);
+                t.push_back({i, by * bw + bx, tw * th, tw});
+            }
     }
     return t;
 }
 
-int upload_tiles(zap_tex_cuda_batch *b, int f, int cta) {
-    std::vector<ztc::BatchTile> t = make_tiles(b, f, cta);
+int upload_tiles(zap_tex_cuda_batch *b, int f, ClassPlan p) {
+    int lg = 0;
+    while ((1 << (lg + 1)) <= p.cta * p.mult) lg++;
+    p.tile_w = 1 << ((lg + 1) / 2);  // 2-D tiles as square as a power of two allows (wider than high)
+    p.tile_h = (p.cta * p.mult) / p.tile_w;
+    std::vector<ztc::BatchTile> t = make_tiles(b, f, p);
     if (b->d_tiles[f]) { cudaFree(b->d_tiles[f]); b->d_tiles[f] = nullptr; }
     b->ntiles[f] = (int)t.size();
-    b->cta[f] = cta;
+    b->plan[f] = p;
     if (t.empty()) return ZTC_OK;
     BCHECK(cudaMalloc(&b->d_tiles[f], t.size() * sizeof(ztc::BatchTile)), "cudaMalloc(tiles)");
     BCHECK(cudaMemcpy(b->d_tiles[f], t.data(), t.size() * sizeof(ztc::BatchTile), cudaMemcpyHostToDevice), "upload tiles");
-    const void *fn = f == ZTC_BC7 ? ztc_batch_bc7_kernel_fn(cta) : ztc_batch_bcn_kernel_fn(f, cta);
+    const void *fn = f == ZTC_BC7 ? ztc_batch_bc7_kernel_fn(p.cta, p.regs) : ztc_batch_bcn_kernel_fn(f, p.cta, p.regs);
     int per_sm = 1;
-    BCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, cta, 0), "occupancy");
+    BCHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, p.cta, 0), "occupancy");
     b->grid[f] = std::max(1, std::min(b->ntiles[f], per_sm * b->sms));
     return ZTC_OK;
 }
@@ -124,8 +149,8 @@ cudaError_t launch_encode(zap_tex_cuda_batch *b, int f, cudaStream_t s) {
         {
             ztc::TraceScope tr("batch_bc7_mode6", s);
             ztc::trace_units(b->blocks[f]);
-            e = ztc_launch_batch_bc7_mode6(b->cta[f], b->grid[f], b->d_levels, b->d_tiles[f], b->ntiles[f], b->d_counters + f, hard_count,
-                                           b->d_hard_items, s);
+            e = ztc_launch_batch_bc7_mode6(b->plan[f].cta, b->plan[f].regs, b->grid[f], b->d_levels, b->d_tiles[f], b->ntiles[f],
+                                           b->d_counters + f, hard_count, b->d_hard_items, s);
             if (e != cudaSuccess) return e;
         }
         ztc::TraceScope tr("batch_bc7_modes51", s);
@@ -135,7 +160,8 @@ cudaError_t launch_encode(zap_tex_cuda_batch *b, int f, cudaStream_t s) {
     }
     ztc::TraceScope tr(f == ZTC_BC1 ? "batch_bc1" : f == ZTC_BC3 ? "batch_bc3" : f == ZTC_BC4 ? "batch_bc4" : "batch_bc5", s);
     ztc::trace_units(b->blocks[f]);
-    return ztc_launch_batch_bcn(f, b->cta[f], b->grid[f], b->d_levels, b->d_tiles[f], b->ntiles[f], b->d_counters + f, s);
+    return ztc_launch_batch_bcn(f, b->plan[f].cta, b->plan[f].regs, b->grid[f], b->d_levels, b->d_tiles[f], b->ntiles[f],
+                                b->d_counters + f, s);
 }
 
 cudaError_t launch_mips(zap_tex_cuda_batch *b, cudaStream_t s) {
@@ -167,32 +193,72 @@ cudaError_t enqueue_all(zap_tex_cuda_batch *b, cudaStream_t s) {
     return cudaSuccess;
 }
 
+// Coordinate search per format class on the batch's own levels: each knob in turn (CTA size, register cap,
+// blocks per tile, tile shape; BC7: then the modes-5/1 grid) is timed at each of its settings with the others held,
+// and the fastest is kept. One warm-up launch per setting, then one timed launch (CUDA events).
 int autotune(zap_tex_cuda_batch *b) {
     cudaEvent_t e0, e1;
     BCHECK(cudaEventCreate(&e0), "event");
     BCHECK(cudaEventCreate(&e1), "event");
     int st = launch_mips(b, b->stream) == cudaSuccess ? ZTC_OK : cuda_err(cudaGetLastError(), "mip launch");
+    auto time_class = [&](int f, double &ms) -> int {
+        cudaError_t e = launch_encode(b, f, b->stream);  // warm-up
+        if (e == cudaSuccess) e = cudaEventRecord(e0, b->stream);
+        if (e == cudaSuccess) e = launch_encode(b, f, b->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) return cuda_err(e, "autotune");
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        ms = t;
+        return ZTC_OK;
+    };
+    char buf[96];
     for (int f = 0; f < kClasses && !st; f++) {
         bool any = false;
         for (auto &l : b->levels) any |= l.fmt == f;
         if (!any) continue;
-        int best_cta = 128;
-        double best = 1e30;
-        for (int c = 0; c < 3 && !st; c++) {
-            st = upload_tiles(b, f, kCtaChoices[c]);
-            if (st) break;
-            launch_encode(b, f, b->stream);  // warm-up
-            cudaEventRecord(e0, b->stream);
-            launch_encode(b, f, b->stream);
-            cudaEventRecord(e1, b->stream);
-            cudaError_t e = cudaEventSynchronize(e1);
-            if (e != cudaSuccess) { st = cuda_err(e, "autotune"); break; }
-            float ms = 0;
-            cudaEventElapsedTime(&ms, e0, e1);
-            b->tune_ms[f][c] = ms;
-            if (ms < best) { best = ms; best_cta = kCtaChoices[c]; }
+        ClassPlan best;
+        std::string log;
+        for (int knob = 0; knob < 4 && !st; knob++) {
+            const int nset = knob == 1 || knob == 3 ? 2 : 3;
+            ClassPlan keep = best;
+            double best_ms = 1e30;
+            log += knob == 0 ? " cta" : knob == 1 ? " regs" : knob == 2 ? " tile_ctas" : " shape";
+            for (int k = 0; k < nset && !st; k++) {
+                ClassPlan p = best;
+                if (knob == 0) p.cta = kCtaChoices[k];
+                else if (knob == 1) p.regs = k;
+                else if (knob == 2) p.mult = kTileMult[k];
+                else p.shape = k;
+                double ms = 0;
+                if (!(st = upload_tiles(b, f, p)) && !(st = time_class(f, ms))) {
+                    std::snprintf(buf, sizeof buf, "%s%.3f", k ? "/" : ":", ms);
+                    log += buf;
+                    if (ms < best_ms) { best_ms = ms; keep = p; }
+                }
+            }
+            best = keep;
         }
-        if (!st) st = upload_tiles(b, f, best_cta);
+        if (!st) st = upload_tiles(b, f, best);
+        if (f == ZTC_BC7 && !st && b->n_bc7_levels) {  // the modes-5/1 grid: 1, 2 or all resident CTAs per SM
+            const int choices[3] = {1, 2, b->hard_per_sm};
+            int best_grid = b->hard_grid;
+            double best_ms = 1e30;
+            log += " hard_ctas_per_sm";
+            for (int k = 0; k < 3 && !st; k++) {
+                if (k == 2 && (choices[2] <= 2)) break;
+                b->hard_grid = choices[k] * b->sms;
+                double ms = 0;
+                if (!(st = time_class(f, ms))) {
+                    std::snprintf(buf, sizeof buf, "%s%.3f", k ? "/" : ":", ms);
+                    log += buf;
+                    if (ms < best_ms) { best_ms = ms; best_grid = b->hard_grid; }
+                }
+            }
+            b->hard_grid = best_grid;
+        }
+        b->tune_log[f] = "tuned_ms" + log;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -355,7 +421,8 @@ int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *it
              "upload BC7 level map");
         int per_sm = 1;
         BTRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ztc_batch_bc7_hard_kernel_fn(), 128, 0), "occupancy");
-        b->hard_grid = std::max(1, per_sm) * b->sms;
+        b->hard_per_sm = std::max(1, per_sm);
+        b->hard_grid = b->hard_per_sm * b->sms;
     }
     float tables[512];
     ztc::srgb_tables_host(tables, tables + 256);
@@ -367,7 +434,14 @@ int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *it
     int st = ZTC_OK;
     if (flags & ZTC_BATCH_AUTOTUNE) st = autotune(b);
     else
-        for (int f = 0; f < kClasses && !st; f++) st = upload_tiles(b, f, 128);
+        for (int f = 0; f < kClasses && !st; f++) {
+            ClassPlan p;
+            p.cta = (flags & ZTC_BATCH_CTA_64) ? 64 : (flags & ZTC_BATCH_CTA_256) ? 256 : 128;
+            p.regs = (flags & ZTC_BATCH_REGS_LOOSE) ? 1 : 0;
+            p.mult = (flags & ZTC_BATCH_TILE_X4) ? 4 : (flags & ZTC_BATCH_TILE_X2) ? 2 : 1;
+            p.shape = (flags & ZTC_BATCH_TILES_2D) ? 1 : 0;
+            st = upload_tiles(b, f, p);
+        }
     if (st) return fail(st);
     // ---- one CUDA graph for the whole batch
     if (!(flags & ZTC_BATCH_NO_GRAPH)) {
@@ -429,9 +503,19 @@ int zap_tex_cuda_batch_info(zap_tex_cuda_batch *b, char *buf, size_t cap) {
     const char *names[kClasses] = {"bc1", "bc3", "bc4", "bc5", "bc7"};
     for (int f = 0; f < kClasses; f++) {
         if (!b->ntiles[f]) continue;
-        std::snprintf(line, sizeof line, "%s tiles %d cta %d grid %d tune_ms %.4f %.4f %.4f\n", names[f], b->ntiles[f], b->cta[f], b->grid[f],
-                      b->tune_ms[f][0], b->tune_ms[f][1], b->tune_ms[f][2]);
+        const ClassPlan &p = b->plan[f];
+        char shape[32];
+        if (p.shape) std::snprintf(shape, sizeof shape, "2d_%dx%d", p.tile_w, p.tile_h);
+        else std::snprintf(shape, sizeof shape, "strip");
+        std::snprintf(line, sizeof line, "%s tiles %d cta %d regs %s blocks_per_tile %d shape %s grid %d", names[f], b->ntiles[f], p.cta,
+                      p.regs ? "loose" : "tight", p.cta * p.mult, shape, b->grid[f]);
         s += line;
+        if (f == ZTC_BC7) {
+            std::snprintf(line, sizeof line, " hard_grid %d", b->hard_grid);
+            s += line;
+        }
+        if (!b->tune_log[f].empty()) s += " " + b->tune_log[f];
+        s += "\n";
     }
     if (buf && cap) { std::strncpy(buf, s.c_str(), cap - 1); buf[cap - 1] = 0; }
     return (int)s.size();

@@ -680,8 +680,8 @@ __global__ void __launch_bounds__(128, ZTC_MINB_BC7_HARD) bc7_hard_kernel(SrcU8 
 // block, at the plain kernel's occupancy. Blocks above SSE 64 go to one work list for the whole batch, keyed by
 // their batch-wide block id (the level's first id + the block index). Modes 5 and 1 then run as one persistent
 // launch of 8-lane groups over that list, so every group has a block to work on until the list is drained.
-template <int CTA>
-__global__ void __launch_bounds__(CTA, ZTC_MINB_BC7_MODE6 * 128 / CTA)
+template <int CTA, int MINB>
+__global__ void __launch_bounds__(CTA, MINB * 128 / CTA)
 batch_bc7_mode6_kernel(const BatchLevel *__restrict__ levels, const BatchTile *__restrict__ tiles, int ntiles,
                        uint32_t *__restrict__ counter, uint32_t *__restrict__ hard_count, uint2 *__restrict__ hard_items) {
     __shared__ int s_tile;
@@ -694,26 +694,30 @@ batch_bc7_mode6_kernel(const BatchLevel *__restrict__ levels, const BatchTile *_
         if (tile >= ntiles) break;
         const BatchTile T = tiles[tile];
         const BatchLevel L = levels[T.level];
-        const int b = T.first + (int)threadIdx.x;
-        const bool valid = (int)threadIdx.x < T.count;
-        uint32_t t[16];
-        if (valid) {
-            const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
-            gather_block(src, b % L.bw, b / L.bw, t);
-            #pragma unroll
-            for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
-        }
-        uint4 blk;
-        const int err = mode6_encode_cta<CTA, true>(valid, t, s_tex, blk);
-        if (valid) store_block16(L.dst + (size_t)b * 16, blk);
-        const bool hard = valid && err > 16 * 4;  // zap_tex.h:758 early exit
-        const unsigned ballot = __ballot_sync(0xFFFFFFFFu, hard);
-        if (ballot) {
-            const int lane = threadIdx.x & 31, leader = __ffs(ballot) - 1;
-            uint32_t base = 0;
-            if (lane == leader) base = atomicAdd(hard_count, (uint32_t)__popc(ballot));
-            base = __shfl_sync(0xFFFFFFFFu, base, leader);
-            if (hard) hard_items[base + __popc(ballot & ((1u << lane) - 1u))] = make_uint2(L.gbase + (uint32_t)b, (uint32_t)err);
+        const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
+        for (int j0 = 0; j0 < T.count; j0 += CTA) {  // the same trip count in every thread: barriers stay uniform
+            const int j = j0 + (int)threadIdx.x;
+            const bool valid = j < T.count;
+            const int b = tile_block(T, L.bw, j);
+            uint32_t t[16];
+            if (valid) {
+                gather_block(src, b % L.bw, b / L.bw, t);
+                #pragma unroll
+                for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
+            }
+            uint4 blk;
+            const int err = mode6_encode_cta<CTA, true>(valid, t, s_tex, blk);
+            if (valid) store_block16(L.dst + (size_t)b * 16, blk);
+            const bool hard = valid && err > 16 * 4;  // zap_tex.h:758 early exit
+            const unsigned ballot = __ballot_sync(0xFFFFFFFFu, hard);
+            if (ballot) {
+                const int lane = threadIdx.x & 31, leader = __ffs(ballot) - 1;
+                uint32_t base = 0;
+                if (lane == leader) base = atomicAdd(hard_count, (uint32_t)__popc(ballot));
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                if (hard) hard_items[base + __popc(ballot & ((1u << lane) - 1u))] = make_uint2(L.gbase + (uint32_t)b, (uint32_t)err);
+            }
+            __syncthreads();  // the next chunk overwrites s_tex
         }
     }
 }
@@ -779,15 +783,12 @@ batch_bc7_phase_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__
 
 }  // namespace ztc
 
-cudaError_t ztc_launch_batch_bc7_mode6(int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
+cudaError_t ztc_launch_batch_bc7_mode6(int cta, int regs, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
                                        uint32_t *counter, uint32_t *hard_count, uint2 *hard_items, cudaStream_t stream) {
-    switch (cta) {
-    case 64: ztc::batch_bc7_mode6_kernel<64><<<grid, 64, 0, stream>>>(levels, tiles, ntiles, counter, hard_count, hard_items); break;
-    case 128: ztc::batch_bc7_mode6_kernel<128><<<grid, 128, 0, stream>>>(levels, tiles, ntiles, counter, hard_count, hard_items); break;
-    case 256: ztc::batch_bc7_mode6_kernel<256><<<grid, 256, 0, stream>>>(levels, tiles, ntiles, counter, hard_count, hard_items); break;
-    default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+    const void *fn = ztc_batch_bc7_kernel_fn(cta, regs);
+    if (!fn) return cudaErrorInvalidValue;
+    void *args[] = {(void *)&levels, (void *)&tiles, (void *)&ntiles, (void *)&counter, (void *)&hard_count, (void *)&hard_items};
+    return cudaLaunchKernel(fn, dim3(grid), dim3(cta), args, 0, stream);
 }
 
 cudaError_t ztc_launch_batch_bc7_hard(int grid, const ztc::BatchLevel *levels, const uint32_t *bases, const int *level_of, int nlevels,
@@ -802,13 +803,17 @@ cudaError_t ztc_launch_batch_bc7_hard(int grid, const ztc::BatchLevel *levels, c
     return cudaGetLastError();
 }
 
-const void *ztc_batch_bc7_kernel_fn(int cta) {
+template <int MINB>
+static const void *batch_bc7_fn_cap(int cta) {
     switch (cta) {
-    case 64: return (const void *)ztc::batch_bc7_mode6_kernel<64>;
-    case 128: return (const void *)ztc::batch_bc7_mode6_kernel<128>;
-    case 256: return (const void *)ztc::batch_bc7_mode6_kernel<256>;
+    case 64: return (const void *)ztc::batch_bc7_mode6_kernel<64, MINB>;
+    case 128: return (const void *)ztc::batch_bc7_mode6_kernel<128, MINB>;
+    case 256: return (const void *)ztc::batch_bc7_mode6_kernel<256, MINB>;
     default: return nullptr;
     }
+}
+const void *ztc_batch_bc7_kernel_fn(int cta, int regs) {
+    return regs ? batch_bc7_fn_cap<ZTC_MINB_BC7_BATCH_LOOSE>(cta) : batch_bc7_fn_cap<ZTC_MINB_BC7_MODE6>(cta);
 }
 
 const void *ztc_batch_bc7_hard_kernel_fn() { return (const void *)ztc::batch_bc7_phase_kernel<5>; }  // both phases: same bounds

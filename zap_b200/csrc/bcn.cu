@@ -340,10 +340,13 @@ cudaError_t ztc_launch_bcn(int fmt, const ztc::SrcU8 &src, int by0, int nby, uin
 }
 
 // ---------------------------------------------------------------- batched: one persistent launch over a tile queue
+// A CTA takes one tile at a time and runs it in chunks of CTA blocks (a tile holds a multiple of the CTA's blocks:
+// blocks per tile and CTA size are separate knobs of the batch autotuner, as are the tile's shape, a row strip or a
+// 2-D tile, and MINB, the minimum resident CTAs of 128 threads per SM that sets the register cap).
 namespace ztc {
-template <int FMT, int CTA>
-__global__ void __launch_bounds__(CTA, ZTC_MINB_BCN_BATCH * 128 / CTA) batch_bcn_kernel(const BatchLevel *__restrict__ levels, const BatchTile *__restrict__ tiles,
-                                                        int ntiles, uint32_t *__restrict__ counter) {
+template <int FMT, int CTA, int MINB>
+__global__ void __launch_bounds__(CTA, MINB * 128 / CTA) batch_bcn_kernel(const BatchLevel *__restrict__ levels, const BatchTile *__restrict__ tiles,
+                                                                         int ntiles, uint32_t *__restrict__ counter) {
     constexpr bool kColour = FMT == ZTC_FMT_BC1 || FMT == ZTC_FMT_BC3;
     __shared__ int s_tile;
     __shared__ uint32_t s_tex[16][kColour ? CTA : 1];  // column threadIdx.x: this thread's block (BC1 / BC3)
@@ -354,58 +357,66 @@ __global__ void __launch_bounds__(CTA, ZTC_MINB_BCN_BATCH * 128 / CTA) batch_bcn
         __syncthreads();  // every thread has read s_tile before thread 0 overwrites it
         if (tile >= ntiles) break;
         const BatchTile T = tiles[tile];
-        const bool valid = (int)threadIdx.x < T.count;
-        if (!kColour && !valid) continue;  // BC4 / BC5 never synchronise inside a tile
         const BatchLevel L = levels[T.level];
         const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
-        const int b = T.first + (int)threadIdx.x;
-        uint32_t t[16];
-        if (valid) {
-            gather_block(src, b % L.bw, b / L.bw, t);
-            if (kColour) {
-                #pragma unroll
-                for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
+        for (int j0 = 0; j0 < T.count; j0 += CTA) {  // the same trip count in every thread: barriers stay uniform
+            const int j = j0 + (int)threadIdx.x;
+            const bool valid = j < T.count;
+            if (!kColour && !valid) continue;  // BC4 / BC5 never synchronise inside a tile
+            const int b = tile_block(T, L.bw, j);
+            uint32_t t[16];
+            if (valid) {
+                gather_block(src, b % L.bw, b / L.bw, t);
+                if (kColour) {
+                    #pragma unroll
+                    for (int i = 0; i < 16; i++) s_tex[i][threadIdx.x] = t[i];
+                }
             }
-        }
-        if (FMT == ZTC_FMT_BC1) {
-            const uint2 c = bc1_encode_cta<CTA, true>(valid, t, (uint32_t(*)[CTA])s_tex);
-            if (valid) store_block8(L.dst + (size_t)b * 8, c);
-        } else if (FMT == ZTC_FMT_BC4) store_block8(L.dst + (size_t)b * 8, bc4_encode(t, 0));
-        else if (FMT == ZTC_FMT_BC3) {
-            const uint2 a = valid ? bc4_encode(t, 3) : make_uint2(0u, 0u);
-            const uint2 c = bc1_encode_cta<CTA, true>(valid, t, (uint32_t(*)[CTA])s_tex);
-            if (valid) store_block16(L.dst + (size_t)b * 16, make_uint4(a.x, a.y, c.x, c.y));
-        } else {
-            uint2 r = bc4_encode(t, 0), g = bc4_encode(t, 1);
-            store_block16(L.dst + (size_t)b * 16, make_uint4(r.x, r.y, g.x, g.y));
+            if (FMT == ZTC_FMT_BC1) {
+                const uint2 c = bc1_encode_cta<CTA, true>(valid, t, (uint32_t(*)[CTA])s_tex);
+                if (valid) store_block8(L.dst + (size_t)b * 8, c);
+            } else if (FMT == ZTC_FMT_BC4) store_block8(L.dst + (size_t)b * 8, bc4_encode(t, 0));
+            else if (FMT == ZTC_FMT_BC3) {
+                const uint2 a = valid ? bc4_encode(t, 3) : make_uint2(0u, 0u);
+                const uint2 c = bc1_encode_cta<CTA, true>(valid, t, (uint32_t(*)[CTA])s_tex);
+                if (valid) store_block16(L.dst + (size_t)b * 16, make_uint4(a.x, a.y, c.x, c.y));
+            } else {
+                uint2 r = bc4_encode(t, 0), g = bc4_encode(t, 1);
+                store_block16(L.dst + (size_t)b * 16, make_uint4(r.x, r.y, g.x, g.y));
+            }
+            if (kColour) __syncthreads();  // the next chunk overwrites s_tex
         }
     }
 }
 
-template <int FMT>
-static const void *batch_fn(int cta) {
+template <int FMT, int MINB>
+static const void *batch_fn_cap(int cta) {
     switch (cta) {
-    case 64: return (const void *)batch_bcn_kernel<FMT, 64>;
-    case 128: return (const void *)batch_bcn_kernel<FMT, 128>;
-    case 256: return (const void *)batch_bcn_kernel<FMT, 256>;
+    case 64: return (const void *)batch_bcn_kernel<FMT, 64, MINB>;
+    case 128: return (const void *)batch_bcn_kernel<FMT, 128, MINB>;
+    case 256: return (const void *)batch_bcn_kernel<FMT, 256, MINB>;
     default: return nullptr;
     }
+}
+template <int FMT>
+static const void *batch_fn(int cta, int regs) {
+    return regs ? batch_fn_cap<FMT, ZTC_MINB_BCN_BATCH_LOOSE>(cta) : batch_fn_cap<FMT, ZTC_MINB_BCN_BATCH>(cta);
 }
 }  // namespace ztc
 
-const void *ztc_batch_bcn_kernel_fn(int fmt, int cta) {
+const void *ztc_batch_bcn_kernel_fn(int fmt, int cta, int regs) {
     switch (fmt) {
-    case ZTC_FMT_BC1: return ztc::batch_fn<ZTC_FMT_BC1>(cta);
-    case ZTC_FMT_BC3: return ztc::batch_fn<ZTC_FMT_BC3>(cta);
-    case ZTC_FMT_BC4: return ztc::batch_fn<ZTC_FMT_BC4>(cta);
-    case ZTC_FMT_BC5: return ztc::batch_fn<ZTC_FMT_BC5>(cta);
+    case ZTC_FMT_BC1: return ztc::batch_fn<ZTC_FMT_BC1>(cta, regs);
+    case ZTC_FMT_BC3: return ztc::batch_fn<ZTC_FMT_BC3>(cta, regs);
+    case ZTC_FMT_BC4: return ztc::batch_fn<ZTC_FMT_BC4>(cta, regs);
+    case ZTC_FMT_BC5: return ztc::batch_fn<ZTC_FMT_BC5>(cta, regs);
     default: return nullptr;
     }
 }
 
-cudaError_t ztc_launch_batch_bcn(int fmt, int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
+cudaError_t ztc_launch_batch_bcn(int fmt, int cta, int regs, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
                                  uint32_t *counter, cudaStream_t stream) {
-    const void *fn = ztc_batch_bcn_kernel_fn(fmt, cta);
+    const void *fn = ztc_batch_bcn_kernel_fn(fmt, cta, regs);
     if (!fn) return cudaErrorInvalidValue;
     void *args[] = {(void *)&levels, (void *)&tiles, (void *)&ntiles, (void *)&counter};
     return cudaLaunchKernel(fn, dim3(grid), dim3(cta), args, 0, stream);

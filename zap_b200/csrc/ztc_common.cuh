@@ -33,6 +33,13 @@
 #ifndef ZTC_MINB_BCN_BATCH
 #define ZTC_MINB_BCN_BATCH ZTC_MINB_BCN
 #endif
+// the batched encoder's second register cap (its autotuner picks per format): fewer resident CTAs, fewer spills
+#ifndef ZTC_MINB_BCN_BATCH_LOOSE
+#define ZTC_MINB_BCN_BATCH_LOOSE 5
+#endif
+#ifndef ZTC_MINB_BC7_BATCH_LOOSE
+#define ZTC_MINB_BC7_BATCH_LOOSE 4
+#endif
 #ifndef ZTC_MINB_ASTC_SINGLE
 #define ZTC_MINB_ASTC_SINGLE 5
 #endif

@@ -76,26 +76,34 @@ ZTC_DEV int anchor_of(int ns, int part, int s) {
 #endif
 }
 
-// full BC7 decode, all 8 modes; reserved mode -> transparent black (zap_tex.h:378-417)
-ZTC_DEV void bc7_block(const uint32_t w[4], uint32_t out[16]) {
+// A BC7 block's fields (zap_tex.h:378-412): mode (8 = reserved), subsets, partition, rotation, whether alpha has
+// its own bits (else it decodes to 255), the expanded 8-bit endpoints (endpoint 2s + k of subset s) and each
+// texel's subset and colour / alpha interpolation weight (0..64). The decode of texel i is
+// lerp64(ep[2s][c], ep[2s+1][c], w) per channel, then alpha swapped with channel rot - 1 when rot > 0; with the
+// weights held fixed it is linear in the endpoints, which the differentiable decode builds on.
+struct Bc7Fields {
+    int mode, ns, part, rot, ab;
+    int ep[6][4];
+    uint8_t subset[16], cw[16], aw[16];
+};
+ZTC_DEV bool bc7_parse(const uint32_t w[4], Bc7Fields &F) {
     int mode = 0;
     while (mode < 8 && !((w[0] >> mode) & 1u)) mode++;
-    if (mode == 8) {
-        for (int i = 0; i < 16; i++) out[i] = 0;
-        return;
-    }
+    F.mode = mode;
+    F.ns = 1; F.part = 0; F.rot = 0; F.ab = 0;
+    if (mode == 8) return false;
     const Mode M = mode_info(mode);
     int pos = mode + 1;
     const int part = (int)get_bits128(w, pos, M.pb); pos += M.pb;
     const int rot = (int)get_bits128(w, pos, M.rb); pos += M.rb;
     const int isb = (int)get_bits128(w, pos, M.isb); pos += M.isb;
     const int ne = 2 * M.ns;
-    int ep[6][4], cb = M.cb, ab = M.ab;
+    int cb = M.cb, ab = M.ab;
     for (int c = 0; c < 3; c++)
-        for (int e = 0; e < ne; e++) { ep[e][c] = (int)get_bits128(w, pos, cb); pos += cb; }
+        for (int e = 0; e < ne; e++) { F.ep[e][c] = (int)get_bits128(w, pos, cb); pos += cb; }
     for (int e = 0; e < ne; e++) {
-        if (ab) { ep[e][3] = (int)get_bits128(w, pos, ab); pos += ab; }
-        else ep[e][3] = 255;
+        if (ab) { F.ep[e][3] = (int)get_bits128(w, pos, ab); pos += ab; }
+        else F.ep[e][3] = 255;
     }
     if (M.epb || M.spb) {
         for (int e = 0; e < ne; e++) {
@@ -103,17 +111,19 @@ ZTC_DEV void bc7_block(const uint32_t w[4], uint32_t out[16]) {
             int p = (int)get_bits128(w, pos, 1); pos += 1;
             int last = M.epb ? e : e + 1;
             for (int k = e; k <= last; k++) {
-                for (int c = 0; c < 3; c++) ep[k][c] = (ep[k][c] << 1) | p;
-                if (ab) ep[k][3] = (ep[k][3] << 1) | p;
+                for (int c = 0; c < 3; c++) F.ep[k][c] = (F.ep[k][c] << 1) | p;
+                if (ab) F.ep[k][3] = (F.ep[k][3] << 1) | p;
             }
         }
         cb++;
         if (ab) ab++;
     }
     for (int e = 0; e < ne; e++) {
-        for (int c = 0; c < 3; c++) ep[e][c] = expand_bits(ep[e][c], cb);
-        if (ab) ep[e][3] = expand_bits(ep[e][3], ab);
+        for (int c = 0; c < 3; c++) F.ep[e][c] = expand_bits(F.ep[e][c], cb);
+        if (ab) F.ep[e][3] = expand_bits(F.ep[e][3], ab);
     }
+    for (int e = ne; e < 6; e++)
+        for (int c = 0; c < 4; c++) F.ep[e][c] = 0;
     int i1[16], i2[16];
     for (int i = 0; i < 16; i++) {
         int anchor = i == anchor_of(M.ns, part, subset_of(M.ns, part, i));
@@ -124,13 +134,28 @@ ZTC_DEV void bc7_block(const uint32_t w[4], uint32_t out[16]) {
         if (M.ib2) { i2[i] = (int)get_bits128(w, pos, M.ib2 - (i == 0)); pos += M.ib2 - (i == 0); }
     }
     for (int i = 0; i < 16; i++) {
-        int s = subset_of(M.ns, part, i);
-        int cw = (M.ib2 && isb) ? wbits(M.ib2, i2[i]) : wbits(M.ib, i1[i]);
-        int aw = !M.ib2 ? cw : isb ? wbits(M.ib, i1[i]) : wbits(M.ib2, i2[i]);
+        F.subset[i] = (uint8_t)subset_of(M.ns, part, i);
+        const int cw = (M.ib2 && isb) ? wbits(M.ib2, i2[i]) : wbits(M.ib, i1[i]);
+        F.cw[i] = (uint8_t)cw;
+        F.aw[i] = (uint8_t)(!M.ib2 ? cw : isb ? wbits(M.ib, i1[i]) : wbits(M.ib2, i2[i]));
+    }
+    F.ns = M.ns; F.part = part; F.rot = rot; F.ab = M.ab > 0;
+    return true;
+}
+
+// full BC7 decode, all 8 modes; reserved mode -> transparent black (zap_tex.h:378-417)
+ZTC_DEV void bc7_block(const uint32_t w[4], uint32_t out[16]) {
+    Bc7Fields F;
+    if (!bc7_parse(w, F)) {
+        for (int i = 0; i < 16; i++) out[i] = 0;
+        return;
+    }
+    for (int i = 0; i < 16; i++) {
+        const int s = F.subset[i];
         int px[4];
-        for (int c = 0; c < 3; c++) px[c] = lerp64(ep[2 * s][c], ep[2 * s + 1][c], cw);
-        px[3] = lerp64(ep[2 * s][3], ep[2 * s + 1][3], aw);
-        if (rot) { int t = px[3]; px[3] = px[rot - 1]; px[rot - 1] = t; }
+        for (int c = 0; c < 3; c++) px[c] = lerp64(F.ep[2 * s][c], F.ep[2 * s + 1][c], F.cw[i]);
+        px[3] = lerp64(F.ep[2 * s][3], F.ep[2 * s + 1][3], F.aw[i]);
+        if (F.rot) { int t = px[3]; px[3] = px[F.rot - 1]; px[F.rot - 1] = t; }
         out[i] = pack_rgba(px[0], px[1], px[2], px[3]);
     }
 }

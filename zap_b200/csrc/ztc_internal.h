@@ -49,9 +49,16 @@ struct BatchLevel {     // one (texture, mip level) to encode
     uint32_t gbase;     // BC7 levels: batch-wide id of the level's first block (ids run over the batch's BC7 levels)
     uint32_t pad;
 };
-struct BatchTile {      // consecutive blocks [first, first + count) of one level
-    int level, first, count, pad;
+struct BatchTile {      // count blocks of one level, from block index `first`
+    int level, first, count;
+    int tw;             // 0: a row strip, blocks first .. first + count - 1; else a 2-D tile tw blocks wide (row-major)
 };
+#ifdef __CUDACC__
+// block index (raster order in a level bw blocks wide) of the tile's j-th block
+__host__ __device__ inline int tile_block(const BatchTile &t, int bw, int j) {
+    return t.tw ? t.first + (j / t.tw) * bw + (j % t.tw) : t.first + j;
+}
+#endif
 struct BatchMip {       // one (texture, level d >= 1): built from level d - 1
     const uint8_t *src;
     uint8_t *dst;
@@ -63,21 +70,22 @@ struct BatchMipTile {   // output texel pairs [first, first + count) of one Batc
 };
 }  // namespace ztc
 
-cudaError_t ztc_launch_batch_bcn(int fmt, int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
+// `regs`: 0 = the register cap of the single-image kernels (more resident CTAs), 1 = a looser cap (fewer spills)
+cudaError_t ztc_launch_batch_bcn(int fmt, int cta, int regs, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
                                  uint32_t *counter, cudaStream_t stream);
 // BC7 in two launches: mode 6 over the tile queue, appending (batch-wide block id, SSE) of the blocks it does not
 // finish to hard_items; then mode 5 over that list, appending its opaque blocks to opaque_items (opaque_count zeroed
 // by the caller), and mode 1 over those (bases / level_of: the BC7 levels' first ids, ascending, and their indices in
 // `levels`)
-cudaError_t ztc_launch_batch_bc7_mode6(int cta, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
+cudaError_t ztc_launch_batch_bc7_mode6(int cta, int regs, int grid, const ztc::BatchLevel *levels, const ztc::BatchTile *tiles, int ntiles,
                                        uint32_t *counter, uint32_t *hard_count, uint2 *hard_items, cudaStream_t stream);
 cudaError_t ztc_launch_batch_bc7_hard(int grid, const ztc::BatchLevel *levels, const uint32_t *bases, const int *level_of, int nlevels,
                                       const uint32_t *hard_count, const uint2 *hard_items, uint32_t *opaque_count, uint2 *opaque_items,
                                       cudaStream_t stream);
 cudaError_t ztc_launch_batch_mip(int grid, const ztc::BatchMip *mips, const ztc::BatchMipTile *tiles, int ntiles, const float *srgb_tables,
                                  cudaStream_t stream);
-const void *ztc_batch_bcn_kernel_fn(int fmt, int cta);
-const void *ztc_batch_bc7_kernel_fn(int cta);  // the mode 6 tile-queue kernel
+const void *ztc_batch_bcn_kernel_fn(int fmt, int cta, int regs);
+const void *ztc_batch_bc7_kernel_fn(int cta, int regs);  // the mode 6 tile-queue kernel
 const void *ztc_batch_bc7_hard_kernel_fn();
 const void *ztc_batch_mip_kernel_fn();
 namespace ztc { void srgb_tables_host(float lin[256], float thr[256]); }
