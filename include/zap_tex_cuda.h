@@ -38,7 +38,7 @@ typedef enum zap_tex_cuda_status {
     ZTC_ERR_UNSUPPORTED = -2, /* rdo != 0 (rate-distortion mode), or a format the call does not take */
     ZTC_ERR_CUDA = -3,        /* a CUDA runtime error; zap_tex_cuda_last_error() has the text */
     ZTC_ERR_NO_MEMORY = -4,   /* device or pinned-host allocation failed */
-    ZTC_ERR_TIMEOUT = -5,     /* a bounded device-side wait gave up (batched queue) */
+    /* -5 is not used: no kernel of this library waits on a flag, a peer or another launch */
     ZTC_ERR_NO_DEVICE = -6    /* no CUDA device, or the device is not sm_100 */
 } zap_tex_cuda_status;
 
@@ -243,6 +243,15 @@ ZTC_API int zap_tex_cuda_tex_file(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, in
    probe instructions the launch executes; the caller times it (CUDA events) and divides. sink: 4 bytes of device
    memory the kernel may write. */
 ZTC_API int zap_tex_cuda_alu_probe_dev(int kind, int iters, void *sink, void *stream, double *instructions);
+/* Test hook: of the library's next device or pinned-host allocations, let `skip` succeed and make the `count` after
+   them fail as if the device were out of memory, so a caller's tests can check that every entry point then returns
+   ZTC_ERR_NO_MEMORY and works again afterwards. (0, 0) clears it. Process-wide. */
+ZTC_API int zap_tex_cuda_debug_fail_allocations(int skip, int count);
+/* The bounds-check build (make -C zap_b200/csrc checks: libzap_tex_cuda_checks.so, -DZTC_CHECKS) checks the
+   kernels' global and shared-memory indices (texel gathers, work lists, per-CTA compacted lists); a failed check
+   skips its access and records (site << 24) | index in a device word. This synchronises the device and returns
+   that word (0: no failure) and clears it. The product build returns ZTC_ERR_UNSUPPORTED. */
+ZTC_API int zap_tex_cuda_debug_checks(unsigned int *first_failure);
 
 /* Allocation-free BC7 encode. No counterpart in the reference (zap_tex.h allocates nothing because it runs on the
    CPU); it exists for callers that cannot allocate device memory when they encode: work recorded into a CUDA

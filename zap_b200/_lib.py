@@ -10,11 +10,12 @@ import threading
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
-LIB_PATH = os.path.join(PKG, "lib", "libzap_tex_cuda.so")
+# ZAP_TEX_CUDA_LIB selects another build of the same library (the bounds-check build, libzap_tex_cuda_checks.so)
+LIB_PATH = os.environ.get("ZAP_TEX_CUDA_LIB") or os.path.join(PKG, "lib", "libzap_tex_cuda.so")
 
 ZTC_OK = 0
 STATUS = {0: "ok", -1: "invalid argument", -2: "unsupported", -3: "CUDA error", -4: "out of memory",
-          -5: "device wait timed out", -6: "no usable CUDA device"}
+          -6: "no usable CUDA device"}
 
 _lock = threading.Lock()
 _lib = None
@@ -27,9 +28,10 @@ class ZapTexError(RuntimeError):
 
 
 def build(verbose=False):
-    """Compile every CUDA source for sm_100a into the in-tree shared library (nvcc cross-compiles without a GPU)."""
+    """Compile every CUDA source for sm_100a into the in-tree shared library, and its bounds-check build
+    (libzap_tex_cuda_checks.so), with nvcc, which cross-compiles without a GPU."""
     jobs = str(min(8, os.cpu_count() or 1))
-    r = subprocess.run(["make", "-C", CSRC, "-j", jobs], capture_output=not verbose, text=True)
+    r = subprocess.run(["make", "-C", CSRC, "-j", jobs, "all", "checks"], capture_output=not verbose, text=True)
     if r.returncode != 0:
         raise RuntimeError("building libzap_tex_cuda.so failed:\n" + (r.stdout or "") + (r.stderr or ""))
     return LIB_PATH
@@ -91,6 +93,8 @@ def _declare(lib):
         "zap_tex_cuda_tex_file_bytes": ([i, i, i, i, i], sz),
         "zap_tex_cuda_tex_file": ([vp, vp, i, i, sz, i, f, i, i, vp, sz], i),
         "zap_tex_cuda_alu_probe_dev": ([i, i, vp, vp, C.POINTER(C.c_double)], i),
+        "zap_tex_cuda_debug_fail_allocations": ([i, i], i),
+        "zap_tex_cuda_debug_checks": ([C.POINTER(C.c_uint)], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -477,10 +477,11 @@ int zap_tex_cuda_palette_adjoint_dev(zap_tex_cuda_ctx *ctx, int fmt, const void 
 int zap_tex_cuda_refine_dev(zap_tex_cuda_ctx *ctx, int fmt, const uint8_t *rgba, int w, int h, size_t stride, void *blocks, int steps,
                             float lr, uint32_t *sse_before, uint32_t *sse_after, void *stream) {
     int st = adj_check(fmt, blocks, 0);
-    if (st || (st = ztc_ctx_activate(ctx))) return st;
+    if (st) return st;
     if (!rgba || w < 1 || h < 1 || stride < (size_t)w * 4 || steps < 0 || steps > 1000 || !(lr >= 0.0f))
         return ztc_set_error(ZTC_ERR_INVALID_ARG, "bad image, steps or learning rate");
     if (floats_misaligned(sse_before, sse_after)) return ztc_set_error(ZTC_ERR_INVALID_ARG, "misaligned SSE outputs");
+    if ((st = ztc_ctx_activate(ctx))) return st;
     const int bw = (w + 3) / 4, nblocks = bw * ((h + 3) / 4);
     ztc::SrcU8 src{rgba, stride, w, h, 4, (((uintptr_t)rgba | stride) & 15u) == 0};
     ztc::TraceScope tr(fmt == ZTC_BC1 ? "refine_bc1" : "refine_bc7", (cudaStream_t)stream);

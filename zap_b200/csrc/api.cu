@@ -70,7 +70,7 @@ void trace_end(cudaStream_t s) {
     cudaEventRecord(r.b, s);
     std::lock_guard<std::mutex> g(g_trace_lock);
     if (r.d_count) {
-        if (!g_slots && cudaMallocHost((void **)&g_slots, kSlots * sizeof(uint32_t)) != cudaSuccess) g_slots = nullptr;
+        if (!g_slots && ztc_malloc_host((void **)&g_slots, kSlots * sizeof(uint32_t)) != cudaSuccess) g_slots = nullptr;
         if (g_slots && g_slot_next < kSlots) {
             uint32_t *slot = g_slots + g_slot_next++;
             *slot = 0;
@@ -200,7 +200,7 @@ int grow(void **p, size_t *cap, size_t need, const char *what) {
     if (*cap >= need) return ZTC_OK;
     if (*p) { cudaFree(*p); *p = nullptr; *cap = 0; }
     size_t n = need + need / 4 + 4096;
-    ZTC_CHECK(cudaMalloc(p, n), what);
+    ZTC_CHECK(ztc_malloc(p, n), what);
     *cap = n;
     return ZTC_OK;
 }
@@ -295,7 +295,7 @@ int dev_encode(zap_tex_cuda_ctx *ctx, int fmt, const ztc::SrcU8 &s8, const ztc::
     const int bh = (h + 3) / 4, bw = (w + 3) / 4;
     const size_t scr = scratch_for(fmt, (size_t)bw * bh);
     void *scratch = nullptr;
-    if (scr) ZTC_CHECK(cudaMallocAsync(&scratch, scr, s), "cudaMallocAsync(scratch)");
+    if (scr) ZTC_CHECK(ztc_malloc_async(&scratch, scr, s), "cudaMallocAsync(scratch)");
     int st = launch_encode(fmt, s8, sh, 0, bh, (uint8_t *)out, scratch, s);
     if (scratch) cudaFreeAsync(scratch, s);
     (void)ctx;
@@ -329,6 +329,34 @@ int check_image(const void *p, const void *out, int w, int h, size_t stride, siz
 }  // namespace
 
 int ztc_set_error(int status, const char *msg) { return fail(status, "%s", msg); }
+
+// ---------------------------------------------------------------- allocations (and the test hook that fails them)
+namespace {
+std::mutex g_alloc_lock;
+long g_alloc_skip = 0, g_alloc_fail = 0;  // let g_alloc_skip allocations through, then fail g_alloc_fail
+bool alloc_fault() {
+    std::lock_guard<std::mutex> g(g_alloc_lock);
+    if (g_alloc_skip > 0) { g_alloc_skip--; return false; }
+    if (g_alloc_fail > 0) { g_alloc_fail--; return true; }
+    return false;
+}
+}  // namespace
+cudaError_t ztc_malloc(void **p, size_t n) {
+    if (alloc_fault()) { *p = nullptr; return cudaErrorMemoryAllocation; }
+    return cudaMalloc(p, n);
+}
+cudaError_t ztc_malloc_async(void **p, size_t n, cudaStream_t s) {
+    if (alloc_fault()) { *p = nullptr; return cudaErrorMemoryAllocation; }
+    return cudaMallocAsync(p, n, s);
+}
+cudaError_t ztc_malloc_host(void **p, size_t n) {
+    if (alloc_fault()) { *p = nullptr; return cudaErrorMemoryAllocation; }
+    return cudaMallocHost(p, n);
+}
+
+#ifdef ZTC_CHECKS
+__device__ unsigned int ztc_check_word = 0u;  // the first failed bounds check of the ZTC_CHECKS build
+#endif
 int ztc_sm_count() {  // SMs of the current device, cached per device (148 on B200; a tuning input only)
     static std::atomic<int> cache[kMaxDevices];
     int dev = 0;
@@ -346,6 +374,30 @@ extern "C" {
 
 int zap_tex_cuda_version(void) { return ZAP_TEX_CUDA_VERSION; }
 
+int zap_tex_cuda_debug_fail_allocations(int skip, int count) {
+    if (skip < 0 || count < 0) return fail(ZTC_ERR_INVALID_ARG, "skip and count must be >= 0");
+    std::lock_guard<std::mutex> g(g_alloc_lock);
+    g_alloc_skip = skip;
+    g_alloc_fail = count;
+    return ZTC_OK;
+}
+
+int zap_tex_cuda_debug_checks(unsigned int *first_failure) {
+    if (!first_failure) return fail(ZTC_ERR_INVALID_ARG, "null first_failure");
+    *first_failure = 0u;
+#ifdef ZTC_CHECKS
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return fail(ZTC_ERR_NO_DEVICE, "no CUDA device"); }
+    ZTC_CHECK(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    ZTC_CHECK(cudaMemcpyFromSymbol(first_failure, ztc_check_word, sizeof(unsigned int)), "read the check word");
+    const unsigned int zero = 0u;
+    ZTC_CHECK(cudaMemcpyToSymbol(ztc_check_word, &zero, sizeof zero), "clear the check word");
+    return ZTC_OK;
+#else
+    return fail(ZTC_ERR_UNSUPPORTED, "this library was built without ZTC_CHECKS (make -C zap_b200/csrc checks)");
+#endif
+}
+
 const char *zap_tex_cuda_status_string(int status) {
     switch (status) {
     case ZTC_OK: return "ok";
@@ -353,7 +405,6 @@ const char *zap_tex_cuda_status_string(int status) {
     case ZTC_ERR_UNSUPPORTED: return "unsupported";
     case ZTC_ERR_CUDA: return "CUDA error";
     case ZTC_ERR_NO_MEMORY: return "out of memory";
-    case ZTC_ERR_TIMEOUT: return "device wait timed out";
     case ZTC_ERR_NO_DEVICE: return "no usable CUDA device";
     default: return "unknown status";
     }
@@ -434,7 +485,7 @@ int zap_tex_cuda_reserve(zap_tex_cuda_ctx *ctx, size_t bytes) {
     uint64_t keep = bytes;
     ZTC_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
     void *p = nullptr;
-    ZTC_CHECK(cudaMallocAsync(&p, bytes ? bytes : 1, ctx->stream[0]), "cudaMallocAsync(reserve)");
+    ZTC_CHECK(ztc_malloc_async(&p, bytes ? bytes : 1, ctx->stream[0]), "cudaMallocAsync(reserve)");
     ZTC_CHECK(cudaFreeAsync(p, ctx->stream[0]), "cudaFreeAsync(reserve)");
     ZTC_CHECK(cudaStreamSynchronize(ctx->stream[0]), "reserve");
     return ZTC_OK;
@@ -612,7 +663,7 @@ int zap_tex_cuda_bc_encode_split_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba,
         return ZTC_OK;
     }
     void *scratch = nullptr;
-    ZTC_CHECK(cudaMallocAsync(&scratch, ztc::bc7_scratch_bytes((size_t)bw * bh), s), "cudaMallocAsync(scratch)");
+    ZTC_CHECK(ztc_malloc_async(&scratch, ztc::bc7_scratch_bytes((size_t)bw * bh), s), "cudaMallocAsync(scratch)");
     cudaError_t e = ztc_launch_bc7_to(s8, 0, bh, planes, 0, scratch, s);
     cudaFreeAsync(scratch, s);
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");

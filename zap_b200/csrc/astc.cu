@@ -446,7 +446,8 @@ __device__ __forceinline__ int astc_single_cta(bool valid, const uint32_t t[16],
                 int base = 0, tk = 0;
                 #pragma unroll
                 for (int w = 0; w < CTA / 32; w++) { const int c = s_wcnt[k][w]; base += w < warp ? c : 0; tk += c; }
-                if ((mores >> k) & 1u) s_list[off + base + __popc(bal[k] & ((1u << lane) - 1u))] = (uint16_t)((tid << 2) | k);
+                const int pos = off + base + __popc(bal[k] & ((1u << lane) - 1u));
+                if (((mores >> k) & 1u) && ZTC_IN_BOUNDS(pos, 3 * CTA, 5)) s_list[pos] = (uint16_t)((tid << 2) | k);
                 off += tk;
             }
             total = off;
@@ -458,6 +459,7 @@ __device__ __forceinline__ int astc_single_cta(bool valid, const uint32_t t[16],
             const int q = tid + (job - 3) * CTA;
             active = q < total;
             if (active) { owner = s_list[q] >> 2; k = s_list[q] & 3; }
+            if (active && !ZTC_IN_BOUNDS(owner, CTA, 8)) active = false;
             first = 2; last = 4;
         }
         if (active) {
@@ -567,7 +569,8 @@ __global__ void __launch_bounds__(128, ZTC_MINB_ASTC_SINGLE) astc_single_kernel(
         uint32_t base = 0;
         if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(ballot));
         base = __shfl_sync(0xFFFFFFFFu, base, leader);
-        if (hard) items[base + __popc(ballot & ((1u << lane) - 1u))] = make_uint2((uint32_t)b, (uint32_t)best);
+        const int pos = (int)base + __popc(ballot & ((1u << lane) - 1u));
+        if (hard && ZTC_IN_BOUNDS(pos, nblocks, 7)) items[pos] = make_uint2((uint32_t)b, (uint32_t)best);
     }
 }
 

@@ -130,7 +130,7 @@ int upload_tiles(zap_tex_cuda_batch *b, int f, ClassPlan p) {
     b->ntiles[f] = (int)t.size();
     b->plan[f] = p;
     if (t.empty()) return ZTC_OK;
-    BCHECK(cudaMalloc(&b->d_tiles[f], t.size() * sizeof(ztc::BatchTile)), "cudaMalloc(tiles)");
+    BCHECK(ztc_malloc((void **)&b->d_tiles[f], t.size() * sizeof(ztc::BatchTile)), "cudaMalloc(tiles)");
     BCHECK(cudaMemcpy(b->d_tiles[f], t.data(), t.size() * sizeof(ztc::BatchTile), cudaMemcpyHostToDevice), "upload tiles");
     const void *fn = f == ZTC_BC7 ? ztc_batch_bc7_kernel_fn(p.cta, p.regs) : ztc_batch_bcn_kernel_fn(f, p.cta, p.regs);
     int per_sm = 1;
@@ -359,7 +359,7 @@ int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *it
         }
     }
     b->mip_bytes = mip_total;
-    if (mip_total) BTRY(cudaMalloc(&b->mip_buf, mip_total), "cudaMalloc(mip levels)");
+    if (mip_total) BTRY(ztc_malloc((void **)&b->mip_buf, mip_total), "cudaMalloc(mip levels)");
     for (size_t k = 0; k < b->levels.size(); k++) {
         HostLevel &hl = b->levels[k];
         if (hl.level == 0) { hl.src = items[hl.item].src; hl.pitch = items[hl.item].stride; }
@@ -381,9 +381,9 @@ int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *it
         }
         ztc::BatchMip *dm = nullptr;
         ztc::BatchMipTile *dt = nullptr;
-        BTRY(cudaMalloc(&dm, std::max<size_t>(1, depth.size()) * sizeof(ztc::BatchMip)), "cudaMalloc(mips)");
+        BTRY(ztc_malloc((void **)&dm, std::max<size_t>(1, depth.size()) * sizeof(ztc::BatchMip)), "cudaMalloc(mips)");
         b->d_mips.push_back(dm);
-        BTRY(cudaMalloc(&dt, std::max<size_t>(1, tiles.size()) * sizeof(ztc::BatchMipTile)), "cudaMalloc(mip tiles)");
+        BTRY(ztc_malloc((void **)&dt, std::max<size_t>(1, tiles.size()) * sizeof(ztc::BatchMipTile)), "cudaMalloc(mip tiles)");
         b->d_mip_tiles.push_back(dt);
         b->n_mip_tiles.push_back((int)tiles.size());
         if (!depth.empty()) BTRY(cudaMemcpy(dm, depth.data(), depth.size() * sizeof(ztc::BatchMip), cudaMemcpyHostToDevice), "upload mips");
@@ -409,13 +409,13 @@ int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *it
     }
     if (bc7_blocks >= ((size_t)1 << 32))
         return fail(ztc_set_error(ZTC_ERR_INVALID_ARG, "batch: more than 2^32 - 1 BC7 blocks in one batch; split it"));
-    BTRY(cudaMalloc(&b->d_levels, dl.size() * sizeof(ztc::BatchLevel)), "cudaMalloc(levels)");
+    BTRY(ztc_malloc((void **)&b->d_levels, dl.size() * sizeof(ztc::BatchLevel)), "cudaMalloc(levels)");
     BTRY(cudaMemcpy(b->d_levels, dl.data(), dl.size() * sizeof(ztc::BatchLevel), cudaMemcpyHostToDevice), "upload levels");
     if (bc7_blocks) {  // BC7 work list: room for every BC7 block of the batch
         b->n_bc7_levels = (int)bc7_bases.size();
-        BTRY(cudaMalloc(&b->d_hard_items, 2 * bc7_blocks * sizeof(uint2)), "cudaMalloc(BC7 work lists)");
-        BTRY(cudaMalloc(&b->d_bc7_bases, bc7_bases.size() * sizeof(uint32_t)), "cudaMalloc(BC7 level bases)");
-        BTRY(cudaMalloc(&b->d_bc7_level_of, bc7_level_of.size() * sizeof(int)), "cudaMalloc(BC7 level map)");
+        BTRY(ztc_malloc((void **)&b->d_hard_items, 2 * bc7_blocks * sizeof(uint2)), "cudaMalloc(BC7 work lists)");
+        BTRY(ztc_malloc((void **)&b->d_bc7_bases, bc7_bases.size() * sizeof(uint32_t)), "cudaMalloc(BC7 level bases)");
+        BTRY(ztc_malloc((void **)&b->d_bc7_level_of, bc7_level_of.size() * sizeof(int)), "cudaMalloc(BC7 level map)");
         BTRY(cudaMemcpy(b->d_bc7_bases, bc7_bases.data(), bc7_bases.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload BC7 bases");
         BTRY(cudaMemcpy(b->d_bc7_level_of, bc7_level_of.data(), bc7_level_of.size() * sizeof(int), cudaMemcpyHostToDevice),
              "upload BC7 level map");
@@ -426,10 +426,10 @@ int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *it
     }
     float tables[512];
     ztc::srgb_tables_host(tables, tables + 256);
-    BTRY(cudaMalloc(&b->d_srgb, sizeof tables), "cudaMalloc(srgb)");
+    BTRY(ztc_malloc((void **)&b->d_srgb, sizeof tables), "cudaMalloc(srgb)");
     BTRY(cudaMemcpy(b->d_srgb, tables, sizeof tables, cudaMemcpyHostToDevice), "upload srgb");
-    BTRY(cudaMalloc(&b->d_counters, 64 * sizeof(uint32_t)), "cudaMalloc(counters)");
-    BTRY(cudaMalloc(&b->plain_scratch, ztc::bc7_scratch_bytes(max_blocks)), "cudaMalloc(plain scratch)");
+    BTRY(ztc_malloc((void **)&b->d_counters, 64 * sizeof(uint32_t)), "cudaMalloc(counters)");
+    BTRY(ztc_malloc((void **)&b->plain_scratch, ztc::bc7_scratch_bytes(max_blocks)), "cudaMalloc(plain scratch)");
     // ---- tiles (autotuned or 128 blocks per CTA)
     int st = ZTC_OK;
     if (flags & ZTC_BATCH_AUTOTUNE) st = autotune(b);

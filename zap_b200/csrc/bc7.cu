@@ -225,10 +225,13 @@ __device__ __forceinline__ int mode6_encode_cta(bool valid, const uint32_t t[16]
         int base = 0, total = 0;
         #pragma unroll
         for (int w = 0; w < CTA / 32; w++) { const int c = s_wcnt[w]; base += w < warp ? c : 0; total += c; }
-        if (more) s_list[base + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)tid;
+        const int pos = base + __popc(bal & ((1u << lane) - 1u));
+        if (more && ZTC_IN_BOUNDS(pos, CTA, 2)) s_list[pos] = (uint16_t)tid;
         __syncthreads();
         active = tid < total;
-        if (active) { owner = s_list[tid]; err = s_err[owner]; idx = s_idx[owner]; }
+        if (active) owner = s_list[tid];
+        if (active && !ZTC_IN_BOUNDS(owner, CTA, 8)) active = false;
+        if (active) { err = s_err[owner]; idx = s_idx[owner]; }
         first = 2;
     }
     __syncthreads();
@@ -269,7 +272,8 @@ __global__ void __launch_bounds__(CTA, mode6_min_ctas<CTA>()) bc7_mode6_kernel(S
         uint32_t base = 0;
         if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(ballot));
         base = __shfl_sync(0xFFFFFFFFu, base, leader);
-        if (hard) items[base + __popc(ballot & ((1u << lane) - 1u))] = make_uint2((uint32_t)b, (uint32_t)err);
+        const int pos = (int)base + __popc(ballot & ((1u << lane) - 1u));
+        if (hard && ZTC_IN_BOUNDS(pos, nblocks, 6)) items[pos] = make_uint2((uint32_t)b, (uint32_t)err);
     }
 }
 

@@ -218,11 +218,13 @@ __device__ __forceinline__ uint2 bc1_encode_cta(bool valid, const uint32_t t[16]
         int base = 0, total = 0;
         #pragma unroll
         for (int w = 0; w < CTA / 32; w++) { const int c = s_wcnt[w]; base += w < warp ? c : 0; total += c; }
-        if (more) s_list[base + __popc(bal & ((1u << lane) - 1u))] = (uint8_t)tid;
+        const int pos = base + __popc(bal & ((1u << lane) - 1u));
+        if (more && ZTC_IN_BOUNDS(pos, CTA, 3)) s_list[pos] = (uint8_t)tid;
         __syncthreads();
         active = tid < total;
+        if (active) owner = s_list[tid];
+        if (active && !ZTC_IN_BOUNDS(owner, CTA, 8)) active = false;
         if (active) {
-            owner = s_list[tid];
             uint32_t u[16];
             #pragma unroll
             for (int i = 0; i < 16; i++) u[i] = s_tex[i][owner];

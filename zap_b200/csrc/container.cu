@@ -106,8 +106,8 @@ int zap_tex_cuda_tex_file(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int
     const size_t total = need - hn;
     cudaStream_t cs = cudaStreamPerThread;
     uint8_t *d_img = nullptr, *d_blocks = nullptr;
-    cudaError_t e = cudaMallocAsync((void **)&d_img, base + chain, cs);
-    if (e == cudaSuccess) e = cudaMallocAsync((void **)&d_blocks, total, cs);
+    cudaError_t e = ztc_malloc_async((void **)&d_img, base + chain, cs);
+    if (e == cudaSuccess) e = ztc_malloc_async((void **)&d_blocks, total, cs);
     if (e == cudaSuccess) e = cudaMemcpy2DAsync(d_img, (size_t)w * 4, rgba, stride, (size_t)w * 4, (size_t)h, cudaMemcpyHostToDevice, cs);
     if (e != cudaSuccess) st = cuda_status(e);
     // levels 1.. of the chain, each zap_mip_next of the one before (zap.c:339-341)

@@ -89,8 +89,8 @@ int host_decode(Kind k, zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, int
     const size_t host_stride = k == kBc6h ? stride * 2 : stride;  // BC6H strides count uint16 elements
     cudaStream_t s = cudaStreamPerThread;
     uint8_t *d_bc = nullptr, *d_px = nullptr;
-    cudaError_t e = cudaMallocAsync((void **)&d_bc, nb, s);
-    if (e == cudaSuccess) e = cudaMallocAsync((void **)&d_px, row * (size_t)h, s);
+    cudaError_t e = ztc_malloc_async((void **)&d_bc, nb, s);
+    if (e == cudaSuccess) e = ztc_malloc_async((void **)&d_px, row * (size_t)h, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_bc, bc, nb, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = launch_decode(k, d_bc, w, h, fmt, d_px, k == kBc6h ? (size_t)w * 4 : row, s);
     if (e == cudaSuccess) e = cudaMemcpy2DAsync(rgba, host_stride, d_px, row, row, (size_t)h, cudaMemcpyDeviceToHost, s);

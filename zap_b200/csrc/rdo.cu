@@ -479,7 +479,7 @@ cudaError_t ztc_launch_rdo(int fmt, const ztc::SrcU8 &src, uint8_t *out, float l
     if (fmt == ZTC_FMT_BC7) {
         const int nblocks = bw * nby;
         uint32_t *dec = nullptr;
-        cudaError_t e = cudaMallocAsync((void **)&dec, (size_t)nblocks * 64, stream);
+        cudaError_t e = ztc_malloc_async((void **)&dec, (size_t)nblocks * 64, stream);
         if (e != cudaSuccess) return e;
         ztc::bc7_decode_bases_kernel<<<(nblocks + 127) / 128, 128, 0, stream>>>(out, nblocks, (uint4 *)dec);
         ztc::rdo_bc7_chain_kernel<<<chains, ztc::kB7Threads, 0, stream>>>(src, bw, nby, band_rows, out, dec, lambda);

@@ -47,6 +47,29 @@
 #define ZTC_MINB_BC6H 5
 #endif
 
+// ---------------------------------------------------------------- bounds checks (the ZTC_CHECKS build)
+// ZTC_IN_BOUNDS(i, n, site) is true when 0 <= i < n. The checks build (-DZTC_CHECKS, relocatable device code,
+// zap_b200/lib/libzap_tex_cuda_checks.so) also records a failure in the device word ztc_check_word, as
+// (site << 24) | (i & 0xFFFFFF), keeping the first one, and the caller skips the access; no kernel traps or waits.
+// zap_tex_cuda_debug_checks reads and clears the word. In the product build every check compiles to `true`.
+// Sites: 1 texel gather, 2 BC7 mode-6 refit list, 3 BC1 climb list, 4 BC6H refit list, 5 ASTC fit list (shared
+// memory), 6 BC7 work list, 7 ASTC work list (global memory), 8 a compacted list's owner (shared memory index).
+#ifdef ZTC_CHECKS
+extern __device__ unsigned int ztc_check_word;
+namespace ztc {
+ZTC_DEV bool in_bounds(long long i, long long n, unsigned site) {
+    const bool ok = i >= 0 && i < n;
+#ifdef __CUDA_ARCH__
+    if (!ok) atomicCAS(&ztc_check_word, 0u, (site << 24) | ((unsigned)i & 0xFFFFFFu));
+#endif
+    return ok;
+}
+}  // namespace ztc
+#define ZTC_IN_BOUNDS(i, n, site) ::ztc::in_bounds((long long)(i), (long long)(n), (site))
+#else
+#define ZTC_IN_BOUNDS(i, n, site) true
+#endif
+
 namespace ztc {
 
 #ifdef __CUDA_ARCH__
@@ -193,6 +216,10 @@ ZTC_DEV uint32_t load_texel(const SrcU8 &s, int x, int y) {
 // 16 texels of block (bx, by), texel i at (i & 3, i >> 2), clamped to the image like the reference
 ZTC_DEV void gather_block(const SrcU8 &s, int bx, int by, uint32_t t[16]) {
     int x0 = bx * 4, y0 = by * 4;
+    if (!ZTC_IN_BOUNDS(x0, s.w, 1) || !ZTC_IN_BOUNDS(y0, s.h, 1)) {  // a block outside the image: nothing is read
+        for (int i = 0; i < 16; i++) t[i] = 0;
+        return;
+    }
     if (s.vec16 && x0 + 3 < s.w && y0 + 3 < s.h) {
         #pragma unroll
         for (int r = 0; r < 4; r++) {

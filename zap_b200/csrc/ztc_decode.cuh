@@ -28,12 +28,12 @@ constexpr uint32_t p3(const char *s) {
     return v;
 }
 // partitions (format spec): two-subset masks (bit i = subset 1) and three-subset rows (texel 0 first)
-__constant__ uint16_t kP2d[64] = {
+static __constant__ uint16_t kP2d[64] = {
     0xCCCC, 0x8888, 0xEEEE, 0xECC8, 0xC880, 0xFEEC, 0xFEC8, 0xEC80, 0xC800, 0xFFEC, 0xFE80, 0xE800, 0xFFE8, 0xFF00, 0xFFF0, 0xF000,
     0xF710, 0x008E, 0x7100, 0x08CE, 0x008C, 0x7310, 0x3100, 0x8CCE, 0x088C, 0x3110, 0x6666, 0x366C, 0x17E8, 0x0FF0, 0x718E, 0x399C,
     0xAAAA, 0xF0F0, 0x5A5A, 0x33CC, 0x3C3C, 0x55AA, 0x9696, 0xA55A, 0x73CE, 0x13C8, 0x324C, 0x3BDC, 0x6996, 0xC33C, 0x9966, 0x0660,
     0x0272, 0x04E4, 0x4E40, 0x2720, 0xC936, 0x936C, 0x39C6, 0x639C, 0x9336, 0x9CC6, 0x817E, 0xE718, 0xCCF0, 0x0FCC, 0x7744, 0xEE22};
-__constant__ uint32_t kP3d[64] = {
+static __constant__ uint32_t kP3d[64] = {
     p3("0011001102212222"), p3("0001001122112221"), p3("0000200122112211"), p3("0222002200110111"), p3("0000000011221122"),
     p3("0011001100220022"), p3("0022002211111111"), p3("0011001122112211"), p3("0000000011112222"), p3("0000111111112222"),
     p3("0000111122222222"), p3("0012001200120012"), p3("0112011201120112"), p3("0122012201220122"), p3("0011011211221222"),
@@ -48,13 +48,13 @@ __constant__ uint32_t kP3d[64] = {
     p3("0000000021122112"), p3("0110011022222222"), p3("0022001100110022"), p3("0022112211220022"), p3("0000000000002112"),
     p3("0002000100020001"), p3("0222122202221222"), p3("0101222222222222"), p3("0111201122012220")};
 // anchor texels (format spec): subset 1 of two, subsets 1 and 2 of three
-__constant__ uint8_t kA2d[64] = {
+static __constant__ uint8_t kA2d[64] = {
     15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 2, 8, 2, 2, 8, 8, 15, 2, 8, 2, 2, 8, 8, 2, 2,
     15, 15, 6, 8, 2, 8, 15, 15, 2, 8, 2, 2, 2, 15, 15, 6, 6, 2, 6, 8, 15, 15, 2, 2, 15, 15, 15, 15, 15, 2, 2, 15};
-__constant__ uint8_t kA3ad[64] = {
+static __constant__ uint8_t kA3ad[64] = {
     3, 3, 15, 15, 8, 3, 15, 15, 8, 8, 6, 6, 6, 5, 3, 3, 3, 3, 8, 15, 3, 3, 6, 10, 5, 8, 8, 6, 8, 5, 15, 15,
     8, 15, 3, 5, 6, 10, 8, 15, 15, 3, 15, 5, 15, 15, 15, 15, 3, 15, 5, 5, 5, 8, 5, 10, 5, 10, 8, 13, 15, 12, 3, 3};
-__constant__ uint8_t kA3bd[64] = {
+static __constant__ uint8_t kA3bd[64] = {
     15, 8, 8, 3, 15, 15, 3, 8, 15, 15, 15, 15, 15, 15, 15, 8, 15, 8, 15, 3, 15, 8, 15, 8, 3, 15, 6, 10, 15, 15, 10, 8,
     15, 3, 15, 10, 10, 8, 9, 10, 6, 15, 8, 15, 3, 6, 6, 8, 15, 3, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 3, 15, 15, 8};
 

@@ -90,6 +90,13 @@ const void *ztc_batch_bc7_hard_kernel_fn();
 const void *ztc_batch_mip_kernel_fn();
 namespace ztc { void srgb_tables_host(float lin[256], float thr[256]); }
 
+// Every device and pinned-host allocation of the library goes through these (api.cu), so a test can make chosen
+// ones fail (zap_tex_cuda_debug_fail_allocations) and check that each entry point reports ZTC_ERR_NO_MEMORY and the
+// library keeps working afterwards.
+cudaError_t ztc_malloc(void **p, size_t n);
+cudaError_t ztc_malloc_async(void **p, size_t n, cudaStream_t s);
+cudaError_t ztc_malloc_host(void **p, size_t n);
+
 // records the calling thread's error message (zap_tex_cuda_last_error) and returns status
 int ztc_set_error(int status, const char *msg);
 // makes ctx's device current (NULL: the current device's default context) with its tables uploaded
