@@ -305,11 +305,19 @@ ZTC_DEV uint32_t part_texel(uint32_t v, int rot, bool alpha) {
     const uint32_t r = rotate_texel(v, rot);
     return alpha ? (r >> 24) : (r & 0x00FFFFFFu);
 }
+// The mode 5 helpers take the part as KIND: kPartRuntime (the `alpha` argument decides, so the colour and alpha
+// lanes of an 8-lane group run one code path), kPartColour or kPartAlpha (the part fixed at compile time: the alpha
+// part's loops shrink to its one channel). All three compute the same values for the same part.
+constexpr int kPartRuntime = 0, kPartColour = 1, kPartAlpha = 2;
+template <int KIND>
+ZTC_DEV bool part_is_alpha(bool alpha) { return KIND == kPartRuntime ? alpha : KIND == kPartAlpha; }
+
+template <int KIND = kPartRuntime>
 ZTC_DEV void m5_quant(const float v[3], int nc, int n, int q[3], int x8[3]) {
     const int top = (1 << n) - 1;
     #pragma unroll
     for (int c = 0; c < 3; c++) {
-        if (c >= nc) { q[c] = 0; x8[c] = 0; continue; }
+        if (c >= nc || (KIND == kPartAlpha && c > 0)) { q[c] = 0; x8[c] = 0; continue; }
         int g = f2i_x86(div255(v[c] * (float)top) + 0.5f), bq = 0, bd = 1 << 30;
         #pragma unroll
         for (int k = 0; k < 3; k++) {
@@ -320,14 +328,16 @@ ZTC_DEV void m5_quant(const float v[3], int nc, int n, int q[3], int x8[3]) {
         q[c] = bq; x8[c] = expand_bits(bq, n);
     }
 }
+template <int KIND = kPartRuntime>
 ZTC_DEV int m5_fit(TexRef ts, int rot, bool alpha, const int x0[3], const int x1[3], uint32_t &idx) {
+    alpha = part_is_alpha<KIND>(alpha);
     uint32_t pal[4];
     int A[4];
     #pragma unroll
     for (int j = 0; j < 4; j++) {
         uint32_t e = 0;
         #pragma unroll
-        for (int c = 0; c < 3; c++) e |= (uint32_t)lerp64(x0[c], x1[c], w2(j)) << (8 * c);
+        for (int c = 0; c < (KIND == kPartAlpha ? 1 : 3); c++) e |= (uint32_t)lerp64(x0[c], x1[c], w2(j)) << (8 * c);
         pal[j] = e; A[j] = (int)dot4(e, e) * 4 + j;
     }
     int err = 0;
@@ -343,34 +353,47 @@ ZTC_DEV int m5_fit(TexRef ts, int rot, bool alpha, const int x0[3], const int x1
     idx = bits;
     return err;
 }
+// Least-squares endpoints for fixed 2-bit indices (zap_tex.h:636-648). The reference sums floats, but every one of
+// its sums is exact: w = k / 64 with k in {0, 21, 43, 64} and u = 1 - w, so u*u, u*w and w*w are multiples of 2^-12
+// below 1, u*x and w*x multiples of 2^-6 below 256, and no partial sum of 16 terms needs more than 24 bits in those
+// units. Integer sums scaled by 2^-12 and 2^-6 are therefore the reference's floats, bit for bit, in any order.
+template <int KIND = kPartRuntime>
 ZTC_DEV bool m5_lsq(TexRef ts, int rot, bool alpha, int nc, uint32_t idx, float lo[3], float hi[3]) {
-    float aa = 0.0f, ab = 0.0f, bb = 0.0f, sa[3] = {0.0f, 0.0f, 0.0f}, sb[3] = {0.0f, 0.0f, 0.0f};
+    alpha = part_is_alpha<KIND>(alpha);
+    constexpr int kC = KIND == kPartAlpha ? 1 : 3;
+    int aa = 0, ab = 0, bb = 0, sa[3] = {0, 0, 0}, sb[3] = {0, 0, 0};
     #pragma unroll 1
     for (int i = 0; i < 16; i++) {
-        float w = (float)w2((int)((idx >> (2 * i)) & 3u)) / 64.0f, u = 1.0f - w;
-        aa = aa + u * u; ab = ab + u * w; bb = bb + w * w;
+        const int k = (int)((0x402B1500u >> (8 * ((idx >> (2 * i)) & 3u))) & 0xFFu), u = 64 - k;  // w2: 0, 21, 43, 64
+        aa += u * u; ab += u * k; bb += k * k;
         const uint32_t p = part_texel(ts[i], rot, alpha);
         #pragma unroll
-        for (int c = 0; c < 3; c++) { float x = (float)chan(p, c); sa[c] = sa[c] + u * x; sb[c] = sb[c] + w * x; }
+        for (int c = 0; c < kC; c++) { const int x = (int)chan(p, c); sa[c] += u * x; sb[c] += k * x; }
     }
-    float det = aa * bb - ab * ab;
+    const float faa = (float)aa * (1.0f / 4096.0f), fab = (float)ab * (1.0f / 4096.0f), fbb = (float)bb * (1.0f / 4096.0f);
+    float det = faa * fbb - fab * fab;
     if (det < 1e-6f && det > -1e-6f) return false;
     #pragma unroll
-    for (int c = 0; c < 3; c++)
-        if (c < nc) { lo[c] = clamp255((sa[c] * bb - sb[c] * ab) / det); hi[c] = clamp255((sb[c] * aa - sa[c] * ab) / det); }
+    for (int c = 0; c < kC; c++)
+        if (c < nc) {
+            const float fa = (float)sa[c] * (1.0f / 64.0f), fb = (float)sb[c] * (1.0f / 64.0f);
+            lo[c] = clamp255((fa * fbb - fb * fab) / det); hi[c] = clamp255((fb * faa - fa * fab) / det);
+        }
     return true;
 }
 // quantise, fit, up to two least-squares refits (zap_tex.h:626-657); lo / hi: the start endpoints
+template <int KIND = kPartRuntime>
 ZTC_DEV int m5_part(TexRef ts, int rot, bool alpha, float lo[3], float hi[3], int q[2][3], uint32_t &idx) {
+    alpha = part_is_alpha<KIND>(alpha);
     const int nc = alpha ? 1 : 3, n = alpha ? 8 : 7;
     int err = 0;
     #pragma unroll 1
     for (int it = 0; it < 3; it++) {
-        if (it > 0 && !m5_lsq(ts, rot, alpha, nc, idx, lo, hi)) break;
+        if (it > 0 && !m5_lsq<KIND>(ts, rot, alpha, nc, idx, lo, hi)) break;
         int tq[2][3], x0[3], x1[3];
-        m5_quant(lo, nc, n, tq[0], x0); m5_quant(hi, nc, n, tq[1], x1);
+        m5_quant<KIND>(lo, nc, n, tq[0], x0); m5_quant<KIND>(hi, nc, n, tq[1], x1);
         uint32_t ti;
-        const int e = m5_fit(ts, rot, alpha, x0, x1, ti);
+        const int e = m5_fit<KIND>(ts, rot, alpha, x0, x1, ti);
         if (it > 0 && e >= err) break;
         err = e; idx = ti;
         #pragma unroll
@@ -662,21 +685,150 @@ __device__ __forceinline__ TexRef stage_group_texels(uint32_t *gtex, const uint3
     return TexRef{gtex, 1};
 }
 
-__global__ void __launch_bounds__(128, ZTC_MINB_BC7_HARD) bc7_hard_kernel(SrcU8 src, int bw, int by0, BlockOut out, size_t b0,
-                                                       const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
-    __shared__ uint32_t s_gtex[128 / kBc7Group][17];  // per group (padded: the four groups of a warp hit distinct banks)
-    const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
-    const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
-    const int ngroups = gridDim.x * (blockDim.x / kBc7Group);
-    const int n = (int)*(volatile const uint32_t *)count;
-    uint32_t *gtex = s_gtex[threadIdx.x / kBc7Group];
-    for (int it = blockIdx.x * (blockDim.x / kBc7Group) + (threadIdx.x / kBc7Group); it < n; it += ngroups) {
-        const uint2 item = items[it];
-        const int b = (int)item.x;
-        uint32_t t[16];
-        gather_block(src, b % bw, by0 + b / bw, t);
-        bc7_group_block(t, stage_group_texels(gtex, t, l, gmask), (int)item.y, out, b0 + (size_t)b, l, gmask);
+// Modes 5 and 1 of single-image encodes over the mode-6 work list. A CTA of two warps takes 8 listed blocks at a
+// time: warp 0 fits their mode-5 colour parts and warp 1 their alpha parts, lane = block * 4 + rotation, each warp
+// on code specialised to its part (no lane of a warp waits on the other part's branch, and the alpha part's loops
+// run over its one channel); the best rotation of each block is then chosen as the reference does, and mode 1 runs
+// for the opaque ones, an 8-lane group per block.
+constexpr int kHardBlocks = 8;
+
+__device__ __forceinline__ int m5_colour_lane(TexRef ts, int rot, uint32_t &qw, uint32_t &qw2, uint32_t &idx) {
+    uint32_t r[16];
+    #pragma unroll
+    for (int i = 0; i < 16; i++) r[i] = rotate_texel(ts[i], rot);
+    float lo[4], hi[4];
+    pca_endpoints<3>(r, 0xFFFFu, lo, hi);  // the colour part starts from the principal axis of the rotated RGB
+    float lo5[3] = {lo[0], lo[1], lo[2]}, hi5[3] = {hi[0], hi[1], hi[2]};
+    int q5[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    uint32_t i5 = 0;
+    const int e5 = m5_part<kPartColour>(ts, rot, false, lo5, hi5, q5, i5);
+    if (i5 & 2u) {  // anchor MSB must be 0 (zap_tex.h:673-674): swap, 3 - i == i ^ 3 for 2-bit indices
+        #pragma unroll
+        for (int c = 0; c < 3; c++) { int t = q5[0][c]; q5[0][c] = q5[1][c]; q5[1][c] = t; }
+        i5 ^= 0xFFFFFFFFu;
     }
+    qw = (uint32_t)q5[0][0] | ((uint32_t)q5[0][1] << 7) | ((uint32_t)q5[0][2] << 14) | ((uint32_t)q5[1][0] << 21);
+    qw2 = (uint32_t)q5[1][1] | ((uint32_t)q5[1][2] << 7);
+    idx = i5;
+    return e5;
+}
+
+__device__ __forceinline__ int m5_alpha_lane(TexRef ts, int rot, uint32_t &qw, uint32_t &idx) {
+    float lo5[3] = {255.0f, 0.0f, 0.0f}, hi5[3] = {0.0f, 0.0f, 0.0f};
+    #pragma unroll 1
+    for (int i = 0; i < 16; i++) {  // the alpha part starts from the rotated alpha's range
+        const float a = (float)(rotate_texel(ts[i], rot) >> 24);
+        if (a < lo5[0]) lo5[0] = a;
+        if (a > hi5[0]) hi5[0] = a;
+    }
+    int q5[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    uint32_t i5 = 0;
+    const int e5 = m5_part<kPartAlpha>(ts, rot, true, lo5, hi5, q5, i5);
+    if (i5 & 2u) {
+        int t = q5[0][0]; q5[0][0] = q5[1][0]; q5[1][0] = t;
+        i5 ^= 0xFFFFFFFFu;
+    }
+    qw = (uint32_t)q5[0][0] | ((uint32_t)q5[1][0] << 8);
+    idx = i5;
+    return e5;
+}
+
+__global__ void __launch_bounds__(64, 8) bc7_hard_kernel(SrcU8 src, int bw, int by0, BlockOut out, size_t b0,
+                                                        const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
+    __shared__ uint32_t s_tex[kHardBlocks][17];  // per block (padded: the groups of a warp hit distinct banks)
+    __shared__ uint2 s_item[kHardBlocks];        // (block index, mode-6 SSE); x = ~0 past the list's end
+    __shared__ int s_cerr[kHardBlocks][4], s_aerr[kHardBlocks][4];
+    __shared__ uint32_t s_cq[kHardBlocks][4], s_cq2[kHardBlocks][4], s_ci[kHardBlocks][4], s_aq[kHardBlocks][4], s_ai[kHardBlocks][4];
+    __shared__ int s_err[kHardBlocks];
+    __shared__ uint4 s_blk[kHardBlocks];
+    __shared__ int s_take[kHardBlocks];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = (int)*(volatile const uint32_t *)count;
+    for (int base = blockIdx.x * kHardBlocks; base < n; base += gridDim.x * kHardBlocks) {
+        if (tid < kHardBlocks) {  // one thread per block gathers its texels (16-byte row loads)
+            const int it = base + tid;
+            uint2 item = make_uint2(0xFFFFFFFFu, 0u);
+            if (it < n) {
+                item = items[it];
+                uint32_t t[16];
+                gather_block(src, (int)item.x % bw, by0 + (int)item.x / bw, t);
+                #pragma unroll
+                for (int i = 0; i < 16; i++) s_tex[tid][i] = t[i];
+            }
+            s_item[tid] = item;
+        }
+        __syncthreads();
+        {  // ---- mode 5 parts (zap_tex.h:659-684): warp 0 colour, warp 1 alpha; lane = block * 4 + rotation
+            const int blk = lane >> 2, rot = lane & 3;
+            if (s_item[blk].x != 0xFFFFFFFFu) {
+                const TexRef ts{s_tex[blk], 1};
+                uint32_t qw = 0, qw2 = 0, idx = 0;
+                if (warp == 0) {
+                    s_cerr[blk][rot] = m5_colour_lane(ts, rot, qw, qw2, idx);
+                    s_cq[blk][rot] = qw; s_cq2[blk][rot] = qw2; s_ci[blk][rot] = idx;
+                } else {
+                    s_aerr[blk][rot] = m5_alpha_lane(ts, rot, qw, idx);
+                    s_aq[blk][rot] = qw; s_ai[blk][rot] = idx;
+                }
+            }
+        }
+        __syncthreads();
+        if (tid < kHardBlocks && s_item[tid].x != 0xFFFFFFFFu) {  // the best rotation: (SSE, rotation) lexicographic
+            uint32_t key = 0xFFFFFFFFu;
+            #pragma unroll
+            for (int r = 0; r < 4; r++) key = min(key, ((uint32_t)(s_cerr[tid][r] + s_aerr[tid][r]) << 2) | (uint32_t)r);
+            const int brot = (int)(key & 3u), best5 = (int)(key >> 2);
+            int err = (int)s_item[tid].y;
+            const bool take5 = best5 < err;  // decoded SSE == fit SSE (see the file header)
+            uint4 blk = make_uint4(0, 0, 0, 0);
+            if (take5) {
+                err = best5;
+                const uint32_t cq = s_cq[tid][brot], cq2 = s_cq2[tid][brot], ci = s_ci[tid][brot], aq = s_aq[tid][brot], ai = s_ai[tid][brot];
+                Bits128 o;
+                o.put(1u << 5, 6);
+                o.put((uint32_t)brot, 2);
+                const uint32_t c0[3] = {cq & 127u, (cq >> 7) & 127u, (cq >> 14) & 127u}, c1[3] = {(cq >> 21) & 127u, cq2 & 127u, (cq2 >> 7) & 127u};
+                #pragma unroll
+                for (int c = 0; c < 3; c++) { o.put(c0[c], 7); o.put(c1[c], 7); }
+                o.put(aq & 255u, 8); o.put((aq >> 8) & 255u, 8);
+                o.put(ci & 1u, 1);
+                #pragma unroll
+                for (int i = 1; i < 16; i++) o.put((ci >> (2 * i)) & 3u, 2);
+                o.put(ai & 1u, 1);
+                #pragma unroll
+                for (int i = 1; i < 16; i++) o.put((ai >> (2 * i)) & 3u, 2);
+                blk = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
+            }
+            s_err[tid] = err; s_blk[tid] = blk; s_take[tid] = take5;
+        }
+        __syncthreads();
+        {  // ---- mode 1 of the opaque blocks (zap_tex.h:764-783): an 8-lane group per block
+            const int g = tid / kBc7Group, l = tid & (kBc7Group - 1);
+            const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
+            const uint2 item = s_item[g];
+            if (item.x != 0xFFFFFFFFu) {
+                uint32_t t[16];
+                #pragma unroll
+                for (int i = 0; i < 16; i++) t[i] = s_tex[g][i];
+                int err = s_err[g];
+                uint4 blk = s_blk[g];
+                bool take = s_take[g] != 0;
+                if (block_opaque(t) && bc7_group_mode1(t, TexRef{s_tex[g], 1}, err, blk, l, gmask)) take = true;  // group-uniform
+                if (take && l == 0) put_block16(out, b0 + (size_t)item.x, blk);
+            }
+        }
+        __syncthreads();  // the next round overwrites the shared arrays
+    }
+}
+
+// the modes-5/1 launch over a work list of at most nblocks items
+cudaError_t launch_hard(const SrcU8 &src, int bw, int by0, int nblocks, const BlockOut &out, size_t b0, const uint32_t *count,
+                        const uint2 *items, cudaStream_t s) {
+    int ctas = (nblocks + kHardBlocks - 1) / kHardBlocks;
+    const int cap = ztc_sm_count() * 8;
+    ctas = ctas < cap ? ctas : cap;
+    bc7_hard_kernel<<<ctas, 64, 0, s>>>(src, bw, by0, out, b0, count, items);
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- batched: tile queue, then one batch-wide list
@@ -838,16 +990,9 @@ cudaError_t ztc_launch_bc7_to(const ztc::SrcU8 &src, int by0, int nby, const ztc
         e = ztc::launch_mode6(src, bw, by0, nblocks, out, b0, count, items, stream);
         if (e != cudaSuccess) return e;  // launch_mode6 read (and cleared) the launch error; the list is not valid
     }
-    int groups_per_cta = 128 / ztc::kBc7Group;
-    int ctas = (nblocks + groups_per_cta - 1) / groups_per_cta;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    ctas = ctas < sms * 8 ? ctas : sms * 8;
     ztc::TraceScope tr("bc7_modes51", stream);
     ztc::trace_units_dev(count, stream);
-    ztc::bc7_hard_kernel<<<ctas, 128, 0, stream>>>(src, bw, by0, out, b0, count, items);
-    return cudaGetLastError();
+    return ztc::launch_hard(src, bw, by0, nblocks, out, b0, count, items, stream);
 }
 
 cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out, void *scratch, cudaStream_t stream) {
@@ -911,14 +1056,7 @@ extern "C" __attribute__((visibility("default"))) int zap_tex_cuda_bc7_encode_no
     const ztc::BlockOut blocks{(uint8_t *)out, 0, ZTC_FMT_BC7, 0};
     cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), s);  // the list must start empty on every call
     if (e == cudaSuccess) e = ztc::launch_mode6(src, (int)bw, 0, nblocks, blocks, 0, count, items, s);
-    if (e == cudaSuccess) {  // modes 5/1 run only over a list that mode 6 has filled
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        int ctas = (nblocks + 15) / 16;
-        ctas = ctas < sms * 8 ? ctas : sms * 8;
-        ztc::bc7_hard_kernel<<<ctas, 128, 0, s>>>(src, (int)bw, 0, blocks, 0, count, items);
-        e = cudaGetLastError();
-    }
+    if (e == cudaSuccess) e = ztc::launch_hard(src, (int)bw, 0, nblocks, blocks, 0, count, items, s);  // over the list mode 6 filled
     if (e != cudaSuccess) { cudaGetLastError(); return ztc_set_error(ZTC_ERR_CUDA, cudaGetErrorString(e)); }
     return ZTC_OK;
 }
