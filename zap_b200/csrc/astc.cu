@@ -10,6 +10,8 @@
 // Tables the reference rebuilds on every call (zap_tex.h:1293-1305) are built once per device.
 #include <cstring>
 
+#include <cstddef>
+
 #include "ztc_common.cuh"
 #include "ztc_internal.h"
 #include "ztc_pca.cuh"
@@ -40,6 +42,9 @@ struct AstcTables {
     int pat_count;
 };
 __constant__ AstcTables kAstc;
+// the same tables in global memory: the kernels stage them into shared memory once per CTA, each thread reading
+// consecutive words (coalesced loads; the constant cache would serialise the threads' different addresses)
+__device__ AstcTables gAstc;
 
 ZTC_DEV int ise_bits(const IseRange &r, int n) { return n * r.bits + (r.trit ? (8 * n + 4) / 5 : r.quint ? (7 * n + 2) / 3 : 0); }
 // the largest range with at least 6 levels whose nvals values fit in avail bits (zap_tex.h:996-999)
@@ -163,24 +168,29 @@ cudaError_t upload_astc_tables() {
     static AstcTables T;
     static bool built = false;
     if (!built) { build_tables(T); built = true; }
-    return cudaMemcpyToSymbol(kAstc, &T, sizeof T);
+    cudaError_t e = cudaMemcpyToSymbol(kAstc, &T, sizeof T);
+    return e == cudaSuccess ? cudaMemcpyToSymbol(gAstc, &T, sizeof T) : e;
 }
 
 // ---------------------------------------------------------------- device pieces
-struct AstcSmem {
+struct __align__(16) AstcSmem {  // staged as 32-bit words
     uint8_t q[8][256], uq[8][256];
     AstcCfg cfg[8];
     uint8_t trit_code[256], quint_code[128];
     uint8_t wq[4][32];
 };
 
+static_assert(offsetof(AstcTables, q) % 4 == 0 && offsetof(AstcTables, trit_code) % 4 == 0 && offsetof(AstcTables, quint_code) % 4 == 0 &&
+                  offsetof(AstcTables, wq) % 4 == 0 && offsetof(AstcTables, pat_mask) % 4 == 0 && offsetof(AstcTables, pat_seed) % 4 == 0 &&
+                  offsetof(AstcSmem, trit_code) % 4 == 0 && offsetof(AstcSmem, quint_code) % 4 == 0 && offsetof(AstcSmem, wq) % 4 == 0,
+              "the tables are staged as 32-bit words");
 __device__ __forceinline__ void load_smem(AstcSmem &S) {
-    const uint32_t *src = (const uint32_t *)&kAstc.q[0][0];
+    const uint32_t *src = (const uint32_t *)&gAstc.q[0][0];
     uint32_t *dst = (uint32_t *)&S.q[0][0];
-    for (int k = threadIdx.x; k < (int)(sizeof(S.q) + sizeof(S.uq)) / 4; k += blockDim.x) dst[k] = src[k];
-    for (int k = threadIdx.x; k < 256; k += blockDim.x) S.trit_code[k] = kAstc.trit_code[k];
-    for (int k = threadIdx.x; k < 128; k += blockDim.x) S.quint_code[k] = kAstc.quint_code[k];
-    for (int k = threadIdx.x; k < 128; k += blockDim.x) (&S.wq[0][0])[k] = (&kAstc.wq[0][0])[k];
+    for (int k = threadIdx.x; k < (int)(sizeof(S.q) + sizeof(S.uq)) / 4; k += blockDim.x) dst[k] = __ldg(src + k);
+    for (int k = threadIdx.x; k < 256 / 4; k += blockDim.x) ((uint32_t *)S.trit_code)[k] = __ldg((const uint32_t *)gAstc.trit_code + k);
+    for (int k = threadIdx.x; k < 128 / 4; k += blockDim.x) ((uint32_t *)S.quint_code)[k] = __ldg((const uint32_t *)gAstc.quint_code + k);
+    for (int k = threadIdx.x; k < 128 / 4; k += blockDim.x) ((uint32_t *)&S.wq[0][0])[k] = __ldg((const uint32_t *)&gAstc.wq[0][0] + k);
     if (threadIdx.x < 8) S.cfg[threadIdx.x] = kAstc.cfg[threadIdx.x];
 }
 
@@ -627,18 +637,25 @@ constexpr int kAstcGroup = 8;
 __global__ void __launch_bounds__(128) astc_two_part_kernel(SrcU8 src, int bw, int by0, uint8_t *__restrict__ out,
                                                             const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
     __shared__ AstcSmem S;
-    __shared__ uint16_t pmask[1024], pseed[1024];
+    __shared__ __align__(16) uint16_t pmask[1024], pseed[1024];  // staged as 32-bit words
     __shared__ uint32_t s_tex[128 / kAstcGroup][17];  // per group: its block's texels (padded: no bank conflicts)
+    // listed blocks go to the CTAs in turn (group g of CTA c takes items c, c + grid, ... of its share), so a short
+    // list spreads over every SM, and CTAs with nothing to do leave before staging the tables
+    const int n = (int)*(volatile const uint32_t *)count;
+    if ((int)blockIdx.x >= n) return;
     load_smem(S);
     const int npat = kAstc.pat_count;
-    for (int k = threadIdx.x; k < npat; k += blockDim.x) { pmask[k] = kAstc.pat_mask[k]; pseed[k] = kAstc.pat_seed[k]; }
+    for (int k = threadIdx.x; k < npat / 2; k += blockDim.x) {
+        ((uint32_t *)pmask)[k] = __ldg((const uint32_t *)gAstc.pat_mask + k);
+        ((uint32_t *)pseed)[k] = __ldg((const uint32_t *)gAstc.pat_seed + k);
+    }
+    if ((npat & 1) && threadIdx.x == 0) { pmask[npat - 1] = gAstc.pat_mask[npat - 1]; pseed[npat - 1] = gAstc.pat_seed[npat - 1]; }
     __syncthreads();
     const int lane = threadIdx.x & 31, l = lane & (kAstcGroup - 1);
     const unsigned gmask = 0xFFu << (lane & ~(kAstcGroup - 1));
     const int ngroups = gridDim.x * (blockDim.x / kAstcGroup);
-    const int n = (int)*(volatile const uint32_t *)count;
     uint32_t *gtex = s_tex[threadIdx.x / kAstcGroup];
-    for (int it = blockIdx.x * (blockDim.x / kAstcGroup) + (threadIdx.x / kAstcGroup); it < n; it += ngroups) {
+    for (int it = (threadIdx.x / kAstcGroup) * gridDim.x + blockIdx.x; it < n; it += ngroups) {
         const uint2 item = items[it];
         const int b = (int)item.x, best = (int)item.y;
         uint32_t t[16];
