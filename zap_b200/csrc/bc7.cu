@@ -305,14 +305,14 @@ ZTC_DEV uint32_t part_texel(uint32_t v, int rot, bool alpha) {
     const uint32_t r = rotate_texel(v, rot);
     return alpha ? (r >> 24) : (r & 0x00FFFFFFu);
 }
-// The mode 5 helpers take the part as KIND: kPartRuntime (the `alpha` argument decides, so the colour and alpha
-// lanes of an 8-lane group run one code path), kPartColour or kPartAlpha (the part fixed at compile time: the alpha
-// part's loops shrink to its one channel). All three compute the same values for the same part.
-constexpr int kPartRuntime = 0, kPartColour = 1, kPartAlpha = 2;
+// The mode 5 helpers take the part at compile time, KIND = kPartColour (rotated RGB, 7-bit endpoints) or kPartAlpha
+// (rotated A, 8-bit endpoints): the alpha part's loops run over its one channel. The `alpha` and `nc` arguments
+// restate the part for the shared code below.
+constexpr int kPartColour = 1, kPartAlpha = 2;
 template <int KIND>
-ZTC_DEV bool part_is_alpha(bool alpha) { return KIND == kPartRuntime ? alpha : KIND == kPartAlpha; }
+ZTC_DEV bool part_is_alpha(bool) { return KIND == kPartAlpha; }
 
-template <int KIND = kPartRuntime>
+template <int KIND>
 ZTC_DEV void m5_quant(const float v[3], int nc, int n, int q[3], int x8[3]) {
     const int top = (1 << n) - 1;
     #pragma unroll
@@ -328,7 +328,7 @@ ZTC_DEV void m5_quant(const float v[3], int nc, int n, int q[3], int x8[3]) {
         q[c] = bq; x8[c] = expand_bits(bq, n);
     }
 }
-template <int KIND = kPartRuntime>
+template <int KIND>
 ZTC_DEV int m5_fit(TexRef ts, int rot, bool alpha, const int x0[3], const int x1[3], uint32_t &idx) {
     alpha = part_is_alpha<KIND>(alpha);
     uint32_t pal[4];
@@ -357,7 +357,7 @@ ZTC_DEV int m5_fit(TexRef ts, int rot, bool alpha, const int x0[3], const int x1
 // its sums is exact: w = k / 64 with k in {0, 21, 43, 64} and u = 1 - w, so u*u, u*w and w*w are multiples of 2^-12
 // below 1, u*x and w*x multiples of 2^-6 below 256, and no partial sum of 16 terms needs more than 24 bits in those
 // units. Integer sums scaled by 2^-12 and 2^-6 are therefore the reference's floats, bit for bit, in any order.
-template <int KIND = kPartRuntime>
+template <int KIND>
 ZTC_DEV bool m5_lsq(TexRef ts, int rot, bool alpha, int nc, uint32_t idx, float lo[3], float hi[3]) {
     alpha = part_is_alpha<KIND>(alpha);
     constexpr int kC = KIND == kPartAlpha ? 1 : 3;
@@ -382,7 +382,7 @@ ZTC_DEV bool m5_lsq(TexRef ts, int rot, bool alpha, int nc, uint32_t idx, float 
     return true;
 }
 // quantise, fit, up to two least-squares refits (zap_tex.h:626-657); lo / hi: the start endpoints
-template <int KIND = kPartRuntime>
+template <int KIND>
 ZTC_DEV int m5_part(TexRef ts, int rot, bool alpha, float lo[3], float hi[3], int q[2][3], uint32_t &idx) {
     alpha = part_is_alpha<KIND>(alpha);
     const int nc = alpha ? 1 : 3, n = alpha ? 8 : 7;
@@ -449,75 +449,9 @@ ZTC_DEV bool rank_less(float e, int p, float e2, int p2) { return e < e2 || (!(e
 constexpr int kBc7Group = 8;
 constexpr int kMode1Tries = 4;  // partitions fully fitted after ranking (ZAP__BC7_M1K, zap_tex.h:750-752)
 
-// Mode 5 of one block (zap_tex.h:659-684) by the 8 lanes of a group (lane l, group mask gmask): when the best
-// rotation's SSE is below err, err becomes that SSE, blk the mode-5 block, and the call returns true. Every lane
-// holds the block's texels t, so all group-level branches are group-uniform; ts: the group's shared-memory copy.
-__device__ __forceinline__ bool bc7_group_mode5(const uint32_t t[16], TexRef ts, int &err, uint4 &blk, const int l,
-                                                const unsigned gmask) {
-    // ---- mode 5: lane = rotation * 2 + part (zap_tex.h:659-684)
-    const int rot = l >> 1;
-    const bool alpha_part = l & 1;
-    int q5[2][3] = {{0, 0, 0}, {0, 0, 0}};
-    uint32_t i5 = 0;
-    float lo5[3] = {255.0f, 0.0f, 0.0f}, hi5[3] = {0.0f, 0.0f, 0.0f};
-    if (!alpha_part) {  // colour part starts from the principal axis of the rotated RGB
-        uint32_t r[16];
-        #pragma unroll
-        for (int i = 0; i < 16; i++) r[i] = rotate_texel(t[i], rot);
-        float lo[4], hi[4];
-        pca_endpoints<3>(r, 0xFFFFu, lo, hi);
-        #pragma unroll
-        for (int c = 0; c < 3; c++) { lo5[c] = lo[c]; hi5[c] = hi[c]; }
-    } else {  // alpha part starts from the rotated alpha's range
-        #pragma unroll
-        for (int i = 0; i < 16; i++) {
-            float a = (float)(rotate_texel(t[i], rot) >> 24);
-            if (a < lo5[0]) lo5[0] = a;
-            if (a > hi5[0]) hi5[0] = a;
-        }
-    }
-    const int e5 = m5_part(ts, rot, alpha_part, lo5, hi5, q5, i5);
-    // anchor fix inside the owning lane (zap_tex.h:673-674): 3 - i == i ^ 3 for 2-bit indices
-    if (i5 & 2u) {
-        #pragma unroll
-        for (int c = 0; c < 3; c++) { int s = q5[0][c]; q5[0][c] = q5[1][c]; q5[1][c] = s; }
-        i5 ^= 0xFFFFFFFFu;
-    }
-    int erot = e5 + (int)__shfl_xor_sync(gmask, (uint32_t)e5, 1, kBc7Group);
-    uint32_t key = ((uint32_t)erot << 2) | (uint32_t)rot;  // (SSE, rotation) lexicographic; SSE < 2^21
-    key = min(key, __shfl_xor_sync(gmask, key, 2, kBc7Group));
-    key = min(key, __shfl_xor_sync(gmask, key, 4, kBc7Group));
-    const int brot = (int)(key & 3u), best5 = (int)(key >> 2);
-    uint32_t qw = alpha_part ? (uint32_t)q5[0][0] | ((uint32_t)q5[1][0] << 8)
-                             : (uint32_t)q5[0][0] | ((uint32_t)q5[0][1] << 7) | ((uint32_t)q5[0][2] << 14) |
-                                   ((uint32_t)q5[1][0] << 21);
-    uint32_t qw2 = (uint32_t)q5[1][1] | ((uint32_t)q5[1][2] << 7);
-    uint32_t cq = __shfl_sync(gmask, qw, 2 * brot, kBc7Group), cq2 = __shfl_sync(gmask, qw2, 2 * brot, kBc7Group);
-    uint32_t ci = __shfl_sync(gmask, i5, 2 * brot, kBc7Group);
-    uint32_t aq = __shfl_sync(gmask, qw, 2 * brot + 1, kBc7Group), ai = __shfl_sync(gmask, i5, 2 * brot + 1, kBc7Group);
-    bool take5 = best5 < err;  // decoded SSE == fit SSE (see the file header)
-    if (take5) {
-        err = best5;
-        Bits128 o;
-        o.put(1u << 5, 6);
-        o.put((uint32_t)brot, 2);
-        uint32_t c0[3] = {cq & 127u, (cq >> 7) & 127u, (cq >> 14) & 127u}, c1[3] = {(cq >> 21) & 127u, cq2 & 127u, (cq2 >> 7) & 127u};
-        #pragma unroll
-        for (int c = 0; c < 3; c++) { o.put(c0[c], 7); o.put(c1[c], 7); }
-        o.put(aq & 255u, 8); o.put((aq >> 8) & 255u, 8);
-        o.put(ci & 1u, 1);
-        #pragma unroll
-        for (int i = 1; i < 16; i++) o.put((ci >> (2 * i)) & 3u, 2);
-        o.put(ai & 1u, 1);
-        #pragma unroll
-        for (int i = 1; i < 16; i++) o.put((ai >> (2 * i)) & 3u, 2);
-        blk = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
-    }
-    return take5;
-}
-
-// Mode 1 of one opaque block (zap_tex.h:764-783), same lanes and contract as bc7_group_mode5: true, with err and
-// blk updated, when the best of the ranked partitions has an SSE below err.
+// Mode 1 of one opaque block (zap_tex.h:764-783) by the 8 lanes of a group (lane l, group mask gmask): true, with err
+// and blk updated, when the best of the ranked partitions has an SSE below err. Every lane holds the block's texels
+// t, so all group-level branches are group-uniform; ts: the group's shared-memory copy of them.
 __device__ __forceinline__ bool bc7_group_mode1(const uint32_t t[16], TexRef ts, int &err, uint4 &blk, const int l,
                                                 const unsigned gmask) {
     // ---- mode 1 ranking: lane scores partitions l, l + 8, ..., l + 56 (zap_tex.h:764-775), four per round:
@@ -663,18 +597,6 @@ ZTC_DEV bool block_opaque(const uint32_t t[16]) {
     return opaque;
 }
 
-// One block that mode 6 did not finish, through modes 5 and 1 (zap_tex.h:759-783), by the 8 lanes of a group
-// (lane l, group mask gmask). err is the block's mode-6 SSE; lane 0 writes the block to dst when mode 5 or 1 wins.
-// Every lane holds the block's texels, so all group-level branches below are group-uniform; ts: the group's
-// shared-memory copy of them.
-__device__ __forceinline__ void bc7_group_block(const uint32_t t[16], TexRef ts, int err, const BlockOut &out, size_t ob, const int l,
-                                                const unsigned gmask) {
-    uint4 blk = make_uint4(0, 0, 0, 0);
-    bool take = bc7_group_mode5(t, ts, err, blk, l, gmask);
-    if (block_opaque(t) && bc7_group_mode1(t, ts, err, blk, l, gmask)) take = true;  // group-uniform
-    if (take && l == 0) put_block16(out, ob, blk);
-}
-
 // the group's shared-memory copy of its block (lane l writes texels l and l + 8), for the rolled loops
 __device__ __forceinline__ TexRef stage_group_texels(uint32_t *gtex, const uint32_t t[16], int l, unsigned gmask) {
     __syncwarp(gmask);  // the group's reads of its previous block are done
@@ -683,6 +605,25 @@ __device__ __forceinline__ TexRef stage_group_texels(uint32_t *gtex, const uint3
         if ((i & (kBc7Group - 1)) == l) gtex[i] = t[i];
     __syncwarp(gmask);
     return TexRef{gtex, 1};
+}
+
+// the mode-5 block (zap_tex.h:674-684) of rotation brot from its colour part (cq, cq2: the 7-bit endpoints, ci: the
+// 2-bit indices, anchor already fixed) and its alpha part (aq: the 8-bit endpoints, ai: the indices)
+__device__ __forceinline__ uint4 pack_mode5_block(int brot, uint32_t cq, uint32_t cq2, uint32_t ci, uint32_t aq, uint32_t ai) {
+    Bits128 o;
+    o.put(1u << 5, 6);
+    o.put((uint32_t)brot, 2);
+    const uint32_t c0[3] = {cq & 127u, (cq >> 7) & 127u, (cq >> 14) & 127u}, c1[3] = {(cq >> 21) & 127u, cq2 & 127u, (cq2 >> 7) & 127u};
+    #pragma unroll
+    for (int c = 0; c < 3; c++) { o.put(c0[c], 7); o.put(c1[c], 7); }
+    o.put(aq & 255u, 8); o.put((aq >> 8) & 255u, 8);
+    o.put(ci & 1u, 1);
+    #pragma unroll
+    for (int i = 1; i < 16; i++) o.put((ci >> (2 * i)) & 3u, 2);
+    o.put(ai & 1u, 1);
+    #pragma unroll
+    for (int i = 1; i < 16; i++) o.put((ai >> (2 * i)) & 3u, 2);
+    return make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
 }
 
 // Modes 5 and 1 of single-image encodes over the mode-6 work list. A CTA of two warps takes 8 listed blocks at a
@@ -783,21 +724,7 @@ __global__ void __launch_bounds__(64, 8) bc7_hard_kernel(SrcU8 src, int bw, int 
             uint4 blk = make_uint4(0, 0, 0, 0);
             if (take5) {
                 err = best5;
-                const uint32_t cq = s_cq[tid][brot], cq2 = s_cq2[tid][brot], ci = s_ci[tid][brot], aq = s_aq[tid][brot], ai = s_ai[tid][brot];
-                Bits128 o;
-                o.put(1u << 5, 6);
-                o.put((uint32_t)brot, 2);
-                const uint32_t c0[3] = {cq & 127u, (cq >> 7) & 127u, (cq >> 14) & 127u}, c1[3] = {(cq >> 21) & 127u, cq2 & 127u, (cq2 >> 7) & 127u};
-                #pragma unroll
-                for (int c = 0; c < 3; c++) { o.put(c0[c], 7); o.put(c1[c], 7); }
-                o.put(aq & 255u, 8); o.put((aq >> 8) & 255u, 8);
-                o.put(ci & 1u, 1);
-                #pragma unroll
-                for (int i = 1; i < 16; i++) o.put((ci >> (2 * i)) & 3u, 2);
-                o.put(ai & 1u, 1);
-                #pragma unroll
-                for (int i = 1; i < 16; i++) o.put((ai >> (2 * i)) & 3u, 2);
-                blk = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
+                blk = pack_mode5_block(brot, s_cq[tid][brot], s_cq2[tid][brot], s_ci[tid][brot], s_aq[tid][brot], s_ai[tid][brot]);
             }
             s_err[tid] = err; s_blk[tid] = blk; s_take[tid] = take5;
         }
@@ -878,17 +805,89 @@ batch_bc7_mode6_kernel(const BatchLevel *__restrict__ levels, const BatchTile *_
     }
 }
 
-// Batched modes 5 and 1 as two launches of one kernel over work lists (bases[k]: batch-wide id of the first block
-// of BC7 level k, ascending; level_of[k]: its index in `levels`). PHASE 5 runs mode 5 on every block of the mode-6
-// list (count, items) and appends each opaque block, with its SSE after mode 5, to (next_count, next_items); PHASE 1
-// runs mode 1 on that list. Groups take one block each per round with a CTA barrier between rounds, so the warps of
-// a CTA run the same part of the search together; each launch holds half the code of one mode-5-then-1 pass, which
-// keeps the code the SM fetches small.
-template <int PHASE>
+// Batched mode 5 over the batch-wide list (bases[k]: batch-wide id of the first block of BC7 level k, ascending;
+// level_of[k]: its index in `levels`), laid out like the single-image kernel: a CTA of two warps takes 8 listed
+// blocks at a time, warp 0 fitting their colour parts and warp 1 their alpha parts (lane = block * 4 + rotation);
+// the block is written when mode 5 wins, and each opaque block goes, with its SSE after mode 5, to the mode-1 list.
+__global__ void __launch_bounds__(64, 8) batch_bc7_mode5_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__restrict__ bases,
+                                                               const int *__restrict__ level_of, int nlevels,
+                                                               const uint32_t *__restrict__ count, const uint2 *__restrict__ items,
+                                                               uint32_t *__restrict__ next_count, uint2 *__restrict__ next_items) {
+    __shared__ uint32_t s_tex[kHardBlocks][17];
+    __shared__ uint2 s_item[kHardBlocks];
+    __shared__ int s_cerr[kHardBlocks][4], s_aerr[kHardBlocks][4];
+    __shared__ uint32_t s_cq[kHardBlocks][4], s_cq2[kHardBlocks][4], s_ci[kHardBlocks][4], s_aq[kHardBlocks][4], s_ai[kHardBlocks][4];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = (int)*(volatile const uint32_t *)count;
+    uint8_t *dst = nullptr;  // threads 0..7: the level's blocks of their item, and the block's index there
+    int bidx = 0;
+    for (int base = blockIdx.x * kHardBlocks; base < n; base += gridDim.x * kHardBlocks) {
+        if (tid < kHardBlocks) {
+            const int it = base + tid;
+            uint2 item = make_uint2(0xFFFFFFFFu, 0u);
+            if (it < n) {
+                item = items[it];
+                int lo = 0, hi = nlevels - 1;  // last level whose first id is <= the block's id
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (__ldg(bases + mid) <= item.x) lo = mid; else hi = mid - 1;
+                }
+                const BatchLevel L = levels[__ldg(level_of + lo)];
+                bidx = (int)(item.x - __ldg(bases + lo));
+                dst = L.dst;
+                const SrcU8 src{L.src, L.pitch, L.w, L.h, 4, (((uintptr_t)L.src | L.pitch) & 15u) == 0};
+                uint32_t t[16];
+                gather_block(src, bidx % L.bw, bidx / L.bw, t);
+                #pragma unroll
+                for (int i = 0; i < 16; i++) s_tex[tid][i] = t[i];
+            }
+            s_item[tid] = item;
+        }
+        __syncthreads();
+        {
+            const int blk = lane >> 2, rot = lane & 3;
+            if (s_item[blk].x != 0xFFFFFFFFu) {
+                const TexRef ts{s_tex[blk], 1};
+                uint32_t qw = 0, qw2 = 0, idx = 0;
+                if (warp == 0) {
+                    s_cerr[blk][rot] = m5_colour_lane(ts, rot, qw, qw2, idx);
+                    s_cq[blk][rot] = qw; s_cq2[blk][rot] = qw2; s_ci[blk][rot] = idx;
+                } else {
+                    s_aerr[blk][rot] = m5_alpha_lane(ts, rot, qw, idx);
+                    s_aq[blk][rot] = qw; s_ai[blk][rot] = idx;
+                }
+            }
+        }
+        __syncthreads();
+        if (tid < kHardBlocks && s_item[tid].x != 0xFFFFFFFFu) {
+            uint32_t key = 0xFFFFFFFFu;
+            #pragma unroll
+            for (int r = 0; r < 4; r++) key = min(key, ((uint32_t)(s_cerr[tid][r] + s_aerr[tid][r]) << 2) | (uint32_t)r);
+            const int brot = (int)(key & 3u), best5 = (int)(key >> 2);
+            uint2 item = s_item[tid];
+            if (best5 < (int)item.y) {  // decoded SSE == fit SSE (see the file header)
+                item.y = (uint32_t)best5;
+                put_block16(BlockOut{dst, 0, 4, 0}, (size_t)bidx,
+                            pack_mode5_block(brot, s_cq[tid][brot], s_cq2[tid][brot], s_ci[tid][brot], s_aq[tid][brot], s_ai[tid][brot]));
+            }
+            bool opaque = true;
+            #pragma unroll
+            for (int i = 0; i < 16; i++) opaque &= (s_tex[tid][i] >> 24) == 255u;
+            if (opaque) {
+                const uint32_t pos = atomicAdd(next_count, 1u);
+                next_items[pos] = item;
+            }
+        }
+        __syncthreads();  // the next round overwrites the shared arrays
+    }
+}
+
+// Batched mode 1 over the list of opaque blocks that batch_bc7_mode5_kernel appended (their SSE after mode 5),
+// one block per 8-lane group. Groups take one block each per round with a CTA barrier between rounds, so the warps
+// of a CTA run the same part of the search together (fewer instruction-fetch stalls than groups drifting apart).
 __global__ void __launch_bounds__(128, ZTC_MINB_BC7_HARD)
-batch_bc7_phase_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__restrict__ bases, const int *__restrict__ level_of,
-                       int nlevels, const uint32_t *__restrict__ count, const uint2 *__restrict__ items, uint32_t *__restrict__ next_count,
-                       uint2 *__restrict__ next_items) {
+batch_bc7_mode1_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__restrict__ bases, const int *__restrict__ level_of,
+                       int nlevels, const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
     __shared__ uint32_t s_gtex[128 / kBc7Group][17];
     const int lane = threadIdx.x & 31, l = lane & (kBc7Group - 1);
     const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
@@ -896,14 +895,12 @@ batch_bc7_phase_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__
     const int n = (int)*(volatile const uint32_t *)count;
     uint32_t *gtex = s_gtex[threadIdx.x / kBc7Group];
     const int gid = blockIdx.x * (blockDim.x / kBc7Group) + (threadIdx.x / kBc7Group);
-    const int rounds = (n + ngroups - 1) / ngroups;  // the same for every warp: the ballot below sees all 32 lanes
+    const int rounds = (n + ngroups - 1) / ngroups;  // the same for every warp
     for (int r = 0; r < rounds; r++) {
         __syncthreads();
         const int it = r * ngroups + gid;
-        uint2 item = make_uint2(0, 0);
-        bool push = false;
         if (it < n) {
-            item = items[it];
+            const uint2 item = items[it];
             int lo = 0, hi = nlevels - 1;  // last level whose first id is <= the block's id
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
@@ -917,22 +914,7 @@ batch_bc7_phase_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__
             const TexRef ts = stage_group_texels(gtex, t, l, gmask);
             int err = (int)item.y;
             uint4 blk = make_uint4(0, 0, 0, 0);
-            const bool take = PHASE == 5 ? bc7_group_mode5(t, ts, err, blk, l, gmask) : bc7_group_mode1(t, ts, err, blk, l, gmask);
-            if (take && l == 0) put_block16(BlockOut{L.dst, 0, 4, 0}, (size_t)b, blk);
-            if (PHASE == 5) {
-                push = l == 0 && block_opaque(t);
-                item.y = (uint32_t)err;
-            }
-        }
-        if (PHASE == 5) {  // one atomic per warp for its groups' opaque blocks
-            const unsigned ballot = __ballot_sync(0xFFFFFFFFu, push);
-            if (ballot) {
-                const int leader = __ffs(ballot) - 1;
-                uint32_t base = 0;
-                if (lane == leader) base = atomicAdd(next_count, (uint32_t)__popc(ballot));
-                base = __shfl_sync(0xFFFFFFFFu, base, leader);
-                if (push) next_items[base + __popc(ballot & ((1u << lane) - 1u))] = item;
-            }
+            if (bc7_group_mode1(t, ts, err, blk, l, gmask) && l == 0) put_block16(BlockOut{L.dst, 0, 4, 0}, (size_t)b, blk);
         }
     }
 }
@@ -950,12 +932,11 @@ cudaError_t ztc_launch_batch_bc7_mode6(int cta, int regs, int grid, const ztc::B
 cudaError_t ztc_launch_batch_bc7_hard(int grid, const ztc::BatchLevel *levels, const uint32_t *bases, const int *level_of, int nlevels,
                                       const uint32_t *hard_count, const uint2 *hard_items, uint32_t *opaque_count, uint2 *opaque_items,
                                       cudaStream_t stream) {
-    ztc::batch_bc7_phase_kernel<5><<<grid, 128, 0, stream>>>(levels, bases, level_of, nlevels, hard_count, hard_items, opaque_count,
-                                                              opaque_items);
+    ztc::batch_bc7_mode5_kernel<<<ztc_sm_count() * 8, 64, 0, stream>>>(levels, bases, level_of, nlevels, hard_count, hard_items,
+                                                                       opaque_count, opaque_items);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    ztc::batch_bc7_phase_kernel<1><<<grid, 128, 0, stream>>>(levels, bases, level_of, nlevels, opaque_count, opaque_items, nullptr,
-                                                              nullptr);
+    ztc::batch_bc7_mode1_kernel<<<grid, 128, 0, stream>>>(levels, bases, level_of, nlevels, opaque_count, opaque_items);
     return cudaGetLastError();
 }
 
@@ -972,7 +953,7 @@ const void *ztc_batch_bc7_kernel_fn(int cta, int regs) {
     return regs ? batch_bc7_fn_cap<ZTC_MINB_BC7_BATCH_LOOSE>(cta) : batch_bc7_fn_cap<ZTC_MINB_BC7_MODE6>(cta);
 }
 
-const void *ztc_batch_bc7_hard_kernel_fn() { return (const void *)ztc::batch_bc7_phase_kernel<5>; }  // both phases: same bounds
+const void *ztc_batch_bc7_hard_kernel_fn() { return (const void *)ztc::batch_bc7_mode1_kernel; }  // the tuned modes-5/1 grid is mode 1's
 
 size_t ztc::bc7_scratch_bytes(size_t nblocks) { return 256 + nblocks * sizeof(uint2); }
 
