@@ -501,6 +501,27 @@ def main():
                        "d2h_bytes_per_step": int(hout.size), "api": "zap_tex_cuda_bc_encode (host pointers)",
                        "ms_per_call_segments": [r * 1e3 for r in runs], "timing": "median of 5 segments of wall-clock calls",
                        "host_cpus": "GPU-local (NVML CPU affinity)" if saved_cpus is not None else "unbound"}
+        # the copies alone, the bound of a host-pointer call: the texture in and the blocks out over PCIe, pinned
+        # buffers, one copy each on one stream (CUDA events), median of 20
+        dtex = torch.empty((H, W, 4), dtype=torch.uint8, device=dev)
+        dblk = torch.empty(zap_b200.bc_size(W, H, zap_b200.BC7), dtype=torch.uint8, device=dev)
+        c0, c1, c2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        h2d, d2h = [], []
+        for _ in range(23):
+            c0.record()
+            dtex.copy_(host_in, non_blocking=True)
+            c1.record()
+            host_out.copy_(dblk, non_blocking=True)
+            c2.record()
+            torch.cuda.synchronize()
+            h2d.append(c0.elapsed_time(c1))
+            d2h.append(c1.elapsed_time(c2))
+        h2d_ms, d2h_ms = statistics.median(h2d[3:]), statistics.median(d2h[3:])
+        line["e2e"]["copy_bound"] = {"h2d_ms": h2d_ms, "d2h_ms": d2h_ms, "h2d_GB_s": W * H * 4 / h2d_ms / 1e6,
+                                     "d2h_GB_s": hout.size / d2h_ms / 1e6, "h2d_fraction_of_call": h2d_ms / (e2e_s * 1e3),
+                                     "note": "the call overlaps its copies out with the copies in, so the texture's "
+                                             "copy in alone bounds it"}
+        del dtex, dblk
         if saved_cpus is not None:
             os.sched_setaffinity(0, saved_cpus)  # the CPU baseline below uses every host thread
         # reference CPU on the same texture; parity of the GPU output against it
