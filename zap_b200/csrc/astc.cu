@@ -282,6 +282,45 @@ ZTC_DEV int astc_fit_weights(TexRef ts, uint32_t cm, int cem, int wb, const uint
     return err;
 }
 
+// The same fit for one partition with the loops turned inside out: entries outer (rolled), the 16 texels inner
+// (unrolled, in registers), each texel keeping its least key. The keys are unique ((|c|^2 - 2 p.c) * LMAX + j), so
+// the minimum, and with it every weight and the SSE, is the one the texel-outer loop finds; the state is the texels
+// and their 16 best keys instead of a palette and key table of up to 2 x 32 registers.
+template <int LMAX>
+ZTC_DEV int astc_fit_weights_1p(TexRef ts, uint32_t cm, int cem, int wb, const uint8_t *wq, const int uv[8], uint32_t wt[4]) {
+    const int L = 1 << wb;
+    int e0[4], e1[4];
+    endpoint_pair(cem, uv, e0, e1);
+    uint32_t p[16];
+    int best[16];
+    #pragma unroll
+    for (int i = 0; i < 16; i++) { p[i] = ts[i] & cm; best[i] = 0x7FFFFFFF; }
+    #pragma unroll 1
+    for (int j = 0; j < L; j++) {
+        const int w = wq[j];
+        const uint32_t e = pack_rgba(astc_lerp(e0[0], e1[0], w), astc_lerp(e0[1], e1[1], w), astc_lerp(e0[2], e1[2], w),
+                                     astc_lerp(e0[3], e1[3], w)) & cm;
+        const int a = (int)dot4(e, e) * LMAX + j;
+        #pragma unroll
+        for (int i = 0; i < 16; i++) best[i] = min(best[i], a - 2 * LMAX * (int)dot4(p[i], e));
+    }
+    int err = 0;
+    uint32_t w0 = 0, w1 = 0, w2 = 0, w3 = 0;
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const int m = best[i];
+        const int q = m >= 0 ? m / LMAX : -((-m + LMAX - 1) / LMAX);
+        err += q + (int)dot4(p[i], p[i]);
+        const uint32_t wi = (uint32_t)(m - q * LMAX);
+        if (i < 4) w0 |= wi << (8 * i);
+        else if (i < 8) w1 |= wi << (8 * (i - 4));
+        else if (i < 12) w2 |= wi << (8 * (i - 8));
+        else w3 |= wi << (8 * (i - 12));
+    }
+    wt[0] = w0; wt[1] = w1; wt[2] = w2; wt[3] = w3;
+    return err;
+}
+
 // Passes [first, last) of one trial configuration (zap_tex.h:1212-1244): pass 0 fits the weights to the endpoint
 // codes code / uv; pass k > 0 is the k-th least-squares refit on the weights wt holds, which stops at SSE 0 or at
 // the first refit that does not lower the SSE (a partition whose system is singular keeps its codes). code, uv, wt
@@ -332,7 +371,8 @@ ZTC_DEV bool astc_passes(TexRef ts, const AstcSmem &S, int cfg, int nc, uint32_t
             }
         }
         uint32_t tw[4];
-        const int e = astc_fit_weights<LMAX, PARTS>(ts, cm, cem, wb, wq, pm, tuv, tw);
+        const int e = PARTS == 1 ? astc_fit_weights_1p<LMAX>(ts, cm, cem, wb, wq, tuv[0], tw)
+                                 : astc_fit_weights<LMAX, PARTS>(ts, cm, cem, wb, wq, pm, tuv, tw);
         if (it > 0 && e >= err) return false;
         err = e;
         #pragma unroll
