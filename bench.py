@@ -641,7 +641,7 @@ def refine_workload(args, dev, n=1024, side=256, steps=8, lr=1.0):
     import zap_b200
     import zap_b200.synth as S
     tex = torch.cat([S.colour_texture(side, side, seed=20000 + k, device=dev) for k in range(n)], 0).contiguous()
-    atlas = atlas_texture(2048, 64, 50000, dev, 0)
+    atlas = atlas_textures(2048, 64, 50000, dev, 1)[0]
     res = {"textures": n, "side": side, "adam_steps": steps, "lr": lr}
     psnr = lambda e, nval: 99.0 if e == 0 else 10 * math.log10(255.0 ** 2 * nval / e)  # noqa: E731
     for fmt, name, chans, img in ((zap_b200.BC1, "bc1", 3, tex), (zap_b200.BC7, "bc7", 4, tex),
@@ -687,18 +687,21 @@ def refine_workload(args, dev, n=1024, side=256, steps=8, lr=1.0):
     return res
 
 
-def atlas_texture(side, tile, seed, device, order_seed):
-    """A side x side texture atlas of tile x tile textures of the batch's recipe (colour_texture, one seed per tile),
-    placed in an order drawn from order_seed: small textures carry more detail per 4x4 block, so more BC7 blocks
-    leave mode 6 than in one large texture of the same recipe."""
+def atlas_textures(side, tile, seed, device, count):
+    """`count` side x side texture atlases of the same (side / tile)^2 textures of the batch's recipe (colour_texture,
+    one seed per tile), each in its own order (seeded 0 .. count - 1): small textures carry more detail per 4x4 block,
+    so more BC7 blocks leave mode 6 than in one large texture of the same recipe."""
     import torch
 
     import zap_b200.synth as S
     n = side // tile
-    tiles = [S.colour_texture(tile, tile, seed=seed + k, device=device) for k in range(n * n)]
-    perm = torch.randperm(n * n, generator=torch.Generator().manual_seed(order_seed)).tolist()
-    rows = [torch.cat([tiles[perm[r * n + c]] for c in range(n)], 1) for r in range(n)]
-    return torch.cat(rows, 0).contiguous()
+    tiles = torch.stack([S.colour_texture(tile, tile, seed=seed + k, device=device) for k in range(n * n)])
+    out = []
+    for k in range(count):
+        perm = torch.randperm(n * n, generator=torch.Generator().manual_seed(k)).to(device)
+        grid = tiles[perm].view(n, n, tile, tile, 4).permute(0, 2, 1, 3, 4).reshape(side, side, 4)
+        out.append(grid.contiguous())
+    return out
 
 
 def log2_psnr(src, dec):
@@ -814,9 +817,9 @@ def extra_workloads(args, dev, sm_mhz=None, sms=148):
     bench("bc6h_2048x2048_rgb16f", lambda k: S.hdr_texture(2048, 2048, seed=k, device=dev), "bc6h", 2048 * 2048, 6, 7.0,
           chans=3, enc=lambda t, o: zap_b200.bc6h_encode_dev(t, out=o), counted="bc6h_encode")
     bench("bc7_2048x2048_opaque", lambda k: S.colour_texture(2048, 2048, seed=k, device=dev), zap_b200.BC7, 2048 * 2048, 10, 5.0)
-    atlas = atlas_texture(2048, 64, 40000, dev, 0)
-    bench("bc7_2048x2048_atlas_of_64x64", lambda k: atlas if k == 0 else atlas_texture(2048, 64, 40000, dev, k), zap_b200.BC7,
-          2048 * 2048, 10, 5.0)
+    atlases = atlas_textures(2048, 64, 40000, dev, 10)
+    bench("bc7_2048x2048_atlas_of_64x64", lambda k: atlases[k], zap_b200.BC7, 2048 * 2048, 10, 5.0)
+    del atlases
     torch.cuda.empty_cache()
     return res
 

@@ -19,8 +19,8 @@
 // more resident warps hide the latency of these long dependent integer / float chains; see the ncu summaries).
 // Measured on 2048x2048 encodes (re-swept after the loops were rolled): bc7_mode6 0.120 -> 0.113 ms at 6 (85
 // registers; the small spill stays in L1), BC1 -1.2 % at 8, ASTC single-partition -4 % at 5, BC6H (texels staged in
-// shared memory) 0.383 -> 0.351 ms at 5 against 3; the
-// BC7 mode 5/1 kernel (124 registers already allow 4 CTAs) gains nothing from more.
+// shared memory) 0.383 -> 0.351 ms at 5 against 3; the batched BC7 mode-1 kernel (118 registers already allow 4
+// CTAs) gains nothing from more.
 #ifndef ZTC_MINB_BC7_MODE6
 #define ZTC_MINB_BC7_MODE6 6
 #endif
