@@ -100,18 +100,35 @@ __attribute__((visibility("default"))) int emu_astc_encode(const uint8_t *img, i
 }
 
 __attribute__((visibility("default"))) int emu_mip_next(const uint8_t *src, int w, int h, size_t stride, int srgb, uint8_t *dst, size_t dst_stride) {
-    float lin[256], thr[256];
-    srgb_tables_host(lin, thr);
+    SrgbTables T;
+    srgb_tables_host(T);
     int nw = w > 1 ? w / 2 : 1, nh = h > 1 ? h / 2 : 1;
     for (int y = 0; y < nh; y++)
         for (int x = 0; x < nw; x++) {
             int x0 = std::min(2 * x, w - 1), x1 = std::min(2 * x + 1, w - 1), y0 = std::min(2 * y, h - 1), y1 = std::min(2 * y + 1, h - 1);
             uint32_t v = box4(ld_texel(src + (size_t)y0 * stride + (size_t)x0 * 4), ld_texel(src + (size_t)y0 * stride + (size_t)x1 * 4),
                               ld_texel(src + (size_t)y1 * stride + (size_t)x0 * 4), ld_texel(src + (size_t)y1 * stride + (size_t)x1 * 4),
-                              srgb != 0, lin, thr);
+                              srgb != 0, T);
             memcpy(dst + (size_t)y * dst_stride + (size_t)x * 4, &v, 4);
         }
     return 0;
+}
+
+// floats v with bit patterns in [lo, hi) for which the mip generator's bucketed sRGB search differs from the
+// reference's binary search (zap_tex.h:1429-1433)
+__attribute__((visibility("default"))) uint64_t emu_srgb_search_mismatches(uint64_t lo, uint64_t hi) {
+    SrgbTables T;
+    srgb_tables_host(T);
+    uint64_t bad = 0;
+    for (uint64_t b = lo; b < hi; b++) {
+        const uint32_t u = (uint32_t)b;
+        float v;
+        memcpy(&v, &u, 4);
+        int l = 0, h = 255;
+        while (l < h) { const int mid = (l + h) >> 1; if (v < T.thr[mid]) h = mid; else l = mid + 1; }
+        bad += lin_to_srgb(T.thr, T.bucket, v) != (uint32_t)l;
+    }
+    return bad;
 }
 
 // finite floats x with bit patterns in [lo, hi) for which ztc::div255(x) differs bitwise from the division x / 255.0f

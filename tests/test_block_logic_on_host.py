@@ -40,6 +40,8 @@ def emu():
     lib.emu_div255_mismatches.restype = C.c_uint64
     lib.emu_div_small_mismatches.argtypes = [i]
     lib.emu_div_small_mismatches.restype = C.c_uint64
+    lib.emu_srgb_search_mismatches.argtypes = [C.c_uint64, C.c_uint64]
+    lib.emu_srgb_search_mismatches.restype = C.c_uint64
     return lib
 
 
@@ -144,4 +146,20 @@ def test_small_divisor_division_equals_ieee_on_its_domain(emu):
     from concurrent.futures import ThreadPoolExecutor
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
         bad = sum(ex.map(emu.emu_div_small_mismatches, range(1, 17)))
+    assert bad == 0
+
+
+def test_srgb_bucket_search_equals_binary_search(emu):
+    """The mip generator maps a linear value back to sRGB by scanning from a per-bucket start instead of the
+    reference's binary search; both must give the same code for every float in [0, 1] (the averages the generator
+    forms lie there) and for the negative, above-one and infinite values around it."""
+    from concurrent.futures import ThreadPoolExecutor
+    top = 0x3F800001  # bit patterns 0 .. 1.0f
+    chunks = 64
+    step = (top + chunks - 1) // chunks
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        bad = sum(ex.map(lambda k: emu.emu_srgb_search_mismatches(k * step, min(top, (k + 1) * step)), range(chunks)))
+    bad += emu.emu_srgb_search_mismatches(0x3F800001, 0x3F800001 + (1 << 20))  # just above 1
+    bad += emu.emu_srgb_search_mismatches(0x7F800000, 0x7F800001)  # +inf
+    bad += emu.emu_srgb_search_mismatches(0x80000000, 0x80000000 + (1 << 20))  # -0 and small negatives
     assert bad == 0

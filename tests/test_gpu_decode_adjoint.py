@@ -58,11 +58,11 @@ def _linear_model_fp64(blocks, fmt, oracle):
         c0 = bb[:, 0] | (bb[:, 1] << 8)
         c1 = bb[:, 2] | (bb[:, 3] << 8)
         idx = bb[:, 4] | (bb[:, 5] << 8) | (bb[:, 6] << 16) | (bb[:, 7] << 24)
-        table = np.array([1.0, 0.0, 2.0 / 3.0, 1.0 / 3.0])
-        for i in range(16):
+        four, three = np.array([1.0, 0.0, 2.0 / 3.0, 1.0 / 3.0]), np.array([1.0, 0.0, 0.5, 0.0])
+        for i in range(16):  # the decoder's rule (zap_tex.h:1508-1517): 3 colours and black when c0 <= c1
             k = ((idx >> np.uint64(2 * i)) & np.uint64(3)).astype(int)
-            k = np.where(c0 <= c1, np.where(k == 1, 1, 0), k)
-            A[:, i, :] = table[k][:, None]
+            A[:, i, :] = np.where(c0 > c1, four[k], three[k])[:, None]
+            fixed[(c0 <= c1) & (k == 3), i, :3] = 0.0
         fixed[:, :, 3] = 0.0
         return A, R0, SC, fixed
     for k in range(n):
@@ -161,8 +161,9 @@ def test_palette_adjoint_against_fp64_and_finite_differences(cuda_lib, oracle):
 
 
 def test_palette_decode_at_stored_endpoints_rounds_to_the_decoder(cuda_lib):
-    """Every BC7 mode (arbitrary blocks, the reserved mode too) and BC1: the linear decode at the blocks' own
-    endpoints is the integer decoder's output before its rounding, so within 0.5 of it."""
+    """Every BC7 mode (arbitrary blocks, the reserved mode too) and BC1 (4-colour, 3-colour and black texels): the
+    linear decode at the blocks' own endpoints is the integer decoder's output before its rounding, so within 0.5
+    of it (and 0 on BC1's black texels)."""
     import torch
     rng = np.random.default_rng(17)
     bc = rng.integers(0, 256, (9 * 256, 16), dtype=np.uint8)

@@ -30,28 +30,32 @@ namespace ztc {
 ZTC_DEV int endpoint_floats(int fmt) { return fmt == ZTC_FMT_BC1 ? 8 : 24; }
 
 // A block's linear form: per texel the weight of the subset's first endpoint for the colour channels (a) and for
-// alpha (aa), the subset (bit i of `s1`: subset 1; `s2`: subset 2), the rotation, and which channels the endpoints
-// decide (nc: BC1 3, BC7 4; alpha_fixed: BC7 alpha without bits, 255).
+// alpha (aa), the subset (bit i of `s1`: subset 1; `s2`: subset 2), the rotation, which channels the endpoints
+// decide (nc: BC1 3, BC7 4; alpha_fixed: BC7 alpha without bits, 255), and the texels whose colour is a constant
+// whatever the endpoints (`black`: index 3 of a BC1 3-colour block, zap_tex.h:1508-1517, which decodes to 0).
 struct LinBlock {
     float a[16], aa[16];
-    uint32_t s1, s2;
+    uint32_t s1, s2, black;
     int rot, nc, mode;
     bool covered, alpha_fixed;
 };
 
 ZTC_DEV void linear_form(int fmt, const uint8_t *blk, LinBlock &L, float e[6][4]) {
-    L.s1 = L.s2 = 0u;
+    L.s1 = L.s2 = L.black = 0u;
     L.rot = 0;
     L.alpha_fixed = false;
     if (fmt == ZTC_FMT_BC1) {
         uint2 v = *(const uint2 *)blk;
         uint32_t c0 = v.x & 0xFFFFu, c1 = v.x >> 16;
         L.nc = 3; L.mode = 0; L.covered = true;
+        const bool four = c0 > c1;  // the decoder's rule: 4 colours, else 3 colours and black (zap_tex.h:1508-1517)
         #pragma unroll
         for (int i = 0; i < 16; i++) {
-            uint32_t k = (v.y >> (2 * i)) & 3u;
-            if (c0 <= c1) k = k == 1 ? 1u : 0u;  // solid / 3-colour blocks: our encoder only emits index 0 there
-            L.a[i] = L.aa[i] = k == 0 ? 1.0f : k == 1 ? 0.0f : k == 2 ? 2.0f / 3.0f : 1.0f / 3.0f;
+            const uint32_t k = (v.y >> (2 * i)) & 3u;
+            if (four) L.a[i] = k == 0 ? 1.0f : k == 1 ? 0.0f : k == 2 ? 2.0f / 3.0f : 1.0f / 3.0f;
+            else L.a[i] = k == 0 ? 1.0f : k == 1 ? 0.0f : k == 2 ? 0.5f : 0.0f;
+            L.aa[i] = L.a[i];
+            if (!four && k == 3) L.black |= 1u << i;
         }
         for (int k = 0; k < 2; k++) {
             uint32_t c = k ? c1 : c0;
@@ -111,7 +115,7 @@ __global__ void decode_kernel(int fmt, const uint8_t *__restrict__ blocks, int n
         for (int c = 0; c < 4; c++) {
             const int sc = stored_channel(L.rot, c);
             float d = 0.0f;
-            if (L.covered && c < L.nc) {
+            if (L.covered && c < L.nc && !((L.black >> i) & 1u)) {
                 if (sc == 3 && L.alpha_fixed) d = 255.0f;
                 else {
                     const float a = sc == 3 ? L.aa[i] : L.a[i];
@@ -134,7 +138,7 @@ __global__ void adjoint_kernel(int fmt, const uint8_t *__restrict__ blocks, int 
         const int s = subset_of_texel(L, i);
         for (int c = 0; c < 4; c++) {
             const int sc = stored_channel(L.rot, c);
-            if (!L.covered || c >= L.nc || (sc == 3 && L.alpha_fixed)) continue;
+            if (!L.covered || c >= L.nc || (sc == 3 && L.alpha_fixed) || ((L.black >> i) & 1u)) continue;
             const float gi = g[((size_t)b * 16 + i) * 4 + c], a = sc == 3 ? L.aa[i] : L.a[i];
             G[2 * s][sc] += a * gi;
             G[2 * s + 1][sc] += (1.0f - a) * gi;
@@ -389,6 +393,7 @@ __global__ void __launch_bounds__(128) refine_kernel(int fmt, SrcU8 src, int bw,
         for (int s = 0; s < steps; s++) {
             float g[4][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
             for (int i = 0; i < 16; i++) {
+                if ((L.black >> i) & 1u) continue;  // a constant: no gradient
                 const bool in1 = (L.s1 >> i) & 1u;
                 for (int c = 0; c < npar; c++) {  // forward decode, residual, adjoint
                     const float a = c == 3 ? L.aa[i] : L.a[i];

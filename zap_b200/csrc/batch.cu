@@ -74,7 +74,7 @@ struct zap_tex_cuda_batch {
     uint32_t *d_bc7_bases = nullptr;         // first batch-wide id of each BC7 level, ascending
     int *d_bc7_level_of = nullptr;           // ... and that level's index in d_levels
     int n_bc7_levels = 0, hard_grid = 1, hard_per_sm = 1;
-    float *d_srgb = nullptr;
+    ztc::SrgbTables *d_srgb = nullptr;
     void *plain_scratch = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -424,10 +424,10 @@ int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *it
         b->hard_per_sm = std::max(1, per_sm);
         b->hard_grid = b->hard_per_sm * b->sms;
     }
-    float tables[512];
-    ztc::srgb_tables_host(tables, tables + 256);
+    ztc::SrgbTables tables;
+    ztc::srgb_tables_host(tables);
     BTRY(ztc_malloc((void **)&b->d_srgb, sizeof tables), "cudaMalloc(srgb)");
-    BTRY(cudaMemcpy(b->d_srgb, tables, sizeof tables, cudaMemcpyHostToDevice), "upload srgb");
+    BTRY(cudaMemcpy(b->d_srgb, &tables, sizeof tables, cudaMemcpyHostToDevice), "upload srgb");
     BTRY(ztc_malloc((void **)&b->d_counters, 64 * sizeof(uint32_t)), "cudaMalloc(counters)");
     BTRY(ztc_malloc((void **)&b->plain_scratch, ztc::bc7_scratch_bytes(max_blocks)), "cudaMalloc(plain scratch)");
     // ---- tiles (autotuned or 128 blocks per CTA)

@@ -2,48 +2,56 @@
 //
 // RGBA8: with srgb, RGB goes through the sRGB->linear table, the four values are summed left to right and scaled
 // by 0.25f, and the result maps back to sRGB as the first k whose threshold exceeds it (the reference's binary
-// search). Alpha (and RGB without srgb) is (a + b + c + d + 2) >> 2. Odd sizes drop the last row / column.
+// search; here a scan from a per-bucket start, below). Alpha (and RGB without srgb) is (a + b + c + d + 2) >> 2.
+// Odd sizes drop the last row / column.
 // The fast path gives each thread two output texels: one 16-byte load from each of the two source rows and one
 // 8-byte store; edge and unaligned texels take a clamped scalar path.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 
 #include "ztc_common.cuh"
 #include "ztc_internal.h"
 
 namespace ztc {
 
-__constant__ float kSrgbLin[256];
-__constant__ float kSrgbThr[256];  // 255 thresholds + a +inf sentinel
+__device__ SrgbTables gSrgb;  // staged into shared memory by each CTA (coalesced loads)
 
-struct MipTables {
-    float lin[256];
-    float thr[256];
-};
-
-ZTC_DEV uint32_t lin_to_srgb(const float *thr, float v) {  // first k with v < thr[k] (zap_tex.h:1429-1433)
-    int lo = 0, hi = 255;
-    #pragma unroll
-    for (int s = 0; s < 8; s++) {
-        int mid = (lo + hi) >> 1;
-        bool below = v < thr[mid];
-        hi = below ? mid : hi;
-        lo = below ? lo : mid + 1;
-    }
-    return (uint32_t)lo;
+// the bucket of a linear value: 0 below 2^-16 (and for negative values), else its exponent and top 6 mantissa bits
+ZTC_DEV int srgb_bucket(float v) {
+    const uint32_t u = f_as_u(v);
+    if (u < 0x37800000u || (u & 0x80000000u)) return 0;
+    const int q = (int)(u >> 17) - (0x37800000 >> 17);
+    return q < kSrgbBuckets - 1 ? q : kSrgbBuckets - 1;
+}
+// first k with v < thr[k] (zap_tex.h:1429-1433), 255 when there is none: the reference's binary search finds it in
+// eight steps; here the scan starts at the bucket's lower bound, one to three steps for the mip generator's values
+ZTC_DEV uint32_t lin_to_srgb(const float *thr, const uint8_t *bucket, float v) {
+    int k = bucket[srgb_bucket(v)];
+    while (k < 255 && !(v < thr[k])) k++;
+    return (uint32_t)k;
 }
 
-ZTC_DEV uint32_t box4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, bool srgb, const float *lin, const float *thr) {
+ZTC_DEV uint32_t box4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, bool srgb, const SrgbTables &T) {
     uint32_t o = 0;
     #pragma unroll
     for (int k = 0; k < 4; k++) {
         uint32_t v0 = chan(a, k), v1 = chan(b, k), v2 = chan(c, k), v3 = chan(d, k), r;
-        if (srgb && k < 3) r = lin_to_srgb(thr, (lin[v0] + lin[v1] + lin[v2] + lin[v3]) * 0.25f);
+        if (srgb && k < 3) r = lin_to_srgb(T.thr, T.bucket, (T.lin[v0] + T.lin[v1] + T.lin[v2] + T.lin[v3]) * 0.25f);
         else r = (v0 + v1 + v2 + v3 + 2) >> 2;
         o |= r << (8 * k);
     }
     return o;
+}
+
+// every thread of the CTA calls it: the tables from global memory into shared memory, 32-bit words
+__device__ __forceinline__ void stage_srgb(SrgbTables &S, const SrgbTables *src) {
+    static_assert(sizeof(SrgbTables) % 4 == 0, "staged as 32-bit words");
+    const uint32_t *g = (const uint32_t *)src;
+    uint32_t *d = (uint32_t *)&S;
+    for (int k = threadIdx.x; k < (int)(sizeof(SrgbTables) / 4); k += blockDim.x) d[k] = __ldg(g + k);
+    __syncthreads();
 }
 
 ZTC_DEV uint32_t ld_texel(const uint8_t *p) {
@@ -57,11 +65,8 @@ ZTC_DEV void st_texel(uint8_t *p, uint32_t v) {
 
 __global__ void __launch_bounds__(256) mip_rgba8_kernel(const uint8_t *__restrict__ src, int w, int h, size_t stride, int srgb,
                                                         uint8_t *__restrict__ dst, size_t dst_stride, int nw, int nh, int vec) {
-    __shared__ float lin[256], thr[256];
-    if (srgb) {
-        for (int k = threadIdx.x; k < 256; k += blockDim.x) { lin[k] = kSrgbLin[k]; thr[k] = kSrgbThr[k]; }
-        __syncthreads();
-    }
+    __shared__ SrgbTables S;
+    if (srgb) stage_srgb(S, &gSrgb);
     const int pairs = (nw + 1) >> 1;
     const long total = (long)pairs * nh;
     for (long id = (long)blockIdx.x * blockDim.x + threadIdx.x; id < total; id += (long)gridDim.x * blockDim.x) {
@@ -71,13 +76,13 @@ __global__ void __launch_bounds__(256) mip_rgba8_kernel(const uint8_t *__restric
         uint8_t *o = dst + (size_t)y * dst_stride + (size_t)x * 4;
         if (vec && 2 * x + 3 < w && x + 1 < nw) {
             uint4 a = __ldg((const uint4 *)(r0 + (size_t)x * 8)), b = __ldg((const uint4 *)(r1 + (size_t)x * 8));
-            uint32_t o0 = box4(a.x, a.y, b.x, b.y, srgb, lin, thr), o1 = box4(a.z, a.w, b.z, b.w, srgb, lin, thr);
+            uint32_t o0 = box4(a.x, a.y, b.x, b.y, srgb, S), o1 = box4(a.z, a.w, b.z, b.w, srgb, S);
             *(uint2 *)o = make_uint2(o0, o1);
         } else {
             for (int k = 0; k < 2 && x + k < nw; k++) {
                 int xx = x + k, x0 = min(2 * xx, w - 1), x1 = min(2 * xx + 1, w - 1);
                 uint32_t v = box4(ld_texel(r0 + (size_t)x0 * 4), ld_texel(r0 + (size_t)x1 * 4), ld_texel(r1 + (size_t)x0 * 4),
-                                  ld_texel(r1 + (size_t)x1 * 4), srgb, lin, thr);
+                                  ld_texel(r1 + (size_t)x1 * 4), srgb, S);
                 st_texel(o + (size_t)k * 4, v);
             }
         }
@@ -114,18 +119,24 @@ static float srgb_to_linear_9g(double c) {
     return std::strtof(buf, nullptr);
 }
 
-void srgb_tables_host(float lin[256], float thr[256]) {
-    for (int k = 0; k < 256; k++) lin[k] = srgb_to_linear_9g(k / 255.0);
-    for (int k = 0; k < 255; k++) thr[k] = srgb_to_linear_9g((k + 0.5) / 255.0);
-    thr[255] = INFINITY;
+void srgb_tables_host(SrgbTables &t) {
+    for (int k = 0; k < 256; k++) t.lin[k] = srgb_to_linear_9g(k / 255.0);
+    for (int k = 0; k < 255; k++) t.thr[k] = srgb_to_linear_9g((k + 0.5) / 255.0);
+    t.thr[255] = INFINITY;
+    for (int q = 0; q < kSrgbBuckets; q++) {  // the answer at the bucket's lowest value (0 for bucket 0)
+        uint32_t u = q ? (uint32_t)(q + (0x37800000 >> 17)) << 17 : 0u;
+        float lo;
+        std::memcpy(&lo, &u, 4);
+        int k = 0;
+        while (k < 255 && !(lo < t.thr[k])) k++;
+        t.bucket[q] = (uint8_t)k;
+    }
 }
 
 cudaError_t upload_mip_tables() {
-    float lin[256], thr[256];
-    srgb_tables_host(lin, thr);
-    cudaError_t e = cudaMemcpyToSymbol(kSrgbLin, lin, sizeof lin);
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(kSrgbThr, thr, sizeof thr);
-    return e;
+    SrgbTables T;
+    srgb_tables_host(T);
+    return cudaMemcpyToSymbol(gSrgb, &T, sizeof T);
 }
 
 static int grid_for(long work, int threads) {
@@ -159,10 +170,9 @@ cudaError_t ztc_launch_mip_f(const float *src, int w, int h, size_t stride, floa
 // ---------------------------------------------------------------- batched: one launch per mip depth, all textures
 namespace ztc {
 __global__ void __launch_bounds__(256) batch_mip_kernel(const BatchMip *__restrict__ mips, const BatchMipTile *__restrict__ tiles, int ntiles,
-                                                        const float *__restrict__ tables) {
-    __shared__ float lin[256], thr[256];
-    for (int k = threadIdx.x; k < 256; k += blockDim.x) { lin[k] = tables[k]; thr[k] = tables[256 + k]; }
-    __syncthreads();
+                                                        const SrgbTables *__restrict__ tables) {
+    __shared__ SrgbTables S;
+    stage_srgb(S, tables);
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const BatchMipTile T = tiles[tile];
         if ((int)threadIdx.x >= T.count) continue;
@@ -175,12 +185,12 @@ __global__ void __launch_bounds__(256) batch_mip_kernel(const BatchMip *__restri
         const bool vec = ((((uintptr_t)M.src) | M.src_pitch) & 15u) == 0 && ((((uintptr_t)M.dst) | M.dst_pitch) & 7u) == 0;
         if (vec && 2 * x + 3 < M.w && x + 1 < M.nw) {
             uint4 a = ldg((const uint4 *)(r0 + (size_t)x * 8)), b = ldg((const uint4 *)(r1 + (size_t)x * 8));
-            *(uint2 *)o = make_uint2(box4(a.x, a.y, b.x, b.y, M.srgb, lin, thr), box4(a.z, a.w, b.z, b.w, M.srgb, lin, thr));
+            *(uint2 *)o = make_uint2(box4(a.x, a.y, b.x, b.y, M.srgb, S), box4(a.z, a.w, b.z, b.w, M.srgb, S));
         } else {
             for (int k = 0; k < 2 && x + k < M.nw; k++) {
                 int xx = x + k, x0 = min(2 * xx, M.w - 1), x1 = min(2 * xx + 1, M.w - 1);
                 st_texel(o + (size_t)k * 4, box4(ld_texel(r0 + (size_t)x0 * 4), ld_texel(r0 + (size_t)x1 * 4), ld_texel(r1 + (size_t)x0 * 4),
-                                                 ld_texel(r1 + (size_t)x1 * 4), M.srgb != 0, lin, thr));
+                                                 ld_texel(r1 + (size_t)x1 * 4), M.srgb != 0, S));
             }
         }
     }
@@ -189,7 +199,7 @@ __global__ void __launch_bounds__(256) batch_mip_kernel(const BatchMip *__restri
 
 const void *ztc_batch_mip_kernel_fn() { return (const void *)ztc::batch_mip_kernel; }
 
-cudaError_t ztc_launch_batch_mip(int grid, const ztc::BatchMip *mips, const ztc::BatchMipTile *tiles, int ntiles, const float *srgb_tables,
+cudaError_t ztc_launch_batch_mip(int grid, const ztc::BatchMip *mips, const ztc::BatchMipTile *tiles, int ntiles, const ztc::SrgbTables *srgb_tables,
                                  cudaStream_t stream) {
     if (ntiles <= 0) return cudaSuccess;
     ztc::batch_mip_kernel<<<grid, 256, 0, stream>>>(mips, tiles, ntiles, srgb_tables);

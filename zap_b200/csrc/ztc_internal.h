@@ -82,13 +82,25 @@ cudaError_t ztc_launch_batch_bc7_mode6(int cta, int regs, int grid, const ztc::B
 cudaError_t ztc_launch_batch_bc7_hard(int grid, const ztc::BatchLevel *levels, const uint32_t *bases, const int *level_of, int nlevels,
                                       const uint32_t *hard_count, const uint2 *hard_items, uint32_t *opaque_count, uint2 *opaque_items,
                                       cudaStream_t stream);
-cudaError_t ztc_launch_batch_mip(int grid, const ztc::BatchMip *mips, const ztc::BatchMipTile *tiles, int ntiles, const float *srgb_tables,
+namespace ztc { struct SrgbTables; }
+cudaError_t ztc_launch_batch_mip(int grid, const ztc::BatchMip *mips, const ztc::BatchMipTile *tiles, int ntiles, const ztc::SrgbTables *srgb_tables,
                                  cudaStream_t stream);
 const void *ztc_batch_bcn_kernel_fn(int fmt, int cta, int regs);
 const void *ztc_batch_bc7_kernel_fn(int cta, int regs);  // the mode 6 tile-queue kernel
 const void *ztc_batch_bc7_hard_kernel_fn();
 const void *ztc_batch_mip_kernel_fn();
-namespace ztc { void srgb_tables_host(float lin[256], float thr[256]); }
+namespace ztc {
+// The sRGB tables of the mip generator: linear value of each sRGB code (zap_tex.h:1360-1393), the thresholds where
+// a code rounds up (:1394-1427, + an infinite sentinel), and a search start per bucket of linear values (bucket =
+// the float's exponent and top 6 mantissa bits over [2^-16, 1], bucket 0 below): the answer at the bucket's lowest
+// value, a lower bound for every value in it.
+constexpr int kSrgbBuckets = 17 * 64;
+struct SrgbTables {
+    float lin[256], thr[256];
+    uint8_t bucket[kSrgbBuckets];
+};
+void srgb_tables_host(SrgbTables &t);
+}  // namespace ztc
 
 // Every device and pinned-host allocation of the library goes through these (api.cu), so a test can make chosen
 // ones fail (zap_tex_cuda_debug_fail_allocations) and check that each entry point reports ZTC_ERR_NO_MEMORY and the
