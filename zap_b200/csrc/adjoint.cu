@@ -40,7 +40,8 @@ struct LinBlock {
     bool covered, alpha_fixed;
 };
 
-ZTC_DEV void linear_form(int fmt, const uint8_t *blk, LinBlock &L, float e[6][4]) {
+// decoded (optional): the block's texels as the integer decoder gives them (zap_tex.h:1508-1517, :378-417)
+ZTC_DEV void linear_form(int fmt, const uint8_t *blk, LinBlock &L, float e[6][4], uint32_t *decoded = nullptr) {
     L.s1 = L.s2 = L.black = 0u;
     L.rot = 0;
     L.alpha_fixed = false;
@@ -57,6 +58,7 @@ ZTC_DEV void linear_form(int fmt, const uint8_t *blk, LinBlock &L, float e[6][4]
             L.aa[i] = L.a[i];
             if (!four && k == 3) L.black |= 1u << i;
         }
+        if (decoded) dec::bc1_block(v, false, decoded);
         for (int k = 0; k < 2; k++) {
             uint32_t c = k ? c1 : c0;
             int R = (c >> 11) & 31, G = (c >> 5) & 63, B = c & 31;
@@ -73,17 +75,27 @@ ZTC_DEV void linear_form(int fmt, const uint8_t *blk, LinBlock &L, float e[6][4]
     L.covered = dec::bc7_parse(w, F);
     L.mode = F.mode;
     if (!L.covered) {  // reserved mode: decodes to 0, zero gradient
-        for (int i = 0; i < 16; i++) L.a[i] = L.aa[i] = 0.0f;
+        #pragma unroll
+        for (int i = 0; i < 16; i++) { L.a[i] = L.aa[i] = 0.0f; if (decoded) decoded[i] = 0u; }
         for (int k = 0; k < 6; k++) for (int c = 0; c < 4; c++) e[k][c] = 0.0f;
         return;
     }
     L.rot = F.rot;
     L.alpha_fixed = !F.ab;
+    #pragma unroll
     for (int i = 0; i < 16; i++) {
         L.a[i] = 1.0f - (float)F.cw[i] / 64.0f;
         L.aa[i] = 1.0f - (float)F.aw[i] / 64.0f;
         L.s1 |= (uint32_t)(F.subset[i] == 1) << i;
         L.s2 |= (uint32_t)(F.subset[i] == 2) << i;
+        if (decoded) {  // the decoder's texel (dec::bc7_block), from the same fields
+            const int sb = F.subset[i];
+            int px[4];
+            for (int c = 0; c < 3; c++) px[c] = lerp64(F.ep[2 * sb][c], F.ep[2 * sb + 1][c], F.cw[i]);
+            px[3] = lerp64(F.ep[2 * sb][3], F.ep[2 * sb + 1][3], F.aw[i]);
+            if (F.rot) { int tmp = px[3]; px[3] = px[F.rot - 1]; px[F.rot - 1] = tmp; }
+            decoded[i] = pack_rgba(px[0], px[1], px[2], px[3]);
+        }
     }
     for (int k = 0; k < 6; k++) for (int c = 0; c < 4; c++) e[k][c] = (float)F.ep[k][c];
 }
@@ -347,17 +359,6 @@ ZTC_DEV int mode1_block_sse(const uint32_t t[16], const float e[6][4], int part,
     return err;
 }
 
-// squared error of a block as stored (the decoder's integer palette)
-ZTC_DEV int stored_sse(int fmt, const uint32_t t[16], const uint8_t *blk) {
-    uint32_t d[16];
-    dec::bcn_block(fmt, blk, d);
-    const int nc = fmt == ZTC_FMT_BC1 ? 3 : 4;
-    int err = 0;
-    for (int i = 0; i < 16; i++)
-        for (int c = 0; c < nc; c++) { int x = (int)chan(t[i], c) - (int)chan(d[i], c); err += x * x; }
-    return err;
-}
-
 // mode 5's rotation on a texel (swap A with R, G or B): decoded order <-> stored order
 ZTC_DEV uint32_t swap_alpha(uint32_t v, int rot) {
     if (!rot) return v;
@@ -366,38 +367,59 @@ ZTC_DEV uint32_t swap_alpha(uint32_t v, int rot) {
     return (v & ~((0xFFu << sh) | 0xFF000000u)) | (a << sh) | (c << 24);
 }
 
-__global__ void __launch_bounds__(128) refine_kernel(int fmt, SrcU8 src, int bw, int nblocks, uint8_t *__restrict__ blocks, int steps,
+// 3 resident CTAs per SM: the unrolled Adam state fits in 168 registers (72 bytes spilled); without a bound the
+// kernel takes 217 registers and 2 CTAs per SM, with 4 it spills 260 bytes
+__global__ void __launch_bounds__(128, 3) refine_kernel(int fmt, SrcU8 src, int bw, int nblocks, uint8_t *__restrict__ blocks, int steps,
                                                      float lr, uint32_t *__restrict__ sse0, uint32_t *__restrict__ sse1) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nblocks) return;
     const size_t bs = fmt == ZTC_FMT_BC1 ? 8 : 16;
     uint8_t *blk = blocks + (size_t)b * bs;
-    uint32_t t[16];
+    uint32_t t[16], d[16];
     gather_block(src, b % bw, b / bw, t);
-    const int before = stored_sse(fmt, t, blk);
-    int after = before;
     LinBlock L;
     float e[6][4];
-    linear_form(fmt, blk, L, e);
+    linear_form(fmt, blk, L, e, d);  // one parse: the linear form and the decoder's texels
+    const int nce = fmt == ZTC_FMT_BC1 ? 3 : 4;
+    int before = 0;
+    #pragma unroll
+    for (int i = 0; i < 16; i++)
+        #pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (c < nce) { const int x = (int)chan(t[i], c) - (int)chan(d[i], c); before += x * x; }
+    int after = before;
     const bool refinable = fmt == ZTC_FMT_BC1 || L.mode == 6 || L.mode == 5 || L.mode == 1;
     if (refinable && before > 0) {
         // Adam in stored channel order (the rotation only permutes channels, so the squared error is the same);
-        // mode 1's alpha is fixed at 255 and not a parameter; a texel of subset 1 moves endpoints 2 and 3
+        // mode 1's alpha is fixed at 255 and not a parameter; a texel of subset 1 moves endpoints 2 and 3. Every
+        // loop over texels, endpoints and channels is unrolled so the block's state stays in registers.
         uint32_t ts[16];
+        #pragma unroll
         for (int i = 0; i < 16; i++) ts[i] = swap_alpha(t[i], L.rot);
-        const int npar = L.alpha_fixed ? 3 : L.nc;
-        float m[4][4], v[4][4];
-        for (int k = 0; k < 4; k++) for (int c = 0; c < 4; c++) m[k][c] = v[k][c] = 0.0f;
+        const int npar = L.alpha_fixed ? 3 : L.nc, nk = L.s1 ? 4 : 2;
+        float P[4][4], m[4][4], v[4][4];
+        #pragma unroll
+        for (int k = 0; k < 4; k++)
+            #pragma unroll
+            for (int c = 0; c < 4; c++) { P[k][c] = e[k][c]; m[k][c] = v[k][c] = 0.0f; }
         const float b1 = 0.9f, b2 = 0.999f, inv_n = 2.0f / (16.0f * (float)L.nc);
         float p1 = 1.0f, p2 = 1.0f;
+        #pragma unroll 1
         for (int s = 0; s < steps; s++) {
-            float g[4][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+            float g[4][4];
+            #pragma unroll
+            for (int k = 0; k < 4; k++)
+                #pragma unroll
+                for (int c = 0; c < 4; c++) g[k][c] = 0.0f;
+            #pragma unroll
             for (int i = 0; i < 16; i++) {
                 if ((L.black >> i) & 1u) continue;  // a constant: no gradient
                 const bool in1 = (L.s1 >> i) & 1u;
-                for (int c = 0; c < npar; c++) {  // forward decode, residual, adjoint
+                #pragma unroll
+                for (int c = 0; c < 4; c++) {  // forward decode, residual, adjoint
+                    if (c >= npar) continue;
                     const float a = c == 3 ? L.aa[i] : L.a[i];
-                    const float e0 = in1 ? e[2][c] : e[0][c], e1 = in1 ? e[3][c] : e[1][c];
+                    const float e0 = in1 ? P[2][c] : P[0][c], e1 = in1 ? P[3][c] : P[1][c];
                     const float r = (a * e0 + (1.0f - a) * e1 - (float)chan(ts[i], c)) * inv_n;
                     const float g0 = a * r, g1 = (1.0f - a) * r;
                     if (in1) { g[2][c] += g0; g[3][c] += g1; }
@@ -405,15 +427,21 @@ __global__ void __launch_bounds__(128) refine_kernel(int fmt, SrcU8 src, int bw,
                 }
             }
             p1 *= b1; p2 *= b2;
-            const int nk = L.s1 ? 4 : 2;
-            for (int k = 0; k < nk; k++)
-                for (int c = 0; c < npar; c++) {
+            #pragma unroll
+            for (int k = 0; k < 4; k++)
+                #pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    if (k >= nk || c >= npar) continue;
                     m[k][c] = b1 * m[k][c] + (1.0f - b1) * g[k][c];
                     v[k][c] = b2 * v[k][c] + (1.0f - b2) * g[k][c] * g[k][c];
                     float mh = m[k][c] / (1.0f - p1), vh = v[k][c] / (1.0f - p2);
-                    e[k][c] = fminf(255.0f, fmaxf(0.0f, e[k][c] - lr * mh / (sqrtf(vh) + 1e-8f)));
+                    P[k][c] = fminf(255.0f, fmaxf(0.0f, P[k][c] - lr * mh / (sqrtf(vh) + 1e-8f)));
                 }
         }
+        #pragma unroll
+        for (int k = 0; k < 4; k++)
+            #pragma unroll
+            for (int c = 0; c < 4; c++) e[k][c] = P[k][c];
         int ne = 1 << 30;
         if (fmt == ZTC_FMT_BC1) {
             uint2 nb;
