@@ -456,13 +456,20 @@ def main():
                 "kernels": {k: {"launches": v[0], "ms": v[1], "units": v[2], "share": v[1] / sum(x[1] for x in rep.values())}
                             for k, v in rep.items()}}
     # the bound that binds: counted algorithmic ops against the SMs' measured issue rate (one launch = one 2048^2
-    # texture); the probe runs after the timed region
+    # texture). The probe runs after every timed workload of the run (its seconds of full load would otherwise warm
+    # the GPU before them); the ALU fractions are filled in then.
     csum = clocks.summary()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    measure_alu_peak(dev, sms, local)
     mhz = csum.get("sm_mhz") or csum.get("sm_max_mhz")
-    roofline["alu"] = alu_roofline(name, (ops_per_texture(name), avg_ms), mhz, sms)
-    roofline["alu_kernels"] = {k: alu_roofline(k, (ops_per_texture(k), v[1] / max(1, v[0])), mhz, sms) for k, v in rep.items()}
+
+    def fill_alu(extra):
+        measure_alu_peak(dev, sms, local)
+        roofline["alu"] = alu_roofline(name, (ops_per_texture(name), avg_ms), mhz, sms)
+        roofline["alu_kernels"] = {k: alu_roofline(k, (ops_per_texture(k), v[1] / max(1, v[0])), mhz, sms) for k, v in rep.items()}
+        for entry in (extra or {}).values():
+            counted, ms_enc = entry.pop("_alu_in", (None, None))
+            if counted:  # the whole encode (all its kernels) against the ALU roofline
+                entry["alu"] = alu_roofline(counted, (ops_per_texture(counted), ms_enc), mhz, sms)
 
     line = {"metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
@@ -470,7 +477,7 @@ def main():
             "config": {"workload": WORKLOAD, "l2": f"inputs larger than L2: ring of {ring} distinct {W}x{H} textures",
                        "parallelism": "independent replicas" if world > 1 else "1 gpu",
                        "step": "replay of a CUDA graph of one zap_tex_cuda_bc_encode_dev call per ring slot"},
-            "roofline": roofline, "gpu_launches": launches, "clocks": clocks.summary(), "alu_peak": ALU_PEAK}
+            "roofline": roofline, "gpu_launches": launches, "clocks": clocks.summary()}
 
     if rank == 0:
         # e2e: host C ABI, pinned host memory, copies inside the timed region. The buffers are allocated and the
@@ -541,6 +548,8 @@ def main():
             line["batched"] = batched_workload(args, dev)
             line["refine"] = refine_workload(args, dev)
             line["rdo"] = rdo_workload(dev)
+        fill_alu(line.get("extra"))
+        line["alu_peak"] = ALU_PEAK
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
@@ -797,8 +806,8 @@ def extra_workloads(args, dev, sm_mhz=None, sms=148):
         mps = steps * npix / 1e6 / (ms / 1e3)
         res[name] = {"Mpix_s": mps, "ms_per_encode": ms / steps, "GB_s_algorithmic": mps * 1e6 * alg_bytes_per_px / 1e9,
                      "timing": "median of 5 segments of %d encodes (CUDA events)" % seg}
-        if counted:  # the whole encode (all its kernels) against the ALU roofline
-            res[name]["alu"] = alu_roofline(counted, (ops_per_texture(counted), ms / steps), sm_mhz, sms)
+        if counted:  # the whole encode against the ALU roofline, once the peak is measured (main's fill_alu)
+            res[name]["_alu_in"] = (counted, ms / steps)
         torch.cuda.synchronize()
         res[name].update(parity(texs[0], outs[0], fmt, chans))
         cpu = res[name].get("cpu_baseline")
