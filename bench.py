@@ -169,6 +169,15 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def library_md5():
+    """First 12 hex digits of the MD5 of the CUDA library this run loaded (which build a line measured)."""
+    import hashlib
+
+    import zap_b200
+    with open(zap_b200._lib.LIB_PATH, "rb") as f:
+        return hashlib.md5(f.read()).hexdigest()[:12]
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -477,7 +486,7 @@ def main():
             "config": {"workload": WORKLOAD, "l2": f"inputs larger than L2: ring of {ring} distinct {W}x{H} textures",
                        "parallelism": "independent replicas" if world > 1 else "1 gpu",
                        "step": "replay of a CUDA graph of one zap_tex_cuda_bc_encode_dev call per ring slot"},
-            "roofline": roofline, "gpu_launches": launches, "clocks": clocks.summary()}
+            "roofline": roofline, "gpu_launches": launches, "clocks": clocks.summary(), "library_md5": library_md5()}
 
     if rank == 0:
         # e2e: host C ABI, pinned host memory, copies inside the timed region. The buffers are allocated and the

@@ -301,16 +301,9 @@ ZTC_DEV uint32_t rotate_texel(uint32_t v, int rot) {  // mode 5 rotation: swap A
     }
     return v;
 }
-ZTC_DEV uint32_t part_texel(uint32_t v, int rot, bool alpha) {
-    const uint32_t r = rotate_texel(v, rot);
-    return alpha ? (r >> 24) : (r & 0x00FFFFFFu);
-}
 // The mode 5 helpers take the part at compile time, KIND = kPartColour (rotated RGB, 7-bit endpoints) or kPartAlpha
-// (rotated A, 8-bit endpoints): the alpha part's loops run over its one channel. The `alpha` and `nc` arguments
-// restate the part for the shared code below.
+// (rotated A, 8-bit endpoints): the alpha part's loops run over its one channel.
 constexpr int kPartColour = 1, kPartAlpha = 2;
-template <int KIND>
-ZTC_DEV bool part_is_alpha(bool) { return KIND == kPartAlpha; }
 
 template <int KIND>
 ZTC_DEV void m5_quant(const float v[3], int nc, int n, int q[3], int x8[3]) {
@@ -328,9 +321,11 @@ ZTC_DEV void m5_quant(const float v[3], int nc, int n, int q[3], int x8[3]) {
         q[c] = bq; x8[c] = expand_bits(bq, n);
     }
 }
+// The part's texels p[16] are in registers (the colour part: rotated RGB in the low three bytes; the alpha part:
+// the rotated alpha in byte 0), and the texel loops are unrolled: the modes-5/1 launch holds few warps per SM, so
+// the length of each lane's dependent chain sets its time.
 template <int KIND>
-ZTC_DEV int m5_fit(TexRef ts, int rot, bool alpha, const int x0[3], const int x1[3], uint32_t &idx) {
-    alpha = part_is_alpha<KIND>(alpha);
+ZTC_DEV int m5_fit(const uint32_t p[16], const int x0[3], const int x1[3], uint32_t &idx) {
     uint32_t pal[4];
     int A[4];
     #pragma unroll
@@ -342,12 +337,11 @@ ZTC_DEV int m5_fit(TexRef ts, int rot, bool alpha, const int x0[3], const int x1
     }
     int err = 0;
     uint32_t bits = 0;
-    #pragma unroll 1
+    #pragma unroll
     for (int i = 0; i < 16; i++) {
-        const uint32_t p = part_texel(ts[i], rot, alpha);
-        int m = min(min(A[0] - 8 * (int)dot4(p, pal[0]), A[1] - 8 * (int)dot4(p, pal[1])),
-                    min(A[2] - 8 * (int)dot4(p, pal[2]), A[3] - 8 * (int)dot4(p, pal[3])));
-        err += (m >> 2) + (int)dot4(p, p);
+        int m = min(min(A[0] - 8 * (int)dot4(p[i], pal[0]), A[1] - 8 * (int)dot4(p[i], pal[1])),
+                    min(A[2] - 8 * (int)dot4(p[i], pal[2]), A[3] - 8 * (int)dot4(p[i], pal[3])));
+        err += (m >> 2) + (int)dot4(p[i], p[i]);
         bits |= (uint32_t)(m & 3) << (2 * i);
     }
     idx = bits;
@@ -358,17 +352,15 @@ ZTC_DEV int m5_fit(TexRef ts, int rot, bool alpha, const int x0[3], const int x1
 // below 1, u*x and w*x multiples of 2^-6 below 256, and no partial sum of 16 terms needs more than 24 bits in those
 // units. Integer sums scaled by 2^-12 and 2^-6 are therefore the reference's floats, bit for bit, in any order.
 template <int KIND>
-ZTC_DEV bool m5_lsq(TexRef ts, int rot, bool alpha, int nc, uint32_t idx, float lo[3], float hi[3]) {
-    alpha = part_is_alpha<KIND>(alpha);
+ZTC_DEV bool m5_lsq(const uint32_t p[16], int nc, uint32_t idx, float lo[3], float hi[3]) {
     constexpr int kC = KIND == kPartAlpha ? 1 : 3;
     int aa = 0, ab = 0, bb = 0, sa[3] = {0, 0, 0}, sb[3] = {0, 0, 0};
-    #pragma unroll 1
+    #pragma unroll
     for (int i = 0; i < 16; i++) {
         const int k = (int)((0x402B1500u >> (8 * ((idx >> (2 * i)) & 3u))) & 0xFFu), u = 64 - k;  // w2: 0, 21, 43, 64
         aa += u * u; ab += u * k; bb += k * k;
-        const uint32_t p = part_texel(ts[i], rot, alpha);
         #pragma unroll
-        for (int c = 0; c < kC; c++) { const int x = (int)chan(p, c); sa[c] += u * x; sb[c] += k * x; }
+        for (int c = 0; c < kC; c++) { const int x = (int)chan(p[i], c); sa[c] += u * x; sb[c] += k * x; }
     }
     const float faa = (float)aa * (1.0f / 4096.0f), fab = (float)ab * (1.0f / 4096.0f), fbb = (float)bb * (1.0f / 4096.0f);
     float det = faa * fbb - fab * fab;
@@ -383,17 +375,17 @@ ZTC_DEV bool m5_lsq(TexRef ts, int rot, bool alpha, int nc, uint32_t idx, float 
 }
 // quantise, fit, up to two least-squares refits (zap_tex.h:626-657); lo / hi: the start endpoints
 template <int KIND>
-ZTC_DEV int m5_part(TexRef ts, int rot, bool alpha, float lo[3], float hi[3], int q[2][3], uint32_t &idx) {
-    alpha = part_is_alpha<KIND>(alpha);
+ZTC_DEV int m5_part(const uint32_t p[16], float lo[3], float hi[3], int q[2][3], uint32_t &idx) {
+    constexpr bool alpha = KIND == kPartAlpha;
     const int nc = alpha ? 1 : 3, n = alpha ? 8 : 7;
     int err = 0;
     #pragma unroll 1
     for (int it = 0; it < 3; it++) {
-        if (it > 0 && !m5_lsq<KIND>(ts, rot, alpha, nc, idx, lo, hi)) break;
+        if (it > 0 && !m5_lsq<KIND>(p, nc, idx, lo, hi)) break;
         int tq[2][3], x0[3], x1[3];
         m5_quant<KIND>(lo, nc, n, tq[0], x0); m5_quant<KIND>(hi, nc, n, tq[1], x1);
         uint32_t ti;
-        const int e = m5_fit<KIND>(ts, rot, alpha, x0, x1, ti);
+        const int e = m5_fit<KIND>(p, x0, x1, ti);
         if (it > 0 && e >= err) break;
         err = e; idx = ti;
         #pragma unroll
@@ -636,13 +628,13 @@ constexpr int kHardBlocks = 8;
 __device__ __forceinline__ int m5_colour_lane(TexRef ts, int rot, uint32_t &qw, uint32_t &qw2, uint32_t &idx) {
     uint32_t r[16];
     #pragma unroll
-    for (int i = 0; i < 16; i++) r[i] = rotate_texel(ts[i], rot);
+    for (int i = 0; i < 16; i++) r[i] = rotate_texel(ts[i], rot) & 0x00FFFFFFu;  // the colour part's texels
     float lo[4], hi[4];
     pca_endpoints<3>(r, 0xFFFFu, lo, hi);  // the colour part starts from the principal axis of the rotated RGB
     float lo5[3] = {lo[0], lo[1], lo[2]}, hi5[3] = {hi[0], hi[1], hi[2]};
     int q5[2][3] = {{0, 0, 0}, {0, 0, 0}};
     uint32_t i5 = 0;
-    const int e5 = m5_part<kPartColour>(ts, rot, false, lo5, hi5, q5, i5);
+    const int e5 = m5_part<kPartColour>(r, lo5, hi5, q5, i5);
     if (i5 & 2u) {  // anchor MSB must be 0 (zap_tex.h:673-674): swap, 3 - i == i ^ 3 for 2-bit indices
         #pragma unroll
         for (int c = 0; c < 3; c++) { int t = q5[0][c]; q5[0][c] = q5[1][c]; q5[1][c] = t; }
@@ -656,15 +648,17 @@ __device__ __forceinline__ int m5_colour_lane(TexRef ts, int rot, uint32_t &qw, 
 
 __device__ __forceinline__ int m5_alpha_lane(TexRef ts, int rot, uint32_t &qw, uint32_t &idx) {
     float lo5[3] = {255.0f, 0.0f, 0.0f}, hi5[3] = {0.0f, 0.0f, 0.0f};
-    #pragma unroll 1
-    for (int i = 0; i < 16; i++) {  // the alpha part starts from the rotated alpha's range
-        const float a = (float)(rotate_texel(ts[i], rot) >> 24);
+    uint32_t r[16];
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {  // the alpha part's texels; it starts from their range
+        r[i] = rotate_texel(ts[i], rot) >> 24;
+        const float a = (float)r[i];
         if (a < lo5[0]) lo5[0] = a;
         if (a > hi5[0]) hi5[0] = a;
     }
     int q5[2][3] = {{0, 0, 0}, {0, 0, 0}};
     uint32_t i5 = 0;
-    const int e5 = m5_part<kPartAlpha>(ts, rot, true, lo5, hi5, q5, i5);
+    const int e5 = m5_part<kPartAlpha>(r, lo5, hi5, q5, i5);
     if (i5 & 2u) {
         int t = q5[0][0]; q5[0][0] = q5[1][0]; q5[1][0] = t;
         i5 ^= 0xFFFFFFFFu;
@@ -674,7 +668,7 @@ __device__ __forceinline__ int m5_alpha_lane(TexRef ts, int rot, uint32_t &qw, u
     return e5;
 }
 
-__global__ void __launch_bounds__(64, 8) bc7_hard_kernel(SrcU8 src, int bw, int by0, BlockOut out, size_t b0,
+__global__ void __launch_bounds__(64, ZTC_MINB_BC7_MODE5) bc7_hard_kernel(SrcU8 src, int bw, int by0, BlockOut out, size_t b0,
                                                         const uint32_t *__restrict__ count, const uint2 *__restrict__ items) {
     __shared__ uint32_t s_tex[kHardBlocks][17];  // per block (padded: the groups of a warp hit distinct banks)
     __shared__ uint2 s_item[kHardBlocks];        // (block index, mode-6 SSE); x = ~0 past the list's end
@@ -809,7 +803,7 @@ batch_bc7_mode6_kernel(const BatchLevel *__restrict__ levels, const BatchTile *_
 // level_of[k]: its index in `levels`), laid out like the single-image kernel: a CTA of two warps takes 8 listed
 // blocks at a time, warp 0 fitting their colour parts and warp 1 their alpha parts (lane = block * 4 + rotation);
 // the block is written when mode 5 wins, and each opaque block goes, with its SSE after mode 5, to the mode-1 list.
-__global__ void __launch_bounds__(64, 8) batch_bc7_mode5_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__restrict__ bases,
+__global__ void __launch_bounds__(64, ZTC_MINB_BC7_MODE5) batch_bc7_mode5_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__restrict__ bases,
                                                                const int *__restrict__ level_of, int nlevels,
                                                                const uint32_t *__restrict__ count, const uint2 *__restrict__ items,
                                                                uint32_t *__restrict__ next_count, uint2 *__restrict__ next_items) {

@@ -27,6 +27,10 @@
 #ifndef ZTC_MINB_BC7_HARD
 #define ZTC_MINB_BC7_HARD 1
 #endif
+// the mode-5 launches (single image and batch): resident 64-thread CTAs per SM
+#ifndef ZTC_MINB_BC7_MODE5
+#define ZTC_MINB_BC7_MODE5 8
+#endif
 #ifndef ZTC_MINB_BCN
 #define ZTC_MINB_BCN 8
 #endif
