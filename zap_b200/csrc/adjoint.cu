@@ -70,8 +70,29 @@ ZTC_DEV void linear_form(int fmt, const uint8_t *blk, LinBlock &L, float e[6][4]
     }
     uint4 v = *(const uint4 *)blk;
     const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-    dec::Bc7Fields F;
     L.nc = 4;
+    if ((w[0] & 0x7Fu) == 0x40u) {  // mode 6, the encoder's common case: its fixed layout read directly
+        L.mode = 6; L.covered = true;  // R0 R1 G0 G1 B0 B1 A0 A1 (7 bits each), a p-bit per endpoint, 4-bit indices
+        int ep[2][4];
+        #pragma unroll
+        for (int c = 0; c < 4; c++)
+            #pragma unroll
+            for (int k = 0; k < 2; k++) {
+                ep[k][c] = (int)((get_bits128(w, 7 + 14 * c + 7 * k, 7) << 1) | get_bits128(w, 63 + k, 1));
+                e[k][c] = (float)ep[k][c];
+            }
+        for (int k = 2; k < 6; k++) for (int c = 0; c < 4; c++) e[k][c] = 0.0f;
+        #pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const int wt = w4(i == 0 ? (int)get_bits128(w, 65, 3) : (int)get_bits128(w, 68 + 4 * (i - 1), 4));
+            L.a[i] = L.aa[i] = 1.0f - (float)wt / 64.0f;
+            if (decoded)
+                decoded[i] = pack_rgba(lerp64(ep[0][0], ep[1][0], wt), lerp64(ep[0][1], ep[1][1], wt), lerp64(ep[0][2], ep[1][2], wt),
+                                       lerp64(ep[0][3], ep[1][3], wt));
+        }
+        return;
+    }
+    dec::Bc7Fields F;
     L.covered = dec::bc7_parse(w, F);
     L.mode = F.mode;
     if (!L.covered) {  // reserved mode: decodes to 0, zero gradient
