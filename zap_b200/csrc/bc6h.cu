@@ -227,9 +227,14 @@ __device__ __forceinline__ uint4 bc6h_encode_cta(bool valid, uint16_t (*s_t)[CTA
                 base0 += w < warp ? c0 : 0; base1 += w < warp ? c1 : 0; t0 += c0; t1 += c1;
             }
             const unsigned below = (1u << lane) - 1u;
-            const int p0 = base0 + __popc(b0 & below), p1 = t0 + base1 + __popc(b1 & below);
-            if (more0 && ZTC_IN_BOUNDS(p0, 2 * CTA, 4)) s_list[p0] = (uint16_t)(tid << 1);
-            if (more1 && ZTC_IN_BOUNDS(p1, 2 * CTA, 4)) s_list[p1] = (uint16_t)((tid << 1) | 1);
+            if (more0) {
+                const int p0 = base0 + __popc(b0 & below);
+                if (ZTC_IN_BOUNDS(p0, 2 * CTA, 4)) s_list[p0] = (uint16_t)(tid << 1);
+            }
+            if (more1) {
+                const int p1 = t0 + base1 + __popc(b1 & below);
+                if (ZTC_IN_BOUNDS(p1, 2 * CTA, 4)) s_list[p1] = (uint16_t)((tid << 1) | 1);
+            }
             total = t0 + t1;
             __syncthreads();
         }
@@ -239,7 +244,9 @@ __device__ __forceinline__ uint4 bc6h_encode_cta(bool valid, uint16_t (*s_t)[CTA
             const int k = tid + (job - 2) * CTA;
             active = k < total;
             if (active) { owner = s_list[k] >> 1; st = s_list[k] & 1; }
+#ifdef ZTC_CHECKS
             if (active && !ZTC_IN_BOUNDS(owner, CTA, 8)) active = false;
+#endif
             first = 3; last = 4;
         }
         if (active) {
