@@ -197,21 +197,45 @@ ZTC_DEV void bc1_palette(uint32_t c0, uint32_t c1, int pal[4][3]) {
         pal[2][c] = (2 * a + b + 1) / 3; pal[3][c] = (a + 2 * b + 1) / 3;
     }
 }
+// Nearest palette entry by squared distance over a texel's bytes: |t - p|^2 = |t|^2 + |p|^2 - 2 t.p, so with |t|^2
+// fixed the entry minimising |p|^2 - 2 t.p wins (the first of equals, as in a plain scan); each candidate costs one
+// four-byte dot product. Entries hold zero in the bytes the distance leaves out. Returns the index; `dist` gets
+// |t - p|^2 for the texel's bytes masked like the entries.
+template <int N>
+ZTC_DEV int nearest_entry(uint32_t t, const uint32_t pal[N], const int pp[N], int tt, int &dist) {
+    int bj = 0, be = 1 << 30;
+    #pragma unroll
+    for (int j = 0; j < N; j++) {
+        const int s = pp[j] - 2 * (int)dot4(t, pal[j]);
+        if (s < be) { be = s; bj = j; }
+    }
+    dist = be + tt;
+    return bj;
+}
+template <int N>
+ZTC_DEV void entry_norms(const uint32_t pal[N], int pp[N]) {
+    #pragma unroll
+    for (int j = 0; j < N; j++) pp[j] = (int)dot4(pal[j], pal[j]);
+}
+
 // canonical BC1 block for endpoints (c0 > c1 with best indices, or solid) and its SSE
 ZTC_DEV int bc1_block_sse(const uint32_t t[16], uint32_t c0, uint32_t c1, uint2 &blk) {
     if (c0 < c1) { uint32_t s = c0; c0 = c1; c1 = s; }
-    int pal[4][3], err = 0;
+    int pal[4][3], pp[4], err = 0;
     bc1_palette(c0, c1, pal);
+    uint32_t pk[4];
+    #pragma unroll
+    for (int k = 0; k < 4; k++) pk[k] = pack_rgb(pal[k][0], pal[k][1], pal[k][2]);
+    if (c0 == c1) pk[1] = pk[2] = pk[3] = pk[0];  // solid: every texel takes index 0 (the first of equals)
+    entry_norms<4>(pk, pp);
     uint32_t bits = 0;
+    #pragma unroll
     for (int i = 0; i < 16; i++) {
-        int bk = 0, be = 1 << 30;
-        for (int k = 0; k < (c0 == c1 ? 1 : 4); k++) {
-            int d = 0;
-            for (int c = 0; c < 3; c++) { int x = (int)chan(t[i], c) - pal[k][c]; d += x * x; }
-            if (d < be) { be = d; bk = k; }
-        }
+        const uint32_t ti = t[i] & 0xFFFFFFu;
+        int d;
+        const int bk = nearest_entry<4>(ti, pk, pp, (int)dot4(ti, ti), d);
         bits |= (uint32_t)bk << (2 * i);
-        err += be;
+        err += d;
     }
     blk = make_uint2(c0 | (c1 << 16), bits);
     return err;
@@ -223,6 +247,7 @@ ZTC_DEV int quant_plain(float v, int n) {
     const int g = f2i_x86(v * (float)top / 255.0f + 0.5f);
     int bq = 0;
     float bd = 3.0e38f;
+    #pragma unroll
     for (int k = 0; k < 3; k++) {
         const int q = clampi(around(g, k), 0, top);
         const float d = fabsf((float)expand_bits(q, n) - v);
@@ -236,6 +261,7 @@ ZTC_DEV int quant_pbit(float v, int n, int p, float &dist) {
     const int g = f2i_x86(((v * (float)((1 << n) - 1) / 255.0f) - (float)p) / 2.0f + 0.5f);
     int bq = 0;
     float bd = 3.0e38f;
+    #pragma unroll
     for (int k = 0; k < 3; k++) {
         const int q = clampi(around(g, k), 0, top);
         const float d = fabsf((float)expand_bits((q << 1) | p, n) - v);
@@ -248,37 +274,52 @@ ZTC_DEV int quant_pbit(float v, int n, int p, float &dist) {
 // BC7 mode 6 (zap_tex.h:520-527 layout): 7 bits + a p-bit per endpoint, 4-bit indices, anchor texel 0
 ZTC_DEV int mode6_block_sse(const uint32_t t[16], const float e[6][4], uint4 &out) {
     int q[2][4], pb[2], x[2][4];
+    #pragma unroll
     for (int k = 0; k < 2; k++) {
         float best = 3.0e38f;
+        #pragma unroll
         for (int p = 0; p < 2; p++) {
             int qq[4];
             float err = 0.0f, d;
+            #pragma unroll
             for (int c = 0; c < 4; c++) { qq[c] = quant_pbit(e[k][c], 8, p, d); err += d * d; }
-            if (err < best) { best = err; pb[k] = p; for (int c = 0; c < 4; c++) q[k][c] = qq[c]; }
+            if (err < best) {
+                best = err; pb[k] = p;
+                #pragma unroll
+                for (int c = 0; c < 4; c++) q[k][c] = qq[c];
+            }
         }
+        #pragma unroll
         for (int c = 0; c < 4; c++) x[k][c] = expand_bits((q[k][c] << 1) | pb[k], 8);
     }
+    uint32_t pal[16];
+    int pp[16];
+    #pragma unroll
+    for (int j = 0; j < 16; j++)
+        pal[j] = pack_rgba(lerp64(x[0][0], x[1][0], w4(j)), lerp64(x[0][1], x[1][1], w4(j)), lerp64(x[0][2], x[1][2], w4(j)),
+                           lerp64(x[0][3], x[1][3], w4(j)));
+    entry_norms<16>(pal, pp);
     int idx[16], err = 0;
+    #pragma unroll
     for (int i = 0; i < 16; i++) {
-        int bj = 0, be = 1 << 30;
-        for (int j = 0; j < 16; j++) {
-            int d = 0;
-            for (int c = 0; c < 4; c++) { int y = (int)chan(t[i], c) - lerp64(x[0][c], x[1][c], w4(j)); d += y * y; }
-            if (d < be) { be = d; bj = j; }
-        }
-        idx[i] = bj;
-        err += be;
+        int d;
+        idx[i] = nearest_entry<16>(t[i], pal, pp, (int)dot4(t[i], t[i]), d);
+        err += d;
     }
     if (idx[0] >= 8) {  // anchor: swap the endpoints, mirror the indices (decoded values unchanged)
+        #pragma unroll
         for (int c = 0; c < 4; c++) { int s = q[0][c]; q[0][c] = q[1][c]; q[1][c] = s; }
         int s = pb[0]; pb[0] = pb[1]; pb[1] = s;
+        #pragma unroll
         for (int i = 0; i < 16; i++) idx[i] = 15 - idx[i];
     }
     Bits128 o;
     o.put(1u << 6, 7);
+    #pragma unroll
     for (int c = 0; c < 4; c++) { o.put((uint32_t)q[0][c], 7); o.put((uint32_t)q[1][c], 7); }
     o.put((uint32_t)pb[0], 1); o.put((uint32_t)pb[1], 1);
     o.put((uint32_t)idx[0], 3);
+    #pragma unroll
     for (int i = 1; i < 16; i++) o.put((uint32_t)idx[i], 4);
     out = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
     return err;
@@ -288,39 +329,58 @@ ZTC_DEV int mode6_block_sse(const uint32_t t[16], const float e[6][4], uint4 &ou
 // colour and alpha indices, each set with its anchor at texel 0; ts: the texels in stored channel order
 ZTC_DEV int mode5_block_sse(const uint32_t ts[16], const float e[6][4], int rot, uint4 &out) {
     int q[2][4], x[2][4];
+    #pragma unroll
     for (int k = 0; k < 2; k++) {
+        #pragma unroll
         for (int c = 0; c < 3; c++) { q[k][c] = quant_plain(e[k][c], 7); x[k][c] = expand_bits(q[k][c], 7); }
         q[k][3] = x[k][3] = clampi(f2i_x86(e[k][3] + 0.5f), 0, 255);
     }
+    uint32_t pal[4];
+    int pp[4], pa[4];
+    #pragma unroll
+    for (int j = 0; j < 4; j++) {
+        pal[j] = pack_rgb(lerp64(x[0][0], x[1][0], w2(j)), lerp64(x[0][1], x[1][1], w2(j)), lerp64(x[0][2], x[1][2], w2(j)));
+        pa[j] = lerp64(x[0][3], x[1][3], w2(j));
+    }
+    entry_norms<4>(pal, pp);
     int ci[16], ai[16], err = 0;
+    #pragma unroll
     for (int i = 0; i < 16; i++) {
-        int bj = 0, be = 1 << 30, bk = 0, bae = 1 << 30;
+        const uint32_t tc = ts[i] & 0xFFFFFFu;
+        int d;
+        ci[i] = nearest_entry<4>(tc, pal, pp, (int)dot4(tc, tc), d);
+        const int ta = (int)(ts[i] >> 24);
+        int bk = 0, bae = 1 << 30;
+        #pragma unroll
         for (int j = 0; j < 4; j++) {
-            int d = 0;
-            for (int c = 0; c < 3; c++) { int y = (int)chan(ts[i], c) - lerp64(x[0][c], x[1][c], w2(j)); d += y * y; }
-            if (d < be) { be = d; bj = j; }
-            int y = (int)chan(ts[i], 3) - lerp64(x[0][3], x[1][3], w2(j));
+            const int y = ta - pa[j];
             if (y * y < bae) { bae = y * y; bk = j; }
         }
-        ci[i] = bj; ai[i] = bk;
-        err += be + bae;
+        ai[i] = bk;
+        err += d + bae;
     }
     if (ci[0] >= 2) {
+        #pragma unroll
         for (int c = 0; c < 3; c++) { int s = q[0][c]; q[0][c] = q[1][c]; q[1][c] = s; }
+        #pragma unroll
         for (int i = 0; i < 16; i++) ci[i] = 3 - ci[i];
     }
     if (ai[0] >= 2) {
         int s = q[0][3]; q[0][3] = q[1][3]; q[1][3] = s;
+        #pragma unroll
         for (int i = 0; i < 16; i++) ai[i] = 3 - ai[i];
     }
     Bits128 o;
     o.put(1u << 5, 6);
     o.put((uint32_t)rot, 2);
+    #pragma unroll
     for (int c = 0; c < 3; c++) { o.put((uint32_t)q[0][c], 7); o.put((uint32_t)q[1][c], 7); }
     o.put((uint32_t)q[0][3], 8); o.put((uint32_t)q[1][3], 8);
     o.put((uint32_t)ci[0], 1);
+    #pragma unroll
     for (int i = 1; i < 16; i++) o.put((uint32_t)ci[i], 2);
     o.put((uint32_t)ai[0], 1);
+    #pragma unroll
     for (int i = 1; i < 16; i++) o.put((uint32_t)ai[i], 2);
     out = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
     return err;
@@ -337,44 +397,75 @@ ZTC_DEV int mode1_block_sse(const uint32_t t[16], const float e[6][4], int part,
     const int anchor1 = 15;
 #endif
     int q[4][3], pb[2], x[4][3];
+    #pragma unroll
     for (int s = 0; s < 2; s++) {
         float best = 3.0e38f;
+        #pragma unroll
         for (int p = 0; p < 2; p++) {
             int qq[2][3];
             float err = 0.0f, d;
+            #pragma unroll
             for (int k = 0; k < 2; k++)
+                #pragma unroll
                 for (int c = 0; c < 3; c++) { qq[k][c] = quant_pbit(e[2 * s + k][c], 7, p, d); err += d * d; }
             if (err < best) {
                 best = err; pb[s] = p;
-                for (int k = 0; k < 2; k++) for (int c = 0; c < 3; c++) q[2 * s + k][c] = qq[k][c];
+                #pragma unroll
+                for (int k = 0; k < 2; k++)
+                    #pragma unroll
+                    for (int c = 0; c < 3; c++) q[2 * s + k][c] = qq[k][c];
             }
         }
-        for (int k = 0; k < 2; k++) for (int c = 0; c < 3; c++) x[2 * s + k][c] = expand_bits((q[2 * s + k][c] << 1) | pb[s], 7);
+        #pragma unroll
+        for (int k = 0; k < 2; k++)
+            #pragma unroll
+            for (int c = 0; c < 3; c++) x[2 * s + k][c] = expand_bits((q[2 * s + k][c] << 1) | pb[s], 7);
+    }
+    uint32_t pal[2][8];
+    int pp[2][8];
+    #pragma unroll
+    for (int s = 0; s < 2; s++) {
+        #pragma unroll
+        for (int j = 0; j < 8; j++)
+            pal[s][j] = pack_rgb(lerp64(x[2 * s][0], x[2 * s + 1][0], w3(j)), lerp64(x[2 * s][1], x[2 * s + 1][1], w3(j)),
+                                 lerp64(x[2 * s][2], x[2 * s + 1][2], w3(j)));
+        entry_norms<8>(pal[s], pp[s]);
     }
     int idx[16], err = 0;
+    #pragma unroll
     for (int i = 0; i < 16; i++) {
-        const int s = (mask >> i) & 1u;
-        int bj = 0, be = 1 << 30;
-        for (int j = 0; j < 8; j++) {
-            int d = 0;
-            for (int c = 0; c < 3; c++) { int y = (int)chan(t[i], c) - lerp64(x[2 * s][c], x[2 * s + 1][c], w3(j)); d += y * y; }
-            if (d < be) { be = d; bj = j; }
-        }
+        const uint32_t tc = t[i] & 0xFFFFFFu;
+        const bool s1 = (mask >> i) & 1u;
+        uint32_t ps[8];
+        int qs[8];
+        #pragma unroll
+        for (int j = 0; j < 8; j++) { ps[j] = s1 ? pal[1][j] : pal[0][j]; qs[j] = s1 ? pp[1][j] : pp[0][j]; }
+        int d;
+        idx[i] = nearest_entry<8>(tc, ps, qs, (int)dot4(tc, tc), d);
         const int ya = (int)chan(t[i], 3) - 255;
-        idx[i] = bj;
-        err += be + ya * ya;
+        err += d + ya * ya;
     }
+    #pragma unroll
     for (int s = 0; s < 2; s++) {
         const int anchor = s ? anchor1 : 0;
-        if (idx[anchor] < 4) continue;
+        int ia = idx[0];
+        #pragma unroll
+        for (int i = 1; i < 16; i++) if (i == anchor) ia = idx[i];
+        if (ia < 4) continue;
+        #pragma unroll
         for (int c = 0; c < 3; c++) { int v = q[2 * s][c]; q[2 * s][c] = q[2 * s + 1][c]; q[2 * s + 1][c] = v; }
+        #pragma unroll
         for (int i = 0; i < 16; i++) if ((int)((mask >> i) & 1u) == s) idx[i] = 7 - idx[i];
     }
     Bits128 o;
     o.put(1u << 1, 2);
     o.put((uint32_t)part, 6);
-    for (int c = 0; c < 3; c++) for (int k = 0; k < 4; k++) o.put((uint32_t)q[k][c], 6);
+    #pragma unroll
+    for (int c = 0; c < 3; c++)
+        #pragma unroll
+        for (int k = 0; k < 4; k++) o.put((uint32_t)q[k][c], 6);
     o.put((uint32_t)pb[0], 1); o.put((uint32_t)pb[1], 1);
+    #pragma unroll
     for (int i = 0; i < 16; i++) o.put((uint32_t)idx[i], (i == 0 || i == anchor1) ? 2 : 3);
     out = make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
     return err;
@@ -388,10 +479,91 @@ ZTC_DEV uint32_t swap_alpha(uint32_t v, int rot) {
     return (v & ~((0xFFu << sh) | 0xFF000000u)) | (a << sh) | (c << 24);
 }
 
-// 3 resident CTAs per SM: the unrolled Adam state fits in 168 registers (72 bytes spilled); without a bound the
-// kernel takes 217 registers and 2 CTAs per SM, with 4 it spills 260 bytes
-__global__ void __launch_bounds__(128, 3) refine_kernel(int fmt, SrcU8 src, int bw, int nblocks, uint8_t *__restrict__ blocks, int steps,
-                                                     float lr, uint32_t *__restrict__ sse0, uint32_t *__restrict__ sse1) {
+// `steps` Adam steps on the block's MSE through the adjoint, in stored channel order (the rotation only permutes
+// channels, so the squared error is the same). NS subsets move: 1 (BC1, BC7 modes 6 and 5: endpoints 0 and 1) or
+// 2 (mode 1: a texel of subset 1 moves endpoints 2 and 3); mode 1's alpha is fixed at 255 and not a parameter.
+// Through the linear decode the gradient is affine in the endpoints. With a a texel's weight, b = 1 - a and t its
+// value, per subset s and channel c
+//   dL/dE[2s][c]   = n (Saa E[2s][c] + Sab E[2s+1][c] - Sat[c])
+//   dL/dE[2s+1][c] = n (Sab E[2s][c] + Sbb E[2s+1][c] - Sbt[c]),   n = 2 / (16 nc)
+// summed over the subset's texels (constant texels left out; alpha with its own weights), so the moments are summed
+// once and a step costs a few operations per endpoint channel. Adam keeps its usual form, with eps^2 added under
+// the root of the second moment rather than eps after it.
+template <int NS>
+ZTC_DEV void adam_refine(const LinBlock &L, const uint32_t ts[16], float e[6][4], int steps, float lr) {
+    const int npar = L.alpha_fixed ? 3 : L.nc;
+    float W[NS][2][3], T[NS][2][4];  // W[s][colour, alpha][aa, ab, bb]; T[s][a, b][c]
+    #pragma unroll
+    for (int s = 0; s < NS; s++)
+        #pragma unroll
+        for (int k = 0; k < 2; k++) {
+            #pragma unroll
+            for (int j = 0; j < 3; j++) W[s][k][j] = 0.0f;
+            #pragma unroll
+            for (int c = 0; c < 4; c++) T[s][k][c] = 0.0f;
+        }
+    #pragma unroll
+    for (int i = 0; i < 16; i++) {
+        if ((L.black >> i) & 1u) continue;  // a constant: no gradient
+        const bool in1 = NS == 2 && ((L.s1 >> i) & 1u);
+        float w[2][3], tv[2][4];
+        #pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const float a = k ? L.aa[i] : L.a[i], b = 1.0f - a;
+            w[k][0] = a * a; w[k][1] = a * b; w[k][2] = b * b;
+        }
+        #pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const float a = c == 3 ? L.aa[i] : L.a[i], t = (float)chan(ts[i], c);
+            tv[0][c] = a * t; tv[1][c] = (1.0f - a) * t;
+        }
+        #pragma unroll
+        for (int s = 0; s < NS; s++) {
+            if ((s == 1) != in1) continue;
+            #pragma unroll
+            for (int k = 0; k < 2; k++) {
+                #pragma unroll
+                for (int j = 0; j < 3; j++) W[s][k][j] += w[k][j];
+                #pragma unroll
+                for (int c = 0; c < 4; c++) T[s][k][c] += tv[k][c];
+            }
+        }
+    }
+    float m[NS][2][4], v[NS][2][4];
+    #pragma unroll
+    for (int s = 0; s < NS; s++)
+        #pragma unroll
+        for (int k = 0; k < 2; k++)
+            #pragma unroll
+            for (int c = 0; c < 4; c++) m[s][k][c] = v[s][k][c] = 0.0f;
+    const float b1 = 0.9f, b2 = 0.999f, n = 2.0f / (16.0f * (float)L.nc);
+    float p1 = 1.0f, p2 = 1.0f;
+    #pragma unroll 1
+    for (int st = 0; st < steps; st++) {
+        p1 *= b1; p2 *= b2;
+        const float c1 = lr / (1.0f - p1), c2 = 1.0f / (1.0f - p2);  // bias corrections
+        #pragma unroll
+        for (int s = 0; s < NS; s++)
+            #pragma unroll
+            for (int c = 0; c < 4; c++) {
+                if (c >= npar) continue;
+                const float *Wk = W[s][c == 3 ? 1 : 0];
+                const float e0 = e[2 * s][c], e1 = e[2 * s + 1][c];
+                const float g[2] = {n * (Wk[0] * e0 + Wk[1] * e1 - T[s][0][c]), n * (Wk[1] * e0 + Wk[2] * e1 - T[s][1][c])};
+                #pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    m[s][k][c] = b1 * m[s][k][c] + (1.0f - b1) * g[k];
+                    v[s][k][c] = b2 * v[s][k][c] + (1.0f - b2) * g[k] * g[k];
+                    const float upd = c1 * m[s][k][c] * rsqrtf(v[s][k][c] * c2 + 1e-16f);
+                    e[2 * s + k][c] = fminf(255.0f, fmaxf(0.0f, e[2 * s + k][c] - upd));
+                }
+            }
+    }
+}
+
+// 4 resident CTAs of 128 threads per SM
+__global__ void __launch_bounds__(128, 4) refine_kernel(int fmt, SrcU8 src, int bw, int nblocks, uint8_t *__restrict__ blocks, int steps,
+                                                        float lr, uint32_t *__restrict__ sse0, uint32_t *__restrict__ sse1) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nblocks) return;
     const size_t bs = fmt == ZTC_FMT_BC1 ? 8 : 16;
@@ -411,58 +583,11 @@ __global__ void __launch_bounds__(128, 3) refine_kernel(int fmt, SrcU8 src, int 
     int after = before;
     const bool refinable = fmt == ZTC_FMT_BC1 || L.mode == 6 || L.mode == 5 || L.mode == 1;
     if (refinable && before > 0) {
-        // Adam in stored channel order (the rotation only permutes channels, so the squared error is the same);
-        // mode 1's alpha is fixed at 255 and not a parameter; a texel of subset 1 moves endpoints 2 and 3. Every
-        // loop over texels, endpoints and channels is unrolled so the block's state stays in registers.
         uint32_t ts[16];
         #pragma unroll
         for (int i = 0; i < 16; i++) ts[i] = swap_alpha(t[i], L.rot);
-        const int npar = L.alpha_fixed ? 3 : L.nc, nk = L.s1 ? 4 : 2;
-        float P[4][4], m[4][4], v[4][4];
-        #pragma unroll
-        for (int k = 0; k < 4; k++)
-            #pragma unroll
-            for (int c = 0; c < 4; c++) { P[k][c] = e[k][c]; m[k][c] = v[k][c] = 0.0f; }
-        const float b1 = 0.9f, b2 = 0.999f, inv_n = 2.0f / (16.0f * (float)L.nc);
-        float p1 = 1.0f, p2 = 1.0f;
-        #pragma unroll 1
-        for (int s = 0; s < steps; s++) {
-            float g[4][4];
-            #pragma unroll
-            for (int k = 0; k < 4; k++)
-                #pragma unroll
-                for (int c = 0; c < 4; c++) g[k][c] = 0.0f;
-            #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                if ((L.black >> i) & 1u) continue;  // a constant: no gradient
-                const bool in1 = (L.s1 >> i) & 1u;
-                #pragma unroll
-                for (int c = 0; c < 4; c++) {  // forward decode, residual, adjoint
-                    if (c >= npar) continue;
-                    const float a = c == 3 ? L.aa[i] : L.a[i];
-                    const float e0 = in1 ? P[2][c] : P[0][c], e1 = in1 ? P[3][c] : P[1][c];
-                    const float r = (a * e0 + (1.0f - a) * e1 - (float)chan(ts[i], c)) * inv_n;
-                    const float g0 = a * r, g1 = (1.0f - a) * r;
-                    if (in1) { g[2][c] += g0; g[3][c] += g1; }
-                    else { g[0][c] += g0; g[1][c] += g1; }
-                }
-            }
-            p1 *= b1; p2 *= b2;
-            #pragma unroll
-            for (int k = 0; k < 4; k++)
-                #pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    if (k >= nk || c >= npar) continue;
-                    m[k][c] = b1 * m[k][c] + (1.0f - b1) * g[k][c];
-                    v[k][c] = b2 * v[k][c] + (1.0f - b2) * g[k][c] * g[k][c];
-                    float mh = m[k][c] / (1.0f - p1), vh = v[k][c] / (1.0f - p2);
-                    P[k][c] = fminf(255.0f, fmaxf(0.0f, P[k][c] - lr * mh / (sqrtf(vh) + 1e-8f)));
-                }
-        }
-        #pragma unroll
-        for (int k = 0; k < 4; k++)
-            #pragma unroll
-            for (int c = 0; c < 4; c++) e[k][c] = P[k][c];
+        if (L.s1) adam_refine<2>(L, ts, e, steps, lr);
+        else adam_refine<1>(L, ts, e, steps, lr);
         int ne = 1 << 30;
         if (fmt == ZTC_FMT_BC1) {
             uint2 nb;
