@@ -807,15 +807,16 @@ def extra_workloads(args, dev, sm_mhz=None, sms=148):
             outs[k % ring] = f(texs[k % ring], outs[k % ring])
         for k in range(ring):  # allocates every output before the timed region
             step(k)
-        # the median of five timed segments: one host-side stall (tens of ms) inside a single short window would
-        # otherwise dominate these few-millisecond figures
-        seg = max(4, steps // 5)
+        # the median of five timed segments, each after 3 untimed encodes: one host-side stall (tens of ms) inside a
+        # single short window would otherwise dominate these few-millisecond figures, and a segment that starts on an
+        # idle GPU carries its ramp-up (4-encode segments without warm-up read ASTC 20 % slow)
+        seg = max(20, steps // 5)
         with ClockSampler(torch.cuda.current_device()) as clk:
-            per = sorted(time_device(step, seg, 0, 1) / seg for _ in range(5))
+            per = sorted(time_device(step, seg, 3, 1) / seg for _ in range(5))
         ms = per[2] * steps
         mps = steps * npix / 1e6 / (ms / 1e3)
         res[name] = {"Mpix_s": mps, "ms_per_encode": ms / steps, "GB_s_algorithmic": mps * 1e6 * alg_bytes_per_px / 1e9,
-                     "timing": "median of 5 segments of %d encodes (CUDA events)" % seg,
+                     "timing": "median of 5 segments of %d encodes after 3 untimed ones (CUDA events)" % seg,
                      "segments_ms_per_encode": per, "clocks": clk.summary()}
         if counted:  # the whole encode against the ALU roofline, once the peak is measured (main's fill_alu)
             res[name]["_alu_in"] = (counted, ms / steps)

@@ -67,17 +67,19 @@ ZTC_DEV bool is_mode6(uint64_t lo) { return (lo & 0x7Fu) == 0x40u; }
 // mode-6 fields: q[e][c] 7 bits each (c-major), p-bits, 4-bit indices (texel 0: 3 bits) packed into idx, 4 bits each
 __device__ __forceinline__ uint64_t key_of(float cost, int order) { return ((uint64_t)__float_as_uint(cost) << 32) | (uint32_t)order; }
 
+
 // ---------------------------------------------------------------- BC7: one lane per texel
 // A BC7 candidate costs a whole palette search or least-squares solve, so this chain spreads each candidate over a
 // 16-lane group: lane i takes texel i (and window slot i when the rate is counted). 25 warps = 50 groups:
 // groups 0-15 kind 1 (neighbour j = group + 1: its endpoints, refit indices), 16-31 kind 2 (its indices, refit
-// endpoints), 32-47 kind 0 (the whole neighbour), 48 the base, 49 loads the next block. Every chosen block enters
+// endpoints), 32-47 kind 0 (the whole neighbour), 48 the base; a 26th warp loads the blocks ahead, software-pipelined
+// like the BC1 / BC4 chains' loader (its own warp, so its global loads hold no candidate's minimum). Every chosen block enters
 // the window with its decoded texels and, for mode 6, its palette and indices, so no candidate decodes a block:
 // kind 0 compares the texels with the stored decode, kind 1 searches the stored palette. The base encodings are
 // decoded for every block by a parallel pass before the chains. Kind 2's least-squares sums are exact in the
 // reference's float accumulation (weights k/64, texels integers: every partial sum is a multiple of 1/4096 below
 // 2^17 of them), so they are reduced as integers and scaled, which gives the same floats in any order.
-constexpr int kB7Warps = 25, kB7Threads = kB7Warps * 32;
+constexpr int kB7Warps = 25, kB7Threads = (kB7Warps + 1) * 32;  // candidate warps, then the loader warp
 
 // Group collectives over a 16-lane group: gm names the caller's half-warp (each half of a warp passes its own
 // mask, as 16-thread tiles do). ZTC_RDO_REDUX selects redux.sync (1) or xor-shuffle trees (0) for the sums and ORs;
@@ -135,12 +137,8 @@ __device__ __forceinline__ uint64_t warp_min_redux(uint64_t k) {
     return k;
 #endif
 }
-ZTC_DEV int sq4px(uint32_t a, uint32_t b) {  // squared RGBA difference (zap__sq4 over 4 channels)
-    int s = 0;
-    #pragma unroll
-    for (int c = 0; c < 4; c++) { const int d = (int)chan(a, c) - (int)chan(b, c); s += d * d; }
-    return s;
-}
+// squared RGBA difference (zap__sq4 over 4 channels) as |a|^2 + |b|^2 - 2 a.b, three dp4a; aa = |a|^2
+ZTC_DEV int sq4px(uint32_t a, int aa, uint32_t b) { return aa + (int)dot4(b, b) - 2 * (int)dot4(a, b); }
 ZTC_DEV uint32_t lerp_px(const int x0[4], const int x1[4], int w) {
     return pack_rgba(lerp64(x0[0], x1[0], w), lerp64(x0[1], x1[1], w), lerp64(x0[2], x1[2], w), lerp64(x0[3], x1[3], w));
 }
@@ -169,78 +167,113 @@ __global__ void __launch_bounds__(128) bc7_decode_bases_kernel(const uint8_t *__
     for (int k = 0; k < 4; k++) dec[(size_t)b * 4 + k] = make_uint4(px[4 * k], px[4 * k + 1], px[4 * k + 2], px[4 * k + 3]);
 }
 
-// the loader group's work for block gk: its texels, decoded base, base and channel sums into slot ns
-__device__ __forceinline__ void load_bc7_block(const SrcU8 &src, int bw, const uint8_t *out, const uint32_t *dec_base, int gk, int ns, int i,
-                                               unsigned gm, uint32_t (*s_tex)[16], uint32_t (*s_dbase)[16], uint64_t (*s_base)[2],
-                                               int (*s_sumx)[4]) {
-    const uint32_t t = load_texel(src, min((gk % bw) * 4 + (i & 3), src.w - 1), min((gk / bw) * 4 + (i >> 2), src.h - 1));
-    s_tex[ns][i] = t;
-    s_dbase[ns][i] = dec_base[(size_t)gk * 16 + i];
-    if (i < 2) s_base[ns][i] = *(const uint64_t *)(out + (size_t)gk * 16 + 8 * i);
-    #pragma unroll
-    for (int c = 0; c < 4; c++) {
-        const int sx = grp_sum((int)chan(t, c), gm);
-        if (i == c) s_sumx[ns][c] = sx;
+// The loader warp's registers for one block: lane i < 16 its texel i and decoded base texel i, every lane the base.
+struct Bc7Fetch {
+    uint32_t tex = 0, dec = 0;
+    uint64_t lo = 0, hi = 0;
+    __device__ __forceinline__ void fetch(const SrcU8 &src, int bw, const uint8_t *out, const uint32_t *dec_base, int gk, int lane) {
+        if (lane < 16) {
+            tex = load_texel(src, min((gk % bw) * 4 + (lane & 3), src.w - 1), min((gk / bw) * 4 + (lane >> 2), src.h - 1));
+            dec = dec_base[(size_t)gk * 16 + lane];
+        }
+        lo = *(const uint64_t *)(out + (size_t)gk * 16);
+        hi = *(const uint64_t *)(out + (size_t)gk * 16 + 8);
     }
-}
+    // into slot ns: texels, decoded base, base, the base's mode-6 palette, and the texels by channel (byte i of
+    // texc[c] is channel c of texel i, for the least-squares sums as dp4a)
+    __device__ __forceinline__ void store(int lane, int ns, uint32_t (*s_tex)[16], uint32_t (*s_dbase)[16], uint64_t (*s_base)[2],
+                                          uint32_t (*s_bpal)[16], uint32_t (*s_texc)[4][4]) const {
+        if (lane < 16) {
+            s_tex[ns][lane] = tex;
+            s_dbase[ns][lane] = dec;
+            int x0[4], x1[4];
+            mode6_ends_of(lo, hi, x0, x1);
+            s_bpal[ns][lane] = lerp_px(x0, x1, w4(lane));
+            #pragma unroll
+            for (int c = 0; c < 4; c++) ((uint8_t *)s_texc[ns][c])[lane] = (uint8_t)chan(tex, c);
+        }
+        if (lane < 2) s_base[ns][lane] = lane ? hi : lo;
+    }
+};
 
 __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src, int bw, int nby, int chain_rows, uint8_t *__restrict__ out,
                                                                       const uint32_t *__restrict__ dec_base, float lambda) {
     __shared__ uint64_t ring[kWindow][2];       // the last 16 chosen blocks, slot = block & 15
     __shared__ uint32_t ring_dec[kWindow][16];  // their decoded texels
-    __shared__ uint32_t ring_pal[kWindow][16];  // mode 6: their palettes
+    __shared__ __align__(16) uint32_t ring_pal[kWindow][16];  // mode 6: their palettes
+    __shared__ __align__(16) int ring_pp[kWindow][16];        // and the entries' squared norms |p|^2
     __shared__ uint64_t ring_idx[kWindow];      // mode 6: their indices, 4 bits per texel
+    __shared__ __align__(16) uint32_t ring_wp[kWindow][4];  // mode 6: their index weights w4(idx), a byte per texel
     __shared__ uint32_t s_tex[3][16], s_dbase[3][16];  // block cur in slot cur % 3, loaded two blocks ahead
     __shared__ uint64_t s_base[3][2];
-    __shared__ int s_sumx[3][4];                       // the block's channel sums
+    __shared__ uint32_t s_bpal[3][16];                 // the base's palette, if mode 6
+    __shared__ __align__(16) uint32_t s_texc[3][4][4];  // the block's texels by channel, a byte per texel
     __shared__ uint64_t s_key[kB7Warps];
     __shared__ int s_dist[2];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, i = lane & 15, grp = tid >> 4;
-    const int kind = grp < 16 ? 1 : grp < 32 ? 2 : grp < 48 ? 0 : grp == 48 ? -1 : -2, j = (grp & 15) + 1;
+    const bool loader = warp == kB7Warps;
+    const int kind = loader ? -2 : grp < 16 ? 1 : grp < 32 ? 2 : grp < 48 ? 0 : grp == 48 ? -1 : -3, j = (grp & 15) + 1;
     const unsigned gm = group_mask(warp, lane);
     const int row0 = blockIdx.x * chain_rows, rows = min(chain_rows, nby - row0);
     if (rows <= 0) return;
     const int first = row0 * bw, count = rows * bw;
-    if (kind == -2)
-        for (int k = 0; k < 2 && k < count; k++) load_bc7_block(src, bw, out, dec_base, first + k, k, i, gm, s_tex, s_dbase, s_base, s_sumx);
+    Bc7Fetch fb;
+    if (loader) {
+        for (int k = 0; k < 2 && k < count; k++) {
+            fb.fetch(src, bw, out, dec_base, first + k, lane);
+            fb.store(lane, k, s_tex, s_dbase, s_base, s_bpal, s_texc);
+        }
+        if (count > 2) fb.fetch(src, bw, out, dec_base, first + 2, lane);
+    }
     if (tid == 0) { s_dist[0] = 1; s_dist[1] = 1; }
     __syncthreads();
     for (int cur = 0; cur < count; cur++) {
         const int g = first + cur, slot = cur % 3, d0 = s_dist[0], d1 = s_dist[1];
         uint64_t key = ~0ull, clo = 0, chi = 0, cidx = 0;
-        uint32_t dec = 0, pal = 0;
-        int nd0 = 0, nd1 = 0;
+        uint32_t dec = 0;
+        int nd0 = 0, nd1 = 0, x0[4], x1[4];  // x0, x1: kind 2's refit endpoints, expanded
+        const int r = (cur - j) & (kWindow - 1);
         if (kind >= -1) {
             const uint32_t t = s_tex[slot][i];
-            const int r = (cur - j) & (kWindow - 1);
+            const int tt = (int)dot4(t, t);
             bool ok;
             int e;
             if (kind == -1) {  // the base (its SSE: the one the reference's encoder returns)
                 clo = s_base[slot][0]; chi = s_base[slot][1];
                 dec = s_dbase[slot][i];
-                e = grp_sum(sq4px(t, dec), gm);
-                int x0[4], x1[4];
-                mode6_ends_of(clo, chi, x0, x1);
-                pal = lerp_px(x0, x1, w4(i));
+                e = grp_sum(sq4px(t, tt, dec), gm);
                 cidx = mode6_idx_of(chi);
                 ok = true;
             } else if (kind == 0) {  // the whole neighbour (zap__bc7_err)
                 clo = ring[r][0]; chi = ring[r][1];
-                dec = ring_dec[r][i]; pal = ring_pal[r][i]; cidx = ring_idx[r];
-                e = grp_sum(sq4px(t, dec), gm);
+                dec = ring_dec[r][i]; cidx = ring_idx[r];
+                e = grp_sum(sq4px(t, tt, dec), gm);
                 ok = j <= cur;
             } else if (kind == 1) {  // its endpoints, best indices; texel 0 keeps to 0..7 (zap__bc7_fit6_idx)
                 const uint64_t nlo = ring[r][0], nhi = ring[r][1];
                 ok = j <= cur && is_mode6(nlo);
-                pal = ring_pal[r][i];
-                int m = 0x7FFFFFFF;
+                // key 16 (|p|^2 - 2 t.p) + k per entry (its minimum is the first nearest entry), minimised as a tree
+                int kk[16];
                 #pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    const uint32_t pk = ring_pal[r][k];
-                    const int kk = 16 * ((int)dot4(pk, pk) - 2 * (int)dot4(t, pk)) + k;
-                    if ((i || k < 8) && kk < m) { m = kk; dec = pk; }
+                for (int k4 = 0; k4 < 4; k4++) {
+                    const uint4 pk = *(const uint4 *)&ring_pal[r][4 * k4];
+                    const int4 pp = *(const int4 *)&ring_pp[r][4 * k4];
+                    kk[4 * k4 + 0] = 16 * (pp.x - 2 * (int)dot4(t, pk.x)) + 4 * k4 + 0;
+                    kk[4 * k4 + 1] = 16 * (pp.y - 2 * (int)dot4(t, pk.y)) + 4 * k4 + 1;
+                    kk[4 * k4 + 2] = 16 * (pp.z - 2 * (int)dot4(t, pk.z)) + 4 * k4 + 2;
+                    kk[4 * k4 + 3] = 16 * (pp.w - 2 * (int)dot4(t, pk.w)) + 4 * k4 + 3;
                 }
-                e = grp_sum((m >> 4) + (int)dot4(t, t), gm);
+                if (i == 0) {  // the anchor texel's index has 3 bits
+                    #pragma unroll
+                    for (int k = 8; k < 16; k++) kk[k] = 0x7FFFFFFF;
+                }
+                #pragma unroll
+                for (int h = 8; h >= 1; h >>= 1)
+                    #pragma unroll
+                    for (int k = 0; k < h; k++) kk[k] = min(kk[k], kk[k + h]);
+                const int m = kk[0];
+                dec = ring_pal[r][m & 15];
+                e = grp_sum((m >> 4) + tt, gm);
                 cidx = grp_or64((uint64_t)(m & 15) << (4 * i), gm);
                 clo = nlo; chi = mode6_hi((int)(nhi & 1u), cidx);
             } else {  // its indices, least-squares endpoints, each endpoint's own p-bit (zap__bc7_fit6_ep)
@@ -248,49 +281,53 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src,
                 ok = j <= cur && is_mode6(nlo);
                 cidx = ring_idx[r];
                 const int w = w4((int)((cidx >> (4 * i)) & 15u));
-                const int ch = i & 3, ep = (i >> 2) & 1, p = i >> 3;
-                // with u = 64 - w: sum u^2 = 16 * 4096 - 128 sum w + sum w^2, sum u w = 64 sum w - sum w^2,
-                // sum u x = 64 sum x - sum w x; sum w (<= 1024) and sum w^2 (<= 65536) share one word
-                const int W12 = grp_sum((w * w) << 11 | w, gm), W1 = W12 & 0x7FF, W2 = W12 >> 11;
-                int SB = 0;
-                #pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    const int sb = grp_sum(w * (int)chan(t, c), gm);
-                    if (c == ch) SB = sb;
-                }
-                const int AA = 16 * 4096 - 128 * W1 + W2, AB = 64 * W1 - W2, BB = W2, SA = 64 * s_sumx[slot][ch] - SB;
+                const int ch = i >> 2, ep = i & 1;  // this lane's (channel, endpoint); lanes 2 apart repeat it
+                // the neighbour's weights and this block's channel ch, a byte per texel: sum w, sum w^2 and sum w x
+                // are four dp4a each; with u = 64 - w: sum u^2 = 16 * 4096 - 128 sum w + sum w^2,
+                // sum u w = 64 sum w - sum w^2, sum u x = 64 sum x - sum w x
+                const uint4 wp = *(const uint4 *)ring_wp[r], xc = *(const uint4 *)s_texc[slot][ch];
+                const int W1 = (int)__dp4a(wp.w, 0x01010101u, __dp4a(wp.z, 0x01010101u, __dp4a(wp.y, 0x01010101u, dot4(wp.x, 0x01010101u))));
+                const int W2 = (int)__dp4a(wp.w, wp.w, __dp4a(wp.z, wp.z, __dp4a(wp.y, wp.y, dot4(wp.x, wp.x))));
+                const int SB = (int)__dp4a(wp.w, xc.w, __dp4a(wp.z, xc.z, __dp4a(wp.y, xc.y, dot4(wp.x, xc.x))));
+                const int SX = (int)__dp4a(xc.w, 0x01010101u, __dp4a(xc.z, 0x01010101u, __dp4a(xc.y, 0x01010101u, dot4(xc.x, 0x01010101u))));
+                const int AA = 16 * 4096 - 128 * W1 + W2, AB = 64 * W1 - W2, BB = W2, SA = 64 * SX - SB;
                 const float aa = (float)AA / 4096.0f, ab = (float)AB / 4096.0f, bb = (float)BB / 4096.0f;
                 const float ax = (float)SA / 64.0f, bx = (float)SB / 64.0f, det = aa * bb - ab * ab;
                 float v;
                 if (det < 1e-6f && det > -1e-6f) v = (ax + bx) / 16.0f;  // one index everywhere: flat
                 else v = ep ? (bx * aa - ax * ab) / det : (ax * bb - bx * ab) / det;
                 v = clamp255(v);
-                // lane (channel, endpoint, p-bit): zap__bc7q for one channel, 7 bits + p
-                const int gq = f2i_x86((v / 255.0f * 255.0f - (float)p) / 2.0f + 0.5f);
-                int bq = 0, be = 1 << 30;
+                // zap__bc7q for this (channel, endpoint), 7 bits + p, for both p-bits
+                const float vv = div255(v) * 255.0f;  // v / 255 correctly rounded, without a division sequence
+                int bq[2], be[2];
                 #pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    const int tq = clampi(around(gq, k), 0, 127);
-                    const float d = (float)((tq << 1) | p) - v;
-                    const int ek = f2i_x86(d * d);
-                    if (ek < be) { be = ek; bq = tq; }
+                for (int p = 0; p < 2; p++) {
+                    const int gq = f2i_x86((vv - (float)p) / 2.0f + 0.5f);
+                    bq[p] = 0; be[p] = 1 << 30;
+                    #pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        const int tq = clampi(around(gq, k), 0, 127);
+                        const float d = (float)((tq << 1) | p) - v;
+                        const int ek = f2i_x86(d * d);
+                        if (ek < be[p]) { be[p] = ek; bq[p] = tq; }
+                    }
                 }
-                int s4 = be + __shfl_xor_sync(gm, be, 1, 16);
-                s4 += __shfl_xor_sync(gm, s4, 2, 16);
-                const int e00 = __shfl_sync(gm, s4, 0, 16), e01 = __shfl_sync(gm, s4, 8, 16);
-                const int e10 = __shfl_sync(gm, s4, 4, 16), e11 = __shfl_sync(gm, s4, 12, 16);
-                const int pb0 = e01 < e00 ? 1 : 0, pb1 = e11 < e10 ? 1 : 0;
-                int x0[4], x1[4];
+                // each endpoint's errors over the four channels, both p-bits in one word (each below 2^16: a
+                // candidate lies within 2 of v); the endpoint keeps the p-bit of the smaller sum, p = 0 on ties
+                int s2 = be[0] | (be[1] << 16);
+                s2 += __shfl_xor_sync(gm, s2, 4, 16);
+                s2 += __shfl_xor_sync(gm, s2, 8, 16);
+                const int pbm = (s2 >> 16) < (s2 & 0xFFFF) ? 1 : 0, qm = pbm ? bq[1] : bq[0];
+                const int pb0 = __shfl_sync(gm, pbm, 0, 16), pb1 = __shfl_sync(gm, pbm, 1, 16);
                 uint64_t lo = 0x40u | ((uint64_t)pb0 << 63);
                 #pragma unroll
                 for (int c = 0; c < 4; c++) {
-                    const int q0 = __shfl_sync(gm, bq, pb0 * 8 + c, 16), q1 = __shfl_sync(gm, bq, pb1 * 8 + 4 + c, 16);
+                    const int q0 = __shfl_sync(gm, qm, 4 * c, 16), q1 = __shfl_sync(gm, qm, 4 * c + 1, 16);
                     x0[c] = (q0 << 1) | pb0; x1[c] = (q1 << 1) | pb1;
                     lo |= ((uint64_t)q0 << (7 + 14 * c)) | ((uint64_t)q1 << (14 + 14 * c));
                 }
                 dec = lerp_px(x0, x1, w);
-                e = grp_sum(sq4px(t, dec), gm);
-                pal = lerp_px(x0, x1, w4(i));
+                e = grp_sum(sq4px(t, tt, dec), gm);
                 clo = lo; chi = (nhi & ~1ull) | (uint64_t)pb1;
             }
             // rate (zap__bc7_rate): lane i compares the candidate's fields with window slot j' = i + 1
@@ -307,18 +344,29 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src,
             if (d1 > 0 && d1 <= cur && ((mB >> (d1 - 1)) & 1u)) fb = 0.0f;
             else if (mB) { nd1 = __ffs((int)mB); fb = 3.0f; }
             if (ok) key = key_of((float)e + lambda * (fa + fb + 1.0f), kind < 0 ? 0 : (j - 1) * 3 + kind + 1);
-        } else if (cur + 2 < count) {  // the loader: the block after next
-            load_bc7_block(src, bw, out, dec_base, g + 2, (cur + 2) % 3, i, gm, s_tex, s_dbase, s_base, s_sumx);
+        } else if (loader) {  // block cur + 2 (fetched the iteration before) to shared memory; fetch block cur + 3
+            if (cur + 2 < count) fb.store(lane, (cur + 2) % 3, s_tex, s_dbase, s_base, s_bpal, s_texc);
+            if (cur + 3 < count) fb.fetch(src, bw, out, dec_base, g + 3, lane);
         }
-        const uint64_t wk = warp_min_redux(key);
-        if (lane == 0) s_key[warp] = wk;
+        if (!loader) {
+            const uint64_t wk = warp_min_redux(key);
+            if (lane == 0) s_key[warp] = wk;
+        }
         __syncthreads();
-        const int order = (int)(uint32_t)warp_min_redux(lane < kB7Warps ? s_key[lane] : ~0ull);
+        const int order = loader ? -1 : (int)(uint32_t)warp_min_redux(lane < kB7Warps ? s_key[lane] : ~0ull);
         const int oc = order - 1, wkind = oc % 3, wgrp = order == 0 ? 48 : wkind == 1 ? oc / 3 : wkind == 2 ? 16 + oc / 3 : 32 + oc / 3;
-        if (grp == wgrp) {  // the winner enters the window
+        if (!loader && grp == wgrp) {  // the winner enters the window
             const int ws = cur & (kWindow - 1);
             ring_dec[ws][i] = dec;
+            // its mode-6 palette: the base's (built by the loader), the neighbour's (kinds 0 and 1 keep its endpoints;
+            // with j = 16 that slot is this one and each lane rewrites its own entry), or from the refit endpoints
+            uint32_t pal;
+            if (order == 0) pal = s_bpal[slot][i];
+            else if (kind != 2) pal = ring_pal[r][i];
+            else pal = lerp_px(x0, x1, w4(i));
             ring_pal[ws][i] = pal;
+            ring_pp[ws][i] = (int)dot4(pal, pal);
+            ((uint8_t *)ring_wp[ws])[i] = (uint8_t)w4((int)((cidx >> (4 * i)) & 15u));
             if (i == 0) {
                 ring[ws][0] = clo; ring[ws][1] = chi; ring_idx[ws] = cidx;
                 s_dist[0] = nd0; s_dist[1] = nd1;
@@ -329,47 +377,89 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src,
     }
 }
 
-// ---------------------------------------------------------------- BC1 / BC4 sub-blocks: one lane per texel
-// The BC7 chain's layout for one sub-block of a BC1-BC5 block: groups 0-15 kind 0 (neighbour j = group + 1: its
-// endpoints, fitted indices), 16-31 kind 1 (these endpoints, its indices), 32-47 kind 2 (the whole neighbour),
-// 48 the base, 49 loads the next block. The two sub-blocks of a BC3 or BC5 block are independent chains (each
-// looks only at its own fields of earlier blocks, with its own match distances, zap_tex.h:1494-1501), so each
-// runs in its own CTA (blockIdx.y) and writes its own 8 bytes of the blocks.
-ZTC_DEV void bc1_palette(uint32_t c0, uint32_t c1, int force4, uint32_t pal[4]) {  // entries as RGB texels
-    #pragma unroll
-    for (int k = 0; k < 4; k++) {
+// Word k of a sub-block's palette as the chain keeps it in shared memory: BC1 entries 0-3 as RGB texels (alpha
+// byte 0), then words 4-7 their squared norms |p|^2, so a texel's squared distance to entry k is
+// |t|^2 + |p_k|^2 - 2 t.p_k with t.p_k one dp4a; BC4 its 8 values. Each chosen sub-block enters the window with its
+// palette and the loader builds each block's base palette two blocks ahead, so no candidate builds one.
+ZTC_DEV int palette_word(const Sub &S, uint64_t v, int k) {
+    if (S.type == kBc1) {
         int r, g, b;
-        bc1_entry(c0, c1, force4, k, r, g, b);
-        pal[k] = pack_rgb(r, g, b);
+        bc1_entry((uint32_t)(v & 0xFFFFu), (uint32_t)((v >> 16) & 0xFFFFu), S.force4, k & 3, r, g, b);
+        const uint32_t p = pack_rgb(r, g, b);
+        return k < 4 ? (int)p : (int)dot4(p, p);
     }
-}
-ZTC_DEV int sq3px(uint32_t t, uint32_t p) {
-    int s = 0;
-    #pragma unroll
-    for (int c = 0; c < 3; c++) { const int d = (int)chan(t, c) - (int)chan(p, c); s += d * d; }
-    return s;
+    return bc4_entry((int)(v & 0xFFu), (int)((v >> 8) & 0xFFu), k);
 }
 
-__global__ void __launch_bounds__(kB7Threads, 1) rdo_sub_chain_kernel(SrcU8 src, int bw, int nby, int chain_rows, uint8_t *__restrict__ out,
-                                                                      int bs, Sub S0, Sub S1, float lambda) {
+// ---------------------------------------------------------------- BC1 / BC4 sub-blocks
+// One chain per CTA and sub-block kind. Per block the 49 candidates are groups of L lanes: groups 0-15 kind 0
+// (neighbour j = group + 1: its endpoints, fitted indices), 16-31 kind 1 (these endpoints, its indices), 32-47 kind 2
+// (the whole neighbour), 48 the base. Lane q of a group takes texels q*T .. q*T + T - 1 (T = 16 / L), and the window
+// slots at those distances minus one when the rate is counted. A last warp of its own loads the blocks ahead,
+// software-pipelined (block cur + 3 fetched into registers while block cur + 2, fetched the iteration before, is
+// stored to shared memory), so no candidate warp and no barrier waits for a global load: with the loader beside the
+// base in one warp, its loads held that warp's minimum and each block's first barrier (about 1,100 of 3,400 cycles
+// per block, measured with clock64 on B200).
+// L = 8 (13 warps) measured fastest on B200: 512x512 BC1 in one chain 24.3 ms, against 25.5 ms at L = 16 (25 warps)
+// and 27.7 ms at L = 4 (7 warps), though L = 4 issues about a quarter of L = 16's warp instructions: a block's time
+// is its critical path (loads, group reductions, rate masks, two CTA-wide minima and barriers), not the candidates'
+// arithmetic. The two sub-blocks of a BC3 or BC5 block are independent chains (each looks only at its own fields of
+// earlier blocks, with its own match distances, zap_tex.h:1494-1501), so each runs in its own CTA (blockIdx.y) and
+// writes its own 8 bytes of the blocks.
+template <int L> struct SubChain {  // kWc candidate warps, then the loader warp
+    static constexpr int T = 16 / L, kWc = (49 * L + 31) / 32, kThreads = (kWc + 1) * 32;
+};
+#ifndef ZTC_RDO_SUB_LANES
+#define ZTC_RDO_SUB_LANES 8
+#endif
+
+template <int L> __device__ __forceinline__ int lsum(int v, unsigned gm) {
+    #pragma unroll
+    for (int m = L / 2; m >= 1; m >>= 1) v += __shfl_xor_sync(gm, v, m, L);
+    return v;
+}
+template <int L> __device__ __forceinline__ uint32_t lor(uint32_t v, unsigned gm) {
+    #pragma unroll
+    for (int m = L / 2; m >= 1; m >>= 1) v |= __shfl_xor_sync(gm, v, m, L);
+    return v;
+}
+
+template <int L>
+__global__ void __launch_bounds__(SubChain<L>::kThreads, 1) rdo_sub_chain_kernel(SrcU8 src, int bw, int nby, int chain_rows, uint8_t *__restrict__ out,
+                                                                                int bs, Sub S0, Sub S1, float lambda) {
+    constexpr int T = SubChain<L>::T, kW = SubChain<L>::kWc;
     __shared__ uint64_t ring[kWindow];  // the sub-block of the last 16 chosen blocks, slot = block & 15
-    __shared__ uint32_t s_tex[3][16];  // block cur in slot cur % 3, loaded two blocks ahead
+    __shared__ __align__(16) int ring_pal[kWindow][8];  // their palettes (palette_word)
+    __shared__ __align__(16) uint32_t s_tex[3][16];  // block cur in slot cur % 3, loaded two blocks ahead
     __shared__ uint64_t s_base[3];
-    __shared__ uint64_t s_key[kB7Warps];
+    __shared__ __align__(16) int s_bpal[3][8];  // the base sub-block's palette
+    __shared__ uint64_t s_key[kW];
     __shared__ int s_dist[2];
     const Sub S = blockIdx.y ? S1 : S0;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, i = lane & 15, grp = tid >> 4;
-    const int kind = grp < 16 ? 0 : grp < 32 ? 1 : grp < 48 ? 2 : grp == 48 ? -1 : -2, j = (grp & 15) + 1;
-    const unsigned gm = group_mask(warp, lane);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, q = tid & (L - 1), grp = tid / L;
+    const bool loader = warp == kW;
+    const int kind = loader ? -2 : grp < 16 ? 0 : grp < 32 ? 1 : grp < 48 ? 2 : grp == 48 ? -1 : -3, j = (grp & 15) + 1;
+    // the warps of groups 0-47 hold one kind each and meet every collective together; the base's group has its own
+    const unsigned gm = warp < 48 * L / 32 ? 0xFFFFFFFFu : ((L == 32 ? 0xFFFFFFFFu : (1u << L) - 1u) << (lane & ~(L - 1)));
     const int row0 = blockIdx.x * chain_rows, rows = min(chain_rows, nby - row0);
     if (rows <= 0) return;
     const int first = row0 * bw, count = rows * bw;
-    if (kind == -2)
-        for (int k = 0; k < 2 && k < count; k++) {
-            const int gk = first + k;
-            s_tex[k][i] = load_texel(src, min((gk % bw) * 4 + (i & 3), src.w - 1), min((gk / bw) * 4 + (i >> 2), src.h - 1));
-            if (i == 0) s_base[k] = *(const uint64_t *)(out + (size_t)gk * bs + S.off);
-        }
+    // the loader warp: lane i < 16 fetches texel i of a block, every lane its base sub-block
+    uint32_t r_tex = 0;
+    uint64_t r_base = 0;
+    auto fetch = [&](int gk) {
+        if (lane < 16) r_tex = load_texel(src, min((gk % bw) * 4 + (lane & 3), src.w - 1), min((gk / bw) * 4 + (lane >> 2), src.h - 1));
+        r_base = *(const uint64_t *)(out + (size_t)gk * bs + S.off);
+    };
+    auto store = [&](int ns) {  // the fetched block into slot ns, with the base's palette
+        if (lane < 16) s_tex[ns][lane] = r_tex;
+        if (lane < 8) s_bpal[ns][lane] = palette_word(S, r_base, lane);
+        if (lane == 0) s_base[ns] = r_base;
+    };
+    if (loader) {
+        for (int k = 0; k < 2 && k < count; k++) { fetch(first + k); store(k); }
+        if (count > 2) fetch(first + 2);
+    }
     if (tid == 0) { s_dist[0] = 1; s_dist[1] = 1; }
     __syncthreads();
     // fields: BC1 {c0 c1, indices} = {4, 4} bytes, BC4 {a0 a1, indices} = {2, 6}
@@ -382,63 +472,94 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_sub_chain_kernel(SrcU8 src,
         uint64_t key = ~0ull, cand = 0;
         int nd0 = 0, nd1 = 0;
         if (kind >= -1) {
-            const uint32_t t = s_tex[slot][i];
+            uint32_t t[T];
+            #pragma unroll
+            for (int u = 0; u < T; u++) t[u] = s_tex[slot][q * T + u];
             const uint64_t base = s_base[slot], nb = ring[(cur - j) & (kWindow - 1)];
+            // kind 1 and the base: these endpoints (the base's palette); kinds 0 and 2: the neighbour's
+            const bool own = kind == 1 || kind == -1;
+            const int *P = own ? s_bpal[slot] : ring_pal[(cur - j) & (kWindow - 1)];
             bool ok = kind == -1 || j <= cur;
-            int e;
+            int e = 0;
             if (bc1) {  // the CTA's sub-block type: uniform
-                const uint32_t p0 = (uint32_t)(nb & 0xFFFFu), p1 = (uint32_t)((nb >> 16) & 0xFFFFu);
-                // kind 1 and the base: these endpoints; kinds 0 and 2: the neighbour's
-                const uint32_t a = kind == 1 || kind == -1 ? (uint32_t)(base & 0xFFFFu) : p0;
-                const uint32_t b = kind == 1 || kind == -1 ? (uint32_t)((base >> 16) & 0xFFFFu) : p1;
-                uint32_t pal[4];
-                bc1_palette(a, b, S.force4, pal);
+                const uint32_t a = (uint32_t)((own ? base : nb) & 0xFFFFu), b = (uint32_t)(((own ? base : nb) >> 16) & 0xFFFFu);
                 uint32_t idx;
                 if (kind == 0) {  // zap__bc1_fit: best of the 4 (3 in 3-colour order) entries, first on ties
-                    const int n = (S.force4 || a > b) ? 4 : 3;
-                    int bk = 0, be = sq3px(t, pal[0]);
+                    const int4 pe = *(const int4 *)P, pn = *(const int4 *)(P + 4);
+                    const bool n4 = S.force4 || a > b;
+                    idx = 0;
                     #pragma unroll
-                    for (int k = 1; k < 4; k++) {
-                        const int ek = sq3px(t, pal[k]);
-                        if (k < n && ek < be) { be = ek; bk = k; }
+                    for (int u = 0; u < T; u++) {
+                        const uint32_t tc = t[u] & 0xFFFFFFu;
+                        int bk = 0, be = pn.x - 2 * (int)dot4(tc, (uint32_t)pe.x), sk;
+                        sk = pn.y - 2 * (int)dot4(tc, (uint32_t)pe.y); if (sk < be) { be = sk; bk = 1; }
+                        sk = pn.z - 2 * (int)dot4(tc, (uint32_t)pe.z); if (sk < be) { be = sk; bk = 2; }
+                        sk = pn.w - 2 * (int)dot4(tc, (uint32_t)pe.w); if (n4 && sk < be) { be = sk; bk = 3; }
+                        e += be + (int)dot4(tc, tc);
+                        idx |= (uint32_t)bk << (2 * (q * T + u));
                     }
-                    e = grp_sum(be, gm);
-                    idx = (uint32_t)grp_or64((uint64_t)bk << (2 * i), gm);
+                    e = lsum<L>(e, gm);
+                    idx = lor<L>(idx, gm);
                 } else {  // zap__bc1_eval with the base's or the neighbour's indices
                     idx = (uint32_t)((kind == -1 ? base : nb) >> 32);
-                    const int k = (int)((idx >> (2 * i)) & 3u);
-                    e = grp_sum(sq3px(t, k == 0 ? pal[0] : k == 1 ? pal[1] : k == 2 ? pal[2] : pal[3]), gm);
+                    #pragma unroll
+                    for (int u = 0; u < T; u++) {
+                        const uint32_t tc = t[u] & 0xFFFFFFu;
+                        const int k = (int)((idx >> (2 * (q * T + u))) & 3u);
+                        e += P[4 + k] - 2 * (int)dot4(tc, (uint32_t)P[k]) + (int)dot4(tc, tc);
+                    }
+                    e = lsum<L>(e, gm);
                 }
                 cand = (uint64_t)a | ((uint64_t)b << 16) | ((uint64_t)idx << 32);
                 // a 3-colour block may not use index 3 (transparent); the base is never checked
                 if (kind >= 0 && !S.force4 && a <= b && (idx & (idx >> 1) & 0x55555555u)) ok = false;
             } else {
-                const int pa0 = (int)(nb & 0xFFu), pa1 = (int)((nb >> 8) & 0xFFu);
-                const int a = kind == 1 || kind == -1 ? (int)(base & 0xFFu) : pa0, b = kind == 1 || kind == -1 ? (int)((base >> 8) & 0xFFu) : pa1;
-                const int v = (int)chan(t, S.chan);
+                const int a = (int)((own ? base : nb) & 0xFFu), b = (int)(((own ? base : nb) >> 8) & 0xFFu);
                 uint64_t idx;
                 if (kind == 0) {  // zap__bc4_fit
-                    int bk = 0, be = (v - bc4_entry(a, b, 0)) * (v - bc4_entry(a, b, 0));
+                    const int4 p0 = *(const int4 *)P, p1 = *(const int4 *)(P + 4);
+                    const int pv[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+                    uint32_t part = 0;  // this lane's T 3-bit indices
                     #pragma unroll
-                    for (int k = 1; k < 8; k++) {
-                        const int d = v - bc4_entry(a, b, k);
-                        if (d * d < be) { be = d * d; bk = k; }
+                    for (int u = 0; u < T; u++) {
+                        const int v = (int)chan(t[u], S.chan);
+                        int bk = 0, be = (v - pv[0]) * (v - pv[0]);
+                        #pragma unroll
+                        for (int k = 1; k < 8; k++) {
+                            const int d = v - pv[k];
+                            if (d * d < be) { be = d * d; bk = k; }
+                        }
+                        e += be;
+                        part |= (uint32_t)bk << (3 * u);
                     }
-                    e = grp_sum(be, gm);
-                    idx = grp_or64((uint64_t)bk << (3 * i), gm);
+                    e = lsum<L>(e, gm);
+                    // lane q's indices start at bit 3 q T: two 32-bit words of the 48
+                    const uint64_t mine = (uint64_t)part << (3 * q * T);
+                    idx = ((uint64_t)lor<L>((uint32_t)(mine >> 32), gm) << 32) | lor<L>((uint32_t)mine, gm);
                 } else {  // zap__bc4_eval
                     idx = (kind == -1 ? base : nb) >> 16;
-                    const int d = v - bc4_entry(a, b, (int)((idx >> (3 * i)) & 7u));
-                    e = grp_sum(d * d, gm);
+                    #pragma unroll
+                    for (int u = 0; u < T; u++) {
+                        const int d = (int)chan(t[u], S.chan) - P[(int)((idx >> (3 * (q * T + u))) & 7u)];
+                        e += d * d;
+                    }
+                    e = lsum<L>(e, gm);
                 }
                 cand = (uint64_t)a | ((uint64_t)b << 8) | (idx << 16);
             }
-            // rate (zap__field_rate per field): lane i compares with window slot j' = i + 1
-            const uint64_t w = ring[(cur - i - 1) & (kWindow - 1)];
-            const bool vw = i + 1 <= cur;
-            const unsigned sh = lane & 16;
-            const unsigned mA = (__ballot_sync(gm, vw && (w & maskA) == (cand & maskA)) >> sh) & 0xFFFFu;
-            const unsigned mB = (__ballot_sync(gm, vw && (w >> (8 * nA)) == (cand >> (8 * nA))) >> sh) & 0xFFFFu;
+            // rate (zap__field_rate per field): bit d - 1 of a mask says the field equals the window's at distance d
+            uint32_t mA = 0, mB = 0;
+            #pragma unroll
+            for (int u = 0; u < T; u++) {
+                const int d = q * T + u + 1;
+                const uint64_t w = ring[(cur - d) & (kWindow - 1)];
+                if (d <= cur) {
+                    mA |= (uint32_t)((w & maskA) == (cand & maskA)) << (d - 1);
+                    mB |= (uint32_t)((w >> (8 * nA)) == (cand >> (8 * nA))) << (d - 1);
+                }
+            }
+            mA = lor<L>(mA, gm);
+            mB = lor<L>(mB, gm);
             float fa = (float)nA, fb = (float)nB;
             nd0 = d0; nd1 = d1;
             if (d0 > 0 && d0 <= cur && ((mA >> (d0 - 1)) & 1u)) fa = 0.0f;
@@ -446,20 +567,27 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_sub_chain_kernel(SrcU8 src,
             if (d1 > 0 && d1 <= cur && ((mB >> (d1 - 1)) & 1u)) fb = 0.0f;
             else if (mB) { nd1 = __ffs((int)mB); fb = newB; }
             if (ok) key = key_of((float)e + lambda * (fa + fb), kind < 0 ? 0 : (j - 1) * 3 + kind + 1);
-        } else if (cur + 2 < count) {  // the loader: texels and base sub-block of the block after next
-            const int gn = g + 2, ns = (cur + 2) % 3;
-            s_tex[ns][i] = load_texel(src, min((gn % bw) * 4 + (i & 3), src.w - 1), min((gn / bw) * 4 + (i >> 2), src.h - 1));
-            if (i == 0) s_base[ns] = *(const uint64_t *)(out + (size_t)gn * bs + S.off);
+        } else if (loader) {  // block cur + 2 (fetched the iteration before) to shared memory; fetch block cur + 3
+            if (cur + 2 < count) store((cur + 2) % 3);
+            if (cur + 3 < count) fetch(g + 3);
         }
-        const uint64_t wk = warp_min_redux(key);
-        if (lane == 0) s_key[warp] = wk;
+        if (!loader) {
+            const uint64_t wk = warp_min_redux(key);
+            if (lane == 0) s_key[warp] = wk;
+        }
         __syncthreads();
-        const int order = (int)(uint32_t)warp_min_redux(lane < kB7Warps ? s_key[lane] : ~0ull);
+        const int order = loader ? -1 : (int)(uint32_t)warp_min_redux(lane < kW ? s_key[lane] : ~0ull);
         const int oc = order - 1, wkind = oc % 3, wgrp = order == 0 ? 48 : wkind * 16 + oc / 3;
-        if (grp == wgrp && i == 0) {  // the winner enters the window
-            ring[cur & (kWindow - 1)] = cand;
-            s_dist[0] = nd0; s_dist[1] = nd1;
-            if (order != 0) *(uint64_t *)(out + (size_t)g * bs + S.off) = cand;
+        if (!loader && grp == wgrp) {  // the winner enters the window, with its palette (the base's, or the neighbour's)
+            // with j = 16 the neighbour's slot is this one: each lane rewrites its own words
+            const int *P = order == 0 || wkind == 1 ? s_bpal[slot] : ring_pal[(cur - j) & (kWindow - 1)];
+            #pragma unroll
+            for (int k = q; k < 8; k += L) ring_pal[cur & (kWindow - 1)][k] = P[k];
+            if (q == 0) {
+                ring[cur & (kWindow - 1)] = cand;
+                s_dist[0] = nd0; s_dist[1] = nd1;
+                if (order != 0) *(uint64_t *)(out + (size_t)g * bs + S.off) = cand;
+            }
         }
         __syncthreads();
     }
@@ -492,7 +620,8 @@ cudaError_t ztc_launch_rdo(int fmt, const ztc::SrcU8 &src, uint8_t *out, float l
         const int ns = ztc::sub_count(fmt), bs = fmt == ZTC_FMT_BC1 || fmt == ZTC_FMT_BC4 ? 8 : 16;
         const dim3 grid(chains, ns);
         if (fmt < ZTC_FMT_BC1 || fmt > ZTC_FMT_BC5) return cudaErrorInvalidValue;
-        ztc::rdo_sub_chain_kernel<<<grid, ztc::kB7Threads, 0, stream>>>(src, bw, nby, band_rows, out, bs, S0, S1, lambda);
+        constexpr int L = ZTC_RDO_SUB_LANES;
+        ztc::rdo_sub_chain_kernel<L><<<grid, ztc::SubChain<L>::kThreads, 0, stream>>>(src, bw, nby, band_rows, out, bs, S0, S1, lambda);
         return cudaGetLastError();
     }
 }
