@@ -68,58 +68,38 @@ ZTC_DEV bool is_mode6(uint64_t lo) { return (lo & 0x7Fu) == 0x40u; }
 __device__ __forceinline__ uint64_t key_of(float cost, int order) { return ((uint64_t)__float_as_uint(cost) << 32) | (uint32_t)order; }
 
 
-// ---------------------------------------------------------------- BC7: one lane per texel
+// ---------------------------------------------------------------- BC7
 // A BC7 candidate costs a whole palette search or least-squares solve, so this chain spreads each candidate over a
-// 16-lane group: lane i takes texel i (and window slot i when the rate is counted). 25 warps = 50 groups:
-// groups 0-15 kind 1 (neighbour j = group + 1: its endpoints, refit indices), 16-31 kind 2 (its indices, refit
-// endpoints), 32-47 kind 0 (the whole neighbour), 48 the base; a 26th warp loads the blocks ahead, software-pipelined
-// like the BC1 / BC4 chains' loader (its own warp, so its global loads hold no candidate's minimum). Every chosen block enters
-// the window with its decoded texels and, for mode 6, its palette and indices, so no candidate decodes a block:
-// kind 0 compares the texels with the stored decode, kind 1 searches the stored palette. The base encodings are
-// decoded for every block by a parallel pass before the chains. Kind 2's least-squares sums are exact in the
-// reference's float accumulation (weights k/64, texels integers: every partial sum is a multiple of 1/4096 below
-// 2^17 of them), so they are reduced as integers and scaled, which gives the same floats in any order.
-constexpr int kB7Warps = 25, kB7Threads = (kB7Warps + 1) * 32;  // candidate warps, then the loader warp
+// group of L lanes: lane q takes texels q*T .. q*T + T - 1 (T = 16 / L), and the window slots at those distances
+// minus one when the rate is counted. Groups 0-15 kind 1 (neighbour j = group + 1: its endpoints, refit indices),
+// 16-31 kind 2 (its indices, refit endpoints), 32-47 kind 0 (the whole neighbour), 48 the base; a last warp loads the
+// blocks ahead, software-pipelined like the BC1 / BC4 chains' loader (its own warp, so its global loads hold no
+// candidate's minimum). Every chosen block enters the window with its decoded texels and, for mode 6, its palette
+// (with the entries' squared norms), indices and index weights, so no candidate decodes a block: kind 0 compares the
+// texels with the stored decode, kind 1 searches the stored palette. The base encodings are decoded for every block
+// by a parallel pass before the chains. Kind 2's least-squares sums are exact in the reference's float accumulation
+// (weights k/64, texels integers: every partial sum is a multiple of 1/4096 below 2^17 of them), so they are integer
+// dot products (the weights and the texels' channels a byte per texel), scaled, which gives the same floats in any
+// order; its solve and quantisation are one (channel, endpoint) per lane, both p-bits.
 
-// Group collectives over a 16-lane group: gm names the caller's half-warp (each half of a warp passes its own
-// mask, as 16-thread tiles do). ZTC_RDO_REDUX selects redux.sync (1) or xor-shuffle trees (0) for the sums and ORs;
-// ZTC_RDO_MIN_REDUX the same for the warp-wide key minimum.
-#ifndef ZTC_RDO_REDUX
-#define ZTC_RDO_REDUX 0
-#endif
+// Collectives over a group of L lanes: gm names the lanes that meet the collective. Warps whose groups all run one
+// kind of candidate pass the whole warp (every group meets each collective at the same point); whole-warp masks
+// measured faster on B200 than each group passing its own (512x512 one chain: BC7 30.6 -> 28.3 ms, BC1 25.8 ->
+// 25.5 ms), and redux.sync for the group sums slower than shuffle trees (BC7 30.6 -> 47 ms). ZTC_RDO_MIN_REDUX
+// selects redux.sync (1) or an xor-shuffle tree (0) for the warp-wide key minimum.
 #ifndef ZTC_RDO_MIN_REDUX
 #define ZTC_RDO_MIN_REDUX 1
 #endif
-__device__ __forceinline__ int grp_sum(int v, unsigned gm) {
-#if ZTC_RDO_REDUX
-    return __reduce_add_sync(gm, v);
-#else
+// sums and ORs over a group of L lanes (gm: the lanes that meet the collective)
+template <int L> __device__ __forceinline__ int lsum(int v, unsigned gm) {
     #pragma unroll
-    for (int m = 8; m >= 1; m >>= 1) v += __shfl_xor_sync(gm, v, m, 16);
+    for (int m = L / 2; m >= 1; m >>= 1) v += __shfl_xor_sync(gm, v, m, L);
     return v;
-#endif
 }
-__device__ __forceinline__ uint64_t grp_or64(uint64_t v, unsigned gm) {
-#if ZTC_RDO_REDUX
-    return ((uint64_t)__reduce_or_sync(gm, (uint32_t)(v >> 32)) << 32) | __reduce_or_sync(gm, (uint32_t)v);
-#else
+template <int L> __device__ __forceinline__ uint32_t lor(uint32_t v, unsigned gm) {
     #pragma unroll
-    for (int m = 8; m >= 1; m >>= 1) {
-        const uint32_t lo = __shfl_xor_sync(gm, (uint32_t)v, m, 16), hi = __shfl_xor_sync(gm, (uint32_t)(v >> 32), m, 16);
-        v |= ((uint64_t)hi << 32) | lo;
-    }
+    for (int m = L / 2; m >= 1; m >>= 1) v |= __shfl_xor_sync(gm, v, m, L);
     return v;
-#endif
-}
-// The mask a lane passes to its group's collectives: its half-warp, or (ZTC_RDO_FULL_MASK) the whole warp in
-// warps 0-23, whose two groups run the same kind of candidate and meet every collective together; warp 24
-// splits into the base and the loader, which run different code. Whole-warp masks measured faster on B200
-// (512x512 one chain: BC7 30.6 -> 28.3 ms, BC1 25.8 -> 25.5 ms).
-#ifndef ZTC_RDO_FULL_MASK
-#define ZTC_RDO_FULL_MASK 1
-#endif
-__device__ __forceinline__ unsigned group_mask(int warp, int lane) {
-    return ZTC_RDO_FULL_MASK && warp < 24 ? 0xFFFFFFFFu : 0xFFFFu << (lane & 16);
 }
 // warp-wide minimum of 64-bit keys
 __device__ __forceinline__ uint64_t warp_min_redux(uint64_t k) {
@@ -196,8 +176,17 @@ struct Bc7Fetch {
     }
 };
 
-__global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src, int bw, int nby, int chain_rows, uint8_t *__restrict__ out,
-                                                                      const uint32_t *__restrict__ dec_base, float lambda) {
+template <int L> struct B7Chain {  // kWc candidate warps, then the loader warp
+    static constexpr int T = 16 / L, kWc = (49 * L + 31) / 32, kThreads = (kWc + 1) * 32;
+};
+#ifndef ZTC_RDO_BC7_LANES
+#define ZTC_RDO_BC7_LANES 8
+#endif
+
+template <int L>
+__global__ void __launch_bounds__(B7Chain<L>::kThreads, 1) rdo_bc7_chain_kernel(SrcU8 src, int bw, int nby, int chain_rows, uint8_t *__restrict__ out,
+                                                                                const uint32_t *__restrict__ dec_base, float lambda) {
+    constexpr int T = B7Chain<L>::T, kW = B7Chain<L>::kWc;
     __shared__ uint64_t ring[kWindow][2];       // the last 16 chosen blocks, slot = block & 15
     __shared__ uint32_t ring_dec[kWindow][16];  // their decoded texels
     __shared__ __align__(16) uint32_t ring_pal[kWindow][16];  // mode 6: their palettes
@@ -208,12 +197,13 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src,
     __shared__ uint64_t s_base[3][2];
     __shared__ uint32_t s_bpal[3][16];                 // the base's palette, if mode 6
     __shared__ __align__(16) uint32_t s_texc[3][4][4];  // the block's texels by channel, a byte per texel
-    __shared__ uint64_t s_key[kB7Warps];
+    __shared__ uint64_t s_key[kW];
     __shared__ int s_dist[2];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, i = lane & 15, grp = tid >> 4;
-    const bool loader = warp == kB7Warps;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, q = tid & (L - 1), grp = tid / L;
+    const bool loader = warp == kW;
     const int kind = loader ? -2 : grp < 16 ? 1 : grp < 32 ? 2 : grp < 48 ? 0 : grp == 48 ? -1 : -3, j = (grp & 15) + 1;
-    const unsigned gm = group_mask(warp, lane);
+    // the warps of groups 0-47 hold one kind each and meet every collective together; the base's group has its own
+    const unsigned gm = warp < 48 * L / 32 ? 0xFFFFFFFFu : (((1u << L) - 1u) << (lane & ~(L - 1)));
     const int row0 = blockIdx.x * chain_rows, rows = min(chain_rows, nby - row0);
     if (rows <= 0) return;
     const int first = row0 * bw, count = rows * bw;
@@ -230,58 +220,67 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src,
     for (int cur = 0; cur < count; cur++) {
         const int g = first + cur, slot = cur % 3, d0 = s_dist[0], d1 = s_dist[1];
         uint64_t key = ~0ull, clo = 0, chi = 0, cidx = 0;
-        uint32_t dec = 0;
+        uint32_t dec[T];  // the candidate's decode of this lane's texels
         int nd0 = 0, nd1 = 0, x0[4], x1[4];  // x0, x1: kind 2's refit endpoints, expanded
         const int r = (cur - j) & (kWindow - 1);
         if (kind >= -1) {
-            const uint32_t t = s_tex[slot][i];
-            const int tt = (int)dot4(t, t);
+            uint32_t t[T];
+            int tt[T];
+            #pragma unroll
+            for (int u = 0; u < T; u++) { t[u] = s_tex[slot][q * T + u]; tt[u] = (int)dot4(t[u], t[u]); }
             bool ok;
-            int e;
+            int e = 0;
             if (kind == -1) {  // the base (its SSE: the one the reference's encoder returns)
                 clo = s_base[slot][0]; chi = s_base[slot][1];
-                dec = s_dbase[slot][i];
-                e = grp_sum(sq4px(t, tt, dec), gm);
+                #pragma unroll
+                for (int u = 0; u < T; u++) { dec[u] = s_dbase[slot][q * T + u]; e += sq4px(t[u], tt[u], dec[u]); }
+                e = lsum<L>(e, gm);
                 cidx = mode6_idx_of(chi);
                 ok = true;
             } else if (kind == 0) {  // the whole neighbour (zap__bc7_err)
-                clo = ring[r][0]; chi = ring[r][1];
-                dec = ring_dec[r][i]; cidx = ring_idx[r];
-                e = grp_sum(sq4px(t, tt, dec), gm);
+                clo = ring[r][0]; chi = ring[r][1]; cidx = ring_idx[r];
+                #pragma unroll
+                for (int u = 0; u < T; u++) { dec[u] = ring_dec[r][q * T + u]; e += sq4px(t[u], tt[u], dec[u]); }
+                e = lsum<L>(e, gm);
                 ok = j <= cur;
             } else if (kind == 1) {  // its endpoints, best indices; texel 0 keeps to 0..7 (zap__bc7_fit6_idx)
                 const uint64_t nlo = ring[r][0], nhi = ring[r][1];
                 ok = j <= cur && is_mode6(nlo);
-                // key 16 (|p|^2 - 2 t.p) + k per entry (its minimum is the first nearest entry), minimised as a tree
-                int kk[16];
+                uint64_t bits = 0;
                 #pragma unroll
-                for (int k4 = 0; k4 < 4; k4++) {
-                    const uint4 pk = *(const uint4 *)&ring_pal[r][4 * k4];
-                    const int4 pp = *(const int4 *)&ring_pp[r][4 * k4];
-                    kk[4 * k4 + 0] = 16 * (pp.x - 2 * (int)dot4(t, pk.x)) + 4 * k4 + 0;
-                    kk[4 * k4 + 1] = 16 * (pp.y - 2 * (int)dot4(t, pk.y)) + 4 * k4 + 1;
-                    kk[4 * k4 + 2] = 16 * (pp.z - 2 * (int)dot4(t, pk.z)) + 4 * k4 + 2;
-                    kk[4 * k4 + 3] = 16 * (pp.w - 2 * (int)dot4(t, pk.w)) + 4 * k4 + 3;
-                }
-                if (i == 0) {  // the anchor texel's index has 3 bits
+                for (int u = 0; u < T; u++) {
+                    // key 16 (|p|^2 - 2 t.p) + k per entry (its minimum is the first nearest entry), minimised as a tree
+                    const int i = q * T + u;
+                    int kk[16];
                     #pragma unroll
-                    for (int k = 8; k < 16; k++) kk[k] = 0x7FFFFFFF;
-                }
-                #pragma unroll
-                for (int h = 8; h >= 1; h >>= 1)
+                    for (int k4 = 0; k4 < 4; k4++) {
+                        const uint4 pk = *(const uint4 *)&ring_pal[r][4 * k4];
+                        const int4 pp = *(const int4 *)&ring_pp[r][4 * k4];
+                        kk[4 * k4 + 0] = 16 * (pp.x - 2 * (int)dot4(t[u], pk.x)) + 4 * k4 + 0;
+                        kk[4 * k4 + 1] = 16 * (pp.y - 2 * (int)dot4(t[u], pk.y)) + 4 * k4 + 1;
+                        kk[4 * k4 + 2] = 16 * (pp.z - 2 * (int)dot4(t[u], pk.z)) + 4 * k4 + 2;
+                        kk[4 * k4 + 3] = 16 * (pp.w - 2 * (int)dot4(t[u], pk.w)) + 4 * k4 + 3;
+                    }
+                    if (i == 0) {  // the anchor texel's index has 3 bits
+                        #pragma unroll
+                        for (int k = 8; k < 16; k++) kk[k] = 0x7FFFFFFF;
+                    }
                     #pragma unroll
-                    for (int k = 0; k < h; k++) kk[k] = min(kk[k], kk[k + h]);
-                const int m = kk[0];
-                dec = ring_pal[r][m & 15];
-                e = grp_sum((m >> 4) + tt, gm);
-                cidx = grp_or64((uint64_t)(m & 15) << (4 * i), gm);
+                    for (int h = 8; h >= 1; h >>= 1)
+                        #pragma unroll
+                        for (int k = 0; k < h; k++) kk[k] = min(kk[k], kk[k + h]);
+                    dec[u] = ring_pal[r][kk[0] & 15];
+                    e += (kk[0] >> 4) + tt[u];
+                    bits |= (uint64_t)(kk[0] & 15) << (4 * i);
+                }
+                e = lsum<L>(e, gm);
+                cidx = ((uint64_t)lor<L>((uint32_t)(bits >> 32), gm) << 32) | lor<L>((uint32_t)bits, gm);
                 clo = nlo; chi = mode6_hi((int)(nhi & 1u), cidx);
             } else {  // its indices, least-squares endpoints, each endpoint's own p-bit (zap__bc7_fit6_ep)
                 const uint64_t nlo = ring[r][0], nhi = ring[r][1];
                 ok = j <= cur && is_mode6(nlo);
                 cidx = ring_idx[r];
-                const int w = w4((int)((cidx >> (4 * i)) & 15u));
-                const int ch = i >> 2, ep = i & 1;  // this lane's (channel, endpoint); lanes 2 apart repeat it
+                const int task = q & 7, ch = task >> 1, ep = task & 1;  // this lane's (channel, endpoint)
                 // the neighbour's weights and this block's channel ch, a byte per texel: sum w, sum w^2 and sum w x
                 // are four dp4a each; with u = 64 - w: sum u^2 = 16 * 4096 - 128 sum w + sum w^2,
                 // sum u w = 64 sum w - sum w^2, sum u x = 64 sum x - sum w x
@@ -315,28 +314,37 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src,
                 // each endpoint's errors over the four channels, both p-bits in one word (each below 2^16: a
                 // candidate lies within 2 of v); the endpoint keeps the p-bit of the smaller sum, p = 0 on ties
                 int s2 = be[0] | (be[1] << 16);
-                s2 += __shfl_xor_sync(gm, s2, 4, 16);
-                s2 += __shfl_xor_sync(gm, s2, 8, 16);
+                s2 += __shfl_xor_sync(gm, s2, 2, L);
+                s2 += __shfl_xor_sync(gm, s2, 4, L);
                 const int pbm = (s2 >> 16) < (s2 & 0xFFFF) ? 1 : 0, qm = pbm ? bq[1] : bq[0];
-                const int pb0 = __shfl_sync(gm, pbm, 0, 16), pb1 = __shfl_sync(gm, pbm, 1, 16);
+                const int pb0 = __shfl_sync(gm, pbm, 0, L), pb1 = __shfl_sync(gm, pbm, 1, L);
                 uint64_t lo = 0x40u | ((uint64_t)pb0 << 63);
                 #pragma unroll
                 for (int c = 0; c < 4; c++) {
-                    const int q0 = __shfl_sync(gm, qm, 4 * c, 16), q1 = __shfl_sync(gm, qm, 4 * c + 1, 16);
+                    const int q0 = __shfl_sync(gm, qm, 2 * c, L), q1 = __shfl_sync(gm, qm, 2 * c + 1, L);
                     x0[c] = (q0 << 1) | pb0; x1[c] = (q1 << 1) | pb1;
                     lo |= ((uint64_t)q0 << (7 + 14 * c)) | ((uint64_t)q1 << (14 + 14 * c));
                 }
-                dec = lerp_px(x0, x1, w);
-                e = grp_sum(sq4px(t, tt, dec), gm);
+                #pragma unroll
+                for (int u = 0; u < T; u++) {
+                    dec[u] = lerp_px(x0, x1, w4((int)((cidx >> (4 * (q * T + u))) & 15u)));
+                    e += sq4px(t[u], tt[u], dec[u]);
+                }
+                e = lsum<L>(e, gm);
                 clo = lo; chi = (nhi & ~1ull) | (uint64_t)pb1;
             }
-            // rate (zap__bc7_rate): lane i compares the candidate's fields with window slot j' = i + 1
-            const int rw = (cur - i - 1) & (kWindow - 1);
-            const bool vw = i + 1 <= cur;
-            const uint64_t wlo = ring[rw][0], whi = ring[rw][1];
-            const unsigned sh = lane & 16;
-            const unsigned mA = (__ballot_sync(gm, vw && wlo == clo) >> sh) & 0xFFFFu;
-            const unsigned mB = (__ballot_sync(gm, vw && (whi >> 8) == (chi >> 8)) >> sh) & 0xFFFFu;
+            // rate (zap__bc7_rate): bit d - 1 of a mask says the field equals the window's at distance d
+            uint32_t mA = 0, mB = 0;
+            #pragma unroll
+            for (int u = 0; u < T; u++) {
+                const int d = q * T + u + 1, rw = (cur - d) & (kWindow - 1);
+                if (d <= cur) {
+                    mA |= (uint32_t)(ring[rw][0] == clo) << (d - 1);
+                    mB |= (uint32_t)((ring[rw][1] >> 8) == (chi >> 8)) << (d - 1);
+                }
+            }
+            mA = lor<L>(mA, gm);
+            mB = lor<L>(mB, gm);
             float fa = 8.0f, fb = 7.0f;
             nd0 = d0; nd1 = d1;
             if (d0 > 0 && d0 <= cur && ((mA >> (d0 - 1)) & 1u)) fa = 0.0f;
@@ -353,21 +361,23 @@ __global__ void __launch_bounds__(kB7Threads, 1) rdo_bc7_chain_kernel(SrcU8 src,
             if (lane == 0) s_key[warp] = wk;
         }
         __syncthreads();
-        const int order = loader ? -1 : (int)(uint32_t)warp_min_redux(lane < kB7Warps ? s_key[lane] : ~0ull);
+        const int order = loader ? -1 : (int)(uint32_t)warp_min_redux(lane < kW ? s_key[lane] : ~0ull);
         const int oc = order - 1, wkind = oc % 3, wgrp = order == 0 ? 48 : wkind == 1 ? oc / 3 : wkind == 2 ? 16 + oc / 3 : 32 + oc / 3;
         if (!loader && grp == wgrp) {  // the winner enters the window
             const int ws = cur & (kWindow - 1);
-            ring_dec[ws][i] = dec;
-            // its mode-6 palette: the base's (built by the loader), the neighbour's (kinds 0 and 1 keep its endpoints;
-            // with j = 16 that slot is this one and each lane rewrites its own entry), or from the refit endpoints
-            uint32_t pal;
-            if (order == 0) pal = s_bpal[slot][i];
-            else if (kind != 2) pal = ring_pal[r][i];
-            else pal = lerp_px(x0, x1, w4(i));
-            ring_pal[ws][i] = pal;
-            ring_pp[ws][i] = (int)dot4(pal, pal);
-            ((uint8_t *)ring_wp[ws])[i] = (uint8_t)w4((int)((cidx >> (4 * i)) & 15u));
-            if (i == 0) {
+            // its decode, its mode-6 palette (the base's, built by the loader; the neighbour's, which kinds 0 and 1
+            // keep: with j = 16 that slot is this one and each lane rewrites its own entries; or from the refit
+            // endpoints) and its index weights
+            #pragma unroll
+            for (int u = 0; u < T; u++) {
+                const int i = q * T + u;
+                ring_dec[ws][i] = dec[u];
+                const uint32_t pal = order == 0 ? s_bpal[slot][i] : kind != 2 ? ring_pal[r][i] : lerp_px(x0, x1, w4(i));
+                ring_pal[ws][i] = pal;
+                ring_pp[ws][i] = (int)dot4(pal, pal);
+                ((uint8_t *)ring_wp[ws])[i] = (uint8_t)w4((int)((cidx >> (4 * i)) & 15u));
+            }
+            if (q == 0) {
                 ring[ws][0] = clo; ring[ws][1] = chi; ring_idx[ws] = cidx;
                 s_dist[0] = nd0; s_dist[1] = nd1;
                 if (order != 0) { *(uint64_t *)(out + (size_t)g * 16) = clo; *(uint64_t *)(out + (size_t)g * 16 + 8) = chi; }
@@ -413,16 +423,6 @@ template <int L> struct SubChain {  // kWc candidate warps, then the loader warp
 #define ZTC_RDO_SUB_LANES 8
 #endif
 
-template <int L> __device__ __forceinline__ int lsum(int v, unsigned gm) {
-    #pragma unroll
-    for (int m = L / 2; m >= 1; m >>= 1) v += __shfl_xor_sync(gm, v, m, L);
-    return v;
-}
-template <int L> __device__ __forceinline__ uint32_t lor(uint32_t v, unsigned gm) {
-    #pragma unroll
-    for (int m = L / 2; m >= 1; m >>= 1) v |= __shfl_xor_sync(gm, v, m, L);
-    return v;
-}
 
 template <int L>
 __global__ void __launch_bounds__(SubChain<L>::kThreads, 1) rdo_sub_chain_kernel(SrcU8 src, int bw, int nby, int chain_rows, uint8_t *__restrict__ out,
@@ -610,7 +610,8 @@ cudaError_t ztc_launch_rdo(int fmt, const ztc::SrcU8 &src, uint8_t *out, float l
         cudaError_t e = ztc_malloc_async((void **)&dec, (size_t)nblocks * 64, stream);
         if (e != cudaSuccess) return e;
         ztc::bc7_decode_bases_kernel<<<(nblocks + 127) / 128, 128, 0, stream>>>(out, nblocks, (uint4 *)dec);
-        ztc::rdo_bc7_chain_kernel<<<chains, ztc::kB7Threads, 0, stream>>>(src, bw, nby, band_rows, out, dec, lambda);
+        constexpr int L = ZTC_RDO_BC7_LANES;
+        ztc::rdo_bc7_chain_kernel<L><<<chains, ztc::B7Chain<L>::kThreads, 0, stream>>>(src, bw, nby, band_rows, out, dec, lambda);
         e = cudaGetLastError();
         cudaFreeAsync(dec, stream);
         return e;
