@@ -195,6 +195,20 @@ __device__ __forceinline__ void load_smem(AstcSmem &S) {
 }
 
 ZTC_DEV int astc_lerp(int a, int b, int w) { return (((a * 257) * (64 - w) + (b * 257) * w + 32) >> 6) >> 8; }
+// astc_lerp over the four channels of one endpoint pair as an affine function of w: the sum inside astc_lerp is
+// a * 257 * 64 + 32 + (b - a) * 257 * w, never negative, and (x >> 6) >> 8 = x >> 14, so an entry is
+// (base + slope * w) >> 14 per channel, astc_lerp's value with two operations a channel
+struct LerpRow {
+    int base[4], slope[4];
+    ZTC_DEV LerpRow(const int e0[4], const int e1[4]) {
+        #pragma unroll
+        for (int c = 0; c < 4; c++) { base[c] = 64 * 257 * e0[c] + 32; slope[c] = 257 * (e1[c] - e0[c]); }
+    }
+    ZTC_DEV uint32_t at(int w) const {
+        return pack_rgba((base[0] + slope[0] * w) >> 14, (base[1] + slope[1] * w) >> 14, (base[2] + slope[2] * w) >> 14,
+                         (base[3] + slope[3] * w) >> 14);
+    }
+};
 ZTC_DEV uint32_t get8(const uint32_t a[4], int i) { return (a[i >> 2] >> (8 * (i & 3))) & 0xFFu; }
 ZTC_DEV void set8(uint32_t a[4], int i, uint32_t v) {
     #pragma unroll
@@ -248,12 +262,11 @@ ZTC_DEV int astc_fit_weights(TexRef ts, uint32_t cm, int cem, int wb, const uint
     for (int k = 0; k < PARTS; k++) {
         int e0[4], e1[4];
         endpoint_pair(cem, uv[k], e0, e1);
+        const LerpRow row(e0, e1);
         #pragma unroll
         for (int j = 0; j < LMAX; j++) {
             if (j >= L) break;
-            const int w = wq[j];
-            uint32_t e = pack_rgba(astc_lerp(e0[0], e1[0], w), astc_lerp(e0[1], e1[1], w), astc_lerp(e0[2], e1[2], w),
-                                   astc_lerp(e0[3], e1[3], w)) & cm;
+            const uint32_t e = row.at(wq[j]) & cm;
             pal[k][j] = e;
             A[k][j] = (int)dot4(e, e) * LMAX + j;
         }
@@ -291,15 +304,14 @@ ZTC_DEV int astc_fit_weights_1p(TexRef ts, uint32_t cm, int cem, int wb, const u
     const int L = 1 << wb;
     int e0[4], e1[4];
     endpoint_pair(cem, uv, e0, e1);
+    const LerpRow row(e0, e1);
     uint32_t p[16];
     int best[16];
     #pragma unroll
     for (int i = 0; i < 16; i++) { p[i] = ts[i] & cm; best[i] = 0x7FFFFFFF; }
     #pragma unroll 1
     for (int j = 0; j < L; j++) {
-        const int w = wq[j];
-        const uint32_t e = pack_rgba(astc_lerp(e0[0], e1[0], w), astc_lerp(e0[1], e1[1], w), astc_lerp(e0[2], e1[2], w),
-                                     astc_lerp(e0[3], e1[3], w)) & cm;
+        const uint32_t e = row.at(wq[j]) & cm;
         const int a = (int)dot4(e, e) * LMAX + j;
         #pragma unroll
         for (int i = 0; i < 16; i++) best[i] = min(best[i], a - 2 * LMAX * (int)dot4(p[i], e));
