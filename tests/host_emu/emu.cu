@@ -131,6 +131,32 @@ __attribute__((visibility("default"))) uint64_t emu_srgb_search_mismatches(uint6
     return bad;
 }
 
+// endpoint pairs and weights for which ztc::Lerp4 (two channels per word) differs from four lerp64 calls: every
+// (a, b) pair in the low fields (R, G) and in the high fields (B, A) at every weight 0..64, against extreme and
+// mixed values in the other field (the low field's negative slopes borrow from the high field)
+__attribute__((visibility("default"))) uint64_t emu_lerp4_mismatches() {
+    const int other[6][2] = {{0, 0}, {255, 255}, {0, 255}, {255, 0}, {17, 200}, {200, 17}};
+    uint64_t bad = 0;
+    for (int hi_field = 0; hi_field < 2; hi_field++)
+        for (int a = 0; a < 256; a++)
+            for (int b = 0; b < 256; b++)
+                for (int o = 0; o < 6; o++) {
+                    int x0[4], x1[4];
+                    for (int c = 0; c < 4; c++) {
+                        const bool mine = (c >= 2) == (hi_field == 1);
+                        x0[c] = mine ? a : other[o][0];
+                        x1[c] = mine ? b : other[o][1];
+                    }
+                    const Lerp4 row(x0, x1);
+                    for (int w = 0; w <= 64; w++) {
+                        const uint32_t want = pack_rgba(lerp64(x0[0], x1[0], w), lerp64(x0[1], x1[1], w), lerp64(x0[2], x1[2], w),
+                                                        lerp64(x0[3], x1[3], w));
+                        bad += row.at(w) != want;
+                    }
+                }
+    return bad;
+}
+
 // finite floats x with bit patterns in [lo, hi) for which ztc::div255(x) differs bitwise from the division x / 255.0f
 // (-0, whose documented quotient is +0, excepted)
 __attribute__((visibility("default"))) uint64_t emu_div255_mismatches(uint64_t lo, uint64_t hi) {

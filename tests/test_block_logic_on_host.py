@@ -42,6 +42,8 @@ def emu():
     lib.emu_div_small_mismatches.restype = C.c_uint64
     lib.emu_srgb_search_mismatches.argtypes = [C.c_uint64, C.c_uint64]
     lib.emu_srgb_search_mismatches.restype = C.c_uint64
+    lib.emu_lerp4_mismatches.argtypes = []
+    lib.emu_lerp4_mismatches.restype = C.c_uint64
     return lib
 
 
@@ -163,3 +165,10 @@ def test_srgb_bucket_search_equals_binary_search(emu):
     bad += emu.emu_srgb_search_mismatches(0x7F800000, 0x7F800001)  # +inf
     bad += emu.emu_srgb_search_mismatches(0x80000000, 0x80000000 + (1 << 20))  # -0 and small negatives
     assert bad == 0
+
+
+def test_packed_lerp_equals_lerp64(emu):
+    """The encoders build BC7 palettes with two channels per 32-bit word (one multiply-add for R and B, one for G
+    and A); every endpoint pair and weight must give lerp64's bytes, including negative slopes that borrow across
+    the fields."""
+    assert emu.emu_lerp4_mismatches() == 0

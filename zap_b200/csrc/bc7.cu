@@ -40,12 +40,11 @@ ZTC_DEV int palette_fit(TexRef ts, uint32_t mask, const int x0[4], const int x1[
     const uint32_t cm = NC == 4 ? 0xFFFFFFFFu : 0x00FFFFFFu;
     uint32_t pal[NP];
     int A[NP];
+    const int y0[4] = {x0[0], x0[1], x0[2], NC == 4 ? x0[3] : 0}, y1[4] = {x1[0], x1[1], x1[2], NC == 4 ? x1[3] : 0};
+    const Lerp4 row(y0, y1);
     #pragma unroll
     for (int j = 0; j < NP; j++) {
-        int wj = wbits(IB, j);
-        uint32_t e = 0;
-        #pragma unroll
-        for (int c = 0; c < NC; c++) e |= (uint32_t)lerp64(x0[c], x1[c], wj) << (8 * c);
+        const uint32_t e = row.at(wbits(IB, j)) & cm;
         pal[j] = e;
         A[j] = (int)dot4(e, e) * NP + j;
     }

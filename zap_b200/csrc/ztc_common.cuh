@@ -136,6 +136,23 @@ ZTC_DEV int w3(int j) { return (64 * j + 3) / 7; }
 ZTC_DEV int w4(int j) { return (64 * j + 7) / 15; }
 ZTC_DEV int wbits(int bits, int j) { return bits == 2 ? w2(j) : bits == 3 ? w3(j) : w4(j); }
 ZTC_DEV int lerp64(int a, int b, int w) { return ((64 - w) * a + w * b + 32) >> 6; }
+// lerp64 over four 8-bit channels at once, packed like a texel. The sum inside lerp64 is 64 a + 32 + (b - a) w, in
+// [0, 2^14) for 8-bit a, b and 0 <= w <= 64, so two channels share a word as 16-bit fields (R with B, G with A):
+// one multiply-add computes both (a negative slope borrows from the upper field, but both fields' results are exact
+// and non-negative, so they separate), and bits 6..13 of each field are the channel's value
+struct Lerp4 {
+    uint32_t rb, ga, srb, sga;
+    ZTC_DEV Lerp4(const int x0[4], const int x1[4]) {  // 8-bit endpoint channels
+        rb = (uint32_t)(64 * x0[0] + 32) | ((uint32_t)(64 * x0[2] + 32) << 16);
+        ga = (uint32_t)(64 * x0[1] + 32) | ((uint32_t)(64 * x0[3] + 32) << 16);
+        srb = (uint32_t)(x1[0] - x0[0]) + ((uint32_t)(x1[2] - x0[2]) << 16);  // modulo 2^32, as the sums are
+        sga = (uint32_t)(x1[1] - x0[1]) + ((uint32_t)(x1[3] - x0[3]) << 16);
+    }
+    ZTC_DEV uint32_t at(int w) const {  // the four channels' lerp64 at weight w, as a texel
+        const uint32_t a = rb + srb * (uint32_t)w, b = ga + sga * (uint32_t)w;
+        return ((a >> 6) & 0x00FF00FFu) | ((b << 2) & 0xFF00FF00u);
+    }
+};
 ZTC_DEV int expand_bits(int v, int n) { v <<= 8 - n; return v | (v >> n); }  // n-bit -> 8-bit replication
 
 // endpoint quantisation with a fixed p-bit (zap_tex.h:426-438); q: stored values, x8: expanded 8-bit values
