@@ -64,10 +64,9 @@ ZTC_DEV int palette_fit(TexRef ts, uint32_t mask, const int x0[4], const int x1[
     return err;
 }
 
-// float endpoints -> best p-bits, quantised endpoints, indices (zap_tex.h:466-486)
-template <int NC, int IB>
-ZTC_DEV int subset_fit(TexRef ts, uint32_t mask, int n, bool shared_p, const float lo[4], const float hi[4],
-                       int q[2][4], int pb[2], uint64_t &idx) {
+// float endpoints -> best p-bits and quantised endpoints q (x0, x1: expanded to 8 bits) (zap_tex.h:466-486)
+template <int NC>
+ZTC_DEV void subset_quant(int n, bool shared_p, const float lo[4], const float hi[4], int q[2][4], int pb[2], int x0[4], int x1[4]) {
     int ql[2][4], qh[2][4], xl[2][4], xh[2][4], el[2], eh[2];
     #pragma unroll
     for (int p = 0; p < 2; p++) { el[p] = quant_pbit<NC>(lo, n, p, ql[p], xl[p]); eh[p] = quant_pbit<NC>(hi, n, p, qh[p], xh[p]); }
@@ -79,21 +78,29 @@ ZTC_DEV int subset_fit(TexRef ts, uint32_t mask, int n, bool shared_p, const flo
         int e = el[p0] + eh[p1];
         if (e < best) { best = e; b0 = p0; b1 = p1; }
     }
-    int x0[4], x1[4];
     #pragma unroll
     for (int c = 0; c < 4; c++) {
         q[0][c] = b0 ? ql[1][c] : ql[0][c]; q[1][c] = b1 ? qh[1][c] : qh[0][c];
         x0[c] = b0 ? xl[1][c] : xl[0][c]; x1[c] = b1 ? xh[1][c] : xh[0][c];
     }
     pb[0] = b0; pb[1] = b1;
-    return palette_fit<NC, IB>(ts, mask, x0, x1, idx);
+}
+// the quantised endpoints and p-bits q, pb equal a, apb (the channels the subset codes)
+template <int NC>
+ZTC_DEV bool same_ends(const int q[2][4], const int pb[2], const int a[2][4], const int apb[2]) {
+    bool same = pb[0] == apb[0] && pb[1] == apb[1];
+    #pragma unroll
+    for (int c = 0; c < NC; c++) same = same && q[0][c] == a[0][c] && q[1][c] == a[1][c];
+    return same;
 }
 
 // Passes [first, last) of a subset's fit sequence (zap_tex.h:489-515): pass 0 fits the endpoints (lo, hi); pass
 // k > 0 is the k-th least-squares refit on the indices `idx` holds, which does not run at SSE 0, stops at a
 // singular system, and is dropped (ending the sequence) when it does not lower the SSE. err: the SSE before
 // `first`; q, pb, idx take each accepted pass. Returns the SSE; more: all the passes ran and the SSE is still
-// above 0, so pass `last` would run. One fit call site keeps the code small.
+// above 0, so pass `last` would run. One fit call site keeps the code small. A refit that quantises to the
+// accepted endpoints and p-bits would fit the same palette to the same texels and give the same SSE, which does not
+// lower it: the sequence ends there without the fit.
 template <int NC, int IB>
 ZTC_DEV int subset_passes(TexRef ts, uint32_t mask, int n, bool shared_p, float lo[4], float hi[4], int first, int last, int err,
                           int q[2][4], int pb[2], uint64_t &idx, bool &more) {
@@ -122,9 +129,11 @@ ZTC_DEV int subset_passes(TexRef ts, uint32_t mask, int n, bool shared_p, float 
                 else { lo[c] = 255.0f; hi[c] = 255.0f; }
             }
         }
-        int nq[2][4], npb[2];
+        int nq[2][4], npb[2], x0[4], x1[4];
+        subset_quant<NC>(n, shared_p, lo, hi, nq, npb, x0, x1);
+        if (it > 0 && same_ends<NC>(nq, npb, q, pb)) return err;
         uint64_t ni;
-        const int ne = subset_fit<NC, IB>(ts, mask, n, shared_p, lo, hi, nq, npb, ni);
+        const int ne = palette_fit<NC, IB>(ts, mask, x0, x1, ni);
         if (it > 0 && ne >= err) return err;
         err = ne; idx = ni; pb[0] = npb[0]; pb[1] = npb[1];
         #pragma unroll
@@ -207,11 +216,10 @@ __device__ __forceinline__ int mode6_encode_cta(bool valid, const uint32_t t[16]
         else pca_endpoints<4>(t, 0xFFFFu, lo, hi);
     }
     bool active = valid;
-    int owner = tid, first = 0, err = 0;
+    int owner = tid, first = 0, err = 0, q[2][4], pb[2];  // q, pb, idx, err: the accepted fit (the owner's in round 1)
     uint64_t idx = 0;
     #pragma unroll 1
     for (int round = 0; round < 2; round++) {
-        int q[2][4], pb[2];
         bool more = false;
         const int e_in = err;
         if (active)
@@ -230,12 +238,11 @@ __device__ __forceinline__ int mode6_encode_cta(bool valid, const uint32_t t[16]
         active = tid < total;
         if (active) owner = s_list[tid];
         if (active && !ZTC_IN_BOUNDS(owner, CTA, 8)) active = false;
-        if (active) { err = s_err[owner]; idx = s_idx[owner]; }
+        if (active) { err = s_err[owner]; idx = s_idx[owner]; unpack_qp(s_qp[owner], q, pb); }
         first = 2;
     }
     __syncthreads();
     if (!valid) return 0;
-    int q[2][4], pb[2];
     unpack_qp(s_qp[tid], q, pb);
     blk = pack_mode6_block(q, pb, s_idx[tid]);
     return s_err[tid];
@@ -383,6 +390,12 @@ ZTC_DEV int m5_part(const uint32_t p[16], float lo[3], float hi[3], int q[2][3],
         if (it > 0 && !m5_lsq<KIND>(p, nc, idx, lo, hi)) break;
         int tq[2][3], x0[3], x1[3];
         m5_quant<KIND>(lo, nc, n, tq[0], x0); m5_quant<KIND>(hi, nc, n, tq[1], x1);
+        if (it > 0) {  // the accepted endpoints again: the same fit and SSE, which ends the refits
+            bool same = true;
+            #pragma unroll
+            for (int c = 0; c < 3; c++) same = same && (c >= nc || (tq[0][c] == q[0][c] && tq[1][c] == q[1][c]));
+            if (same) break;
+        }
         uint32_t ti;
         const int e = m5_fit<KIND>(p, x0, x1, ti);
         if (it > 0 && e >= err) break;

@@ -117,6 +117,8 @@ ZTC_DEV void bc1_one_start(const Bc1Texels &T, TexRef tx, int start, float mu0, 
         if (det < 1e-6f && det > -1e-6f) break;
         uint32_t n0 = pack565((sa0 * bb - sb0 * ab) / det, (sa1 * bb - sb1 * ab) / det, (sa2 * bb - sb2 * ab) / det);
         uint32_t n1 = pack565((sb0 * aa - sa0 * ab) / det, (sb1 * aa - sa1 * ab) / det, (sb2 * aa - sa2 * ab) / det);
+        // the accepted pair again (bc1_try orders it c0 >= c1): the same fit and SSE, which ends the refits
+        if (max(n0, n1) == c0 && min(n0, n1) == c1) break;
         uint32_t ni = 0;
         int ne = bc1_try(T, n0, n1, ni);
         if (ne >= e) break;
