@@ -133,13 +133,9 @@ ZTC_DEV void bc1_one_start(const Bc1Texels &T, TexRef tx, int start, float mu0, 
 // shared memory
 template <int UNROLL = 16>
 ZTC_DEV void bc1_start(const Bc1Texels &T, TexRef tx, uint32_t &b0, uint32_t &b1, uint32_t &bidx, int &best) {
-    float mu0 = 0.0f, mu1 = 0.0f, mu2 = 0.0f;
-    for_texels<UNROLL>([&](int i) {
-        const uint32_t x = bc1_texel<UNROLL>(T, tx, i);
-        mu0 = mu0 + (float)chan(x, 0) / 16.0f;
-        mu1 = mu1 + (float)chan(x, 1) / 16.0f;
-        mu2 = mu2 + (float)chan(x, 2) / 16.0f;
-    });
+    // the reference's mean sums x / 16 in texel order; every term and every partial sum is exact (a multiple of 1/16
+    // below 256), so the float sum is the channel's integer sum / 16
+    const float mu0 = (float)T.sr / 16.0f, mu1 = (float)T.sg / 16.0f, mu2 = (float)T.sb / 16.0f;
     float C0 = 0, C1 = 0, C2 = 0, C3 = 0, C4 = 0, C5 = 0;
     for_texels<UNROLL>([&](int i) {
         const uint32_t x = bc1_texel<UNROLL>(T, tx, i);

@@ -31,17 +31,28 @@ ZTC_DEV void pca_endpoints(const Tex &t, uint32_t mask, float lo[4], float hi[4]
     const float cnt = (float)popc(mask), cnti = 1.0f / cnt;
     const bool whole = mask == 0xFFFFu;  // a compile-time constant for whole-block calls: x / 16 is a multiply there
     float mu[NC];
-    #pragma unroll
-    for (int c = 0; c < NC; c++) mu[c] = 0.0f;
-    for_texels<UNROLL>([&](int i) {
-        if ((mask >> i) & 1u) {
-            #pragma unroll
-            for (int c = 0; c < NC; c++) {
-                const float x = (float)chan(t[i], c);
-                mu[c] = mu[c] + (whole ? x / 16.0f : div_small(x, cnt, cnti));
+    if (whole) {
+        // every term x / 16 and every partial sum of the mean is exact (a multiple of 1/16 below 256), so the
+        // float sum is the channel's integer sum / 16; the four sums in two words of 16-bit fields
+        uint32_t s02 = 0, s13 = 0;
+        for_texels<UNROLL>([&](int i) {
+            const uint32_t x = t[i];
+            s02 += x & 0x00FF00FFu;
+            s13 += (x >> 8) & 0x00FF00FFu;
+        });
+        const uint32_t S[4] = {s02 & 0xFFFFu, s13 & 0xFFFFu, s02 >> 16, s13 >> 16};
+        #pragma unroll
+        for (int c = 0; c < NC; c++) mu[c] = (float)S[c] / 16.0f;
+    } else {
+        #pragma unroll
+        for (int c = 0; c < NC; c++) mu[c] = 0.0f;
+        for_texels<UNROLL>([&](int i) {
+            if ((mask >> i) & 1u) {
+                #pragma unroll
+                for (int c = 0; c < NC; c++) mu[c] = mu[c] + div_small((float)chan(t[i], c), cnt, cnti);
             }
-        }
-    });
+        });
+    }
     // upper triangle only: cov[a][b] and cov[b][a] add bitwise-identical products in the same order
     float C[NC][NC];
     #pragma unroll
