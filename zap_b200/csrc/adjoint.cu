@@ -624,6 +624,7 @@ static int launch_status(const char *what) {
 extern "C" {
 
 int zap_tex_cuda_block_endpoints_dev(zap_tex_cuda_ctx *ctx, int fmt, const void *blocks, int nblocks, float *endpoints, void *stream) {
+    ZTC_NVTX();
     int st = adj_check(fmt, blocks, nblocks);
     if (st || (st = ztc_ctx_activate(ctx))) return st;
     if (!endpoints || floats_misaligned(endpoints)) return ztc_set_error(ZTC_ERR_INVALID_ARG, "null or misaligned endpoints");
@@ -633,6 +634,7 @@ int zap_tex_cuda_block_endpoints_dev(zap_tex_cuda_ctx *ctx, int fmt, const void 
 
 int zap_tex_cuda_palette_decode_dev(zap_tex_cuda_ctx *ctx, int fmt, const void *blocks, int nblocks, const float *endpoints, float *decoded,
                                     void *stream) {
+    ZTC_NVTX();
     int st = adj_check(fmt, blocks, nblocks);
     if (st || (st = ztc_ctx_activate(ctx))) return st;
     if (!endpoints || !decoded || floats_misaligned(endpoints, decoded))
@@ -643,6 +645,7 @@ int zap_tex_cuda_palette_decode_dev(zap_tex_cuda_ctx *ctx, int fmt, const void *
 
 int zap_tex_cuda_palette_adjoint_dev(zap_tex_cuda_ctx *ctx, int fmt, const void *blocks, int nblocks, const float *grad_decoded,
                                      float *grad_endpoints, void *stream) {
+    ZTC_NVTX();
     int st = adj_check(fmt, blocks, nblocks);
     if (st || (st = ztc_ctx_activate(ctx))) return st;
     if (!grad_decoded || !grad_endpoints || floats_misaligned(grad_decoded, grad_endpoints))
@@ -655,6 +658,7 @@ int zap_tex_cuda_palette_adjoint_dev(zap_tex_cuda_ctx *ctx, int fmt, const void 
 
 int zap_tex_cuda_refine_dev(zap_tex_cuda_ctx *ctx, int fmt, const uint8_t *rgba, int w, int h, size_t stride, void *blocks, int steps,
                             float lr, uint32_t *sse_before, uint32_t *sse_after, void *stream) {
+    ZTC_NVTX();
     int st = adj_check(fmt, blocks, 0);
     if (st) return st;
     if (!rgba || w < 1 || h < 1 || stride < (size_t)w * 4 || steps < 0 || steps > 1000 || !(lr >= 0.0f))

@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(kProbeThreads) alu_probe_kernel(uint32_t *sink
 }  // namespace ztc
 
 extern "C" ZTC_API int zap_tex_cuda_alu_probe_dev(int kind, int iters, void *sink, void *stream, double *instructions) {
+    ZTC_NVTX();
     if (kind < 0 || kind > 3 || iters < 1 || !sink || ((uintptr_t)sink & 3u)) return ztc_set_error(ZTC_ERR_INVALID_ARG, "bad probe arguments");
     int dev = 0, major = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return ztc_set_error(ZTC_ERR_NO_DEVICE, "no CUDA device"); }

@@ -453,12 +453,14 @@ int zap_tex_cuda_trace_report(char *buf, size_t cap) {
 }
 
 int zap_tex_cuda_create(int device, zap_tex_cuda_ctx **out) {
+    ZTC_NVTX();
     if (!out) return fail(ZTC_ERR_INVALID_ARG, "null out");
     *out = nullptr;
     return create_ctx(device, out);
 }
 
 int zap_tex_cuda_destroy(zap_tex_cuda_ctx *c) {
+    ZTC_NVTX();
     if (!c) return ZTC_OK;
     int prev = 0;
     cudaGetDevice(&prev);
@@ -477,6 +479,7 @@ int zap_tex_cuda_destroy(zap_tex_cuda_ctx *c) {
 }
 
 int zap_tex_cuda_reserve(zap_tex_cuda_ctx *ctx, size_t bytes) {
+    ZTC_NVTX();
     int st = resolve(ctx);
     if (st) return st;
     // _dev calls draw scratch from the device's default memory pool: keep that much resident across frees
@@ -504,6 +507,7 @@ int zap_tex_cuda_mip_levels(int w, int h) {
 
 // ------------------------------------------------------------------ host memory
 int zap_tex_cuda_bc_encode(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo, void *out) {
+    ZTC_NVTX();
     int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
     if (st) return st;
     if (!valid_fmt_bc(fmt)) return fail(ZTC_ERR_UNSUPPORTED, "format %d", fmt);
@@ -524,6 +528,7 @@ int zap_tex_cuda_bc_encode(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, in
 }
 
 int zap_tex_cuda_bc6h_encode(zap_tex_cuda_ctx *ctx, const float *rgba, int w, int h, size_t stride, void *out) {
+    ZTC_NVTX();
     int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
     if (st) return st;
     if ((st = resolve(ctx))) return st;
@@ -531,6 +536,7 @@ int zap_tex_cuda_bc6h_encode(zap_tex_cuda_ctx *ctx, const float *rgba, int w, in
 }
 
 int zap_tex_cuda_astc_encode(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, void *out) {
+    ZTC_NVTX();
     int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
     if (st) return st;
     if ((st = resolve(ctx))) return st;
@@ -555,6 +561,7 @@ static int host_mip(zap_tex_cuda_ctx *ctx, const void *src, int w, int h, size_t
 }
 
 int zap_tex_cuda_mip_next(zap_tex_cuda_ctx *ctx, const uint8_t *src, int w, int h, size_t stride, int srgb, uint8_t *dst, size_t dst_stride) {
+    ZTC_NVTX();
     int st = check_image(src, dst, w, h, stride, (size_t)w * 4);
     if (st) return st;
     if (dst_stride < (size_t)(w > 1 ? w / 2 : 1) * 4) return fail(ZTC_ERR_INVALID_ARG, "dst_stride %zu too small", dst_stride);
@@ -563,6 +570,7 @@ int zap_tex_cuda_mip_next(zap_tex_cuda_ctx *ctx, const uint8_t *src, int w, int 
 }
 
 int zap_tex_cuda_mip_next_f(zap_tex_cuda_ctx *ctx, const float *src, int w, int h, size_t stride, float *dst, size_t dst_stride) {
+    ZTC_NVTX();
     int st = check_image(src, dst, w, h, stride, (size_t)w * 4);
     if (st) return st;
     if (dst_stride < (size_t)(w > 1 ? w / 2 : 1) * 4) return fail(ZTC_ERR_INVALID_ARG, "dst_stride %zu too small", dst_stride);
@@ -573,6 +581,7 @@ int zap_tex_cuda_mip_next_f(zap_tex_cuda_ctx *ctx, const float *src, int w, int 
 // ------------------------------------------------------------------ device memory
 int zap_tex_cuda_bc_encode_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo, void *out,
                                void *stream) {
+    ZTC_NVTX();
     if (!valid_fmt_bc(fmt)) return fail(ZTC_ERR_UNSUPPORTED, "format %d", fmt);
     int st = check_lambda(rdo);
     if (st) return st;
@@ -582,6 +591,7 @@ int zap_tex_cuda_bc_encode_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w
 
 int zap_tex_cuda_bc_encode_rdo_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo, int band_rows,
                                    void *out, void *stream) {
+    ZTC_NVTX();
     int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
     if (st) return st;
     if (!valid_fmt_bc(fmt)) return fail(ZTC_ERR_UNSUPPORTED, "format %d", fmt);
@@ -596,6 +606,7 @@ int zap_tex_cuda_bc_encode_rdo_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, i
 
 int zap_tex_cuda_bc_encode_u8_dev(zap_tex_cuda_ctx *ctx, const uint8_t *src, int channels, int w, int h, size_t stride, int fmt, void *out,
                                   void *stream) {
+    ZTC_NVTX();
     if (channels != 1 && channels != 2 && channels != 4) return fail(ZTC_ERR_INVALID_ARG, "channels %d", channels);
     int st = check_image(src, out, w, h, stride, (size_t)w * channels);
     if (st) return st;
@@ -637,19 +648,26 @@ static int dev_regroup(zap_tex_cuda_ctx *ctx, const void *in, size_t n, int fmt,
     return ZTC_OK;
 }
 
-int zap_tex_cuda_bc_split(zap_tex_cuda_ctx *ctx, const void *bc, size_t n, int fmt, void *out) { return host_regroup(ctx, bc, n, fmt, out, 1); }
+int zap_tex_cuda_bc_split(zap_tex_cuda_ctx *ctx, const void *bc, size_t n, int fmt, void *out) {
+    ZTC_NVTX();
+    return host_regroup(ctx, bc, n, fmt, out, 1);
+}
 int zap_tex_cuda_bc_merge(zap_tex_cuda_ctx *ctx, const void *planes, size_t n, int fmt, void *out) {
+    ZTC_NVTX();
     return host_regroup(ctx, planes, n, fmt, out, 0);
 }
 int zap_tex_cuda_bc_split_dev(zap_tex_cuda_ctx *ctx, const void *bc, size_t n, int fmt, void *out, void *stream) {
+    ZTC_NVTX();
     return dev_regroup(ctx, bc, n, fmt, out, 1, stream);
 }
 int zap_tex_cuda_bc_merge_dev(zap_tex_cuda_ctx *ctx, const void *planes, size_t n, int fmt, void *out, void *stream) {
+    ZTC_NVTX();
     return dev_regroup(ctx, planes, n, fmt, out, 0, stream);
 }
 
 int zap_tex_cuda_bc_encode_split_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, void *out,
                                      void *stream) {
+    ZTC_NVTX();
     int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
     if (st) return st;
     if (!valid_fmt_bc(fmt)) return fail(ZTC_ERR_UNSUPPORTED, "format %d (the split form exists for BC1..BC7)", fmt);
@@ -671,6 +689,7 @@ int zap_tex_cuda_bc_encode_split_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba,
 }
 
 int zap_tex_cuda_bc6h_encode_dev(zap_tex_cuda_ctx *ctx, const float *rgba, int w, int h, size_t stride, void *out, void *stream) {
+    ZTC_NVTX();
     int st = check_image(rgba, out, w, h, stride, (size_t)w * 4);
     if (st) return st;
     if (misaligned(rgba, 4) || misaligned(out, 16)) return fail(ZTC_ERR_INVALID_ARG, "misaligned texels (4 B) or blocks (16 B)");
@@ -682,6 +701,7 @@ int zap_tex_cuda_bc6h_encode_dev(zap_tex_cuda_ctx *ctx, const float *rgba, int w
 
 int zap_tex_cuda_bc6h_encode_half_dev(zap_tex_cuda_ctx *ctx, const uint16_t *src, int channels, int w, int h, size_t stride, void *out,
                                       void *stream) {
+    ZTC_NVTX();
     if (channels != 3 && channels != 4) return fail(ZTC_ERR_INVALID_ARG, "channels %d", channels);
     int st = check_image(src, out, w, h, stride, (size_t)w * channels);
     if (st) return st;
@@ -693,11 +713,13 @@ int zap_tex_cuda_bc6h_encode_half_dev(zap_tex_cuda_ctx *ctx, const uint16_t *src
 }
 
 int zap_tex_cuda_astc_encode_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, void *out, void *stream) {
+    ZTC_NVTX();
     return zap_tex_cuda_bc_encode_u8_dev(ctx, rgba, 4, w, h, stride, ZTC_ASTC4X4, out, stream);
 }
 
 int zap_tex_cuda_mip_next_dev(zap_tex_cuda_ctx *ctx, const uint8_t *src, int w, int h, size_t stride, int srgb, uint8_t *dst,
                               size_t dst_stride, void *stream) {
+    ZTC_NVTX();
     int st = check_image(src, dst, w, h, stride, (size_t)w * 4);
     if (st) return st;
     if ((st = resolve(ctx))) return st;
@@ -707,6 +729,7 @@ int zap_tex_cuda_mip_next_dev(zap_tex_cuda_ctx *ctx, const uint8_t *src, int w, 
 
 int zap_tex_cuda_mip_next_f_dev(zap_tex_cuda_ctx *ctx, const float *src, int w, int h, size_t stride, float *dst, size_t dst_stride,
                                 void *stream) {
+    ZTC_NVTX();
     int st = check_image(src, dst, w, h, stride, (size_t)w * 4);
     if (st) return st;
     if (misaligned(src, 4) || misaligned(dst, 4)) return fail(ZTC_ERR_INVALID_ARG, "float texels must be 4-byte aligned");
@@ -725,6 +748,7 @@ size_t zap_tex_cuda_mip_chain_bytes(int w, int h) {
 }
 
 int zap_tex_cuda_mip_chain_dev(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int srgb, uint8_t *dst, void *stream) {
+    ZTC_NVTX();
     int st = check_image(rgba, dst, w, h, stride, (size_t)w * 4);
     if (st) return st;
     if ((st = resolve(ctx))) return st;

@@ -281,6 +281,7 @@ size_t zap_tex_cuda_batch_item_bytes(int w, int h, int fmt, int levels) {
 }
 
 int zap_tex_cuda_batch_destroy(zap_tex_cuda_batch *b) {
+    ZTC_NVTX();
     if (!b) return ZTC_OK;
     int prev = 0;
     cudaGetDevice(&prev);
@@ -305,6 +306,7 @@ int zap_tex_cuda_batch_destroy(zap_tex_cuda_batch *b) {
 }
 
 int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *items, int n, int flags, zap_tex_cuda_batch **out) {
+    ZTC_NVTX();
     if (!out || !items || n < 1) return ztc_set_error(ZTC_ERR_INVALID_ARG, "batch: null items / out or n < 1");
     *out = nullptr;
     for (int i = 0; i < n; i++) {
@@ -463,6 +465,7 @@ int zap_tex_cuda_batch_create(zap_tex_cuda_ctx *ctx, const zap_tex_cuda_item *it
 }
 
 int zap_tex_cuda_batch_run(zap_tex_cuda_batch *b, void *stream) {
+    ZTC_NVTX();
     if (!b) return ztc_set_error(ZTC_ERR_INVALID_ARG, "null batch");
     BCHECK(cudaSetDevice(b->device), "cudaSetDevice");
     cudaStream_t s = (cudaStream_t)stream;

@@ -1006,6 +1006,7 @@ void *g_noalloc_addr[64];  // per device: device address of g_bc7_noalloc_scratc
 
 extern "C" __attribute__((visibility("default"))) int zap_tex_cuda_bc7_encode_noalloc_dev(const uint8_t *rgba, int w, int h,
                                                                                            size_t stride, void *out, void *stream) {
+    ZTC_NVTX();
     if (!rgba || !out) return ztc_set_error(ZTC_ERR_INVALID_ARG, "null pointer");
     if (w < 1 || h < 1 || w > (1 << 24) || h > (1 << 24)) return ztc_set_error(ZTC_ERR_INVALID_ARG, "size out of range");
     if (stride < (size_t)w * 4) return ztc_set_error(ZTC_ERR_INVALID_ARG, "stride below 4 * width");

@@ -88,6 +88,7 @@ size_t zap_tex_cuda_tex_file_bytes(int w, int h, int fmt, int mips, int srgb) {
 
 int zap_tex_cuda_tex_file(zap_tex_cuda_ctx *ctx, const uint8_t *rgba, int w, int h, size_t stride, int fmt, float rdo, int mips,
                           int srgb, void *out, size_t out_cap) {
+    ZTC_NVTX();
     if (!rgba || !out || w < 1 || h < 1 || stride < (size_t)w * 4) return ztc_set_error(ZTC_ERR_INVALID_ARG, "bad texture file arguments");
     if (!dds_format(fmt) && fmt != ZTC_ASTC4X4) return ztc_set_error(ZTC_ERR_UNSUPPORTED, "file format must be BC1..BC7 or ASTC 4x4");
     const size_t need = zap_tex_cuda_tex_file_bytes(w, h, fmt, mips, srgb);

@@ -110,26 +110,32 @@ int host_decode(Kind k, zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, int
 extern "C" {
 
 int zap_tex_cuda_bc_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, int fmt, uint8_t *rgba, size_t stride, void *stream) {
+    ZTC_NVTX();
     return dev_decode(kBcn, ctx, bc, w, h, fmt, rgba, stride, stream);
 }
 
 int zap_tex_cuda_bc6h_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint16_t *rgba, size_t stride, void *stream) {
+    ZTC_NVTX();
     return dev_decode(kBc6h, ctx, bc, w, h, ZTC_BC6H, rgba, stride, stream);
 }
 
 int zap_tex_cuda_astc_decode_dev(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint8_t *rgba, size_t stride, void *stream) {
+    ZTC_NVTX();
     return dev_decode(kAstc, ctx, bc, w, h, ZTC_ASTC4X4, rgba, stride, stream);
 }
 
 int zap_tex_cuda_bc_decode(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, int fmt, uint8_t *rgba, size_t stride) {
+    ZTC_NVTX();
     return host_decode(kBcn, ctx, bc, w, h, fmt, rgba, stride, 4);
 }
 
 int zap_tex_cuda_bc6h_decode(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint16_t *rgba, size_t stride) {
+    ZTC_NVTX();
     return host_decode(kBc6h, ctx, bc, w, h, ZTC_BC6H, rgba, stride, 8);
 }
 
 int zap_tex_cuda_astc_decode(zap_tex_cuda_ctx *ctx, const void *bc, int w, int h, uint8_t *rgba, size_t stride) {
+    ZTC_NVTX();
     return host_decode(kAstc, ctx, bc, w, h, ZTC_ASTC4X4, rgba, stride, 4);
 }
 

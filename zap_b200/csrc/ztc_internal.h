@@ -3,6 +3,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 enum { ZTC_FMT_BC1 = 0, ZTC_FMT_BC3 = 1, ZTC_FMT_BC4 = 2, ZTC_FMT_BC5 = 3, ZTC_FMT_BC7 = 4, ZTC_FMT_BC6H = 5, ZTC_FMT_ASTC = 6 };
 
@@ -17,6 +18,17 @@ struct SrcHdr {
     size_t stride;  // elements (floats or halfs) per row
     int w, h, channels, f32;
 };
+
+// An NVTX range over one C-ABI call, named after the entry point, so a timeline profiler shows each call with its
+// copies and kernels under it. NVTX v3 is header-only: with no profiler attached, a push and a pop each test one
+// pointer.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+#define ZTC_NVTX() ::ztc::NvtxRange ztc_nvtx_range_(__func__)
 
 // Kernel tracing (off by default): CUDA events around each launch, aggregated per kernel name on report.
 void trace_begin(const char *name, cudaStream_t s);
