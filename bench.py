@@ -142,6 +142,12 @@ class ClockSampler:
             threading.Thread(target=self._read, daemon=True).start()
         except OSError:
             self.proc = None
+        # nvidia-smi's start (process launch, NVML set-up) contends with the driver: wait for its first sample, at
+        # most 3 s, so it is sampling steadily before the caller's timed work begins (timed regions of a few ms read up
+        # to 1 ms slow when they overlapped its start)
+        t0 = time.perf_counter()
+        while self.proc and not self.rows and self.proc.poll() is None and time.perf_counter() - t0 < 3.0:
+            time.sleep(0.01)
         return self
 
     def _read(self):
@@ -373,7 +379,11 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
-def time_device(fn, steps, warmup, world):
+def time_device(fn, steps, warmup, world, lead_in_ms=0.0):
+    """Device time of `steps` calls of fn (CUDA events on the current stream, synchronised on both sides). lead_in_ms:
+    a fixed-length spin kernel queued just before the start event, so the host queues the timed work while the GPU
+    runs it and the events bracket device work only (a host descheduled for a few ms inside a short timed region
+    would otherwise leave the GPU idle inside it: one 20-step headline region read 0.254 ms per step against 0.114)."""
     import torch
     for k in range(warmup):
         fn(k)
@@ -382,6 +392,8 @@ def time_device(fn, steps, warmup, world):
         dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if lead_in_ms > 0:
+        torch.cuda._sleep(int(lead_in_ms * 2e6))  # about 2e6 cycles per ms at the B200's 1.97 GHz
     e0.record()
     for k in range(steps):
         fn(k)
@@ -419,24 +431,32 @@ def main():
     for k in range(max(3, args.warmup)):
         step(k)
     torch.cuda.synchronize()
-    # The timed steps replay one CUDA graph per ring slot, each holding that slot's zap_tex_cuda_bc_encode_dev call
-    # (scratch allocation, counter reset, both kernels): the device work of a step without the host's per-call launch
-    # overhead, which on a slow host exceeds the 0.14 ms of GPU work per 2048^2 encode. e2e keeps the host path.
+    # The timed steps replay CUDA graphs of zap_tex_cuda_bc_encode_dev calls (scratch allocation, counter reset, both
+    # kernels): the device work of a step without the host's per-call launch overhead, which on a slow host exceeds
+    # the 0.12 ms of GPU work per 2048^2 encode. Whole passes over the ring replay one graph of the ring's 10 steps
+    # (one launch per 1.2 ms of GPU work, so a host that stalls between launches does not starve the GPU); the
+    # K % 10 steps left over replay one graph per ring slot. e2e keeps the host path.
     graphs = []
     for k in range(ring):
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
             step(k)
         graphs.append(g)
+    ring_graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(ring_graph):
+        for k in range(ring):
+            step(k)
 
-    def graph_step(k):
-        graphs[k % ring].replay()
+    def graph_steps(n):  # n consecutive steps from ring slot 0
+        for _ in range(n // ring):
+            ring_graph.replay()
+        for k in range(n % ring):
+            graphs[k].replay()
 
-    for k in range(max(3, args.warmup)):
-        graph_step(k)
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        ms = time_device(graph_step, args.steps, 0, world)
+    with ClockSampler(local) as clocks:  # started (and sampling) before the warm-up, so it runs through the timed steps
+        graph_steps(max(3, args.warmup))
+        torch.cuda.synchronize()
+        ms = time_device(lambda k: graph_steps(args.steps), 1, 0, world, lead_in_ms=3.0)
     # per-kernel figures from a second pass of the same steps with the library's event trace on (the trace's own
     # event records stay out of the timed pass above); its launch count is the timed pass's
     zap_b200.trace(True)
@@ -485,7 +505,8 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "l2": f"inputs larger than L2: ring of {ring} distinct {W}x{H} textures",
                        "parallelism": "independent replicas" if world > 1 else "1 gpu",
-                       "step": "replay of a CUDA graph of one zap_tex_cuda_bc_encode_dev call per ring slot"},
+                       "step": "one zap_tex_cuda_bc_encode_dev call on the next ring texture; the K steps replay CUDA graphs "
+                               "of 10 consecutive steps (one pass over the ring), the K % 10 left over one graph each"},
             "roofline": roofline, "gpu_launches": launches, "clocks": clocks.summary(), "library_md5": library_md5()}
 
     if rank == 0:
@@ -812,11 +833,12 @@ def extra_workloads(args, dev, sm_mhz=None, sms=148):
         # idle GPU carries its ramp-up (4-encode segments without warm-up read ASTC 20 % slow)
         seg = max(20, steps // 5)
         with ClockSampler(torch.cuda.current_device()) as clk:
-            per = sorted(time_device(step, seg, 3, 1) / seg for _ in range(5))
+            per = sorted(time_device(step, seg, 3, 1, lead_in_ms=3.0) / seg for _ in range(5))
         ms = per[2] * steps
         mps = steps * npix / 1e6 / (ms / 1e3)
         res[name] = {"Mpix_s": mps, "ms_per_encode": ms / steps, "GB_s_algorithmic": mps * 1e6 * alg_bytes_per_px / 1e9,
-                     "timing": "median of 5 segments of %d encodes after 3 untimed ones (CUDA events)" % seg,
+                     "timing": "median of 5 segments of %d encodes after 3 untimed ones (CUDA events; the host queues each "
+                               "segment behind a 3 ms spin kernel, so the events bracket device work)" % seg,
                      "segments_ms_per_encode": per, "clocks": clk.summary()}
         if counted:  # the whole encode against the ALU roofline, once the peak is measured (main's fill_alu)
             res[name]["_alu_in"] = (counted, ms / steps)
