@@ -402,45 +402,150 @@ ZTC_DEV int palette_word(const Sub &S, uint64_t v, int k) {
 }
 
 // ---------------------------------------------------------------- BC1 / BC4 sub-blocks
-// One chain per CTA and sub-block kind. Per block the 49 candidates are groups of L lanes: groups 0-15 kind 0
-// (neighbour j = group + 1: its endpoints, fitted indices), 16-31 kind 1 (these endpoints, its indices), 32-47 kind 2
-// (the whole neighbour), 48 the base. Lane q of a group takes texels q*T .. q*T + T - 1 (T = 16 / L), and the window
-// slots at those distances minus one when the rate is counted. A last warp of its own loads the blocks ahead,
-// software-pipelined (block cur + 3 fetched into registers while block cur + 2, fetched the iteration before, is
-// stored to shared memory), so no candidate warp and no barrier waits for a global load: with the loader beside the
-// base in one warp, its loads held that warp's minimum and each block's first barrier (about 1,100 of 3,400 cycles
-// per block, measured with clock64 on B200).
-// L = 8 (13 warps) measured fastest on B200: 512x512 BC1 in one chain 24.3 ms, against 25.5 ms at L = 16 (25 warps)
-// and 27.7 ms at L = 4 (7 warps), though L = 4 issues about a quarter of L = 16's warp instructions: a block's time
-// is its critical path (loads, group reductions, rate masks, two CTA-wide minima and barriers), not the candidates'
-// arithmetic. The two sub-blocks of a BC3 or BC5 block are independent chains (each looks only at its own fields of
-// earlier blocks, with its own match distances, zap_tex.h:1494-1501), so each runs in its own CTA (blockIdx.y) and
-// writes its own 8 bytes of the blocks.
-template <int L> struct SubChain {  // kWc candidate warps, then the loader warp
-    static constexpr int T = 16 / L, kWc = (49 * L + 31) / 32, kThreads = (kWc + 1) * 32;
+// One chain per CTA and sub-block kind, in two roles. The candidates of a block that do not involve the block
+// chosen just before it (the base, and every neighbour at distance j >= 2) depend only on decisions at least two
+// blocks back, so producer warps evaluate them one block ahead: while block b - 1 is being chosen, they compute
+// block b's candidates (SSE, fields, and the match masks against window distances 2..16) into shared memory. A
+// chooser warp then decides block b alone: it evaluates the three candidates of neighbour distance 1 itself, adds
+// each other candidate's distance-1 match bit, turns the masks into rates and keys for all 49, and takes the minimum
+// of (cost, candidate order) across its lanes. One barrier per block; no CTA-wide minimum. The 49 candidates are
+// evaluated by groups of 8 lanes, lane q taking texels 2q, 2q + 1 and window distances 2q + 1, 2q + 2. Producer
+// groups: 0-15 kind 0 (neighbour j = (group & 15) + 2: its endpoints, fitted indices), 16-31 kind 1 (these
+// endpoints, its indices), 32-47 kind 2 (the whole neighbour), the last group of each kind idle (it repeats j = 16
+// and keeps nothing), 48 the base; a last warp loads the blocks ahead, software-pipelined (block b + 2 stored while
+// block b + 3 is fetched into registers), so no warp waits for a global load inside a step. The two sub-blocks of a
+// BC3 or BC5 block are independent chains (each looks only at its own fields of earlier blocks, with its own match
+// distances, zap_tex.h:1494-1501), so each runs in its own CTA (blockIdx.y) and writes its own 8 bytes of the blocks.
+// The chooser is three warps: one fits the distance-1 kind-0 candidate, one evaluates kinds 1 and 2 (the same code
+// path), and the deciding warp meanwhile turns the other 46 candidates into keys (they do not depend on the distance-1
+// results); a named barrier over the three joins them, and the deciding warp adds the three distance-1 keys and takes
+// the minimum. Phase timers (clock64, a scratch build) put the chooser's step at ~2,950 cycles per block with all
+// three roles in one warp (the fit and evaluation branches serialised, then two candidates' keys per lane).
+constexpr int kSubL = 8, kSubProducerWarps = 13, kSubFit = 13, kSubEval = 14, kSubDecide = 15, kSubLoader = 16,
+              kSubThreads = 17 * 32;
+
+struct SubCand {
+    int e;
+    uint64_t cand;
+    bool ok;
+    uint32_t mA, mB;  // bit d - 1: the field equals the window's at distance d (from distance dlo on)
 };
-#ifndef ZTC_RDO_SUB_LANES
-#define ZTC_RDO_SUB_LANES 8
-#endif
 
+// One candidate of chain block b on a group of 8 lanes (gm: the lanes that meet its collectives). kind -1: the base;
+// 0: neighbour j's endpoints with fitted indices; 1: the base's endpoints with neighbour j's indices; 2: the whole
+// neighbour j. Its window masks cover distances dlo..16 (up to b).
+__device__ __forceinline__ SubCand sub_candidate(const Sub &S, int kind, int j, int b, int q, unsigned gm, int dlo,
+                                                 const uint32_t (*s_tex)[16], const uint64_t *s_base, const int (*s_bpal)[8],
+                                                 const uint64_t *ring, const int (*ring_pal)[8]) {
+    constexpr int T = 16 / kSubL;
+    const bool bc1 = S.type == kBc1;
+    const int nA = bc1 ? 4 : 2, slot = b % 3;
+    const uint64_t maskA = (1ull << (8 * nA)) - 1ull;
+    uint32_t t[T];
+    #pragma unroll
+    for (int u = 0; u < T; u++) t[u] = s_tex[slot][q * T + u];
+    const uint64_t base = s_base[slot], nb = ring[(b - j) & (kWindow - 1)];
+    // kind 1 and the base: these endpoints (the base's palette); kinds 0 and 2: the neighbour's
+    const bool own = kind == 1 || kind == -1;
+    const int *P = own ? s_bpal[slot] : ring_pal[(b - j) & (kWindow - 1)];
+    SubCand r;
+    r.ok = kind == -1 || j <= b;
+    int e = 0;
+    if (bc1) {  // the CTA's sub-block type: uniform
+        const uint32_t a = (uint32_t)((own ? base : nb) & 0xFFFFu), c = (uint32_t)(((own ? base : nb) >> 16) & 0xFFFFu);
+        uint32_t idx;
+        if (kind == 0) {  // zap__bc1_fit: best of the 4 (3 in 3-colour order) entries, first on ties
+            const int4 pe = *(const int4 *)P, pn = *(const int4 *)(P + 4);
+            const bool n4 = S.force4 || a > c;
+            idx = 0;
+            #pragma unroll
+            for (int u = 0; u < T; u++) {
+                const uint32_t tc = t[u] & 0xFFFFFFu;
+                int bk = 0, be = pn.x - 2 * (int)dot4(tc, (uint32_t)pe.x), sk;
+                sk = pn.y - 2 * (int)dot4(tc, (uint32_t)pe.y); if (sk < be) { be = sk; bk = 1; }
+                sk = pn.z - 2 * (int)dot4(tc, (uint32_t)pe.z); if (sk < be) { be = sk; bk = 2; }
+                sk = pn.w - 2 * (int)dot4(tc, (uint32_t)pe.w); if (n4 && sk < be) { be = sk; bk = 3; }
+                e += be + (int)dot4(tc, tc);
+                idx |= (uint32_t)bk << (2 * (q * T + u));
+            }
+            e = lsum<kSubL>(e, gm);
+            idx = lor<kSubL>(idx, gm);
+        } else {  // zap__bc1_eval with the base's or the neighbour's indices
+            idx = (uint32_t)((kind == -1 ? base : nb) >> 32);
+            #pragma unroll
+            for (int u = 0; u < T; u++) {
+                const uint32_t tc = t[u] & 0xFFFFFFu;
+                const int k = (int)((idx >> (2 * (q * T + u))) & 3u);
+                e += P[4 + k] - 2 * (int)dot4(tc, (uint32_t)P[k]) + (int)dot4(tc, tc);
+            }
+            e = lsum<kSubL>(e, gm);
+        }
+        r.cand = (uint64_t)a | ((uint64_t)c << 16) | ((uint64_t)idx << 32);
+        // a 3-colour block may not use index 3 (transparent); the base is never checked
+        if (kind >= 0 && !S.force4 && a <= c && (idx & (idx >> 1) & 0x55555555u)) r.ok = false;
+    } else {
+        const int a = (int)((own ? base : nb) & 0xFFu), c = (int)(((own ? base : nb) >> 8) & 0xFFu);
+        uint64_t idx;
+        if (kind == 0) {  // zap__bc4_fit
+            const int4 p0 = *(const int4 *)P, p1 = *(const int4 *)(P + 4);
+            const int pv[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+            uint32_t part = 0;  // this lane's T 3-bit indices
+            #pragma unroll
+            for (int u = 0; u < T; u++) {
+                const int v = (int)chan(t[u], S.chan);
+                int bk = 0, be = (v - pv[0]) * (v - pv[0]);
+                #pragma unroll
+                for (int k = 1; k < 8; k++) {
+                    const int d = v - pv[k];
+                    if (d * d < be) { be = d * d; bk = k; }
+                }
+                e += be;
+                part |= (uint32_t)bk << (3 * u);
+            }
+            e = lsum<kSubL>(e, gm);
+            // lane q's indices start at bit 3 q T: two 32-bit words of the 48
+            const uint64_t mine = (uint64_t)part << (3 * q * T);
+            idx = ((uint64_t)lor<kSubL>((uint32_t)(mine >> 32), gm) << 32) | lor<kSubL>((uint32_t)mine, gm);
+        } else {  // zap__bc4_eval
+            idx = (kind == -1 ? base : nb) >> 16;
+            #pragma unroll
+            for (int u = 0; u < T; u++) {
+                const int d = (int)chan(t[u], S.chan) - P[(int)((idx >> (3 * (q * T + u))) & 7u)];
+                e += d * d;
+            }
+            e = lsum<kSubL>(e, gm);
+        }
+        r.cand = (uint64_t)a | ((uint64_t)c << 8) | (idx << 16);
+    }
+    r.e = e;
+    // rate inputs (zap__field_rate per field): which window fields equal this candidate's
+    uint32_t mA = 0, mB = 0;
+    #pragma unroll
+    for (int u = 0; u < T; u++) {
+        const int d = q * T + u + 1;
+        const uint64_t w = ring[(b - d) & (kWindow - 1)];
+        if (d >= dlo && d <= b) {
+            mA |= (uint32_t)((w & maskA) == (r.cand & maskA)) << (d - 1);
+            mB |= (uint32_t)((w >> (8 * nA)) == (r.cand >> (8 * nA))) << (d - 1);
+        }
+    }
+    r.mA = lor<kSubL>(mA, gm);
+    r.mB = lor<kSubL>(mB, gm);
+    return r;
+}
 
-template <int L>
-__global__ void __launch_bounds__(SubChain<L>::kThreads, 1) rdo_sub_chain_kernel(SrcU8 src, int bw, int nby, int chain_rows, uint8_t *__restrict__ out,
-                                                                                int bs, Sub S0, Sub S1, float lambda) {
-    constexpr int T = SubChain<L>::T, kW = SubChain<L>::kWc;
+__global__ void __launch_bounds__(kSubThreads, 1) rdo_sub_chain_kernel(SrcU8 src, int bw, int nby, int chain_rows, uint8_t *__restrict__ out,
+                                                                      int bs, Sub S0, Sub S1, float lambda) {
     __shared__ uint64_t ring[kWindow];  // the sub-block of the last 16 chosen blocks, slot = block & 15
     __shared__ __align__(16) int ring_pal[kWindow][8];  // their palettes (palette_word)
-    __shared__ __align__(16) uint32_t s_tex[3][16];  // block cur in slot cur % 3, loaded two blocks ahead
+    __shared__ __align__(16) uint32_t s_tex[3][16];  // block b in slot b % 3
     __shared__ uint64_t s_base[3];
     __shared__ __align__(16) int s_bpal[3][8];  // the base sub-block's palette
-    __shared__ uint64_t s_key[kW];
-    __shared__ int s_dist[2];
+    // the candidates of block b by candidate order (0 the base, (j - 1) * 3 + kind + 1 the others), buffer b & 1
+    __shared__ uint64_t c_cand[2][49];
+    __shared__ uint64_t c_meta[2][49];  // SSE (bit 31 set: not allowed) | mA << 32 | mB << 48
     const Sub S = blockIdx.y ? S1 : S0;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, q = tid & (L - 1), grp = tid / L;
-    const bool loader = warp == kW;
-    const int kind = loader ? -2 : grp < 16 ? 0 : grp < 32 ? 1 : grp < 48 ? 2 : grp == 48 ? -1 : -3, j = (grp & 15) + 1;
-    // the warps of groups 0-47 hold one kind each and meet every collective together; the base's group has its own
-    const unsigned gm = warp < 48 * L / 32 ? 0xFFFFFFFFu : ((L == 32 ? 0xFFFFFFFFu : (1u << L) - 1u) << (lane & ~(L - 1)));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, q = tid & (kSubL - 1), grp = tid / kSubL;
     const int row0 = blockIdx.x * chain_rows, rows = min(chain_rows, nby - row0);
     if (rows <= 0) return;
     const int first = row0 * bw, count = rows * bw;
@@ -456,138 +561,96 @@ __global__ void __launch_bounds__(SubChain<L>::kThreads, 1) rdo_sub_chain_kernel
         if (lane < 8) s_bpal[ns][lane] = palette_word(S, r_base, lane);
         if (lane == 0) s_base[ns] = r_base;
     };
-    if (loader) {
-        for (int k = 0; k < 2 && k < count; k++) { fetch(first + k); store(k); }
-        if (count > 2) fetch(first + 2);
+    if (warp == kSubLoader) {
+        fetch(first);
+        store(0);
+        if (count > 1) fetch(first + 1);
     }
-    if (tid == 0) { s_dist[0] = 1; s_dist[1] = 1; }
     __syncthreads();
-    // fields: BC1 {c0 c1, indices} = {4, 4} bytes, BC4 {a0 a1, indices} = {2, 6}
+    // producers: kind and neighbour distance of the group (the idle groups repeat j = 16), which warps hold one kind
+    const int pkind = grp < 48 ? grp >> 4 : grp == 48 ? -1 : -3, pj = min((grp & 15) + 2, 16);
+    const bool pkeep = grp < 48 ? (grp & 15) < 15 : grp == 48;
+    const unsigned pgm = warp < 12 ? 0xFFFFFFFFu : 0xFFu << (lane & 24);
+    // the chooser's fields and rates
     const bool bc1 = S.type == kBc1;
     const int nA = bc1 ? 4 : 2, nB = bc1 ? 4 : 6;
     const uint64_t maskA = (1ull << (8 * nA)) - 1ull;
     const float newA = bc1 ? 3.0f : 2.0f, newB = 3.0f;  // min(size, 3)
-    for (int cur = 0; cur < count; cur++) {
-        const int g = first + cur, slot = cur % 3, d0 = s_dist[0], d1 = s_dist[1];
-        uint64_t key = ~0ull, cand = 0;
-        int nd0 = 0, nd1 = 0;
-        if (kind >= -1) {
-            uint32_t t[T];
-            #pragma unroll
-            for (int u = 0; u < T; u++) t[u] = s_tex[slot][q * T + u];
-            const uint64_t base = s_base[slot], nb = ring[(cur - j) & (kWindow - 1)];
-            // kind 1 and the base: these endpoints (the base's palette); kinds 0 and 2: the neighbour's
-            const bool own = kind == 1 || kind == -1;
-            const int *P = own ? s_bpal[slot] : ring_pal[(cur - j) & (kWindow - 1)];
-            bool ok = kind == -1 || j <= cur;
-            int e = 0;
-            if (bc1) {  // the CTA's sub-block type: uniform
-                const uint32_t a = (uint32_t)((own ? base : nb) & 0xFFFFu), b = (uint32_t)(((own ? base : nb) >> 16) & 0xFFFFu);
-                uint32_t idx;
-                if (kind == 0) {  // zap__bc1_fit: best of the 4 (3 in 3-colour order) entries, first on ties
-                    const int4 pe = *(const int4 *)P, pn = *(const int4 *)(P + 4);
-                    const bool n4 = S.force4 || a > b;
-                    idx = 0;
-                    #pragma unroll
-                    for (int u = 0; u < T; u++) {
-                        const uint32_t tc = t[u] & 0xFFFFFFu;
-                        int bk = 0, be = pn.x - 2 * (int)dot4(tc, (uint32_t)pe.x), sk;
-                        sk = pn.y - 2 * (int)dot4(tc, (uint32_t)pe.y); if (sk < be) { be = sk; bk = 1; }
-                        sk = pn.z - 2 * (int)dot4(tc, (uint32_t)pe.z); if (sk < be) { be = sk; bk = 2; }
-                        sk = pn.w - 2 * (int)dot4(tc, (uint32_t)pe.w); if (n4 && sk < be) { be = sk; bk = 3; }
-                        e += be + (int)dot4(tc, tc);
-                        idx |= (uint32_t)bk << (2 * (q * T + u));
-                    }
-                    e = lsum<L>(e, gm);
-                    idx = lor<L>(idx, gm);
-                } else {  // zap__bc1_eval with the base's or the neighbour's indices
-                    idx = (uint32_t)((kind == -1 ? base : nb) >> 32);
-                    #pragma unroll
-                    for (int u = 0; u < T; u++) {
-                        const uint32_t tc = t[u] & 0xFFFFFFu;
-                        const int k = (int)((idx >> (2 * (q * T + u))) & 3u);
-                        e += P[4 + k] - 2 * (int)dot4(tc, (uint32_t)P[k]) + (int)dot4(tc, tc);
-                    }
-                    e = lsum<L>(e, gm);
-                }
-                cand = (uint64_t)a | ((uint64_t)b << 16) | ((uint64_t)idx << 32);
-                // a 3-colour block may not use index 3 (transparent); the base is never checked
-                if (kind >= 0 && !S.force4 && a <= b && (idx & (idx >> 1) & 0x55555555u)) ok = false;
-            } else {
-                const int a = (int)((own ? base : nb) & 0xFFu), b = (int)(((own ? base : nb) >> 8) & 0xFFu);
-                uint64_t idx;
-                if (kind == 0) {  // zap__bc4_fit
-                    const int4 p0 = *(const int4 *)P, p1 = *(const int4 *)(P + 4);
-                    const int pv[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
-                    uint32_t part = 0;  // this lane's T 3-bit indices
-                    #pragma unroll
-                    for (int u = 0; u < T; u++) {
-                        const int v = (int)chan(t[u], S.chan);
-                        int bk = 0, be = (v - pv[0]) * (v - pv[0]);
-                        #pragma unroll
-                        for (int k = 1; k < 8; k++) {
-                            const int d = v - pv[k];
-                            if (d * d < be) { be = d * d; bk = k; }
-                        }
-                        e += be;
-                        part |= (uint32_t)bk << (3 * u);
-                    }
-                    e = lsum<L>(e, gm);
-                    // lane q's indices start at bit 3 q T: two 32-bit words of the 48
-                    const uint64_t mine = (uint64_t)part << (3 * q * T);
-                    idx = ((uint64_t)lor<L>((uint32_t)(mine >> 32), gm) << 32) | lor<L>((uint32_t)mine, gm);
-                } else {  // zap__bc4_eval
-                    idx = (kind == -1 ? base : nb) >> 16;
-                    #pragma unroll
-                    for (int u = 0; u < T; u++) {
-                        const int d = (int)chan(t[u], S.chan) - P[(int)((idx >> (3 * (q * T + u))) & 7u)];
-                        e += d * d;
-                    }
-                    e = lsum<L>(e, gm);
-                }
-                cand = (uint64_t)a | ((uint64_t)b << 8) | (idx << 16);
-            }
-            // rate (zap__field_rate per field): bit d - 1 of a mask says the field equals the window's at distance d
-            uint32_t mA = 0, mB = 0;
-            #pragma unroll
-            for (int u = 0; u < T; u++) {
-                const int d = q * T + u + 1;
-                const uint64_t w = ring[(cur - d) & (kWindow - 1)];
-                if (d <= cur) {
-                    mA |= (uint32_t)((w & maskA) == (cand & maskA)) << (d - 1);
-                    mB |= (uint32_t)((w >> (8 * nA)) == (cand >> (8 * nA))) << (d - 1);
+    int d0 = 1, d1 = 1;  // the chooser's current match distances (zap_tex.h:234)
+    for (int it = -1; it < count; it++) {
+        const int b = it + 1;  // the producers' block
+        if (warp < kSubProducerWarps) {
+            if (pkind >= -1 && b < count) {
+                const SubCand c = sub_candidate(S, pkind, pj, b, q, pgm, 2, s_tex, s_base, s_bpal, ring, ring_pal);
+                if (pkeep && q == 0) {
+                    const int o = pkind < 0 ? 0 : (pj - 1) * 3 + pkind + 1;
+                    c_cand[b & 1][o] = c.cand;
+                    c_meta[b & 1][o] = (uint32_t)c.e | (c.ok ? 0u : 0x80000000u) | ((uint64_t)c.mA << 32) | ((uint64_t)c.mB << 48);
                 }
             }
-            mA = lor<L>(mA, gm);
-            mB = lor<L>(mB, gm);
-            float fa = (float)nA, fb = (float)nB;
-            nd0 = d0; nd1 = d1;
-            if (d0 > 0 && d0 <= cur && ((mA >> (d0 - 1)) & 1u)) fa = 0.0f;
-            else if (mA) { nd0 = __ffs((int)mA); fa = newA; }
-            if (d1 > 0 && d1 <= cur && ((mB >> (d1 - 1)) & 1u)) fb = 0.0f;
-            else if (mB) { nd1 = __ffs((int)mB); fb = newB; }
-            if (ok) key = key_of((float)e + lambda * (fa + fb), kind < 0 ? 0 : (j - 1) * 3 + kind + 1);
-        } else if (loader) {  // block cur + 2 (fetched the iteration before) to shared memory; fetch block cur + 3
-            if (cur + 2 < count) store((cur + 2) % 3);
-            if (cur + 3 < count) fetch(g + 3);
-        }
-        if (!loader) {
-            const uint64_t wk = warp_min_redux(key);
-            if (lane == 0) s_key[warp] = wk;
-        }
-        __syncthreads();
-        const int order = loader ? -1 : (int)(uint32_t)warp_min_redux(lane < kW ? s_key[lane] : ~0ull);
-        const int oc = order - 1, wkind = oc % 3, wgrp = order == 0 ? 48 : wkind * 16 + oc / 3;
-        if (!loader && grp == wgrp) {  // the winner enters the window, with its palette (the base's, or the neighbour's)
-            // with j = 16 the neighbour's slot is this one: each lane rewrites its own words
-            const int *P = order == 0 || wkind == 1 ? s_bpal[slot] : ring_pal[(cur - j) & (kWindow - 1)];
-            #pragma unroll
-            for (int k = q; k < 8; k += L) ring_pal[cur & (kWindow - 1)][k] = P[k];
-            if (q == 0) {
-                ring[cur & (kWindow - 1)] = cand;
-                s_dist[0] = nd0; s_dist[1] = nd1;
-                if (order != 0) *(uint64_t *)(out + (size_t)g * bs + S.off) = cand;
+        } else if (warp == kSubFit || warp == kSubEval) {
+            // the candidates of neighbour distance 1 (block it - 1, chosen in the previous step): kind 0 on the fit
+            // warp's lanes 0-7, kinds 1 and 2 on the evaluation warp's lanes 0-7 and 8-15
+            if (it >= 0) {
+                const int ck = warp == kSubFit ? 0 : 1 + (lane >> 3);
+                if (lane < (warp == kSubFit ? 8 : 16)) {
+                    const SubCand c = sub_candidate(S, ck, 1, it, q, warp == kSubFit ? 0xFFu : 0xFFFFu, 1, s_tex, s_base, s_bpal, ring, ring_pal);
+                    if (q == 0) {
+                        c_cand[it & 1][ck + 1] = c.cand;
+                        c_meta[it & 1][ck + 1] = (uint32_t)c.e | (c.ok ? 0u : 0x80000000u) | ((uint64_t)c.mA << 32) | ((uint64_t)c.mB << 48);
+                    }
+                }
+                asm volatile("bar.sync 1, 96;" ::: "memory");  // with the deciding warp
             }
+        } else if (warp == kSubDecide) {
+            if (it >= 0) {
+                const int cur = it, bi = cur & 1;
+                const uint64_t w1 = ring[(cur - 1) & (kWindow - 1)];  // the block chosen in the previous step
+                uint64_t best = ~0ull;
+                int bd0 = d0, bd1 = d1;
+                // candidate o's key (zap__field_rate per field, the window's distance-1 bits added for the candidates
+                // the producers evaluated), kept if below the lane's best
+                auto consider = [&](int o) {
+                    const uint64_t cand = c_cand[bi][o], meta = c_meta[bi][o];
+                    uint32_t mA = (uint32_t)(meta >> 32) & 0xFFFFu, mB = (uint32_t)(meta >> 48);
+                    if ((o == 0 || o > 3) && cur >= 1) {
+                        mA |= (uint32_t)((w1 & maskA) == (cand & maskA));
+                        mB |= (uint32_t)((w1 >> (8 * nA)) == (cand >> (8 * nA)));
+                    }
+                    float fa = (float)nA, fb = (float)nB;
+                    int nd0 = d0, nd1 = d1;
+                    if (d0 > 0 && d0 <= cur && ((mA >> (d0 - 1)) & 1u)) fa = 0.0f;
+                    else if (mA) { nd0 = __ffs((int)mA); fa = newA; }
+                    if (d1 > 0 && d1 <= cur && ((mB >> (d1 - 1)) & 1u)) fb = 0.0f;
+                    else if (mB) { nd1 = __ffs((int)mB); fb = newB; }
+                    const int e = (int)(uint32_t)meta;
+                    const uint64_t key = e >= 0 ? key_of((float)e + lambda * (fa + fb), o) : ~0ull;
+                    if (key < best) { best = key; bd0 = nd0; bd1 = nd1; }
+                };
+                consider(lane == 0 ? 0 : lane + 3);  // the base and orders 4..34
+                if (lane + 35 < 49) consider(lane + 35);  // orders 35..48
+                asm volatile("bar.sync 1, 96;" ::: "memory");  // the distance-1 candidates are in
+                if (lane >= 1 && lane <= 3) consider(lane);
+                const int order = (int)(uint32_t)warp_min_redux(best);
+                const int src = order <= 3 ? order : order <= 34 ? order - 3 : order - 35;  // the lane that keyed it
+                d0 = __shfl_sync(0xFFFFFFFFu, bd0, src);
+                d1 = __shfl_sync(0xFFFFFFFFu, bd1, src);
+                // the winner enters the window with its palette (the base's, or the neighbour's: with j = 16 the
+                // neighbour's slot is this one, and each lane rewrites its own word)
+                const int oc = order - 1, wkind = oc % 3, wj = oc / 3 + 1;
+                const uint64_t wc = c_cand[bi][order];
+                if (lane < 8) {
+                    const int *P = order == 0 || wkind == 1 ? s_bpal[cur % 3] : ring_pal[(cur - wj) & (kWindow - 1)];
+                    ring_pal[cur & (kWindow - 1)][lane] = P[lane];
+                }
+                if (lane == 0) {
+                    ring[cur & (kWindow - 1)] = wc;
+                    if (order != 0) *(uint64_t *)(out + (size_t)(first + cur) * bs + S.off) = wc;
+                }
+            }
+        } else {  // the loader: block it + 2 (fetched the step before) to shared memory; fetch block it + 3
+            if (it + 2 < count) store((it + 2) % 3);
+            if (it + 3 < count) fetch(first + it + 3);
         }
         __syncthreads();
     }
@@ -621,8 +684,7 @@ cudaError_t ztc_launch_rdo(int fmt, const ztc::SrcU8 &src, uint8_t *out, float l
         const int ns = ztc::sub_count(fmt), bs = fmt == ZTC_FMT_BC1 || fmt == ZTC_FMT_BC4 ? 8 : 16;
         const dim3 grid(chains, ns);
         if (fmt < ZTC_FMT_BC1 || fmt > ZTC_FMT_BC5) return cudaErrorInvalidValue;
-        constexpr int L = ZTC_RDO_SUB_LANES;
-        ztc::rdo_sub_chain_kernel<L><<<grid, ztc::SubChain<L>::kThreads, 0, stream>>>(src, bw, nby, band_rows, out, bs, S0, S1, lambda);
+        ztc::rdo_sub_chain_kernel<<<grid, ztc::kSubThreads, 0, stream>>>(src, bw, nby, band_rows, out, bs, S0, S1, lambda);
         return cudaGetLastError();
     }
 }
