@@ -369,7 +369,8 @@ def run_reference(args, world, rank):
         ref.bc_encode(img, 4, threads=threads)
     dt = time.perf_counter() - t0
     v = args.steps * W * H / 1e6 / dt
-    line = {"metric": METRIC, "value": v, "unit": "Mpix/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+    # n_gpus: the N this arm was launched with (rank 0 alone runs it, on the host's cores)
+    line = {"metric": METRIC, "value": v, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "parallelism": f"{threads} host threads, 8-block-row bands"},
