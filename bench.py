@@ -829,18 +829,25 @@ def extra_workloads(args, dev, sm_mhz=None, sms=148):
             outs[k % ring] = f(texs[k % ring], outs[k % ring])
         for k in range(ring):  # allocates every output before the timed region
             step(k)
-        # the median of five timed segments, each after 3 untimed encodes: one host-side stall (tens of ms) inside a
-        # single short window would otherwise dominate these few-millisecond figures, and a segment that starts on an
-        # idle GPU carries its ramp-up (4-encode segments without warm-up read ASTC 20 % slow)
+        # A segment is `seg` consecutive encodes over the ring, captured once as a CUDA graph, so a timed segment is
+        # one launch queued behind a 3 ms spin kernel and the events bracket device work: encodes issued one by one
+        # left the GPU idle whenever the host stalled (one run's ASTC segments read 0.24 to 2.6 ms per encode). The
+        # median of five segments, each after one untimed replay (a segment that starts on an idle GPU carries its
+        # ramp-up).
         seg = max(20, steps // 5)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            for k in range(seg):
+                step(k)
         with ClockSampler(torch.cuda.current_device()) as clk:
-            per = sorted(time_device(step, seg, 3, 1, lead_in_ms=3.0) / seg for _ in range(5))
+            per = sorted(time_device(lambda k: graph.replay(), 1, 1, 1, lead_in_ms=3.0) / seg for _ in range(5))
         ms = per[2] * steps
         mps = steps * npix / 1e6 / (ms / 1e3)
         res[name] = {"Mpix_s": mps, "ms_per_encode": ms / steps, "GB_s_algorithmic": mps * 1e6 * alg_bytes_per_px / 1e9,
-                     "timing": "median of 5 segments of %d encodes after 3 untimed ones (CUDA events; the host queues each "
-                               "segment behind a 3 ms spin kernel, so the events bracket device work)" % seg,
+                     "timing": "median of 5 segments of %d encodes (one CUDA graph over the ring, replayed once untimed "
+                               "before each timed replay; CUDA events, the replay queued behind a 3 ms spin kernel)" % seg,
                      "segments_ms_per_encode": per, "clocks": clk.summary()}
+        del graph
         if counted:  # the whole encode against the ALU roofline, once the peak is measured (main's fill_alu)
             res[name]["_alu_in"] = (counted, ms / steps)
         torch.cuda.synchronize()
