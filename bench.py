@@ -579,12 +579,59 @@ def main():
             line["batched"] = batched_workload(args, dev)
             line["refine"] = refine_workload(args, dev)
             line["rdo"] = rdo_workload(dev)
+            line["hbm_kernels"] = hbm_workloads(dev)
         fill_alu(line.get("extra"))
         line["alu_peak"] = ALU_PEAK
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def hbm_workloads(dev, side=4096, ring=4):
+    """The HBM-bound kernels against the HBM roofline: one mip level of a side^2 RGBA8 texture (linear and sRGB
+    averaging) and the BC1 / BC7 decoders of side^2 textures, over rings of `ring` distinct textures (256 MB of source
+    texels, twice the L2). Algorithmic bytes: a mip level reads its source and writes a quarter of it; a decode reads
+    the blocks and writes the texels. Timed like the secondary figures: one captured CUDA graph per segment of `ring`
+    steps, queued behind a 3 ms spin kernel, median of five segments."""
+    import torch
+
+    import zap_b200
+    import zap_b200.synth as S
+    hbm, peak_kind = peaks()
+    texs = [S.colour_texture(side, side, seed=60000 + k, alpha="noise", device=dev) for k in range(ring)]
+    res = {"peak_GB_s": hbm, "peak_source": peak_kind, "texture": f"{side}x{side} RGBA8, ring of {ring}"}
+
+    def measure(name, step, alg_bytes):
+        for k in range(ring):  # every output allocated before the capture
+            step(k)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            for k in range(ring):
+                step(k)
+        per = sorted(time_device(lambda k: g.replay(), 1, 1, 1, lead_in_ms=3.0) / ring for _ in range(5))
+        gbs = alg_bytes / (per[2] / 1e3) / 1e9
+        res[name] = {"ms_per_step": per[2], "GB_s_algorithmic": gbs, "frac_of_peak": gbs / hbm, "alg_bytes_per_step": alg_bytes,
+                     "segments_ms_per_step": per}
+        del g
+
+    half = side // 2
+    for srgb in (0, 1):
+        mips = [torch.empty((half, half, 4), dtype=torch.uint8, device=dev) for _ in range(ring)]
+        measure("mip_next_srgb" if srgb else "mip_next_linear",
+                lambda k, srgb=srgb, mips=mips: zap_b200.mip_next_dev(texs[k], srgb, out=mips[k]), side * side * 4 + half * half * 4)
+        del mips
+    for fmt, name, bs in ((zap_b200.BC1, "bc1_decode", 8), (zap_b200.BC7, "bc7_decode", 16)):
+        blocks = [zap_b200.bc_encode_dev(t, fmt) for t in texs]
+        outs = [None] * ring
+
+        def dec(k, blocks=blocks, outs=outs, fmt=fmt):
+            outs[k] = zap_b200.bc_decode_dev(blocks[k], side, side, fmt)
+        measure(name, dec, (side // 4) * (side // 4) * bs + side * side * 4)
+        del blocks, outs
+    del texs
+    torch.cuda.empty_cache()
+    return res
 
 
 def batched_workload(args, dev, n=4096):

@@ -13,6 +13,7 @@
 #include <cstddef>
 
 #include "ztc_common.cuh"
+#include "ztc_decode.cuh"
 #include "ztc_internal.h"
 #include "ztc_pca.cuh"
 
@@ -855,15 +856,8 @@ __global__ void __launch_bounds__(128) astc_decode_kernel(const uint8_t *__restr
     const uint32_t wd[4] = {q.x, q.y, q.z, q.w};
     uint32_t px[16];
     astc_decode_block(wd, px);
-    const int bx = (int)(b % bw), by = (int)(b / bw);
-    #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        const int x = bx * 4 + (i & 3), y = by * 4 + (i >> 2);
-        if (x < w && y < h) {
-            uint8_t *p = out + (size_t)y * stride + (size_t)x * 4;
-            p[0] = (uint8_t)px[i]; p[1] = (uint8_t)(px[i] >> 8); p[2] = (uint8_t)(px[i] >> 16); p[3] = (uint8_t)(px[i] >> 24);
-        }
-    }
+    const bool vec = (((uintptr_t)out | stride) & 15u) == 0, aligned4 = (((uintptr_t)out | stride) & 3u) == 0;
+    dec::store_block_rgba8(out, stride, w, h, (int)(b % bw), (int)(b / bw), px, vec, aligned4);
 }
 
 }  // namespace ztc

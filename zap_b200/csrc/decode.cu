@@ -17,14 +17,8 @@ __global__ void __launch_bounds__(128) bcn_decode_kernel(int fmt, const uint8_t 
     if (b >= nblocks) return;
     uint32_t px[16];
     dec::bcn_block(fmt, bc + (size_t)b * ((fmt == 0 || fmt == 2) ? 8 : 16), px);
-    const int bx = b % bw, by = b / bw;
-    for (int i = 0; i < 16; i++) {
-        int x = bx * 4 + (i & 3), y = by * 4 + (i >> 2);
-        if (x < w && y < h) {
-            uint8_t *p = out + (size_t)y * stride + (size_t)x * 4;
-            p[0] = (uint8_t)px[i]; p[1] = (uint8_t)(px[i] >> 8); p[2] = (uint8_t)(px[i] >> 16); p[3] = (uint8_t)(px[i] >> 24);
-        }
-    }
+    const bool vec = (((uintptr_t)out | stride) & 15u) == 0, aligned4 = (((uintptr_t)out | stride) & 3u) == 0;
+    dec::store_block_rgba8(out, stride, w, h, b % bw, b / bw, px, vec, aligned4);
 }
 
 __global__ void __launch_bounds__(128) bc6h_decode_kernel(const uint8_t *__restrict__ bc, int w, int h, uint16_t *__restrict__ out, size_t stride) {
@@ -36,10 +30,26 @@ __global__ void __launch_bounds__(128) bc6h_decode_kernel(const uint8_t *__restr
     uint16_t px[16][4];
     dec::bc6h_block(wd, px);
     const int bx = b % bw, by = b / bw;
-    for (int i = 0; i < 16; i++) {
-        int x = bx * 4 + (i & 3), y = by * 4 + (i >> 2);
-        if (x < w && y < h)
-            for (int c = 0; c < 4; c++) out[(size_t)y * stride + (size_t)x * 4 + c] = px[i][c];
+    // a row of four texels inside the image as two 16-byte stores when the image and its pitch (stride halves) are
+    // 16-byte aligned; else element by element
+    const bool vec = ((uintptr_t)out & 15u) == 0 && (stride & 7u) == 0;
+    #pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int y = by * 4 + r, x0 = bx * 4;
+        if (y >= h) break;
+        uint16_t *row = out + (size_t)y * stride + (size_t)x0 * 4;
+        if (vec && x0 + 3 < w) {
+            uint32_t q[8];
+            #pragma unroll
+            for (int k = 0; k < 8; k++) q[k] = (uint32_t)px[4 * r + (k >> 1)][2 * (k & 1)] | ((uint32_t)px[4 * r + (k >> 1)][2 * (k & 1) + 1] << 16);
+            ((uint4 *)row)[0] = make_uint4(q[0], q[1], q[2], q[3]);
+            ((uint4 *)row)[1] = make_uint4(q[4], q[5], q[6], q[7]);
+            continue;
+        }
+        for (int c = 0; c < 4; c++) {
+            if (x0 + c >= w) break;
+            for (int k = 0; k < 4; k++) row[4 * c + k] = px[4 * r + c][k];
+        }
     }
 }
 

@@ -192,6 +192,30 @@ ZTC_DEV void bc4_block(uint2 v, uint8_t out[16]) {
 }
 
 // one block of format fmt (0..4) to 16 RGBA8 texels (zap_tex.h:1526-1547)
+// A decoded 4x4 block of RGBA8 texels (px[i]: texel i, R in the low byte) into an image: each row of four texels
+// inside the image as one 16-byte store when vec (the image and its pitch 16-byte aligned), texels past the right
+// or bottom edge left out, a row the right edge cuts texel by texel (4-byte stores if aligned4, else bytes).
+ZTC_DEV void store_block_rgba8(uint8_t *out, size_t stride, int w, int h, int bx, int by, const uint32_t px[16], bool vec,
+                               bool aligned4) {
+    #pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int y = by * 4 + r, x0 = bx * 4;
+        if (y >= h) break;
+        uint8_t *row = out + (size_t)y * stride + (size_t)x0 * 4;
+        if (vec && x0 + 3 < w) {
+            *(uint4 *)row = make_uint4(px[4 * r], px[4 * r + 1], px[4 * r + 2], px[4 * r + 3]);
+            continue;
+        }
+        #pragma unroll
+        for (int c = 0; c < 4; c++) {
+            if (x0 + c >= w) break;
+            const uint32_t v = px[4 * r + c];
+            if (aligned4) *(uint32_t *)(row + 4 * c) = v;
+            else { row[4 * c] = (uint8_t)v; row[4 * c + 1] = (uint8_t)(v >> 8); row[4 * c + 2] = (uint8_t)(v >> 16); row[4 * c + 3] = (uint8_t)(v >> 24); }
+        }
+    }
+}
+
 ZTC_DEV void bcn_block(int fmt, const uint8_t *b, uint32_t out[16]) {
     if (fmt == 0) { bc1_block(*(const uint2 *)b, false, out); return; }
     if (fmt == 4) {
