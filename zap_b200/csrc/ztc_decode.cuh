@@ -145,6 +145,21 @@ ZTC_DEV bool bc7_parse(const uint32_t w[4], Bc7Fields &F) {
 
 // full BC7 decode, all 8 modes; reserved mode -> transparent black (zap_tex.h:378-417)
 ZTC_DEV void bc7_block(const uint32_t w[4], uint32_t out[16]) {
+    if ((w[0] & 0x7Fu) == 0x40u) {  // mode 6, the encoder's common case, straight from its fixed layout
+        // R0 R1 G0 G1 B0 B1 A0 A1 (7 bits each) from bit 7, p-bits at 63 and 64, indices from bit 65 (texel 0: 3 bits)
+        const uint64_t lo = w[0] | ((uint64_t)w[1] << 32), hi = w[2] | ((uint64_t)w[3] << 32);
+        const int p0 = (int)(lo >> 63), p1 = (int)(hi & 1u);
+        int x0[4], x1[4];
+        #pragma unroll
+        for (int c = 0; c < 4; c++) {
+            x0[c] = (int)(((lo >> (7 + 14 * c)) & 0x7Fu) << 1) | p0;
+            x1[c] = (int)(((lo >> (14 + 14 * c)) & 0x7Fu) << 1) | p1;
+        }
+        const Lerp4 row(x0, x1);
+        #pragma unroll
+        for (int i = 0; i < 16; i++) out[i] = row.at(w4(i == 0 ? (int)((hi >> 1) & 7u) : (int)((hi >> (4 * i)) & 15u)));
+        return;
+    }
     Bc7Fields F;
     if (!bc7_parse(w, F)) {
         for (int i = 0; i < 16; i++) out[i] = 0;
