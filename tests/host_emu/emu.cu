@@ -52,17 +52,19 @@ __attribute__((visibility("default"))) int emu_bc6h_encode(const float *img, int
     int bw = (w + 3) / 4, bh = (h + 3) / 4;
     for (int by = 0; by < bh; by++)
         for (int bx = 0; bx < bw; bx++) {
-            uint16_t t[48];
+            int16_t t[48];
             float U[48];
             for (int i = 0; i < 16; i++) {
                 int x = std::min(bx * 4 + (i & 3), w - 1), y = std::min(by * 4 + (i >> 2), h - 1);
                 for (int c = 0; c < 3; c++) {
                     uint32_t hb = f2h_unsigned(img[(size_t)y * stride + (size_t)x * 4 + c]);
-                    t[3 * i + c] = (uint16_t)hb;
+                    t[3 * i + c] = (int16_t)hb;
                     U[3 * i + c] = (float)hb * 64.0f / 31.0f;
                 }
             }
-            uint4 v = bc6h_encode_block(HalfRef{t, U, 1});
+            uint32_t ts;
+            const uint64_t cw = bc6_center(t, 1, ts);
+            uint4 v = bc6h_encode_block(HalfRef{t, U, 1, cw, ts});
             memcpy(out + ((size_t)by * bw + bx) * 16, &v, 16);
         }
     return 0;
@@ -173,7 +175,26 @@ __attribute__((visibility("default"))) uint64_t emu_div255_mismatches(uint64_t l
     return bad;
 }
 
-// (x, n) pairs, x an integer in [0, 2^24) and n in [1, 16], for which ztc::div_small(x, n, 1 / n) differs bitwise from
+// floats u with bit patterns in [lo, hi) for which ztc::bc6_nearest(u) differs from the reference's rule as written
+// (zap_tex.h:841-851): g truncated as x86 does, candidates g - 1, g, g + 1 clamped, the first of least distance
+__attribute__((visibility("default"))) uint64_t emu_bc6_nearest_mismatches(uint64_t lo, uint64_t hi) {
+    uint64_t bad = 0;
+    for (uint64_t b = lo; b < hi; b++) {
+        const float u = u_as_f((uint32_t)b);
+        const int g = f2i_x86((u - 32.0f) / 64.0f + 0.5f);
+        int best = 0;
+        float bd = 1e30f;
+        for (int k = 0; k < 3; k++) {
+            const int e = clampi(around(g, k), 0, 1023);
+            const float d = std::fabs((float)bc6_unq(e) - u);
+            if (d < bd) { bd = d; best = e; }
+        }
+        if (bc6_nearest(u) != best) bad++;
+    }
+    return bad;
+}
+
+// (x, n) pairs, x an integer in [0, 2^24) and the given n, for which ztc::div_small(x, n, 1 / n) differs bitwise from
 // the division x / n
 __attribute__((visibility("default"))) uint64_t emu_div_small_mismatches(int n) {
     volatile float dv = (float)n;  // a runtime divisor: the host compiler emits true divisions

@@ -38,6 +38,8 @@ def emu():
     lib.emu_mip_next.argtypes = [vp, i, i, sz, i, vp, sz]
     lib.emu_div255_mismatches.argtypes = [C.c_uint64, C.c_uint64]
     lib.emu_div255_mismatches.restype = C.c_uint64
+    lib.emu_bc6_nearest_mismatches.argtypes = [C.c_uint64, C.c_uint64]
+    lib.emu_bc6_nearest_mismatches.restype = C.c_uint64
     lib.emu_div_small_mismatches.argtypes = [i]
     lib.emu_div_small_mismatches.restype = C.c_uint64
     lib.emu_srgb_search_mismatches.argtypes = [C.c_uint64, C.c_uint64]
@@ -142,12 +144,24 @@ def test_div255_equals_division_for_every_float(emu):
     assert bad == 0
 
 
+def test_bc6h_nearest_endpoint_for_every_float(emu):
+    """BC6H's nearest 10-bit endpoint clamps its guess before truncating it without a conversion; it must pick the
+    reference's endpoint for all 2^32 bit patterns of the pre-finish value, NaN, infinities and negatives included."""
+    from concurrent.futures import ThreadPoolExecutor
+    chunks = 64
+    step = (1 << 32) // chunks
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        bad = sum(ex.map(lambda k: emu.emu_bc6_nearest_mismatches(k * step, (k + 1) * step), range(chunks)))
+    assert bad == 0
+
+
 def test_small_divisor_division_equals_ieee_on_its_domain(emu):
-    """The partition scores and subset means divide integer-valued floats below 2^24 by counts 1..16 with the same
-    FMA correction; every such pair must give the IEEE quotient bit for bit."""
+    """The partition scores and subset means divide integer-valued floats below 2^24 by counts 1..16, and the BC6H
+    texel load divides 64 h (h a half's bits) by 31, with the same FMA correction; every such pair must give the IEEE
+    quotient bit for bit."""
     from concurrent.futures import ThreadPoolExecutor
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
-        bad = sum(ex.map(emu.emu_div_small_mismatches, range(1, 17)))
+        bad = sum(ex.map(emu.emu_div_small_mismatches, list(range(1, 17)) + [31]))
     assert bad == 0
 
 

@@ -80,6 +80,7 @@ namespace ztc {
 ZTC_DEV uint32_t dot4(uint32_t a, uint32_t b) { return __dp4a(a, b, 0u); }  // sum of byte products (exact, unsigned)
 ZTC_DEV int popc(uint32_t v) { return __popc(v); }
 ZTC_DEV uint32_t f_as_u(float f) { return __float_as_uint(f); }
+ZTC_DEV float u_as_f(uint32_t u) { return __uint_as_float(u); }
 ZTC_DEV uint32_t brev(uint32_t v) { return __brev(v); }
 ZTC_DEV int trunc_i(float f) { return __float2int_rz(f); }
 ZTC_DEV float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
@@ -92,6 +93,7 @@ inline uint32_t dot4(uint32_t a, uint32_t b) {
 }
 inline int popc(uint32_t v) { return __builtin_popcount(v); }
 inline uint32_t f_as_u(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+inline float u_as_f(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
 inline uint32_t brev(uint32_t v) { uint32_t r = 0; for (int k = 0; k < 32; k++) r |= ((v >> k) & 1u) << (31 - k); return r; }
 inline int trunc_i(float f) { return (int)f; }  // only called on in-range values
 inline float fma_rn(float a, float b, float c) { return std::fmaf(a, b, c); }
@@ -108,6 +110,18 @@ ZTC_DEV int f2i_x86(float f) {
 // the clamped value (the BC6H endpoint unquantiser) was observed to produce wrong results on the device (a
 // mid-range value took the == 1023 branch); the host build and this form are correct.
 ZTC_DEV int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
+// an integer in [0, 2^23) as a float, exactly: 2^23 + n has n as its mantissa bits, and subtracting 2^23 is exact
+// (one logic op and one add instead of a conversion, which issues at a quarter of the rate)
+ZTC_DEV float small_u2f(uint32_t n) { return u_as_f(0x4B000000u | n) - 8388608.0f; }
+// (int)v for v in [0, 2^23): v + 2^23 rounded toward zero holds floor(v) in its mantissa bits (an add instead of a
+// conversion)
+ZTC_DEV int trunc_small(float v) {
+#ifdef __CUDA_ARCH__
+    return (int)(__float_as_uint(__fadd_rz(v, 8388608.0f)) & 0x7FFFFFu);
+#else
+    return (int)v;
+#endif
+}
 ZTC_DEV float clamp255(float v) { return v < 0.0f ? 0.0f : v > 255.0f ? 255.0f : v; }  // NaN passes through
 // x / 255 correctly rounded, without a division instruction sequence: Markstein's method (P. Markstein,
 // "Computation of elementary functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990):
@@ -120,8 +134,8 @@ ZTC_DEV float div255(float x) {
     const float q = x * kInv;
     return fma_rn(fma_rn(-255.0f, q, x), kInv, q);
 }
-// x / n for an integer-valued x in [0, 2^24) and an integer n in [1, 16], from ni = RN(1/n): the same correction as
-// div255, exact on that whole domain (the host test enumerates it). The callers' operands are texel channel values
+// x / n for an integer-valued x in [0, 2^24) and an integer n in [1, 16] or n = 31, from ni = RN(1/n): the same
+// correction as div255, exact on that whole domain (the host test enumerates it). The callers' operands are texel channel values
 // or products of two sums of at most 16 of them (at most 4080^2 < 2^24), all exact integers in float.
 ZTC_DEV float div_small(float x, float n, float ni) {
     const float q = x * ni;
