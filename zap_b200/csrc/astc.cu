@@ -441,8 +441,8 @@ ZTC_DEV int astc_try(TexRef ts, const AstcSmem &S, int cfg, int nc, uint32_t pm,
 ZTC_DEV int astc_single_block(const uint32_t t[16], TexRef ts, const AstcSmem &S, bool opaque, int &bc, uint32_t bcodes[4],
                               uint32_t bwt[4]) {
     float lo[1][4], hi[1][4];
-    if (opaque) pca_endpoints<3>(t, 0xFFFFu, lo[0], hi[0]);
-    else pca_endpoints<4>(t, 0xFFFFu, lo[0], hi[0]);
+    if (opaque) pca_endpoints<3, 16, false>(t, 0xFFFFu, lo[0], hi[0]);
+    else pca_endpoints<4, 16, false>(t, 0xFFFFu, lo[0], hi[0]);
     int best = 1 << 30;
     bc = 0;
     #pragma unroll 1
@@ -487,8 +487,8 @@ __device__ __forceinline__ int astc_single_cta(bool valid, const uint32_t t[16],
     float lo[1][4], hi[1][4];
     if (valid) {  // principal axis in rolled loops over the block's column of s_tex
         const TexRef own{&s_tex[0][tid], CTA};
-        if (opaque) pca_endpoints<3, 1>(own, 0xFFFFu, lo[0], hi[0]);
-        else pca_endpoints<4, 1>(own, 0xFFFFu, lo[0], hi[0]);
+        if (opaque) pca_endpoints<3, 1, false>(own, 0xFFFFu, lo[0], hi[0]);
+        else pca_endpoints<4, 1, false>(own, 0xFFFFu, lo[0], hi[0]);
         s_opq[tid] = opaque;
     }
     unsigned mores = 0;  // bit k: trial k's third fit would run
@@ -761,7 +761,7 @@ __global__ void __launch_bounds__(128) astc_two_part_kernel(SrcU8 src, int bw, i
             for (int k = 0; k < 2; k++) {
                 uint32_t m = k ? pm : (~pm & 0xFFFFu);
                 if (!m) m = 1u;  // empty partition: the reference fits texel 0
-                pca_endpoints<3>(t, m, lo[k], hi[k]);
+                pca_endpoints<3, 16, false>(t, m, lo[k], hi[k]);
             }
             e = astc_try<8, 2>(TexRef{gtex, 1}, S, cfg, 3, pm, lo, hi, codes, wt);
         }

@@ -115,11 +115,11 @@ ZTC_DEV int subset_passes(TexRef ts, uint32_t mask, int n, bool shared_p, float 
             #pragma unroll 1
             for (int i = 0; i < 16; i++) {
                 if (!((mask >> i) & 1u)) continue;
-                float w = (float)wbits(IB, (int)((idx >> (4 * i)) & 15u)) / 64.0f, u = 1.0f - w;
+                float w = small_u2f((uint32_t)wbits(IB, (int)((idx >> (4 * i)) & 15u))) / 64.0f, u = 1.0f - w;
                 aa = aa + u * u; ab = ab + u * w; bb = bb + w * w;
                 const uint32_t x = ts[i];
                 #pragma unroll
-                for (int c = 0; c < NC; c++) { float xc = (float)chan(x, c); sa[c] = sa[c] + u * xc; sb[c] = sb[c] + w * xc; }
+                for (int c = 0; c < NC; c++) { float xc = small_u2f(chan(x, c)); sa[c] = sa[c] + u * xc; sb[c] = sb[c] + w * xc; }
             }
             float det = aa * bb - ab * ab;
             if (det < 1e-6f && det > -1e-6f) return err;
@@ -317,11 +317,16 @@ ZTC_DEV void m5_quant(const float v[3], int nc, int n, int q[3], int x8[3]) {
     #pragma unroll
     for (int c = 0; c < 3; c++) {
         if (c >= nc || (KIND == kPartAlpha && c > 0)) { q[c] = 0; x8[c] = 0; continue; }
-        int g = f2i_x86(div255(v[c] * (float)top) + 0.5f), bq = 0, bd = 1 << 30;
+        // finite v within [-510, 765] (clamped least-squares endpoints, or the starts), as for quant_pbit
+        const float gv = div255(v[c] * (float)top) + 0.5f;
+        ZTC_TRUNC_DOMAIN(gv);
+        int g = trunc_mid(gv), bq = 0, bd = 1 << 30;
         #pragma unroll
         for (int k = 0; k < 3; k++) {
             int tq = clampi(around(g, k), 0, top);
-            int d = f2i_x86(fabsf((float)expand_bits(tq, n) - v[c]));
+            const float dv = fabsf(small_u2f((uint32_t)expand_bits(tq, n)) - v[c]);
+            ZTC_TRUNC_DOMAIN(dv);
+            int d = trunc_small(dv);
             if (d < bd) { bd = d; bq = tq; }
         }
         q[c] = bq; x8[c] = expand_bits(bq, n);
@@ -368,13 +373,14 @@ ZTC_DEV bool m5_lsq(const uint32_t p[16], int nc, uint32_t idx, float lo[3], flo
         #pragma unroll
         for (int c = 0; c < kC; c++) { const int x = (int)chan(p[i], c); sa[c] += u * x; sb[c] += k * x; }
     }
-    const float faa = (float)aa * (1.0f / 4096.0f), fab = (float)ab * (1.0f / 4096.0f), fbb = (float)bb * (1.0f / 4096.0f);
+    const float faa = small_u2f((uint32_t)aa) * (1.0f / 4096.0f), fab = small_u2f((uint32_t)ab) * (1.0f / 4096.0f),
+                fbb = small_u2f((uint32_t)bb) * (1.0f / 4096.0f);  // sums below 2^17
     float det = faa * fbb - fab * fab;
     if (det < 1e-6f && det > -1e-6f) return false;
     #pragma unroll
     for (int c = 0; c < kC; c++)
         if (c < nc) {
-            const float fa = (float)sa[c] * (1.0f / 64.0f), fb = (float)sb[c] * (1.0f / 64.0f);
+            const float fa = small_u2f((uint32_t)sa[c]) * (1.0f / 64.0f), fb = small_u2f((uint32_t)sb[c]) * (1.0f / 64.0f);  // below 2^18
             lo[c] = clamp255((fa * fbb - fb * fab) / det); hi[c] = clamp255((fb * faa - fa * fab) / det);
         }
     return true;
@@ -416,7 +422,7 @@ ZTC_DEV float partition_score(const float s1[9], int n1, const float tot[9]) {
         float m[9];
         #pragma unroll
         for (int j = 0; j < 9; j++) m[j] = k ? s1[j] : tot[j] - s1[j];
-        float n = (float)(k ? n1 : 16 - n1);
+        float n = small_u2f((uint32_t)(k ? n1 : 16 - n1));
         if (n < 2) continue;
         const float ni = 1.0f / n;  // the six quotients below: integer-valued numerators below 2^24 (div_small)
         float S00 = m[3] - div_small(m[0] * m[0], n, ni), S01 = m[6] - div_small(m[0] * m[1], n, ni);
@@ -482,7 +488,7 @@ __device__ __forceinline__ bool bc7_group_mode1(const uint32_t t[16], TexRef ts,
         #pragma unroll 1
         for (int i = 0; i < 16; i++) {
             const uint32_t x = ts[i];
-            const float rr = (float)chan(x, 0), gg = (float)chan(x, 1), bb = (float)chan(x, 2);
+            const float rr = small_u2f(chan(x, 0)), gg = small_u2f(chan(x, 1)), bb = small_u2f(chan(x, 2));
             const float mo[9] = {rr, gg, bb, rr * rr, gg * gg, bb * bb, rr * gg, rr * bb, gg * bb};
             #pragma unroll
             for (int j = 0; j < 9; j++) tot[j] = tot[j] + mo[j];
@@ -664,7 +670,7 @@ __device__ __forceinline__ int m5_alpha_lane(TexRef ts, int rot, uint32_t &qw, u
     #pragma unroll
     for (int i = 0; i < 16; i++) {  // the alpha part's texels; it starts from their range
         r[i] = rotate_texel(ts[i], rot) >> 24;
-        const float a = (float)r[i];
+        const float a = small_u2f(r[i]);
         if (a < lo5[0]) lo5[0] = a;
         if (a > hi5[0]) hi5[0] = a;
     }

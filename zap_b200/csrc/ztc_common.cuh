@@ -57,7 +57,8 @@
 // (site << 24) | (i & 0xFFFFFF), keeping the first one, and the caller skips the access; no kernel traps or waits.
 // zap_tex_cuda_debug_checks reads and clears the word. In the product build every check compiles to `true`.
 // Sites: 1 texel gather, 2 BC7 mode-6 refit list, 3 BC1 climb list, 4 BC6H refit list, 5 ASTC fit list (shared
-// memory), 6 BC7 work list, 7 ASTC work list (global memory), 8 a compacted list's owner (shared memory index).
+// memory), 6 BC7 work list, 7 ASTC work list (global memory), 8 a compacted list's owner (shared memory index),
+// 9 a conversion-free truncation's argument outside the domain its caller proves (ZTC_TRUNC_DOMAIN; i = 0).
 #ifdef ZTC_CHECKS
 extern __device__ unsigned int ztc_check_word;
 namespace ztc {
@@ -70,8 +71,10 @@ ZTC_DEV bool in_bounds(long long i, long long n, unsigned site) {
 }
 }  // namespace ztc
 #define ZTC_IN_BOUNDS(i, n, site) ::ztc::in_bounds((long long)(i), (long long)(n), (site))
+#define ZTC_TRUNC_DOMAIN(x) ((void)::ztc::in_bounds(fabsf(x) < 4194304.0f ? 0 : -1, 1, 9))
 #else
 #define ZTC_IN_BOUNDS(i, n, site) true
+#define ZTC_TRUNC_DOMAIN(x) ((void)0)
 #endif
 
 namespace ztc {
@@ -118,6 +121,15 @@ ZTC_DEV float small_u2f(uint32_t n) { return u_as_f(0x4B000000u | n) - 8388608.0
 ZTC_DEV int trunc_small(float v) {
 #ifdef __CUDA_ARCH__
     return (int)(__float_as_uint(__fadd_rz(v, 8388608.0f)) & 0x7FFFFFu);
+#else
+    return (int)v;
+#endif
+}
+// (int)v, truncation toward zero, for |v| < 2^23 (f2i_x86 on that domain), without a conversion
+ZTC_DEV int trunc_mid(float v) {
+#ifdef __CUDA_ARCH__
+    const int m = (int)(__float_as_uint(__fadd_rz(fabsf(v), 8388608.0f)) & 0x7FFFFFu);
+    return v < 0.0f ? -m : m;
 #else
     return (int)v;
 #endif
@@ -169,18 +181,24 @@ struct Lerp4 {
 };
 ZTC_DEV int expand_bits(int v, int n) { v <<= 8 - n; return v | (v >> n); }  // n-bit -> 8-bit replication
 
-// endpoint quantisation with a fixed p-bit (zap_tex.h:426-438); q: stored values, x8: expanded 8-bit values
+// endpoint quantisation with a fixed p-bit (zap_tex.h:426-438); q: stored values, x8: expanded 8-bit values. The
+// endpoints v are finite and within [-510, 765]: least-squares ones are clamped to [0, 255], and a principal-axis
+// start is the mean (in the cube) plus an offset no longer than a texel's distance from it (at most 255 * 2).
+// So the guess lies in (-256, 384) and d * d below 2^20, where the conversion-free truncations equal f2i_x86.
 template <int NC>
 ZTC_DEV int quant_pbit(const float v[4], int n, int p, int q[4], int x8[4]) {
     int err = 0, top = (1 << (n - 1)) - 1;
     #pragma unroll
     for (int c = 0; c < NC; c++) {
-        int g = f2i_x86((div255(v[c]) * (float)((1 << n) - 1) - (float)p) / 2.0f + 0.5f), bq = 0, be = 1 << 30;
+        const float gv = (div255(v[c]) * (float)((1 << n) - 1) - (float)p) / 2.0f + 0.5f;
+        ZTC_TRUNC_DOMAIN(gv);
+        int g = trunc_mid(gv), bq = 0, be = 1 << 30;
         #pragma unroll
         for (int k = 0; k < 3; k++) {
             int tq = clampi(around(g, k), 0, top);
-            float d = (float)expand_bits((tq << 1) | p, n) - v[c];
-            int e = f2i_x86(d * d);
+            float d = small_u2f((uint32_t)expand_bits((tq << 1) | p, n)) - v[c];
+            ZTC_TRUNC_DOMAIN(d * d);
+            int e = trunc_small(d * d);
             if (e < be) { be = e; bq = tq; }
         }
         q[c] = bq; x8[c] = expand_bits((bq << 1) | p, n); err += be;

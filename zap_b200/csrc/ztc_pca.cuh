@@ -24,11 +24,16 @@ ZTC_DEV bool pca_power_step(const float C[NC][NC], float ax[NC]) {
     return true;
 }
 
+// a byte or a small count as a float: a conversion, or (BITS) small_u2f's logic op and add; the same value either
+// way, and which is faster depends on the kernel's other work
+template <bool BITS>
+ZTC_DEV float pca_u2f(uint32_t n) { return BITS ? small_u2f(n) : (float)n; }
+
 // t: the texels in registers (uint32_t[16]) or a TexRef; UNROLL 1 rolls the texel loops and the power iteration
-// (the same operations in the same order, in less code), UNROLL 16 unrolls them
-template <int NC, int UNROLL = 16, typename Tex>
+// (the same operations in the same order, in less code), UNROLL 16 unrolls them; U2F_BITS: pca_u2f's form
+template <int NC, int UNROLL = 16, bool U2F_BITS = true, typename Tex>
 ZTC_DEV void pca_endpoints(const Tex &t, uint32_t mask, float lo[4], float hi[4]) {
-    const float cnt = (float)popc(mask), cnti = 1.0f / cnt;
+    const float cnt = pca_u2f<U2F_BITS>((uint32_t)popc(mask)), cnti = 1.0f / cnt;
     const bool whole = mask == 0xFFFFu;  // a compile-time constant for whole-block calls: x / 16 is a multiply there
     float mu[NC];
     if (whole) {
@@ -42,14 +47,14 @@ ZTC_DEV void pca_endpoints(const Tex &t, uint32_t mask, float lo[4], float hi[4]
         });
         const uint32_t S[4] = {s02 & 0xFFFFu, s13 & 0xFFFFu, s02 >> 16, s13 >> 16};
         #pragma unroll
-        for (int c = 0; c < NC; c++) mu[c] = (float)S[c] / 16.0f;
+        for (int c = 0; c < NC; c++) mu[c] = pca_u2f<U2F_BITS>(S[c]) / 16.0f;
     } else {
         #pragma unroll
         for (int c = 0; c < NC; c++) mu[c] = 0.0f;
         for_texels<UNROLL>([&](int i) {
             if ((mask >> i) & 1u) {
                 #pragma unroll
-                for (int c = 0; c < NC; c++) mu[c] = mu[c] + div_small((float)chan(t[i], c), cnt, cnti);
+                for (int c = 0; c < NC; c++) mu[c] = mu[c] + div_small(pca_u2f<U2F_BITS>(chan(t[i], c)), cnt, cnti);
             }
         });
     }
@@ -63,7 +68,7 @@ ZTC_DEV void pca_endpoints(const Tex &t, uint32_t mask, float lo[4], float hi[4]
         if ((mask >> i) & 1u) {
             float d[NC];
             #pragma unroll
-            for (int c = 0; c < NC; c++) d[c] = (float)chan(t[i], c) - mu[c];
+            for (int c = 0; c < NC; c++) d[c] = pca_u2f<U2F_BITS>(chan(t[i], c)) - mu[c];
             #pragma unroll
             for (int a = 0; a < NC; a++)
                 #pragma unroll
@@ -92,7 +97,7 @@ ZTC_DEV void pca_endpoints(const Tex &t, uint32_t mask, float lo[4], float hi[4]
         if ((mask >> i) & 1u) {
             float s = 0.0f;
             #pragma unroll
-            for (int c = 0; c < NC; c++) s = s + ((float)chan(t[i], c) - mu[c]) * ax[c];
+            for (int c = 0; c < NC; c++) s = s + (pca_u2f<U2F_BITS>(chan(t[i], c)) - mu[c]) * ax[c];
             if (s < tl) tl = s;
             if (s > th) th = s;
         }
