@@ -295,12 +295,13 @@ ZTC_DEV uint64_t bc6_center(int16_t *tc, int stride, uint32_t &tsum) {
     return cw;
 }
 
-// The search for the CTA's blocks, one per thread, with each start's last least-squares refit compacted: every
-// thread runs its block's two starts up to the third pass; the (block, start) pairs whose fourth pass would run
-// (a tenth of them on the HDR test content, yet nearly every warp holds one) are listed in shared memory, and the
-// first threads of the CTA run those passes on the owners' texels. Same bytes as bc6h_encode_block. Every thread
-// of the CTA calls it (it synchronises); a `valid` thread's block is in column threadIdx.x of s_t / s_U, its block
-// word and tsum in s_cw[threadIdx.x] and s_ts[threadIdx.x].
+// The search for the CTA's blocks, one per thread, with each start's later passes compacted. Stage 0: every thread
+// runs its block's two starts through passes 0 and 1 (all of them do). Stage 1: the (block, start) pairs whose
+// pass 2 would run (about half of them on the HDR test content, yet nearly every warp holds several) are listed in
+// shared memory and run by the first threads; stage 2 lists and runs those whose pass 3 would run (a tenth). A
+// pair's state between stages is its shared-memory slots. Same bytes as bc6h_encode_block. Every thread of the
+// CTA calls it (it synchronises); a `valid` thread's block is in column threadIdx.x of s_t / s_U, its block word
+// and tsum in s_cw[threadIdx.x] and s_ts[threadIdx.x].
 template <int CTA>
 __device__ __forceinline__ uint4 bc6h_encode_cta(bool valid, int16_t (*s_t)[CTA], float (*s_U)[CTA], const uint64_t *s_cw, const uint32_t *s_ts) {
     __shared__ uint64_t s_ends[2][CTA], s_idx[2][CTA], s_err[2][CTA];
@@ -313,11 +314,12 @@ __device__ __forceinline__ uint4 bc6h_encode_cta(bool valid, int16_t (*s_t)[CTA]
         s_ends[0][tid] = se[0];
         s_ends[1][tid] = se[1];
     }
+    // the thread's two items of the stage (pairs as block << 1 | start) and whether each one's next pass would run
+    int item0 = tid << 1, item1 = (tid << 1) | 1, total = 0;
     bool more0 = false, more1 = false;
-    int total = 0;
     #pragma unroll 1
-    for (int job = 0; job < 4; job++) {
-        if (job == 2) {  // list the (block, start) pairs whose fourth pass would run, in thread order
+    for (int stage = 0; stage < 3; stage++) {
+        if (stage > 0) {  // list the pairs whose next pass would run: round 0's in thread order, then round 1's
             const unsigned b0 = __ballot_sync(0xFFFFFFFFu, more0), b1 = __ballot_sync(0xFFFFFFFFu, more1);
             if (lane == 0) { s_wcnt[0][warp] = __popc(b0); s_wcnt[1][warp] = __popc(b1); }
             __syncthreads();
@@ -330,32 +332,34 @@ __device__ __forceinline__ uint4 bc6h_encode_cta(bool valid, int16_t (*s_t)[CTA]
             const unsigned below = (1u << lane) - 1u;
             if (more0) {
                 const int p0 = base0 + __popc(b0 & below);
-                if (ZTC_IN_BOUNDS(p0, 2 * CTA, 4)) s_list[p0] = (uint16_t)(tid << 1);
+                if (ZTC_IN_BOUNDS(p0, 2 * CTA, 4)) s_list[p0] = (uint16_t)item0;
             }
             if (more1) {
                 const int p1 = t0 + base1 + __popc(b1 & below);
-                if (ZTC_IN_BOUNDS(p1, 2 * CTA, 4)) s_list[p1] = (uint16_t)((tid << 1) | 1);
+                if (ZTC_IN_BOUNDS(p1, 2 * CTA, 4)) s_list[p1] = (uint16_t)item1;
             }
             total = t0 + t1;
             __syncthreads();
         }
-        int owner = tid, st = job, first = 0, last = 3;
-        bool active = valid;
-        if (job >= 2) {
-            const int k = tid + (job - 2) * CTA;
-            active = k < total;
-            if (active) { owner = s_list[k] >> 1; st = s_list[k] & 1; }
+        const int first = stage == 0 ? 0 : stage + 1, last = stage + 2;
+        #pragma unroll 1
+        for (int r = 0; r < 2; r++) {
+            int it = r ? item1 : item0;
+            bool active = valid;
+            if (stage > 0) {
+                const int k = tid + r * CTA;
+                active = k < total;
+                it = active ? (int)s_list[k] : 0;
+            }
+            const int owner = it >> 1, st = it & 1;
 #ifdef ZTC_CHECKS
             if (active && !ZTC_IN_BOUNDS(owner, CTA, 8)) active = false;
 #endif
-            first = 3; last = 4;
-        }
-        if (active) {
-            // jobs 0 and 1 start from the start's endpoints, jobs 2 and 3 from the state after the third pass
-            const bool more = bc6_passes(HalfRef{&s_t[0][owner], &s_U[0][owner], CTA, s_cw[owner], s_ts[owner]}, s_ends[st][owner],
-                                         first, last, &s_ends[st][owner], &s_idx[st][owner], &s_err[st][owner]);
-            if (job == 0) more0 = more;
-            if (job == 1) more1 = more;
+            bool more = false;
+            if (active)  // stage 0 starts from the start's endpoints, later stages from the pair's state
+                more = bc6_passes(HalfRef{&s_t[0][owner], &s_U[0][owner], CTA, s_cw[owner], s_ts[owner]}, s_ends[st][owner],
+                                  first, last, &s_ends[st][owner], &s_idx[st][owner], &s_err[st][owner]);
+            if (r) { item1 = it; more1 = more; } else { item0 = it; more0 = more; }
         }
     }
     __syncthreads();
