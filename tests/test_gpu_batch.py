@@ -60,6 +60,28 @@ def test_batch_matches_oracle(cuda_lib, autotune, graph, plan):
     b.close()
 
 
+def test_batch_workload_recipe_matches_oracle(cuda_lib):
+    """The batched workload's own recipe at 256 textures (power-of-two sides 64..512, aspect <= 4:1, full sRGB mip
+    chains, 40 % BC1 / 20 % BC3 / 40 % BC7, per-texture seeds; about a quarter of its BC7 blocks take modes 5 / 1),
+    autotuned and graph-launched: every level of every texture is the reference's bytes (21.9 Mpix in all)."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    import zap_b200.synth as S
+    ref = oracle_lib.best()
+    sizes = S.batch_sizes(256, seed=0, lo=6, hi=9)
+    fmts = S.batch_formats(256, seed=0)
+    texs = [S.colour_texture(w, h, seed=10000 + k, device="cuda") for k, (w, h) in enumerate(sizes)]
+    b = cuda_lib.Batch(texs, fmts, autotune=True)
+    b.run()
+    torch.cuda.synchronize()
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as pool:  # the oracle's calls release the GIL
+        list(pool.map(lambda i: _check_item(b, i, ref, True), range(len(texs))))
+    b.close()
+
+
 def test_batch_replay_reads_new_inputs_and_plain_path_agrees(cuda_lib):
     import torch
     ref = oracle_lib.best()
