@@ -71,6 +71,14 @@ def test_benchmark_textures_match_reference(cuda_lib):
     wide[..., 0], wide[..., 3] = host[..., 0], 255
     assert np.array_equal(cuda_lib.bc_encode_dev(opaque[..., :1].contiguous(), BC4).cpu().numpy(),
                           ref.bc_encode(wide, BC4, threads=THREADS))
+    # BC7 on the opaque texture: few blocks leave mode 6 (at most one per CTA of the modes-5/1 launch)
+    assert np.array_equal(cuda_lib.bc_encode_dev(opaque, BC7).cpu().numpy(), ref.bc_encode(host, BC7, threads=THREADS))
+    # BC7 on an atlas of 1024 textures of 64x64 in a seeded order: a quarter of the blocks leave mode 6, several
+    # rounds per CTA of the modes-5/1 launch
+    tiles = torch.stack([S.colour_texture(64, 64, seed=30000 + k, device=dev) for k in range(1024)])
+    perm = torch.randperm(1024, generator=torch.Generator().manual_seed(0)).to(dev)
+    atlas = tiles[perm].view(32, 32, 64, 64, 4).permute(0, 2, 1, 3, 4).reshape(2048, 2048, 4).contiguous()
+    assert np.array_equal(cuda_lib.bc_encode_dev(atlas, BC7).cpu().numpy(), ref.bc_encode(atlas.cpu().numpy(), BC7, threads=THREADS))
 
 
 def _huge_image(w, h, device):

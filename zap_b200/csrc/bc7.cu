@@ -459,11 +459,12 @@ ZTC_DEV bool rank_less(float e, int p, float e2, int p2) { return e < e2 || (!(e
 constexpr int kBc7Group = 8;
 constexpr int kMode1Tries = 4;  // partitions fully fitted after ranking (ZAP__BC7_M1K, zap_tex.h:750-752)
 
-// Mode 1 of one opaque block (zap_tex.h:764-783) by the 8 lanes of a group (lane l, group mask gmask): true, with err
-// and blk updated, when the best of the ranked partitions has an SSE below err. Every lane holds the block's texels
-// t, so all group-level branches are group-uniform; ts: the group's shared-memory copy of them.
-__device__ __forceinline__ bool bc7_group_mode1(const uint32_t t[16], TexRef ts, int &err, uint4 &blk, const int l,
-                                                const unsigned gmask) {
+__device__ __forceinline__ bool mode1_fits(TexRef ts, const int cand[kMode1Tries], int &err, uint4 &blk, const int l, const unsigned gmask);
+
+// Mode 1's ranking of one opaque block (zap_tex.h:764-775) by the 8 lanes of a group (lane l, group mask gmask):
+// cand[0..3] the partitions of the four least (score, partition), -1 past the last valid one (group-uniform).
+// ts: the block's texels (the group's shared-memory copy).
+__device__ __forceinline__ void group_rank(TexRef ts, int cand[kMode1Tries], const int l, const unsigned gmask) {
     // ---- mode 1 ranking: lane scores partitions l, l + 8, ..., l + 56 (zap_tex.h:764-775), four per round:
     // one pass over the texels adds each texel's 9 moments to the block totals and to the sums of the
     // four partitions' subset 1, every sum in texel order as the reference adds them
@@ -523,7 +524,6 @@ __device__ __forceinline__ bool bc7_group_mode1(const uint32_t t[16], TexRef ts,
         }
     }
     // merge the eight sorted lists: four rounds of a group-wide (score, partition) minimum
-    int cand[kMode1Tries];
     #pragma unroll
     for (int j = 0; j < kMode1Tries; j++) {
         float he = ce[0];
@@ -541,7 +541,68 @@ __device__ __forceinline__ bool bc7_group_mode1(const uint32_t t[16], TexRef ts,
             ce[kMode1Tries - 1] = 1e30f; cp[kMode1Tries - 1] = 64;
         }
     }
-    // ---- mode 1 fits: lane = candidate * 2 + subset (zap_tex.h:687-708, 776)
+}
+
+// Mode 1 of one opaque block (zap_tex.h:764-783) by the 8 lanes of a group: true, with err and blk updated, when the
+// best of the ranked partitions has an SSE below err
+__device__ __forceinline__ bool bc7_group_mode1(TexRef ts, int &err, uint4 &blk, const int l, const unsigned gmask) {
+    int cand[kMode1Tries];
+    group_rank(ts, cand, l, gmask);
+    return mode1_fits(ts, cand, err, blk, l, gmask);
+}
+
+// Mode 1's ranking of one opaque block by all 64 threads of a CTA, one partition each (tid = partition; the same
+// sums, scores and order as group_rank), then four rounds of a CTA-wide (score, partition) minimum; for lists of at
+// most one block per CTA, where a block's ranking by one group (8 partitions per lane) is the longest chain of the
+// launch. Every thread of the CTA calls it; s_e, s_p: two slots each.
+__device__ __forceinline__ void cta_rank64(TexRef ts, int cand[kMode1Tries], float *s_e, int *s_p) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t pm = kP2[tid];
+    float s1[9], tot[9];
+    int n1 = 0;
+    #pragma unroll
+    for (int j = 0; j < 9; j++) { s1[j] = 0.0f; tot[j] = 0.0f; }
+    #pragma unroll 1
+    for (int i = 0; i < 16; i++) {
+        const uint32_t x = ts[i];
+        const float rr = small_u2f(chan(x, 0)), gg = small_u2f(chan(x, 1)), bb = small_u2f(chan(x, 2));
+        const float mo[9] = {rr, gg, bb, rr * rr, gg * gg, bb * bb, rr * gg, rr * bb, gg * bb};
+        #pragma unroll
+        for (int j = 0; j < 9; j++) tot[j] = tot[j] + mo[j];
+        if ((pm >> i) & 1u) {
+            n1++;
+            #pragma unroll
+            for (int j = 0; j < 9; j++) s1[j] = s1[j] + mo[j];
+        }
+    }
+    const float e = partition_score(s1, n1, tot);
+    const bool valid = e < 1e30f;  // NaN and >= 1e30 never enter, as in the reference
+    float me = valid ? e : 1e30f;
+    int mp = valid ? tid : 64;
+    #pragma unroll 1
+    for (int j = 0; j < kMode1Tries; j++) {
+        float he = me;
+        int hp = mp;
+        #pragma unroll
+        for (int m = 16; m >= 1; m >>= 1) {
+            const float oe = __shfl_xor_sync(0xFFFFFFFFu, he, m);
+            const int op = __shfl_xor_sync(0xFFFFFFFFu, hp, m);
+            if (rank_less(oe, op, he, hp)) { he = oe; hp = op; }
+        }
+        if (lane == 0) { s_e[warp] = he; s_p[warp] = hp; }
+        __syncthreads();
+        const bool second = rank_less(s_e[1], s_p[1], s_e[0], s_p[0]);
+        const int bp = second ? s_p[1] : s_p[0];
+        cand[j] = bp < 64 ? bp : -1;
+        if (bp < 64 && bp == tid) { me = 1e30f; mp = 64; }  // taken
+        __syncthreads();  // the slots are written again next round
+    }
+}
+
+// Mode 1's fits of the ranked partitions cand[0..3] (-1: none) by the 8 lanes of a group, lane = candidate * 2 +
+// subset (zap_tex.h:687-708, 776): true, with err and blk updated, when the first candidate of the least SSE is
+// below err. cand is group-uniform.
+__device__ __forceinline__ bool mode1_fits(TexRef ts, const int cand[kMode1Tries], int &err, uint4 &blk, const int l, const unsigned gmask) {
     const int j = l >> 1, sub = l & 1;
     int pj = 0;
     #pragma unroll
@@ -693,18 +754,22 @@ __global__ void __launch_bounds__(64, ZTC_MINB_BC7_MODE5) bc7_hard_kernel(SrcU8 
     __shared__ int s_cerr[kHardBlocks][4], s_aerr[kHardBlocks][4];
     __shared__ uint32_t s_cq[kHardBlocks][4], s_cq2[kHardBlocks][4], s_ci[kHardBlocks][4], s_aq[kHardBlocks][4], s_ai[kHardBlocks][4];
     __shared__ int s_op[64], s_wcnt[2];          // pass 2: the list positions of a chunk's opaque blocks
+    __shared__ float s_re[2];                    // cta_rank64's slots
+    __shared__ int s_rp[2];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = (int)*(volatile const uint32_t *)count;
-    // one round per CTA at most (short lists): pass 2 finds the round's blocks in shared memory
-    const bool one_round = n <= (int)gridDim.x * kHardBlocks;
-    // ---- pass 1, mode 5 (zap_tex.h:659-684) of every listed block the CTA holds, 8 per round: warp 0 fits the
+    // one round per CTA at most (short lists): pass 2 finds the round's blocks in shared memory; one block per CTA at
+    // most (the shortest lists): that block's mode-1 ranking takes all 64 threads (these tests are grid-uniform)
+    const bool one_round = n <= (int)gridDim.x * kHardBlocks, sparse = n <= (int)gridDim.x;
+    const int per = sparse ? 1 : kHardBlocks;  // listed blocks per CTA and round
+    // ---- pass 1, mode 5 (zap_tex.h:659-684) of every listed block the CTA holds, `per` per round: warp 0 fits the
     // colour parts and warp 1 the alpha parts, lane = block * 4 + rotation; the block is stored when mode 5 wins, and
     // its list entry keeps its SSE so far and, in bit 31 of the index, whether it is opaque (mode 1 is next)
-    for (int base = blockIdx.x * kHardBlocks; base < n; base += gridDim.x * kHardBlocks) {
+    for (int base = blockIdx.x * per; base < n; base += gridDim.x * per) {
         if (tid < kHardBlocks) {  // one thread per block gathers its texels (16-byte row loads)
             const int it = base + tid;
             uint2 item = make_uint2(0xFFFFFFFFu, 0u);
-            if (it < n) {
+            if (tid < per && it < n) {
                 item = items[it];
                 uint32_t t[16];
                 gather_block(src, (int)item.x % bw, by0 + (int)item.x / bw, t);
@@ -754,10 +819,11 @@ __global__ void __launch_bounds__(64, ZTC_MINB_BC7_MODE5) bc7_hard_kernel(SrcU8 
     // entries are read 64 at a time (its next 8 rounds) and the opaque ones compacted, so every group has a block
     // while any is left. Each warp runs one mode for long stretches instead of alternating with mode 5 every round
     // (an atlas of 64x64 textures, a quarter of its blocks listed: 0.98 -> 0.80 ms per 2048x2048 encode). After a
-    // single round the blocks are still in shared memory, and group g takes slot g.
+    // single round the blocks are still in shared memory, and group g takes slot g; with one block per CTA, the
+    // whole CTA ranks its partitions and group 0 fits the four best.
     const int g = tid / kBc7Group, l = tid & (kBc7Group - 1);
     const unsigned gmask = 0xFFu << (lane & ~(kBc7Group - 1));
-    for (int chunk = 0; (blockIdx.x + 8 * chunk * gridDim.x) * kHardBlocks < n; chunk++) {  // CTA-uniform
+    for (int chunk = 0; (blockIdx.x + 8 * chunk * gridDim.x) * per < n; chunk++) {  // CTA-uniform
         int total = kHardBlocks;  // one round: group g takes slot g, whose own flag decides
         if (!one_round) {
             const int it = (blockIdx.x + (8 * chunk + (tid >> 3)) * gridDim.x) * kHardBlocks + (tid & 7);
@@ -772,24 +838,28 @@ __global__ void __launch_bounds__(64, ZTC_MINB_BC7_MODE5) bc7_hard_kernel(SrcU8 
         }
         for (int k = g; k - g < total; k += kHardBlocks) {  // group-uniform: rounds of one block per group
             uint2 item = make_uint2(0xFFFFFFFFu, 0u);
-            int j = k;
-            if (one_round) item = s_item[k];
-            else if (k < total) { j = s_op[k]; item = items[j]; }
-            if (item.x != 0xFFFFFFFFu && (item.x >> 31) != 0u) {
-                const int b = (int)(item.x & 0x7FFFFFFFu);
-                uint32_t t[16];
-                TexRef ts{s_tex[g], 1};
-                if (one_round) {
-                    #pragma unroll
-                    for (int i = 0; i < 16; i++) t[i] = s_tex[g][i];
-                } else {
+            if (sparse) item = s_item[0];  // CTA-uniform
+            else if (one_round) item = s_item[k];
+            else if (k < total) item = items[s_op[k]];
+            bool go = item.x != 0xFFFFFFFFu && (item.x >> 31) != 0u;
+            const int slot = sparse ? 0 : g;
+            TexRef ts{s_tex[slot], 1};
+            int cand[kMode1Tries];
+            if (sparse) {
+                if (go) cta_rank64(ts, cand, s_re, s_rp);  // every thread of the CTA
+                go = go && g == 0;
+            } else if (go) {
+                if (!one_round) {
+                    const int b = (int)(item.x & 0x7FFFFFFFu);
+                    uint32_t t[16];
                     gather_block(src, b % bw, by0 + b / bw, t);
                     ts = stage_group_texels(s_tex[g], t, l, gmask);
                 }
-                int err = (int)item.y;
-                uint4 blk = make_uint4(0, 0, 0, 0);
-                if (bc7_group_mode1(t, ts, err, blk, l, gmask) && l == 0) put_block16(out, b0 + (size_t)b, blk);
+                group_rank(ts, cand, l, gmask);
             }
+            int err = (int)item.y;
+            uint4 blk = make_uint4(0, 0, 0, 0);
+            if (go && mode1_fits(ts, cand, err, blk, l, gmask) && l == 0) put_block16(out, b0 + (size_t)(item.x & 0x7FFFFFFFu), blk);
         }
         if (!one_round) __syncthreads();  // s_op, s_wcnt and s_tex are written again by the next chunk
     }
@@ -961,7 +1031,7 @@ batch_bc7_mode1_kernel(const BatchLevel *__restrict__ levels, const uint32_t *__
             const TexRef ts = stage_group_texels(gtex, t, l, gmask);
             int err = (int)item.y;
             uint4 blk = make_uint4(0, 0, 0, 0);
-            if (bc7_group_mode1(t, ts, err, blk, l, gmask) && l == 0) put_block16(BlockOut{L.dst, 0, 4, 0}, (size_t)b, blk);
+            if (bc7_group_mode1(ts, err, blk, l, gmask) && l == 0) put_block16(BlockOut{L.dst, 0, 4, 0}, (size_t)b, blk);
         }
     }
 }
