@@ -3,10 +3,12 @@
 // Two kernels over a device work list:
 //   A  one thread per block: mode 6 (PCA start, p-bit search, two least-squares refits). Blocks whose SSE is
 //      <= 64 are final (the reference's early exit, zap_tex.h:758); the others are appended to a work list.
-//   B  one 8-lane group per listed block:
-//        mode 5  lane = (rotation, colour|alpha): 8 independent part fits, combined per rotation;
-//        mode 1  the 64 partitions are scored 8 per lane, the top 4 by (score, partition) are merged across the
-//                group, then lane = (candidate, subset) fits the 8 subsets.
+//   B  over the listed blocks, in two passes per CTA:
+//        mode 5  8 blocks per round, lane = block * 4 + rotation, the colour parts on one warp and the alpha parts
+//                on the other, combined per rotation;
+//        mode 1  the opaque ones, an 8-lane group per block: the 64 partitions are scored 8 per lane, the top 4 by
+//                (score, partition) are merged across the group, then lane = (candidate, subset) fits the 8
+//                subsets; with at most one listed block per CTA, the CTA's 64 threads score one partition each.
 //      Decoded SSE checks of the reference (zap__bc7_err, zap_tex.h:761,780) equal the fit SSE here: the expand and
 //      interpolation are the decoder's, anchor swaps preserve decoded values because every weight table satisfies
 //      w(n-1-j) = 64 - w(j), mode 1 shares its p-bit between a subset's endpoints, and mode 1 decodes alpha 255
