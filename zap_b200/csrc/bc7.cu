@@ -556,7 +556,8 @@ __device__ __forceinline__ bool bc7_group_mode1(TexRef ts, int &err, uint4 &blk,
 // Mode 1's ranking of one opaque block by all 64 threads of a CTA, one partition each (tid = partition; the same
 // sums, scores and order as group_rank), then four rounds of a CTA-wide (score, partition) minimum; for lists of at
 // most one block per CTA, where a block's ranking by one group (8 partitions per lane) is the longest chain of the
-// launch. Every thread of the CTA calls it; s_e, s_p: two slots each.
+// launch. The CTA has 64 threads (two warps, one partition per thread), and every one of them calls it (it
+// synchronises); s_e, s_p: two slots each. cand is the same in every thread.
 __device__ __forceinline__ void cta_rank64(TexRef ts, int cand[kMode1Tries], float *s_e, int *s_p) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t pm = kP2[tid];
