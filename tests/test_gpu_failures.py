@@ -5,7 +5,8 @@
   hook cleared, must succeed with the reference's bytes. The batch planner is failed at each of its allocations in
   turn and must release what it had taken each time.
 - The bounds-check build (libzap_tex_cuda_checks.so, -DZTC_CHECKS) runs small odd-size cases of every encoder in a
-  child process; its output must equal the oracle's and its device check word must stay 0.
+  child process, and every device entry point on a texture past that build's 4096 blocks per launch (so the encode
+  runs as several launches); its output must equal the oracle's and its device check word must stay 0.
 No kernel faults, traps or waits in any of these: the failures are made by the host.
 """
 import ctypes as C
@@ -118,6 +119,17 @@ for img in imgs:
 hdr = np.ones((19, 27, 4), np.float32)
 hdr[..., :3] = S.hdr_texture(27, 19, seed=4).numpy().astype(np.float32)
 assert np.array_equal(zap_b200.bc6h_encode(hdr), ref.bc6h_encode(hdr))
+# device entry points on 75 x 66 blocks: more than the build's 4096 blocks per launch, so each encode runs as two
+# launches of whole block rows
+big = S.colour_texture(300, 261, seed=5, alpha="noise")
+bg = big.cuda()
+for fmt in range(5):
+    assert np.array_equal(zap_b200.bc_encode_dev(bg, fmt).cpu().numpy(), ref.bc_encode(big.numpy(), fmt)), ("dev", fmt)
+assert np.array_equal(zap_b200.astc_encode_dev(bg).cpu().numpy(), ref.astc_encode(big.numpy()))
+half = S.hdr_texture(300, 261, seed=6)
+f32 = np.ones((261, 300, 4), np.float32)
+f32[..., :3] = half.numpy().astype(np.float32)
+assert np.array_equal(zap_b200.bc6h_encode_dev(half.cuda()).cpu().numpy(), ref.bc6h_encode(f32))
 texs = [torch.from_numpy(i).cuda() for i in imgs]
 b = zap_b200.Batch(texs, [4, 0, 1, 4], plan=("tiles_2d", "tile_x2"))
 b.run(); torch.cuda.synchronize(); b.close()

@@ -4,6 +4,7 @@
 // of block rows and pipelined over two streams, so the host->device copy of one band overlaps the kernels and
 // the device->host copy of the previous one. Device-pointer (_dev) calls enqueue on the caller's stream and take
 // their scratch from the stream-ordered allocator, so concurrent calls on different streams do not share it.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -291,12 +292,27 @@ int host_encode(zap_tex_cuda_ctx *ctx, int fmt, const void *src, int w, int h, s
     return st;
 }
 
+// Blocks per encode launch at most (whole block rows): the kernels index a launch's blocks with 32-bit ints, and a
+// texture a B200 can hold may have more than 2^31 blocks (2^31 blocks of RGBA8 are 128 GB of texels). The
+// bounds-check build uses a small limit, so its tests run the chunked path on small images.
+#ifndef ZTC_LAUNCH_BLOCKS
+#ifdef ZTC_CHECKS
+#define ZTC_LAUNCH_BLOCKS 4096
+#else
+#define ZTC_LAUNCH_BLOCKS (1 << 30)
+#endif
+#endif
+
 int dev_encode(zap_tex_cuda_ctx *ctx, int fmt, const ztc::SrcU8 &s8, const ztc::SrcHdr *sh, int w, int h, void *out, cudaStream_t s) {
     const int bh = (h + 3) / 4, bw = (w + 3) / 4;
-    const size_t scr = scratch_for(fmt, (size_t)bw * bh);
+    const int rows = (int)std::min<size_t>((size_t)bh, std::max<size_t>(1, (size_t)ZTC_LAUNCH_BLOCKS / (size_t)bw));  // per launch
+    const size_t bs = fmt == ZTC_BC6H || fmt == ZTC_ASTC4X4 ? 16 : block_bytes(fmt);
+    const size_t scr = scratch_for(fmt, (size_t)bw * rows);
     void *scratch = nullptr;
     if (scr) ZTC_CHECK(ztc_malloc_async(&scratch, scr, s), "cudaMallocAsync(scratch)");
-    int st = launch_encode(fmt, s8, sh, 0, bh, (uint8_t *)out, scratch, s);
+    int st = ZTC_OK;
+    for (int y = 0; y < bh && !st; y += rows)  // launches on one stream, so they share the scratch in turn
+        st = launch_encode(fmt, s8, sh, y, rows < bh - y ? rows : bh - y, (uint8_t *)out + (size_t)y * bw * bs, scratch, s);
     if (scratch) cudaFreeAsync(scratch, s);
     (void)ctx;
     return st;
