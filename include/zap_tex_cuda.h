@@ -254,9 +254,9 @@ ZTC_API int zap_tex_cuda_debug_fail_allocations(int skip, int count);
 ZTC_API int zap_tex_cuda_debug_checks(unsigned int *first_failure);
 
 /* Allocation-free BC7 encode. No counterpart in the reference (zap_tex.h allocates nothing because it runs on the
-   CPU); it exists for callers that cannot allocate device memory when they encode: work recorded into a CUDA
-   graph, real-time frame loops, engines with a fixed up-front GPU budget, plug-in hosts that only hand over their
-   own buffers. Same bytes as zap_tex_cuda_bc_encode_dev(..., ZTC_BC7, ...), device pointers, async on `stream`.
+   CPU); it exists for callers that cannot allocate device memory when they encode: real-time frame loops where an
+   allocation would stall or is not allowed, engines with a fixed up-front GPU budget, plug-in hosts that only hand
+   over their own buffers. Same bytes as zap_tex_cuda_bc_encode_dev(..., ZTC_BC7, ...), device pointers, async on `stream`.
    It never calls cudaMalloc/cudaFree: its work list is a static device array sized for at most 1048576 4x4
    blocks (4096 x 4096 texels, about 8 MB held by every GPU that loads the library); larger textures return
    ZTC_ERR_INVALID_ARG. The first call on a device looks up that array's address (make it before any stream

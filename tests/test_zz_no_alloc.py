@@ -1,7 +1,7 @@
 """The allocation-free BC7 entry point (zap_tex_cuda_bc7_encode_noalloc_dev), through the C ABI.
 
-Some callers cannot allocate device memory while they encode - work recorded into a CUDA graph, real-time frame
-loops, engines with a fixed up-front GPU budget, plug-in hosts that only hand over their own buffers. This entry
+Some callers cannot allocate device memory while they encode - real-time frame loops where an allocation would
+stall, engines with a fixed up-front GPU budget, plug-in hosts that only hand over their own buffers. This entry
 point keeps its BC7 work list in a static device array instead of allocating one. Its output must be byte-for-byte
 the output of the allocating entry point, also on consecutive calls that share that array (the list must start
 empty every time), and oversize textures must be refused before anything runs. At exactly its limit (4096 x 4096

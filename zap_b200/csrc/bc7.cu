@@ -1101,8 +1101,8 @@ cudaError_t ztc_launch_bc7(const ztc::SrcU8 &src, int by0, int nby, uint8_t *out
 }
 
 // ---------------------------------------------------------------- allocation-free BC7 entry point
-// Some callers cannot allocate device memory at encode time: code running inside a CUDA graph capture or a
-// real-time frame loop where an allocation would stall or be forbidden, engines that own a fixed GPU memory
+// Some callers cannot allocate device memory at encode time: code running inside a real-time frame loop where an
+// allocation would stall or be forbidden, engines that own a fixed GPU memory
 // budget handed out up front, or plug-in hosts that give a texture tool only the buffers it is called with.
 // zap_tex_cuda_bc7_encode_noalloc_dev serves them: its BC7 work list lives in the file-scope array below, sized
 // for at most kNoAllocMaxBlocks 4x4 blocks (a 4096 x 4096 texture), which every GPU that loads this library holds
