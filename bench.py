@@ -33,7 +33,7 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 METRIC = "BC1/BC7 encode Mpix/s on 1 B200 at ref PSNR; batched vs plain launch; vs CPU"
 W, H = 2048, 2048
-WORKLOAD = "bc7 2048x2048 rgba8, colour gradients + value noise + rectangles, noise alpha (config 1)"
+WORKLOAD = "bc7 2048x2048 rgba8, colour gradients + value noise + rectangles, noise alpha"
 
 
 def parse():
@@ -635,8 +635,8 @@ def hbm_workloads(dev, side=4096, ring=4):
 
 
 def batched_workload(args, dev, n=4096):
-    """Config 2: n textures, power-of-two sides 64..2048 (log-uniform, aspect <= 4:1), full sRGB mip chains,
-    40% BC1 / 20% BC3 / 40% BC7, content as config 0 per texture seed. One autotuned graph launch per step against
+    """Batched encode: n textures, power-of-two sides 64..2048 (log-uniform, aspect <= 4:1), full sRGB mip chains,
+    40% BC1 / 20% BC3 / 40% BC7, opaque colour-texture content per texture seed. One autotuned graph launch per step against
     the same work as one plain launch per texture and per level (issued natively, no Python in the loop)."""
     import torch
 
@@ -717,7 +717,7 @@ def bc7_modes(blocks):
 
 
 def refine_workload(args, dev, n=1024, side=256, steps=8, lr=1.0):
-    """Config 4: n textures of side^2 (config 0 content, per-texture seed), BC1 and BC7; the encoder's blocks then
+    """Refinement: n textures of side^2 (opaque colour-texture content, per-texture seed), BC1 and BC7; the encoder's blocks then
     `steps` Adam steps of gradient endpoint refinement through the palette-decode adjoint, accepted per block only
     if the error drops. Textures are stacked into one image: blocks are independent, so this is n encodes at once.
     BC7's gain is split by the blocks' mode (6, 5, 1); its cost is also timed on an atlas of 64x64 textures, where
@@ -803,8 +803,8 @@ def log2_psnr(src, dec):
 
 
 def extra_workloads(args, dev, sm_mhz=None, sms=148):
-    """Secondary figures, one entry per format and input: BC1 (config 0 512^2, and 2048^2), BC4 R8 / BC5 RG8
-    (config 1), BC6H / ASTC (config 3), and BC7 on content where many blocks go past mode 6 (opaque 2048^2, and an
+    """Secondary figures, one entry per format and input: BC1 (512^2 from seed 0, and 2048^2), BC4 R8 / BC5 RG8
+    (2048^2), BC6H / ASTC (2048^2), and BC7 on content where many blocks go past mode 6 (opaque 2048^2, and an
     atlas of 64^2 textures). Each entry has, beside its device figure (CUDA events, inputs resident): the fraction of
     blocks identical to the reference encoder on the first ring texture, the PSNR of both outputs (as the reference's
     tex_bench.c:200-214 table prints it), and the reference's CPU figure on that texture, on all host threads
@@ -904,7 +904,7 @@ def extra_workloads(args, dev, sm_mhz=None, sms=148):
             res[name]["speedup_vs_cpu_all_threads"] = mps / cpu["value"]
         del texs, outs
 
-    bench("bc1_512x512_config0", lambda k: S.colour_texture(512, 512, seed=k, device=dev), zap_b200.BC1, 512 * 512, 64, 4.5)
+    bench("bc1_512x512_seed0", lambda k: S.colour_texture(512, 512, seed=k, device=dev), zap_b200.BC1, 512 * 512, 64, 4.5)
     bench("bc1_2048x2048", lambda k: S.colour_texture(2048, 2048, seed=k, device=dev), zap_b200.BC1, 2048 * 2048, 10, 4.5,
           counted="bc1_encode")
     bench("bc4_2048x2048_r8", lambda k: S.colour_texture(2048, 2048, seed=k, device=dev)[..., :1].contiguous(), zap_b200.BC4,
